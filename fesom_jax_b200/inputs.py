@@ -1,0 +1,177 @@
+"""Seeded synthetic inputs for the FCT path (host numpy, float64).
+
+The reference drives ``advect_one_fct`` from a full model step; here the inputs are
+generated directly with the shapes, layouts and value ranges the workloads name:
+
+  * rest layer thicknesses from ``zbar`` (fesom_jax/state.py:165-187):
+    ``hnode[n,k] = zbar[k]-zbar[k+1]`` on wet layers, ``helem`` likewise, 0 elsewhere;
+  * ``T`` 2-28 degC decreasing with the layer mid-depth ``Z`` plus N(0, 0.5) noise,
+    ``S`` 34-36 psu increasing with depth plus N(0, 0.1), both 0 below the bottom;
+  * element velocities ``u, v ~ N(0, sigma)`` with a linear decay with depth, masked
+    to each element's layers;
+  * ``w`` from discrete continuity, :func:`compute_w` (fesom_jax/ale.py:309-365).
+"""
+
+from __future__ import annotations
+
+import dataclasses
+
+import numpy as np
+
+from .mesh import Mesh, R_EARTH
+
+
+def rest_thickness(mesh: Mesh):
+    """``(hnode [N,nl], helem [E,nl])`` rest thicknesses (fesom_jax/state.py:165-187)."""
+    nl = mesh.nl
+    dz = np.zeros(nl)
+    dz[:-1] = mesh.zbar[:-1] - mesh.zbar[1:]
+    hnode = np.where(mesh.node_layer_mask, dz[None, :], 0.0)
+    helem = np.where(mesh.elem_layer_mask, dz[None, :], 0.0)
+    return hnode, helem
+
+
+def layer_depth_fraction(mesh: Mesh) -> np.ndarray:
+    """``|Z_k| / max|Z|`` per layer ``k`` (``[nl]``; the last slot repeats ``Z[-1]``)."""
+    Zp = np.concatenate([mesh.Z, mesh.Z[-1:]])
+    return np.abs(Zp) / np.max(np.abs(Zp))
+
+
+def compute_w(mesh: Mesh, uv: np.ndarray, helem: np.ndarray) -> np.ndarray:
+    """Vertical velocity at interfaces ``[N, nl]`` from continuity.
+
+    Restates fesom_jax/ale.py:309-365: per-level antisymmetric edge->node divergence
+    scatter of ``(v*dx - u*dy)*h`` (minus the second cell's), a bottom-to-top suffix
+    sum over levels, division by ``area`` (safe where 0) and the interface mask.
+    """
+    et = mesh.edge_tri
+    el1, el2 = et[:, 0], et[:, 1]
+    has1, has2 = el1 >= 0, el2 >= 0
+    e1 = np.where(has1, el1, 0)
+    e2 = np.where(has2, el2, 0)
+    cr = mesh.edge_cross_dxdy
+    U, V = uv[:, :, 0], uv[:, :, 1]
+    lm = mesh.elem_layer_mask
+    t1 = np.where(lm[e1] & has1[:, None],
+                  (V[e1] * cr[:, 0:1] - U[e1] * cr[:, 1:2]) * helem[e1], 0.0)
+    t2 = np.where(lm[e2] & has2[:, None],
+                  (V[e2] * cr[:, 2:3] - U[e2] * cr[:, 3:4]) * helem[e2], 0.0)
+    c = t1 - t2
+    div = np.zeros((mesh.nod2D, mesh.nl))
+    np.add.at(div, mesh.edges[:, 0], c)
+    np.add.at(div, mesh.edges[:, 1], -c)
+    w = np.flip(np.cumsum(np.flip(div, axis=1), axis=1), axis=1)
+    w = w / np.where(mesh.area > 0.0, mesh.area, 1.0)
+    return np.where(mesh.node_iface_mask, w, 0.0)
+
+
+def tracer_profiles(mesh: Mesh, rng: np.random.Generator):
+    """``(T, S)`` ``[N, nl]``: depth profiles plus seeded noise, 0 below the bottom."""
+    frac = layer_depth_fraction(mesh)[None, :]
+    shape = (mesh.nod2D, mesh.nl)
+    T = 28.0 - 26.0 * frac + rng.normal(0.0, 0.5, shape)
+    S = 34.0 + 2.0 * frac + rng.normal(0.0, 0.1, shape)
+    m = mesh.node_layer_mask
+    return np.where(m, T, 0.0), np.where(m, S, 0.0)
+
+
+def passive_tracer(mesh: Mesh, rng: np.random.Generator) -> np.ndarray:
+    """A passive tracer ``U[0, 1]`` on wet layers, 0 below the bottom."""
+    return np.where(mesh.node_layer_mask, rng.uniform(0.0, 1.0, (mesh.nod2D, mesh.nl)), 0.0)
+
+
+def element_centres(mesh: Mesh):
+    """Element centroid (lon, lat) in rotated radians, cyclic-safe in lon."""
+    lon = mesh.coord_nod2D[:, 0][mesh.elem_nodes]
+    lat = mesh.coord_nod2D[:, 1][mesh.elem_nodes]
+    half = 0.5 * 2.0 * np.pi
+    d = lon - lon[:, :1]
+    lon = np.where(d > half, lon - 2 * np.pi, np.where(d < -half, lon + 2 * np.pi, lon))
+    return lon.mean(axis=1), lat.mean(axis=1)
+
+
+def velocities(mesh: Mesh, rng: np.random.Generator, sigma: float = 0.1,
+               n_vortices: int = 0, vortex_radius_km=(50.0, 200.0),
+               vortex_speed: float = 0.5) -> np.ndarray:
+    """Element velocities ``uv [E, nl, 2]`` (m/s).
+
+    ``u, v ~ N(0, sigma)`` per element, times a linear decay ``1 - 0.9*|Z_k|/max|Z|``,
+    masked to each element's layers. ``n_vortices > 0`` adds seeded Gaussian eddies
+    (azimuthal speed ``vortex_speed * r/R * exp(1/2 - r^2/(2R^2))``, radius ``R`` drawn
+    from ``vortex_radius_km``) centred on random elements.
+    """
+    E, nl = mesh.elem2D, mesh.nl
+    decay = 1.0 - 0.9 * layer_depth_fraction(mesh)
+    base = rng.normal(0.0, sigma, (E, 2))
+    if n_vortices:
+        lon, lat = element_centres(mesh)
+        xyz = np.stack([np.cos(lat) * np.cos(lon), np.cos(lat) * np.sin(lon), np.sin(lat)], 1)
+        east = np.stack([-np.sin(lon), np.cos(lon), np.zeros_like(lon)], 1)
+        north = np.stack([-np.sin(lat) * np.cos(lon), -np.sin(lat) * np.sin(lon), np.cos(lat)], 1)
+        centres = rng.integers(0, E, n_vortices)
+        radii = rng.uniform(*vortex_radius_km, n_vortices) * 1e3
+        signs = rng.choice([-1.0, 1.0], n_vortices)
+        for c, R, s in zip(centres, radii, signs):
+            cx = xyz[c]
+            cosang = np.clip(xyz @ cx, -1.0, 1.0)
+            r = R_EARTH * np.arccos(cosang)
+            near = r < 4.0 * R
+            if not np.any(near):
+                continue
+            # tangent direction: the centre axis crossed with the position vector
+            t = np.cross(cx[None, :], xyz[near])
+            tn = np.linalg.norm(t, axis=1, keepdims=True)
+            t = t / np.where(tn > 0, tn, 1.0)
+            speed = s * vortex_speed * (r[near] / R) * np.exp(0.5 - 0.5 * (r[near] / R) ** 2)
+            base[near, 0] += speed * np.sum(t * east[near], 1)
+            base[near, 1] += speed * np.sum(t * north[near], 1)
+    uv = base[:, None, :] * decay[None, :, None]
+    return np.where(mesh.elem_layer_mask[:, :, None], uv, 0.0)
+
+
+@dataclasses.dataclass
+class Fields:
+    """One FCT instance's inputs (host numpy, reference layouts)."""
+
+    uv: np.ndarray          # [E, nl, 2]
+    w_e: np.ndarray         # [N, nl]
+    helem: np.ndarray       # [E, nl]
+    hnode: np.ndarray       # [N, nl]
+    hnode_new: np.ndarray   # [N, nl]
+    tracers: np.ndarray     # [ntr, N, nl]  (T, then S, then passives)
+    tracers_old: np.ndarray  # [ntr, N, nl]
+
+
+def make_fields(mesh: Mesh, seed: int = 0, n_passive: int = 0, sigma: float = 0.1,
+                ab2: bool = False, n_vortices: int = 0, uv: np.ndarray | None = None,
+                tracers: np.ndarray | None = None) -> Fields:
+    """Seeded inputs for one instance: T, S (+ passive tracers), velocities, ``w``.
+
+    ``ab2=False`` gives ``T_old = T`` (step-1 convention, fesom_jax/ic.py:91-110);
+    ``ab2=True`` perturbs ``T_old`` so the AB2 extrapolation is exercised.
+    """
+    rng = np.random.default_rng(seed)
+    if tracers is None:
+        T, S = tracer_profiles(mesh, rng)
+        tr = [T, S] + [passive_tracer(mesh, rng) for _ in range(n_passive)]
+        tracers = np.stack(tr)
+    hnode, helem = rest_thickness(mesh)
+    if uv is None:
+        uv = velocities(mesh, rng, sigma=sigma, n_vortices=n_vortices)
+    w = compute_w(mesh, uv, helem)
+    if ab2:
+        pert = rng.normal(0.0, 0.05, tracers.shape) * mesh.node_layer_mask[None]
+        old = tracers + pert
+    else:
+        old = tracers.copy()
+    return Fields(uv=uv, w_e=w, helem=helem, hnode=hnode, hnode_new=hnode.copy(),
+                  tracers=np.ascontiguousarray(tracers), tracers_old=np.ascontiguousarray(old))
+
+
+def max_cfl_z(mesh: Mesh, w: np.ndarray, hnode_new: np.ndarray, dt: float) -> float:
+    """Max vertical CFL ``|w|*dt*(1/h[k] + 1/h[k-1])`` over interfaces
+    (fesom_jax/ale.py:368-395)."""
+    lm = mesh.node_layer_mask
+    inv = np.where(lm & (hnode_new > 0), 1.0 / np.where(hnode_new > 0, hnode_new, 1.0), 0.0)
+    inv_above = np.concatenate([np.zeros((mesh.nod2D, 1)), inv[:, :-1]], axis=1)
+    return float(np.max(np.abs(w) * dt * (inv + inv_above)))

@@ -1,0 +1,86 @@
+"""Rebuild the inputs of the golden pi cases (``tests/golden/make_golden.py``) without the
+reference checkout, and compare a result against the stored vectors."""
+
+from __future__ import annotations
+
+import hashlib
+from pathlib import Path
+
+import numpy as np
+
+from fesom_jax_b200 import inputs as I
+
+GOLDEN = Path(__file__).resolve().parent / "golden" / "fct_pi_golden.npz"
+DT = 3600.0
+SAMPLE = slice(0, None, 4)
+# max-norm relative tolerance of the FCT path (per step, over wet lanes)
+RTOL = 1e-12
+
+
+def field_digest(m, x, mask=None):
+    mask = m.node_layer_mask if mask is None else mask
+    wts = np.random.default_rng(1234).normal(size=mask.shape)
+    xm = np.where(mask, x, 0.0)
+    return np.array([xm.sum(), (wts * xm).sum(), np.abs(wts * xm).sum(), (xm * xm).sum()])
+
+
+def _sha(*arrays):
+    h = hashlib.sha256()
+    for a in arrays:
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.digest()
+
+
+def cases(m):
+    """name -> dict(uv, w_e, helem, hnode, hnode_new, T, T_old, kw)."""
+    lm = m.node_layer_mask
+    f = I.make_fields(m, seed=0)
+    f_ab2 = I.make_fields(m, seed=0, ab2=True)
+    k = np.arange(m.nl)[None, :]
+    sharp = np.where(lm, 10.0 + 5.0 * np.sin(np.arange(m.nod2D)[:, None] * 0.7)
+                     * np.cos(k * 1.3), 0.0)
+    ten = np.where(lm, 10.0, 0.0)
+    const = np.where(lm, 20.0, 0.0)
+    zbar3 = np.broadcast_to(m.zbar, (m.nod2D, m.nl)).copy()
+    zbar3[:, 1:] *= 1.0 + 0.01 * np.sin(np.arange(m.nod2D))[:, None]
+    Z3d = np.concatenate([0.5 * (zbar3[:, :-1] + zbar3[:, 1:]),
+                          0.5 * (zbar3[:, -2:-1] + zbar3[:, -1:])], axis=1)
+    w_i = 0.3 * f.w_e
+    base = dict(helem=f.helem, hnode=f.hnode, hnode_new=f.hnode_new)
+    out = {
+        "T_step1": dict(uv=f.uv, w_e=f.w_e, T=f.tracers[0], T_old=f.tracers_old[0], kw={}),
+        "S_step1": dict(uv=f.uv, w_e=f.w_e, T=f.tracers[1], T_old=f.tracers_old[1], kw={}),
+        "T_ab2": dict(uv=f_ab2.uv, w_e=f_ab2.w_e, T=f_ab2.tracers[0],
+                      T_old=f_ab2.tracers_old[0], kw={}),
+        "sharp_x5": dict(uv=f.uv * 5.0, w_e=f.w_e * 5.0, T=sharp, T_old=ten, kw={}),
+        "const": dict(uv=f.uv, w_e=f.w_e, T=const, T_old=const, kw={}),
+        "T_wsplit_zstar": dict(uv=f.uv, w_e=f.w_e - w_i, T=f.tracers[0],
+                               T_old=f_ab2.tracers_old[0],
+                               kw=dict(w_i=w_i, Z3d=Z3d, zbar3=zbar3)),
+    }
+    for c in out.values():
+        c.update(base)
+    return out
+
+
+def load_golden():
+    return dict(np.load(GOLDEN))
+
+
+def check_against_golden(m, g, name, case, T_new, rtol=RTOL):
+    """Assert ``T_new`` matches the golden case: input digest, sampled lanes (max-norm
+    relative), and the full-field digest. Returns the sampled relative error."""
+    c = case
+    assert _sha(c["uv"], c["w_e"], c["T"], c["T_old"], *c["kw"].values()) == \
+        g[f"{name}__in_digest"].tobytes(), f"{name}: input generation drifted"
+    lm = m.node_layer_mask
+    ref = g[f"{name}__T_new"]
+    got = T_new[SAMPLE][lm[SAMPLE]]
+    scale = max(np.max(np.abs(ref)), 1e-300)
+    err = np.max(np.abs(got - ref)) / scale
+    assert err <= rtol, f"{name}: sampled max|d|/max|ref| = {err:.3e}"
+    dg, dr = field_digest(m, T_new), g[f"{name}__digest"]
+    assert abs(dg[0] - dr[0]) <= rtol * abs(dr[0]) * 10 + 1e-300, f"{name}: sum"
+    assert abs(dg[1] - dr[1]) <= rtol * dr[2] * 10, f"{name}: weighted sum"
+    assert abs(dg[3] - dr[3]) <= rtol * dr[3] * 10, f"{name}: sum of squares"
+    return err
