@@ -1,0 +1,43 @@
+// Host-side helpers shared by the libfesom_fct translation units.
+#pragma once
+
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+
+#include <cuda_runtime.h>
+
+#include "fct_internal.cuh"
+
+namespace fct {
+
+// Record the calling thread's last error and return ``status``.
+int set_error(int status, const char* fmt, ...);
+
+inline int cuda_error(cudaError_t e, const char* what) {
+  return set_error(FCT_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define FCT_CUDA(call)                                   \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) return ::fct::cuda_error(e_, #call); \
+  } while (0)
+
+// Launch the forward kernel sequence for ``n`` instances. ``single`` is used when
+// ``tab`` is null (n == 1), otherwise ``tab`` is a device array of ``n`` instances
+// whose lane counts are bounded by the ``max_*`` arguments.
+struct LaunchDims {
+  int64_t max_iface, max_layer, max_edge, max_elem, max_dense, max_nodes;
+  int max_ntr;
+};
+int launch_forward(const Inst& single, const Inst* tab, int n, const LaunchDims& d,
+                   cudaStream_t s);
+
+// Fill a workspace with its resting values (BIG bounds, unit factors, zeros).
+int init_workspace(const Workspace& ws, int ntr, cudaStream_t s);
+
+Workspace carve_workspace(double* base, int64_t N, int64_t E, int64_t Ed, int64_t L, int ntr);
+int64_t workspace_doubles(int64_t N, int64_t E, int64_t Ed, int64_t L, int ntr);
+
+}  // namespace fct

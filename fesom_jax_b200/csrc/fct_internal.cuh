@@ -1,0 +1,104 @@
+// Internal device-side structures of libfesom_fct (not part of the public ABI).
+//
+// Storage: every per-level field is dense row-major [entity, L] float64 (the
+// reference layout, fesom_jax/mesh.py:16-20). Kernels walk compact *lane lists*
+// (entity, level) that enumerate only wet levels, so dry levels cost no threads and
+// no bytes; a lane is packed as (entity << 7) | level (requires L <= 128).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/fesom_fct.h"
+
+namespace fct {
+
+constexpr int kLevelBits = 7;
+constexpr int kMaxLevels = 1 << kLevelBits;
+constexpr unsigned kLevelMask = kMaxLevels - 1;
+
+constexpr double kREarth = 6367500.0;   // fesom_jax/config.py:41
+constexpr double kAbOld = -(0.5 + 0.1);  // tracer_adv.py:44-46
+constexpr double kAbNew = (1.5 + 0.1);
+constexpr double kFluxEps = 1e-16;       // tracer_adv.py:192
+constexpr double kBig = 1e3;             // tracer_adv.py:193
+
+__host__ __device__ inline int lane_ent(uint32_t lane) { return int(lane >> kLevelBits); }
+__host__ __device__ inline int lane_lev(uint32_t lane) { return int(lane & kLevelMask); }
+
+// Static mesh on the device (pointers into one plan allocation).
+struct DevMesh {
+  int N, E, Ed, L;
+  // nodes
+  const int* nzmin;      // ulevels_nod2D - 1
+  const int* nzmax;      // nlevels_nod2D - 1 (exclusive layer bound; bottom interface)
+  const int* ulmax;      // ulevels_nod2D_max
+  const int* nlmin;      // nlevels_nod2D_min
+  const int* ne_off;     // node -> incident edges CSR, ascending edge id
+  const int* ne_idx;     //   entry = 2*edge + (node is the edge's second node)
+  const int* nel_off;    // node -> elements CSR (nod_in_elem2D, element-ascending)
+  const int* nel_idx;
+  const double* area;    // [N,L]
+  const double* areasvol;
+  // elements
+  const int* enodes;     // [E,3]
+  const int* eul;        // ulevels - 1
+  const int* enl;        // nlevels - 1 (exclusive)
+  const double* gsca;    // [E,6]
+  const double* earea;   // [E]
+  // edges
+  const int* edges;      // [Ed,2]
+  const int* etri;       // [Ed,2]
+  const int* eupdn;      // [Ed,2]
+  const double* cross;   // [Ed,4]
+  const double* ecoef;   // [Ed,2]: edx*a, edy*R  (a = R*cos, averaged over the two cells)
+  // vertical
+  const double* Zp;      // [L]  Z padded with Z[L-2] (tracer_adv.py:233)
+  const double* zbar;    // [L]
+  // lanes
+  const uint32_t* iface_lanes;  int64_t n_iface;   // nodes, k in [nzmin, nzmax]
+  const uint32_t* layer_lanes;  int64_t n_layer;   // nodes, k in [nzmin, nzmax)
+  const uint32_t* edge_lanes;   int64_t n_edge;    // edges, k in the union of cell layers
+  const uint32_t* elem_lanes;   int64_t n_elem;    // elements, k in [eul, enl)
+};
+
+// Per-tracer intermediates of one instance (dense [entity, L]; tracer t at +t*stride).
+struct Workspace {
+  double* vflux;                 // [Ed,L] shared by all tracers of the instance
+  double *gx, *gy;               // [E,L] element gradients
+  double *amax, *amin;           // [E,L] per-element cluster bounds (init -+BIG)
+  double *lo, *gnx, *gny;        // [N,L]
+  double* adfv;                  // [N,L] antidiffusive vertical flux (interfaces)
+  double *tvmax, *tvmin;         // [N,L]
+  double *pf, *mf;               // [N,L] limiter factors (init 1)
+  double* adfh;                  // [Ed,L] antidiffusive horizontal flux
+  int64_t sN, sE, sEd;           // per-tracer strides (doubles)
+};
+
+// One FCT instance: a mesh, its per-call fields, and a workspace.
+struct Inst {
+  const DevMesh* m;
+  const double *uv, *w_e, *helem, *hnode, *hnode_new;
+  const double *T, *T_old;
+  double* T_new;
+  int64_t tstride;
+  const double *Z3d, *zbar3, *w_i;
+  Workspace ws;
+  double dt;
+  int ntr;
+  int copy_dry;   // 1: write T_new = T on dry levels (fresh output buffers)
+};
+
+}  // namespace fct
+
+struct FctPlan {
+  int device = 0;
+  int N = 0, E = 0, Ed = 0, L = 0;
+  fct::DevMesh hm{};               // device pointers (host copy)
+  fct::DevMesh* d_mesh = nullptr;  // device copy
+  void* d_static = nullptr;        // one allocation for all static arrays
+  int max_tracers = 0;
+  double* d_ws = nullptr;          // workspace allocation
+  fct::Workspace ws{};
+  int64_t n_wet_elem_layers = 0;
+};

@@ -1,0 +1,375 @@
+// Plan construction and the single-instance C-ABI entry points of libfesom_fct.
+//
+// A plan replaces the reference's per-call Mesh pytree operands (fesom_jax/mesh.py:62-129):
+// the mesh is validated and uploaded once, and the derived data the kernels need is
+// built on the host here:
+//   * node -> incident-edge CSR in ascending edge id (the order in which the reference's
+//     edge->node segment_sum accumulates, fesom_jax/ops.py:56-81, so the gathers add the
+//     same terms in the same order);
+//   * level ranges per node/element and the wet-lane lists the kernels iterate;
+//   * per-edge MFCT coefficients (edx*a, edy*R) with a = R*cos averaged over the edge's
+//     cells, evaluated with the reference's expression (tracer_adv.py:216-220).
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "fct_host.h"
+
+namespace fct {
+
+static thread_local std::string g_last_error;
+
+int set_error(int status, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return status;
+}
+
+int64_t workspace_doubles(int64_t N, int64_t E, int64_t Ed, int64_t L, int ntr) {
+  return Ed * L + int64_t(ntr) * (4 * E * L + 9 * N * L + Ed * L);
+}
+
+Workspace carve_workspace(double* base, int64_t N, int64_t E, int64_t Ed, int64_t L, int ntr) {
+  Workspace w{};
+  w.sN = N * L;
+  w.sE = E * L;
+  w.sEd = Ed * L;
+  double* p = base;
+  auto take = [&](int64_t n) { double* q = p; p += n; return q; };
+  w.vflux = take(Ed * L);
+  w.gx = take(ntr * w.sE);
+  w.gy = take(ntr * w.sE);
+  w.amax = take(ntr * w.sE);
+  w.amin = take(ntr * w.sE);
+  w.lo = take(ntr * w.sN);
+  w.gnx = take(ntr * w.sN);
+  w.gny = take(ntr * w.sN);
+  w.adfv = take(ntr * w.sN);
+  w.tvmax = take(ntr * w.sN);
+  w.tvmin = take(ntr * w.sN);
+  w.pf = take(ntr * w.sN);
+  w.mf = take(ntr * w.sN);
+  w.adfh = take(ntr * w.sEd);
+  return w;
+}
+
+namespace {
+
+struct Blob {
+  std::vector<char> bytes;
+  template <class T>
+  size_t add(const T* src, size_t n) {
+    size_t off = (bytes.size() + 255) & ~size_t(255);
+    bytes.resize(off + n * sizeof(T));
+    if (n) std::memcpy(bytes.data() + off, src, n * sizeof(T));
+    return off;
+  }
+};
+
+int validate_desc(const FctMeshDesc* d) {
+  if (!d) return set_error(FCT_ERR_INVALID, "mesh descriptor is NULL");
+  if (d->nod2D <= 0 || d->elem2D <= 0 || d->edge2D <= 0)
+    return set_error(FCT_ERR_INVALID, "mesh counts must be positive");
+  if (d->nl < 3 || d->nl > kMaxLevels)
+    return set_error(FCT_ERR_INVALID, "nl=%d outside [3, %d]", d->nl, kMaxLevels);
+  if (int64_t(d->nod2D) >= (int64_t(1) << (32 - kLevelBits)) ||
+      int64_t(d->edge2D) >= (int64_t(1) << (32 - kLevelBits)) ||
+      int64_t(d->elem2D) >= (int64_t(1) << (32 - kLevelBits)))
+    return set_error(FCT_ERR_INVALID, "mesh too large for 25-bit entity ids");
+  const void* req[] = {d->edges, d->edge_tri, d->edge_up_dn_tri, d->edge_cross_dxdy,
+                       d->edge_dxdy, d->elem_nodes, d->gradient_sca, d->elem_cos,
+                       d->elem_area, d->nlevels, d->ulevels, d->nlevels_nod2D,
+                       d->nlevels_nod2D_min, d->ulevels_nod2D, d->ulevels_nod2D_max,
+                       d->nod_in_elem2D_offsets, d->nod_in_elem2D, d->area, d->areasvol,
+                       d->Z, d->zbar};
+  for (const void* p : req)
+    if (!p) return set_error(FCT_ERR_INVALID, "mesh descriptor has a NULL array");
+  const int N = d->nod2D, E = d->elem2D, Ed = d->edge2D, L = d->nl;
+  for (int i = 0; i < 2 * Ed; ++i)
+    if (d->edges[i] < 0 || d->edges[i] >= N)
+      return set_error(FCT_ERR_INVALID, "edges[%d]=%d out of range", i, d->edges[i]);
+  for (int e = 0; e < Ed; ++e) {
+    if (d->edge_tri[2 * e] < 0 || d->edge_tri[2 * e] >= E)
+      return set_error(FCT_ERR_INVALID, "edge_tri[%d,0] must be a valid element", e);
+    for (int j = 0; j < 2; ++j) {
+      int t = d->edge_tri[2 * e + j], u = d->edge_up_dn_tri[2 * e + j];
+      if (t < -1 || t >= E || u < -1 || u >= E)
+        return set_error(FCT_ERR_INVALID, "edge %d: element id out of range", e);
+    }
+  }
+  for (int i = 0; i < 3 * E; ++i)
+    if (d->elem_nodes[i] < 0 || d->elem_nodes[i] >= N)
+      return set_error(FCT_ERR_INVALID, "elem_nodes[%d] out of range", i);
+  for (int e = 0; e < E; ++e)
+    if (d->ulevels[e] < 1 || d->nlevels[e] > L || d->nlevels[e] < d->ulevels[e])
+      return set_error(FCT_ERR_INVALID, "element %d level range invalid", e);
+  for (int n = 0; n < N; ++n) {
+    if (d->ulevels_nod2D[n] < 1 || d->nlevels_nod2D[n] > L ||
+        d->nlevels_nod2D[n] < d->ulevels_nod2D[n] || d->nlevels_nod2D_min[n] > L ||
+        d->ulevels_nod2D_max[n] < 1)
+      return set_error(FCT_ERR_INVALID, "node %d level range invalid", n);
+    if (d->nod_in_elem2D_offsets[n + 1] < d->nod_in_elem2D_offsets[n])
+      return set_error(FCT_ERR_INVALID, "nod_in_elem2D_offsets not monotone at %d", n);
+  }
+  if (d->nod_in_elem2D_offsets[0] != 0)
+    return set_error(FCT_ERR_INVALID, "nod_in_elem2D_offsets[0] != 0");
+  const int nie = d->nod_in_elem2D_offsets[N];
+  for (int i = 0; i < nie; ++i)
+    if (d->nod_in_elem2D[i] < 0 || d->nod_in_elem2D[i] >= E)
+      return set_error(FCT_ERR_INVALID, "nod_in_elem2D[%d] out of range", i);
+  return FCT_OK;
+}
+
+}  // namespace
+
+__global__ void k_fill(double* p, int64_t n, double v) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x)
+    p[i] = v;
+}
+
+int init_workspace(const Workspace& ws, int ntr, cudaStream_t s) {
+  auto fill = [&](double* p, int64_t n, double v) -> int {
+    if (n <= 0) return FCT_OK;
+    int blocks = int(std::min<int64_t>((n + 255) / 256, 148 * 16));
+    k_fill<<<blocks, 256, 0, s>>>(p, n, v);
+    FCT_CUDA(cudaGetLastError());
+    return FCT_OK;
+  };
+  int st;
+  if ((st = fill(ws.vflux, ws.sEd, 0.0))) return st;
+  double* zero_fields[] = {ws.gx, ws.gy};
+  for (double* p : zero_fields)
+    if ((st = fill(p, ntr * ws.sE, 0.0))) return st;
+  if ((st = fill(ws.amax, ntr * ws.sE, -kBig))) return st;
+  if ((st = fill(ws.amin, ntr * ws.sE, kBig))) return st;
+  double* zn[] = {ws.lo, ws.gnx, ws.gny, ws.adfv, ws.tvmax, ws.tvmin};
+  for (double* p : zn)
+    if ((st = fill(p, ntr * ws.sN, 0.0))) return st;
+  if ((st = fill(ws.pf, ntr * ws.sN, 1.0))) return st;
+  if ((st = fill(ws.mf, ntr * ws.sN, 1.0))) return st;
+  if ((st = fill(ws.adfh, ntr * ws.sEd, 0.0))) return st;
+  return FCT_OK;
+}
+
+}  // namespace fct
+
+using namespace fct;
+
+static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
+  const int N = d->nod2D, E = d->elem2D, Ed = d->edge2D, L = d->nl;
+  P->device = device;
+  P->N = N; P->E = E; P->Ed = Ed; P->L = L;
+
+  std::vector<int> nzmin(N), nzmax(N), eul(E), enl(E);
+  for (int n = 0; n < N; ++n) {
+    nzmin[n] = d->ulevels_nod2D[n] - 1;
+    nzmax[n] = d->nlevels_nod2D[n] - 1;
+  }
+  for (int e = 0; e < E; ++e) {
+    eul[e] = d->ulevels[e] - 1;
+    enl[e] = d->nlevels[e] - 1;
+  }
+  // node -> edge CSR (ascending edge id per node)
+  std::vector<int> ne_off(N + 1, 0), ne_idx(2 * size_t(Ed));
+  for (int e = 0; e < Ed; ++e) {
+    ne_off[d->edges[2 * e] + 1]++;
+    ne_off[d->edges[2 * e + 1] + 1]++;
+  }
+  for (int n = 0; n < N; ++n) ne_off[n + 1] += ne_off[n];
+  {
+    std::vector<int> fillp(ne_off.begin(), ne_off.end() - 1);
+    for (int e = 0; e < Ed; ++e) {
+      ne_idx[fillp[d->edges[2 * e]]++] = 2 * e;
+      ne_idx[fillp[d->edges[2 * e + 1]]++] = 2 * e + 1;
+    }
+  }
+  // per-edge MFCT coefficients, reference expression (tracer_adv.py:216-222)
+  std::vector<double> ecoef(2 * size_t(Ed));
+  for (int e = 0; e < Ed; ++e) {
+    const int el1 = d->edge_tri[2 * e], el2 = d->edge_tri[2 * e + 1];
+    double a = kREarth * d->elem_cos[el1 >= 0 ? el1 : 0];
+    if (el2 >= 0) a = 0.5 * (a + kREarth * d->elem_cos[el2]);
+    ecoef[2 * e] = d->edge_dxdy[2 * e] * a;
+    ecoef[2 * e + 1] = d->edge_dxdy[2 * e + 1] * kREarth;
+  }
+  std::vector<double> Zp(L);
+  for (int k = 0; k < L - 1; ++k) Zp[k] = d->Z[k];
+  Zp[L - 1] = d->Z[L - 2];
+  // lanes
+  std::vector<uint32_t> iface, layer, edgel, eleml;
+  for (int n = 0; n < N; ++n) {
+    for (int k = std::max(nzmin[n], 0); k <= std::min(nzmax[n], L - 1); ++k) {
+      iface.push_back((uint32_t(n) << kLevelBits) | uint32_t(k));
+      if (k < nzmax[n]) layer.push_back((uint32_t(n) << kLevelBits) | uint32_t(k));
+    }
+  }
+  int64_t wet_elem = 0;
+  for (int e = 0; e < E; ++e)
+    for (int k = std::max(eul[e], 0); k < std::min(enl[e], L); ++k) {
+      eleml.push_back((uint32_t(e) << kLevelBits) | uint32_t(k));
+      ++wet_elem;
+    }
+  for (int e = 0; e < Ed; ++e) {
+    const int el1 = d->edge_tri[2 * e], el2 = d->edge_tri[2 * e + 1];
+    int lo = eul[el1], hi = enl[el1];
+    if (el2 >= 0) {
+      lo = std::min(lo, eul[el2]);
+      hi = std::max(hi, enl[el2]);
+    }
+    for (int k = std::max(lo, 0); k < std::min(hi, L); ++k)
+      edgel.push_back((uint32_t(e) << kLevelBits) | uint32_t(k));
+  }
+  P->n_wet_elem_layers = wet_elem;
+
+  Blob b;
+  const int nie = d->nod_in_elem2D_offsets[N];
+  size_t o_nzmin = b.add(nzmin.data(), N), o_nzmax = b.add(nzmax.data(), N);
+  size_t o_ulmax = b.add(d->ulevels_nod2D_max, N), o_nlmin = b.add(d->nlevels_nod2D_min, N);
+  size_t o_neoff = b.add(ne_off.data(), N + 1), o_neidx = b.add(ne_idx.data(), ne_idx.size());
+  size_t o_neloff = b.add(d->nod_in_elem2D_offsets, N + 1);
+  size_t o_nelidx = b.add(d->nod_in_elem2D, nie);
+  size_t o_area = b.add(d->area, size_t(N) * L), o_av = b.add(d->areasvol, size_t(N) * L);
+  size_t o_en = b.add(d->elem_nodes, 3 * size_t(E));
+  size_t o_eul = b.add(eul.data(), E), o_enl = b.add(enl.data(), E);
+  size_t o_gs = b.add(d->gradient_sca, 6 * size_t(E)), o_ea = b.add(d->elem_area, E);
+  size_t o_edges = b.add(d->edges, 2 * size_t(Ed)), o_etri = b.add(d->edge_tri, 2 * size_t(Ed));
+  size_t o_eud = b.add(d->edge_up_dn_tri, 2 * size_t(Ed));
+  size_t o_cross = b.add(d->edge_cross_dxdy, 4 * size_t(Ed));
+  size_t o_ecoef = b.add(ecoef.data(), ecoef.size());
+  size_t o_Zp = b.add(Zp.data(), L), o_zbar = b.add(d->zbar, L);
+  size_t o_if = b.add(iface.data(), iface.size()), o_ly = b.add(layer.data(), layer.size());
+  size_t o_ed = b.add(edgel.data(), edgel.size()), o_el = b.add(eleml.data(), eleml.size());
+
+  FCT_CUDA(cudaSetDevice(device));
+  FCT_CUDA(cudaMalloc(&P->d_static, b.bytes.size()));
+  FCT_CUDA(cudaMemcpy(P->d_static, b.bytes.data(), b.bytes.size(), cudaMemcpyHostToDevice));
+  char* base = static_cast<char*>(P->d_static);
+  DevMesh& m = P->hm;
+  m.N = N; m.E = E; m.Ed = Ed; m.L = L;
+  m.nzmin = (const int*)(base + o_nzmin);
+  m.nzmax = (const int*)(base + o_nzmax);
+  m.ulmax = (const int*)(base + o_ulmax);
+  m.nlmin = (const int*)(base + o_nlmin);
+  m.ne_off = (const int*)(base + o_neoff);
+  m.ne_idx = (const int*)(base + o_neidx);
+  m.nel_off = (const int*)(base + o_neloff);
+  m.nel_idx = (const int*)(base + o_nelidx);
+  m.area = (const double*)(base + o_area);
+  m.areasvol = (const double*)(base + o_av);
+  m.enodes = (const int*)(base + o_en);
+  m.eul = (const int*)(base + o_eul);
+  m.enl = (const int*)(base + o_enl);
+  m.gsca = (const double*)(base + o_gs);
+  m.earea = (const double*)(base + o_ea);
+  m.edges = (const int*)(base + o_edges);
+  m.etri = (const int*)(base + o_etri);
+  m.eupdn = (const int*)(base + o_eud);
+  m.cross = (const double*)(base + o_cross);
+  m.ecoef = (const double*)(base + o_ecoef);
+  m.Zp = (const double*)(base + o_Zp);
+  m.zbar = (const double*)(base + o_zbar);
+  m.iface_lanes = (const uint32_t*)(base + o_if);  m.n_iface = int64_t(iface.size());
+  m.layer_lanes = (const uint32_t*)(base + o_ly);  m.n_layer = int64_t(layer.size());
+  m.edge_lanes = (const uint32_t*)(base + o_ed);   m.n_edge = int64_t(edgel.size());
+  m.elem_lanes = (const uint32_t*)(base + o_el);   m.n_elem = int64_t(eleml.size());
+  FCT_CUDA(cudaMalloc(&P->d_mesh, sizeof(DevMesh)));
+  FCT_CUDA(cudaMemcpy(P->d_mesh, &m, sizeof(DevMesh), cudaMemcpyHostToDevice));
+  return FCT_OK;
+}
+
+extern "C" {
+
+const char* fct_last_error(void) { return fct::g_last_error.c_str(); }
+
+const char* fct_version(void) { return "fesom_fct 0.1.0 (sm_100a, fp64)"; }
+
+int fct_plan_destroy(FctPlan* P) {
+  if (!P) return FCT_OK;
+  cudaSetDevice(P->device);
+  if (P->d_ws) cudaFree(P->d_ws);
+  if (P->d_mesh) cudaFree(P->d_mesh);
+  if (P->d_static) cudaFree(P->d_static);
+  delete P;
+  return FCT_OK;
+}
+
+int fct_plan_reserve(FctPlan* P, int max_tracers) {
+  if (!P) return set_error(FCT_ERR_INVALID, "plan is NULL");
+  if (max_tracers < 1) return set_error(FCT_ERR_INVALID, "max_tracers must be >= 1");
+  if (max_tracers <= P->max_tracers) return FCT_OK;
+  FCT_CUDA(cudaSetDevice(P->device));
+  const int64_t nd = workspace_doubles(P->N, P->E, P->Ed, P->L, max_tracers);
+  double* ws = nullptr;
+  FCT_CUDA(cudaMalloc(&ws, size_t(nd) * sizeof(double)));
+  Workspace w = carve_workspace(ws, P->N, P->E, P->Ed, P->L, max_tracers);
+  int st = init_workspace(w, max_tracers, 0);
+  if (st) { cudaFree(ws); return st; }
+  FCT_CUDA(cudaDeviceSynchronize());
+  if (P->d_ws) cudaFree(P->d_ws);
+  P->d_ws = ws;
+  P->ws = w;
+  P->max_tracers = max_tracers;
+  return FCT_OK;
+}
+
+int fct_plan_create(const FctMeshDesc* desc, int device, int max_tracers, FctPlan** out) {
+  if (!out) return set_error(FCT_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  int st = validate_desc(desc);
+  if (st) return st;
+  FctPlan* P = new FctPlan();
+  st = plan_build(desc, device, P);
+  if (!st) st = fct_plan_reserve(P, max_tracers < 1 ? 1 : max_tracers);
+  if (st) { fct_plan_destroy(P); return st; }
+  *out = P;
+  return FCT_OK;
+}
+
+int fct_plan_info(const FctPlan* P, int64_t out[8]) {
+  if (!P || !out) return set_error(FCT_ERR_INVALID, "NULL argument");
+  out[0] = P->N; out[1] = P->E; out[2] = P->Ed; out[3] = P->L;
+  out[4] = P->hm.n_layer; out[5] = P->n_wet_elem_layers; out[6] = P->hm.n_edge;
+  out[7] = P->max_tracers;
+  return FCT_OK;
+}
+
+int fct_forward(FctPlan* P, const FctFields* f, double dt, int ntr, fct_stream_t stream) {
+  if (!P || !f) return set_error(FCT_ERR_INVALID, "NULL plan or fields");
+  if (ntr < 1) return set_error(FCT_ERR_INVALID, "ntr must be >= 1");
+  if (ntr > P->max_tracers)
+    return set_error(FCT_ERR_CAPACITY, "ntr=%d exceeds reserved workspace (%d tracers); "
+                     "call fct_plan_reserve first", ntr, P->max_tracers);
+  if (!f->uv || !f->w_e || !f->helem || !f->hnode || !f->hnode_new || !f->T ||
+      !f->T_old || !f->T_new)
+    return set_error(FCT_ERR_INVALID, "a required field pointer is NULL");
+  if ((f->Z3d == nullptr) != (f->zbar3 == nullptr))
+    return set_error(FCT_ERR_INVALID, "Z3d and zbar3 must be given together");
+  if (!(dt > 0.0)) return set_error(FCT_ERR_INVALID, "dt must be positive");
+  Inst in{};
+  in.m = P->d_mesh;
+  in.uv = f->uv; in.w_e = f->w_e; in.helem = f->helem;
+  in.hnode = f->hnode; in.hnode_new = f->hnode_new;
+  in.T = f->T; in.T_old = f->T_old; in.T_new = f->T_new;
+  in.tstride = f->tracer_stride ? f->tracer_stride : int64_t(P->N) * P->L;
+  in.Z3d = f->Z3d; in.zbar3 = f->zbar3; in.w_i = f->w_i;
+  in.ws = P->ws;
+  in.dt = dt;
+  in.ntr = ntr;
+  in.copy_dry = 1;
+  LaunchDims dims{P->hm.n_iface, P->hm.n_layer, P->hm.n_edge, P->hm.n_elem,
+                  int64_t(P->N) * P->L, int64_t(P->N), ntr};
+  int prev = -1;
+  cudaGetDevice(&prev);
+  if (prev != P->device) cudaSetDevice(P->device);
+  const int st = launch_forward(in, nullptr, 1, dims, static_cast<cudaStream_t>(stream));
+  if (prev >= 0 && prev != P->device) cudaSetDevice(prev);
+  return st;
+}
+
+}  // extern "C"

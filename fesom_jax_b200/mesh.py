@@ -59,7 +59,7 @@ def level_masks(ulevels, nlevels, nl: int):
     return top & (k < (n - 1)), top & (k < n)
 
 
-@dataclasses.dataclass
+@dataclasses.dataclass(eq=False)
 class Mesh:
     """FESOM2 mesh arrays used by FCT advection (host numpy, reference names)."""
 
