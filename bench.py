@@ -1,0 +1,430 @@
+#!/usr/bin/env python
+"""FCT tracer-advection benchmark on B200 (one JSON line on rank 0).
+
+Default workload ("batched"): a CORE2-size synthetic mesh (127,000 nodes, 48 levels,
+bottom level 5-48), 32 ensemble members x 8 tracers (T, S, 6 passive) with
+seed-perturbed velocities, 30 FCT steps (dt = 1800 s) captured as one CUDA graph. One
+bench step is one such 30-step graph over all members; ``value`` is node-level updates/s
+(one tracer value at one wet node layer advanced one FCT step) over all ranks.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config batched|pi|large]
+    python bench.py --impl reference ...   # the CPU arm (C restatement, all host threads)
+
+Multi-GPU: one rank per GPU (torchrun); every rank advances its own 32 members (weak
+scaling, no data-path collective); time = max over ranks of the CUDA-event time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "FCT node-level updates/s FP64, batched vs plain on 1 B200; serve p50/p99 ms"
+UNIT = "node-level updates/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return dict(hbm_gbs=float(d["hbm_gbs"]), source="measured")
+    return dict(hbm_gbs=FALLBACK_HBM_GBS, source="fallback")
+
+
+# ------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi sampling (200 ms) of SM clocks and throttle reasons during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.gpu)], stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self) -> dict | None:
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append(dict(sm=float(parts[1]), smax=float(parts[2]), power=float(parts[3]),
+                                 hw=parts[5], hwt=parts[6], swt=parts[7], pcap=parts[8]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        loaded = [r for r in rows if r["power"] > 250.0] or rows
+        reasons = set()
+        for r in rows:
+            for key, name in (("hw", "hw_slowdown"), ("hwt", "hw_thermal_slowdown"),
+                              ("swt", "sw_thermal_slowdown"), ("pcap", "sw_power_cap")):
+                if r[key].lower() == "active":
+                    reasons.add(name)
+        return dict(sm_mhz=float(np.median([r["sm"] for r in loaded])),
+                    sm_max_mhz=float(max(r["smax"] for r in rows)), reasons=sorted(reasons),
+                    samples=len(rows), power_w_max=float(max(r["power"] for r in rows)))
+
+
+def gpu_index(local_rank: int) -> int:
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [x.strip() for x in vis.split(",") if x.strip()]
+        if local_rank < len(ids) and ids[local_rank].isdigit():
+            return int(ids[local_rank])
+    return local_rank
+
+
+# -------------------------------------------------------------------- distributed
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = False
+
+    def init(self, backend: str):
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+            self.pg = True
+
+    def barrier(self):
+        if self.pg:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max(self, x: float, device) -> float:
+        if not self.pg:
+            return x
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+# -------------------------------------------------------------------- CPU oracle
+def cpu_oracle_rate(mesh, fields_host, ntr: int, dt: float, min_seconds: float = 10.0,
+                    max_reps: int = 3) -> dict:
+    """Time the C restatement (all host threads) on one member's ``ntr`` tracers, one
+    FCT step, repeated until ``min_seconds`` or ``max_reps``; returns updates/s."""
+    from oracle import fct_c
+    keep = []
+    from fesom_jax_b200 import _lib as fl
+    desc = fl.mesh_desc(mesh, keep)
+    f = fields_host
+    reps, t_total = 0, 0.0
+    while reps < max_reps and (t_total < min_seconds or reps == 0):
+        t0 = time.perf_counter()
+        for t in range(ntr):
+            fct_c.advect_one_fct(mesh, f["uv"], f["w_e"], f["helem"], f["hnode"],
+                                 f["hnode_new"], f["T"][t], f["T_old"][t], dt=dt, desc=desc)
+        t_total += time.perf_counter() - t0
+        reps += 1
+    upd = reps * ntr * mesh.n_wet_layers
+    return dict(value=upd / t_total, unit=UNIT, cores=fct_c.max_threads(), kind="port",
+                sample=f"C loop restatement (OpenMP), {reps} x (1 member x {ntr} tracers x 1 "
+                       f"FCT step) on {mesh.name}, {t_total:.1f} s")
+
+
+# ------------------------------------------------------------------------ our arm
+def run_ours(args, D: Dist) -> dict | None:
+    import torch
+
+    from fesom_jax_b200 import workloads as W
+    from fesom_jax_b200.ensemble import Ensemble
+
+    torch.cuda.set_device(D.local_rank)
+    dev = torch.device("cuda", D.local_rank)
+    cfg = dict(W.WORKLOADS[args.config])
+    if args.members:
+        cfg["members"] = args.members
+    if args.fct_steps:
+        cfg["fct_steps"] = args.fct_steps
+    if args.ntr:
+        cfg["ntr"] = args.ntr
+    mesh = W.make_workload_mesh(args.config, seed=0)
+    thick = W.rest_thickness_gpu(mesh, dev)
+    ens = Ensemble(device=D.local_rank, workspace_budget=int(args.workspace_gb * (1 << 30)))
+    member_inputs = []
+    for i in range(cfg["members"]):
+        inp = W.member_inputs_gpu(mesh, seed=1000 * D.rank + i, ntr=cfg["ntr"], device=dev,
+                                  thickness=thick, sigma=cfg["sigma"],
+                                  n_vortices=cfg["n_vortices"])
+        ens.add_member(mesh, inp["uv"], inp["w_e"], inp["helem"], inp["hnode"],
+                       inp["hnode_new"], inp["T"], inp["T_old"], cfg["dt"])
+        member_inputs.append(inp if i == 0 else None)
+        del inp
+    ens.build()
+    info = ens.info()
+    S = cfg["fct_steps"]
+    stream = torch.cuda.current_stream(dev)
+    torch.cuda.synchronize()
+    for _ in range(args.warmup):
+        ens.run(S)
+    torch.cuda.synchronize()
+    D.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(gpu_index(D.local_rank))
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        ens.run(S)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    D.barrier()
+    clk = clocks.stop()
+    t_local = e0.elapsed_time(e1) / 1e3
+    t = D.max(t_local, dev)
+    upd_rank = info["updates_per_step"] * S * args.steps
+    value = upd_rank * D.world / t
+
+    # per-stage breakdown (events on the launching stream, one step, synchronised)
+    prof = {}
+    for _ in range(3):
+        for k, v in ens.profile_step().items():
+            prof[k] = prof.get(k, 0.0) + v / 3
+    fct_step_ms = t_local / (S * args.steps) * 1e3
+    finite = bool(torch.isfinite(ens.state(0)[0]).all().item())
+    alg = W.algorithmic_bytes(mesh, cfg["ntr"], cfg["members"])
+    pk = peaks()
+    achieved = alg / (fct_step_ms / 1e3) / 1e9
+    n_kernels = 8 * info["groups"]
+    out = dict(value=value, t=t, info=info, clocks=clk, prof=prof, fct_step_ms=fct_step_ms,
+               finite=finite, mesh=mesh, cfg=cfg, alg_bytes=alg,
+               roofline=dict(bound="hbm", kernel="fct step (8 stage kernels)",
+                             achieved=achieved, peak=pk["hbm_gbs"], unit="GB/s",
+                             frac=achieved / pk["hbm_gbs"], peak_source=pk["source"],
+                             traffic=None, alg_bytes_per_step=alg),
+               gpu_launches=n_kernels * S * args.steps)
+
+    # plain one-instance-per-launch comparison (the reference's call granularity:
+    # one tracer per advect_one_fct call), member 0, one FCT step per call
+    if D.rank == 0 and member_inputs[0] is not None:
+        from fesom_jax_b200.tracer_adv import get_plan
+        inp = member_inputs[0]
+        plan = get_plan(mesh, D.local_rank)
+        outb = torch.empty_like(inp["T"][0])
+        for _ in range(2):
+            plan.forward(inp["uv"], inp["w_e"], inp["helem"], inp["hnode"], inp["hnode_new"],
+                         inp["T"][0], inp["T_old"][0], cfg["dt"], out=outb)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        reps = 3
+        for _ in range(reps):
+            for tr in range(cfg["ntr"]):
+                plan.forward(inp["uv"], inp["w_e"], inp["helem"], inp["hnode"],
+                             inp["hnode_new"], inp["T"][tr], inp["T_old"][tr], cfg["dt"],
+                             out=outb)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        tp = e0.elapsed_time(e1) / 1e3
+        out["plain"] = dict(value=reps * cfg["ntr"] * mesh.n_wet_layers / tp, unit=UNIT,
+                            how="fct_forward, 1 tracer per call, 1 FCT step per call")
+        if not args.no_e2e:
+            out["e2e"] = e2e_host(args, mesh, cfg, dev)
+        if not args.no_cpu:
+            host = {k: (v.cpu().numpy() if hasattr(v, "cpu") else v) for k, v in inp.items()}
+            out["cpu_baseline"] = cpu_oracle_rate(mesh, host, cfg["ntr"], cfg["dt"])
+    ens.close()
+    return out
+
+
+def e2e_host(args, mesh, cfg, dev) -> dict:
+    """The same metric through the public ensemble API with HOST buffers: every bench step
+    copies each member's inputs (T, T_old, uv, w_e) from pinned host memory, runs the
+    FCT steps and copies the final T back; copies are inside the timed region."""
+    import torch
+
+    from fesom_jax_b200 import workloads as W
+    from fesom_jax_b200.ensemble import Ensemble
+    nm = min(args.e2e_members, cfg["members"])
+    thick = W.rest_thickness_gpu(mesh, dev)
+    ens = Ensemble(device=dev.index, workspace_budget=int(args.workspace_gb * (1 << 30)))
+    host = []
+    for i in range(nm):
+        inp = W.member_inputs_gpu(mesh, seed=500000 + i, ntr=cfg["ntr"], device=dev,
+                                  thickness=thick, sigma=cfg["sigma"], n_vortices=cfg["n_vortices"])
+        ens.add_member(mesh, inp["uv"], inp["w_e"], inp["helem"], inp["hnode"], inp["hnode_new"],
+                       inp["T"], inp["T_old"], cfg["dt"])
+        host.append({k: inp[k].cpu().pin_memory() for k in ("T", "T_old", "uv", "w_e")})
+        host[-1]["out"] = torch.empty_like(host[-1]["T"]).pin_memory()
+        del inp
+    ens.build()
+    S = cfg["fct_steps"]
+    stream = torch.cuda.current_stream(dev)
+    h2d = sum(h[k].numel() * 8 for h in host for k in ("T", "T_old", "uv", "w_e"))
+    d2h = sum(h["out"].numel() * 8 for h in host)
+
+    def one():
+        for i, h in enumerate(host):
+            mb = ens.members[i]
+            ens.set_state(i, h["T"], h["T_old"], non_blocking=True)
+            mb.uv.copy_(h["uv"], non_blocking=True)
+            mb.w_e.copy_(h["w_e"], non_blocking=True)
+        ens.run(S)
+        for i, h in enumerate(host):
+            h["out"].copy_(ens.state(i)[0], non_blocking=True)
+
+    for _ in range(max(1, min(args.warmup, 2))):
+        one()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = max(1, min(args.steps, 3))
+    w0 = time.perf_counter()
+    e0.record(stream)
+    for _ in range(reps):
+        one()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - w0
+    t = max(e0.elapsed_time(e1) / 1e3, 1e-9)
+    upd = ens.info()["updates_per_step"] * S * reps
+    ens.close()
+    return dict(value=upd / t, unit=UNIT, h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h,
+                members=nm, steps=reps, wall_s=wall,
+                how="Ensemble API, pinned host buffers in/out every step")
+
+
+# ------------------------------------------------------------------ reference arm
+def run_reference(args, D: Dist):
+    """CPU arm: the C restatement of the reference algorithm on the box's host cores
+    (JAX is not installed, so the reference's own jax.jit CPU path cannot run); rank 0
+    only, each step one member x ntr tracers x 1 FCT step of the same workload."""
+    if D.rank != 0:
+        return
+    from fesom_jax_b200 import inputs as I
+    from fesom_jax_b200 import workloads as W
+    from oracle import fct_c
+    cfg = dict(W.WORKLOADS[args.config])
+    mesh = W.make_workload_mesh(args.config, seed=0)
+    f = I.make_fields(mesh, seed=1, n_passive=max(cfg["ntr"] - 2, 0), ab2=True,
+                      sigma=cfg["sigma"])
+    ntr = cfg["ntr"]
+    keep = []
+    from fesom_jax_b200 import _lib as fl
+    desc = fl.mesh_desc(mesh, keep)
+
+    def step():
+        for t in range(ntr):
+            fct_c.advect_one_fct(mesh, f.uv, f.w_e, f.helem, f.hnode, f.hnode_new,
+                                 f.tracers[t], f.tracers_old[t], dt=cfg["dt"], desc=desc)
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    t = time.perf_counter() - t0
+    value = args.steps * ntr * mesh.n_wet_layers / t
+    cores = fct_c.max_threads()
+    sample = (f"C loop restatement (OpenMP, {cores} threads): per step 1 member x {ntr} "
+              f"tracers x 1 FCT step on {mesh.name}")
+    line = dict(metric=METRIC, value=value, unit=UNIT, impl="reference", n_gpus=args.gpus,
+                steps=args.steps, warmup=args.warmup, ms_per_step=t / args.steps * 1e3,
+                higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64",
+                data="synthetic", config=workload_config(args.config, cfg, mesh),
+                cpu_baseline=dict(value=value, unit=UNIT, cores=cores, kind="port",
+                                  sample=sample),
+                e2e=dict(value=value, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(name, cfg, mesh) -> dict:
+    return dict(workload=f"{name}: FCT tracer advection, {mesh.name} mesh", nod2D=mesh.nod2D,
+                elem2D=mesh.elem2D, edge2D=mesh.edge2D, nl=mesh.nl,
+                wet_node_layers=mesh.n_wet_layers, members=cfg["members"], tracers=cfg["ntr"],
+                fct_steps_per_bench_step=cfg["fct_steps"], dt=cfg["dt"],
+                l2="inputs larger than L2 (resident state >> 126 MB)",
+                parallelism="replicas: members per GPU, no collective")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=["batched", "pi", "large"], default="batched")
+    ap.add_argument("--members", type=int, default=0)
+    ap.add_argument("--fct-steps", type=int, default=0)
+    ap.add_argument("--ntr", type=int, default=0, help="override tracers per member")
+    ap.add_argument("--workspace-gb", type=float, default=40.0)
+    ap.add_argument("--e2e-members", type=int, default=8)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    D = Dist()
+    if args.impl == "reference":
+        run_reference(args, D)
+        return
+    D.init("nccl")
+    try:
+        r = run_ours(args, D)
+    finally:
+        D.close()
+    if D.rank != 0 or r is None:
+        return
+    cfg, mesh = r["cfg"], r["mesh"]
+    line = dict(metric=METRIC, value=r["value"], unit=UNIT, n_gpus=D.world, steps=args.steps,
+                warmup=args.warmup, ms_per_step=r["t"] / args.steps * 1e3,
+                higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64",
+                data="synthetic (seeded mesh, velocities and tracers)",
+                config=workload_config(args.config, cfg, mesh), roofline=r["roofline"],
+                clocks=r["clocks"], gpu_launches=r["gpu_launches"],
+                fct_step_ms=r["fct_step_ms"], stage_ms=r["prof"], finite=r["finite"],
+                batch=r["info"])
+    for k in ("plain", "e2e", "cpu_baseline"):
+        if k in r:
+            line[k] = r[k]
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -125,7 +125,7 @@ __device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i) {
       for (int j = e0; j < e1; ++j) {
         const int idx = m.ne_idx[j];
         const int e = idx >> 1;
-        const double vf = in.ws.vflux[int64_t(e) * L + k];
+        const double vf = (k >= m.ekmin[e] && k < m.ekmax[e]) ? in.ws.vflux[int64_t(e) * L + k] : 0.0;
         const double avf = fabs(vf);
         const int n1 = m.edges[2 * e], n2 = m.edges[2 * e + 1];
         const double fl = -0.5 * (T[int64_t(n1) * L + k] * (vf + avf) +
@@ -289,9 +289,15 @@ __device__ __forceinline__ void body_node_cluster(const Inst& in, int64_t i) {
   for (int t = 0; t < in.ntr; ++t) {
     double mx = -INFINITY, mn = INFINITY;
     for (int j = c0; j < c1; ++j) {
-      const int64_t q = t * in.ws.sE + int64_t(m.nel_idx[j]) * L + k;
-      mx = fmax(mx, in.ws.amax[q]);
-      mn = fmin(mn, in.ws.amin[q]);
+      const int el = m.nel_idx[j];
+      if (k >= m.eul[el] && k < m.enl[el]) {
+        const int64_t q = t * in.ws.sE + int64_t(el) * L + k;
+        mx = fmax(mx, in.ws.amax[q]);
+        mn = fmin(mn, in.ws.amin[q]);
+      } else {   // a cell without this level pads with -+BIG (tracer_adv.py:396-397)
+        mx = fmax(mx, -kBig);
+        mn = fmin(mn, kBig);
+      }
     }
     in.ws.tvmax[t * in.ws.sN + qn] = mx;
     in.ws.tvmin[t * in.ws.sN + qn] = mn;
@@ -335,8 +341,9 @@ __device__ __forceinline__ void body_node_factors(const Inst& in, int64_t i) {
     const double neg_v = fmin(fvt, 0.0) + fmin(-fvb, 0.0);
     double sp = 0.0, sm = 0.0;
     for (int j = e0; j < e1; ++j) {
-      const int idx = m.ne_idx[j];
-      const double a = in.ws.adfh[t * in.ws.sEd + int64_t(idx >> 1) * L + k];
+      const int idx = m.ne_idx[j], e = idx >> 1;
+      if (k < m.ekmin[e] || k >= m.ekmax[e]) continue;   // no flux on this level
+      const double a = in.ws.adfh[t * in.ws.sEd + int64_t(e) * L + k];
       const double s = (idx & 1) ? -a : a;
       sp += fmax(s, 0.0);
       sm += fmin(s, 0.0);
@@ -357,7 +364,7 @@ __device__ __forceinline__ void body_node_factors(const Inst& in, int64_t i) {
 // Limited vertical antidiffusive flux at interface j (tracer_adv.py:453-459).
 __device__ __forceinline__ double adfv_lim(const double* adfv, const double* pf,
                                            const double* mf, int j, int nzmin, int nzmax) {
-  if (j > nzmax) return 0.0;
+  if (j >= nzmax && j != nzmin) return 0.0;   // adf_v[nzmax] == 0 by construction
   const double f = adfv[j];
   double ae;
   if (j == nzmin) {
@@ -392,6 +399,7 @@ __device__ __forceinline__ void body_node_final(const Inst& in, int64_t i) {
     for (int j = e0; j < e1; ++j) {
       const int idx = m.ne_idx[j];
       const int e = idx >> 1;
+      if (k < m.ekmin[e] || k >= m.ekmax[e]) continue;   // no flux on this level
       const double a = in.ws.adfh[t * in.ws.sEd + int64_t(e) * L + k];
       const int64_t p1 = int64_t(m.edges[2 * e]) * L + k, p2 = int64_t(m.edges[2 * e + 1]) * L + k;
       const double ae = a >= 0.0 ? fmin(pf[p1], mf[p2]) : fmin(mf[p1], pf[p2]);
@@ -412,7 +420,7 @@ __device__ __forceinline__ void body_node_final(const Inst& in, int64_t i) {
 __device__ __forceinline__ void body_copy_dry(const Inst& in, int64_t i) {
   const DevMesh& m = *in.m;
   const int64_t NL = int64_t(m.N) * m.L;
-  if (i >= NL || !in.copy_dry) return;
+  if (i >= NL) return;
   const int n = int(i / m.L), k = int(i - int64_t(n) * m.L);
   if (k >= m.nzmin[n] && k < m.nzmax[n]) return;
   for (int t = 0; t < in.ntr; ++t) in.T_new[t * in.tstride + i] = in.T[t * in.tstride + i];
@@ -437,32 +445,55 @@ FCT_KERNEL_PAIR(k_copy_dry, body_copy_dry)
 
 }  // namespace
 
-int launch_forward(const Inst& single, const Inst* tab, int n, const LaunchDims& d,
-                   cudaStream_t s) {
+const char* const kStageNames[kNumStages] = {
+    "vflux", "elem_grad", "node_lo", "vert_impl", "edge_adf", "elem_bounds",
+    "node_cluster", "node_factors", "node_final", "copy_dry"};
+
+int launch_forward_events(const Inst& single, const Inst* tab, int n, const LaunchDims& d,
+                          cudaStream_t s, cudaEvent_t* after) {
   constexpr int B = 256;
   auto grid = [&](int64_t lanes) {
     return dim3(unsigned(std::max<int64_t>(1, (lanes + B - 1) / B)), unsigned(n), 1);
   };
-#define FCT_LAUNCH(name, lanes)                                   \
-  do {                                                            \
-    if (tab) name##_n<<<grid(lanes), B, 0, s>>>(tab);             \
-    else name##_1<<<grid(lanes), B, 0, s>>>(single);              \
+  int stage = 0;
+  auto mark = [&]() {
+    if (after) cudaEventRecord(after[stage], s);
+    ++stage;
+  };
+#define FCT_LAUNCH(name, lanes, enabled)                            \
+  do {                                                              \
+    if (enabled) {                                                  \
+      if (tab) name##_n<<<grid(lanes), B, 0, s>>>(tab);             \
+      else name##_1<<<grid(lanes), B, 0, s>>>(single);              \
+    }                                                               \
+    mark();                                                         \
   } while (0)
-  const bool any_wi = tab ? true : (single.w_i != nullptr);
-  FCT_LAUNCH(k_vflux, d.max_edge);
-  FCT_LAUNCH(k_elem_grad, d.max_elem);
-  FCT_LAUNCH(k_node_lo, d.max_iface);
-  if (any_wi) FCT_LAUNCH(k_vert_impl, d.max_nodes);
-  FCT_LAUNCH(k_edge_adf, d.max_edge);
-  FCT_LAUNCH(k_elem_bounds, d.max_elem);
-  FCT_LAUNCH(k_node_cluster, d.max_layer);
-  FCT_LAUNCH(k_node_factors, d.max_layer);
-  FCT_LAUNCH(k_node_final, d.max_layer);
-  FCT_LAUNCH(k_copy_dry, d.max_dense);
+  FCT_LAUNCH(k_vflux, d.max_edge, true);
+  FCT_LAUNCH(k_elem_grad, d.max_elem, true);
+  FCT_LAUNCH(k_node_lo, d.max_iface, true);
+  FCT_LAUNCH(k_vert_impl, d.max_nodes, d.any_wi);
+  FCT_LAUNCH(k_edge_adf, d.max_edge, true);
+  FCT_LAUNCH(k_elem_bounds, d.max_elem, true);
+  FCT_LAUNCH(k_node_cluster, d.max_layer, true);
+  FCT_LAUNCH(k_node_factors, d.max_layer, true);
+  FCT_LAUNCH(k_node_final, d.max_layer, true);
+  FCT_LAUNCH(k_copy_dry, d.max_dense, d.copy_dry);
 #undef FCT_LAUNCH
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_error(e, "forward kernel launch");
   return FCT_OK;
+}
+
+int launch_forward(const Inst& single, const Inst* tab, int n, const LaunchDims& d,
+                   cudaStream_t s) {
+  return launch_forward_events(single, tab, n, d, s, nullptr);
+}
+
+int launch_copy_dry(const Inst* tab, int n, int64_t max_dense, cudaStream_t s) {
+  const dim3 g(unsigned(std::max<int64_t>(1, (max_dense + 255) / 256)), unsigned(n), 1);
+  k_copy_dry_n<<<g, 256, 0, s>>>(tab);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? FCT_OK : cuda_error(e, "copy_dry launch");
 }
 
 }  // namespace fct

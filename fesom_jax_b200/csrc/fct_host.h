@@ -30,12 +30,19 @@ inline int cuda_error(cudaError_t e, const char* what) {
 struct LaunchDims {
   int64_t max_iface, max_layer, max_edge, max_elem, max_dense, max_nodes;
   int max_ntr;
+  bool any_wi;      // launch the implicit w_i stage
+  bool copy_dry;    // launch the dry-level copy
 };
 int launch_forward(const Inst& single, const Inst* tab, int n, const LaunchDims& d,
                    cudaStream_t s);
+// Same, recording ``after[i]`` on ``s`` after stage i (skipped stages record too).
+constexpr int kNumStages = 10;
+extern const char* const kStageNames[kNumStages];
+int launch_forward_events(const Inst& single, const Inst* tab, int n, const LaunchDims& d,
+                          cudaStream_t s, cudaEvent_t* after);
 
-// Fill a workspace with its resting values (BIG bounds, unit factors, zeros).
-int init_workspace(const Workspace& ws, int ntr, cudaStream_t s);
+// Copy T's dry levels into T_new for ``n`` instances of ``tab`` (ignores Inst::copy_dry).
+int launch_copy_dry(const Inst* tab, int n, int64_t max_dense, cudaStream_t s);
 
 Workspace carve_workspace(double* base, int64_t N, int64_t E, int64_t Ed, int64_t L, int ntr);
 int64_t workspace_doubles(int64_t N, int64_t E, int64_t Ed, int64_t L, int ntr);

@@ -52,6 +52,8 @@ struct DevMesh {
   const int* eupdn;      // [Ed,2]
   const double* cross;   // [Ed,4]
   const double* ecoef;   // [Ed,2]: edx*a, edy*R  (a = R*cos, averaged over the two cells)
+  const int* ekmin;      // [Ed] first level of the edge's lanes (union of its cells' layers)
+  const int* ekmax;      // [Ed] one past the last such level
   // vertical
   const double* Zp;      // [L]  Z padded with Z[L-2] (tracer_adv.py:233)
   const double* zbar;    // [L]
@@ -63,14 +65,17 @@ struct DevMesh {
 };
 
 // Per-tracer intermediates of one instance (dense [entity, L]; tracer t at +t*stride).
+// Kernels read only entries written earlier in the same step (every reader masks by the
+// level range of the entity it reads), so a workspace needs no initial values and may be
+// shared by instances of different meshes that run one after another.
 struct Workspace {
   double* vflux;                 // [Ed,L] shared by all tracers of the instance
   double *gx, *gy;               // [E,L] element gradients
-  double *amax, *amin;           // [E,L] per-element cluster bounds (init -+BIG)
+  double *amax, *amin;           // [E,L] per-element cluster bounds
   double *lo, *gnx, *gny;        // [N,L]
   double* adfv;                  // [N,L] antidiffusive vertical flux (interfaces)
   double *tvmax, *tvmin;         // [N,L]
-  double *pf, *mf;               // [N,L] limiter factors (init 1)
+  double *pf, *mf;               // [N,L] limiter factors
   double* adfh;                  // [Ed,L] antidiffusive horizontal flux
   int64_t sN, sE, sEd;           // per-tracer strides (doubles)
 };
@@ -86,7 +91,6 @@ struct Inst {
   Workspace ws;
   double dt;
   int ntr;
-  int copy_dry;   // 1: write T_new = T on dry levels (fresh output buffers)
 };
 
 }  // namespace fct

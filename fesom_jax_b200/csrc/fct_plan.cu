@@ -127,36 +127,6 @@ int validate_desc(const FctMeshDesc* d) {
 
 }  // namespace
 
-__global__ void k_fill(double* p, int64_t n, double v) {
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
-       i += int64_t(gridDim.x) * blockDim.x)
-    p[i] = v;
-}
-
-int init_workspace(const Workspace& ws, int ntr, cudaStream_t s) {
-  auto fill = [&](double* p, int64_t n, double v) -> int {
-    if (n <= 0) return FCT_OK;
-    int blocks = int(std::min<int64_t>((n + 255) / 256, 148 * 16));
-    k_fill<<<blocks, 256, 0, s>>>(p, n, v);
-    FCT_CUDA(cudaGetLastError());
-    return FCT_OK;
-  };
-  int st;
-  if ((st = fill(ws.vflux, ws.sEd, 0.0))) return st;
-  double* zero_fields[] = {ws.gx, ws.gy};
-  for (double* p : zero_fields)
-    if ((st = fill(p, ntr * ws.sE, 0.0))) return st;
-  if ((st = fill(ws.amax, ntr * ws.sE, -kBig))) return st;
-  if ((st = fill(ws.amin, ntr * ws.sE, kBig))) return st;
-  double* zn[] = {ws.lo, ws.gnx, ws.gny, ws.adfv, ws.tvmax, ws.tvmin};
-  for (double* p : zn)
-    if ((st = fill(p, ntr * ws.sN, 0.0))) return st;
-  if ((st = fill(ws.pf, ntr * ws.sN, 1.0))) return st;
-  if ((st = fill(ws.mf, ntr * ws.sN, 1.0))) return st;
-  if ((st = fill(ws.adfh, ntr * ws.sEd, 0.0))) return st;
-  return FCT_OK;
-}
-
 }  // namespace fct
 
 using namespace fct;
@@ -198,6 +168,17 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
     ecoef[2 * e] = d->edge_dxdy[2 * e] * a;
     ecoef[2 * e + 1] = d->edge_dxdy[2 * e + 1] * kREarth;
   }
+  std::vector<int> ekmin(Ed), ekmax(Ed);
+  for (int e = 0; e < Ed; ++e) {
+    const int el1 = d->edge_tri[2 * e], el2 = d->edge_tri[2 * e + 1];
+    int lo = eul[el1], hi = enl[el1];
+    if (el2 >= 0) {
+      lo = std::min(lo, eul[el2]);
+      hi = std::max(hi, enl[el2]);
+    }
+    ekmin[e] = std::max(lo, 0);
+    ekmax[e] = std::min(hi, L);
+  }
   std::vector<double> Zp(L);
   for (int k = 0; k < L - 1; ++k) Zp[k] = d->Z[k];
   Zp[L - 1] = d->Z[L - 2];
@@ -215,16 +196,9 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
       eleml.push_back((uint32_t(e) << kLevelBits) | uint32_t(k));
       ++wet_elem;
     }
-  for (int e = 0; e < Ed; ++e) {
-    const int el1 = d->edge_tri[2 * e], el2 = d->edge_tri[2 * e + 1];
-    int lo = eul[el1], hi = enl[el1];
-    if (el2 >= 0) {
-      lo = std::min(lo, eul[el2]);
-      hi = std::max(hi, enl[el2]);
-    }
-    for (int k = std::max(lo, 0); k < std::min(hi, L); ++k)
+  for (int e = 0; e < Ed; ++e)
+    for (int k = ekmin[e]; k < ekmax[e]; ++k)
       edgel.push_back((uint32_t(e) << kLevelBits) | uint32_t(k));
-  }
   P->n_wet_elem_layers = wet_elem;
 
   Blob b;
@@ -242,6 +216,7 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   size_t o_eud = b.add(d->edge_up_dn_tri, 2 * size_t(Ed));
   size_t o_cross = b.add(d->edge_cross_dxdy, 4 * size_t(Ed));
   size_t o_ecoef = b.add(ecoef.data(), ecoef.size());
+  size_t o_ekmin = b.add(ekmin.data(), Ed), o_ekmax = b.add(ekmax.data(), Ed);
   size_t o_Zp = b.add(Zp.data(), L), o_zbar = b.add(d->zbar, L);
   size_t o_if = b.add(iface.data(), iface.size()), o_ly = b.add(layer.data(), layer.size());
   size_t o_ed = b.add(edgel.data(), edgel.size()), o_el = b.add(eleml.data(), eleml.size());
@@ -272,6 +247,8 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   m.eupdn = (const int*)(base + o_eud);
   m.cross = (const double*)(base + o_cross);
   m.ecoef = (const double*)(base + o_ecoef);
+  m.ekmin = (const int*)(base + o_ekmin);
+  m.ekmax = (const int*)(base + o_ekmax);
   m.Zp = (const double*)(base + o_Zp);
   m.zbar = (const double*)(base + o_zbar);
   m.iface_lanes = (const uint32_t*)(base + o_if);  m.n_iface = int64_t(iface.size());
@@ -308,9 +285,6 @@ int fct_plan_reserve(FctPlan* P, int max_tracers) {
   double* ws = nullptr;
   FCT_CUDA(cudaMalloc(&ws, size_t(nd) * sizeof(double)));
   Workspace w = carve_workspace(ws, P->N, P->E, P->Ed, P->L, max_tracers);
-  int st = init_workspace(w, max_tracers, 0);
-  if (st) { cudaFree(ws); return st; }
-  FCT_CUDA(cudaDeviceSynchronize());
   if (P->d_ws) cudaFree(P->d_ws);
   P->d_ws = ws;
   P->ws = w;
@@ -361,9 +335,8 @@ int fct_forward(FctPlan* P, const FctFields* f, double dt, int ntr, fct_stream_t
   in.ws = P->ws;
   in.dt = dt;
   in.ntr = ntr;
-  in.copy_dry = 1;
   LaunchDims dims{P->hm.n_iface, P->hm.n_layer, P->hm.n_edge, P->hm.n_elem,
-                  int64_t(P->N) * P->L, int64_t(P->N), ntr};
+                  int64_t(P->N) * P->L, int64_t(P->N), ntr, f->w_i != nullptr, true};
   int prev = -1;
   cudaGetDevice(&prev);
   if (prev != P->device) cudaSetDevice(P->device);

@@ -1,0 +1,202 @@
+"""Resident ensembles: many FCT instances advanced together on one GPU.
+
+The reference advances one tracer of one model per ``advect_one_fct`` call from a host
+time loop (fesom_jax/step.py:497-516, integrate.py:43-169). An :class:`Ensemble` keeps
+every member's velocities, thicknesses and three rotating tracer buffers resident in HBM
+and advances all members (each with ``ntr`` tracers sharing its velocities, on meshes of
+any size) with the batched C ABI (``fct_batch_*``): one launch per stage for all
+members of a workspace group, multi-step runs captured once as a CUDA graph.
+
+The AB2 history rotates through the three buffers (step ``p`` reads ``T_old = buf[p%3]``,
+``T = buf[(p+1)%3]`` and writes ``buf[(p+2)%3]``), which is exactly the reference's
+``(T, T_old) <- advect_one_fct(..., T, T_old)`` carry with ``T_old_new = T``.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+
+import numpy as np
+
+from . import _lib
+from .mesh import Mesh
+from .tracer_adv import FctPlan
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("Ensemble needs a CUDA GPU; there is no CPU fallback")
+    return torch
+
+
+class FctInstance(C.Structure):
+    _fields_ = [("plan", C.c_void_p), ("uv", C.c_void_p), ("w_e", C.c_void_p),
+                ("helem", C.c_void_p), ("hnode", C.c_void_p), ("hnode_new", C.c_void_p),
+                ("buf", C.c_void_p * 3), ("ntr", C.c_int), ("dt", C.c_double)]
+
+
+def _bind_batch(L):
+    if getattr(L, "_batch_bound", False):
+        return L
+    L.fct_batch_create.argtypes = [C.POINTER(FctInstance), C.c_int, C.c_int64, C.POINTER(C.c_void_p)]
+    L.fct_batch_destroy.argtypes = [C.c_void_p]
+    L.fct_batch_info.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
+    L.fct_batch_prepare.argtypes = [C.c_void_p, C.c_void_p]
+    L.fct_batch_step.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+    L.fct_batch_run.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+    L.fct_batch_profile.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.c_int,
+                                    C.c_void_p]
+    L.fct_stage_name.restype = C.c_char_p
+    for n in ("fct_batch_create", "fct_batch_destroy", "fct_batch_info", "fct_batch_prepare",
+              "fct_batch_step", "fct_batch_run", "fct_batch_profile"):
+        getattr(L, n).restype = C.c_int
+    L._batch_bound = True
+    return L
+
+
+@dataclasses.dataclass
+class Member:
+    """One ensemble member: a mesh and its ``ntr`` tracers' device state."""
+
+    mesh: Mesh
+    ntr: int
+    dt: float
+    uv: object          # torch [E, nl, 2]
+    w_e: object         # torch [N, nl]
+    helem: object
+    hnode: object
+    hnode_new: object
+    buf: object         # torch [3, ntr, N, nl]
+
+
+class Ensemble:
+    """Members resident on ``device``; see the module docstring."""
+
+    def __init__(self, device: int = 0, workspace_budget: int = 24 << 30):
+        self.torch = _torch()
+        self.device = int(device)
+        self.workspace_budget = int(workspace_budget)
+        self.members: list[Member] = []
+        self._plans: dict[int, FctPlan] = {}
+        self._h = None
+        self.phase = 0
+
+    # ---------------------------------------------------------------- members
+    def plan(self, mesh: Mesh) -> FctPlan:
+        p = self._plans.get(id(mesh))
+        if p is None:
+            p = self._plans[id(mesh)] = FctPlan(mesh, self.device, max_tracers=1)
+        return p
+
+    def add_member(self, mesh: Mesh, uv, w_e, helem, hnode, hnode_new, T, T_old, dt: float) -> int:
+        """Add a member (host numpy or device tensors); ``T``/``T_old`` are ``[ntr, N, nl]``."""
+        if self._h is not None:
+            raise RuntimeError("members must be added before the ensemble is built")
+        t = self.torch
+        dev = t.device("cuda", self.device)
+
+        def d(x):
+            if isinstance(x, np.ndarray):
+                return t.from_numpy(np.ascontiguousarray(x, np.float64)).to(dev)
+            return x.to(device=dev, dtype=t.float64).contiguous()
+
+        T, T_old = d(T), d(T_old)
+        if T.dim() == 2:
+            T, T_old = T[None], T_old[None]
+        ntr = int(T.shape[0])
+        N, nl = mesh.nod2D, mesh.nl
+        if tuple(T.shape) != (ntr, N, nl) or tuple(T_old.shape) != (ntr, N, nl):
+            raise ValueError("T/T_old must be [ntr, nod2D, nl]")
+        buf = t.empty((3, ntr, N, nl), dtype=t.float64, device=dev)
+        buf[0].copy_(T_old)
+        buf[1].copy_(T)
+        buf[2].copy_(T)
+        self.plan(mesh)
+        self.members.append(Member(mesh, ntr, float(dt), d(uv), d(w_e), d(helem), d(hnode),
+                                   d(hnode_new), buf))
+        return len(self.members) - 1
+
+    # ------------------------------------------------------------------ build
+    def build(self) -> None:
+        L = _bind_batch(_lib.lib())
+        n = len(self.members)
+        if n == 0:
+            raise ValueError("empty ensemble")
+        arr = (FctInstance * n)()
+        for i, mb in enumerate(self.members):
+            q = arr[i]
+            q.plan = self.plan(mb.mesh).handle.value
+            q.uv, q.w_e, q.helem = mb.uv.data_ptr(), mb.w_e.data_ptr(), mb.helem.data_ptr()
+            q.hnode, q.hnode_new = mb.hnode.data_ptr(), mb.hnode_new.data_ptr()
+            for j in range(3):
+                q.buf[j] = mb.buf[j].data_ptr()
+            q.ntr, q.dt = mb.ntr, mb.dt
+        h = C.c_void_p()
+        _lib.check(L.fct_batch_create(arr, n, self.workspace_budget, C.byref(h)))
+        self._h = h
+        self.phase = 0
+        self.prepare()
+
+    def info(self) -> dict:
+        out = (C.c_int64 * 4)()
+        _lib.check(_bind_batch(_lib.lib()).fct_batch_info(self._h, out))
+        return dict(instances=out[0], groups=out[1], workspace_bytes=out[2],
+                    updates_per_step=out[3])
+
+    def _stream(self, stream):
+        t = self.torch
+        return C.c_void_p(int(stream if stream is not None
+                              else t.cuda.current_stream(self.device).cuda_stream))
+
+    def prepare(self, stream=None) -> None:
+        """Make the dry levels of all three buffers equal (they never change)."""
+        _lib.check(_bind_batch(_lib.lib()).fct_batch_prepare(self._h, self._stream(stream)))
+
+    def step(self, stream=None) -> None:
+        _lib.check(_bind_batch(_lib.lib()).fct_batch_step(self._h, self.phase % 3,
+                                                          self._stream(stream)))
+        self.phase += 1
+
+    def run(self, steps: int, stream=None) -> None:
+        """``steps`` FCT steps of every member as one CUDA graph launch."""
+        _lib.check(_bind_batch(_lib.lib()).fct_batch_run(self._h, self.phase % 3, int(steps),
+                                                         self._stream(stream)))
+        self.phase += int(steps)
+
+    def profile_step(self, stream=None) -> dict:
+        """Run one step stage by stage (synchronising) and return ``{stage: ms}``."""
+        L = _bind_batch(_lib.lib())
+        ms = (C.c_double * 16)()
+        _lib.check(L.fct_batch_profile(self._h, self.phase % 3, ms, 16, self._stream(stream)))
+        self.phase += 1
+        out = {}
+        for i in range(16):
+            name = L.fct_stage_name(i).decode()
+            if name:
+                out[name] = float(ms[i])
+        return out
+
+    # ------------------------------------------------------------------ state
+    def state(self, i: int):
+        """``(T, T_old)`` views ``[ntr, N, nl]`` of member ``i`` (device)."""
+        b = self.members[i].buf
+        p = self.phase
+        return b[(p + 1) % 3], b[p % 3]
+
+    def set_state(self, i: int, T, T_old, non_blocking: bool = False) -> None:
+        Tc, To = self.state(i)
+        Tc.copy_(T, non_blocking=non_blocking)
+        To.copy_(T_old, non_blocking=non_blocking)
+
+    def close(self) -> None:
+        if self._h is not None and self._h.value:
+            _bind_batch(_lib.lib()).fct_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

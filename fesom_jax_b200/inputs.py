@@ -7,8 +7,9 @@ generated directly with the shapes, layouts and value ranges the workloads name:
     ``hnode[n,k] = zbar[k]-zbar[k+1]`` on wet layers, ``helem`` likewise, 0 elsewhere;
   * ``T`` 2-28 degC decreasing with the layer mid-depth ``Z`` plus N(0, 0.5) noise,
     ``S`` 34-36 psu increasing with depth plus N(0, 0.1), both 0 below the bottom;
-  * element velocities ``u, v ~ N(0, sigma)`` with a linear decay with depth, masked
-    to each element's layers;
+  * element velocities with standard deviation ``sigma`` (default 0.1 m/s) from a smooth
+    seeded streamfunction, with a linear decay with depth, masked to each element's
+    layers (:func:`velocities`);
   * ``w`` from discrete continuity, :func:`compute_w` (fesom_jax/ale.py:309-365).
 """
 
@@ -80,53 +81,73 @@ def passive_tracer(mesh: Mesh, rng: np.random.Generator) -> np.ndarray:
     return np.where(mesh.node_layer_mask, rng.uniform(0.0, 1.0, (mesh.nod2D, mesh.nl)), 0.0)
 
 
-def element_centres(mesh: Mesh):
-    """Element centroid (lon, lat) in rotated radians, cyclic-safe in lon."""
-    lon = mesh.coord_nod2D[:, 0][mesh.elem_nodes]
-    lat = mesh.coord_nod2D[:, 1][mesh.elem_nodes]
-    half = 0.5 * 2.0 * np.pi
-    d = lon - lon[:, :1]
-    lon = np.where(d > half, lon - 2 * np.pi, np.where(d < -half, lon + 2 * np.pi, lon))
-    return lon.mean(axis=1), lat.mean(axis=1)
+def node_xyz(mesh: Mesh) -> np.ndarray:
+    lon, lat = mesh.coord_nod2D[:, 0], mesh.coord_nod2D[:, 1]
+    return np.stack([np.cos(lat) * np.cos(lon), np.cos(lat) * np.sin(lon), np.sin(lat)], 1)
 
 
-def velocities(mesh: Mesh, rng: np.random.Generator, sigma: float = 0.1,
+def streamfunction_velocity(mesh: Mesh, psi: np.ndarray) -> np.ndarray:
+    """Element velocity ``(u, v) = (-dpsi/dy, dpsi/dx)`` ``[E, 2]`` of a nodal P1
+    streamfunction, using the mesh's own ``gradient_sca``. The edge face fluxes of such a
+    field telescope around every interior node's dual cell, so its discrete divergence
+    (and hence ``w``) comes only from coasts and bathymetry steps."""
+    t = psi[mesh.elem_nodes]
+    gs = mesh.gradient_sca
+    gx = (gs[:, 0:3] * t).sum(1)
+    gy = (gs[:, 3:6] * t).sum(1)
+    return np.stack([-gy, gx], axis=1)
+
+
+def velocities(mesh: Mesh, rng: np.random.Generator, sigma: float = 0.1, kind: str = "psi",
                n_vortices: int = 0, vortex_radius_km=(50.0, 200.0),
                vortex_speed: float = 0.5) -> np.ndarray:
-    """Element velocities ``uv [E, nl, 2]`` (m/s).
-
-    ``u, v ~ N(0, sigma)`` per element, times a linear decay ``1 - 0.9*|Z_k|/max|Z|``,
-    masked to each element's layers. ``n_vortices > 0`` adds seeded Gaussian eddies
-    (azimuthal speed ``vortex_speed * r/R * exp(1/2 - r^2/(2R^2))``, radius ``R`` drawn
-    from ``vortex_radius_km``) centred on random elements.
-    """
-    E, nl = mesh.elem2D, mesh.nl
+    """Element velocities ``uv [E, nl, 2]`` (m/s): :func:`velocity_base` expanded over the
+    levels with the linear decay and masked to each element's layers."""
+    base = velocity_base(mesh, rng, sigma, kind, n_vortices, vortex_radius_km, vortex_speed)
     decay = 1.0 - 0.9 * layer_depth_fraction(mesh)
-    base = rng.normal(0.0, sigma, (E, 2))
+    uv = base[:, None, :] * decay[None, :, None]
+    return np.where(mesh.elem_layer_mask[:, :, None], uv, 0.0)
+
+
+def velocity_base(mesh: Mesh, rng: np.random.Generator, sigma: float = 0.1, kind: str = "psi",
+                  n_vortices: int = 0, vortex_radius_km=(50.0, 200.0),
+                  vortex_speed: float = 0.5) -> np.ndarray:
+    """Depth-independent element velocity ``[E, 2]`` (m/s) with standard deviation ``sigma``.
+
+    ``kind="psi"``: a smooth seeded random streamfunction (sum of random plane waves on the
+    sphere) turned into velocities by :func:`streamfunction_velocity` and scaled to
+    ``sigma``; ``kind="white"``: independent ``N(0, sigma)`` per element (strongly
+    divergent, large vertical CFL). Both are multiplied by the linear decay
+    ``1 - 0.9*|Z_k|/max|Z|`` and masked to each element's layers.
+    ``n_vortices > 0`` adds seeded Gaussian streamfunction eddies (radius ``R`` drawn from
+    ``vortex_radius_km``, peak azimuthal speed ``vortex_speed`` at ``r = R``).
+    """
+    E = mesh.elem2D
+    if kind == "white":
+        base = rng.normal(0.0, sigma, (E, 2))
+    elif kind == "psi":
+        xyz = node_xyz(mesh)
+        psi = np.zeros(mesh.nod2D)
+        for _ in range(24):
+            k = rng.normal(size=3)
+            k *= rng.uniform(2.0, 12.0) / np.linalg.norm(k)
+            psi += rng.normal() * np.cos(xyz @ k + rng.uniform(0.0, 2.0 * np.pi))
+        base = streamfunction_velocity(mesh, psi)
+        base *= sigma / max(base.std(), 1e-300)
+    else:
+        raise ValueError(f"unknown velocity kind {kind!r}")
     if n_vortices:
-        lon, lat = element_centres(mesh)
-        xyz = np.stack([np.cos(lat) * np.cos(lon), np.cos(lat) * np.sin(lon), np.sin(lat)], 1)
-        east = np.stack([-np.sin(lon), np.cos(lon), np.zeros_like(lon)], 1)
-        north = np.stack([-np.sin(lat) * np.cos(lon), -np.sin(lat) * np.sin(lon), np.cos(lat)], 1)
-        centres = rng.integers(0, E, n_vortices)
+        xyz = node_xyz(mesh)
+        psi = np.zeros(mesh.nod2D)
+        centres = xyz[rng.integers(0, mesh.nod2D, n_vortices)]
         radii = rng.uniform(*vortex_radius_km, n_vortices) * 1e3
         signs = rng.choice([-1.0, 1.0], n_vortices)
         for c, R, s in zip(centres, radii, signs):
-            cx = xyz[c]
-            cosang = np.clip(xyz @ cx, -1.0, 1.0)
-            r = R_EARTH * np.arccos(cosang)
-            near = r < 4.0 * R
-            if not np.any(near):
-                continue
-            # tangent direction: the centre axis crossed with the position vector
-            t = np.cross(cx[None, :], xyz[near])
-            tn = np.linalg.norm(t, axis=1, keepdims=True)
-            t = t / np.where(tn > 0, tn, 1.0)
-            speed = s * vortex_speed * (r[near] / R) * np.exp(0.5 - 0.5 * (r[near] / R) ** 2)
-            base[near, 0] += speed * np.sum(t * east[near], 1)
-            base[near, 1] += speed * np.sum(t * north[near], 1)
-    uv = base[:, None, :] * decay[None, :, None]
-    return np.where(mesh.elem_layer_mask[:, :, None], uv, 0.0)
+            r = R_EARTH * np.arccos(np.clip(xyz @ c, -1.0, 1.0))
+            near = r < 5.0 * R
+            psi[near] += s * vortex_speed * R * np.exp(0.5) * np.exp(-0.5 * (r[near] / R) ** 2)
+        base = base + streamfunction_velocity(mesh, psi)
+    return base
 
 
 @dataclasses.dataclass
@@ -144,7 +165,7 @@ class Fields:
 
 def make_fields(mesh: Mesh, seed: int = 0, n_passive: int = 0, sigma: float = 0.1,
                 ab2: bool = False, n_vortices: int = 0, uv: np.ndarray | None = None,
-                tracers: np.ndarray | None = None) -> Fields:
+                tracers: np.ndarray | None = None, kind: str = "psi") -> Fields:
     """Seeded inputs for one instance: T, S (+ passive tracers), velocities, ``w``.
 
     ``ab2=False`` gives ``T_old = T`` (step-1 convention, fesom_jax/ic.py:91-110);
@@ -157,7 +178,7 @@ def make_fields(mesh: Mesh, seed: int = 0, n_passive: int = 0, sigma: float = 0.
         tracers = np.stack(tr)
     hnode, helem = rest_thickness(mesh)
     if uv is None:
-        uv = velocities(mesh, rng, sigma=sigma, n_vortices=n_vortices)
+        uv = velocities(mesh, rng, sigma=sigma, kind=kind, n_vortices=n_vortices)
     w = compute_w(mesh, uv, helem)
     if ab2:
         pert = rng.normal(0.0, 0.05, tracers.shape) * mesh.node_layer_mask[None]

@@ -101,27 +101,37 @@ def generate_raw(n_nodes: int, zbar: np.ndarray, seed: int = 0, bottom=(5, None)
     rng = np.random.default_rng(seed)
     nl = len(zbar)
     blo, bhi = bottom[0], (bottom[1] if bottom[1] is not None else nl)
-    # fraction of the sphere kept (caps + land) -> oversample the Fibonacci set
-    keep_frac = np.sin(cap_deg * RAD) * (1.0 - 0.02 * n_land * np.mean(land_radius_deg) / 10)
-    M = int(n_nodes / max(keep_frac, 0.2)) + 16
-    i = np.arange(M) + 0.5
-    z = 1.0 - 2.0 * i / M
-    ga = PI * (3.0 - np.sqrt(5.0))
-    lon = (ga * i) % (2 * PI)
-    r = np.sqrt(1.0 - z * z)
-    xyz = np.stack([r * np.cos(lon), r * np.sin(lon), z], axis=1)
-    spacing = np.sqrt(4.0 * PI / M)
-    xyz += rng.normal(scale=jitter * spacing / 2.0, size=xyz.shape)
-    xyz /= np.linalg.norm(xyz, axis=1, keepdims=True)
-    glat = np.arcsin(np.clip(xyz[:, 2], -1, 1))
-    glon = np.arctan2(xyz[:, 1], xyz[:, 0])
-    rlon, rlat = geo_to_rot(glon, glat)
-    ocean = np.abs(rlat) < cap_deg * RAD
+    lands = []
     for _ in range(n_land):
         c = rng.normal(size=3)
-        c /= np.linalg.norm(c)
-        rad = rng.uniform(*land_radius_deg) * RAD
-        ocean &= (xyz @ c) < np.cos(rad)
+        lands.append((c / np.linalg.norm(c), rng.uniform(*land_radius_deg) * RAD))
+    jit_seed = int(rng.integers(0, 2**31 - 1))
+
+    def sphere(M):
+        i = np.arange(M) + 0.5
+        z = 1.0 - 2.0 * i / M
+        lon = (PI * (3.0 - np.sqrt(5.0)) * i) % (2 * PI)
+        r = np.sqrt(1.0 - z * z)
+        xyz = np.stack([r * np.cos(lon), r * np.sin(lon), z], axis=1)
+        xyz += np.random.default_rng(jit_seed).normal(
+            scale=jitter * np.sqrt(4.0 * PI / M) / 2.0, size=xyz.shape)
+        xyz /= np.linalg.norm(xyz, axis=1, keepdims=True)
+        glat = np.arcsin(np.clip(xyz[:, 2], -1, 1))
+        glon = np.arctan2(xyz[:, 1], xyz[:, 0])
+        rlon, rlat = geo_to_rot(glon, glat)
+        ocean = np.abs(rlat) < cap_deg * RAD
+        for c, rad in lands:
+            ocean &= (xyz @ c) < np.cos(rad)
+        return xyz, glon, glat, ocean
+
+    # size the Fibonacci set so that about n_nodes ocean nodes remain
+    M = int(n_nodes / max(np.sin(cap_deg * RAD), 0.2)) + 16
+    for _ in range(4):
+        xyz, glon, glat, ocean = sphere(M)
+        kept = int(ocean.sum())
+        if abs(kept - n_nodes) <= max(2, n_nodes // 1000):
+            break
+        M = max(16, int(round(M * n_nodes / max(kept, 1))))
     tri = ConvexHull(xyz).simplices
     tri = tri[np.all(ocean[tri], axis=1)]
     used = np.unique(tri)

@@ -110,6 +110,58 @@ int fct_plan_info(const FctPlan* plan, int64_t out[8]);
 int fct_forward(FctPlan* plan, const FctFields* fields, double dt, int ntr,
                 fct_stream_t stream);
 
+/* Vertical velocity at interfaces from continuity, fesom_jax/ale.py:309-365
+ * (``compute_w(mesh, uv, helem)``): ``w`` [nod2D,nl] (DEVICE), all levels written. */
+int fct_compute_w(FctPlan* plan, const double* uv, const double* helem, double* w,
+                  fct_stream_t stream);
+
+/*
+ * Batched ensemble stepping: many FCT instances (ensemble members x tracers, on meshes
+ * of different sizes) advanced together, one launch per stage for all instances of a
+ * workspace group. Each instance owns three rotating tracer buffers of ``ntr`` tracers
+ * (``[ntr, nod2D, nl]``, DEVICE); a step of phase p reads T_old = buf[p],
+ * T = buf[(p+1)%3] and writes T_new = buf[(p+2)%3], so consecutive phases carry the AB2
+ * history (T_old_new = T) without copies. Start with T_old in buf[0], T in buf[1].
+ */
+typedef struct FctInstance {
+  FctPlan* plan;            /* the instance's mesh */
+  const double* uv;         /* [elem2D,nl,2] */
+  const double* w_e;        /* [nod2D,nl] */
+  const double* helem;      /* [elem2D,nl] */
+  const double* hnode;      /* [nod2D,nl] */
+  const double* hnode_new;  /* [nod2D,nl] */
+  double* buf[3];           /* rotating tracer buffers, each ntr x [nod2D,nl] */
+  int ntr;
+  double dt;
+} FctInstance;
+
+typedef struct FctBatch FctBatch;
+
+/* Group the instances so that each group's workspace fits ``workspace_budget_bytes``
+ * (at least one instance per group), allocate one workspace arena (reused by the groups
+ * in turn) and the per-phase device instance tables. */
+int fct_batch_create(const FctInstance* insts, int n, int64_t workspace_budget_bytes,
+                     FctBatch** out);
+int fct_batch_destroy(FctBatch* b);
+/* [instances, groups, workspace bytes, total wet node layers x tracers] */
+int fct_batch_info(const FctBatch* b, int64_t out[4]);
+/* Copy the dry levels of buf[1] into buf[0] and buf[2] (dry levels never change). */
+int fct_batch_prepare(FctBatch* b, fct_stream_t stream);
+/* One FCT step of every instance with rotation phase ``phase`` (0, 1 or 2). */
+int fct_batch_step(FctBatch* b, int phase, fct_stream_t stream);
+/* ``steps`` consecutive steps starting at ``first_phase``, captured once into a CUDA
+ * graph (cached per (first_phase, steps)) and launched on ``stream``. The instance that
+ * holds T after the run is buf[(first_phase + steps + 1) % 3]. */
+int fct_batch_run(FctBatch* b, int first_phase, int steps, fct_stream_t stream);
+
+/* Profiling aid: run one step of phase ``phase`` stage by stage with CUDA events recorded
+ * on ``stream`` between stages, synchronise, and add each stage's time (ms, summed over
+ * workspace groups) into ``stage_ms[0..max_stages)`` (needs >= 10 entries). */
+int fct_batch_profile(FctBatch* b, int phase, double* stage_ms, int max_stages,
+                      fct_stream_t stream);
+/* Name of forward stage ``i`` (as reported by fct_batch_profile), "" if out of range. */
+const char* fct_stage_name(int i);
+
 /* Last error message on this thread ("" if none). */
 const char* fct_last_error(void);
 /* Library version string. */

@@ -168,6 +168,7 @@ def main():
 
     f = I.make_fields(m, seed=0)
     f_ab2 = I.make_fields(m, seed=0, ab2=True)
+    f_white = I.make_fields(m, seed=0, kind="white")
     w_ref = np.asarray(ale.compute_w(rm, f.uv, f.helem))
     out["w_e__digest"] = field_digest(m, w_ref, m.node_iface_mask)
     print("compute_w  ours vs reference max|d| =", np.max(np.abs(w_ref - f.w_e)))
@@ -188,7 +189,7 @@ def main():
         "T_step1": (f.uv, f.w_e, f.tracers[0], f.tracers_old[0], {}, True),
         "S_step1": (f.uv, f.w_e, f.tracers[1], f.tracers_old[1], {}, True),
         "T_ab2": (f_ab2.uv, f_ab2.w_e, f_ab2.tracers[0], f_ab2.tracers_old[0], {}, True),
-        "sharp_x5": (f.uv * 5.0, f.w_e * 5.0, sharp, ten, {}, True),
+        "sharp_x5": (f_white.uv * 5.0, f_white.w_e * 5.0, sharp, ten, {}, True),
         "const": (f.uv, f.w_e, const, const, {}, False),
         "T_wsplit_zstar": (f.uv, f.w_e - w_i, f.tracers[0], f_ab2.tracers_old[0],
                            dict(w_i=w_i, Z3d=Z3d, zbar3=zbar3), False),

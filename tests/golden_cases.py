@@ -36,6 +36,7 @@ def cases(m):
     lm = m.node_layer_mask
     f = I.make_fields(m, seed=0)
     f_ab2 = I.make_fields(m, seed=0, ab2=True)
+    f_white = I.make_fields(m, seed=0, kind="white")
     k = np.arange(m.nl)[None, :]
     sharp = np.where(lm, 10.0 + 5.0 * np.sin(np.arange(m.nod2D)[:, None] * 0.7)
                      * np.cos(k * 1.3), 0.0)
@@ -52,7 +53,7 @@ def cases(m):
         "S_step1": dict(uv=f.uv, w_e=f.w_e, T=f.tracers[1], T_old=f.tracers_old[1], kw={}),
         "T_ab2": dict(uv=f_ab2.uv, w_e=f_ab2.w_e, T=f_ab2.tracers[0],
                       T_old=f_ab2.tracers_old[0], kw={}),
-        "sharp_x5": dict(uv=f.uv * 5.0, w_e=f.w_e * 5.0, T=sharp, T_old=ten, kw={}),
+        "sharp_x5": dict(uv=f_white.uv * 5.0, w_e=f_white.w_e * 5.0, T=sharp, T_old=ten, kw={}),
         "const": dict(uv=f.uv, w_e=f.w_e, T=const, T_old=const, kw={}),
         "T_wsplit_zstar": dict(uv=f.uv, w_e=f.w_e - w_i, T=f.tracers[0],
                                T_old=f_ab2.tracers_old[0],

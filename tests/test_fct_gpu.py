@@ -96,3 +96,17 @@ def test_exch_rejected(pi, pi_cases):
     with pytest.raises(NotImplementedError):
         advect_one_fct(pi, c["uv"], c["w_e"], c["helem"], c["hnode"], c["hnode_new"],
                        c["T"], c["T_old"], dt=DT, exch=lambda f, kind: f)
+
+
+def test_compute_w_gpu_matches_reference_digest(torch, pi, golden, pi_cases):
+    """The CUDA w producer (ale.py:309-365) against the reference-generated digest."""
+    from fesom_jax_b200.ale import compute_w
+    from tests.golden_cases import field_digest
+    c = pi_cases["T_step1"]
+    w = compute_w(pi, _dev(torch, c["uv"]), _dev(torch, c["helem"])).cpu().numpy()
+    d, r = field_digest(pi, w, pi.node_iface_mask), golden["w_e__digest"]
+    assert abs(d[1] - r[1]) <= 1e-12 * r[2]
+    assert abs(d[3] - r[3]) <= 1e-12 * r[3]
+    ref = c["w_e"]
+    assert np.max(np.abs(w - ref)) <= 1e-12 * np.max(np.abs(ref))
+    assert np.all(w[~pi.node_iface_mask] == 0.0)
