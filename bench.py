@@ -202,6 +202,9 @@ def run_ours(args, D: Dist) -> dict | None:
     info = ens.info()
     S = cfg["fct_steps"]
     stream = torch.cuda.current_stream(dev)
+    tune = ens.autotune(steps=2) if not args.chunk else None
+    if args.chunk:
+        ens.set_chunk(args.chunk)
     torch.cuda.synchronize()
     for _ in range(args.warmup):
         ens.run(S)
@@ -233,14 +236,15 @@ def run_ours(args, D: Dist) -> dict | None:
     alg = W.algorithmic_bytes(mesh, cfg["ntr"], cfg["members"])
     pk = peaks()
     achieved = alg / (fct_step_ms / 1e3) / 1e9
-    n_kernels = 8 * info["groups"]
+    n_kernels = (1 + 7 * -(-cfg["ntr"] // ens.chunk)) * info["groups"]
     out = dict(value=value, t=t, info=info, clocks=clk, prof=prof, fct_step_ms=fct_step_ms,
                finite=finite, mesh=mesh, cfg=cfg, alg_bytes=alg,
                roofline=dict(bound="hbm", kernel="fct step (8 stage kernels)",
                              achieved=achieved, peak=pk["hbm_gbs"], unit="GB/s",
                              frac=achieved / pk["hbm_gbs"], peak_source=pk["source"],
                              traffic=None, alg_bytes_per_step=alg),
-               gpu_launches=n_kernels * S * args.steps)
+               gpu_launches=n_kernels * S * args.steps,
+               tuning=dict(chunk=ens.chunk, candidates_ms_per_2_steps=tune))
 
     # plain one-instance-per-launch comparison (the reference's call granularity:
     # one tracer per advect_one_fct call), member 0, one FCT step per call
@@ -291,7 +295,10 @@ def e2e_host(args, mesh, cfg, dev) -> dict:
                                   thickness=thick, sigma=cfg["sigma"], n_vortices=cfg["n_vortices"])
         ens.add_member(mesh, inp["uv"], inp["w_e"], inp["helem"], inp["hnode"], inp["hnode_new"],
                        inp["T"], inp["T_old"], cfg["dt"])
-        host.append({k: inp[k].cpu().pin_memory() for k in ("T", "T_old", "uv", "w_e")})
+        host.append({k: inp[k].cpu().pin_memory() for k in ("uv", "w_e")})
+        # host state in the resident interleaved layout [N, nl, ntr]
+        for k in ("T", "T_old"):
+            host[-1][k] = inp[k].permute(1, 2, 0).contiguous().cpu().pin_memory()
         host[-1]["out"] = torch.empty_like(host[-1]["T"]).pin_memory()
         del inp
     ens.build()
@@ -303,12 +310,12 @@ def e2e_host(args, mesh, cfg, dev) -> dict:
     def one():
         for i, h in enumerate(host):
             mb = ens.members[i]
-            ens.set_state(i, h["T"], h["T_old"], non_blocking=True)
+            ens.set_state(i, h["T"], h["T_old"], non_blocking=True, interleaved=True)
             mb.uv.copy_(h["uv"], non_blocking=True)
             mb.w_e.copy_(h["w_e"], non_blocking=True)
         ens.run(S)
         for i, h in enumerate(host):
-            h["out"].copy_(ens.state(i)[0], non_blocking=True)
+            h["out"].copy_(ens.state_interleaved(i)[0], non_blocking=True)
 
     for _ in range(max(1, min(args.warmup, 2))):
         one()
@@ -393,6 +400,7 @@ def main():
     ap.add_argument("--members", type=int, default=0)
     ap.add_argument("--fct-steps", type=int, default=0)
     ap.add_argument("--ntr", type=int, default=0, help="override tracers per member")
+    ap.add_argument("--chunk", type=int, default=0, help="fix the tracer chunk (no autotune)")
     ap.add_argument("--workspace-gb", type=float, default=40.0)
     ap.add_argument("--e2e-members", type=int, default=8)
     ap.add_argument("--no-e2e", action="store_true")
@@ -419,7 +427,7 @@ def main():
                 config=workload_config(args.config, cfg, mesh), roofline=r["roofline"],
                 clocks=r["clocks"], gpu_launches=r["gpu_launches"],
                 fct_step_ms=r["fct_step_ms"], stage_ms=r["prof"], finite=r["finite"],
-                batch=r["info"])
+                batch=r["info"], tuning=r["tuning"])
     for k in ("plain", "e2e", "cpu_baseline"):
         if k in r:
             line[k] = r[k]

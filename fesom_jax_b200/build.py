@@ -44,7 +44,9 @@ def build(force: bool = False, verbose: bool = False, extra=()) -> Path:
     if not force and not needs_build():
         return LIB
     tmp = LIB.with_suffix(".so.tmp")
-    cmd = [nvcc(), ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared",
+    # --fmad=false: no implicit FMA contraction, so every template instantiation (tracer
+    # chunk size, layout) rounds identically and results do not depend on the chunking
+    cmd = [nvcc(), ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "--fmad=false",
            "-Xcompiler", "-fPIC,-O3", "-cudart", "static", "--expt-relaxed-constexpr",
            "-I", str(PKG.parent / "include"), *extra,
            *[str(s) for s in sources()], "-o", str(tmp)]

@@ -6,7 +6,10 @@
 // sizes -- advance in one launch per stage: blockIdx.y selects the instance from a
 // device table, blockIdx.x its lanes. Instances are packed into workspace groups that
 // fit a memory budget; groups run back to back on one stream and reuse one arena.
-// Multi-step runs are captured once into a CUDA graph and replayed.
+// Multi-step runs are captured once into a CUDA graph and replayed. Tracer buffers and
+// workspaces are interleaved ([entity, nl, ntr]): the tracers of one entity-level are
+// contiguous, so every gather moves one contiguous chunk; a group holds instances with
+// the same ntr.
 #include <algorithm>
 #include <map>
 #include <mutex>
@@ -73,7 +76,7 @@ int fct_batch_create(const FctInstance* insts, int n, int64_t budget, FctBatch**
   FctBatch::Group g;
   for (int i = 0; i < n; ++i) {
     const int64_t bytes = ws_doubles[i] * int64_t(sizeof(double));
-    if (g.count > 0 && cur + bytes > budget) {
+    if (g.count > 0 && (cur + bytes > budget || insts[i].ntr != insts[g.first].ntr)) {
       B->groups.push_back(g);
       g = FctBatch::Group();
       g.first = i;
@@ -111,7 +114,7 @@ int fct_batch_create(const FctInstance* insts, int n, int64_t budget, FctBatch**
       d.max_elem = std::max(d.max_elem, P->hm.n_elem);
       d.max_dense = std::max(d.max_dense, int64_t(P->N) * P->L);
       d.max_nodes = std::max(d.max_nodes, int64_t(P->N));
-      d.max_ntr = std::max(d.max_ntr, q.ntr);
+      d.ntr = q.ntr;
       B->total_updates += int64_t(q.ntr) * P->hm.n_layer;
       for (int p = 0; p < 3; ++p) {
         Inst& in = tab[size_t(p) * n + i];
@@ -121,7 +124,8 @@ int fct_batch_create(const FctInstance* insts, int n, int64_t budget, FctBatch**
         in.T_old = q.buf[p % 3];
         in.T = q.buf[(p + 1) % 3];
         in.T_new = q.buf[(p + 2) % 3];
-        in.tstride = int64_t(P->N) * P->L;
+        in.tstride = 0;
+        in.tg = q.ntr;   // interleaved [nod2D, nl, ntr]
         in.Z3d = in.zbar3 = in.w_i = nullptr;
         in.ws = ws;
         in.dt = q.dt;
@@ -130,6 +134,7 @@ int fct_batch_create(const FctInstance* insts, int n, int64_t budget, FctBatch**
     }
     d.any_wi = false;
     d.copy_dry = false;
+    d.chunk = 8;
     gr.dims = d;
   }
   e = cudaMalloc(&B->d_tables, tab.size() * sizeof(Inst));
@@ -155,6 +160,17 @@ int fct_batch_destroy(FctBatch* B) {
   if (B->arena) cudaFree(B->arena);
   if (prev >= 0) cudaSetDevice(prev);
   delete B;
+  return FCT_OK;
+}
+
+int fct_batch_set_chunk(FctBatch* B, int chunk) {
+  if (!B) return set_error(FCT_ERR_INVALID, "batch is NULL");
+  if (chunk != 1 && chunk != 2 && chunk != 4 && chunk != 8)
+    return set_error(FCT_ERR_INVALID, "chunk must be 1, 2, 4 or 8");
+  std::lock_guard<std::mutex> lk(B->graph_mu);
+  for (auto& g : B->groups) g.dims.chunk = chunk;
+  for (auto& kv : B->graphs) cudaGraphExecDestroy(kv.second);   // recapture with the new chunk
+  B->graphs.clear();
   return FCT_OK;
 }
 

@@ -16,6 +16,11 @@
 //   zalesak_limit b3 (:453-465), flux2dtracer_fct (:469-484),
 //   ale_reconstruct (:142-151)                               -> k_node_final (layer lanes)
 //   invalid lanes keep T (ale_reconstruct)                   -> k_copy_dry   (dense)
+//
+// Each thread owns one lane and NTR tracers (a compile-time chunk of the instance's
+// tracers, which share its velocities): mesh indices, geometry and velocity terms are
+// loaded once per lane and every neighbour gather issues NTR independent loads (one
+// contiguous chunk in the interleaved layout), so the gathers overlap.
 #include <algorithm>
 
 #include "fct_host.h"
@@ -31,154 +36,262 @@ __device__ __forceinline__ int64_t lane_index() {
   return int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
 }
 
+template <class T>
+__device__ __forceinline__ T ld(const T* p) { return __ldg(p); }
+
+// Address of tracer t at entity-level q: interleaved q*tg + t, else t*stride + q.
+template <bool IL>
+__device__ __forceinline__ int64_t tix(int64_t q, int t, int64_t stride, int tg) {
+  return IL ? q * tg + t : int64_t(t) * stride + q;
+}
+
+// Tracers [t0, t0+NTR) of entity-level q.
+template <int NTR, bool IL>
+__device__ __forceinline__ void ldn(const double* __restrict__ p, int64_t q, int t0,
+                                    int64_t stride, int tg, double (&v)[NTR]) {
+  if constexpr (IL && (NTR % 2 == 0)) {
+    const double* b = p + q * tg + t0;
+    if ((reinterpret_cast<uintptr_t>(b) & 15) == 0) {
+#pragma unroll
+      for (int i = 0; i < NTR; i += 2) {
+        const double2 x = __ldg(reinterpret_cast<const double2*>(b + i));
+        v[i] = x.x;
+        v[i + 1] = x.y;
+      }
+      return;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < NTR; ++i) v[i] = __ldg(p + tix<IL>(q, t0 + i, stride, tg));
+}
+
+template <int NTR, bool IL>
+__device__ __forceinline__ void stn(double* __restrict__ p, int64_t q, int t0, int64_t stride,
+                                    int tg, const double (&v)[NTR]) {
+  if constexpr (IL && (NTR % 2 == 0)) {
+    double* b = p + q * tg + t0;
+    if ((reinterpret_cast<uintptr_t>(b) & 15) == 0) {
+#pragma unroll
+      for (int i = 0; i < NTR; i += 2)
+        *reinterpret_cast<double2*>(b + i) = make_double2(v[i], v[i + 1]);
+      return;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < NTR; ++i) p[tix<IL>(q, t0 + i, stride, tg)] = v[i];
+}
+
 // ---------------------------------------------------------------- edge_vflux
 __device__ __forceinline__ void body_vflux(const Inst& in, int64_t i) {
   const DevMesh& m = *in.m;
   if (i >= m.n_edge) return;
-  const uint32_t lane = m.edge_lanes[i];
+  const uint32_t lane = ld(m.edge_lanes + i);
   const int e = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const int el1 = m.etri[2 * e], el2 = m.etri[2 * e + 1];
+  const int el1 = ld(m.etri + 2 * e), el2 = ld(m.etri + 2 * e + 1);
   const double* cr = m.cross + 4 * int64_t(e);
   double t1 = 0.0, t2 = 0.0;
-  if (k >= m.eul[el1] && k < m.enl[el1]) {
+  if (k >= ld(m.eul + el1) && k < ld(m.enl + el1)) {
     const int64_t q = int64_t(el1) * L + k;
-    const double U = in.uv[2 * q], V = in.uv[2 * q + 1];
-    t1 = (U * cr[1] - V * cr[0]) * in.helem[q];
+    const double2 U = __ldg(reinterpret_cast<const double2*>(in.uv) + q);
+    t1 = (U.x * ld(cr + 1) - U.y * ld(cr + 0)) * ld(in.helem + q);
   }
-  if (el2 >= 0 && k >= m.eul[el2] && k < m.enl[el2]) {
+  if (el2 >= 0 && k >= ld(m.eul + el2) && k < ld(m.enl + el2)) {
     const int64_t q = int64_t(el2) * L + k;
-    const double U = in.uv[2 * q], V = in.uv[2 * q + 1];
-    t2 = (V * cr[2] - U * cr[3]) * in.helem[q];
+    const double2 U = __ldg(reinterpret_cast<const double2*>(in.uv) + q);
+    t2 = (U.y * ld(cr + 2) - U.x * ld(cr + 3)) * ld(in.helem + q);
   }
   in.ws.vflux[int64_t(e) * L + k] = t1 + t2;
 }
 
 // ---------------------------------------------------- tracer_gradient_elements
-__device__ __forceinline__ void body_elem_grad(const Inst& in, int64_t i) {
+template <int NTR, bool IL>
+__device__ __forceinline__ void body_elem_grad(const Inst& in, int64_t i, int t0) {
   const DevMesh& m = *in.m;
   if (i >= m.n_elem) return;
-  const uint32_t lane = m.elem_lanes[i];
+  const uint32_t lane = ld(m.elem_lanes + i);
   const int e = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const int v0 = m.enodes[3 * e], v1 = m.enodes[3 * e + 1], v2 = m.enodes[3 * e + 2];
+  const int v0 = ld(m.enodes + 3 * e), v1 = ld(m.enodes + 3 * e + 1), v2 = ld(m.enodes + 3 * e + 2);
   const double* g = m.gsca + 6 * int64_t(e);
-  const double g0 = g[0], g1 = g[1], g2 = g[2], g3 = g[3], g4 = g[4], g5 = g[5];
-  const int64_t q = int64_t(e) * L + k;
-  for (int t = 0; t < in.ntr; ++t) {
-    const double* T = in.T + t * in.tstride;
-    const double t0 = T[int64_t(v0) * L + k], t1 = T[int64_t(v1) * L + k],
-                 t2 = T[int64_t(v2) * L + k];
-    in.ws.gx[t * in.ws.sE + q] = g0 * t0 + g1 * t1 + g2 * t2;
-    in.ws.gy[t * in.ws.sE + q] = g3 * t0 + g4 * t1 + g5 * t2;
+  const double g0 = ld(g), g1 = ld(g + 1), g2 = ld(g + 2), g3 = ld(g + 3), g4 = ld(g + 4),
+               g5 = ld(g + 5);
+  double a0[NTR], a1[NTR], a2[NTR], gx[NTR], gy[NTR];
+  ldn<NTR, IL>(in.T, int64_t(v0) * L + k, t0, in.tstride, in.tg, a0);
+  ldn<NTR, IL>(in.T, int64_t(v1) * L + k, t0, in.tstride, in.tg, a1);
+  ldn<NTR, IL>(in.T, int64_t(v2) * L + k, t0, in.tstride, in.tg, a2);
+#pragma unroll
+  for (int t = 0; t < NTR; ++t) {
+    gx[t] = g0 * a0[t] + g1 * a1[t] + g2 * a2[t];
+    gy[t] = g3 * a0[t] + g4 * a1[t] + g5 * a2[t];
   }
+  const int64_t q = int64_t(e) * L + k;
+  stn<NTR, IL>(in.ws.gx, q, t0, in.ws.sE, in.tg, gx);
+  stn<NTR, IL>(in.ws.gy, q, t0, in.ws.sE, in.tg, gy);
 }
 
-// Upwind vertical flux at interface j of a column (layer-masked), tracer_adv.py:108-120.
-__device__ __forceinline__ double vflux_up(const double* col, const double* area_col,
-                                           double w, int j, bool layer) {
-  if (!layer) return 0.0;
+// Upwind vertical flux at interface j (layer-masked), tracer_adv.py:108-120, given the
+// tracer below (Tb = T[j]) and above (Ta = T[j-1], edge-replicated at j = 0).
+__device__ __forceinline__ double vflux_up(double Tb, double Ta, double w, double area) {
   const double aw = fabs(w);
-  const double Tb = col[j], Ta = col[j > 0 ? j - 1 : 0];
-  return -0.5 * (Tb * (w + aw) + Ta * (w - aw)) * area_col[j];
+  return -0.5 * (Tb * (w + aw) + Ta * (w - aw)) * area;
 }
 
 // -------------------------------- LO solution, node-average gradient, adf_v
-__device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i) {
+template <int NTR, bool IL>
+__device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i, int t0) {
   const DevMesh& m = *in.m;
   if (i >= m.n_iface) return;
-  const uint32_t lane = m.iface_lanes[i];
+  const uint32_t lane = ld(m.iface_lanes + i);
   const int n = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const int nzmin = m.nzmin[n], nzmax = m.nzmax[n];
-  const int64_t base = int64_t(n) * L;
+  const int nzmin = ld(m.nzmin + n), nzmax = ld(m.nzmax + n);
+  const int64_t base = int64_t(n) * L, qn = base + k;
   const bool layer = k < nzmax;
   const bool layer1 = (k + 1) < nzmax;
-  const double* area_col = m.area + base;
-  const double w = in.w_e[base + k];
-  const double w1 = layer1 ? in.w_e[base + k + 1] : 0.0;
-  const double Wf = in.w_i ? w + in.w_i[base + k] : w;   // w_full for the HO flux
-  const double area_k = area_col[k];
-  const double hn = in.hnode[base + k], hnn = in.hnode_new[base + k];
-  const double av = m.areasvol[base + k];
-  const double dt = in.dt;
-  const int e0 = m.ne_off[n], e1 = m.ne_off[n + 1];
-  const int c0 = m.nel_off[n], c1 = m.nel_off[n + 1];
+  const int km1 = k > 0 ? k - 1 : 0;
+  const double w = ld(in.w_e + qn);
+  const double Wf = in.w_i ? w + ld(in.w_i + qn) : w;   // w_full for the HO flux
+  const double area_k = ld(m.area + qn);
+  const int64_t ts = in.tstride;
+  const int tg = in.tg;
 
-  // QR4C stencil depths (tracer_adv.py:228-238, 265-273)
-  double Znz, Zm1, Zm2, Zp1, zb;
-  if (in.Z3d) {
-    const double* Zc = in.Z3d + base;
-    Znz = Zc[k]; Zm1 = Zc[k > 0 ? k - 1 : 0]; Zm2 = Zc[k > 1 ? k - 2 : 0];
-    Zp1 = Zc[k + 1 < L ? k + 1 : L - 1]; zb = in.zbar3[base + k];
-  } else {
-    Znz = m.Zp[k]; Zm1 = m.Zp[k > 0 ? k - 1 : 0]; Zm2 = m.Zp[k > 1 ? k - 2 : 0];
-    Zp1 = m.Zp[k + 1 < L ? k + 1 : L - 1]; zb = m.zbar[k];
+  double Tc[NTR], Ta[NTR];   // T[k], T[k-1]
+  ldn<NTR, IL>(in.T, qn, t0, ts, tg, Tc);
+  ldn<NTR, IL>(in.T, base + km1, t0, ts, tg, Ta);
+  double fvk[NTR];
+#pragma unroll
+  for (int t = 0; t < NTR; ++t) fvk[t] = layer ? vflux_up(Tc[t], Ta[t], w, area_k) : 0.0;
+
+  if (layer) {
+    const double hn = ld(in.hnode + qn), hnn = ld(in.hnode_new + qn);
+    const double av = ld(m.areasvol + qn);
+    const double dt = in.dt;
+    double fvk1[NTR];
+    if (layer1) {
+      const double w1 = ld(in.w_e + qn + 1), area1 = ld(m.area + qn + 1);
+      double Tb[NTR];
+      ldn<NTR, IL>(in.T, qn + 1, t0, ts, tg, Tb);
+#pragma unroll
+      for (int t = 0; t < NTR; ++t) fvk1[t] = vflux_up(Tb[t], Tc[t], w1, area1);
+    } else {
+#pragma unroll
+      for (int t = 0; t < NTR; ++t) fvk1[t] = 0.0;
+    }
+    // compute_fct_lo: edge->node upwind divergence in ascending edge id
+    double div[NTR];
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) div[t] = 0.0;
+    const int e0 = ld(m.ne_off + n), e1 = ld(m.ne_off + n + 1);
+    for (int j = e0; j < e1; ++j) {
+      const int idx = ld(m.ne_idx + j), e = idx >> 1;
+      if (k < ld(m.ekmin + e) || k >= ld(m.ekmax + e)) continue;   // vflux == 0 there
+      const int oth = ld(m.ne_oth + j);
+      const double vf = ld(in.ws.vflux + int64_t(e) * L + k);
+      const double avf = fabs(vf);
+      double To[NTR];
+      ldn<NTR, IL>(in.T, int64_t(oth) * L + k, t0, ts, tg, To);
+#pragma unroll
+      for (int t = 0; t < NTR; ++t) {
+        const double T1 = (idx & 1) ? To[t] : Tc[t], T2 = (idx & 1) ? Tc[t] : To[t];
+        const double fl = -0.5 * (T1 * (vf + avf) + T2 * (vf - avf));
+        div[t] += (idx & 1) ? -fl : fl;
+      }
+    }
+    const bool valid = (hnn > 0.0) && (av > 0.0);
+    double lo[NTR];
+#pragma unroll
+    for (int t = 0; t < NTR; ++t)
+      lo[t] = valid ? (Tc[t] * hn + (div[t] + (fvk[t] - fvk1[t])) * dt / av) / hnn : 0.0;
+    stn<NTR, IL>(in.ws.lo, qn, t0, in.ws.sN, tg, lo);
+    // _node_avg_grad: area-weighted mean over the node's active elements
+    double nx[NTR], ny[NTR], den = 0.0;
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) nx[t] = ny[t] = 0.0;
+    const int c0 = ld(m.nel_off + n), c1 = ld(m.nel_off + n + 1);
+    for (int j = c0; j < c1; ++j) {
+      const int el = ld(m.nel_idx + j);
+      if (k >= ld(m.eul + el) && k < ld(m.enl + el)) {
+        const double a = ld(m.earea + el);
+        const int64_t qe = int64_t(el) * L + k;
+        double gx[NTR], gy[NTR];
+        ldn<NTR, IL>(in.ws.gx, qe, t0, in.ws.sE, tg, gx);
+        ldn<NTR, IL>(in.ws.gy, qe, t0, in.ws.sE, tg, gy);
+#pragma unroll
+        for (int t = 0; t < NTR; ++t) {
+          nx[t] += gx[t] * a;
+          ny[t] += gy[t] * a;
+        }
+        den += a;
+      }
+    }
+    const double dd = den > 0.0 ? den : 1.0;
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) {
+      nx[t] = nx[t] / dd;
+      ny[t] = ny[t] / dd;
+    }
+    stn<NTR, IL>(in.ws.gnx, qn, t0, in.ws.sN, tg, nx);
+    stn<NTR, IL>(in.ws.gny, qn, t0, in.ws.sN, tg, ny);
   }
 
-  for (int t = 0; t < in.ntr; ++t) {
-    const double* T = in.T + t * in.tstride;
-    const double* To = in.T_old + t * in.tstride;
-    const double* Tc = T + base;
-    const double fvk = vflux_up(Tc, area_col, w, k, layer);
-    if (layer) {
-      const double fvk1 = vflux_up(Tc, area_col, w1, k + 1, layer1);
-      // compute_fct_lo: edge->node upwind divergence, ascending edge id
-      double div_h = 0.0;
-      for (int j = e0; j < e1; ++j) {
-        const int idx = m.ne_idx[j];
-        const int e = idx >> 1;
-        const double vf = (k >= m.ekmin[e] && k < m.ekmax[e]) ? in.ws.vflux[int64_t(e) * L + k] : 0.0;
-        const double avf = fabs(vf);
-        const int n1 = m.edges[2 * e], n2 = m.edges[2 * e + 1];
-        const double fl = -0.5 * (T[int64_t(n1) * L + k] * (vf + avf) +
-                                  T[int64_t(n2) * L + k] * (vf - avf));
-        div_h += (idx & 1) ? -fl : fl;
-      }
-      const bool valid = (hnn > 0.0) && (av > 0.0);
-      const double lo = valid ? (Tc[k] * hn + (div_h + (fvk - fvk1)) * dt / av) / hnn : 0.0;
-      in.ws.lo[t * in.ws.sN + base + k] = lo;
-      // _node_avg_grad: area-weighted mean over the node's active elements
-      double nx = 0.0, ny = 0.0, den = 0.0;
-      for (int j = c0; j < c1; ++j) {
-        const int el = m.nel_idx[j];
-        if (k >= m.eul[el] && k < m.enl[el]) {
-          const double a = m.earea[el];
-          const int64_t q = t * in.ws.sE + int64_t(el) * L + k;
-          nx += in.ws.gx[q] * a;
-          ny += in.ws.gy[q] * a;
-          den += a;
-        }
-      }
-      const double dd = den > 0.0 ? den : 1.0;
-      in.ws.gnx[t * in.ws.sN + base + k] = nx / dd;
-      in.ws.gny[t * in.ws.sN + base + k] = ny / dd;
+  // adv_flux_ver_ho (QR4C on ttfAB) minus the LO vertical flux (tracer_adv.py:241-295)
+  double hi[NTR];
+#pragma unroll
+  for (int t = 0; t < NTR; ++t) hi[t] = 0.0;
+  if (k == nzmin) {
+    double To[NTR];
+    ldn<NTR, IL>(in.T_old, qn, t0, ts, tg, To);
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) hi[t] = -ab2(Tc[t], To[t]) * Wf * area_k;
+  } else if (k == nzmax) {
+    // bottom interface: no flux
+  } else if (k == nzmin + 1 || k == nzmax - 1) {
+    double To[NTR], Tom[NTR];
+    ldn<NTR, IL>(in.T_old, qn, t0, ts, tg, To);
+    ldn<NTR, IL>(in.T_old, qn - 1, t0, ts, tg, Tom);
+#pragma unroll
+    for (int t = 0; t < NTR; ++t)
+      hi[t] = -0.5 * (ab2(Ta[t], Tom[t]) + ab2(Tc[t], To[t])) * Wf * area_k;
+  } else if (k >= nzmin + 2 && k <= nzmax - 2) {
+    double Znz, Zm1, Zm2, Zp1, zb;   // QR4C stencil depths (tracer_adv.py:228-238, 265-273)
+    if (in.Z3d) {
+      const double* Zc = in.Z3d + base;
+      Znz = ld(Zc + k); Zm1 = ld(Zc + k - 1); Zm2 = ld(Zc + k - 2);
+      Zp1 = ld(Zc + (k + 1 < L ? k + 1 : L - 1)); zb = ld(in.zbar3 + qn);
+    } else {
+      Znz = ld(m.Zp + k); Zm1 = ld(m.Zp + k - 1); Zm2 = ld(m.Zp + k - 2);
+      Zp1 = ld(m.Zp + (k + 1 < L ? k + 1 : L - 1)); zb = ld(m.zbar + k);
     }
-    // adv_flux_ver_ho (QR4C on ttfAB) minus the LO vertical flux
-    double hi = 0.0;
-    if (k == nzmin) {
-      hi = -ab2(Tc[k], To[base + k]) * Wf * area_k;
-    } else if (k == nzmax) {
-      hi = 0.0;
-    } else if (k == nzmin + 1 || k == nzmax - 1) {
-      const double A0 = ab2(Tc[k], To[base + k]), Am1 = ab2(Tc[k - 1], To[base + k - 1]);
-      hi = -0.5 * (Am1 + A0) * Wf * area_k;
-    } else if (k >= nzmin + 2 && k <= nzmax - 2) {
-      const double A0 = ab2(Tc[k], To[base + k]);
-      const double Am1 = ab2(Tc[k - 1], To[base + k - 1]);
-      const double Am2 = ab2(Tc[k - 2], To[base + k - 2]);
-      const double Ap1 = ab2(Tc[k + 1], To[base + k + 1]);
-      const double qc = (Am1 - A0) / safe_nz(Zm1 - Znz);
-      const double qu = (A0 - Ap1) / safe_nz(Znz - Zp1);
-      const double qd = (Am2 - Am1) / safe_nz(Zm2 - Zm1);
+    const double dc = safe_nz(Zm1 - Znz), du = safe_nz(Znz - Zp1), dd = safe_nz(Zm2 - Zm1);
+    double To[NTR], Tom[NTR], Tm2[NTR], Tom2[NTR], Tp[NTR], Top[NTR];
+    ldn<NTR, IL>(in.T_old, qn, t0, ts, tg, To);
+    ldn<NTR, IL>(in.T_old, qn - 1, t0, ts, tg, Tom);
+    ldn<NTR, IL>(in.T, qn - 2, t0, ts, tg, Tm2);
+    ldn<NTR, IL>(in.T_old, qn - 2, t0, ts, tg, Tom2);
+    ldn<NTR, IL>(in.T, qn + 1, t0, ts, tg, Tp);
+    ldn<NTR, IL>(in.T_old, qn + 1, t0, ts, tg, Top);
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) {
+      const double A0 = ab2(Tc[t], To[t]), Am1 = ab2(Ta[t], Tom[t]);
+      const double Am2 = ab2(Tm2[t], Tom2[t]), Ap1 = ab2(Tp[t], Top[t]);
+      const double qc = (Am1 - A0) / dc;
+      const double qu = (A0 - Ap1) / du;
+      const double qd = (Am2 - Am1) / dd;
       const double Tmean1 = A0 + (2.0 * qc + qu) * (zb - Znz) / 3.0;
       const double Tmean2 = Am1 + (2.0 * qc + qd) * (zb - Zm1) / 3.0;
-      hi = -0.5 * (Tmean1 + Tmean2) * Wf * area_k;
+      hi[t] = -0.5 * (Tmean1 + Tmean2) * Wf * area_k;
     }
-    const double lo_v = in.w_i ? vflux_up(Tc, area_col, Wf, k, layer) : fvk;
-    in.ws.adfv[t * in.ws.sN + base + k] = hi - lo_v;
   }
+  double adf[NTR];
+#pragma unroll
+  for (int t = 0; t < NTR; ++t) {
+    const double lo_v = in.w_i ? (layer ? vflux_up(Tc[t], Ta[t], Wf, area_k) : 0.0) : fvk[t];
+    adf[t] = hi[t] - lo_v;
+  }
+  stn<NTR, IL>(in.ws.adfv, qn, t0, in.ws.sN, tg, adf);
 }
 
 // ---------------------------- adv_tra_vert_impl: implicit w_i advection of LO
-__device__ __forceinline__ void body_vert_impl(const Inst& in, int64_t n) {
+template <int NTR, bool IL>
+__device__ __forceinline__ void body_vert_impl(const Inst& in, int64_t n, int t0) {
   const DevMesh& m = *in.m;
   if (n >= m.N || !in.w_i) return;
   const int L = m.L;
@@ -187,8 +300,8 @@ __device__ __forceinline__ void body_vert_impl(const Inst& in, int64_t n) {
   const int64_t base = n * L;
   const double dt = in.dt;
   double cp[kMaxLevels], dp[kMaxLevels];
-  for (int t = 0; t < in.ntr; ++t) {
-    double* lo = in.ws.lo + t * in.ws.sN + base;
+  for (int t = t0; t < t0 + NTR; ++t) {
+    auto LO = [&](int k) -> double& { return in.ws.lo[tix<IL>(base + k, t, in.ws.sN, in.tg)]; };
     double cprev = 0.0, dprev = 0.0;
     for (int k = nzmin; k < nzmax; ++k) {
       const double av = m.areasvol[base + k];
@@ -204,7 +317,7 @@ __device__ __forceinline__ void body_vert_impl(const Inst& in, int64_t n) {
       const double c = (bot ? 0.0 : -fmax(0.0, wd)) * v_bot;
       const double b_adv = b_top + b_bot;
       const double b = in.hnode_new[base + k] + b_adv;
-      const double Tm = lo[k > 0 ? k - 1 : 0], T0 = lo[k], Tp = k + 1 < L ? lo[k + 1] : 0.0;
+      const double Tm = LO(k > 0 ? k - 1 : 0), T0 = LO(k), Tp = k + 1 < L ? LO(k + 1) : 0.0;
       const double rhs = -(a * Tm + b_adv * T0 + c * Tp);
       const double md = b - a * cprev;
       cprev = c / md;
@@ -217,237 +330,356 @@ __device__ __forceinline__ void body_vert_impl(const Inst& in, int64_t n) {
       x = dp[k] - cp[k] * x;
       dp[k] = x;
     }
-    for (int k = nzmin; k < nzmax; ++k) lo[k] = lo[k] + dp[k];
+    for (int k = nzmin; k < nzmax; ++k) LO(k) = LO(k) + dp[k];
   }
 }
 
 // -------------------------- fill_up_dn_grad + adv_flux_hor_ho - LO flux = adf_h
-__device__ __forceinline__ void body_edge_adf(const Inst& in, int64_t i) {
+template <int NTR, bool IL>
+__device__ __forceinline__ void body_edge_adf(const Inst& in, int64_t i, int t0) {
   const DevMesh& m = *in.m;
   if (i >= m.n_edge) return;
-  const uint32_t lane = m.edge_lanes[i];
+  const uint32_t lane = ld(m.edge_lanes + i);
   const int e = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const int n1 = m.edges[2 * e], n2 = m.edges[2 * e + 1];
-  const int up = m.eupdn[2 * e], dn = m.eupdn[2 * e + 1];
-  const int kmin = max(m.ulmax[n1], m.ulmax[n2]) - 1;
-  const int kmax = min(m.nlmin[n1], m.nlmin[n2]) - 1;
+  const int n1 = ld(m.edges + 2 * e), n2 = ld(m.edges + 2 * e + 1);
+  const int up = ld(m.eupdn + 2 * e), dn = ld(m.eupdn + 2 * e + 1);
+  const int kmin = max(ld(m.ulmax + n1), ld(m.ulmax + n2)) - 1;
+  const int kmax = min(ld(m.nlmin + n1), ld(m.nlmin + n2)) - 1;
   const bool use_tri = (up >= 0) && (dn >= 0) && k >= kmin && k < kmax;
-  const double vf = in.ws.vflux[int64_t(e) * L + k];
+  const double vf = ld(in.ws.vflux + int64_t(e) * L + k);
   const double avf = fabs(vf);
-  const double c1 = m.ecoef[2 * e], c2 = m.ecoef[2 * e + 1];
+  const double c1 = ld(m.ecoef + 2 * e), c2 = ld(m.ecoef + 2 * e + 1);
   const int64_t q1 = int64_t(n1) * L + k, q2 = int64_t(n2) * L + k;
-  for (int t = 0; t < in.ntr; ++t) {
-    const double* T = in.T + t * in.tstride;
-    const double* To = in.T_old + t * in.tstride;
-    const double T1 = T[q1], T2 = T[q2];
-    const double fl = -0.5 * (T1 * (vf + avf) + T2 * (vf - avf));
-    double g0, g1, g2, g3;
-    if (use_tri) {
-      const int64_t qu = t * in.ws.sE + int64_t(up) * L + k;
-      const int64_t qd = t * in.ws.sE + int64_t(dn) * L + k;
-      g0 = in.ws.gx[qu]; g1 = in.ws.gx[qd]; g2 = in.ws.gy[qu]; g3 = in.ws.gy[qd];
-    } else {
-      const int64_t o = t * in.ws.sN;
-      g0 = in.ws.gnx[o + q1]; g1 = in.ws.gnx[o + q2]; g2 = in.ws.gny[o + q1]; g3 = in.ws.gny[o + q2];
-    }
-    const double A1 = ab2(T1, To[q1]), A2 = ab2(T2, To[q2]);
-    const double diff = A2 - A1;
-    const double Tm1 = A1 + (2.0 * diff + c1 * g0 + c2 * g2) / 6.0;
-    const double Tm2 = A2 - (2.0 * diff + c1 * g1 + c2 * g3) / 6.0;
-    const double ho = -0.5 * ((vf + avf) * Tm1 + (vf - avf) * Tm2);
-    in.ws.adfh[t * in.ws.sEd + int64_t(e) * L + k] = ho - fl;
+  const int64_t ts = in.tstride;
+  const int tg = in.tg;
+  double T1[NTR], T2[NTR], O1[NTR], O2[NTR], g0[NTR], g1[NTR], g2[NTR], g3[NTR];
+  ldn<NTR, IL>(in.T, q1, t0, ts, tg, T1);
+  ldn<NTR, IL>(in.T, q2, t0, ts, tg, T2);
+  ldn<NTR, IL>(in.T_old, q1, t0, ts, tg, O1);
+  ldn<NTR, IL>(in.T_old, q2, t0, ts, tg, O2);
+  if (use_tri) {
+    const int64_t qu = int64_t(up) * L + k, qd = int64_t(dn) * L + k;
+    ldn<NTR, IL>(in.ws.gx, qu, t0, in.ws.sE, tg, g0);
+    ldn<NTR, IL>(in.ws.gx, qd, t0, in.ws.sE, tg, g1);
+    ldn<NTR, IL>(in.ws.gy, qu, t0, in.ws.sE, tg, g2);
+    ldn<NTR, IL>(in.ws.gy, qd, t0, in.ws.sE, tg, g3);
+  } else {
+    ldn<NTR, IL>(in.ws.gnx, q1, t0, in.ws.sN, tg, g0);
+    ldn<NTR, IL>(in.ws.gnx, q2, t0, in.ws.sN, tg, g1);
+    ldn<NTR, IL>(in.ws.gny, q1, t0, in.ws.sN, tg, g2);
+    ldn<NTR, IL>(in.ws.gny, q2, t0, in.ws.sN, tg, g3);
   }
+  double adf[NTR];
+#pragma unroll
+  for (int t = 0; t < NTR; ++t) {
+    const double fl = -0.5 * (T1[t] * (vf + avf) + T2[t] * (vf - avf));
+    const double A1 = ab2(T1[t], O1[t]), A2 = ab2(T2[t], O2[t]);
+    const double diff = A2 - A1;
+    const double Tm1 = A1 + (2.0 * diff + c1 * g0[t] + c2 * g2[t]) / 6.0;
+    const double Tm2 = A2 - (2.0 * diff + c1 * g1[t] + c2 * g3[t]) / 6.0;
+    const double ho = -0.5 * ((vf + avf) * Tm1 + (vf - avf) * Tm2);
+    adf[t] = ho - fl;
+  }
+  stn<NTR, IL>(in.ws.adfh, int64_t(e) * L + k, t0, in.ws.sEd, tg, adf);
 }
 
 // ------------------------ zalesak a2: element max/min of the LO/T window
-__device__ __forceinline__ void body_elem_bounds(const Inst& in, int64_t i) {
+template <int NTR, bool IL>
+__device__ __forceinline__ void body_elem_bounds(const Inst& in, int64_t i, int t0) {
   const DevMesh& m = *in.m;
   if (i >= m.n_elem) return;
-  const uint32_t lane = m.elem_lanes[i];
+  const uint32_t lane = ld(m.elem_lanes + i);
   const int e = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const int64_t q0 = int64_t(m.enodes[3 * e]) * L + k, q1 = int64_t(m.enodes[3 * e + 1]) * L + k,
-                q2 = int64_t(m.enodes[3 * e + 2]) * L + k;
-  const int64_t qe = int64_t(e) * L + k;
-  for (int t = 0; t < in.ntr; ++t) {
-    const double* T = in.T + t * in.tstride;
-    const double* lo = in.ws.lo + t * in.ws.sN;
-    const double a0 = lo[q0], a1 = lo[q1], a2 = lo[q2];
-    const double b0 = T[q0], b1 = T[q1], b2 = T[q2];
-    in.ws.amax[t * in.ws.sE + qe] = fmax(fmax(fmax(a0, b0), fmax(a1, b1)), fmax(a2, b2));
-    in.ws.amin[t * in.ws.sE + qe] = fmin(fmin(fmin(a0, b0), fmin(a1, b1)), fmin(a2, b2));
+  const int64_t q[3] = {int64_t(ld(m.enodes + 3 * e)) * L + k,
+                        int64_t(ld(m.enodes + 3 * e + 1)) * L + k,
+                        int64_t(ld(m.enodes + 3 * e + 2)) * L + k};
+  double mx[NTR], mn[NTR];
+#pragma unroll
+  for (int t = 0; t < NTR; ++t) { mx[t] = -INFINITY; mn[t] = INFINITY; }
+#pragma unroll
+  for (int v = 0; v < 3; ++v) {
+    double a[NTR], b[NTR];
+    ldn<NTR, IL>(in.ws.lo, q[v], t0, in.ws.sN, in.tg, a);
+    ldn<NTR, IL>(in.T, q[v], t0, in.tstride, in.tg, b);
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) {
+      mx[t] = fmax(mx[t], fmax(a[t], b[t]));
+      mn[t] = fmin(mn[t], fmin(a[t], b[t]));
+    }
   }
+  const int64_t qe = int64_t(e) * L + k;
+  stn<NTR, IL>(in.ws.amax, qe, t0, in.ws.sE, in.tg, mx);
+  stn<NTR, IL>(in.ws.amin, qe, t0, in.ws.sE, in.tg, mn);
 }
 
 // ------------------------ zalesak a3: node cluster max/min over elements
-__device__ __forceinline__ void body_node_cluster(const Inst& in, int64_t i) {
+template <int NTR, bool IL>
+__device__ __forceinline__ void body_node_cluster(const Inst& in, int64_t i, int t0) {
   const DevMesh& m = *in.m;
   if (i >= m.n_layer) return;
-  const uint32_t lane = m.layer_lanes[i];
+  const uint32_t lane = ld(m.layer_lanes + i);
   const int n = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const int c0 = m.nel_off[n], c1 = m.nel_off[n + 1];
-  const int64_t qn = int64_t(n) * L + k;
-  for (int t = 0; t < in.ntr; ++t) {
-    double mx = -INFINITY, mn = INFINITY;
-    for (int j = c0; j < c1; ++j) {
-      const int el = m.nel_idx[j];
-      if (k >= m.eul[el] && k < m.enl[el]) {
-        const int64_t q = t * in.ws.sE + int64_t(el) * L + k;
-        mx = fmax(mx, in.ws.amax[q]);
-        mn = fmin(mn, in.ws.amin[q]);
-      } else {   // a cell without this level pads with -+BIG (tracer_adv.py:396-397)
-        mx = fmax(mx, -kBig);
-        mn = fmin(mn, kBig);
+  const int c0 = ld(m.nel_off + n), c1 = ld(m.nel_off + n + 1);
+  double mx[NTR], mn[NTR];
+#pragma unroll
+  for (int t = 0; t < NTR; ++t) { mx[t] = -INFINITY; mn[t] = INFINITY; }
+  for (int j = c0; j < c1; ++j) {
+    const int el = ld(m.nel_idx + j);
+    if (k >= ld(m.eul + el) && k < ld(m.enl + el)) {
+      const int64_t q = int64_t(el) * L + k;
+      double a[NTR], b[NTR];
+      ldn<NTR, IL>(in.ws.amax, q, t0, in.ws.sE, in.tg, a);
+      ldn<NTR, IL>(in.ws.amin, q, t0, in.ws.sE, in.tg, b);
+#pragma unroll
+      for (int t = 0; t < NTR; ++t) {
+        mx[t] = fmax(mx[t], a[t]);
+        mn[t] = fmin(mn[t], b[t]);
+      }
+    } else {   // a cell without this level pads with -+BIG (tracer_adv.py:396-397)
+#pragma unroll
+      for (int t = 0; t < NTR; ++t) {
+        mx[t] = fmax(mx[t], -kBig);
+        mn[t] = fmin(mn[t], kBig);
       }
     }
-    in.ws.tvmax[t * in.ws.sN + qn] = mx;
-    in.ws.tvmin[t * in.ws.sN + qn] = mn;
   }
+  const int64_t qn = int64_t(n) * L + k;
+  stn<NTR, IL>(in.ws.tvmax, qn, t0, in.ws.sN, in.tg, mx);
+  stn<NTR, IL>(in.ws.tvmin, qn, t0, in.ws.sN, in.tg, mn);
 }
 
 // ------------------- zalesak a4 + b1 + b2: admissible window, sums, factors
-__device__ __forceinline__ void body_node_factors(const Inst& in, int64_t i) {
+template <int NTR, bool IL>
+__device__ __forceinline__ void body_node_factors(const Inst& in, int64_t i, int t0) {
   const DevMesh& m = *in.m;
   if (i >= m.n_layer) return;
-  const uint32_t lane = m.layer_lanes[i];
+  const uint32_t lane = ld(m.layer_lanes + i);
   const int n = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const int nzmin = m.nzmin[n], nzmax = m.nzmax[n];
+  const int nzmin = ld(m.nzmin + n), nzmax = ld(m.nzmax + n);
   const int64_t base = int64_t(n) * L, qn = base + k;
   const bool use_own = (k == nzmin) || (k == nzmax - 1);
-  const double av = m.areasvol[qn], hnn = in.hnode_new[qn];
+  const double av = ld(m.areasvol + qn), hnn = ld(in.hnode_new + qn);
   const bool valid = (av > 0.0) && (hnn > 0.0);
   const double sa = av > 0.0 ? av : 1.0, sh = hnn > 0.0 ? hnn : 1.0;
   const double dt = in.dt;
-  const int e0 = m.ne_off[n], e1 = m.ne_off[n + 1];
-  for (int t = 0; t < in.ntr; ++t) {
-    const int64_t o = t * in.ws.sN;
-    const double* tvmax = in.ws.tvmax + o + base;
-    const double* tvmin = in.ws.tvmin + o + base;
-    double tmax, tmin;
-    if (use_own) {
-      tmax = tvmax[k];
-      tmin = tvmin[k];
-    } else {
-      const int km = k > 0 ? k - 1 : 0;
-      const double up_max = k + 1 < L ? tvmax[k + 1] : 0.0;
-      const double up_min = k + 1 < L ? tvmin[k + 1] : 0.0;
-      tmax = fmax(fmax(tvmax[km], tvmax[k]), up_max);
-      tmin = fmin(fmin(tvmin[km], tvmin[k]), up_min);
+  const int tg = in.tg;
+  const int64_t sN = in.ws.sN;
+  double tmax[NTR], tmin[NTR];
+  ldn<NTR, IL>(in.ws.tvmax, qn, t0, sN, tg, tmax);
+  ldn<NTR, IL>(in.ws.tvmin, qn, t0, sN, tg, tmin);
+  if (!use_own) {   // interior: max/min over k-1, k, k+1 (all layers of this column)
+    double am[NTR], an[NTR], bm[NTR], bn[NTR];
+    ldn<NTR, IL>(in.ws.tvmax, qn - 1, t0, sN, tg, am);
+    ldn<NTR, IL>(in.ws.tvmin, qn - 1, t0, sN, tg, an);
+    ldn<NTR, IL>(in.ws.tvmax, qn + 1, t0, sN, tg, bm);
+    ldn<NTR, IL>(in.ws.tvmin, qn + 1, t0, sN, tg, bn);
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) {
+      tmax[t] = fmax(fmax(am[t], tmax[t]), bm[t]);
+      tmin[t] = fmin(fmin(an[t], tmin[t]), bn[t]);
     }
-    const double lo = in.ws.lo[o + qn];
-    const double fmax_w = tmax - lo, fmin_w = tmin - lo;
-    const double* adfv = in.ws.adfv + o + base;
-    const double fvt = adfv[k], fvb = k + 1 < L ? adfv[k + 1] : 0.0;
-    const double pos_v = fmax(fvt, 0.0) + fmax(-fvb, 0.0);
-    const double neg_v = fmin(fvt, 0.0) + fmin(-fvb, 0.0);
-    double sp = 0.0, sm = 0.0;
-    for (int j = e0; j < e1; ++j) {
-      const int idx = m.ne_idx[j], e = idx >> 1;
-      if (k < m.ekmin[e] || k >= m.ekmax[e]) continue;   // no flux on this level
-      const double a = in.ws.adfh[t * in.ws.sEd + int64_t(e) * L + k];
-      const double s = (idx & 1) ? -a : a;
-      sp += fmax(s, 0.0);
-      sm += fmin(s, 0.0);
+  }
+  double lo[NTR], ft[NTR], fb[NTR];
+  ldn<NTR, IL>(in.ws.lo, qn, t0, sN, tg, lo);
+  ldn<NTR, IL>(in.ws.adfv, qn, t0, sN, tg, ft);
+  ldn<NTR, IL>(in.ws.adfv, qn + 1, t0, sN, tg, fb);   // k+1 <= nzmax < L
+  double sp[NTR], sm[NTR];
+#pragma unroll
+  for (int t = 0; t < NTR; ++t) sp[t] = sm[t] = 0.0;
+  const int e0 = ld(m.ne_off + n), e1 = ld(m.ne_off + n + 1);
+  for (int j = e0; j < e1; ++j) {
+    const int idx = ld(m.ne_idx + j), e = idx >> 1;
+    if (k < ld(m.ekmin + e) || k >= ld(m.ekmax + e)) continue;   // no flux on this level
+    double a[NTR];
+    ldn<NTR, IL>(in.ws.adfh, int64_t(e) * L + k, t0, in.ws.sEd, tg, a);
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) {
+      const double s = (idx & 1) ? -a[t] : a[t];
+      sp[t] += fmax(s, 0.0);
+      sm[t] += fmin(s, 0.0);
     }
-    const double plus = pos_v + sp, minus = neg_v + sm;
-    double pf = 1.0, mf = 1.0;
+  }
+  double pf[NTR], mf[NTR];
+#pragma unroll
+  for (int t = 0; t < NTR; ++t) {
+    const double plus = (fmax(ft[t], 0.0) + fmax(-fb[t], 0.0)) + sp[t];
+    const double minus = (fmin(ft[t], 0.0) + fmin(-fb[t], 0.0)) + sm[t];
+    pf[t] = 1.0;
+    mf[t] = 1.0;
     if (valid) {
       const double flux_pos = plus * dt / sa / sh + kFluxEps;
       const double flux_neg = minus * dt / sa / sh - kFluxEps;
-      pf = fmin(1.0, fmax_w / flux_pos);
-      mf = fmin(1.0, fmin_w / flux_neg);
+      pf[t] = fmin(1.0, (tmax[t] - lo[t]) / flux_pos);
+      mf[t] = fmin(1.0, (tmin[t] - lo[t]) / flux_neg);
     }
-    in.ws.pf[o + qn] = pf;
-    in.ws.mf[o + qn] = mf;
   }
-}
-
-// Limited vertical antidiffusive flux at interface j (tracer_adv.py:453-459).
-__device__ __forceinline__ double adfv_lim(const double* adfv, const double* pf,
-                                           const double* mf, int j, int nzmin, int nzmax) {
-  if (j >= nzmax && j != nzmin) return 0.0;   // adf_v[nzmax] == 0 by construction
-  const double f = adfv[j];
-  double ae;
-  if (j == nzmin) {
-    ae = f >= 0.0 ? pf[j] : mf[j];
-  } else {
-    ae = f >= 0.0 ? fmin(mf[j - 1], pf[j]) : fmin(pf[j - 1], mf[j]);
-  }
-  return ae * f;
+  stn<NTR, IL>(in.ws.pf, qn, t0, sN, tg, pf);
+  stn<NTR, IL>(in.ws.mf, qn, t0, sN, tg, mf);
 }
 
 // ---------- zalesak b3 + flux2dtracer_fct + ale_reconstruct: T_new on layers
-__device__ __forceinline__ void body_node_final(const Inst& in, int64_t i) {
+template <int NTR, bool IL>
+__device__ __forceinline__ void body_node_final(const Inst& in, int64_t i, int t0) {
   const DevMesh& m = *in.m;
   if (i >= m.n_layer) return;
-  const uint32_t lane = m.layer_lanes[i];
+  const uint32_t lane = ld(m.layer_lanes + i);
   const int n = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const int nzmin = m.nzmin[n], nzmax = m.nzmax[n];
+  const int nzmin = ld(m.nzmin + n), nzmax = ld(m.nzmax + n);
   const int64_t base = int64_t(n) * L, qn = base + k;
-  const double av = m.areasvol[qn];
+  const double av = ld(m.areasvol + qn);
   const double sa = av > 0.0 ? av : 1.0;
-  const double hn = in.hnode[qn], hnn = in.hnode_new[qn];
+  const double hn = ld(in.hnode + qn), hnn = ld(in.hnode_new + qn);
   const double dt = in.dt;
-  const int e0 = m.ne_off[n], e1 = m.ne_off[n + 1];
-  for (int t = 0; t < in.ntr; ++t) {
-    const int64_t o = t * in.ws.sN;
-    const double* pf = in.ws.pf + o;
-    const double* mf = in.ws.mf + o;
-    const double* adfv = in.ws.adfv + o + base;
-    const double vt = adfv_lim(adfv, pf + base, mf + base, k, nzmin, nzmax);
-    const double vb = adfv_lim(adfv, pf + base, mf + base, k + 1, nzmin, nzmax);
-    double hsc = 0.0;
-    for (int j = e0; j < e1; ++j) {
-      const int idx = m.ne_idx[j];
-      const int e = idx >> 1;
-      if (k < m.ekmin[e] || k >= m.ekmax[e]) continue;   // no flux on this level
-      const double a = in.ws.adfh[t * in.ws.sEd + int64_t(e) * L + k];
-      const int64_t p1 = int64_t(m.edges[2 * e]) * L + k, p2 = int64_t(m.edges[2 * e + 1]) * L + k;
-      const double ae = a >= 0.0 ? fmin(pf[p1], mf[p2]) : fmin(mf[p1], pf[p2]);
-      const double lim = ae * a;
-      hsc += (idx & 1) ? -lim : lim;
-    }
-    const double T = in.T[t * in.tstride + qn];
-    const double lo = in.ws.lo[o + qn];
-    const double lo_trans = -T * hn + lo * hnn;
-    const double vdiv = av > 0.0 ? (vt - vb) * dt / sa : 0.0;
-    double d = hsc * dt / sa + (lo_trans + vdiv);
-    d = d + T * (hn - hnn);
-    in.T_new[t * in.tstride + qn] = T + (hnn > 0.0 ? d / hnn : 0.0);
+  const int tg = in.tg;
+  const int64_t sN = in.ws.sN;
+  // own limiter factors at k (and k-1 / k+1 for the vertical fluxes)
+  double pf0[NTR], mf0[NTR], ft[NTR];
+  ldn<NTR, IL>(in.ws.pf, qn, t0, sN, tg, pf0);
+  ldn<NTR, IL>(in.ws.mf, qn, t0, sN, tg, mf0);
+  ldn<NTR, IL>(in.ws.adfv, qn, t0, sN, tg, ft);
+  // limited vertical flux at the top interface k (tracer_adv.py:453-459)
+  double vt[NTR];
+  if (k == nzmin) {
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) vt[t] = (ft[t] >= 0.0 ? pf0[t] : mf0[t]) * ft[t];
+  } else {
+    double pfa[NTR], mfa[NTR];
+    ldn<NTR, IL>(in.ws.pf, qn - 1, t0, sN, tg, pfa);
+    ldn<NTR, IL>(in.ws.mf, qn - 1, t0, sN, tg, mfa);
+#pragma unroll
+    for (int t = 0; t < NTR; ++t)
+      vt[t] = (ft[t] >= 0.0 ? fmin(mfa[t], pf0[t]) : fmin(pfa[t], mf0[t])) * ft[t];
   }
+  // limited vertical flux at the bottom interface k+1 (0 at the node's bottom)
+  double vb[NTR];
+  if (k + 1 >= nzmax) {
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) vb[t] = 0.0;
+  } else {
+    double fb[NTR], pfb[NTR], mfb[NTR];
+    ldn<NTR, IL>(in.ws.adfv, qn + 1, t0, sN, tg, fb);
+    ldn<NTR, IL>(in.ws.pf, qn + 1, t0, sN, tg, pfb);
+    ldn<NTR, IL>(in.ws.mf, qn + 1, t0, sN, tg, mfb);
+#pragma unroll
+    for (int t = 0; t < NTR; ++t)
+      vb[t] = (fb[t] >= 0.0 ? fmin(mf0[t], pfb[t]) : fmin(pf0[t], mfb[t])) * fb[t];
+  }
+  // limited horizontal fluxes, ascending edge id
+  double hsc[NTR];
+#pragma unroll
+  for (int t = 0; t < NTR; ++t) hsc[t] = 0.0;
+  const int e0 = ld(m.ne_off + n), e1 = ld(m.ne_off + n + 1);
+  for (int j = e0; j < e1; ++j) {
+    const int idx = ld(m.ne_idx + j), e = idx >> 1;
+    if (k < ld(m.ekmin + e) || k >= ld(m.ekmax + e)) continue;   // no flux on this level
+    const int64_t qo = int64_t(ld(m.ne_oth + j)) * L + k;
+    double a[NTR], pfo[NTR], mfo[NTR];
+    ldn<NTR, IL>(in.ws.adfh, int64_t(e) * L + k, t0, in.ws.sEd, tg, a);
+    ldn<NTR, IL>(in.ws.pf, qo, t0, sN, tg, pfo);
+    ldn<NTR, IL>(in.ws.mf, qo, t0, sN, tg, mfo);
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) {
+      // (pf, mf) at the edge's first node n1 and second node n2
+      const double pf1 = (idx & 1) ? pfo[t] : pf0[t], mf1 = (idx & 1) ? mfo[t] : mf0[t];
+      const double pf2 = (idx & 1) ? pf0[t] : pfo[t], mf2 = (idx & 1) ? mf0[t] : mfo[t];
+      const double ae = a[t] >= 0.0 ? fmin(pf1, mf2) : fmin(mf1, pf2);
+      const double lim = ae * a[t];
+      hsc[t] += (idx & 1) ? -lim : lim;
+    }
+  }
+  double Tv[NTR], lo[NTR], out[NTR];
+  ldn<NTR, IL>(in.T, qn, t0, in.tstride, tg, Tv);
+  ldn<NTR, IL>(in.ws.lo, qn, t0, sN, tg, lo);
+#pragma unroll
+  for (int t = 0; t < NTR; ++t) {
+    const double lo_trans = -Tv[t] * hn + lo[t] * hnn;
+    const double vdiv = av > 0.0 ? (vt[t] - vb[t]) * dt / sa : 0.0;
+    double d = hsc[t] * dt / sa + (lo_trans + vdiv);
+    d = d + Tv[t] * (hn - hnn);
+    out[t] = Tv[t] + (hnn > 0.0 ? d / hnn : 0.0);
+  }
+  stn<NTR, IL>(in.T_new, qn, t0, in.tstride, tg, out);
 }
 
 // ------------------------------------------- dry levels keep T (ale_reconstruct)
+template <bool IL>
 __device__ __forceinline__ void body_copy_dry(const Inst& in, int64_t i) {
   const DevMesh& m = *in.m;
   const int64_t NL = int64_t(m.N) * m.L;
   if (i >= NL) return;
   const int n = int(i / m.L), k = int(i - int64_t(n) * m.L);
   if (k >= m.nzmin[n] && k < m.nzmax[n]) return;
-  for (int t = 0; t < in.ntr; ++t) in.T_new[t * in.tstride + i] = in.T[t * in.tstride + i];
+  for (int t = 0; t < in.ntr; ++t) {
+    const int64_t a = tix<IL>(i, t, in.tstride, in.tg);
+    in.T_new[a] = in.T[a];
+  }
 }
 
-#define FCT_KERNEL_PAIR(name, body)                                               \
-  __global__ void __launch_bounds__(256) name##_1(Inst in) { body(in, lane_index()); } \
-  __global__ void __launch_bounds__(256) name##_n(const Inst* __restrict__ tab) {  \
-    body(tab[blockIdx.y], lane_index());                                          \
+// Kernel wrappers: ``_1`` takes one instance by value (tracer-major layout, the
+// single-call path); ``_n`` reads instance blockIdx.y of a device table (interleaved
+// layout, the batched path).
+#define FCT_KERNEL_T(name, body)                                                        \
+  template <int NTR>                                                                    \
+  __global__ void __launch_bounds__(256) name##_1(Inst in, int t0) {                    \
+    body<NTR, false>(in, lane_index(), t0);                                             \
+  }                                                                                     \
+  template <int NTR>                                                                    \
+  __global__ void __launch_bounds__(256) name##_n(const Inst* __restrict__ tab, int t0) { \
+    body<NTR, true>(tab[blockIdx.y], lane_index(), t0);                                 \
   }
 
-FCT_KERNEL_PAIR(k_vflux, body_vflux)
-FCT_KERNEL_PAIR(k_elem_grad, body_elem_grad)
-FCT_KERNEL_PAIR(k_node_lo, body_node_lo)
-FCT_KERNEL_PAIR(k_vert_impl, body_vert_impl)
-FCT_KERNEL_PAIR(k_edge_adf, body_edge_adf)
-FCT_KERNEL_PAIR(k_elem_bounds, body_elem_bounds)
-FCT_KERNEL_PAIR(k_node_cluster, body_node_cluster)
-FCT_KERNEL_PAIR(k_node_factors, body_node_factors)
-FCT_KERNEL_PAIR(k_node_final, body_node_final)
-FCT_KERNEL_PAIR(k_copy_dry, body_copy_dry)
+FCT_KERNEL_T(k_elem_grad, body_elem_grad)
+FCT_KERNEL_T(k_node_lo, body_node_lo)
+FCT_KERNEL_T(k_vert_impl, body_vert_impl)
+FCT_KERNEL_T(k_edge_adf, body_edge_adf)
+FCT_KERNEL_T(k_elem_bounds, body_elem_bounds)
+FCT_KERNEL_T(k_node_cluster, body_node_cluster)
+FCT_KERNEL_T(k_node_factors, body_node_factors)
+FCT_KERNEL_T(k_node_final, body_node_final)
+
+__global__ void __launch_bounds__(256) k_vflux_1(Inst in) { body_vflux(in, lane_index()); }
+__global__ void __launch_bounds__(256) k_vflux_n(const Inst* __restrict__ tab) {
+  body_vflux(tab[blockIdx.y], lane_index());
+}
+__global__ void __launch_bounds__(256) k_copy_dry_1(Inst in) {
+  body_copy_dry<false>(in, lane_index());
+}
+__global__ void __launch_bounds__(256) k_copy_dry_n(const Inst* __restrict__ tab) {
+  body_copy_dry<true>(tab[blockIdx.y], lane_index());
+}
 
 }  // namespace
 
 const char* const kStageNames[kNumStages] = {
     "vflux", "elem_grad", "node_lo", "vert_impl", "edge_adf", "elem_bounds",
     "node_cluster", "node_factors", "node_final", "copy_dry"};
+
+// One stage over all tracer chunks (NTR in {8, 4, 2, 1}, largest first, at most
+// d.chunk tracers per thread).
+#define FCT_STAGE(name, lanes)                                                          \
+  do {                                                                                  \
+    const dim3 g = grid(lanes);                                                         \
+    for (int t0 = 0; t0 < d.ntr;) {                                                     \
+      const int rem = std::min(d.ntr - t0, d.chunk);                                    \
+      if (rem >= 8) {                                                                   \
+        if (tab) name##_n<8><<<g, B, 0, s>>>(tab, t0);                                  \
+        else name##_1<8><<<g, B, 0, s>>>(single, t0);                                   \
+        t0 += 8;                                                                        \
+      } else if (rem >= 4) {                                                            \
+        if (tab) name##_n<4><<<g, B, 0, s>>>(tab, t0);                                  \
+        else name##_1<4><<<g, B, 0, s>>>(single, t0);                                   \
+        t0 += 4;                                                                        \
+      } else if (rem >= 2) {                                                            \
+        if (tab) name##_n<2><<<g, B, 0, s>>>(tab, t0);                                  \
+        else name##_1<2><<<g, B, 0, s>>>(single, t0);                                   \
+        t0 += 2;                                                                        \
+      } else {                                                                          \
+        if (tab) name##_n<1><<<g, B, 0, s>>>(tab, t0);                                  \
+        else name##_1<1><<<g, B, 0, s>>>(single, t0);                                   \
+        t0 += 1;                                                                        \
+      }                                                                                 \
+    }                                                                                   \
+  } while (0)
 
 int launch_forward_events(const Inst& single, const Inst* tab, int n, const LaunchDims& d,
                           cudaStream_t s, cudaEvent_t* after) {
@@ -460,25 +692,30 @@ int launch_forward_events(const Inst& single, const Inst* tab, int n, const Laun
     if (after) cudaEventRecord(after[stage], s);
     ++stage;
   };
-#define FCT_LAUNCH(name, lanes, enabled)                            \
-  do {                                                              \
-    if (enabled) {                                                  \
-      if (tab) name##_n<<<grid(lanes), B, 0, s>>>(tab);             \
-      else name##_1<<<grid(lanes), B, 0, s>>>(single);              \
-    }                                                               \
-    mark();                                                         \
-  } while (0)
-  FCT_LAUNCH(k_vflux, d.max_edge, true);
-  FCT_LAUNCH(k_elem_grad, d.max_elem, true);
-  FCT_LAUNCH(k_node_lo, d.max_iface, true);
-  FCT_LAUNCH(k_vert_impl, d.max_nodes, d.any_wi);
-  FCT_LAUNCH(k_edge_adf, d.max_edge, true);
-  FCT_LAUNCH(k_elem_bounds, d.max_elem, true);
-  FCT_LAUNCH(k_node_cluster, d.max_layer, true);
-  FCT_LAUNCH(k_node_factors, d.max_layer, true);
-  FCT_LAUNCH(k_node_final, d.max_layer, true);
-  FCT_LAUNCH(k_copy_dry, d.max_dense, d.copy_dry);
-#undef FCT_LAUNCH
+  if (tab) k_vflux_n<<<grid(d.max_edge), B, 0, s>>>(tab);
+  else k_vflux_1<<<grid(d.max_edge), B, 0, s>>>(single);
+  mark();
+  FCT_STAGE(k_elem_grad, d.max_elem);
+  mark();
+  FCT_STAGE(k_node_lo, d.max_iface);
+  mark();
+  if (d.any_wi) FCT_STAGE(k_vert_impl, d.max_nodes);
+  mark();
+  FCT_STAGE(k_edge_adf, d.max_edge);
+  mark();
+  FCT_STAGE(k_elem_bounds, d.max_elem);
+  mark();
+  FCT_STAGE(k_node_cluster, d.max_layer);
+  mark();
+  FCT_STAGE(k_node_factors, d.max_layer);
+  mark();
+  FCT_STAGE(k_node_final, d.max_layer);
+  mark();
+  if (d.copy_dry) {
+    if (tab) k_copy_dry_n<<<grid(d.max_dense), B, 0, s>>>(tab);
+    else k_copy_dry_1<<<grid(d.max_dense), B, 0, s>>>(single);
+  }
+  mark();
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_error(e, "forward kernel launch");
   return FCT_OK;

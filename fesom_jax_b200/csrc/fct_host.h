@@ -29,7 +29,8 @@ inline int cuda_error(cudaError_t e, const char* what) {
 // whose lane counts are bounded by the ``max_*`` arguments.
 struct LaunchDims {
   int64_t max_iface, max_layer, max_edge, max_elem, max_dense, max_nodes;
-  int max_ntr;
+  int ntr;         // tracers per instance (every instance of a launch has the same)
+  int chunk = 8;   // most tracers one thread carries (8, 4, 2 or 1): the tuning knob
   bool any_wi;      // launch the implicit w_i stage
   bool copy_dry;    // launch the dry-level copy
 };

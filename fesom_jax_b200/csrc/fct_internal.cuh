@@ -36,6 +36,7 @@ struct DevMesh {
   const int* nlmin;      // nlevels_nod2D_min
   const int* ne_off;     // node -> incident edges CSR, ascending edge id
   const int* ne_idx;     //   entry = 2*edge + (node is the edge's second node)
+  const int* ne_oth;     //   the edge's other node, aligned with ne_idx
   const int* nel_off;    // node -> elements CSR (nod_in_elem2D, element-ascending)
   const int* nel_idx;
   const double* area;    // [N,L]
@@ -81,12 +82,18 @@ struct Workspace {
 };
 
 // One FCT instance: a mesh, its per-call fields, and a workspace.
+//
+// Tracer layouts: tracer-major (the reference's, one [entity, L] array per tracer,
+// ``tstride`` doubles apart; ``tg == 0``) or interleaved (``[entity, L, tg]``: the ``tg``
+// tracers of one entity-level are contiguous, so a neighbour gather is one contiguous
+// chunk). The workspace uses the same convention (interleaved with the same ``tg``).
 struct Inst {
   const DevMesh* m;
   const double *uv, *w_e, *helem, *hnode, *hnode_new;
   const double *T, *T_old;
   double* T_new;
   int64_t tstride;
+  int tg;
   const double *Z3d, *zbar3, *w_i;
   Workspace ws;
   double dt;

@@ -146,7 +146,7 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
     enl[e] = d->nlevels[e] - 1;
   }
   // node -> edge CSR (ascending edge id per node)
-  std::vector<int> ne_off(N + 1, 0), ne_idx(2 * size_t(Ed));
+  std::vector<int> ne_off(N + 1, 0), ne_idx(2 * size_t(Ed)), ne_oth(2 * size_t(Ed));
   for (int e = 0; e < Ed; ++e) {
     ne_off[d->edges[2 * e] + 1]++;
     ne_off[d->edges[2 * e + 1] + 1]++;
@@ -155,8 +155,11 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   {
     std::vector<int> fillp(ne_off.begin(), ne_off.end() - 1);
     for (int e = 0; e < Ed; ++e) {
-      ne_idx[fillp[d->edges[2 * e]]++] = 2 * e;
-      ne_idx[fillp[d->edges[2 * e + 1]]++] = 2 * e + 1;
+      const int a = d->edges[2 * e], b = d->edges[2 * e + 1];
+      ne_oth[fillp[a]] = b;
+      ne_idx[fillp[a]++] = 2 * e;
+      ne_oth[fillp[b]] = a;
+      ne_idx[fillp[b]++] = 2 * e + 1;
     }
   }
   // per-edge MFCT coefficients, reference expression (tracer_adv.py:216-222)
@@ -206,6 +209,7 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   size_t o_nzmin = b.add(nzmin.data(), N), o_nzmax = b.add(nzmax.data(), N);
   size_t o_ulmax = b.add(d->ulevels_nod2D_max, N), o_nlmin = b.add(d->nlevels_nod2D_min, N);
   size_t o_neoff = b.add(ne_off.data(), N + 1), o_neidx = b.add(ne_idx.data(), ne_idx.size());
+  size_t o_neoth = b.add(ne_oth.data(), ne_oth.size());
   size_t o_neloff = b.add(d->nod_in_elem2D_offsets, N + 1);
   size_t o_nelidx = b.add(d->nod_in_elem2D, nie);
   size_t o_area = b.add(d->area, size_t(N) * L), o_av = b.add(d->areasvol, size_t(N) * L);
@@ -233,6 +237,7 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   m.nlmin = (const int*)(base + o_nlmin);
   m.ne_off = (const int*)(base + o_neoff);
   m.ne_idx = (const int*)(base + o_neidx);
+  m.ne_oth = (const int*)(base + o_neoth);
   m.nel_off = (const int*)(base + o_neloff);
   m.nel_idx = (const int*)(base + o_nelidx);
   m.area = (const double*)(base + o_area);
@@ -331,12 +336,22 @@ int fct_forward(FctPlan* P, const FctFields* f, double dt, int ntr, fct_stream_t
   in.hnode = f->hnode; in.hnode_new = f->hnode_new;
   in.T = f->T; in.T_old = f->T_old; in.T_new = f->T_new;
   in.tstride = f->tracer_stride ? f->tracer_stride : int64_t(P->N) * P->L;
+  in.tg = 0;
   in.Z3d = f->Z3d; in.zbar3 = f->zbar3; in.w_i = f->w_i;
   in.ws = P->ws;
   in.dt = dt;
   in.ntr = ntr;
-  LaunchDims dims{P->hm.n_iface, P->hm.n_layer, P->hm.n_edge, P->hm.n_elem,
-                  int64_t(P->N) * P->L, int64_t(P->N), ntr, f->w_i != nullptr, true};
+  LaunchDims dims{};
+  dims.max_iface = P->hm.n_iface;
+  dims.max_layer = P->hm.n_layer;
+  dims.max_edge = P->hm.n_edge;
+  dims.max_elem = P->hm.n_elem;
+  dims.max_dense = int64_t(P->N) * P->L;
+  dims.max_nodes = P->N;
+  dims.ntr = ntr;
+  dims.chunk = 8;
+  dims.any_wi = f->w_i != nullptr;
+  dims.copy_dry = true;   // a fresh T_new: dry levels keep T (tracer_adv.py:147-151)
   int prev = -1;
   cudaGetDevice(&prev);
   if (prev != P->device) cudaSetDevice(P->device);

@@ -49,8 +49,9 @@ def _bind_batch(L):
     L.fct_batch_profile.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.c_int,
                                     C.c_void_p]
     L.fct_stage_name.restype = C.c_char_p
+    L.fct_batch_set_chunk.argtypes = [C.c_void_p, C.c_int]
     for n in ("fct_batch_create", "fct_batch_destroy", "fct_batch_info", "fct_batch_prepare",
-              "fct_batch_step", "fct_batch_run", "fct_batch_profile"):
+              "fct_batch_step", "fct_batch_run", "fct_batch_profile", "fct_batch_set_chunk"):
         getattr(L, n).restype = C.c_int
     L._batch_bound = True
     return L
@@ -68,7 +69,7 @@ class Member:
     helem: object
     hnode: object
     hnode_new: object
-    buf: object         # torch [3, ntr, N, nl]
+    buf: object         # torch [3, N, nl, ntr] (tracers interleaved innermost)
 
 
 class Ensemble:
@@ -82,6 +83,7 @@ class Ensemble:
         self._plans: dict[int, FctPlan] = {}
         self._h = None
         self.phase = 0
+        self.chunk = 8
 
     # ---------------------------------------------------------------- members
     def plan(self, mesh: Mesh) -> FctPlan:
@@ -109,10 +111,10 @@ class Ensemble:
         N, nl = mesh.nod2D, mesh.nl
         if tuple(T.shape) != (ntr, N, nl) or tuple(T_old.shape) != (ntr, N, nl):
             raise ValueError("T/T_old must be [ntr, nod2D, nl]")
-        buf = t.empty((3, ntr, N, nl), dtype=t.float64, device=dev)
-        buf[0].copy_(T_old)
-        buf[1].copy_(T)
-        buf[2].copy_(T)
+        buf = t.empty((3, N, nl, ntr), dtype=t.float64, device=dev)
+        buf[0].copy_(T_old.permute(1, 2, 0))
+        buf[1].copy_(T.permute(1, 2, 0))
+        buf[2].copy_(T.permute(1, 2, 0))
         self.plan(mesh)
         self.members.append(Member(mesh, ntr, float(dt), d(uv), d(w_e), d(helem), d(hnode),
                                    d(hnode_new), buf))
@@ -165,6 +167,32 @@ class Ensemble:
                                                          self._stream(stream)))
         self.phase += int(steps)
 
+    def set_chunk(self, chunk: int) -> None:
+        _lib.check(_bind_batch(_lib.lib()).fct_batch_set_chunk(self._h, int(chunk)))
+        self.chunk = int(chunk)
+
+    def autotune(self, steps: int = 2, candidates=(8, 4, 2, 1), reps: int = 2) -> dict:
+        """Time ``steps``-step graph runs for each tracer-chunk candidate (the member state
+        advances while tuning) and keep the fastest; returns ``{chunk: ms}``."""
+        t = self.torch
+        stream = t.cuda.current_stream(self.device)
+        times = {}
+        for c in candidates:
+            if c > max(m.ntr for m in self.members) and c != min(candidates):
+                continue
+            self.set_chunk(c)
+            self.run(steps)                      # capture + warm
+            e0, e1 = t.cuda.Event(enable_timing=True), t.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                self.run(steps)
+            e1.record(stream)
+            e1.synchronize()
+            times[c] = e0.elapsed_time(e1) / reps
+        best = min(times, key=times.get)
+        self.set_chunk(best)
+        return times
+
     def profile_step(self, stream=None) -> dict:
         """Run one step stage by stage (synchronising) and return ``{stage: ms}``."""
         L = _bind_batch(_lib.lib())
@@ -180,13 +208,25 @@ class Ensemble:
 
     # ------------------------------------------------------------------ state
     def state(self, i: int):
-        """``(T, T_old)`` views ``[ntr, N, nl]`` of member ``i`` (device)."""
+        """``(T, T_old)`` of member ``i`` as ``[ntr, N, nl]`` views (device, strided:
+        the resident buffers keep the tracers innermost)."""
+        b = self.members[i].buf
+        p = self.phase
+        return b[(p + 1) % 3].permute(2, 0, 1), b[p % 3].permute(2, 0, 1)
+
+    def state_interleaved(self, i: int):
+        """``(T, T_old)`` of member ``i`` in the resident ``[N, nl, ntr]`` layout."""
         b = self.members[i].buf
         p = self.phase
         return b[(p + 1) % 3], b[p % 3]
 
-    def set_state(self, i: int, T, T_old, non_blocking: bool = False) -> None:
-        Tc, To = self.state(i)
+    def set_state(self, i: int, T, T_old, non_blocking: bool = False,
+                  interleaved: bool = False) -> None:
+        """Copy ``T``/``T_old`` (``[ntr, N, nl]``, or ``[N, nl, ntr]`` when
+        ``interleaved``) into member ``i``'s current buffers."""
+        Tc, To = self.state_interleaved(i)
+        if not interleaved:
+            T, T_old = T.permute(1, 2, 0), T_old.permute(1, 2, 0)
         Tc.copy_(T, non_blocking=non_blocking)
         To.copy_(T_old, non_blocking=non_blocking)
 

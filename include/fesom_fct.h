@@ -118,8 +118,9 @@ int fct_compute_w(FctPlan* plan, const double* uv, const double* helem, double* 
 /*
  * Batched ensemble stepping: many FCT instances (ensemble members x tracers, on meshes
  * of different sizes) advanced together, one launch per stage for all instances of a
- * workspace group. Each instance owns three rotating tracer buffers of ``ntr`` tracers
- * (``[ntr, nod2D, nl]``, DEVICE); a step of phase p reads T_old = buf[p],
+ * workspace group. Each instance owns three rotating tracer buffers of ``ntr`` tracers,
+ * INTERLEAVED ``[nod2D, nl, ntr]`` (DEVICE; the tracers of one node-level contiguous);
+ * a step of phase p reads T_old = buf[p],
  * T = buf[(p+1)%3] and writes T_new = buf[(p+2)%3], so consecutive phases carry the AB2
  * history (T_old_new = T) without copies. Start with T_old in buf[0], T in buf[1].
  */
@@ -130,7 +131,7 @@ typedef struct FctInstance {
   const double* helem;      /* [elem2D,nl] */
   const double* hnode;      /* [nod2D,nl] */
   const double* hnode_new;  /* [nod2D,nl] */
-  double* buf[3];           /* rotating tracer buffers, each ntr x [nod2D,nl] */
+  double* buf[3];           /* rotating tracer buffers, each [nod2D,nl,ntr] */
   int ntr;
   double dt;
 } FctInstance;
@@ -143,6 +144,10 @@ typedef struct FctBatch FctBatch;
 int fct_batch_create(const FctInstance* insts, int n, int64_t workspace_budget_bytes,
                      FctBatch** out);
 int fct_batch_destroy(FctBatch* b);
+/* Tuning: the most tracers one thread carries (1, 2, 4 or 8; default 8). Fewer use fewer
+ * registers (higher occupancy), more share each gather's index work. Drops cached
+ * graphs. */
+int fct_batch_set_chunk(FctBatch* b, int chunk);
 /* [instances, groups, workspace bytes, total wet node layers x tracers] */
 int fct_batch_info(const FctBatch* b, int64_t out[4]);
 /* Copy the dry levels of buf[1] into buf[0] and buf[2] (dry levels never change). */

@@ -110,3 +110,22 @@ def test_compute_w_gpu_matches_reference_digest(torch, pi, golden, pi_cases):
     ref = c["w_e"]
     assert np.max(np.abs(w - ref)) <= 1e-12 * np.max(np.abs(ref))
     assert np.all(w[~pi.node_iface_mask] == 0.0)
+
+
+def test_dry_levels_keep_T_exactly(torch, pi, pi_cases):
+    """Invalid lanes keep T (tracer_adv.py:147-151) even when T is nonzero there and the
+    output buffer holds stale data."""
+    from fesom_jax_b200.tracer_adv import get_plan
+    c = pi_cases["T_ab2"]
+    lm = pi.node_layer_mask
+    T = np.where(lm, c["T"], 99.0)
+    To = np.where(lm, c["T_old"], -7.0)
+    args = [_dev(torch, c[k]) for k in ("uv", "w_e", "helem", "hnode", "hnode_new")]
+    out = torch.full((2, pi.nod2D, pi.nl), 12345.0, dtype=torch.float64, device="cuda")
+    TT, TO = _dev(torch, np.stack([T, T])), _dev(torch, np.stack([To, To]))
+    get_plan(pi, 0).forward(*args, TT, TO, DT, out=out)
+    got = out.cpu().numpy()
+    assert np.all(got[:, ~lm] == 99.0)
+    ref, _ = fct_np.advect_one_fct(pi, c["uv"], c["w_e"], c["helem"], c["hnode"],
+                                   c["hnode_new"], T, To, dt=DT)
+    assert np.max(np.abs(got[0][lm] - ref[lm])) / np.max(np.abs(ref[lm])) <= RTOL
