@@ -110,6 +110,18 @@ int fct_plan_info(const FctPlan* plan, int64_t out[8]);
 int fct_forward(FctPlan* plan, const FctFields* fields, double dt, int ntr,
                 fct_stream_t stream);
 
+/* The same step as fct_forward for callers that cannot allocate device memory at call
+ * time (an XLA/JAX custom-call handler running inside a runtime that owns the GPU's
+ * memory, a stream under CUDA-graph capture, a serving loop that must not block on the
+ * allocator). Its scratch is a 64 MiB file-scope device array instead of the plan's
+ * workspace, so the plan may have been created with any max_tracers; sizes whose scratch
+ * exceeds the array return FCT_ERR_CAPACITY. No reference counterpart: the reference
+ * lets XLA allocate its temporaries. The first call on a device looks up the array's
+ * address (make it before any stream capture); all calls share the array, so calls that
+ * overlap on the GPU race. */
+int fct_forward_noalloc(FctPlan* plan, const FctFields* fields, double dt, int ntr,
+                        fct_stream_t stream);
+
 /* Vertical velocity at interfaces from continuity, fesom_jax/ale.py:309-365
  * (``compute_w(mesh, uv, helem)``): ``w`` [nod2D,nl] (DEVICE), all levels written. */
 int fct_compute_w(FctPlan* plan, const double* uv, const double* helem, double* w,
