@@ -682,7 +682,7 @@ const char* const kStageNames[kNumStages] = {
   } while (0)
 
 int launch_forward_events(const Inst& single, const Inst* tab, int n, const LaunchDims& d,
-                          cudaStream_t s, cudaEvent_t* after) {
+                          cudaStream_t s, cudaEvent_t* after, bool stop_before_final) {
   constexpr int B = 256;
   auto grid = [&](int64_t lanes) {
     return dim3(unsigned(std::max<int64_t>(1, (lanes + B - 1) / B)), unsigned(n), 1);
@@ -709,6 +709,10 @@ int launch_forward_events(const Inst& single, const Inst* tab, int n, const Laun
   mark();
   FCT_STAGE(k_node_factors, d.max_layer);
   mark();
+  if (stop_before_final) {
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? FCT_OK : cuda_error(e, "forward kernel launch");
+  }
   FCT_STAGE(k_node_final, d.max_layer);
   mark();
   if (d.copy_dry) {
@@ -723,7 +727,12 @@ int launch_forward_events(const Inst& single, const Inst* tab, int n, const Laun
 
 int launch_forward(const Inst& single, const Inst* tab, int n, const LaunchDims& d,
                    cudaStream_t s) {
-  return launch_forward_events(single, tab, n, d, s, nullptr);
+  return launch_forward_events(single, tab, n, d, s, nullptr, false);
+}
+
+int launch_forward_stages(const Inst& single, const LaunchDims& d, cudaStream_t s,
+                          bool through_factors) {
+  return launch_forward_events(single, nullptr, 1, d, s, nullptr, through_factors);
 }
 
 int launch_copy_dry(const Inst* tab, int n, int64_t max_dense, cudaStream_t s) {

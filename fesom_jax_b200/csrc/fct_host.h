@@ -40,7 +40,12 @@ int launch_forward(const Inst& single, const Inst* tab, int n, const LaunchDims&
 constexpr int kNumStages = 10;
 extern const char* const kStageNames[kNumStages];
 int launch_forward_events(const Inst& single, const Inst* tab, int n, const LaunchDims& d,
-                          cudaStream_t s, cudaEvent_t* after);
+                          cudaStream_t s, cudaEvent_t* after, bool stop_before_final = false);
+// Single-instance forward stages; ``through_factors`` stops after the limiter factors
+// (everything the reverse pass reads), without writing T_new.
+int launch_forward_stages(const Inst& single, const LaunchDims& d, cudaStream_t s,
+                          bool through_factors);
+// fct_plan_reserve (declared in the public header) is used by the adjoint reservation.
 
 // Copy T's dry levels into T_new for ``n`` instances of ``tab`` (ignores Inst::copy_dry).
 int launch_copy_dry(const Inst* tab, int n, int64_t max_dense, cudaStream_t s);

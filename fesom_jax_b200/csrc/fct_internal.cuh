@@ -53,6 +53,9 @@ struct DevMesh {
   const int* eupdn;      // [Ed,2]
   const double* cross;   // [Ed,4]
   const double* ecoef;   // [Ed,2]: edx*a, edy*R  (a = R*cos, averaged over the two cells)
+  const int* eedge;      // [E,3] the element's edges: 2*edge + (element is edge_tri[:,1])
+  const int* eud_off;    // element -> edges that use it as MFCT up/down triangle (CSR)
+  const int* eud_idx;    //   entry = 2*edge + slot (edge_up_dn_tri[edge, slot] == element)
   const int* ekmin;      // [Ed] first level of the edge's lanes (union of its cells' layers)
   const int* ekmax;      // [Ed] one past the last such level
   // vertical
@@ -100,6 +103,19 @@ struct Inst {
   int ntr;
 };
 
+// Reverse-pass intermediates of one instance (tracer-major, dense [entity, L]).
+struct AdjWorkspace {
+  // node [N, L] per tracer
+  double *gdel, *gLOd, *gTd, *gpf, *gmf, *gtmax, *gtmin, *gplus, *gminus, *gLOl;
+  double *gtvmax, *gtvmin, *gLOb, *gTb, *gdiv, *ggnx, *ggny, *gTp, *gTtr, *gTv, *gAv, *gw;
+  // edge [Ed, L] per tracer
+  double *gA1, *gA2, *gT1, *gT2, *gg0, *gg1, *gg2, *gg3, *gvf;
+  // element [E, L] per tracer
+  double *gamax, *gamin, *gtrx, *gtry;
+  int64_t sN, sE, sEd;
+};
+constexpr int kAdjNodeFields = 22, kAdjEdgeFields = 9, kAdjElemFields = 4;
+
 }  // namespace fct
 
 struct FctPlan {
@@ -112,4 +128,7 @@ struct FctPlan {
   double* d_ws = nullptr;          // workspace allocation
   fct::Workspace ws{};
   int64_t n_wet_elem_layers = 0;
+  double* d_adj = nullptr;         // reverse-pass workspace
+  int adj_tracers = 0;
+  fct::AdjWorkspace aws{};
 };

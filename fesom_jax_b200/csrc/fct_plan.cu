@@ -171,6 +171,31 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
     ecoef[2 * e] = d->edge_dxdy[2 * e] * a;
     ecoef[2 * e + 1] = d->edge_dxdy[2 * e + 1] * kREarth;
   }
+  // element -> its three edges (with its role), element -> edges using it as up/dn
+  std::vector<int> eedge(3 * size_t(E), -1), ecount(E, 0);
+  std::vector<int> eud_off(E + 1, 0), eud_idx;
+  for (int e = 0; e < Ed; ++e)
+    for (int r = 0; r < 2; ++r) {
+      const int el = d->edge_tri[2 * e + r];
+      if (el < 0) continue;
+      if (ecount[el] >= 3) return set_error(FCT_ERR_INVALID, "element %d has more than 3 edges", el);
+      eedge[3 * size_t(el) + ecount[el]++] = 2 * e + r;
+    }
+  for (int e = 0; e < Ed; ++e)
+    for (int r = 0; r < 2; ++r) {
+      const int el = d->edge_up_dn_tri[2 * e + r];
+      if (el >= 0) eud_off[el + 1]++;
+    }
+  for (int el = 0; el < E; ++el) eud_off[el + 1] += eud_off[el];
+  eud_idx.assign(size_t(eud_off[E]), 0);
+  {
+    std::vector<int> fillp(eud_off.begin(), eud_off.end() - 1);
+    for (int e = 0; e < Ed; ++e)
+      for (int r = 0; r < 2; ++r) {
+        const int el = d->edge_up_dn_tri[2 * e + r];
+        if (el >= 0) eud_idx[fillp[el]++] = 2 * e + r;
+      }
+  }
   std::vector<int> ekmin(Ed), ekmax(Ed);
   for (int e = 0; e < Ed; ++e) {
     const int el1 = d->edge_tri[2 * e], el2 = d->edge_tri[2 * e + 1];
@@ -221,6 +246,9 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   size_t o_cross = b.add(d->edge_cross_dxdy, 4 * size_t(Ed));
   size_t o_ecoef = b.add(ecoef.data(), ecoef.size());
   size_t o_ekmin = b.add(ekmin.data(), Ed), o_ekmax = b.add(ekmax.data(), Ed);
+  size_t o_eedge = b.add(eedge.data(), eedge.size());
+  size_t o_eudoff = b.add(eud_off.data(), eud_off.size());
+  size_t o_eudidx = b.add(eud_idx.data(), std::max<size_t>(eud_idx.size(), 1));
   size_t o_Zp = b.add(Zp.data(), L), o_zbar = b.add(d->zbar, L);
   size_t o_if = b.add(iface.data(), iface.size()), o_ly = b.add(layer.data(), layer.size());
   size_t o_ed = b.add(edgel.data(), edgel.size()), o_el = b.add(eleml.data(), eleml.size());
@@ -253,6 +281,9 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   m.cross = (const double*)(base + o_cross);
   m.ecoef = (const double*)(base + o_ecoef);
   m.ekmin = (const int*)(base + o_ekmin);
+  m.eedge = (const int*)(base + o_eedge);
+  m.eud_off = (const int*)(base + o_eudoff);
+  m.eud_idx = (const int*)(base + o_eudidx);
   m.ekmax = (const int*)(base + o_ekmax);
   m.Zp = (const double*)(base + o_Zp);
   m.zbar = (const double*)(base + o_zbar);
@@ -274,6 +305,7 @@ const char* fct_version(void) { return "fesom_fct 0.1.0 (sm_100a, fp64)"; }
 int fct_plan_destroy(FctPlan* P) {
   if (!P) return FCT_OK;
   cudaSetDevice(P->device);
+  if (P->d_adj) cudaFree(P->d_adj);
   if (P->d_ws) cudaFree(P->d_ws);
   if (P->d_mesh) cudaFree(P->d_mesh);
   if (P->d_static) cudaFree(P->d_static);

@@ -110,6 +110,34 @@ int fct_plan_info(const FctPlan* plan, int64_t out[8]);
 int fct_forward(FctPlan* plan, const FctFields* fields, double dt, int ntr,
                 fct_stream_t stream);
 
+/*
+ * Reverse mode (the reference's autodiff surface: jax.grad through advect_one_fct,
+ * fesom_jax/integrate.py:43-169 under jax.grad). Cotangents follow JAX's subgradient
+ * conventions: maximum/minimum split equally at a tie, segment_max/min and max over an
+ * element's vertices spread evenly over tied entries, abs'(0) = 0.
+ */
+typedef struct FctGrads {
+  double* gT;       /* ntr x [nod2D,nl] cotangent of T (written) */
+  double* gT_old;   /* ntr x [nod2D,nl] cotangent of T_old (written) */
+  double* guv;      /* [elem2D,nl,2] cotangent of uv, summed over tracers (written) */
+  double* gw_e;     /* [nod2D,nl] cotangent of w_e, summed over tracers (written) */
+} FctGrads;
+
+/* Reserve the reverse-pass workspace for ``max_tracers`` tracers (allocates). */
+int fct_plan_reserve_adjoint(FctPlan* plan, int max_tracers);
+/* Vector-Jacobian product of one FCT step (fct_forward's inputs, tracer-major layout):
+ * given ``gT_new`` (ntr x [nod2D,nl], same tracer stride as fields->T) write the
+ * cotangents of T, T_old, uv and w_e. Recomputes the forward step internally (per-step
+ * recomputation checkpointing: only the step's inputs need to be kept). The w_split
+ * option (fields->w_i) is not differentiated (FCT_ERR_UNSUPPORTED); Z3d/zbar3 are
+ * treated as constants. */
+int fct_adjoint(FctPlan* plan, const FctFields* fields, const double* gT_new, double dt,
+                int ntr, const FctGrads* grads, fct_stream_t stream);
+/* Vector-Jacobian product of fct_compute_w (fesom_jax/ale.py:309-365) w.r.t. uv:
+ * guv (+)= J^T gw, [elem2D,nl,2]; ``accumulate`` = 0 overwrites, 1 adds. */
+int fct_compute_w_adjoint(FctPlan* plan, const double* gw, const double* helem,
+                          double* guv, int accumulate, fct_stream_t stream);
+
 /* The same step as fct_forward for callers that cannot allocate device memory at call
  * time (an XLA/JAX custom-call handler running inside a runtime that owns the GPU's
  * memory, a stream under CUDA-graph capture, a serving loop that must not block on the
