@@ -236,7 +236,8 @@ def run_ours(args, D: Dist) -> dict | None:
     alg = W.algorithmic_bytes(mesh, cfg["ntr"], cfg["members"])
     pk = peaks()
     achieved = alg / (fct_step_ms / 1e3) / 1e9
-    n_kernels = (1 + 7 * -(-cfg["ntr"] // ens.chunk)) * info["groups"]
+    info = ens.info()   # after tuning: launches per step depend on tracers per thread
+    n_kernels = info["launches_per_step"]
     out = dict(value=value, t=t, info=info, clocks=clk, prof=prof, fct_step_ms=fct_step_ms,
                finite=finite, mesh=mesh, cfg=cfg, alg_bytes=alg,
                roofline=dict(bound="hbm", kernel="fct step (8 stage kernels)",

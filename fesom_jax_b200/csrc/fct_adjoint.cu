@@ -822,6 +822,7 @@ int fct_adjoint(FctPlan* P, const FctFields* f, const double* gT_new, double dt,
   in.T_new = nullptr;
   in.tstride = f->tracer_stride ? f->tracer_stride : int64_t(P->N) * P->L;
   in.tg = 0;
+  in.wtg = ntr;
   in.Z3d = f->Z3d; in.zbar3 = f->zbar3; in.w_i = nullptr;
   in.ws = P->ws;
   in.dt = dt;
@@ -833,7 +834,7 @@ int fct_adjoint(FctPlan* P, const FctFields* f, const double* gT_new, double dt,
   LaunchDims d{};
   d.max_iface = P->hm.n_iface; d.max_layer = P->hm.n_layer; d.max_edge = P->hm.n_edge;
   d.max_elem = P->hm.n_elem; d.max_dense = int64_t(P->N) * P->L; d.max_nodes = P->N;
-  d.ntr = ntr; d.chunk = 8; d.any_wi = false; d.copy_dry = false;
+  d.ntr = ntr; d.chunk = 0; d.per_thread = 8; d.any_wi = false; d.copy_dry = false;
   int st = launch_forward_stages(in, d, s, /*through_factors=*/true);
   if (st) return restore(st);
   auto grid = [](int64_t lanes, int b) {

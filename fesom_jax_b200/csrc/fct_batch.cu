@@ -55,6 +55,7 @@ int fct_batch_create(const FctInstance* insts, int n, int64_t budget, FctBatch**
   if (n > 65535) return set_error(FCT_ERR_INVALID, "at most 65535 instances per batch");
   const int dev = insts[0].plan ? insts[0].plan->device : 0;
   std::vector<int64_t> ws_doubles(n);
+  std::vector<int> wchunk(n);
   for (int i = 0; i < n; ++i) {
     const FctInstance& q = insts[i];
     if (!q.plan) return set_error(FCT_ERR_INVALID, "instance %d: plan is NULL", i);
@@ -66,7 +67,13 @@ int fct_batch_create(const FctInstance* insts, int n, int64_t budget, FctBatch**
       return set_error(FCT_ERR_INVALID, "instance %d: a field pointer is NULL", i);
     if (!(q.dt > 0.0)) return set_error(FCT_ERR_INVALID, "instance %d: dt <= 0", i);
     const FctPlan* P = q.plan;
-    ws_doubles[i] = workspace_doubles(P->N, P->E, P->Ed, P->L, q.ntr);
+    // the workspace holds a chunk of the instance's tracers (stages run chunk by chunk):
+    // up to 8, halved until one instance fits the budget
+    int wc = q.ntr < 8 ? q.ntr : 8;
+    while (wc > 1 && workspace_doubles(P->N, P->E, P->Ed, P->L, wc) * int64_t(sizeof(double)) > budget)
+      wc = (wc + 1) / 2;
+    wchunk[i] = wc;
+    ws_doubles[i] = workspace_doubles(P->N, P->E, P->Ed, P->L, wc);
   }
   FctBatch* B = new FctBatch();
   B->device = dev;
@@ -76,7 +83,8 @@ int fct_batch_create(const FctInstance* insts, int n, int64_t budget, FctBatch**
   FctBatch::Group g;
   for (int i = 0; i < n; ++i) {
     const int64_t bytes = ws_doubles[i] * int64_t(sizeof(double));
-    if (g.count > 0 && (cur + bytes > budget || insts[i].ntr != insts[g.first].ntr)) {
+    if (g.count > 0 && (cur + bytes > budget || insts[i].ntr != insts[g.first].ntr ||
+                        wchunk[i] != wchunk[g.first])) {
       B->groups.push_back(g);
       g = FctBatch::Group();
       g.first = i;
@@ -106,7 +114,7 @@ int fct_batch_create(const FctInstance* insts, int n, int64_t budget, FctBatch**
     for (int i = gr.first; i < gr.first + gr.count; ++i) {
       const FctInstance& q = insts[i];
       const FctPlan* P = q.plan;
-      const Workspace ws = carve_workspace(B->arena + off, P->N, P->E, P->Ed, P->L, q.ntr);
+      const Workspace ws = carve_workspace(B->arena + off, P->N, P->E, P->Ed, P->L, wchunk[i]);
       off += ws_doubles[i];
       d.max_iface = std::max(d.max_iface, P->hm.n_iface);
       d.max_layer = std::max(d.max_layer, P->hm.n_layer);
@@ -115,6 +123,7 @@ int fct_batch_create(const FctInstance* insts, int n, int64_t budget, FctBatch**
       d.max_dense = std::max(d.max_dense, int64_t(P->N) * P->L);
       d.max_nodes = std::max(d.max_nodes, int64_t(P->N));
       d.ntr = q.ntr;
+      d.chunk = wchunk[i];
       B->total_updates += int64_t(q.ntr) * P->hm.n_layer;
       for (int p = 0; p < 3; ++p) {
         Inst& in = tab[size_t(p) * n + i];
@@ -126,6 +135,7 @@ int fct_batch_create(const FctInstance* insts, int n, int64_t budget, FctBatch**
         in.T_new = q.buf[(p + 2) % 3];
         in.tstride = 0;
         in.tg = q.ntr;   // interleaved [nod2D, nl, ntr]
+        in.wtg = wchunk[i];
         in.Z3d = in.zbar3 = in.w_i = nullptr;
         in.ws = ws;
         in.dt = q.dt;
@@ -134,7 +144,7 @@ int fct_batch_create(const FctInstance* insts, int n, int64_t budget, FctBatch**
     }
     d.any_wi = false;
     d.copy_dry = false;
-    d.chunk = 8;
+    d.per_thread = d.chunk < 8 ? d.chunk : 8;
     gr.dims = d;
   }
   e = cudaMalloc(&B->d_tables, tab.size() * sizeof(Inst));
@@ -168,18 +178,31 @@ int fct_batch_set_chunk(FctBatch* B, int chunk) {
   if (chunk != 1 && chunk != 2 && chunk != 4 && chunk != 8)
     return set_error(FCT_ERR_INVALID, "chunk must be 1, 2, 4 or 8");
   std::lock_guard<std::mutex> lk(B->graph_mu);
-  for (auto& g : B->groups) g.dims.chunk = chunk;
+  for (auto& g : B->groups) g.dims.per_thread = chunk;
   for (auto& kv : B->graphs) cudaGraphExecDestroy(kv.second);   // recapture with the new chunk
   B->graphs.clear();
   return FCT_OK;
 }
 
-int fct_batch_info(const FctBatch* B, int64_t out[4]) {
+int fct_batch_info(const FctBatch* B, int64_t out[6]) {
   if (!B || !out) return set_error(FCT_ERR_INVALID, "NULL argument");
   out[0] = int64_t(B->insts.size());
   out[1] = int64_t(B->groups.size());
   out[2] = B->arena_bytes;
   out[3] = B->total_updates;
+  int64_t wmax = 0, launches = 0;
+  for (const auto& g : B->groups) {
+    const int chunk = g.dims.chunk > 0 ? g.dims.chunk : g.dims.ntr;
+    wmax = std::max<int64_t>(wmax, chunk);
+    int64_t per_chunk_launches = 0;
+    for (int c0 = 0; c0 < g.dims.ntr; c0 += chunk) {
+      const int csz = std::min(chunk, g.dims.ntr - c0);
+      per_chunk_launches += (csz + g.dims.per_thread - 1) / g.dims.per_thread;
+    }
+    launches += 1 + int64_t(g.dims.any_wi ? 8 : 7) * per_chunk_launches;
+  }
+  out[4] = wmax;
+  out[5] = launches;
   return FCT_OK;
 }
 
@@ -257,21 +280,176 @@ int fct_batch_profile(FctBatch* B, int phase, double* stage_ms, int max_stages,
   for (int i = 0; i < kNumStages; ++i) stage_ms[i] = 0.0;
   int st = FCT_OK;
   for (auto& g : B->groups) {
-    Inst dummy{};
-    cudaEventRecord(ev[0], s);
-    st = launch_forward_events(dummy, g.d_tab[phase % 3], g.count, g.dims, s, ev + 1);
-    if (st) break;
-    cudaError_t e = cudaEventSynchronize(ev[kNumStages]);
-    if (e != cudaSuccess) { st = cuda_error(e, "profile synchronize"); break; }
-    for (int i = 0; i < kNumStages; ++i) {
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
-      stage_ms[i] += ms;
+    const int chunk = g.dims.chunk > 0 ? g.dims.chunk : g.dims.ntr;
+    const int nchunks = (g.dims.ntr + chunk - 1) / chunk;
+    for (int ci = 0; ci < nchunks && !st; ++ci) {
+      Inst dummy{};
+      cudaEventRecord(ev[0], s);
+      st = launch_forward_events(dummy, g.d_tab[phase % 3], g.count, g.dims, s, ev + 1, false, ci);
+      if (st) break;
+      cudaError_t e = cudaEventSynchronize(ev[kNumStages]);
+      if (e != cudaSuccess) { st = cuda_error(e, "profile synchronize"); break; }
+      for (int i = 0; i < kNumStages; ++i) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
+        stage_ms[i] += ms;
+      }
     }
+    if (st) break;
   }
   for (auto& e : ev) cudaEventDestroy(e);
   if (prev >= 0) cudaSetDevice(prev);
   return st;
+}
+
+}  // extern "C"
+
+struct FctServe {
+  int device = 0;
+  int max_instances = 0;
+  double* arena = nullptr;
+  int64_t arena_doubles = 0;
+  Inst* d_tab = nullptr;      // device instance table
+  Inst* h_tab = nullptr;      // pinned staging
+  cudaEvent_t uploaded = nullptr;
+  bool pending = false;       // an upload from h_tab may still be in flight
+};
+
+extern "C" {
+
+int fct_serve_create(int device, int max_instances, int64_t workspace_bytes, FctServe** out) {
+  if (!out || max_instances < 1 || workspace_bytes < 0)
+    return set_error(FCT_ERR_INVALID, "bad serve arguments");
+  *out = nullptr;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  FctServe* S = new FctServe();
+  S->device = device;
+  S->max_instances = max_instances;
+  S->arena_doubles = workspace_bytes / int64_t(sizeof(double));
+  auto fail = [&](cudaError_t e, const char* what) {
+    const int st = cuda_error(e, what);
+    fct_serve_destroy(S);
+    if (prev >= 0) cudaSetDevice(prev);
+    return st;
+  };
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return fail(e, "cudaSetDevice");
+  if (S->arena_doubles > 0 &&
+      (e = cudaMalloc(&S->arena, size_t(S->arena_doubles) * sizeof(double))) != cudaSuccess)
+    return fail(e, "serve workspace cudaMalloc");
+  if ((e = cudaMalloc(&S->d_tab, size_t(max_instances) * sizeof(Inst))) != cudaSuccess)
+    return fail(e, "serve table cudaMalloc");
+  if ((e = cudaMallocHost(&S->h_tab, size_t(max_instances) * sizeof(Inst))) != cudaSuccess)
+    return fail(e, "serve staging cudaMallocHost");
+  if ((e = cudaEventCreateWithFlags(&S->uploaded, cudaEventDisableTiming)) != cudaSuccess)
+    return fail(e, "cudaEventCreate");
+  if (prev >= 0) cudaSetDevice(prev);
+  *out = S;
+  return FCT_OK;
+}
+
+int fct_serve_destroy(FctServe* S) {
+  if (!S) return FCT_OK;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(S->device);
+  if (S->uploaded) {
+    cudaEventSynchronize(S->uploaded);
+    cudaEventDestroy(S->uploaded);
+  }
+  if (S->h_tab) cudaFreeHost(S->h_tab);
+  if (S->d_tab) cudaFree(S->d_tab);
+  if (S->arena) cudaFree(S->arena);
+  if (prev >= 0) cudaSetDevice(prev);
+  delete S;
+  return FCT_OK;
+}
+
+int fct_serve_step(FctServe* S, const FctInstance* insts, const int32_t* phases, int n,
+                   fct_stream_t stream) {
+  if (!S || (n > 0 && (!insts || !phases))) return set_error(FCT_ERR_INVALID, "NULL argument");
+  if (n < 0 || n > S->max_instances)
+    return set_error(FCT_ERR_CAPACITY, "%d instances exceed the serve table (%d)", n,
+                     S->max_instances);
+  if (n == 0) return FCT_OK;
+  // order instances by ntr so that each launch group has one ntr
+  std::vector<int> order(n);
+  for (int i = 0; i < n; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return insts[a].ntr < insts[b].ntr; });
+  int64_t need = 0;
+  for (int i = 0; i < n; ++i) {
+    const FctInstance& q = insts[i];
+    if (!q.plan || q.plan->device != S->device || q.ntr < 1 || !q.buf[0] || !q.buf[1] ||
+        !q.buf[2] || !q.uv || !q.w_e || !q.helem || !q.hnode || !q.hnode_new || !(q.dt > 0.0))
+      return set_error(FCT_ERR_INVALID, "instance %d is invalid", i);
+    need += workspace_doubles(q.plan->N, q.plan->E, q.plan->Ed, q.plan->L, q.ntr);
+  }
+  if (need > S->arena_doubles)
+    return set_error(FCT_ERR_CAPACITY, "instances need %lld workspace doubles, arena holds %lld",
+                     (long long)need, (long long)S->arena_doubles);
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(S->device);
+  auto restore = [&](int st) { if (prev >= 0) cudaSetDevice(prev); return st; };
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (S->pending) {   // the previous call's upload must have left the staging buffer
+    cudaError_t e = cudaEventSynchronize(S->uploaded);
+    if (e != cudaSuccess) return restore(cuda_error(e, "serve staging wait"));
+  }
+  int64_t off = 0;
+  for (int j = 0; j < n; ++j) {
+    const FctInstance& q = insts[order[j]];
+    const FctPlan* P = q.plan;
+    const int p = ((phases[order[j]] % 3) + 3) % 3;
+    Inst& in = S->h_tab[j];
+    in = Inst{};
+    in.m = P->d_mesh;
+    in.uv = q.uv; in.w_e = q.w_e; in.helem = q.helem;
+    in.hnode = q.hnode; in.hnode_new = q.hnode_new;
+    in.T_old = q.buf[p];
+    in.T = q.buf[(p + 1) % 3];
+    in.T_new = q.buf[(p + 2) % 3];
+    in.tstride = 0;
+    in.tg = q.ntr;
+    in.wtg = q.ntr;
+    in.ws = carve_workspace(S->arena + off, P->N, P->E, P->Ed, P->L, q.ntr);
+    off += workspace_doubles(P->N, P->E, P->Ed, P->L, q.ntr);
+    in.dt = q.dt;
+    in.ntr = q.ntr;
+  }
+  cudaError_t e = cudaMemcpyAsync(S->d_tab, S->h_tab, size_t(n) * sizeof(Inst),
+                                  cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return restore(cuda_error(e, "serve table upload"));
+  e = cudaEventRecord(S->uploaded, s);
+  if (e != cudaSuccess) return restore(cuda_error(e, "serve event record"));
+  S->pending = true;
+  for (int j0 = 0; j0 < n;) {
+    int j1 = j0;
+    LaunchDims d{};
+    const int ntr = insts[order[j0]].ntr;
+    while (j1 < n && insts[order[j1]].ntr == ntr) {
+      const FctPlan* P = insts[order[j1]].plan;
+      d.max_iface = std::max(d.max_iface, P->hm.n_iface);
+      d.max_layer = std::max(d.max_layer, P->hm.n_layer);
+      d.max_edge = std::max(d.max_edge, P->hm.n_edge);
+      d.max_elem = std::max(d.max_elem, P->hm.n_elem);
+      d.max_dense = std::max(d.max_dense, int64_t(P->N) * P->L);
+      d.max_nodes = std::max(d.max_nodes, int64_t(P->N));
+      ++j1;
+    }
+    d.ntr = ntr;
+    d.chunk = 0;
+    d.per_thread = ntr >= 4 ? 4 : ntr;
+    d.any_wi = false;
+    d.copy_dry = false;
+    Inst dummy{};
+    const int st = launch_forward(dummy, S->d_tab + j0, j1 - j0, d, s);
+    if (st) return restore(st);
+    j0 = j1;
+  }
+  return restore(FCT_OK);
 }
 
 const char* fct_stage_name(int i) {

@@ -105,7 +105,7 @@ __device__ __forceinline__ void body_vflux(const Inst& in, int64_t i) {
 
 // ---------------------------------------------------- tracer_gradient_elements
 template <int NTR, bool IL>
-__device__ __forceinline__ void body_elem_grad(const Inst& in, int64_t i, int t0) {
+__device__ __forceinline__ void body_elem_grad(const Inst& in, int64_t i, int t0, int w0) {
   const DevMesh& m = *in.m;
   if (i >= m.n_elem) return;
   const uint32_t lane = ld(m.elem_lanes + i);
@@ -124,8 +124,8 @@ __device__ __forceinline__ void body_elem_grad(const Inst& in, int64_t i, int t0
     gy[t] = g3 * a0[t] + g4 * a1[t] + g5 * a2[t];
   }
   const int64_t q = int64_t(e) * L + k;
-  stn<NTR, IL>(in.ws.gx, q, t0, in.ws.sE, in.tg, gx);
-  stn<NTR, IL>(in.ws.gy, q, t0, in.ws.sE, in.tg, gy);
+  stn<NTR, IL>(in.ws.gx, q, w0, in.ws.sE, in.wtg, gx);
+  stn<NTR, IL>(in.ws.gy, q, w0, in.ws.sE, in.wtg, gy);
 }
 
 // Upwind vertical flux at interface j (layer-masked), tracer_adv.py:108-120, given the
@@ -137,7 +137,7 @@ __device__ __forceinline__ double vflux_up(double Tb, double Ta, double w, doubl
 
 // -------------------------------- LO solution, node-average gradient, adf_v
 template <int NTR, bool IL>
-__device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i, int t0) {
+__device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i, int t0, int w0) {
   const DevMesh& m = *in.m;
   if (i >= m.n_iface) return;
   const uint32_t lane = ld(m.iface_lanes + i);
@@ -200,7 +200,7 @@ __device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i, int t0) 
 #pragma unroll
     for (int t = 0; t < NTR; ++t)
       lo[t] = valid ? (Tc[t] * hn + (div[t] + (fvk[t] - fvk1[t])) * dt / av) / hnn : 0.0;
-    stn<NTR, IL>(in.ws.lo, qn, t0, in.ws.sN, tg, lo);
+    stn<NTR, IL>(in.ws.lo, qn, w0, in.ws.sN, in.wtg, lo);
     // _node_avg_grad: area-weighted mean over the node's active elements
     double nx[NTR], ny[NTR], den = 0.0;
 #pragma unroll
@@ -212,8 +212,8 @@ __device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i, int t0) 
         const double a = ld(m.earea + el);
         const int64_t qe = int64_t(el) * L + k;
         double gx[NTR], gy[NTR];
-        ldn<NTR, IL>(in.ws.gx, qe, t0, in.ws.sE, tg, gx);
-        ldn<NTR, IL>(in.ws.gy, qe, t0, in.ws.sE, tg, gy);
+        ldn<NTR, IL>(in.ws.gx, qe, w0, in.ws.sE, in.wtg, gx);
+        ldn<NTR, IL>(in.ws.gy, qe, w0, in.ws.sE, in.wtg, gy);
 #pragma unroll
         for (int t = 0; t < NTR; ++t) {
           nx[t] += gx[t] * a;
@@ -228,8 +228,8 @@ __device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i, int t0) 
       nx[t] = nx[t] / dd;
       ny[t] = ny[t] / dd;
     }
-    stn<NTR, IL>(in.ws.gnx, qn, t0, in.ws.sN, tg, nx);
-    stn<NTR, IL>(in.ws.gny, qn, t0, in.ws.sN, tg, ny);
+    stn<NTR, IL>(in.ws.gnx, qn, w0, in.ws.sN, in.wtg, nx);
+    stn<NTR, IL>(in.ws.gny, qn, w0, in.ws.sN, in.wtg, ny);
   }
 
   // adv_flux_ver_ho (QR4C on ttfAB) minus the LO vertical flux (tracer_adv.py:241-295)
@@ -286,12 +286,12 @@ __device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i, int t0) 
     const double lo_v = in.w_i ? (layer ? vflux_up(Tc[t], Ta[t], Wf, area_k) : 0.0) : fvk[t];
     adf[t] = hi[t] - lo_v;
   }
-  stn<NTR, IL>(in.ws.adfv, qn, t0, in.ws.sN, tg, adf);
+  stn<NTR, IL>(in.ws.adfv, qn, w0, in.ws.sN, in.wtg, adf);
 }
 
 // ---------------------------- adv_tra_vert_impl: implicit w_i advection of LO
 template <int NTR, bool IL>
-__device__ __forceinline__ void body_vert_impl(const Inst& in, int64_t n, int t0) {
+__device__ __forceinline__ void body_vert_impl(const Inst& in, int64_t n, int t0, int w0) {
   const DevMesh& m = *in.m;
   if (n >= m.N || !in.w_i) return;
   const int L = m.L;
@@ -300,8 +300,8 @@ __device__ __forceinline__ void body_vert_impl(const Inst& in, int64_t n, int t0
   const int64_t base = n * L;
   const double dt = in.dt;
   double cp[kMaxLevels], dp[kMaxLevels];
-  for (int t = t0; t < t0 + NTR; ++t) {
-    auto LO = [&](int k) -> double& { return in.ws.lo[tix<IL>(base + k, t, in.ws.sN, in.tg)]; };
+  for (int tw = w0; tw < w0 + NTR; ++tw) {
+    auto LO = [&](int k) -> double& { return in.ws.lo[tix<IL>(base + k, tw, in.ws.sN, in.wtg)]; };
     double cprev = 0.0, dprev = 0.0;
     for (int k = nzmin; k < nzmax; ++k) {
       const double av = m.areasvol[base + k];
@@ -336,7 +336,7 @@ __device__ __forceinline__ void body_vert_impl(const Inst& in, int64_t n, int t0
 
 // -------------------------- fill_up_dn_grad + adv_flux_hor_ho - LO flux = adf_h
 template <int NTR, bool IL>
-__device__ __forceinline__ void body_edge_adf(const Inst& in, int64_t i, int t0) {
+__device__ __forceinline__ void body_edge_adf(const Inst& in, int64_t i, int t0, int w0) {
   const DevMesh& m = *in.m;
   if (i >= m.n_edge) return;
   const uint32_t lane = ld(m.edge_lanes + i);
@@ -359,15 +359,15 @@ __device__ __forceinline__ void body_edge_adf(const Inst& in, int64_t i, int t0)
   ldn<NTR, IL>(in.T_old, q2, t0, ts, tg, O2);
   if (use_tri) {
     const int64_t qu = int64_t(up) * L + k, qd = int64_t(dn) * L + k;
-    ldn<NTR, IL>(in.ws.gx, qu, t0, in.ws.sE, tg, g0);
-    ldn<NTR, IL>(in.ws.gx, qd, t0, in.ws.sE, tg, g1);
-    ldn<NTR, IL>(in.ws.gy, qu, t0, in.ws.sE, tg, g2);
-    ldn<NTR, IL>(in.ws.gy, qd, t0, in.ws.sE, tg, g3);
+    ldn<NTR, IL>(in.ws.gx, qu, w0, in.ws.sE, in.wtg, g0);
+    ldn<NTR, IL>(in.ws.gx, qd, w0, in.ws.sE, in.wtg, g1);
+    ldn<NTR, IL>(in.ws.gy, qu, w0, in.ws.sE, in.wtg, g2);
+    ldn<NTR, IL>(in.ws.gy, qd, w0, in.ws.sE, in.wtg, g3);
   } else {
-    ldn<NTR, IL>(in.ws.gnx, q1, t0, in.ws.sN, tg, g0);
-    ldn<NTR, IL>(in.ws.gnx, q2, t0, in.ws.sN, tg, g1);
-    ldn<NTR, IL>(in.ws.gny, q1, t0, in.ws.sN, tg, g2);
-    ldn<NTR, IL>(in.ws.gny, q2, t0, in.ws.sN, tg, g3);
+    ldn<NTR, IL>(in.ws.gnx, q1, w0, in.ws.sN, in.wtg, g0);
+    ldn<NTR, IL>(in.ws.gnx, q2, w0, in.ws.sN, in.wtg, g1);
+    ldn<NTR, IL>(in.ws.gny, q1, w0, in.ws.sN, in.wtg, g2);
+    ldn<NTR, IL>(in.ws.gny, q2, w0, in.ws.sN, in.wtg, g3);
   }
   double adf[NTR];
 #pragma unroll
@@ -380,12 +380,12 @@ __device__ __forceinline__ void body_edge_adf(const Inst& in, int64_t i, int t0)
     const double ho = -0.5 * ((vf + avf) * Tm1 + (vf - avf) * Tm2);
     adf[t] = ho - fl;
   }
-  stn<NTR, IL>(in.ws.adfh, int64_t(e) * L + k, t0, in.ws.sEd, tg, adf);
+  stn<NTR, IL>(in.ws.adfh, int64_t(e) * L + k, w0, in.ws.sEd, in.wtg, adf);
 }
 
 // ------------------------ zalesak a2: element max/min of the LO/T window
 template <int NTR, bool IL>
-__device__ __forceinline__ void body_elem_bounds(const Inst& in, int64_t i, int t0) {
+__device__ __forceinline__ void body_elem_bounds(const Inst& in, int64_t i, int t0, int w0) {
   const DevMesh& m = *in.m;
   if (i >= m.n_elem) return;
   const uint32_t lane = ld(m.elem_lanes + i);
@@ -399,7 +399,7 @@ __device__ __forceinline__ void body_elem_bounds(const Inst& in, int64_t i, int 
 #pragma unroll
   for (int v = 0; v < 3; ++v) {
     double a[NTR], b[NTR];
-    ldn<NTR, IL>(in.ws.lo, q[v], t0, in.ws.sN, in.tg, a);
+    ldn<NTR, IL>(in.ws.lo, q[v], w0, in.ws.sN, in.wtg, a);
     ldn<NTR, IL>(in.T, q[v], t0, in.tstride, in.tg, b);
 #pragma unroll
     for (int t = 0; t < NTR; ++t) {
@@ -408,13 +408,13 @@ __device__ __forceinline__ void body_elem_bounds(const Inst& in, int64_t i, int 
     }
   }
   const int64_t qe = int64_t(e) * L + k;
-  stn<NTR, IL>(in.ws.amax, qe, t0, in.ws.sE, in.tg, mx);
-  stn<NTR, IL>(in.ws.amin, qe, t0, in.ws.sE, in.tg, mn);
+  stn<NTR, IL>(in.ws.amax, qe, w0, in.ws.sE, in.wtg, mx);
+  stn<NTR, IL>(in.ws.amin, qe, w0, in.ws.sE, in.wtg, mn);
 }
 
 // ------------------------ zalesak a3: node cluster max/min over elements
 template <int NTR, bool IL>
-__device__ __forceinline__ void body_node_cluster(const Inst& in, int64_t i, int t0) {
+__device__ __forceinline__ void body_node_cluster(const Inst& in, int64_t i, int t0, int w0) {
   const DevMesh& m = *in.m;
   if (i >= m.n_layer) return;
   const uint32_t lane = ld(m.layer_lanes + i);
@@ -428,8 +428,8 @@ __device__ __forceinline__ void body_node_cluster(const Inst& in, int64_t i, int
     if (k >= ld(m.eul + el) && k < ld(m.enl + el)) {
       const int64_t q = int64_t(el) * L + k;
       double a[NTR], b[NTR];
-      ldn<NTR, IL>(in.ws.amax, q, t0, in.ws.sE, in.tg, a);
-      ldn<NTR, IL>(in.ws.amin, q, t0, in.ws.sE, in.tg, b);
+      ldn<NTR, IL>(in.ws.amax, q, w0, in.ws.sE, in.wtg, a);
+      ldn<NTR, IL>(in.ws.amin, q, w0, in.ws.sE, in.wtg, b);
 #pragma unroll
       for (int t = 0; t < NTR; ++t) {
         mx[t] = fmax(mx[t], a[t]);
@@ -444,13 +444,13 @@ __device__ __forceinline__ void body_node_cluster(const Inst& in, int64_t i, int
     }
   }
   const int64_t qn = int64_t(n) * L + k;
-  stn<NTR, IL>(in.ws.tvmax, qn, t0, in.ws.sN, in.tg, mx);
-  stn<NTR, IL>(in.ws.tvmin, qn, t0, in.ws.sN, in.tg, mn);
+  stn<NTR, IL>(in.ws.tvmax, qn, w0, in.ws.sN, in.wtg, mx);
+  stn<NTR, IL>(in.ws.tvmin, qn, w0, in.ws.sN, in.wtg, mn);
 }
 
 // ------------------- zalesak a4 + b1 + b2: admissible window, sums, factors
 template <int NTR, bool IL>
-__device__ __forceinline__ void body_node_factors(const Inst& in, int64_t i, int t0) {
+__device__ __forceinline__ void body_node_factors(const Inst& in, int64_t i, int t0, int w0) {
   const DevMesh& m = *in.m;
   if (i >= m.n_layer) return;
   const uint32_t lane = ld(m.layer_lanes + i);
@@ -462,17 +462,16 @@ __device__ __forceinline__ void body_node_factors(const Inst& in, int64_t i, int
   const bool valid = (av > 0.0) && (hnn > 0.0);
   const double sa = av > 0.0 ? av : 1.0, sh = hnn > 0.0 ? hnn : 1.0;
   const double dt = in.dt;
-  const int tg = in.tg;
   const int64_t sN = in.ws.sN;
   double tmax[NTR], tmin[NTR];
-  ldn<NTR, IL>(in.ws.tvmax, qn, t0, sN, tg, tmax);
-  ldn<NTR, IL>(in.ws.tvmin, qn, t0, sN, tg, tmin);
+  ldn<NTR, IL>(in.ws.tvmax, qn, w0, sN, in.wtg, tmax);
+  ldn<NTR, IL>(in.ws.tvmin, qn, w0, sN, in.wtg, tmin);
   if (!use_own) {   // interior: max/min over k-1, k, k+1 (all layers of this column)
     double am[NTR], an[NTR], bm[NTR], bn[NTR];
-    ldn<NTR, IL>(in.ws.tvmax, qn - 1, t0, sN, tg, am);
-    ldn<NTR, IL>(in.ws.tvmin, qn - 1, t0, sN, tg, an);
-    ldn<NTR, IL>(in.ws.tvmax, qn + 1, t0, sN, tg, bm);
-    ldn<NTR, IL>(in.ws.tvmin, qn + 1, t0, sN, tg, bn);
+    ldn<NTR, IL>(in.ws.tvmax, qn - 1, w0, sN, in.wtg, am);
+    ldn<NTR, IL>(in.ws.tvmin, qn - 1, w0, sN, in.wtg, an);
+    ldn<NTR, IL>(in.ws.tvmax, qn + 1, w0, sN, in.wtg, bm);
+    ldn<NTR, IL>(in.ws.tvmin, qn + 1, w0, sN, in.wtg, bn);
 #pragma unroll
     for (int t = 0; t < NTR; ++t) {
       tmax[t] = fmax(fmax(am[t], tmax[t]), bm[t]);
@@ -480,9 +479,9 @@ __device__ __forceinline__ void body_node_factors(const Inst& in, int64_t i, int
     }
   }
   double lo[NTR], ft[NTR], fb[NTR];
-  ldn<NTR, IL>(in.ws.lo, qn, t0, sN, tg, lo);
-  ldn<NTR, IL>(in.ws.adfv, qn, t0, sN, tg, ft);
-  ldn<NTR, IL>(in.ws.adfv, qn + 1, t0, sN, tg, fb);   // k+1 <= nzmax < L
+  ldn<NTR, IL>(in.ws.lo, qn, w0, sN, in.wtg, lo);
+  ldn<NTR, IL>(in.ws.adfv, qn, w0, sN, in.wtg, ft);
+  ldn<NTR, IL>(in.ws.adfv, qn + 1, w0, sN, in.wtg, fb);   // k+1 <= nzmax < L
   double sp[NTR], sm[NTR];
 #pragma unroll
   for (int t = 0; t < NTR; ++t) sp[t] = sm[t] = 0.0;
@@ -491,7 +490,7 @@ __device__ __forceinline__ void body_node_factors(const Inst& in, int64_t i, int
     const int idx = ld(m.ne_idx + j), e = idx >> 1;
     if (k < ld(m.ekmin + e) || k >= ld(m.ekmax + e)) continue;   // no flux on this level
     double a[NTR];
-    ldn<NTR, IL>(in.ws.adfh, int64_t(e) * L + k, t0, in.ws.sEd, tg, a);
+    ldn<NTR, IL>(in.ws.adfh, int64_t(e) * L + k, w0, in.ws.sEd, in.wtg, a);
 #pragma unroll
     for (int t = 0; t < NTR; ++t) {
       const double s = (idx & 1) ? -a[t] : a[t];
@@ -513,13 +512,13 @@ __device__ __forceinline__ void body_node_factors(const Inst& in, int64_t i, int
       mf[t] = fmin(1.0, (tmin[t] - lo[t]) / flux_neg);
     }
   }
-  stn<NTR, IL>(in.ws.pf, qn, t0, sN, tg, pf);
-  stn<NTR, IL>(in.ws.mf, qn, t0, sN, tg, mf);
+  stn<NTR, IL>(in.ws.pf, qn, w0, sN, in.wtg, pf);
+  stn<NTR, IL>(in.ws.mf, qn, w0, sN, in.wtg, mf);
 }
 
 // ---------- zalesak b3 + flux2dtracer_fct + ale_reconstruct: T_new on layers
 template <int NTR, bool IL>
-__device__ __forceinline__ void body_node_final(const Inst& in, int64_t i, int t0) {
+__device__ __forceinline__ void body_node_final(const Inst& in, int64_t i, int t0, int w0) {
   const DevMesh& m = *in.m;
   if (i >= m.n_layer) return;
   const uint32_t lane = ld(m.layer_lanes + i);
@@ -534,9 +533,9 @@ __device__ __forceinline__ void body_node_final(const Inst& in, int64_t i, int t
   const int64_t sN = in.ws.sN;
   // own limiter factors at k (and k-1 / k+1 for the vertical fluxes)
   double pf0[NTR], mf0[NTR], ft[NTR];
-  ldn<NTR, IL>(in.ws.pf, qn, t0, sN, tg, pf0);
-  ldn<NTR, IL>(in.ws.mf, qn, t0, sN, tg, mf0);
-  ldn<NTR, IL>(in.ws.adfv, qn, t0, sN, tg, ft);
+  ldn<NTR, IL>(in.ws.pf, qn, w0, sN, in.wtg, pf0);
+  ldn<NTR, IL>(in.ws.mf, qn, w0, sN, in.wtg, mf0);
+  ldn<NTR, IL>(in.ws.adfv, qn, w0, sN, in.wtg, ft);
   // limited vertical flux at the top interface k (tracer_adv.py:453-459)
   double vt[NTR];
   if (k == nzmin) {
@@ -544,8 +543,8 @@ __device__ __forceinline__ void body_node_final(const Inst& in, int64_t i, int t
     for (int t = 0; t < NTR; ++t) vt[t] = (ft[t] >= 0.0 ? pf0[t] : mf0[t]) * ft[t];
   } else {
     double pfa[NTR], mfa[NTR];
-    ldn<NTR, IL>(in.ws.pf, qn - 1, t0, sN, tg, pfa);
-    ldn<NTR, IL>(in.ws.mf, qn - 1, t0, sN, tg, mfa);
+    ldn<NTR, IL>(in.ws.pf, qn - 1, w0, sN, in.wtg, pfa);
+    ldn<NTR, IL>(in.ws.mf, qn - 1, w0, sN, in.wtg, mfa);
 #pragma unroll
     for (int t = 0; t < NTR; ++t)
       vt[t] = (ft[t] >= 0.0 ? fmin(mfa[t], pf0[t]) : fmin(pfa[t], mf0[t])) * ft[t];
@@ -557,9 +556,9 @@ __device__ __forceinline__ void body_node_final(const Inst& in, int64_t i, int t
     for (int t = 0; t < NTR; ++t) vb[t] = 0.0;
   } else {
     double fb[NTR], pfb[NTR], mfb[NTR];
-    ldn<NTR, IL>(in.ws.adfv, qn + 1, t0, sN, tg, fb);
-    ldn<NTR, IL>(in.ws.pf, qn + 1, t0, sN, tg, pfb);
-    ldn<NTR, IL>(in.ws.mf, qn + 1, t0, sN, tg, mfb);
+    ldn<NTR, IL>(in.ws.adfv, qn + 1, w0, sN, in.wtg, fb);
+    ldn<NTR, IL>(in.ws.pf, qn + 1, w0, sN, in.wtg, pfb);
+    ldn<NTR, IL>(in.ws.mf, qn + 1, w0, sN, in.wtg, mfb);
 #pragma unroll
     for (int t = 0; t < NTR; ++t)
       vb[t] = (fb[t] >= 0.0 ? fmin(mf0[t], pfb[t]) : fmin(pf0[t], mfb[t])) * fb[t];
@@ -574,9 +573,9 @@ __device__ __forceinline__ void body_node_final(const Inst& in, int64_t i, int t
     if (k < ld(m.ekmin + e) || k >= ld(m.ekmax + e)) continue;   // no flux on this level
     const int64_t qo = int64_t(ld(m.ne_oth + j)) * L + k;
     double a[NTR], pfo[NTR], mfo[NTR];
-    ldn<NTR, IL>(in.ws.adfh, int64_t(e) * L + k, t0, in.ws.sEd, tg, a);
-    ldn<NTR, IL>(in.ws.pf, qo, t0, sN, tg, pfo);
-    ldn<NTR, IL>(in.ws.mf, qo, t0, sN, tg, mfo);
+    ldn<NTR, IL>(in.ws.adfh, int64_t(e) * L + k, w0, in.ws.sEd, in.wtg, a);
+    ldn<NTR, IL>(in.ws.pf, qo, w0, sN, in.wtg, pfo);
+    ldn<NTR, IL>(in.ws.mf, qo, w0, sN, in.wtg, mfo);
 #pragma unroll
     for (int t = 0; t < NTR; ++t) {
       // (pf, mf) at the edge's first node n1 and second node n2
@@ -589,7 +588,7 @@ __device__ __forceinline__ void body_node_final(const Inst& in, int64_t i, int t
   }
   double Tv[NTR], lo[NTR], out[NTR];
   ldn<NTR, IL>(in.T, qn, t0, in.tstride, tg, Tv);
-  ldn<NTR, IL>(in.ws.lo, qn, t0, sN, tg, lo);
+  ldn<NTR, IL>(in.ws.lo, qn, w0, sN, in.wtg, lo);
 #pragma unroll
   for (int t = 0; t < NTR; ++t) {
     const double lo_trans = -Tv[t] * hn + lo[t] * hnn;
@@ -620,12 +619,13 @@ __device__ __forceinline__ void body_copy_dry(const Inst& in, int64_t i) {
 // layout, the batched path).
 #define FCT_KERNEL_T(name, body)                                                        \
   template <int NTR>                                                                    \
-  __global__ void __launch_bounds__(256) name##_1(Inst in, int t0) {                    \
-    body<NTR, false>(in, lane_index(), t0);                                             \
+  __global__ void __launch_bounds__(256) name##_1(Inst in, int t0, int w0) {            \
+    body<NTR, false>(in, lane_index(), t0, w0);                                         \
   }                                                                                     \
   template <int NTR>                                                                    \
-  __global__ void __launch_bounds__(256) name##_n(const Inst* __restrict__ tab, int t0) { \
-    body<NTR, true>(tab[blockIdx.y], lane_index(), t0);                                 \
+  __global__ void __launch_bounds__(256) name##_n(const Inst* __restrict__ tab, int t0,  \
+                                                  int w0) {                             \
+    body<NTR, true>(tab[blockIdx.y], lane_index(), t0, w0);                             \
   }
 
 FCT_KERNEL_T(k_elem_grad, body_elem_grad)
@@ -654,72 +654,80 @@ const char* const kStageNames[kNumStages] = {
     "vflux", "elem_grad", "node_lo", "vert_impl", "edge_adf", "elem_bounds",
     "node_cluster", "node_factors", "node_final", "copy_dry"};
 
-// One stage over all tracer chunks (NTR in {8, 4, 2, 1}, largest first, at most
-// d.chunk tracers per thread).
+// One stage over the tracers [c0, c1) of a workspace chunk, split into launches of
+// NTR in {8, 4, 2, 1} tracers per thread (largest first, at most d.per_thread); the
+// workspace index of tracer t is t - c0.
 #define FCT_STAGE(name, lanes)                                                          \
   do {                                                                                  \
     const dim3 g = grid(lanes);                                                         \
-    for (int t0 = 0; t0 < d.ntr;) {                                                     \
-      const int rem = std::min(d.ntr - t0, d.chunk);                                    \
+    for (int t0 = c0; t0 < c1;) {                                                       \
+      const int rem = std::min(c1 - t0, d.per_thread);                                  \
+      const int w0 = t0 - c0;                                                           \
       if (rem >= 8) {                                                                   \
-        if (tab) name##_n<8><<<g, B, 0, s>>>(tab, t0);                                  \
-        else name##_1<8><<<g, B, 0, s>>>(single, t0);                                   \
+        if (tab) name##_n<8><<<g, B, 0, s>>>(tab, t0, w0);                              \
+        else name##_1<8><<<g, B, 0, s>>>(single, t0, w0);                               \
         t0 += 8;                                                                        \
       } else if (rem >= 4) {                                                            \
-        if (tab) name##_n<4><<<g, B, 0, s>>>(tab, t0);                                  \
-        else name##_1<4><<<g, B, 0, s>>>(single, t0);                                   \
+        if (tab) name##_n<4><<<g, B, 0, s>>>(tab, t0, w0);                              \
+        else name##_1<4><<<g, B, 0, s>>>(single, t0, w0);                               \
         t0 += 4;                                                                        \
       } else if (rem >= 2) {                                                            \
-        if (tab) name##_n<2><<<g, B, 0, s>>>(tab, t0);                                  \
-        else name##_1<2><<<g, B, 0, s>>>(single, t0);                                   \
+        if (tab) name##_n<2><<<g, B, 0, s>>>(tab, t0, w0);                              \
+        else name##_1<2><<<g, B, 0, s>>>(single, t0, w0);                               \
         t0 += 2;                                                                        \
       } else {                                                                          \
-        if (tab) name##_n<1><<<g, B, 0, s>>>(tab, t0);                                  \
-        else name##_1<1><<<g, B, 0, s>>>(single, t0);                                   \
+        if (tab) name##_n<1><<<g, B, 0, s>>>(tab, t0, w0);                              \
+        else name##_1<1><<<g, B, 0, s>>>(single, t0, w0);                               \
         t0 += 1;                                                                        \
       }                                                                                 \
     }                                                                                   \
   } while (0)
 
 int launch_forward_events(const Inst& single, const Inst* tab, int n, const LaunchDims& d,
-                          cudaStream_t s, cudaEvent_t* after, bool stop_before_final) {
+                          cudaStream_t s, cudaEvent_t* after, bool stop_before_final,
+                          int chunk_sel) {
   constexpr int B = 256;
   auto grid = [&](int64_t lanes) {
     return dim3(unsigned(std::max<int64_t>(1, (lanes + B - 1) / B)), unsigned(n), 1);
   };
-  int stage = 0;
-  auto mark = [&]() {
-    if (after) cudaEventRecord(after[stage], s);
-    ++stage;
-  };
-  if (tab) k_vflux_n<<<grid(d.max_edge), B, 0, s>>>(tab);
-  else k_vflux_1<<<grid(d.max_edge), B, 0, s>>>(single);
-  mark();
-  FCT_STAGE(k_elem_grad, d.max_elem);
-  mark();
-  FCT_STAGE(k_node_lo, d.max_iface);
-  mark();
-  if (d.any_wi) FCT_STAGE(k_vert_impl, d.max_nodes);
-  mark();
-  FCT_STAGE(k_edge_adf, d.max_edge);
-  mark();
-  FCT_STAGE(k_elem_bounds, d.max_elem);
-  mark();
-  FCT_STAGE(k_node_cluster, d.max_layer);
-  mark();
-  FCT_STAGE(k_node_factors, d.max_layer);
-  mark();
-  if (stop_before_final) {
-    const cudaError_t e = cudaGetLastError();
-    return e == cudaSuccess ? FCT_OK : cuda_error(e, "forward kernel launch");
+  const int chunk = d.chunk > 0 ? d.chunk : d.ntr;
+  const int nchunks = (d.ntr + chunk - 1) / chunk;
+  for (int ci = 0; ci < nchunks; ++ci) {
+    if (chunk_sel >= 0 && ci != chunk_sel) continue;
+    const int c0 = ci * chunk, c1 = std::min(d.ntr, c0 + chunk);
+    int stage = 0;
+    auto mark = [&]() {
+      if (after) cudaEventRecord(after[stage], s);
+      ++stage;
+    };
+    if (ci == 0) {   // the volume flux is shared by all tracers
+      if (tab) k_vflux_n<<<grid(d.max_edge), B, 0, s>>>(tab);
+      else k_vflux_1<<<grid(d.max_edge), B, 0, s>>>(single);
+    }
+    mark();
+    FCT_STAGE(k_elem_grad, d.max_elem);
+    mark();
+    FCT_STAGE(k_node_lo, d.max_iface);
+    mark();
+    if (d.any_wi) FCT_STAGE(k_vert_impl, d.max_nodes);
+    mark();
+    FCT_STAGE(k_edge_adf, d.max_edge);
+    mark();
+    FCT_STAGE(k_elem_bounds, d.max_elem);
+    mark();
+    FCT_STAGE(k_node_cluster, d.max_layer);
+    mark();
+    FCT_STAGE(k_node_factors, d.max_layer);
+    mark();
+    if (stop_before_final) continue;
+    FCT_STAGE(k_node_final, d.max_layer);
+    mark();
   }
-  FCT_STAGE(k_node_final, d.max_layer);
-  mark();
-  if (d.copy_dry) {
+  if (d.copy_dry && !stop_before_final && (chunk_sel < 0 || chunk_sel == nchunks - 1)) {
     if (tab) k_copy_dry_n<<<grid(d.max_dense), B, 0, s>>>(tab);
     else k_copy_dry_1<<<grid(d.max_dense), B, 0, s>>>(single);
   }
-  mark();
+  if (after) cudaEventRecord(after[kNumStages - 1], s);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_error(e, "forward kernel launch");
   return FCT_OK;
@@ -727,12 +735,12 @@ int launch_forward_events(const Inst& single, const Inst* tab, int n, const Laun
 
 int launch_forward(const Inst& single, const Inst* tab, int n, const LaunchDims& d,
                    cudaStream_t s) {
-  return launch_forward_events(single, tab, n, d, s, nullptr, false);
+  return launch_forward_events(single, tab, n, d, s, nullptr, false, -1);
 }
 
 int launch_forward_stages(const Inst& single, const LaunchDims& d, cudaStream_t s,
                           bool through_factors) {
-  return launch_forward_events(single, nullptr, 1, d, s, nullptr, through_factors);
+  return launch_forward_events(single, nullptr, 1, d, s, nullptr, through_factors, -1);
 }
 
 int launch_copy_dry(const Inst* tab, int n, int64_t max_dense, cudaStream_t s) {

@@ -29,18 +29,22 @@ inline int cuda_error(cudaError_t e, const char* what) {
 // whose lane counts are bounded by the ``max_*`` arguments.
 struct LaunchDims {
   int64_t max_iface, max_layer, max_edge, max_elem, max_dense, max_nodes;
-  int ntr;         // tracers per instance (every instance of a launch has the same)
-  int chunk = 8;   // most tracers one thread carries (8, 4, 2 or 1): the tuning knob
+  int ntr;           // tracers per instance (every instance of a launch has the same)
+  int chunk = 0;     // tracers whose intermediates share the workspace (0 = all ntr);
+                     // stages run chunk by chunk
+  int per_thread = 8;  // most tracers one thread carries (8, 4, 2 or 1): the tuning knob
   bool any_wi;      // launch the implicit w_i stage
   bool copy_dry;    // launch the dry-level copy
 };
 int launch_forward(const Inst& single, const Inst* tab, int n, const LaunchDims& d,
                    cudaStream_t s);
-// Same, recording ``after[i]`` on ``s`` after stage i (skipped stages record too).
+// Same, recording ``after[i]`` on ``s`` after stage i of a chunk (skipped stages record
+// too); ``chunk_sel >= 0`` launches only that workspace chunk.
 constexpr int kNumStages = 10;
 extern const char* const kStageNames[kNumStages];
 int launch_forward_events(const Inst& single, const Inst* tab, int n, const LaunchDims& d,
-                          cudaStream_t s, cudaEvent_t* after, bool stop_before_final = false);
+                          cudaStream_t s, cudaEvent_t* after, bool stop_before_final = false,
+                          int chunk_sel = -1);
 // Single-instance forward stages; ``through_factors`` stops after the limiter factors
 // (everything the reverse pass reads), without writing T_new.
 int launch_forward_stages(const Inst& single, const LaunchDims& d, cudaStream_t s,

@@ -97,6 +97,7 @@ struct Inst {
   double* T_new;
   int64_t tstride;
   int tg;
+  int wtg;   // tracers held by the workspace (its interleave stride when interleaved)
   const double *Z3d, *zbar3, *w_i;
   Workspace ws;
   double dt;

@@ -83,6 +83,7 @@ extern "C" int fct_forward_noalloc(FctPlan* P, const FctFields* f, double dt, in
   in.T = f->T; in.T_old = f->T_old; in.T_new = f->T_new;
   in.tstride = f->tracer_stride ? f->tracer_stride : int64_t(P->N) * P->L;
   in.tg = 0;
+  in.wtg = ntr;
   in.Z3d = f->Z3d; in.zbar3 = f->zbar3; in.w_i = f->w_i;
   in.ws = carve_workspace(scratch, P->N, P->E, P->Ed, P->L, ntr);
   in.dt = dt;
@@ -95,7 +96,8 @@ extern "C" int fct_forward_noalloc(FctPlan* P, const FctFields* f, double dt, in
   dims.max_dense = int64_t(P->N) * P->L;
   dims.max_nodes = P->N;
   dims.ntr = ntr;
-  dims.chunk = 8;
+  dims.chunk = 0;
+  dims.per_thread = 8;
   dims.any_wi = f->w_i != nullptr;
   dims.copy_dry = true;
   return restore(launch_forward(in, nullptr, 1, dims, static_cast<cudaStream_t>(stream)));

@@ -369,6 +369,7 @@ int fct_forward(FctPlan* P, const FctFields* f, double dt, int ntr, fct_stream_t
   in.T = f->T; in.T_old = f->T_old; in.T_new = f->T_new;
   in.tstride = f->tracer_stride ? f->tracer_stride : int64_t(P->N) * P->L;
   in.tg = 0;
+  in.wtg = ntr;
   in.Z3d = f->Z3d; in.zbar3 = f->zbar3; in.w_i = f->w_i;
   in.ws = P->ws;
   in.dt = dt;
@@ -381,7 +382,8 @@ int fct_forward(FctPlan* P, const FctFields* f, double dt, int ntr, fct_stream_t
   dims.max_dense = int64_t(P->N) * P->L;
   dims.max_nodes = P->N;
   dims.ntr = ntr;
-  dims.chunk = 8;
+  dims.chunk = 0;       // one workspace chunk: all ntr tracers
+  dims.per_thread = 8;
   dims.any_wi = f->w_i != nullptr;
   dims.copy_dry = true;   // a fresh T_new: dry levels keep T (tracer_adv.py:147-151)
   int prev = -1;

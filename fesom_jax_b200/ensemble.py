@@ -142,10 +142,11 @@ class Ensemble:
         self.prepare()
 
     def info(self) -> dict:
-        out = (C.c_int64 * 4)()
+        out = (C.c_int64 * 6)()
         _lib.check(_bind_batch(_lib.lib()).fct_batch_info(self._h, out))
         return dict(instances=out[0], groups=out[1], workspace_bytes=out[2],
-                    updates_per_step=out[3])
+                    updates_per_step=out[3], workspace_tracers=out[4],
+                    launches_per_step=out[5])
 
     def _stream(self, stream):
         t = self.torch

@@ -184,12 +184,13 @@ typedef struct FctBatch FctBatch;
 int fct_batch_create(const FctInstance* insts, int n, int64_t workspace_budget_bytes,
                      FctBatch** out);
 int fct_batch_destroy(FctBatch* b);
-/* Tuning: the most tracers one thread carries (1, 2, 4 or 8; default 8). Fewer use fewer
- * registers (higher occupancy), more share each gather's index work. Drops cached
- * graphs. */
+/* Tuning: the most tracers one thread carries (1, 2, 4 or 8; default: the workspace
+ * chunk, at most 8). Fewer use fewer registers (higher occupancy), more share each
+ * gather's index work. Drops cached graphs. */
 int fct_batch_set_chunk(FctBatch* b, int chunk);
-/* [instances, groups, workspace bytes, total wet node layers x tracers] */
-int fct_batch_info(const FctBatch* b, int64_t out[4]);
+/* [instances, groups, workspace bytes, total wet node layers x tracers,
+ *  tracers per workspace chunk (largest over groups), kernel launches per step] */
+int fct_batch_info(const FctBatch* b, int64_t out[6]);
 /* Copy the dry levels of buf[1] into buf[0] and buf[2] (dry levels never change). */
 int fct_batch_prepare(FctBatch* b, fct_stream_t stream);
 /* One FCT step of every instance with rotation phase ``phase`` (0, 1 or 2). */
@@ -198,6 +199,21 @@ int fct_batch_step(FctBatch* b, int phase, fct_stream_t stream);
  * graph (cached per (first_phase, steps)) and launched on ``stream``. The instance that
  * holds T after the run is buf[(first_phase + steps + 1) % 3]. */
 int fct_batch_run(FctBatch* b, int first_phase, int steps, fct_stream_t stream);
+
+/*
+ * Continuous batching: one FCT step for an arbitrary set of instances that changes from
+ * call to call (requests joining and leaving), on any meshes. ``FctServe`` owns a
+ * workspace arena (carved per call in instance order; a call whose instances need more
+ * returns FCT_ERR_CAPACITY) and a device instance table uploaded from pinned host memory.
+ * Instance i steps with rotation phase ``phases[i]`` (same convention as fct_batch_step).
+ * Instances with different ntr are launched in separate groups. Calls on one FctServe
+ * must be ordered on one stream.
+ */
+typedef struct FctServe FctServe;
+int fct_serve_create(int device, int max_instances, int64_t workspace_bytes, FctServe** out);
+int fct_serve_destroy(FctServe* s);
+int fct_serve_step(FctServe* s, const FctInstance* insts, const int32_t* phases, int n,
+                   fct_stream_t stream);
 
 /* Profiling aid: run one step of phase ``phase`` stage by stage with CUDA events recorded
  * on ``stream`` between stages, synchronise, and add each stage's time (ms, summed over

@@ -95,3 +95,33 @@ def test_profile_step_reports_every_stage(torch, members):
     assert {"node_lo", "edge_adf", "node_final"} <= set(prof)
     assert all(v >= 0.0 for v in prof.values()) and prof["node_final"] > 0.0
     ens.close()
+
+
+def _ws_bytes(m, ntr):
+    L = m.nl
+    return 8 * (m.edge2D * L + ntr * (4 * m.elem2D * L + 9 * m.nod2D * L + m.edge2D * L))
+
+
+@pytest.mark.parametrize("per_thread", [8, 2, 1])
+def test_chunked_workspace_equals_plain(torch, pi, per_thread):
+    """A budget that holds the workspace of 4 of a member's 10 tracers: the stages run
+    chunk by chunk (4, 4, 2 tracers) through one small workspace; results equal the
+    plain path bit for bit whatever the tracers per thread."""
+    f = I.make_fields(pi, seed=21, n_passive=8, ab2=True)
+    assert f.tracers.shape[0] == 10
+    ens = _ensemble(torch, [(pi, f)], _ws_bytes(pi, 4) + 1024)
+    info = ens.info()
+    assert info["workspace_tracers"] == 4 and info["groups"] == 1
+    ens.set_chunk(per_thread)
+    ens.run(STEPS)
+    torch.cuda.synchronize()
+    launches = ens.info()["launches_per_step"]
+    per_chunk = sum(-(-c // per_thread) for c in (4, 4, 2))
+    assert launches == 1 + 7 * per_chunk
+    T, To = ens.state(0)
+    Tp, Top = _plain(torch, pi, f, STEPS)
+    assert np.array_equal(T.cpu().numpy(), Tp)
+    assert np.array_equal(To.cpu().numpy(), Top)
+    prof = ens.profile_step()
+    assert prof["node_final"] > 0.0
+    ens.close()
