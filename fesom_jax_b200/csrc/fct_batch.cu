@@ -197,7 +197,7 @@ int fct_batch_info(const FctBatch* B, int64_t out[6]) {
     int64_t per_chunk_launches = 0;
     for (int c0 = 0; c0 < g.dims.ntr; c0 += chunk) {
       const int csz = std::min(chunk, g.dims.ntr - c0);
-      per_chunk_launches += (csz + g.dims.per_thread - 1) / g.dims.per_thread;
+      per_chunk_launches += stage_launches(csz, g.dims.per_thread);
     }
     launches += 1 + int64_t(g.dims.any_wi ? 8 : 7) * per_chunk_launches;
   }

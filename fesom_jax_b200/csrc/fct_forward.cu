@@ -616,16 +616,22 @@ __device__ __forceinline__ void body_copy_dry(const Inst& in, int64_t i) {
 
 // Kernel wrappers: ``_1`` takes one instance by value (tracer-major layout, the
 // single-call path); ``_n`` reads instance blockIdx.y of a device table (interleaved
-// layout, the batched path).
+// layout, the batched path). A launch covers S = 2^lg tracer slices of NTR tracers each:
+// in ``_n`` the S threads of a lane are adjacent (slice = thread index mod S), so they
+// read one contiguous run of S*NTR interleaved tracers together; in ``_1`` the slice is
+// blockIdx.y, so lanes stay contiguous along x within each tracer plane.
 #define FCT_KERNEL_T(name, body)                                                        \
   template <int NTR>                                                                    \
   __global__ void __launch_bounds__(256) name##_1(Inst in, int t0, int w0) {            \
-    body<NTR, false>(in, lane_index(), t0, w0);                                         \
+    const int sub = int(blockIdx.y) * NTR;                                              \
+    body<NTR, false>(in, lane_index(), t0 + sub, w0 + sub);                             \
   }                                                                                     \
   template <int NTR>                                                                    \
   __global__ void __launch_bounds__(256) name##_n(const Inst* __restrict__ tab, int t0,  \
-                                                  int w0) {                             \
-    body<NTR, true>(tab[blockIdx.y], lane_index(), t0, w0);                             \
+                                                  int w0, int lg) {                     \
+    const int64_t g = lane_index();                                                     \
+    const int sub = int(g & ((int64_t(1) << lg) - 1)) * NTR;                            \
+    body<NTR, true>(tab[blockIdx.y], g >> lg, t0 + sub, w0 + sub);                      \
   }
 
 FCT_KERNEL_T(k_elem_grad, body_elem_grad)
@@ -654,32 +660,33 @@ const char* const kStageNames[kNumStages] = {
     "vflux", "elem_grad", "node_lo", "vert_impl", "edge_adf", "elem_bounds",
     "node_cluster", "node_factors", "node_final", "copy_dry"};
 
-// One stage over the tracers [c0, c1) of a workspace chunk, split into launches of
-// NTR in {8, 4, 2, 1} tracers per thread (largest first, at most d.per_thread); the
-// workspace index of tracer t is t - c0.
+// One stage over the tracers [c0, c1) of a workspace chunk: launches of S slices x NTR
+// tracers, NTR in {8, 4, 2, 1} (largest first, at most d.per_thread) and S the largest
+// power of two (at most 8) with S*NTR tracers left; the workspace index of tracer t is
+// t - c0.
+#define FCT_STAGE_AS(name, lanes, P)                                                    \
+  do {                                                                                  \
+    if (tab)                                                                            \
+      name##_n<P><<<dim3(xblocks(int64_t(lanes) << lg), unsigned(n)), B, 0, s>>>(        \
+          tab, t0, w0, lg);                                                             \
+    else                                                                                \
+      name##_1<P><<<dim3(xblocks(lanes), 1u << lg), B, 0, s>>>(single, t0, w0);          \
+  } while (0)
+
 #define FCT_STAGE(name, lanes)                                                          \
   do {                                                                                  \
-    const dim3 g = grid(lanes);                                                         \
     for (int t0 = c0; t0 < c1;) {                                                       \
-      const int rem = std::min(c1 - t0, d.per_thread);                                  \
+      const int rem = c1 - t0;                                                          \
+      const int lim = std::min(rem, d.per_thread);                                      \
+      const int P = lim >= 8 ? 8 : lim >= 4 ? 4 : lim >= 2 ? 2 : 1;                     \
+      int lg = 0;                                                                       \
+      while (lg < 3 && (P << (lg + 1)) <= rem) ++lg;                                    \
       const int w0 = t0 - c0;                                                           \
-      if (rem >= 8) {                                                                   \
-        if (tab) name##_n<8><<<g, B, 0, s>>>(tab, t0, w0);                              \
-        else name##_1<8><<<g, B, 0, s>>>(single, t0, w0);                               \
-        t0 += 8;                                                                        \
-      } else if (rem >= 4) {                                                            \
-        if (tab) name##_n<4><<<g, B, 0, s>>>(tab, t0, w0);                              \
-        else name##_1<4><<<g, B, 0, s>>>(single, t0, w0);                               \
-        t0 += 4;                                                                        \
-      } else if (rem >= 2) {                                                            \
-        if (tab) name##_n<2><<<g, B, 0, s>>>(tab, t0, w0);                              \
-        else name##_1<2><<<g, B, 0, s>>>(single, t0, w0);                               \
-        t0 += 2;                                                                        \
-      } else {                                                                          \
-        if (tab) name##_n<1><<<g, B, 0, s>>>(tab, t0, w0);                              \
-        else name##_1<1><<<g, B, 0, s>>>(single, t0, w0);                               \
-        t0 += 1;                                                                        \
-      }                                                                                 \
+      if (P == 8) FCT_STAGE_AS(name, lanes, 8);                                         \
+      else if (P == 4) FCT_STAGE_AS(name, lanes, 4);                                    \
+      else if (P == 2) FCT_STAGE_AS(name, lanes, 2);                                    \
+      else FCT_STAGE_AS(name, lanes, 1);                                                \
+      t0 += P << lg;                                                                    \
     }                                                                                   \
   } while (0)
 
@@ -687,9 +694,10 @@ int launch_forward_events(const Inst& single, const Inst* tab, int n, const Laun
                           cudaStream_t s, cudaEvent_t* after, bool stop_before_final,
                           int chunk_sel) {
   constexpr int B = 256;
-  auto grid = [&](int64_t lanes) {
-    return dim3(unsigned(std::max<int64_t>(1, (lanes + B - 1) / B)), unsigned(n), 1);
+  auto xblocks = [&](int64_t lanes) {
+    return unsigned(std::max<int64_t>(1, (lanes + B - 1) / B));
   };
+  auto grid = [&](int64_t lanes) { return dim3(xblocks(lanes), unsigned(n), 1); };
   const int chunk = d.chunk > 0 ? d.chunk : d.ntr;
   const int nchunks = (d.ntr + chunk - 1) / chunk;
   for (int ci = 0; ci < nchunks; ++ci) {

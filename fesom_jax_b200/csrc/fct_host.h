@@ -57,4 +57,19 @@ int launch_copy_dry(const Inst* tab, int n, int64_t max_dense, cudaStream_t s);
 Workspace carve_workspace(double* base, int64_t N, int64_t E, int64_t Ed, int64_t L, int ntr);
 int64_t workspace_doubles(int64_t N, int64_t E, int64_t Ed, int64_t L, int ntr);
 
+// Launches one stage takes for `csz` tracers of a workspace chunk with at most
+// `per_thread` tracers per thread (the split rule of the stage launcher).
+inline int stage_launches(int csz, int per_thread) {
+  int count = 0;
+  for (int t = 0; t < csz;) {
+    const int rem = csz - t, lim = rem < per_thread ? rem : per_thread;
+    const int P = lim >= 8 ? 8 : lim >= 4 ? 4 : lim >= 2 ? 2 : 1;
+    int lg = 0;
+    while (lg < 3 && (P << (lg + 1)) <= rem) ++lg;
+    t += P << lg;
+    ++count;
+  }
+  return count;
+}
+
 }  // namespace fct
