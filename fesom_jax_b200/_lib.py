@@ -66,10 +66,11 @@ def lib() -> C.CDLL:
     L.fct_plan_destroy.argtypes = [C.c_void_p]
     L.fct_plan_reserve.argtypes = [C.c_void_p, C.c_int]
     L.fct_plan_info.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
+    L.fct_plan_set_fused.argtypes = [C.c_void_p, C.c_int]
     L.fct_forward.argtypes = [C.c_void_p, C.POINTER(FctFields), C.c_double, C.c_int, C.c_void_p]
     L.fct_compute_w.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     for name in ("fct_plan_create", "fct_plan_destroy", "fct_plan_reserve", "fct_plan_info",
-                 "fct_forward", "fct_compute_w"):
+                 "fct_plan_set_fused", "fct_forward", "fct_compute_w"):
         getattr(L, name).restype = C.c_int
     _lib = L
     return L

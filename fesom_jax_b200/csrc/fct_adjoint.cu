@@ -835,6 +835,7 @@ int fct_adjoint(FctPlan* P, const FctFields* f, const double* gT_new, double dt,
   d.max_iface = P->hm.n_iface; d.max_layer = P->hm.n_layer; d.max_edge = P->hm.n_edge;
   d.max_elem = P->hm.n_elem; d.max_dense = int64_t(P->N) * P->L; d.max_nodes = P->N;
   d.ntr = ntr; d.chunk = 0; d.per_thread = 8; d.any_wi = false; d.copy_dry = false;
+  d.fused = false;   // the reverse kernels read every stage's intermediates
   int st = launch_forward_stages(in, d, s, /*through_factors=*/true);
   if (st) return restore(st);
   auto grid = [](int64_t lanes, int b) {

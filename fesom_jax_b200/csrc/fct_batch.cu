@@ -70,10 +70,10 @@ int fct_batch_create(const FctInstance* insts, int n, int64_t budget, FctBatch**
     // the workspace holds a chunk of the instance's tracers (stages run chunk by chunk):
     // up to 8, halved until one instance fits the budget
     int wc = q.ntr < 8 ? q.ntr : 8;
-    while (wc > 1 && workspace_doubles(P->N, P->E, P->Ed, P->L, wc) * int64_t(sizeof(double)) > budget)
+    while (wc > 1 && workspace_doubles_fused(P->N, P->Ed, P->L, wc) * int64_t(sizeof(double)) > budget)
       wc = (wc + 1) / 2;
     wchunk[i] = wc;
-    ws_doubles[i] = workspace_doubles(P->N, P->E, P->Ed, P->L, wc);
+    ws_doubles[i] = workspace_doubles_fused(P->N, P->Ed, P->L, wc);
   }
   FctBatch* B = new FctBatch();
   B->device = dev;
@@ -114,7 +114,8 @@ int fct_batch_create(const FctInstance* insts, int n, int64_t budget, FctBatch**
     for (int i = gr.first; i < gr.first + gr.count; ++i) {
       const FctInstance& q = insts[i];
       const FctPlan* P = q.plan;
-      const Workspace ws = carve_workspace(B->arena + off, P->N, P->E, P->Ed, P->L, wchunk[i]);
+      const Workspace ws =
+          carve_workspace(B->arena + off, P->N, P->E, P->Ed, P->L, wchunk[i], /*fused=*/true);
       off += ws_doubles[i];
       d.max_iface = std::max(d.max_iface, P->hm.n_iface);
       d.max_layer = std::max(d.max_layer, P->hm.n_layer);
@@ -199,7 +200,8 @@ int fct_batch_info(const FctBatch* B, int64_t out[6]) {
       const int csz = std::min(chunk, g.dims.ntr - c0);
       per_chunk_launches += stage_launches(csz, g.dims.per_thread);
     }
-    launches += 1 + int64_t(g.dims.any_wi ? 8 : 7) * per_chunk_launches;
+    const int stages = (g.dims.fused ? 4 : 7) + (g.dims.any_wi ? 1 : 0);
+    launches += 1 + int64_t(stages) * per_chunk_launches;
   }
   out[4] = wmax;
   out[5] = launches;
@@ -384,7 +386,7 @@ int fct_serve_step(FctServe* S, const FctInstance* insts, const int32_t* phases,
     if (!q.plan || q.plan->device != S->device || q.ntr < 1 || !q.buf[0] || !q.buf[1] ||
         !q.buf[2] || !q.uv || !q.w_e || !q.helem || !q.hnode || !q.hnode_new || !(q.dt > 0.0))
       return set_error(FCT_ERR_INVALID, "instance %d is invalid", i);
-    need += workspace_doubles(q.plan->N, q.plan->E, q.plan->Ed, q.plan->L, q.ntr);
+    need += workspace_doubles_fused(q.plan->N, q.plan->Ed, q.plan->L, q.ntr);
   }
   if (need > S->arena_doubles)
     return set_error(FCT_ERR_CAPACITY, "instances need %lld workspace doubles, arena holds %lld",
@@ -414,8 +416,8 @@ int fct_serve_step(FctServe* S, const FctInstance* insts, const int32_t* phases,
     in.tstride = 0;
     in.tg = q.ntr;
     in.wtg = q.ntr;
-    in.ws = carve_workspace(S->arena + off, P->N, P->E, P->Ed, P->L, q.ntr);
-    off += workspace_doubles(P->N, P->E, P->Ed, P->L, q.ntr);
+    in.ws = carve_workspace(S->arena + off, P->N, P->E, P->Ed, P->L, q.ntr, /*fused=*/true);
+    off += workspace_doubles_fused(P->N, P->Ed, P->L, q.ntr);
     in.dt = q.dt;
     in.ntr = q.ntr;
   }

@@ -104,17 +104,16 @@ __device__ __forceinline__ void body_vflux(const Inst& in, int64_t i) {
 }
 
 // ---------------------------------------------------- tracer_gradient_elements
+// Gradient of T on cell `el` (nodes v0, v1, v2) at level k; the stored (elem_grad) and the
+// recomputed (fused stages) gradients both come from here, so they are the same bits.
 template <int NTR, bool IL>
-__device__ __forceinline__ void body_elem_grad(const Inst& in, int64_t i, int t0, int w0) {
-  const DevMesh& m = *in.m;
-  if (i >= m.n_elem) return;
-  const uint32_t lane = ld(m.elem_lanes + i);
-  const int e = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const int v0 = ld(m.enodes + 3 * e), v1 = ld(m.enodes + 3 * e + 1), v2 = ld(m.enodes + 3 * e + 2);
-  const double* g = m.gsca + 6 * int64_t(e);
+__device__ __forceinline__ void cell_grad(const Inst& in, int el, int v0, int v1, int v2, int k,
+                                          int t0, double (&gx)[NTR], double (&gy)[NTR]) {
+  const int L = in.m->L;
+  const double* g = in.m->gsca + 6 * int64_t(el);
   const double g0 = ld(g), g1 = ld(g + 1), g2 = ld(g + 2), g3 = ld(g + 3), g4 = ld(g + 4),
                g5 = ld(g + 5);
-  double a0[NTR], a1[NTR], a2[NTR], gx[NTR], gy[NTR];
+  double a0[NTR], a1[NTR], a2[NTR];
   ldn<NTR, IL>(in.T, int64_t(v0) * L + k, t0, in.tstride, in.tg, a0);
   ldn<NTR, IL>(in.T, int64_t(v1) * L + k, t0, in.tstride, in.tg, a1);
   ldn<NTR, IL>(in.T, int64_t(v2) * L + k, t0, in.tstride, in.tg, a2);
@@ -123,6 +122,28 @@ __device__ __forceinline__ void body_elem_grad(const Inst& in, int64_t i, int t0
     gx[t] = g0 * a0[t] + g1 * a1[t] + g2 * a2[t];
     gy[t] = g3 * a0[t] + g4 * a1[t] + g5 * a2[t];
   }
+}
+
+template <int NTR, bool IL>
+__device__ __forceinline__ void cell_grad(const Inst& in, int el, int k, int t0,
+                                          double (&gx)[NTR], double (&gy)[NTR]) {
+  const int* en = in.m->enodes + 3 * int64_t(el);
+  cell_grad<NTR, IL>(in, el, ld(en), ld(en + 1), ld(en + 2), k, t0, gx, gy);
+}
+
+// k in [r & 255, (r >> 8) & 255): the packed level ranges of the fused stages' slots
+__device__ __forceinline__ bool in_range(int k, unsigned r) {
+  return k >= int(r & 255u) && k < int((r >> 8) & 255u);
+}
+
+template <int NTR, bool IL>
+__device__ __forceinline__ void body_elem_grad(const Inst& in, int64_t i, int t0, int w0) {
+  const DevMesh& m = *in.m;
+  if (i >= m.n_elem) return;
+  const uint32_t lane = ld(m.elem_lanes + i);
+  const int e = lane_ent(lane), k = lane_lev(lane), L = m.L;
+  double gx[NTR], gy[NTR];
+  cell_grad<NTR, IL>(in, e, k, t0, gx, gy);
   const int64_t q = int64_t(e) * L + k;
   stn<NTR, IL>(in.ws.gx, q, w0, in.ws.sE, in.wtg, gx);
   stn<NTR, IL>(in.ws.gy, q, w0, in.ws.sE, in.wtg, gy);
@@ -136,7 +157,9 @@ __device__ __forceinline__ double vflux_up(double Tb, double Ta, double w, doubl
 }
 
 // -------------------------------- LO solution, node-average gradient, adf_v
-template <int NTR, bool IL>
+// FUSED: packed edge slots, and the cell gradients recomputed from T instead of read
+// from the elem_grad stage.
+template <int NTR, bool IL, bool FUSED>
 __device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i, int t0, int w0) {
   const DevMesh& m = *in.m;
   if (i >= m.n_iface) return;
@@ -180,19 +203,40 @@ __device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i, int t0, 
 #pragma unroll
     for (int t = 0; t < NTR; ++t) div[t] = 0.0;
     const int e0 = ld(m.ne_off + n), e1 = ld(m.ne_off + n + 1);
-    for (int j = e0; j < e1; ++j) {
-      const int idx = ld(m.ne_idx + j), e = idx >> 1;
-      if (k < ld(m.ekmin + e) || k >= ld(m.ekmax + e)) continue;   // vflux == 0 there
-      const int oth = ld(m.ne_oth + j);
-      const double vf = ld(in.ws.vflux + int64_t(e) * L + k);
-      const double avf = fabs(vf);
-      double To[NTR];
-      ldn<NTR, IL>(in.T, int64_t(oth) * L + k, t0, ts, tg, To);
+    if constexpr (FUSED) {
+      // loads are unconditional (all in bounds) and inactive edges are selected away,
+      // so consecutive slots' loads overlap
+#pragma unroll 2
+      for (int j = e0; j < e1; ++j) {
+        const int4 sl = __ldg(m.ne4 + j);
+        const bool on = in_range(k, unsigned(sl.z));
+        const bool second = sl.x & 1;
+        const double vf = ld(in.ws.vflux + int64_t(sl.x >> 1) * L + k);
+        const double avf = fabs(vf);
+        double To[NTR];
+        ldn<NTR, IL>(in.T, int64_t(sl.y) * L + k, t0, ts, tg, To);
 #pragma unroll
-      for (int t = 0; t < NTR; ++t) {
-        const double T1 = (idx & 1) ? To[t] : Tc[t], T2 = (idx & 1) ? Tc[t] : To[t];
-        const double fl = -0.5 * (T1 * (vf + avf) + T2 * (vf - avf));
-        div[t] += (idx & 1) ? -fl : fl;
+        for (int t = 0; t < NTR; ++t) {
+          const double T1 = second ? To[t] : Tc[t], T2 = second ? Tc[t] : To[t];
+          const double fl = -0.5 * (T1 * (vf + avf) + T2 * (vf - avf));
+          div[t] = on ? div[t] + (second ? -fl : fl) : div[t];
+        }
+      }
+    } else {
+      for (int j = e0; j < e1; ++j) {
+        const int idx = ld(m.ne_idx + j), e = idx >> 1;
+        if (k < ld(m.ekmin + e) || k >= ld(m.ekmax + e)) continue;   // vflux == 0 there
+        const int oth = ld(m.ne_oth + j);
+        const double vf = ld(in.ws.vflux + int64_t(e) * L + k);
+        const double avf = fabs(vf);
+        double To[NTR];
+        ldn<NTR, IL>(in.T, int64_t(oth) * L + k, t0, ts, tg, To);
+#pragma unroll
+        for (int t = 0; t < NTR; ++t) {
+          const double T1 = (idx & 1) ? To[t] : Tc[t], T2 = (idx & 1) ? Tc[t] : To[t];
+          const double fl = -0.5 * (T1 * (vf + avf) + T2 * (vf - avf));
+          div[t] += (idx & 1) ? -fl : fl;
+        }
       }
     }
     const bool valid = (hnn > 0.0) && (av > 0.0);
@@ -206,20 +250,36 @@ __device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i, int t0, 
 #pragma unroll
     for (int t = 0; t < NTR; ++t) nx[t] = ny[t] = 0.0;
     const int c0 = ld(m.nel_off + n), c1 = ld(m.nel_off + n + 1);
-    for (int j = c0; j < c1; ++j) {
-      const int el = ld(m.nel_idx + j);
-      if (k >= ld(m.eul + el) && k < ld(m.enl + el)) {
-        const double a = ld(m.earea + el);
-        const int64_t qe = int64_t(el) * L + k;
+    if constexpr (FUSED) {
+      for (int j = c0; j < c1; ++j) {
+        if (!in_range(k, unsigned(ld(m.nelr + j)))) continue;
+        const int4 sl = __ldg(m.nel4 + j);
+        const double a = ld(m.earea + sl.x);
         double gx[NTR], gy[NTR];
-        ldn<NTR, IL>(in.ws.gx, qe, w0, in.ws.sE, in.wtg, gx);
-        ldn<NTR, IL>(in.ws.gy, qe, w0, in.ws.sE, in.wtg, gy);
+        cell_grad<NTR, IL>(in, sl.x, sl.y, sl.z, sl.w, k, t0, gx, gy);
 #pragma unroll
         for (int t = 0; t < NTR; ++t) {
           nx[t] += gx[t] * a;
           ny[t] += gy[t] * a;
         }
         den += a;
+      }
+    } else {
+      for (int j = c0; j < c1; ++j) {
+        const int el = ld(m.nel_idx + j);
+        if (k >= ld(m.eul + el) && k < ld(m.enl + el)) {
+          const double a = ld(m.earea + el);
+          const int64_t qe = int64_t(el) * L + k;
+          double gx[NTR], gy[NTR];
+          ldn<NTR, IL>(in.ws.gx, qe, w0, in.ws.sE, in.wtg, gx);
+          ldn<NTR, IL>(in.ws.gy, qe, w0, in.ws.sE, in.wtg, gy);
+#pragma unroll
+          for (int t = 0; t < NTR; ++t) {
+            nx[t] += gx[t] * a;
+            ny[t] += gy[t] * a;
+          }
+          den += a;
+        }
       }
     }
     const double dd = den > 0.0 ? den : 1.0;
@@ -335,7 +395,7 @@ __device__ __forceinline__ void body_vert_impl(const Inst& in, int64_t n, int t0
 }
 
 // -------------------------- fill_up_dn_grad + adv_flux_hor_ho - LO flux = adf_h
-template <int NTR, bool IL>
+template <int NTR, bool IL, bool FUSED>
 __device__ __forceinline__ void body_edge_adf(const Inst& in, int64_t i, int t0, int w0) {
   const DevMesh& m = *in.m;
   if (i >= m.n_edge) return;
@@ -358,11 +418,17 @@ __device__ __forceinline__ void body_edge_adf(const Inst& in, int64_t i, int t0,
   ldn<NTR, IL>(in.T_old, q1, t0, ts, tg, O1);
   ldn<NTR, IL>(in.T_old, q2, t0, ts, tg, O2);
   if (use_tri) {
-    const int64_t qu = int64_t(up) * L + k, qd = int64_t(dn) * L + k;
-    ldn<NTR, IL>(in.ws.gx, qu, w0, in.ws.sE, in.wtg, g0);
-    ldn<NTR, IL>(in.ws.gx, qd, w0, in.ws.sE, in.wtg, g1);
-    ldn<NTR, IL>(in.ws.gy, qu, w0, in.ws.sE, in.wtg, g2);
-    ldn<NTR, IL>(in.ws.gy, qd, w0, in.ws.sE, in.wtg, g3);
+    // both cells are wet at k here (k is above every adjacent cell's bottom)
+    if constexpr (FUSED) {
+      cell_grad<NTR, IL>(in, up, k, t0, g0, g2);
+      cell_grad<NTR, IL>(in, dn, k, t0, g1, g3);
+    } else {
+      const int64_t qu = int64_t(up) * L + k, qd = int64_t(dn) * L + k;
+      ldn<NTR, IL>(in.ws.gx, qu, w0, in.ws.sE, in.wtg, g0);
+      ldn<NTR, IL>(in.ws.gx, qd, w0, in.ws.sE, in.wtg, g1);
+      ldn<NTR, IL>(in.ws.gy, qu, w0, in.ws.sE, in.wtg, g2);
+      ldn<NTR, IL>(in.ws.gy, qd, w0, in.ws.sE, in.wtg, g3);
+    }
   } else {
     ldn<NTR, IL>(in.ws.gnx, q1, w0, in.ws.sN, in.wtg, g0);
     ldn<NTR, IL>(in.ws.gnx, q2, w0, in.ws.sN, in.wtg, g1);
@@ -516,8 +582,117 @@ __device__ __forceinline__ void body_node_factors(const Inst& in, int64_t i, int
   stn<NTR, IL>(in.ws.mf, qn, w0, sN, in.wtg, mf);
 }
 
-// ---------- zalesak b3 + flux2dtracer_fct + ale_reconstruct: T_new on layers
+// ------- fused zalesak a2 + a3 + a4 + b1 + b2: cluster bounds, window, factors
+// The cluster bound of node n at level k is the max (min) of max(LO, T) (min(LO, T)) over
+// the nodes of n's cells that are wet at k, padded with -BIG (+BIG) when one of n's cells
+// is dry at k (tracer_adv.py:389-405). Every cell of n has two edges at n, so those nodes
+// are n itself (when any cell is wet at k) and the edge neighbours with a wet cell at k:
+// one gather over the packed edge slots, which also sums the antidiffusive fluxes (b1).
+// max/min are exact, so the result equals the per-cell evaluation bit for bit.
+// The a4 window (k-1, k, k+1 of the same column) comes from the neighbouring lanes'
+// cluster bounds in shared memory: a block computes bounds for its lanes plus one halo
+// lane on each side, and finishes the factors for its core lanes only.
 template <int NTR, bool IL>
+__device__ __forceinline__ void node_limit(const Inst& in, int64_t lane, bool core, int t0,
+                                           int w0, int tid, int nb, double* smx, double* smn) {
+  const DevMesh& m = *in.m;
+  const bool valid = lane >= 0 && lane < m.n_layer;
+  const int L = m.L;
+  const int64_t sN = in.ws.sN;
+  int n = 0, k = 0;
+  int64_t qn = 0;
+  double mx[NTR], mn[NTR], sp[NTR], sm[NTR], lo[NTR];
+  if (valid) {
+    const uint32_t ln = ld(m.layer_lanes + lane);
+    n = lane_ent(ln);
+    k = lane_lev(ln);
+    qn = int64_t(n) * L + k;
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) {
+      mx[t] = -INFINITY; mn[t] = INFINITY; sp[t] = 0.0; sm[t] = 0.0;
+    }
+    bool own = false, off = false;
+    const int e0 = ld(m.ne_off + n), e1 = ld(m.ne_off + n + 1);
+#pragma unroll 2
+    for (int j = e0; j < e1; ++j) {
+      const int4 sl = __ldg(m.ne4 + j);
+      const unsigned tr = unsigned(sl.w);
+      const bool c1 = in_range(k, tr & 0xffffu);
+      const bool has2 = ((tr >> 16) & 255u) != kNoCell;
+      const bool c2 = has2 && in_range(k, tr >> 16);
+      const bool wet = c1 || c2;
+      own = own || wet;
+      off = off || !c1 || (has2 && !c2);
+      const bool on = in_range(k, unsigned(sl.z));
+      const bool second = sl.x & 1;
+      const int64_t qo = int64_t(sl.y) * L + k;
+      double a[NTR], lv[NTR], tv[NTR];
+      ldn<NTR, IL>(in.ws.adfh, int64_t(sl.x >> 1) * L + k, w0, in.ws.sEd, in.wtg, a);
+      ldn<NTR, IL>(in.ws.lo, qo, w0, sN, in.wtg, lv);
+      ldn<NTR, IL>(in.T, qo, t0, in.tstride, in.tg, tv);
+#pragma unroll
+      for (int t = 0; t < NTR; ++t) {
+        mx[t] = wet ? fmax(mx[t], fmax(lv[t], tv[t])) : mx[t];
+        mn[t] = wet ? fmin(mn[t], fmin(lv[t], tv[t])) : mn[t];
+        const double sv = second ? -a[t] : a[t];
+        sp[t] = on ? sp[t] + fmax(sv, 0.0) : sp[t];
+        sm[t] = on ? sm[t] + fmin(sv, 0.0) : sm[t];
+      }
+    }
+    double tv[NTR];
+    ldn<NTR, IL>(in.ws.lo, qn, w0, sN, in.wtg, lo);
+    ldn<NTR, IL>(in.T, qn, t0, in.tstride, in.tg, tv);
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) {
+      if (own) {
+        mx[t] = fmax(mx[t], fmax(lo[t], tv[t]));
+        mn[t] = fmin(mn[t], fmin(lo[t], tv[t]));
+      }
+      if (off) {
+        mx[t] = fmax(mx[t], -kBig);
+        mn[t] = fmin(mn[t], kBig);
+      }
+      smx[t * 256 + tid] = mx[t];
+      smn[t * 256 + tid] = mn[t];
+    }
+  }
+  __syncthreads();
+  if (!valid || !core) return;
+  const int nzmin = ld(m.nzmin + n), nzmax = ld(m.nzmax + n);
+  if (k != nzmin && k != nzmax - 1) {   // interior: window over k-1, k, k+1 (lanes +-1)
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) {
+      mx[t] = fmax(fmax(smx[t * 256 + tid - nb], mx[t]), smx[t * 256 + tid + nb]);
+      mn[t] = fmin(fmin(smn[t * 256 + tid - nb], mn[t]), smn[t * 256 + tid + nb]);
+    }
+  }
+  const double av = ld(m.areasvol + qn), hnn = ld(in.hnode_new + qn);
+  const bool valid_n = (av > 0.0) && (hnn > 0.0);
+  const double sa = av > 0.0 ? av : 1.0, sh = hnn > 0.0 ? hnn : 1.0;
+  const double dt = in.dt;
+  double ft[NTR], fb[NTR];
+  ldn<NTR, IL>(in.ws.adfv, qn, w0, sN, in.wtg, ft);
+  ldn<NTR, IL>(in.ws.adfv, qn + 1, w0, sN, in.wtg, fb);   // k+1 <= nzmax < L
+  double pf[NTR], mf[NTR];
+#pragma unroll
+  for (int t = 0; t < NTR; ++t) {
+    const double plus = (fmax(ft[t], 0.0) + fmax(-fb[t], 0.0)) + sp[t];
+    const double minus = (fmin(ft[t], 0.0) + fmin(-fb[t], 0.0)) + sm[t];
+    pf[t] = 1.0;
+    mf[t] = 1.0;
+    if (valid_n) {
+      const double flux_pos = plus * dt / sa / sh + kFluxEps;
+      const double flux_neg = minus * dt / sa / sh - kFluxEps;
+      pf[t] = fmin(1.0, (mx[t] - lo[t]) / flux_pos);
+      mf[t] = fmin(1.0, (mn[t] - lo[t]) / flux_neg);
+    }
+  }
+  stn<NTR, IL>(in.ws.pf, qn, w0, sN, in.wtg, pf);
+  stn<NTR, IL>(in.ws.mf, qn, w0, sN, in.wtg, mf);
+}
+
+// ---------- zalesak b3 + flux2dtracer_fct + ale_reconstruct: T_new on layers
+template <int NTR, bool IL, bool FUSED>
 __device__ __forceinline__ void body_node_final(const Inst& in, int64_t i, int t0, int w0) {
   const DevMesh& m = *in.m;
   if (i >= m.n_layer) return;
@@ -568,22 +743,44 @@ __device__ __forceinline__ void body_node_final(const Inst& in, int64_t i, int t
 #pragma unroll
   for (int t = 0; t < NTR; ++t) hsc[t] = 0.0;
   const int e0 = ld(m.ne_off + n), e1 = ld(m.ne_off + n + 1);
-  for (int j = e0; j < e1; ++j) {
-    const int idx = ld(m.ne_idx + j), e = idx >> 1;
-    if (k < ld(m.ekmin + e) || k >= ld(m.ekmax + e)) continue;   // no flux on this level
-    const int64_t qo = int64_t(ld(m.ne_oth + j)) * L + k;
-    double a[NTR], pfo[NTR], mfo[NTR];
-    ldn<NTR, IL>(in.ws.adfh, int64_t(e) * L + k, w0, in.ws.sEd, in.wtg, a);
-    ldn<NTR, IL>(in.ws.pf, qo, w0, sN, in.wtg, pfo);
-    ldn<NTR, IL>(in.ws.mf, qo, w0, sN, in.wtg, mfo);
+  if constexpr (FUSED) {
+#pragma unroll 2
+    for (int j = e0; j < e1; ++j) {
+      const int4 sl = __ldg(m.ne4 + j);
+      const bool on = in_range(k, unsigned(sl.z));
+      const bool second = sl.x & 1;
+      const int64_t qo = int64_t(sl.y) * L + k;
+      double a[NTR], pfo[NTR], mfo[NTR];
+      ldn<NTR, IL>(in.ws.adfh, int64_t(sl.x >> 1) * L + k, w0, in.ws.sEd, in.wtg, a);
+      ldn<NTR, IL>(in.ws.pf, qo, w0, sN, in.wtg, pfo);
+      ldn<NTR, IL>(in.ws.mf, qo, w0, sN, in.wtg, mfo);
 #pragma unroll
-    for (int t = 0; t < NTR; ++t) {
-      // (pf, mf) at the edge's first node n1 and second node n2
-      const double pf1 = (idx & 1) ? pfo[t] : pf0[t], mf1 = (idx & 1) ? mfo[t] : mf0[t];
-      const double pf2 = (idx & 1) ? pf0[t] : pfo[t], mf2 = (idx & 1) ? mf0[t] : mfo[t];
-      const double ae = a[t] >= 0.0 ? fmin(pf1, mf2) : fmin(mf1, pf2);
-      const double lim = ae * a[t];
-      hsc[t] += (idx & 1) ? -lim : lim;
+      for (int t = 0; t < NTR; ++t) {
+        const double pf1 = second ? pfo[t] : pf0[t], mf1 = second ? mfo[t] : mf0[t];
+        const double pf2 = second ? pf0[t] : pfo[t], mf2 = second ? mf0[t] : mfo[t];
+        const double ae = a[t] >= 0.0 ? fmin(pf1, mf2) : fmin(mf1, pf2);
+        const double lim = ae * a[t];
+        hsc[t] = on ? hsc[t] + (second ? -lim : lim) : hsc[t];
+      }
+    }
+  } else {
+    for (int j = e0; j < e1; ++j) {
+      const int idx = ld(m.ne_idx + j), e = idx >> 1;
+      if (k < ld(m.ekmin + e) || k >= ld(m.ekmax + e)) continue;   // no flux on this level
+      const int64_t qo = int64_t(ld(m.ne_oth + j)) * L + k;
+      double a[NTR], pfo[NTR], mfo[NTR];
+      ldn<NTR, IL>(in.ws.adfh, int64_t(e) * L + k, w0, in.ws.sEd, in.wtg, a);
+      ldn<NTR, IL>(in.ws.pf, qo, w0, sN, in.wtg, pfo);
+      ldn<NTR, IL>(in.ws.mf, qo, w0, sN, in.wtg, mfo);
+#pragma unroll
+      for (int t = 0; t < NTR; ++t) {
+        // (pf, mf) at the edge's first node n1 and second node n2
+        const double pf1 = (idx & 1) ? pfo[t] : pf0[t], mf1 = (idx & 1) ? mfo[t] : mf0[t];
+        const double pf2 = (idx & 1) ? pf0[t] : pfo[t], mf2 = (idx & 1) ? mf0[t] : mfo[t];
+        const double ae = a[t] >= 0.0 ? fmin(pf1, mf2) : fmin(mf1, pf2);
+        const double lim = ae * a[t];
+        hsc[t] += (idx & 1) ? -lim : lim;
+      }
     }
   }
   double Tv[NTR], lo[NTR], out[NTR];
@@ -634,14 +831,55 @@ __device__ __forceinline__ void body_copy_dry(const Inst& in, int64_t i) {
     body<NTR, true>(tab[blockIdx.y], g >> lg, t0 + sub, w0 + sub);                      \
   }
 
+#define FCT_BODY_VARIANT(name, body, fused)                                             \
+  template <int NTR, bool IL>                                                           \
+  __device__ __forceinline__ void name(const Inst& in, int64_t i, int t0, int w0) {     \
+    body<NTR, IL, fused>(in, i, t0, w0);                                                \
+  }
+FCT_BODY_VARIANT(body_node_lo_u, body_node_lo, false)
+FCT_BODY_VARIANT(body_node_lo_f, body_node_lo, true)
+FCT_BODY_VARIANT(body_edge_adf_u, body_edge_adf, false)
+FCT_BODY_VARIANT(body_edge_adf_f, body_edge_adf, true)
+FCT_BODY_VARIANT(body_node_final_u, body_node_final, false)
+FCT_BODY_VARIANT(body_node_final_f, body_node_final, true)
+
+// unfused stages (every intermediate in the workspace; the reverse pass reads them)
 FCT_KERNEL_T(k_elem_grad, body_elem_grad)
-FCT_KERNEL_T(k_node_lo, body_node_lo)
+FCT_KERNEL_T(k_node_lo, body_node_lo_u)
 FCT_KERNEL_T(k_vert_impl, body_vert_impl)
-FCT_KERNEL_T(k_edge_adf, body_edge_adf)
+FCT_KERNEL_T(k_edge_adf, body_edge_adf_u)
 FCT_KERNEL_T(k_elem_bounds, body_elem_bounds)
 FCT_KERNEL_T(k_node_cluster, body_node_cluster)
 FCT_KERNEL_T(k_node_factors, body_node_factors)
-FCT_KERNEL_T(k_node_final, body_node_final)
+FCT_KERNEL_T(k_node_final, body_node_final_u)
+// fused stages
+FCT_KERNEL_T(k_node_lo_f, body_node_lo_f)
+FCT_KERNEL_T(k_edge_adf_f, body_edge_adf_f)
+FCT_KERNEL_T(k_node_final_f, body_node_final_f)
+
+// node_limit blocks hold 256 threads: `_1` one lane per thread (slice = blockIdx.y),
+// `_n` 256 >> lg lanes of 2^lg adjacent slice threads; the first and last lane of a
+// block are halo lanes.
+template <int NTR>
+__global__ void __launch_bounds__(256) k_node_limit_1(Inst in, int t0, int w0) {
+  __shared__ double smx[NTR * 256], smn[NTR * 256];
+  const int tid = threadIdx.x;
+  const int64_t lane = int64_t(blockIdx.x) * 254 + tid - 1;
+  const int sub = int(blockIdx.y) * NTR;
+  node_limit<NTR, false>(in, lane, tid >= 1 && tid <= 254, t0 + sub, w0 + sub, tid, 1, smx,
+                         smn);
+}
+template <int NTR>
+__global__ void __launch_bounds__(256) k_node_limit_n(const Inst* __restrict__ tab, int t0,
+                                                      int w0, int lg) {
+  __shared__ double smx[NTR * 256], smn[NTR * 256];
+  const int tid = threadIdx.x;
+  const int ll = tid >> lg, bl = 256 >> lg;
+  const int64_t lane = int64_t(blockIdx.x) * (bl - 2) + ll - 1;
+  const int sub = (tid & ((1 << lg) - 1)) * NTR;
+  node_limit<NTR, true>(tab[blockIdx.y], lane, ll >= 1 && ll <= bl - 2, t0 + sub, w0 + sub,
+                        tid, 1 << lg, smx, smn);
+}
 
 __global__ void __launch_bounds__(256) k_vflux_1(Inst in) { body_vflux(in, lane_index()); }
 __global__ void __launch_bounds__(256) k_vflux_n(const Inst* __restrict__ tab) {
@@ -673,7 +911,18 @@ const char* const kStageNames[kNumStages] = {
       name##_1<P><<<dim3(xblocks(lanes), 1u << lg), B, 0, s>>>(single, t0, w0);          \
   } while (0)
 
-#define FCT_STAGE(name, lanes)                                                          \
+#define FCT_LIMIT_AS(name, lanes, P)                                                    \
+  do {                                                                                  \
+    if (tab)                                                                            \
+      k_node_limit_n<P><<<dim3(unsigned(std::max<int64_t>(                              \
+                               1, (int64_t(lanes) + (B >> lg) - 3) / ((B >> lg) - 2))), \
+                           unsigned(n)), B, 0, s>>>(tab, t0, w0, lg);                   \
+    else                                                                                \
+      k_node_limit_1<P><<<dim3(unsigned(std::max<int64_t>(1, (int64_t(lanes) + 253) / 254)), \
+                           1u << lg), B, 0, s>>>(single, t0, w0);                       \
+  } while (0)
+
+#define FCT_SPLIT(AS, name, lanes)                                                      \
   do {                                                                                  \
     for (int t0 = c0; t0 < c1;) {                                                       \
       const int rem = c1 - t0;                                                          \
@@ -682,13 +931,15 @@ const char* const kStageNames[kNumStages] = {
       int lg = 0;                                                                       \
       while (lg < 3 && (P << (lg + 1)) <= rem) ++lg;                                    \
       const int w0 = t0 - c0;                                                           \
-      if (P == 8) FCT_STAGE_AS(name, lanes, 8);                                         \
-      else if (P == 4) FCT_STAGE_AS(name, lanes, 4);                                    \
-      else if (P == 2) FCT_STAGE_AS(name, lanes, 2);                                    \
-      else FCT_STAGE_AS(name, lanes, 1);                                                \
+      if (P == 8) AS(name, lanes, 8);                                                   \
+      else if (P == 4) AS(name, lanes, 4);                                              \
+      else if (P == 2) AS(name, lanes, 2);                                              \
+      else AS(name, lanes, 1);                                                          \
       t0 += P << lg;                                                                    \
     }                                                                                   \
   } while (0)
+#define FCT_STAGE(name, lanes) FCT_SPLIT(FCT_STAGE_AS, name, lanes)
+#define FCT_LIMIT(lanes) FCT_SPLIT(FCT_LIMIT_AS, k_node_limit, lanes)
 
 int launch_forward_events(const Inst& single, const Inst* tab, int n, const LaunchDims& d,
                           cudaStream_t s, cudaEvent_t* after, bool stop_before_final,
@@ -713,6 +964,26 @@ int launch_forward_events(const Inst& single, const Inst* tab, int n, const Laun
       else k_vflux_1<<<grid(d.max_edge), B, 0, s>>>(single);
     }
     mark();
+    if (d.fused) {
+      // 4 launches per chunk; the stages folded into others record empty intervals
+      // (elem_grad into node_lo and edge_adf, elem_bounds and node_cluster into the
+      // factors stage, k_node_limit)
+      mark();
+      FCT_STAGE(k_node_lo_f, d.max_iface);
+      mark();
+      if (d.any_wi) FCT_STAGE(k_vert_impl, d.max_nodes);
+      mark();
+      FCT_STAGE(k_edge_adf_f, d.max_edge);
+      mark();
+      mark();
+      mark();
+      FCT_LIMIT(d.max_layer);
+      mark();
+      if (stop_before_final) continue;
+      FCT_STAGE(k_node_final_f, d.max_layer);
+      mark();
+      continue;
+    }
     FCT_STAGE(k_elem_grad, d.max_elem);
     mark();
     FCT_STAGE(k_node_lo, d.max_iface);

@@ -35,6 +35,8 @@ struct LaunchDims {
   int per_thread = 8;  // most tracers one thread carries (8, 4, 2 or 1): the tuning knob
   bool any_wi;      // launch the implicit w_i stage
   bool copy_dry;    // launch the dry-level copy
+  bool fused = true;  // fused stages (lean workspace); false: every stage kernel writes its
+                      // intermediates (what the reverse pass reads)
 };
 int launch_forward(const Inst& single, const Inst* tab, int n, const LaunchDims& d,
                    cudaStream_t s);
@@ -54,8 +56,12 @@ int launch_forward_stages(const Inst& single, const LaunchDims& d, cudaStream_t 
 // Copy T's dry levels into T_new for ``n`` instances of ``tab`` (ignores Inst::copy_dry).
 int launch_copy_dry(const Inst* tab, int n, int64_t max_dense, cudaStream_t s);
 
-Workspace carve_workspace(double* base, int64_t N, int64_t E, int64_t Ed, int64_t L, int ntr);
+// Workspace of `ntr` tracers: every stage field (the unfused stages, which the reverse
+// pass recomputes and reads), or with `fused` only the fields the fused forward keeps.
+Workspace carve_workspace(double* base, int64_t N, int64_t E, int64_t Ed, int64_t L, int ntr,
+                          bool fused = false);
 int64_t workspace_doubles(int64_t N, int64_t E, int64_t Ed, int64_t L, int ntr);
+int64_t workspace_doubles_fused(int64_t N, int64_t Ed, int64_t L, int ntr);
 
 // Launches one stage takes for `csz` tracers of a workspace chunk with at most
 // `per_thread` tracers per thread (the split rule of the stage launcher).

@@ -24,6 +24,13 @@ constexpr double kFluxEps = 1e-16;       // tracer_adv.py:192
 constexpr double kBig = 1e3;             // tracer_adv.py:193
 
 __host__ __device__ inline int lane_ent(uint32_t lane) { return int(lane >> kLevelBits); }
+// The layer ranges [eul, enl) of an edge's two cells in one word: cell 1 in the low
+// 16 bits, cell 2 in the high 16 (a coast edge has no cell 2: its range is stored as
+// [255, 0), empty, and its flag is the eul byte 255).
+constexpr unsigned kNoCell = 255u;
+__host__ __device__ inline unsigned pack_tri(int ul1, int nl1, int ul2, int nl2) {
+  return unsigned(ul1) | (unsigned(nl1) << 8) | (unsigned(ul2) << 16) | (unsigned(nl2) << 24);
+}
 __host__ __device__ inline int lane_lev(uint32_t lane) { return int(lane & kLevelMask); }
 
 // Static mesh on the device (pointers into one plan allocation).
@@ -58,6 +65,11 @@ struct DevMesh {
   const int* eud_idx;    //   entry = 2*edge + slot (edge_up_dn_tri[edge, slot] == element)
   const int* ekmin;      // [Ed] first level of the edge's lanes (union of its cells' layers)
   const int* ekmax;      // [Ed] one past the last such level
+  // packed CSR slots for the fused stage kernels (one 16-byte load per neighbour)
+  const int4* ne4;       // per node->edge slot: {2*edge + second, other node,
+                         //   ekmin | ekmax << 8, cell layer ranges (see pack_tri)}
+  const int4* nel4;      // per node->element slot: {element, its three nodes}
+  const int* nelr;       // per node->element slot: eul | enl << 8
   // vertical
   const double* Zp;      // [L]  Z padded with Z[L-2] (tracer_adv.py:233)
   const double* zbar;    // [L]
@@ -126,6 +138,7 @@ struct FctPlan {
   fct::DevMesh* d_mesh = nullptr;  // device copy
   void* d_static = nullptr;        // one allocation for all static arrays
   int max_tracers = 0;
+  bool fused = true;               // fct_forward runs the fused stage kernels
   double* d_ws = nullptr;          // workspace allocation
   fct::Workspace ws{};
   int64_t n_wet_elem_layers = 0;

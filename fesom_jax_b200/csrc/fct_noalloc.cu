@@ -52,7 +52,7 @@ extern "C" int fct_forward_noalloc(FctPlan* P, const FctFields* f, double dt, in
   if (!(dt > 0.0)) return set_error(FCT_ERR_INVALID, "dt must be positive");
   if (P->device < 0 || P->device >= kMaxDevices)
     return set_error(FCT_ERR_INVALID, "device %d out of range", P->device);
-  const int64_t need = workspace_doubles(P->N, P->E, P->Ed, P->L, ntr);
+  const int64_t need = workspace_doubles_fused(P->N, P->Ed, P->L, ntr);
   if (need > kStaticScratchDoubles)
     return set_error(FCT_ERR_CAPACITY,
                      "fct_forward_noalloc: %d tracers on this mesh need %lld doubles of "
@@ -85,7 +85,7 @@ extern "C" int fct_forward_noalloc(FctPlan* P, const FctFields* f, double dt, in
   in.tg = 0;
   in.wtg = ntr;
   in.Z3d = f->Z3d; in.zbar3 = f->zbar3; in.w_i = f->w_i;
-  in.ws = carve_workspace(scratch, P->N, P->E, P->Ed, P->L, ntr);
+  in.ws = carve_workspace(scratch, P->N, P->E, P->Ed, P->L, ntr, /*fused=*/true);
   in.dt = dt;
   in.ntr = ntr;
   LaunchDims dims{};

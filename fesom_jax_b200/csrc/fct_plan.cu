@@ -34,7 +34,12 @@ int64_t workspace_doubles(int64_t N, int64_t E, int64_t Ed, int64_t L, int ntr) 
   return Ed * L + int64_t(ntr) * (4 * E * L + 9 * N * L + Ed * L);
 }
 
-Workspace carve_workspace(double* base, int64_t N, int64_t E, int64_t Ed, int64_t L, int ntr) {
+int64_t workspace_doubles_fused(int64_t N, int64_t Ed, int64_t L, int ntr) {
+  return Ed * L + int64_t(ntr) * (6 * N * L + Ed * L);
+}
+
+Workspace carve_workspace(double* base, int64_t N, int64_t E, int64_t Ed, int64_t L, int ntr,
+                          bool fused) {
   Workspace w{};
   w.sN = N * L;
   w.sE = E * L;
@@ -42,6 +47,16 @@ Workspace carve_workspace(double* base, int64_t N, int64_t E, int64_t Ed, int64_
   double* p = base;
   auto take = [&](int64_t n) { double* q = p; p += n; return q; };
   w.vflux = take(Ed * L);
+  if (fused) {   // the fused stages keep no element fields and no cluster bounds
+    w.lo = take(ntr * w.sN);
+    w.gnx = take(ntr * w.sN);
+    w.gny = take(ntr * w.sN);
+    w.adfv = take(ntr * w.sN);
+    w.pf = take(ntr * w.sN);
+    w.mf = take(ntr * w.sN);
+    w.adfh = take(ntr * w.sEd);
+    return w;
+  }
   w.gx = take(ntr * w.sE);
   w.gy = take(ntr * w.sE);
   w.amax = take(ntr * w.sE);
@@ -207,6 +222,25 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
     ekmin[e] = std::max(lo, 0);
     ekmax[e] = std::min(hi, L);
   }
+  // packed slots for the fused kernels
+  std::vector<int4> ne4(2 * size_t(Ed));
+  for (int n = 0; n < N; ++n)
+    for (int j = ne_off[n]; j < ne_off[n + 1]; ++j) {
+      const int e = ne_idx[j] >> 1;
+      const int el1 = d->edge_tri[2 * e], el2 = d->edge_tri[2 * e + 1];
+      const unsigned tri = el2 >= 0 ? pack_tri(eul[el1], enl[el1], eul[el2], enl[el2])
+                                    : pack_tri(eul[el1], enl[el1], int(kNoCell), 0);
+      ne4[j] = make_int4(ne_idx[j], ne_oth[j], ekmin[e] | (ekmax[e] << 8), int(tri));
+    }
+  const int nie_all = d->nod_in_elem2D_offsets[N];
+  std::vector<int4> nel4(std::max(nie_all, 1));
+  std::vector<int> nelr(std::max(nie_all, 1));
+  for (int j = 0; j < nie_all; ++j) {
+    const int el = d->nod_in_elem2D[j];
+    nel4[j] = make_int4(el, d->elem_nodes[3 * el], d->elem_nodes[3 * el + 1],
+                        d->elem_nodes[3 * el + 2]);
+    nelr[j] = eul[el] | (enl[el] << 8);
+  }
   std::vector<double> Zp(L);
   for (int k = 0; k < L - 1; ++k) Zp[k] = d->Z[k];
   Zp[L - 1] = d->Z[L - 2];
@@ -249,6 +283,8 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   size_t o_eedge = b.add(eedge.data(), eedge.size());
   size_t o_eudoff = b.add(eud_off.data(), eud_off.size());
   size_t o_eudidx = b.add(eud_idx.data(), std::max<size_t>(eud_idx.size(), 1));
+  size_t o_ne4 = b.add(ne4.data(), ne4.size()), o_nel4 = b.add(nel4.data(), nel4.size());
+  size_t o_nelr = b.add(nelr.data(), nelr.size());
   size_t o_Zp = b.add(Zp.data(), L), o_zbar = b.add(d->zbar, L);
   size_t o_if = b.add(iface.data(), iface.size()), o_ly = b.add(layer.data(), layer.size());
   size_t o_ed = b.add(edgel.data(), edgel.size()), o_el = b.add(eleml.data(), eleml.size());
@@ -285,6 +321,9 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   m.eud_off = (const int*)(base + o_eudoff);
   m.eud_idx = (const int*)(base + o_eudidx);
   m.ekmax = (const int*)(base + o_ekmax);
+  m.ne4 = (const int4*)(base + o_ne4);
+  m.nel4 = (const int4*)(base + o_nel4);
+  m.nelr = (const int*)(base + o_nelr);
   m.Zp = (const double*)(base + o_Zp);
   m.zbar = (const double*)(base + o_zbar);
   m.iface_lanes = (const uint32_t*)(base + o_if);  m.n_iface = int64_t(iface.size());
@@ -350,6 +389,12 @@ int fct_plan_info(const FctPlan* P, int64_t out[8]) {
   return FCT_OK;
 }
 
+int fct_plan_set_fused(FctPlan* P, int fused) {
+  if (!P) return set_error(FCT_ERR_INVALID, "NULL plan");
+  P->fused = fused != 0;
+  return FCT_OK;
+}
+
 int fct_forward(FctPlan* P, const FctFields* f, double dt, int ntr, fct_stream_t stream) {
   if (!P || !f) return set_error(FCT_ERR_INVALID, "NULL plan or fields");
   if (ntr < 1) return set_error(FCT_ERR_INVALID, "ntr must be >= 1");
@@ -386,6 +431,7 @@ int fct_forward(FctPlan* P, const FctFields* f, double dt, int ntr, fct_stream_t
   dims.per_thread = 8;
   dims.any_wi = f->w_i != nullptr;
   dims.copy_dry = true;   // a fresh T_new: dry levels keep T (tracer_adv.py:147-151)
+  dims.fused = P->fused;
   int prev = -1;
   cudaGetDevice(&prev);
   if (prev != P->device) cudaSetDevice(P->device);

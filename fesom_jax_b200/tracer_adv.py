@@ -69,6 +69,10 @@ class FctPlan:
     def reserve(self, ntr: int) -> None:
         _lib.check(_lib.lib().fct_plan_reserve(self._h, int(ntr)))
 
+    def set_fused(self, fused: bool) -> None:
+        """Fused stage kernels (default) or one kernel per reference stage; same bits."""
+        _lib.check(_lib.lib().fct_plan_set_fused(self._h, int(bool(fused))))
+
     def close(self) -> None:
         if getattr(self, "_h", None) is not None and self._h.value:
             _lib.lib().fct_plan_destroy(self._h)

@@ -104,6 +104,11 @@ int fct_plan_reserve(FctPlan* plan, int max_tracers);
 /* Counts: [nod2D, elem2D, edge2D, nl, wet node layers, wet element layers, wet edge
  * layers, max_tracers]. */
 int fct_plan_info(const FctPlan* plan, int64_t out[8]);
+/* Which stage kernels fct_forward runs: fused (1, the default: 4 launches per tracer
+ * chunk, element gradients and cluster bounds recomputed instead of stored) or one kernel
+ * per reference stage (0: 7 launches, every intermediate written to the workspace, the
+ * form the reverse pass recomputes). Both give the same T_new bit for bit. */
+int fct_plan_set_fused(FctPlan* plan, int fused);
 
 /* One FCT step for ``ntr`` tracers: fesom_jax/tracer_adv.py:532-578 (advect_one_fct),
  * with exch=None. Writes T_new; T_old_new is T itself (the caller keeps the alias). */

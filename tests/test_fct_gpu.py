@@ -129,3 +129,37 @@ def test_dry_levels_keep_T_exactly(torch, pi, pi_cases):
     ref, _ = fct_np.advect_one_fct(pi, c["uv"], c["w_e"], c["helem"], c["hnode"],
                                    c["hnode_new"], T, To, dt=DT)
     assert np.max(np.abs(got[0][lm] - ref[lm])) / np.max(np.abs(ref[lm])) <= RTOL
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_fused_equals_unfused(torch, pi, pi_cases, name):
+    """The fused stage kernels (the default) and one kernel per reference stage give the
+    same T_new (equal values; max/min of +-0 may differ in the sign of a zero)."""
+    from fesom_jax_b200.tracer_adv import get_plan
+    plan = get_plan(pi, 0)
+    c = pi_cases[name]
+    try:
+        plan.set_fused(False)
+        ref = run_gpu(torch, pi, c)
+    finally:
+        plan.set_fused(True)
+    got = run_gpu(torch, pi, c)
+    assert np.array_equal(got, ref)
+
+
+def test_fused_equals_unfused_generated_mesh(torch):
+    from fesom_jax_b200 import inputs as I
+    from fesom_jax_b200 import meshgen
+    from fesom_jax_b200.tracer_adv import advect_one_fct, get_plan
+    m = meshgen.make_mesh(2000, seed=11, name="gen2000")
+    f = I.make_fields(m, seed=4, n_passive=3, ab2=True)
+    args = [_dev(torch, x) for x in (f.uv, f.w_e, f.helem, f.hnode, f.hnode_new,
+                                     f.tracers, f.tracers_old)]
+    plan = get_plan(m, 0)
+    try:
+        plan.set_fused(False)
+        ref = advect_one_fct(m, *args, dt=DT)[0].cpu().numpy()
+    finally:
+        plan.set_fused(True)
+    got = advect_one_fct(m, *args, dt=DT)[0].cpu().numpy()
+    assert np.array_equal(got, ref)
