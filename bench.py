@@ -198,6 +198,7 @@ def run_ours(args, D: Dist) -> dict | None:
                        inp["hnode_new"], inp["T"], inp["T_old"], cfg["dt"])
         member_inputs.append(inp if i == 0 else None)
         del inp
+    torch.cuda.empty_cache()   # hand the input temporaries back before the arena is allocated
     ens.build()
     info = ens.info()
     S = cfg["fct_steps"]
@@ -270,12 +271,20 @@ def run_ours(args, D: Dist) -> dict | None:
         tp = e0.elapsed_time(e1) / 1e3
         out["plain"] = dict(value=reps * cfg["ntr"] * mesh.n_wet_layers / tp, unit=UNIT,
                             how="fct_forward, 1 tracer per call, 1 FCT step per call")
+    ens.close()   # the end-to-end run below builds its own ensemble
+    del ens
+    torch.cuda.empty_cache()
+    if D.rank == 0 and member_inputs[0] is not None:
+        inp = member_inputs[0]
+        if not args.no_cpu:
+            host = {k: (v.cpu().numpy() if hasattr(v, "cpu") else v) for k, v in inp.items()}
+        member_inputs.clear()
+        del inp
+        torch.cuda.empty_cache()
         if not args.no_e2e:
             out["e2e"] = e2e_host(args, mesh, cfg, dev)
         if not args.no_cpu:
-            host = {k: (v.cpu().numpy() if hasattr(v, "cpu") else v) for k, v in inp.items()}
             out["cpu_baseline"] = cpu_oracle_rate(mesh, host, cfg["ntr"], cfg["dt"])
-    ens.close()
     return out
 
 
@@ -302,6 +311,7 @@ def e2e_host(args, mesh, cfg, dev) -> dict:
             host[-1][k] = inp[k].permute(1, 2, 0).contiguous().cpu().pin_memory()
         host[-1]["out"] = torch.empty_like(host[-1]["T"]).pin_memory()
         del inp
+    torch.cuda.empty_cache()
     ens.build()
     S = cfg["fct_steps"]
     stream = torch.cuda.current_stream(dev)
@@ -336,6 +346,137 @@ def e2e_host(args, mesh, cfg, dev) -> dict:
     return dict(value=upd / t, unit=UNIT, h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h,
                 members=nm, steps=reps, wall_s=wall,
                 how="Ensemble API, pinned host buffers in/out every step")
+
+
+# ---------------------------------------------------------------- adjoint (config 3)
+def run_adjoint(args, D: Dist) -> dict:
+    """Gradient of loss = sum_n areasvol[n,0] (T_K[n,0] - target_n)^2 after K = 10 FCT
+    steps on the CORE2-size mesh, w.r.t. the initial T and uv, with w_e = compute_w(uv)
+    inside the loss (chain_loss_and_grad: per-step recomputation checkpointing). Reports
+    its cost against the forward alone (compute_w + K steps) and central finite
+    differences (eps = 1e-7) along 20 seeded directions (10 for T0, 10 for uv).
+
+    The velocities here are white noise (sigma 0.002 m/s, vertical CFL < 1): a
+    streamfunction flow is
+    discretely divergence-free, so w = compute_w(uv) is roundoff and the upwind |w| sits
+    at its kink, where central differences and any subgradient disagree."""
+    import torch
+
+    from fesom_jax_b200 import inputs as I
+    from fesom_jax_b200 import workloads as W
+    from fesom_jax_b200.adjoint import chain_loss_and_grad
+    from fesom_jax_b200.ale import compute_w
+    from fesom_jax_b200.tracer_adv import get_plan
+    torch.cuda.set_device(D.local_rank)
+    dev = torch.device("cuda", D.local_rank)
+    mesh = W.make_workload_mesh("batched", seed=0)
+    K, dt = 10, 1800.0
+    f = I.make_fields(mesh, seed=3 + D.rank, ab2=True, kind="white", sigma=0.002)
+    d = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev)  # noqa: E731
+    T0, To0, uv = d(f.tracers[0]), d(f.tracers_old[0]), d(f.uv)
+    helem, hn, hnn = d(f.helem), d(f.hnode), d(f.hnode_new)
+    target = torch.from_numpy(np.random.default_rng(7).normal(15.0, 3.0, mesh.nod2D))
+    plan = get_plan(mesh, D.local_rank)
+    stream = torch.cuda.current_stream(dev)
+
+    def forward():
+        w = compute_w(mesh, uv, helem)
+        T, To = T0, To0
+        for _ in range(K):
+            T, To = plan.forward(uv, w, helem, hn, hnn, T, To, dt), T
+        return T
+
+    def grad():
+        return chain_loss_and_grad(mesh, T0, uv, helem, hn, hnn, target, K, dt=dt, T_old0=To0)
+
+    def timed(fn, reps):
+        for _ in range(max(args.warmup, 1)):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps / 1e3
+
+    D.barrier()
+    t_fwd = timed(forward, args.steps)
+    t_grad = timed(grad, args.steps)
+    t = D.max(t_grad, dev)
+    loss, gT0, guv = grad()
+    # central finite differences
+    rng = np.random.default_rng(2024)
+    lm = torch.from_numpy(mesh.node_layer_mask).to(dev)
+    em = torch.from_numpy(mesh.elem_layer_mask).to(dev)[:, :, None]
+    rel = []
+    eps = 1e-7
+    for j in range(0 if args.no_fd else 20):
+        if j < 10:
+            v = d(rng.normal(size=T0.shape)) * lm
+            Lp = chain_loss_and_grad(mesh, T0 + eps * v, uv, helem, hn, hnn, target, K, dt=dt,
+                                     T_old0=To0)[0]
+            Lm = chain_loss_and_grad(mesh, T0 - eps * v, uv, helem, hn, hnn, target, K, dt=dt,
+                                     T_old0=To0)[0]
+            ad = float((gT0 * v).sum())
+        else:
+            v = d(rng.normal(size=uv.shape)) * em
+            Lp = chain_loss_and_grad(mesh, T0, uv + eps * v, helem, hn, hnn, target, K, dt=dt,
+                                     T_old0=To0)[0]
+            Lm = chain_loss_and_grad(mesh, T0, uv - eps * v, helem, hn, hnn, target, K, dt=dt,
+                                     T_old0=To0)[0]
+            ad = float((guv * v).sum())
+        fd = (Lp - Lm) / (2 * eps)
+        rel.append(abs(fd - ad) / max(abs(ad), 1e-300))
+    upd = K * mesh.n_wet_layers * D.world
+    return dict(value=upd / t, t=t * args.steps, mesh=mesh, t_fwd=t_fwd, t_grad=t_grad,
+                cfg=dict(members=1, ntr=1, fct_steps=K, dt=dt),
+                adjoint=dict(forward_ms=t_fwd * 1e3, loss_and_grad_ms=t_grad * 1e3,
+                             ratio=t_grad / t_fwd, K=K, loss=loss,
+                             fd_rel_err_max=float(max(rel)) if rel else None,
+                             fd_rel_err_median=float(np.median(rel)) if rel else None,
+                             fd_directions=len(rel), fd_eps=eps, max_cfl_z=float(I.max_cfl_z(
+                                 mesh, f.w_e, f.hnode, dt)),
+                             how="chain_loss_and_grad (fct_forward x K, fct_adjoint x K, "
+                                 "fct_compute_w_adjoint) vs compute_w + fct_forward x K"))
+
+
+# ---------------------------------------------------------------- serving (config 5)
+def run_serve(args, D: Dist) -> dict:
+    """Continuous-batching serving (ServingEngine): Poisson arrivals at 200 req/s mixing
+    the pi, CORE2-size and 1.3M-node meshes (0.6/0.3/0.1), each request K ~ U{1..50} FCT
+    steps of a resident member (T, S), 20 % with the adjoint of the last step; admission
+    by a 150 GB HBM budget. The offered load is far above one GPU's capacity, so the
+    stream is bounded (``--serve-seconds`` of arrivals) and the run also reports a
+    sustainable-rate stream and the serial plain-launch baseline on the same requests."""
+    import torch
+
+    from fesom_jax_b200 import workloads as W
+    from fesom_jax_b200.mesh import pi_mesh
+    from fesom_jax_b200.serve import ServingEngine, poisson_requests
+    torch.cuda.set_device(D.local_rank)
+    meshes = {"pi": pi_mesh(), "core2": W.make_workload_mesh("batched", seed=0),
+              "large": W.make_workload_mesh("large", seed=0)}
+    dts = {"pi": 3600.0, "core2": 1800.0, "large": 600.0}
+    eng = ServingEngine(meshes, dts, budget_bytes=150e9, device=D.local_rank, ntr=2,
+                        workspace_bytes=45e9, sigma={"large": 0.2})
+    out = {}
+    reqs = poisson_requests(200.0, args.serve_seconds, seed=1 + D.rank)
+    clocks = ClockSampler(gpu_index(D.local_rank))
+    clocks.start()
+    sat = eng.run(reqs, time_limit=args.serve_limit)
+    out["clocks"] = clocks.stop()
+    out["saturated"] = dict(rate_req_s=200.0, arrivals_s=args.serve_seconds, **sat)
+    cap = sat["throughput_req_s"]
+    low = poisson_requests(max(0.5 * cap, 0.2), args.serve_seconds * 4, seed=100 + D.rank)
+    out["sustainable"] = dict(rate_req_s=max(0.5 * cap, 0.2),
+                              **eng.run(low, time_limit=args.serve_limit))
+    out["serial"] = eng.run_serial(reqs, time_limit=args.serve_limit / 2)
+    eng.close()
+    out["value"] = sat["updates_per_s"] * D.world
+    out["t"] = sat["wall_s"]
+    return out
 
 
 # ------------------------------------------------------------------ reference arm
@@ -382,6 +523,28 @@ def run_reference(args, D: Dist):
     print(json.dumps(line), flush=True)
 
 
+def side_line(args, D: Dist, r: dict) -> dict:
+    """The JSON line of the adjoint and serving workloads."""
+    line = dict(metric=METRIC, value=r["value"], unit=UNIT, n_gpus=D.world, steps=args.steps,
+                warmup=args.warmup, ms_per_step=r["t"] / max(args.steps, 1) * 1e3,
+                higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64",
+                data="synthetic (seeded mesh, velocities and tracers)")
+    if args.config == "adjoint":
+        m = r["mesh"]
+        line["config"] = dict(workload=f"adjoint: 10-step loss gradient (T0, uv), {m.name} mesh",
+                              nod2D=m.nod2D, nl=m.nl, wet_node_layers=m.n_wet_layers,
+                              tracers=1, fct_steps=10, dt=1800.0,
+                              value_is="forward-equivalent updates/s of the loss+gradient")
+        line["adjoint"] = r["adjoint"]
+    else:
+        line["config"] = dict(workload="serve: Poisson 200 req/s, pi/CORE2/1.3M mix 0.6/0.3/0.1, "
+                                       "K~U{1..50}, 20% adjoint, 150 GB budget, T+S",
+                              value_is="node-level updates/s served (saturated stream)")
+        for k in ("saturated", "sustainable", "serial", "clocks"):
+            line[k] = r[k]
+    return line
+
+
 def workload_config(name, cfg, mesh) -> dict:
     return dict(workload=f"{name}: FCT tracer advection, {mesh.name} mesh", nod2D=mesh.nod2D,
                 elem2D=mesh.elem2D, edge2D=mesh.edge2D, nl=mesh.nl,
@@ -397,7 +560,12 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=["batched", "pi", "large"], default="batched")
+    ap.add_argument("--config", choices=["batched", "pi", "large", "adjoint", "serve"],
+                    default="batched")
+    ap.add_argument("--serve-seconds", type=float, default=2.0,
+                    help="serve: seconds of Poisson arrivals at 200 req/s")
+    ap.add_argument("--serve-limit", type=float, default=90.0,
+                    help="serve: wall-clock cap per stream")
     ap.add_argument("--members", type=int, default=0)
     ap.add_argument("--fct-steps", type=int, default=0)
     ap.add_argument("--ntr", type=int, default=0, help="override tracers per member")
@@ -406,6 +574,7 @@ def main():
     ap.add_argument("--e2e-members", type=int, default=8)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-fd", action="store_true", help="adjoint: skip the FD check")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
@@ -415,10 +584,18 @@ def main():
         return
     D.init("nccl")
     try:
-        r = run_ours(args, D)
+        if args.config == "adjoint":
+            r = run_adjoint(args, D)
+        elif args.config == "serve":
+            r = run_serve(args, D)
+        else:
+            r = run_ours(args, D)
     finally:
         D.close()
     if D.rank != 0 or r is None:
+        return
+    if args.config in ("adjoint", "serve"):
+        print(json.dumps(side_line(args, D, r)), flush=True)
         return
     cfg, mesh = r["cfg"], r["mesh"]
     line = dict(metric=METRIC, value=r["value"], unit=UNIT, n_gpus=D.world, steps=args.steps,

@@ -762,7 +762,7 @@ int fct_plan_reserve_adjoint(FctPlan* P, int max_tracers) {
   if (!P) return set_error(FCT_ERR_INVALID, "plan is NULL");
   if (max_tracers < 1) return set_error(FCT_ERR_INVALID, "max_tracers must be >= 1");
   if (max_tracers <= P->adj_tracers) return FCT_OK;
-  int st = fct_plan_reserve(P, max_tracers);
+  int st = plan_reserve_ws(P, max_tracers, /*full=*/true);   // the recompute keeps every field
   if (st) return st;
   FCT_CUDA(cudaSetDevice(P->device));
   const int64_t sN = int64_t(P->N) * P->L, sE = int64_t(P->E) * P->L, sEd = int64_t(P->Ed) * P->L;

@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <map>
 #include <mutex>
+#include <tuple>
 #include <utility>
 #include <vector>
 
@@ -375,11 +376,15 @@ int fct_serve_step(FctServe* S, const FctInstance* insts, const int32_t* phases,
     return set_error(FCT_ERR_CAPACITY, "%d instances exceed the serve table (%d)", n,
                      S->max_instances);
   if (n == 0) return FCT_OK;
-  // order instances by ntr so that each launch group has one ntr
+  // order instances by (ntr, mesh): a launch group holds one ntr and one mesh, so its
+  // grid is sized for that mesh (a pi-size instance never rides a 1.3M-node grid)
   std::vector<int> order(n);
   for (int i = 0; i < n; ++i) order[i] = i;
-  std::stable_sort(order.begin(), order.end(),
-                   [&](int a, int b) { return insts[a].ntr < insts[b].ntr; });
+  auto key = [&](int i) {
+    const FctPlan* P = insts[i].plan;
+    return std::make_tuple(insts[i].ntr, P ? P->hm.n_layer : 0, reinterpret_cast<uintptr_t>(P));
+  };
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key(a) < key(b); });
   int64_t need = 0;
   for (int i = 0; i < n; ++i) {
     const FctInstance& q = insts[i];
@@ -431,7 +436,8 @@ int fct_serve_step(FctServe* S, const FctInstance* insts, const int32_t* phases,
     int j1 = j0;
     LaunchDims d{};
     const int ntr = insts[order[j0]].ntr;
-    while (j1 < n && insts[order[j1]].ntr == ntr) {
+    const FctPlan* P0 = insts[order[j0]].plan;
+    while (j1 < n && insts[order[j1]].ntr == ntr && insts[order[j1]].plan == P0) {
       const FctPlan* P = insts[order[j1]].plan;
       d.max_iface = std::max(d.max_iface, P->hm.n_iface);
       d.max_layer = std::max(d.max_layer, P->hm.n_layer);

@@ -139,6 +139,7 @@ struct FctPlan {
   void* d_static = nullptr;        // one allocation for all static arrays
   int max_tracers = 0;
   bool fused = true;               // fct_forward runs the fused stage kernels
+  bool ws_full = false;            // workspace holds every stage field (unfused / adjoint)
   double* d_ws = nullptr;          // workspace allocation
   fct::Workspace ws{};
   int64_t n_wet_elem_layers = 0;

@@ -73,6 +73,24 @@ Workspace carve_workspace(double* base, int64_t N, int64_t E, int64_t Ed, int64_
   return w;
 }
 
+int plan_reserve_ws(FctPlan* P, int ntr, bool full) {
+  if (ntr <= P->max_tracers && (P->ws_full || !full)) return FCT_OK;
+  ntr = std::max(ntr, P->max_tracers);
+  full = full || P->ws_full;
+  FCT_CUDA(cudaSetDevice(P->device));
+  const int64_t nd = full ? workspace_doubles(P->N, P->E, P->Ed, P->L, ntr)
+                          : workspace_doubles_fused(P->N, P->Ed, P->L, ntr);
+  double* ws = nullptr;
+  FCT_CUDA(cudaMalloc(&ws, size_t(nd) * sizeof(double)));
+  Workspace w = carve_workspace(ws, P->N, P->E, P->Ed, P->L, ntr, /*fused=*/!full);
+  if (P->d_ws) cudaFree(P->d_ws);
+  P->d_ws = ws;
+  P->ws = w;
+  P->max_tracers = ntr;
+  P->ws_full = full;
+  return FCT_OK;
+}
+
 namespace {
 
 struct Blob {
@@ -355,17 +373,7 @@ int fct_plan_destroy(FctPlan* P) {
 int fct_plan_reserve(FctPlan* P, int max_tracers) {
   if (!P) return set_error(FCT_ERR_INVALID, "plan is NULL");
   if (max_tracers < 1) return set_error(FCT_ERR_INVALID, "max_tracers must be >= 1");
-  if (max_tracers <= P->max_tracers) return FCT_OK;
-  FCT_CUDA(cudaSetDevice(P->device));
-  const int64_t nd = workspace_doubles(P->N, P->E, P->Ed, P->L, max_tracers);
-  double* ws = nullptr;
-  FCT_CUDA(cudaMalloc(&ws, size_t(nd) * sizeof(double)));
-  Workspace w = carve_workspace(ws, P->N, P->E, P->Ed, P->L, max_tracers);
-  if (P->d_ws) cudaFree(P->d_ws);
-  P->d_ws = ws;
-  P->ws = w;
-  P->max_tracers = max_tracers;
-  return FCT_OK;
+  return plan_reserve_ws(P, max_tracers, !P->fused);
 }
 
 int fct_plan_create(const FctMeshDesc* desc, int device, int max_tracers, FctPlan** out) {
@@ -391,6 +399,10 @@ int fct_plan_info(const FctPlan* P, int64_t out[8]) {
 
 int fct_plan_set_fused(FctPlan* P, int fused) {
   if (!P) return set_error(FCT_ERR_INVALID, "NULL plan");
+  if (!fused) {   // the unfused stages need every stage field
+    const int st = plan_reserve_ws(P, P->max_tracers, true);
+    if (st) return st;
+  }
   P->fused = fused != 0;
   return FCT_OK;
 }

@@ -143,7 +143,7 @@ class ServingEngine:
         for name in self.adjoint_meshes:
             from .adjoint import _bind as _bind_adj
             _lib.check(_bind_adj(self.L).fct_plan_reserve_adjoint(self.meshes[name].plan.handle,
-                                                                 ntr))
+                                                                 1))
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
@@ -159,15 +159,16 @@ class ServingEngine:
 
     # -------------------------------------------------------------- members
     def ws_need(self, r: Request) -> int:
+        """Doubles of the fused-stage workspace one instance takes in the arena."""
         m = self.meshes[r.mesh].mesh
-        N, E, Ed, L = m.nod2D, m.elem2D, m.edge2D, m.nl
-        return Ed * L + self.ntr * (4 * E * L + 9 * N * L + Ed * L)
+        N, Ed, L = m.nod2D, m.edge2D, m.nl
+        return Ed * L + self.ntr * (6 * N * L + Ed * L)
 
     def state_bytes(self, r: Request) -> int:
         m = self.meshes[r.mesh].mesh
         b = 3 * m.nod2D * m.nl * self.ntr * 8
-        if r.adjoint and r.mesh in self.adjoint_meshes:
-            b += 6 * m.nod2D * m.nl * self.ntr * 8 + 2 * m.elem2D * m.nl * 8
+        if r.adjoint and r.mesh in self.adjoint_meshes:   # tracer-0 VJP buffers
+            b += 6 * m.nod2D * m.nl * 8 + 2 * m.elem2D * m.nl * 8
         return b
 
     def init_state(self, r: Request):
@@ -208,7 +209,9 @@ class ServingEngine:
         return q
 
     def _adjoint(self, r: Request, stream, after_event):
-        """VJP of the request's last step for the loss sum_n areasvol[n,0] T_K[n,0]^2 / 2."""
+        """VJP of the request's last step for the loss sum_n areasvol[n,0] T_K[n,0]^2 / 2.
+        The loss reads tracer 0 only and the tracers of a step are independent, so the VJP
+        runs on tracer 0 (the other tracers' cotangents are zero)."""
         torch = self.torch
         from .adjoint import advect_one_fct_vjp
         e = self.meshes[r.mesh]
@@ -216,11 +219,11 @@ class ServingEngine:
         p = r.K   # phase after K steps
         with torch.cuda.stream(stream):
             stream.wait_event(after_event)
-            TK = r.state[(p + 1) % 3].permute(2, 0, 1)
-            Tm1 = r.state[p % 3].permute(2, 0, 1).contiguous()
-            Tm2 = r.state[(p + 2) % 3].permute(2, 0, 1).contiguous()
+            TK = r.state[(p + 1) % 3][:, :, 0]
+            Tm1 = r.state[p % 3][:, :, 0].contiguous()
+            Tm2 = r.state[(p + 2) % 3][:, :, 0].contiguous()
             gTn = torch.zeros_like(Tm1)
-            gTn[0, :, 0] = e.av0 * TK[0, :, 0]
+            gTn[:, 0] = e.av0 * TK[:, 0]
             gT, _, guv, _ = advect_one_fct_vjp(e.mesh, uv, w, e.thick.helem, e.thick.hnode,
                                                e.thick.hnode_new, Tm1, Tm2, gTn, dt=e.dt)
             r.grad = (gT, guv)
@@ -338,18 +341,22 @@ class ServingEngine:
             st = self.init_state(r)
             T = st[1].permute(2, 0, 1).contiguous()
             To = T.clone()
+            Tm2 = To
             torch.cuda.synchronize(self.dev)
             t0 = time.perf_counter()
-            for _ in range(r.K):
-                Tn = e.plan.forward(uv, w, e.thick.helem, e.thick.hnode, e.thick.hnode_new, T,
-                                    To, e.dt)
-                To, T = T, Tn
+            for _ in range(r.K):   # one tracer per call, the reference's granularity
+                Tn = torch.empty_like(T)
+                for t in range(self.ntr):
+                    e.plan.forward(uv, w, e.thick.helem, e.thick.hnode, e.thick.hnode_new,
+                                   T[t], To[t], e.dt, out=Tn[t])
+                Tm2, To, T = To, T, Tn
             if r.adjoint and r.mesh in self.adjoint_meshes:
                 from .adjoint import advect_one_fct_vjp
-                gTn = torch.zeros_like(T)
-                gTn[0, :, 0] = e.av0 * T[0, :, 0]
+                gTn = torch.zeros_like(T[0])
+                gTn[:, 0] = e.av0 * T[0, :, 0]
                 advect_one_fct_vjp(e.mesh, uv, w, e.thick.helem, e.thick.hnode,
-                                   e.thick.hnode_new, To, To, gTn, dt=e.dt)
+                                   e.thick.hnode_new, To[0].contiguous(), Tm2[0].contiguous(),
+                                   gTn, dt=e.dt)
             torch.cuda.synchronize(self.dev)
             service.append((r, time.perf_counter() - t0))
             del st, T, To

@@ -135,7 +135,7 @@ def get_plan(mesh: Mesh, device: int = 0) -> FctPlan:
         per = _plans.setdefault(mesh, {})
         p = per.get(device)
         if p is None:
-            p = per[device] = FctPlan(mesh, device)
+            p = per[device] = FctPlan(mesh, device, max_tracers=1)   # grows on demand
         return p
 
 

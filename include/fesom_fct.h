@@ -211,8 +211,8 @@ int fct_batch_run(FctBatch* b, int first_phase, int steps, fct_stream_t stream);
  * workspace arena (carved per call in instance order; a call whose instances need more
  * returns FCT_ERR_CAPACITY) and a device instance table uploaded from pinned host memory.
  * Instance i steps with rotation phase ``phases[i]`` (same convention as fct_batch_step).
- * Instances with different ntr are launched in separate groups. Calls on one FctServe
- * must be ordered on one stream.
+ * Instances are launched in groups of one ntr and one mesh (each group's grid is sized
+ * for its mesh). Calls on one FctServe must be ordered on one stream.
  */
 typedef struct FctServe FctServe;
 int fct_serve_create(int device, int max_instances, int64_t workspace_bytes, FctServe** out);
