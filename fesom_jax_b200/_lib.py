@@ -6,6 +6,7 @@ Loading fails loudly when the library is missing: there is no CPU fallback.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
 import numpy as np
@@ -56,10 +57,12 @@ def lib() -> C.CDLL:
     global _lib
     if _lib is not None:
         return _lib
-    if not LIB_PATH.exists():
-        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m fesom_jax_b200.build` "
+    # FESOM_FCT_LIB: load another build of the same library (e.g. for A/B timing)
+    path = Path(os.environ.get("FESOM_FCT_LIB", str(LIB_PATH)))
+    if not path.exists():
+        raise ImportError(f"{path} is missing: build it with `python -m fesom_jax_b200.build` "
                           "(the FCT path has no CPU fallback)")
-    L = C.CDLL(str(LIB_PATH))
+    L = C.CDLL(str(path))
     L.fct_last_error.restype = C.c_char_p
     L.fct_version.restype = C.c_char_p
     L.fct_plan_create.argtypes = [C.POINTER(FctMeshDesc), C.c_int, C.c_int, C.POINTER(C.c_void_p)]

@@ -23,6 +23,7 @@
 // contiguous chunk in the interleaved layout), so the gathers overlap.
 #include <algorithm>
 
+#include "fct_div.cuh"
 #include "fct_host.h"
 
 namespace fct {
@@ -186,6 +187,7 @@ __device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i, int t0, 
   if (layer) {
     const double hn = ld(in.hnode + qn), hnn = ld(in.hnode_new + qn);
     const double av = ld(m.areasvol + qn);
+    const Rcp rav = rcp(av), rhn = rcp(hnn);   // shared by the NTR quotients below
     const double dt = in.dt;
     double fvk1[NTR];
     if (layer1) {
@@ -243,7 +245,8 @@ __device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i, int t0, 
     double lo[NTR];
 #pragma unroll
     for (int t = 0; t < NTR; ++t)
-      lo[t] = valid ? (Tc[t] * hn + (div[t] + (fvk[t] - fvk1[t])) * dt / av) / hnn : 0.0;
+      lo[t] = valid ? divr(Tc[t] * hn + divr((div[t] + (fvk[t] - fvk1[t])) * dt, rav), rhn)
+                    : 0.0;
     stn<NTR, IL>(in.ws.lo, qn, w0, in.ws.sN, in.wtg, lo);
     // _node_avg_grad: area-weighted mean over the node's active elements
     double nx[NTR], ny[NTR], den = 0.0;
@@ -282,11 +285,11 @@ __device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i, int t0, 
         }
       }
     }
-    const double dd = den > 0.0 ? den : 1.0;
+    const Rcp rdd = rcp(den > 0.0 ? den : 1.0);
 #pragma unroll
     for (int t = 0; t < NTR; ++t) {
-      nx[t] = nx[t] / dd;
-      ny[t] = ny[t] / dd;
+      nx[t] = divr(nx[t], rdd);
+      ny[t] = divr(ny[t], rdd);
     }
     stn<NTR, IL>(in.ws.gnx, qn, w0, in.ws.sN, in.wtg, nx);
     stn<NTR, IL>(in.ws.gny, qn, w0, in.ws.sN, in.wtg, ny);
@@ -320,7 +323,9 @@ __device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i, int t0, 
       Znz = ld(m.Zp + k); Zm1 = ld(m.Zp + k - 1); Zm2 = ld(m.Zp + k - 2);
       Zp1 = ld(m.Zp + (k + 1 < L ? k + 1 : L - 1)); zb = ld(m.zbar + k);
     }
-    const double dc = safe_nz(Zm1 - Znz), du = safe_nz(Znz - Zp1), dd = safe_nz(Zm2 - Zm1);
+    const Rcp rdc = rcp(safe_nz(Zm1 - Znz)), rdu = rcp(safe_nz(Znz - Zp1)),
+              rdd = rcp(safe_nz(Zm2 - Zm1));
+    const Rcp r3{3.0, 1.0 / 3.0, true};
     double To[NTR], Tom[NTR], Tm2[NTR], Tom2[NTR], Tp[NTR], Top[NTR];
     ldn<NTR, IL>(in.T_old, qn, t0, ts, tg, To);
     ldn<NTR, IL>(in.T_old, qn - 1, t0, ts, tg, Tom);
@@ -332,11 +337,11 @@ __device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i, int t0, 
     for (int t = 0; t < NTR; ++t) {
       const double A0 = ab2(Tc[t], To[t]), Am1 = ab2(Ta[t], Tom[t]);
       const double Am2 = ab2(Tm2[t], Tom2[t]), Ap1 = ab2(Tp[t], Top[t]);
-      const double qc = (Am1 - A0) / dc;
-      const double qu = (A0 - Ap1) / du;
-      const double qd = (Am2 - Am1) / dd;
-      const double Tmean1 = A0 + (2.0 * qc + qu) * (zb - Znz) / 3.0;
-      const double Tmean2 = Am1 + (2.0 * qc + qd) * (zb - Zm1) / 3.0;
+      const double qc = divr(Am1 - A0, rdc);
+      const double qu = divr(A0 - Ap1, rdu);
+      const double qd = divr(Am2 - Am1, rdd);
+      const double Tmean1 = A0 + divr((2.0 * qc + qu) * (zb - Znz), r3);
+      const double Tmean2 = Am1 + divr((2.0 * qc + qd) * (zb - Zm1), r3);
       hi[t] = -0.5 * (Tmean1 + Tmean2) * Wf * area_k;
     }
   }
@@ -436,13 +441,14 @@ __device__ __forceinline__ void body_edge_adf(const Inst& in, int64_t i, int t0,
     ldn<NTR, IL>(in.ws.gny, q2, w0, in.ws.sN, in.wtg, g3);
   }
   double adf[NTR];
+  const Rcp r6{6.0, 1.0 / 6.0, true};
 #pragma unroll
   for (int t = 0; t < NTR; ++t) {
     const double fl = -0.5 * (T1[t] * (vf + avf) + T2[t] * (vf - avf));
     const double A1 = ab2(T1[t], O1[t]), A2 = ab2(T2[t], O2[t]);
     const double diff = A2 - A1;
-    const double Tm1 = A1 + (2.0 * diff + c1 * g0[t] + c2 * g2[t]) / 6.0;
-    const double Tm2 = A2 - (2.0 * diff + c1 * g1[t] + c2 * g3[t]) / 6.0;
+    const double Tm1 = A1 + divr(2.0 * diff + c1 * g0[t] + c2 * g2[t], r6);
+    const double Tm2 = A2 - divr(2.0 * diff + c1 * g1[t] + c2 * g3[t], r6);
     const double ho = -0.5 * ((vf + avf) * Tm1 + (vf - avf) * Tm2);
     adf[t] = ho - fl;
   }
@@ -527,6 +533,7 @@ __device__ __forceinline__ void body_node_factors(const Inst& in, int64_t i, int
   const double av = ld(m.areasvol + qn), hnn = ld(in.hnode_new + qn);
   const bool valid = (av > 0.0) && (hnn > 0.0);
   const double sa = av > 0.0 ? av : 1.0, sh = hnn > 0.0 ? hnn : 1.0;
+  const Rcp rsa = rcp(sa), rsh = rcp(sh);
   const double dt = in.dt;
   const int64_t sN = in.ws.sN;
   double tmax[NTR], tmin[NTR];
@@ -572,8 +579,8 @@ __device__ __forceinline__ void body_node_factors(const Inst& in, int64_t i, int
     pf[t] = 1.0;
     mf[t] = 1.0;
     if (valid) {
-      const double flux_pos = plus * dt / sa / sh + kFluxEps;
-      const double flux_neg = minus * dt / sa / sh - kFluxEps;
+      const double flux_pos = divr(divr(plus * dt, rsa), rsh) + kFluxEps;
+      const double flux_neg = divr(divr(minus * dt, rsa), rsh) - kFluxEps;
       pf[t] = fmin(1.0, (tmax[t] - lo[t]) / flux_pos);
       mf[t] = fmin(1.0, (tmin[t] - lo[t]) / flux_neg);
     }
@@ -669,6 +676,7 @@ __device__ __forceinline__ void node_limit(const Inst& in, int64_t lane, bool co
   const double av = ld(m.areasvol + qn), hnn = ld(in.hnode_new + qn);
   const bool valid_n = (av > 0.0) && (hnn > 0.0);
   const double sa = av > 0.0 ? av : 1.0, sh = hnn > 0.0 ? hnn : 1.0;
+  const Rcp rsa = rcp(sa), rsh = rcp(sh);
   const double dt = in.dt;
   double ft[NTR], fb[NTR];
   ldn<NTR, IL>(in.ws.adfv, qn, w0, sN, in.wtg, ft);
@@ -681,8 +689,8 @@ __device__ __forceinline__ void node_limit(const Inst& in, int64_t lane, bool co
     pf[t] = 1.0;
     mf[t] = 1.0;
     if (valid_n) {
-      const double flux_pos = plus * dt / sa / sh + kFluxEps;
-      const double flux_neg = minus * dt / sa / sh - kFluxEps;
+      const double flux_pos = divr(divr(plus * dt, rsa), rsh) + kFluxEps;
+      const double flux_neg = divr(divr(minus * dt, rsa), rsh) - kFluxEps;
       pf[t] = fmin(1.0, (mx[t] - lo[t]) / flux_pos);
       mf[t] = fmin(1.0, (mn[t] - lo[t]) / flux_neg);
     }
@@ -703,6 +711,7 @@ __device__ __forceinline__ void body_node_final(const Inst& in, int64_t i, int t
   const double av = ld(m.areasvol + qn);
   const double sa = av > 0.0 ? av : 1.0;
   const double hn = ld(in.hnode + qn), hnn = ld(in.hnode_new + qn);
+  const Rcp rsa = rcp(sa), rhn = rcp(hnn);
   const double dt = in.dt;
   const int tg = in.tg;
   const int64_t sN = in.ws.sN;
@@ -789,10 +798,10 @@ __device__ __forceinline__ void body_node_final(const Inst& in, int64_t i, int t
 #pragma unroll
   for (int t = 0; t < NTR; ++t) {
     const double lo_trans = -Tv[t] * hn + lo[t] * hnn;
-    const double vdiv = av > 0.0 ? (vt[t] - vb[t]) * dt / sa : 0.0;
-    double d = hsc[t] * dt / sa + (lo_trans + vdiv);
+    const double vdiv = av > 0.0 ? divr((vt[t] - vb[t]) * dt, rsa) : 0.0;
+    double d = divr(hsc[t] * dt, rsa) + (lo_trans + vdiv);
     d = d + Tv[t] * (hn - hnn);
-    out[t] = Tv[t] + (hnn > 0.0 ? d / hnn : 0.0);
+    out[t] = Tv[t] + (hnn > 0.0 ? divr(d, rhn) : 0.0);
   }
   stn<NTR, IL>(in.T_new, qn, t0, in.tstride, tg, out);
 }

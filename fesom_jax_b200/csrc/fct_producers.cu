@@ -7,6 +7,9 @@
 // reference's segment_sum over the flattened [edge, 2] contributions adds them), then a
 // bottom-to-top running sum gives w, divided by ``area`` (safe where 0) and masked to the
 // node's interfaces.
+#include <algorithm>
+
+#include "fct_div.cuh"
 #include "fct_host.h"
 
 using namespace fct;
@@ -63,4 +66,33 @@ extern "C" int fct_compute_w(FctPlan* P, const double* uv, const double* helem, 
   cudaError_t e = cudaGetLastError();
   if (prev >= 0 && prev != P->device) cudaSetDevice(prev);
   return e == cudaSuccess ? FCT_OK : cuda_error(e, "compute_w launch");
+}
+
+namespace {
+
+// divr (shared-reciprocal division) against the native IEEE division, bit for bit
+__global__ void __launch_bounds__(256) k_div_check(const double* __restrict__ x,
+                                                   const double* __restrict__ y, int64_t n,
+                                                   unsigned long long* result) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    const double a = x[i] / y[i];
+    const double b = fct::divr(x[i], fct::rcp(y[i]));
+    if (__double_as_longlong(a) != __double_as_longlong(b)) {
+      atomicAdd(result, 1ull);
+      atomicMin(result + 1, static_cast<unsigned long long>(i));
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" int fct_div_check(const double* x, const double* y, int64_t n,
+                             unsigned long long* result, fct_stream_t stream) {
+  if (!x || !y || !result || n < 0) return set_error(FCT_ERR_INVALID, "invalid argument");
+  if (n == 0) return FCT_OK;
+  const int64_t blocks = std::min<int64_t>((n + 255) / 256, 148 * 16);
+  k_div_check<<<unsigned(blocks), 256, 0, static_cast<cudaStream_t>(stream)>>>(x, y, n, result);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? FCT_OK : cuda_error(e, "div_check launch");
 }

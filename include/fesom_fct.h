@@ -220,6 +220,16 @@ int fct_serve_destroy(FctServe* s);
 int fct_serve_step(FctServe* s, const FctInstance* insts, const int32_t* phases, int n,
                    fct_stream_t stream);
 
+/* Self-check of the division the kernels use for quotients that share a divisor (the
+ * divisor's reciprocal computed once, then an FMA correction per quotient; see
+ * fesom_jax_b200/csrc/fct_div.cuh): compares it with the native IEEE division for the n
+ * device pairs x[i] / y[i] and accumulates into the device words result[0] (number of
+ * bitwise mismatches, add) and result[1] (smallest mismatching index, min). The caller
+ * initialises result to {0, UINT64_MAX}. No reference counterpart (the reference divides
+ * with XLA's IEEE division); test infrastructure for the kernels' arithmetic. */
+int fct_div_check(const double* x, const double* y, int64_t n, unsigned long long* result,
+                  fct_stream_t stream);
+
 /* Profiling aid: run one step of phase ``phase`` stage by stage with CUDA events recorded
  * on ``stream`` between stages, synchronise, and add each stage's time (ms, summed over
  * workspace groups) into ``stage_ms[0..max_stages)`` (needs >= 10 entries). */
