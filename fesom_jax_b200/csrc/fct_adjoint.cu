@@ -16,7 +16,7 @@
 //   adv_flux_hor_ho (:196-225), adv_flux_hor (:96-105), b1 edges   -> r_edge
 //   fill_up_dn_grad (:344-368), _node_avg_grad (:329-341)          -> r_gnode, r_tr
 //   tracer_gradient_elements (:316-326)                            -> r_grad_t
-//   adv_flux_ver_ho (:241-295), adv_flux_ver (:108-120), b1 vertical -> r_column
+//   adv_flux_ver_ho (:241-295), adv_flux_ver (:108-120), b1 vertical -> r_vert_a, r_vert_b
 //   tracer_ab (:59-66), assembly of dT, dT_old                    -> r_final
 //   edge_vflux (:69-93)                                            -> r_uv
 //   ale.compute_w (fesom_jax/ale.py:309-365)                       -> r_w_div, r_w_uv
@@ -166,25 +166,6 @@ __global__ void __launch_bounds__(B) r_factors(Adj A) {
   }
 }
 
-// Forward helper: fct_plus / fct_minus of node-level qn (tracer t).
-__device__ __forceinline__ void plus_minus(const Inst& in, const DevMesh& m, int n, int k,
-                                           int64_t qn, int t, double& plus, double& minus) {
-  const int L = m.L;
-  const int64_t o = t * in.ws.sN;
-  const double ft = in.ws.adfv[o + qn], fb = in.ws.adfv[o + qn + 1];
-  double sp = 0.0, sm = 0.0;
-  for (int j = m.ne_off[n]; j < m.ne_off[n + 1]; ++j) {
-    const int idx = m.ne_idx[j], e = idx >> 1;
-    if (!edge_on(m, e, k)) continue;
-    const double a = in.ws.adfh[t * in.ws.sEd + int64_t(e) * L + k];
-    const double s = (idx & 1) ? -a : a;
-    sp += fmax(s, 0.0);
-    sm += fmin(s, 0.0);
-  }
-  plus = (fmax(ft, 0.0) + fmax(-fb, 0.0)) + sp;
-  minus = (fmin(ft, 0.0) + fmin(-fb, 0.0)) + sm;
-}
-
 // ------------------------------- r_ratio: pf = min(1, fmax_w / flux_pos), likewise mf
 __global__ void __launch_bounds__(B) r_ratio(Adj A) {
   const Inst& in = A.in;
@@ -212,8 +193,7 @@ __global__ void __launch_bounds__(B) r_ratio(Adj A) {
         tmin = fmin(fmin(tn[qn - 1], tn[qn]), tn[qn + 1]);
       }
       const double lo = in.ws.lo[o + qn];
-      double plus, minus;
-      plus_minus(in, m, n, k, qn, t, plus, minus);
+      const double plus = in.ws.fplus[o + qn], minus = in.ws.fminus[o + qn];
       const double fmax_w = tmax - lo, fmin_w = tmin - lo;
       const double flux_pos = plus * dt / sa / sh + kFluxEps;
       const double flux_neg = minus * dt / sa / sh - kFluxEps;
@@ -277,13 +257,6 @@ __global__ void __launch_bounds__(B) r_window(Adj A) {
   }
 }
 
-// value of element el at level k in node clusters: its bound, -+BIG when it has no layer k
-__device__ __forceinline__ double elem_val(const DevMesh& m, const double* amx, int el, int k,
-                                           bool is_max) {
-  if (!elem_on(m, el, k)) return is_max ? -kBig : kBig;
-  return amx[int64_t(el) * m.L + k];
-}
-
 // ------------------- r_cluster: segment_max/min over a node's elements (even split)
 __global__ void __launch_bounds__(B) r_cluster(Adj A) {
   const Inst& in = A.in;
@@ -297,20 +270,11 @@ __global__ void __launch_bounds__(B) r_cluster(Adj A) {
     const double* amin = in.ws.amin + t * in.ws.sE;
     const double vx = amax[int64_t(e) * L + k], vn = amin[int64_t(e) * L + k];
     double gx = 0.0, gn = 0.0;
-    for (int v = 0; v < 3; ++v) {
+    for (int v = 0; v < 3; ++v) {   // tie counts come from the forward recompute
       const int n = m.enodes[3 * e + v];
-      const int64_t qn = int64_t(n) * L + k;
-      const double tvx = in.ws.tvmax[t * in.ws.sN + qn], tvn = in.ws.tvmin[t * in.ws.sN + qn];
-      if (vx == tvx || vn == tvn) {
-        int cx = 0, cn = 0;
-        for (int j = m.nel_off[n]; j < m.nel_off[n + 1]; ++j) {
-          const int el = m.nel_idx[j];
-          cx += elem_val(m, amax, el, k, true) == tvx;
-          cn += elem_val(m, amin, el, k, false) == tvn;
-        }
-        if (vx == tvx) gx += A.a.gtvmax[t * A.a.sN + qn] / cx;
-        if (vn == tvn) gn += A.a.gtvmin[t * A.a.sN + qn] / cn;
-      }
+      const int64_t qn = int64_t(n) * L + k, qt = t * in.ws.sN + qn;
+      if (vx == in.ws.tvmax[qt]) gx += A.a.gtvmax[t * A.a.sN + qn] / int(in.ws.ccx[qt]);
+      if (vn == in.ws.tvmin[qt]) gn += A.a.gtvmin[t * A.a.sN + qn] / int(in.ws.ccn[qt]);
     }
     A.a.gamax[t * A.a.sE + int64_t(e) * L + k] = gx;
     A.a.gamin[t * A.a.sE + int64_t(e) * L + k] = gn;
@@ -337,14 +301,9 @@ __global__ void __launch_bounds__(B) r_bounds(Adj A) {
       const int64_t qe = int64_t(el) * L + k;
       const double ex = in.ws.amax[t * in.ws.sE + qe], en = in.ws.amin[t * in.ws.sE + qe];
       if (mxv != ex && mnv != en) continue;
-      int cx = 0, cn = 0;
-      for (int v = 0; v < 3; ++v) {
-        const int64_t qv = int64_t(m.enodes[3 * el + v]) * L + k;
-        cx += fmax(lo[qv], T[qv]) == ex;
-        cn += fmin(lo[qv], T[qv]) == en;
-      }
-      if (mxv == ex) gx += A.a.gamax[t * A.a.sE + qe] / cx;
-      if (mnv == en) gn += A.a.gamin[t * A.a.sE + qe] / cn;
+      const int64_t qc = t * in.ws.sE + qe;   // tie counts from the forward recompute
+      if (mxv == ex) gx += A.a.gamax[t * A.a.sE + qe] / int(in.ws.ecx[qc]);
+      if (mnv == en) gn += A.a.gamin[t * A.a.sE + qe] / int(in.ws.ecn[qc]);
     }
     const int64_t oa = t * A.a.sN;
     A.a.gLOb[oa + qn] = gx * smax_a(lo[qn], T[qn]) + gn * smin_a(lo[qn], T[qn]);
@@ -500,13 +459,8 @@ __global__ void __launch_bounds__(B) r_tr(Adj A) {
     }
     for (int v = 0; v < 3; ++v) {   // gnode(n) = sum_e a_e tr_e / den(n)
       const int n = m.enodes[3 * el + v];
-      double den = 0.0;
-      for (int j = m.nel_off[n]; j < m.nel_off[n + 1]; ++j) {
-        const int e2 = m.nel_idx[j];
-        if (elem_on(m, e2, k)) den += m.earea[e2];
-      }
-      const double dd = den > 0.0 ? den : 1.0;
       const int64_t qn = int64_t(n) * L + k;
+      const double dd = in.ws.nden[qn];   // the forward's (safe) denominator
       gx += A.a.ggnx[oa + qn] * aw / dd;
       gy += A.a.ggny[oa + qn] * aw / dd;
     }
@@ -537,90 +491,140 @@ __global__ void __launch_bounds__(B) r_grad_t(Adj A) {
   }
 }
 
-// ----------- r_column: vertical fluxes (QR4C HO, upwind LO) and their limiter terms
-__global__ void __launch_bounds__(128) r_column(Adj A) {
+// ------- r_vert_a / r_vert_b: vertical fluxes (QR4C HO, upwind LO) and their limiter terms.
+// r_vert_a (one thread per layer interface j of a node): the cotangent gf of adf_v[j]
+// (limiter application and the plus/minus sums), ghi = gf and gfv = -gf + gdiv terms,
+// stored in the dead r_ratio outputs gtmax / gtmin, and gw[j] complete (only interface
+// j feeds it). r_vert_b (one thread per node level k): gT[k] and gA[k] gathered from the
+// interfaces j = k-1 .. k+2 in ascending j (the order of a column loop over j that
+// scatters into gT / gA), so the per-level sums do not depend on the parallel split.
+__device__ __forceinline__ void qr4c_depths(const Inst& in, const DevMesh& m, int64_t base,
+                                            int j, double& Znz, double& Zm1, double& Zm2,
+                                            double& Zp1, double& zb) {
+  const int L = m.L;
+  if (in.Z3d) {
+    const double* Zc = in.Z3d + base;
+    Znz = Zc[j]; Zm1 = Zc[j - 1]; Zm2 = Zc[j - 2]; Zp1 = Zc[j + 1 < L ? j + 1 : L - 1];
+    zb = in.zbar3[base + j];
+  } else {
+    Znz = m.Zp[j]; Zm1 = m.Zp[j - 1]; Zm2 = m.Zp[j - 2]; Zp1 = m.Zp[j + 1 < L ? j + 1 : L - 1];
+    zb = m.zbar[j];
+  }
+}
+
+__global__ void __launch_bounds__(B) r_vert_a(Adj A) {
   const Inst& in = A.in;
   const DevMesh& m = *in.m;
-  const int64_t n = lane_index();
-  if (n >= m.N) return;
-  const int L = m.L;
+  const int64_t i = lane_index();
+  if (i >= m.n_layer) return;
+  const uint32_t lane = m.layer_lanes[i];
+  const int n = lane_ent(lane), j = lane_lev(lane), L = m.L;
   const int nzmin = m.nzmin[n], nzmax = m.nzmax[n];
-  const int64_t base = n * L;
+  const int64_t base = int64_t(n) * L;
   const double dt = in.dt;
-  double gA[kMaxLevels], gT[kMaxLevels], gw[kMaxLevels];
+  const double w = in.w_e[base + j], area = m.area[base + j];
+  const int jm = j > 0 ? j - 1 : 0;
   for (int t = 0; t < in.ntr; ++t) {
     const double* T = in.T + t * in.tstride + base;
     const double* To = in.T_old + t * in.tstride + base;
     const int64_t o = t * in.ws.sN, oa = t * A.a.sN;
-    const double* adfv = in.ws.adfv + o + base;
     const double* pf = in.ws.pf + o + base;
     const double* mf = in.ws.mf + o + base;
-    const double* gdel = A.a.gdel + oa;
     const double* gplus = A.a.gplus + oa + base;
     const double* gminus = A.a.gminus + oa + base;
     const double* gdiv = A.a.gdiv + oa + base;
-    for (int k = 0; k < L; ++k) gA[k] = gT[k] = gw[k] = 0.0;
-    for (int j = nzmin; j < nzmax; ++j) {   // adf_v[nzmax] == 0: no cotangent flows there
-      const double f = adfv[j];
-      // limiter application at interface j
-      double ae;
-      if (j == nzmin) ae = f >= 0.0 ? pf[j] : mf[j];
-      else ae = f >= 0.0 ? fmin(mf[j - 1], pf[j]) : fmin(pf[j - 1], mf[j]);
-      double gf = gvl_at(m, gdel, base, j, nzmin, nzmax, dt) * ae;
-      // fct_plus / fct_minus vertical terms of layer j (top) and layer j-1 (bottom)
-      gf += gplus[j] * dmax0(f) + gminus[j] * dmin0(f);
-      if (j - 1 >= nzmin) gf -= gplus[j - 1] * dmax0(-f) + gminus[j - 1] * dmin0(-f);
-      // adf_v = hi - fv; LO uses fv[j] (layer j) and -fv[j] (layer j-1)
-      const double ghi = gf;
-      double gfv = -gf + gdiv[j];
-      if (j - 1 >= nzmin) gfv -= gdiv[j - 1];
-      const double w = in.w_e[base + j], area = m.area[base + j];
-      const int jm = j > 0 ? j - 1 : 0;
-      // fv[j] = -0.5 (T[j] (w + |w|) + T[j-1] (w - |w|)) area
-      gT[j] += -0.5 * (w + fabs(w)) * area * gfv;
-      gT[jm] += -0.5 * (w - fabs(w)) * area * gfv;
-      gw[j] += -0.5 * (T[j] * (1.0 + sgn(w)) + T[jm] * (1.0 - sgn(w))) * area * gfv;
-      // hi[j]: QR4C on ttfAB (surface, centred, interior branches)
-      if (j == nzmin) {
-        const double A0 = ab2(T[j], To[j]);
-        gA[j] += -w * area * ghi;
-        gw[j] += -A0 * area * ghi;
-      } else if (j == nzmin + 1 || j == nzmax - 1) {
-        const double Am = ab2(T[j - 1], To[j - 1]), A0 = ab2(T[j], To[j]);
-        gA[j - 1] += -0.5 * w * area * ghi;
-        gA[j] += -0.5 * w * area * ghi;
-        gw[j] += -0.5 * (Am + A0) * area * ghi;
-      } else if (j >= nzmin + 2 && j <= nzmax - 2) {
-        double Znz, Zm1, Zm2, Zp1, zb;
-        if (in.Z3d) {
-          const double* Zc = in.Z3d + base;
-          Znz = Zc[j]; Zm1 = Zc[j - 1]; Zm2 = Zc[j - 2]; Zp1 = Zc[j + 1 < L ? j + 1 : L - 1];
-          zb = in.zbar3[base + j];
-        } else {
-          Znz = m.Zp[j]; Zm1 = m.Zp[j - 1]; Zm2 = m.Zp[j - 2]; Zp1 = m.Zp[j + 1 < L ? j + 1 : L - 1];
-          zb = m.zbar[j];
-        }
-        const double dc = safe_nz(Zm1 - Znz), du = safe_nz(Znz - Zp1), dd = safe_nz(Zm2 - Zm1);
-        const double A0 = ab2(T[j], To[j]), Am1 = ab2(T[j - 1], To[j - 1]);
-        const double Am2 = ab2(T[j - 2], To[j - 2]), Ap1 = ab2(T[j + 1], To[j + 1]);
-        const double qc = (Am1 - A0) / dc, qu = (A0 - Ap1) / du, qd = (Am2 - Am1) / dd;
-        const double Tmean1 = A0 + (2.0 * qc + qu) * (zb - Znz) / 3.0;
-        const double Tmean2 = Am1 + (2.0 * qc + qd) * (zb - Zm1) / 3.0;
-        const double gS = -0.5 * w * area * ghi;
-        gw[j] += -0.5 * (Tmean1 + Tmean2) * area * ghi;
-        const double gq1 = gS * (zb - Znz) / 3.0, gq2 = gS * (zb - Zm1) / 3.0;
-        const double gqc = 2.0 * gq1 + 2.0 * gq2, gqu = gq1, gqd = gq2;
-        gA[j] += gS - gqc / dc + gqu / du;
-        gA[j - 1] += gS + gqc / dc - gqd / dd;
-        gA[j - 2] += gqd / dd;
-        gA[j + 1] += -gqu / du;
+    const double f = in.ws.adfv[o + base + j];
+    double ae;
+    if (j == nzmin) ae = f >= 0.0 ? pf[j] : mf[j];
+    else ae = f >= 0.0 ? fmin(mf[j - 1], pf[j]) : fmin(pf[j - 1], mf[j]);
+    double gf = gvl_at(m, A.a.gdel + oa, base, j, nzmin, nzmax, dt) * ae;
+    gf += gplus[j] * dmax0(f) + gminus[j] * dmin0(f);
+    if (j - 1 >= nzmin) gf -= gplus[j - 1] * dmax0(-f) + gminus[j - 1] * dmin0(-f);
+    const double ghi = gf;
+    double gfv = -gf + gdiv[j];
+    if (j - 1 >= nzmin) gfv -= gdiv[j - 1];
+    A.a.gtmax[oa + base + j] = ghi;
+    A.a.gtmin[oa + base + j] = gfv;
+    double gw = 0.0;
+    gw += -0.5 * (T[j] * (1.0 + sgn(w)) + T[jm] * (1.0 - sgn(w))) * area * gfv;
+    if (j == nzmin) {
+      gw += -ab2(T[j], To[j]) * area * ghi;
+    } else if (j == nzmin + 1 || j == nzmax - 1) {
+      gw += -0.5 * (ab2(T[j - 1], To[j - 1]) + ab2(T[j], To[j])) * area * ghi;
+    } else if (j >= nzmin + 2 && j <= nzmax - 2) {
+      double Znz, Zm1, Zm2, Zp1, zb;
+      qr4c_depths(in, m, base, j, Znz, Zm1, Zm2, Zp1, zb);
+      const double dc = safe_nz(Zm1 - Znz), du = safe_nz(Znz - Zp1), dd = safe_nz(Zm2 - Zm1);
+      const double A0 = ab2(T[j], To[j]), Am1 = ab2(T[j - 1], To[j - 1]);
+      const double Am2 = ab2(T[j - 2], To[j - 2]), Ap1 = ab2(T[j + 1], To[j + 1]);
+      const double qc = (Am1 - A0) / dc, qu = (A0 - Ap1) / du, qd = (Am2 - Am1) / dd;
+      const double Tmean1 = A0 + (2.0 * qc + qu) * (zb - Znz) / 3.0;
+      const double Tmean2 = Am1 + (2.0 * qc + qd) * (zb - Zm1) / 3.0;
+      gw += -0.5 * (Tmean1 + Tmean2) * area * ghi;
+    }
+    A.a.gw[oa + base + j] = gw;
+  }
+}
+
+// contribution of interface j to gA[k] (QR4C on ttfAB)
+__device__ __forceinline__ double ga_term(const Inst& in, const DevMesh& m, int64_t base, int j,
+                                         int k, int nzmin, int nzmax, double ghi) {
+  const double w = in.w_e[base + j], area = m.area[base + j];
+  if (j == nzmin) return k == j ? -w * area * ghi : 0.0;
+  if (j == nzmin + 1 || j == nzmax - 1)
+    return (k == j - 1 || k == j) ? -0.5 * w * area * ghi : 0.0;
+  double Znz, Zm1, Zm2, Zp1, zb;
+  qr4c_depths(in, m, base, j, Znz, Zm1, Zm2, Zp1, zb);
+  const double dc = safe_nz(Zm1 - Znz), du = safe_nz(Znz - Zp1), dd = safe_nz(Zm2 - Zm1);
+  const double gS = -0.5 * w * area * ghi;
+  const double gq1 = gS * (zb - Znz) / 3.0, gq2 = gS * (zb - Zm1) / 3.0;
+  const double gqc = 2.0 * gq1 + 2.0 * gq2, gqu = gq1, gqd = gq2;
+  if (k == j) return gS - gqc / dc + gqu / du;
+  if (k == j - 1) return gS + gqc / dc - gqd / dd;
+  if (k == j - 2) return gqd / dd;
+  return -gqu / du;   // k == j + 1
+}
+
+__global__ void __launch_bounds__(B) r_vert_b(Adj A) {
+  const Inst& in = A.in;
+  const DevMesh& m = *in.m;
+  const int64_t i = lane_index();
+  const int64_t NL = int64_t(m.N) * m.L;
+  if (i >= NL) return;
+  const int L = m.L;
+  const int n = int(i / L), k = int(i - int64_t(n) * L);
+  const int nzmin = m.nzmin[n], nzmax = m.nzmax[n];
+  const int64_t base = int64_t(n) * L;
+  const bool layer = k >= nzmin && k < nzmax;
+  // the upwind LO flux of interface j adds to gT[j] and gT[jm], jm = max(j - 1, 0), so
+  // level k takes interface k (layers only) and interface k+1 (also k = nzmin - 1, dry)
+  const bool below = k + 1 >= nzmin && k + 1 < nzmax;
+  for (int t = 0; t < in.ntr; ++t) {
+    const int64_t oa = t * A.a.sN;
+    const double* ghi = A.a.gtmax + oa + base;
+    const double* gfv = A.a.gtmin + oa + base;
+    double gT = 0.0, gA = 0.0;
+    if (layer) {
+      const double w = in.w_e[base + k], area = m.area[base + k];
+      gT += -0.5 * (w + fabs(w)) * area * gfv[k];
+      if (k == 0) gT += -0.5 * (w - fabs(w)) * area * gfv[k];
+    }
+    if (below) {
+      const double w = in.w_e[base + k + 1], area = m.area[base + k + 1];
+      gT += -0.5 * (w - fabs(w)) * area * gfv[k + 1];
+    }
+    if (layer) {
+      // QR4C terms from interfaces k-1 .. k+2 in ascending j (a term that does not reach
+      // k is +0.0; gA starts at +0.0, so adding it changes no bit)
+      for (int j = k - 1; j <= k + 2; ++j) {
+        if (j < nzmin || j >= nzmax) continue;
+        gA += ga_term(in, m, base, j, k, nzmin, nzmax, ghi[j]);
       }
+    } else {
+      A.a.gw[oa + i] = 0.0;
     }
-    for (int k = 0; k < L; ++k) {
-      A.a.gAv[oa + base + k] = gA[k];
-      A.a.gTv[oa + base + k] = gT[k];
-      A.a.gw[oa + base + k] = gw[k];
-    }
+    A.a.gTv[oa + i] = gT;
+    A.a.gAv[oa + i] = gA;
   }
 }
 
@@ -853,7 +857,8 @@ int fct_adjoint(FctPlan* P, const FctFields* f, const double* gT_new, double dt,
   r_gnode<<<grid(hm.n_layer, B), B, 0, s>>>(A);
   r_tr<<<grid(hm.n_elem, B), B, 0, s>>>(A);
   r_grad_t<<<grid(hm.n_layer, B), B, 0, s>>>(A);
-  r_column<<<grid(P->N, 128), 128, 0, s>>>(A);
+  r_vert_a<<<grid(hm.n_layer, B), B, 0, s>>>(A);
+  r_vert_b<<<grid(int64_t(P->N) * P->L, B), B, 0, s>>>(A);
   r_final<<<grid(int64_t(P->N) * P->L, B), B, 0, s>>>(A);
   r_uv<<<grid(int64_t(P->E) * P->L, B), B, 0, s>>>(A);
   r_wsum<<<grid(int64_t(P->N) * P->L, B), B, 0, s>>>(A);

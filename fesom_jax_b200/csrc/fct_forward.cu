@@ -82,6 +82,14 @@ __device__ __forceinline__ void stn(double* __restrict__ p, int64_t q, int t0, i
   for (int i = 0; i < NTR; ++i) p[tix<IL>(q, t0 + i, stride, tg)] = v[i];
 }
 
+// tie counts (bytes) of tracers [t0, t0+NTR) at entity-level q
+template <int NTR, bool IL>
+__device__ __forceinline__ void stc(uint8_t* __restrict__ p, int64_t q, int t0, int64_t stride,
+                                    int tg, const int (&v)[NTR]) {
+#pragma unroll
+  for (int i = 0; i < NTR; ++i) p[tix<IL>(q, t0 + i, stride, tg)] = uint8_t(v[i]);
+}
+
 // ---------------------------------------------------------------- edge_vflux
 __device__ __forceinline__ void body_vflux(const Inst& in, int64_t i) {
   const DevMesh& m = *in.m;
@@ -286,6 +294,9 @@ __device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i, int t0, 
       }
     }
     const Rcp rdd = rcp(den > 0.0 ? den : 1.0);
+    if constexpr (!FUSED) {   // kept for the reverse pass (tracer independent)
+      if (w0 == 0) in.ws.nden[qn] = rdd.y;
+    }
 #pragma unroll
     for (int t = 0; t < NTR; ++t) {
       nx[t] = divr(nx[t], rdd);
@@ -465,7 +476,7 @@ __device__ __forceinline__ void body_elem_bounds(const Inst& in, int64_t i, int 
   const int64_t q[3] = {int64_t(ld(m.enodes + 3 * e)) * L + k,
                         int64_t(ld(m.enodes + 3 * e + 1)) * L + k,
                         int64_t(ld(m.enodes + 3 * e + 2)) * L + k};
-  double mx[NTR], mn[NTR];
+  double mx[NTR], mn[NTR], hi[3][NTR], lw[3][NTR];
 #pragma unroll
   for (int t = 0; t < NTR; ++t) { mx[t] = -INFINITY; mn[t] = INFINITY; }
 #pragma unroll
@@ -475,11 +486,23 @@ __device__ __forceinline__ void body_elem_bounds(const Inst& in, int64_t i, int 
     ldn<NTR, IL>(in.T, q[v], t0, in.tstride, in.tg, b);
 #pragma unroll
     for (int t = 0; t < NTR; ++t) {
-      mx[t] = fmax(mx[t], fmax(a[t], b[t]));
-      mn[t] = fmin(mn[t], fmin(a[t], b[t]));
+      hi[v][t] = fmax(a[t], b[t]);
+      lw[v][t] = fmin(a[t], b[t]);
+      mx[t] = fmax(mx[t], hi[v][t]);
+      mn[t] = fmin(mn[t], lw[v][t]);
     }
   }
   const int64_t qe = int64_t(e) * L + k;
+  {   // vertices attaining the bounds (the reverse pass splits cotangents evenly over them)
+    int cx[NTR], cn[NTR];
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) {
+      cx[t] = (hi[0][t] == mx[t]) + (hi[1][t] == mx[t]) + (hi[2][t] == mx[t]);
+      cn[t] = (lw[0][t] == mn[t]) + (lw[1][t] == mn[t]) + (lw[2][t] == mn[t]);
+    }
+    stc<NTR, IL>(in.ws.ecx, qe, w0, in.ws.sE, in.wtg, cx);
+    stc<NTR, IL>(in.ws.ecn, qe, w0, in.ws.sE, in.wtg, cn);
+  }
   stn<NTR, IL>(in.ws.amax, qe, w0, in.ws.sE, in.wtg, mx);
   stn<NTR, IL>(in.ws.amin, qe, w0, in.ws.sE, in.wtg, mn);
 }
@@ -518,6 +541,29 @@ __device__ __forceinline__ void body_node_cluster(const Inst& in, int64_t i, int
   const int64_t qn = int64_t(n) * L + k;
   stn<NTR, IL>(in.ws.tvmax, qn, w0, in.ws.sN, in.wtg, mx);
   stn<NTR, IL>(in.ws.tvmin, qn, w0, in.ws.sN, in.wtg, mn);
+  // cells attaining the cluster bounds (padded values included), for the reverse pass
+  int cx[NTR], cn[NTR];
+#pragma unroll
+  for (int t = 0; t < NTR; ++t) cx[t] = cn[t] = 0;
+  for (int j = c0; j < c1; ++j) {
+    const int el = ld(m.nel_idx + j);
+    double a[NTR], b[NTR];
+    if (k >= ld(m.eul + el) && k < ld(m.enl + el)) {
+      const int64_t q = int64_t(el) * L + k;
+      ldn<NTR, IL>(in.ws.amax, q, w0, in.ws.sE, in.wtg, a);
+      ldn<NTR, IL>(in.ws.amin, q, w0, in.ws.sE, in.wtg, b);
+    } else {
+#pragma unroll
+      for (int t = 0; t < NTR; ++t) { a[t] = -kBig; b[t] = kBig; }
+    }
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) {
+      cx[t] += a[t] == mx[t];
+      cn[t] += b[t] == mn[t];
+    }
+  }
+  stc<NTR, IL>(in.ws.ccx, qn, w0, in.ws.sN, in.wtg, cx);
+  stc<NTR, IL>(in.ws.ccn, qn, w0, in.ws.sN, in.wtg, cn);
 }
 
 // ------------------- zalesak a4 + b1 + b2: admissible window, sums, factors
@@ -571,11 +617,13 @@ __device__ __forceinline__ void body_node_factors(const Inst& in, int64_t i, int
       sm[t] += fmin(s, 0.0);
     }
   }
-  double pf[NTR], mf[NTR];
+  double pf[NTR], mf[NTR], pl[NTR], mi[NTR];
 #pragma unroll
   for (int t = 0; t < NTR; ++t) {
     const double plus = (fmax(ft[t], 0.0) + fmax(-fb[t], 0.0)) + sp[t];
     const double minus = (fmin(ft[t], 0.0) + fmin(-fb[t], 0.0)) + sm[t];
+    pl[t] = plus;
+    mi[t] = minus;
     pf[t] = 1.0;
     mf[t] = 1.0;
     if (valid) {
@@ -587,6 +635,8 @@ __device__ __forceinline__ void body_node_factors(const Inst& in, int64_t i, int
   }
   stn<NTR, IL>(in.ws.pf, qn, w0, sN, in.wtg, pf);
   stn<NTR, IL>(in.ws.mf, qn, w0, sN, in.wtg, mf);
+  stn<NTR, IL>(in.ws.fplus, qn, w0, sN, in.wtg, pl);    // kept for the reverse pass
+  stn<NTR, IL>(in.ws.fminus, qn, w0, sN, in.wtg, mi);
 }
 
 // ------- fused zalesak a2 + a3 + a4 + b1 + b2: cluster bounds, window, factors
@@ -826,14 +876,22 @@ __device__ __forceinline__ void body_copy_dry(const Inst& in, int64_t i) {
 // in ``_n`` the S threads of a lane are adjacent (slice = thread index mod S), so they
 // read one contiguous run of S*NTR interleaved tracers together; in ``_1`` the slice is
 // blockIdx.y, so lanes stay contiguous along x within each tracer plane.
+// Resident 256-thread blocks per SM the compiler must fit (registers capped
+// accordingly): latency hiding pays more than the spills it costs (measured on the
+// CORE2-size batched step: +9% over the register-unconstrained build).
+template <int NTR>
+constexpr int kMinBlocks = NTR == 1 ? 6 : NTR == 2 ? 4 : NTR == 4 ? 3 : 1;
+
 #define FCT_KERNEL_T(name, body)                                                        \
   template <int NTR>                                                                    \
-  __global__ void __launch_bounds__(256) name##_1(Inst in, int t0, int w0) {            \
+  __global__ void __launch_bounds__(256, kMinBlocks<NTR>) name##_1(Inst in, int t0,     \
+                                                                   int w0) {            \
     const int sub = int(blockIdx.y) * NTR;                                              \
     body<NTR, false>(in, lane_index(), t0 + sub, w0 + sub);                             \
   }                                                                                     \
   template <int NTR>                                                                    \
-  __global__ void __launch_bounds__(256) name##_n(const Inst* __restrict__ tab, int t0,  \
+  __global__ void __launch_bounds__(256, kMinBlocks<NTR>) name##_n(                     \
+      const Inst* __restrict__ tab, int t0,                                             \
                                                   int w0, int lg) {                     \
     const int64_t g = lane_index();                                                     \
     const int sub = int(g & ((int64_t(1) << lg) - 1)) * NTR;                            \
@@ -870,7 +928,8 @@ FCT_KERNEL_T(k_node_final_f, body_node_final_f)
 // `_n` 256 >> lg lanes of 2^lg adjacent slice threads; the first and last lane of a
 // block are halo lanes.
 template <int NTR>
-__global__ void __launch_bounds__(256) k_node_limit_1(Inst in, int t0, int w0) {
+__global__ void __launch_bounds__(256, kMinBlocks<NTR>) k_node_limit_1(Inst in, int t0,
+                                                                      int w0) {
   __shared__ double smx[NTR * 256], smn[NTR * 256];
   const int tid = threadIdx.x;
   const int64_t lane = int64_t(blockIdx.x) * 254 + tid - 1;
@@ -879,7 +938,8 @@ __global__ void __launch_bounds__(256) k_node_limit_1(Inst in, int t0, int w0) {
                          smn);
 }
 template <int NTR>
-__global__ void __launch_bounds__(256) k_node_limit_n(const Inst* __restrict__ tab, int t0,
+__global__ void __launch_bounds__(256, kMinBlocks<NTR>) k_node_limit_n(const Inst* __restrict__ tab,
+                                                                      int t0,
                                                       int w0, int lg) {
   __shared__ double smx[NTR * 256], smn[NTR * 256];
   const int tid = threadIdx.x;

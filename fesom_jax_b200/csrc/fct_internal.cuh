@@ -93,7 +93,12 @@ struct Workspace {
   double *tvmax, *tvmin;         // [N,L]
   double *pf, *mf;               // [N,L] limiter factors
   double* adfh;                  // [Ed,L] antidiffusive horizontal flux
-  int64_t sN, sE, sEd;           // per-tracer strides (doubles)
+  // kept only by the full workspace (what the reverse pass reads besides the above):
+  double* nden;                  // [N,L] node-average denominator (safe), shared by tracers
+  double *fplus, *fminus;        // [N,L] limiter sums fct_plus / fct_minus
+  uint8_t *ccx, *ccn;            // [N,L] cells attaining the node's cluster max / min
+  uint8_t *ecx, *ecn;            // [E,L] vertices attaining the cell's max / min
+  int64_t sN, sE, sEd;           // per-tracer strides (doubles, or bytes for the counts)
 };
 
 // One FCT instance: a mesh, its per-call fields, and a workspace.

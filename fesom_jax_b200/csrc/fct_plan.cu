@@ -31,7 +31,9 @@ int set_error(int status, const char* fmt, ...) {
 }
 
 int64_t workspace_doubles(int64_t N, int64_t E, int64_t Ed, int64_t L, int ntr) {
-  return Ed * L + int64_t(ntr) * (4 * E * L + 9 * N * L + Ed * L);
+  const int64_t count_bytes = int64_t(ntr) * 2 * (N * L + E * L);
+  return Ed * L + N * L + int64_t(ntr) * (4 * E * L + 11 * N * L + Ed * L) +
+         (count_bytes + 7) / 8;
 }
 
 int64_t workspace_doubles_fused(int64_t N, int64_t Ed, int64_t L, int ntr) {
@@ -70,6 +72,14 @@ Workspace carve_workspace(double* base, int64_t N, int64_t E, int64_t Ed, int64_
   w.pf = take(ntr * w.sN);
   w.mf = take(ntr * w.sN);
   w.adfh = take(ntr * w.sEd);
+  w.nden = take(w.sN);
+  w.fplus = take(ntr * w.sN);
+  w.fminus = take(ntr * w.sN);
+  uint8_t* b = reinterpret_cast<uint8_t*>(p);
+  w.ccx = b; b += ntr * w.sN;
+  w.ccn = b; b += ntr * w.sN;
+  w.ecx = b; b += ntr * w.sE;
+  w.ecn = b;
   return w;
 }
 
