@@ -115,22 +115,57 @@ __device__ __forceinline__ void body_vflux(const Inst& in, int64_t i) {
 // ---------------------------------------------------- tracer_gradient_elements
 // Gradient of T on cell `el` (nodes v0, v1, v2) at level k; the stored (elem_grad) and the
 // recomputed (fused stages) gradients both come from here, so they are the same bits.
-template <int NTR, bool IL>
-__device__ __forceinline__ void cell_grad(const Inst& in, int el, int v0, int v1, int v2, int k,
-                                          int t0, double (&gx)[NTR], double (&gy)[NTR]) {
-  const int L = in.m->L;
-  const double* g = in.m->gsca + 6 * int64_t(el);
-  const double g0 = ld(g), g1 = ld(g + 1), g2 = ld(g + 2), g3 = ld(g + 3), g4 = ld(g + 4),
-               g5 = ld(g + 5);
-  double a0[NTR], a1[NTR], a2[NTR];
-  ldn<NTR, IL>(in.T, int64_t(v0) * L + k, t0, in.tstride, in.tg, a0);
-  ldn<NTR, IL>(in.T, int64_t(v1) * L + k, t0, in.tstride, in.tg, a1);
-  ldn<NTR, IL>(in.T, int64_t(v2) * L + k, t0, in.tstride, in.tg, a2);
+template <int NTR>
+__device__ __forceinline__ void cell_grad_vals(const Inst& in, int el, const double (&a0)[NTR],
+                                               const double (&a1)[NTR], const double (&a2)[NTR],
+                                               double (&gx)[NTR], double (&gy)[NTR]) {
+  // gradient_sca row of the cell: 48 bytes, 16-byte aligned (3 double2 loads)
+  const double2* g = reinterpret_cast<const double2*>(in.m->gsca + 6 * int64_t(el));
+  const double2 p = __ldg(g), q = __ldg(g + 1), r = __ldg(g + 2);
+  const double g0 = p.x, g1 = p.y, g2 = q.x, g3 = q.y, g4 = r.x, g5 = r.y;
 #pragma unroll
   for (int t = 0; t < NTR; ++t) {
     gx[t] = g0 * a0[t] + g1 * a1[t] + g2 * a2[t];
     gy[t] = g3 * a0[t] + g4 * a1[t] + g5 * a2[t];
   }
+}
+
+template <int NTR, bool IL>
+__device__ __forceinline__ void cell_grad(const Inst& in, int el, int v0, int v1, int v2, int k,
+                                          int t0, double (&gx)[NTR], double (&gy)[NTR]) {
+  const int L = in.m->L;
+  double a0[NTR], a1[NTR], a2[NTR];
+  ldn<NTR, IL>(in.T, int64_t(v0) * L + k, t0, in.tstride, in.tg, a0);
+  ldn<NTR, IL>(in.T, int64_t(v1) * L + k, t0, in.tstride, in.tg, a1);
+  ldn<NTR, IL>(in.T, int64_t(v2) * L + k, t0, in.tstride, in.tg, a2);
+  cell_grad_vals<NTR>(in, el, a0, a1, a2, gx, gy);
+}
+
+// The same gradient when the tracer values at the lane's own node (vertex `pos` of the
+// cell) are already in registers: only the other two vertices are gathered.
+template <int NTR, bool IL>
+__device__ __forceinline__ void cell_grad_own(const Inst& in, int el, int v0, int v1, int v2,
+                                              int pos, const double (&own)[NTR], int k, int t0,
+                                              double (&gx)[NTR], double (&gy)[NTR]) {
+  const int L = in.m->L;
+  double a0[NTR], a1[NTR], a2[NTR];
+  if (pos == 0) {
+    ldn<NTR, IL>(in.T, int64_t(v1) * L + k, t0, in.tstride, in.tg, a1);
+    ldn<NTR, IL>(in.T, int64_t(v2) * L + k, t0, in.tstride, in.tg, a2);
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) a0[t] = own[t];
+  } else if (pos == 1) {
+    ldn<NTR, IL>(in.T, int64_t(v0) * L + k, t0, in.tstride, in.tg, a0);
+    ldn<NTR, IL>(in.T, int64_t(v2) * L + k, t0, in.tstride, in.tg, a2);
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) a1[t] = own[t];
+  } else {
+    ldn<NTR, IL>(in.T, int64_t(v0) * L + k, t0, in.tstride, in.tg, a0);
+    ldn<NTR, IL>(in.T, int64_t(v1) * L + k, t0, in.tstride, in.tg, a1);
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) a2[t] = own[t];
+  }
+  cell_grad_vals<NTR>(in, el, a0, a1, a2, gx, gy);
 }
 
 template <int NTR, bool IL>
@@ -263,11 +298,13 @@ __device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i, int t0, 
     const int c0 = ld(m.nel_off + n), c1 = ld(m.nel_off + n + 1);
     if constexpr (FUSED) {
       for (int j = c0; j < c1; ++j) {
-        if (!in_range(k, unsigned(ld(m.nelr + j)))) continue;
+        const unsigned r = unsigned(ld(m.nelr + j));
+        if (!in_range(k, r)) continue;
         const int4 sl = __ldg(m.nel4 + j);
         const double a = ld(m.earea + sl.x);
         double gx[NTR], gy[NTR];
-        cell_grad<NTR, IL>(in, sl.x, sl.y, sl.z, sl.w, k, t0, gx, gy);
+        cell_grad_own<NTR, IL>(in, sl.x, sl.y, sl.z, sl.w, int((r >> 16) & 3u), Tc, k, t0, gx,
+                               gy);
 #pragma unroll
         for (int t = 0; t < NTR; ++t) {
           nx[t] += gx[t] * a;

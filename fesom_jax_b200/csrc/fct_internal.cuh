@@ -69,7 +69,7 @@ struct DevMesh {
   const int4* ne4;       // per node->edge slot: {2*edge + second, other node,
                          //   ekmin | ekmax << 8, cell layer ranges (see pack_tri)}
   const int4* nel4;      // per node->element slot: {element, its three nodes}
-  const int* nelr;       // per node->element slot: eul | enl << 8
+  const int* nelr;       // per node->element slot: eul | enl << 8 | (node's vertex index) << 16
   // vertical
   const double* Zp;      // [L]  Z padded with Z[L-2] (tracer_adv.py:233)
   const double* zbar;    // [L]

@@ -263,12 +263,14 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   const int nie_all = d->nod_in_elem2D_offsets[N];
   std::vector<int4> nel4(std::max(nie_all, 1));
   std::vector<int> nelr(std::max(nie_all, 1));
-  for (int j = 0; j < nie_all; ++j) {
-    const int el = d->nod_in_elem2D[j];
-    nel4[j] = make_int4(el, d->elem_nodes[3 * el], d->elem_nodes[3 * el + 1],
-                        d->elem_nodes[3 * el + 2]);
-    nelr[j] = eul[el] | (enl[el] << 8);
-  }
+  for (int n = 0; n < N; ++n)
+    for (int j = d->nod_in_elem2D_offsets[n]; j < d->nod_in_elem2D_offsets[n + 1]; ++j) {
+      const int el = d->nod_in_elem2D[j];
+      const int* en = d->elem_nodes + 3 * size_t(el);
+      nel4[j] = make_int4(el, en[0], en[1], en[2]);
+      const int pos = en[0] == n ? 0 : (en[1] == n ? 1 : 2);   // n's place in the cell
+      nelr[j] = eul[el] | (enl[el] << 8) | (pos << 16);
+    }
   std::vector<double> Zp(L);
   for (int k = 0; k < L - 1; ++k) Zp[k] = d->Z[k];
   Zp[L - 1] = d->Z[L - 2];
