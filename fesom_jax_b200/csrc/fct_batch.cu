@@ -142,6 +142,10 @@ int fct_batch_create(const FctInstance* insts, int n, int64_t budget, FctBatch**
         in.ws = ws;
         in.dt = q.dt;
         in.ntr = q.ntr;
+        in.Kv = q.Kv;   // optional diffusion epilogue, in place on T_new
+        in.vd_T = in.T_new;
+        in.sw_tracer = -1;
+        if (q.Kv) d.any_vdiff = true;
       }
     }
     d.any_wi = false;
@@ -201,7 +205,8 @@ int fct_batch_info(const FctBatch* B, int64_t out[6]) {
       const int csz = std::min(chunk, g.dims.ntr - c0);
       per_chunk_launches += stage_launches(csz, g.dims.per_thread);
     }
-    const int stages = (g.dims.fused ? 4 : 7) + (g.dims.any_wi ? 1 : 0);
+    const int stages = (g.dims.fused ? 4 : 7) + (g.dims.any_wi ? 1 : 0) +
+                       (g.dims.any_vdiff ? 1 : 0);
     launches += 1 + int64_t(stages) * per_chunk_launches;
   }
   out[4] = wmax;

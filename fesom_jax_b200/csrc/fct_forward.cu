@@ -893,6 +893,98 @@ __device__ __forceinline__ void body_node_final(const Inst& in, int64_t i, int t
   stn<NTR, IL>(in.T_new, qn, t0, in.tstride, tg, out);
 }
 
+// ------------- implicit vertical diffusion (tracer_diff.py:68-123, ops.py:121-168)
+// One thread per node column and NTR tracers: the Thomas algorithm over the column's wet
+// layers [nzmin, nzmax) (the reference's padded rows above and below solve to exactly 0,
+// so starting and ending the recursions there gives the same numbers). The elimination
+// factors m and cp do not depend on the tracer: one reciprocal of m serves c/m and every
+// tracer's dp/m. cp goes to workspace slot w0 of gnx, dp to the tracer's slots of lo
+// (both free after the FCT stages); the back substitution reads them in reverse.
+template <int NTR, bool IL>
+__device__ __forceinline__ void body_vdiff(const Inst& in, int64_t n, int t0, int w0) {
+  const DevMesh& m = *in.m;
+  if (n >= m.N || !in.Kv) return;
+  const int L = m.L;
+  const int nzmin = ld(m.nzmin + n), nzmax = ld(m.nzmax + n);
+  const int64_t base = n * L;
+  const int64_t ts = in.tstride, sN = in.ws.sN;
+  const int tg = in.tg;
+  const double* Tin = in.vd_T;
+  if (Tin != in.T_new) {   // out of place: dry levels keep T
+    for (int k = 0; k < L; ++k) {
+      if (k >= nzmin && k < nzmax) continue;
+      double v[NTR];
+      ldn<NTR, IL>(Tin, base + k, t0, ts, tg, v);
+      stn<NTR, IL>(in.T_new, base + k, t0, ts, tg, v);
+    }
+  }
+  if (nzmax <= nzmin) return;
+  const double dt = in.dt;
+  const double* Zc = in.vd_Z3d ? in.vd_Z3d + base : m.Zp;
+  double cprev = 0.0, dprev[NTR], Tm[NTR], Tc[NTR], Tp[NTR];
+#pragma unroll
+  for (int t = 0; t < NTR; ++t) dprev[t] = 0.0;
+  ldn<NTR, IL>(Tin, base + nzmin, t0, ts, tg, Tc);
+  ldn<NTR, IL>(Tin, base + (nzmin > 0 ? nzmin - 1 : 0), t0, ts, tg, Tm);
+  for (int k = nzmin; k < nzmax; ++k) {
+    const int64_t q = base + k;
+    const bool last = k + 1 >= L;
+    if (last) {
+#pragma unroll
+      for (int t = 0; t < NTR; ++t) Tp[t] = 0.0;
+    } else {
+      ldn<NTR, IL>(Tin, q + 1, t0, ts, tg, Tp);
+    }
+    double dzu = k == 0 ? 0.0 : ld(Zc + k - 1) - ld(Zc + k);
+    double dzd = ld(Zc + k) - (last ? 0.0 : ld(Zc + k + 1));
+    dzu = dzu == 0.0 ? 1.0 : dzu;
+    dzd = dzd == 0.0 ? 1.0 : dzd;
+    const double av = ld(m.areasvol + q);
+    const double sav = av > 0.0 ? av : 1.0;
+    const double ar = ld(m.area + q), arp = last ? 0.0 : ld(m.area + q + 1);
+    const double kv = ld(in.Kv + q), kvp = last ? 0.0 : ld(in.Kv + q + 1);
+    const double a_full = -kv * dt / dzu * (ar / sav);
+    const double c_full = -kvp * dt / dzd * (arp / sav);
+    const double a = k == nzmin ? 0.0 : a_full;
+    const double c = k == nzmax - 1 ? 0.0 : c_full;
+    const double b = -a - c + ld(in.hnode_new + q);
+    const Rcp rm = rcp(b - a * cprev);
+    cprev = divr(c, rm);
+    in.ws.gnx[tix<IL>(q, w0, sN, in.wtg)] = cprev;
+    double swd = 0.0;
+    if (in.sw_3d) {
+      const double sw = ld(in.sw_3d + q), swp = last ? 0.0 : ld(in.sw_3d + q + 1);
+      swd = (sw - swp * (arp / sav)) * dt;
+    }
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) {
+      double rhs = a * (Tc[t] - Tm[t]) + c * (Tc[t] - Tp[t]);
+      if (in.bc_surf) rhs = rhs + (k == nzmin ? ld(in.bc_surf + (t0 + t) * in.bc_stride + n) : 0.0);
+      if (in.sw_3d && t0 + t == in.sw_tracer) rhs = rhs + swd;
+      dprev[t] = divr(rhs - a * dprev[t], rm);
+      Tm[t] = Tc[t];
+      Tc[t] = Tp[t];
+    }
+    stn<NTR, IL>(in.ws.lo, q, w0, sN, in.wtg, dprev);
+  }
+  double x[NTR];
+#pragma unroll
+  for (int t = 0; t < NTR; ++t) x[t] = 0.0;
+  for (int k = nzmax - 1; k >= nzmin; --k) {
+    const int64_t q = base + k;
+    const double cp = in.ws.gnx[tix<IL>(q, w0, sN, in.wtg)];
+    double dp[NTR], Tv[NTR];
+    ldn<NTR, IL>(in.ws.lo, q, w0, sN, in.wtg, dp);
+    ldn<NTR, IL>(Tin, q, t0, ts, tg, Tv);
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) {
+      x[t] = dp[t] - cp * x[t];
+      Tv[t] = Tv[t] + x[t];
+    }
+    stn<NTR, IL>(in.T_new, q, t0, ts, tg, Tv);
+  }
+}
+
 // ------------------------------------------- dry levels keep T (ale_reconstruct)
 template <bool IL>
 __device__ __forceinline__ void body_copy_dry(const Inst& in, int64_t i) {
@@ -960,6 +1052,7 @@ FCT_KERNEL_T(k_node_final, body_node_final_u)
 FCT_KERNEL_T(k_node_lo_f, body_node_lo_f)
 FCT_KERNEL_T(k_edge_adf_f, body_edge_adf_f)
 FCT_KERNEL_T(k_node_final_f, body_node_final_f)
+FCT_KERNEL_T(k_vdiff, body_vdiff)
 
 // node_limit blocks hold 256 threads: `_1` one lane per thread (slice = blockIdx.y),
 // `_n` 256 >> lg lanes of 2^lg adjacent slice threads; the first and last lane of a
@@ -1087,6 +1180,13 @@ int launch_forward_events(const Inst& single, const Inst* tab, int n, const Laun
       mark();
       if (stop_before_final) continue;
       FCT_STAGE(k_node_final_f, d.max_layer);
+      if (d.any_vdiff) {   // epilogue: implicit vertical diffusion of this chunk, in place
+        if (d.copy_dry) {  // the dry levels of T_new must hold T before it runs
+          if (tab) k_copy_dry_n<<<grid(d.max_dense), B, 0, s>>>(tab);
+          else k_copy_dry_1<<<grid(d.max_dense), B, 0, s>>>(single);
+        }
+        FCT_STAGE(k_vdiff, d.max_nodes);
+      }
       mark();
       continue;
     }
@@ -1126,6 +1226,19 @@ int launch_forward(const Inst& single, const Inst* tab, int n, const LaunchDims&
 int launch_forward_stages(const Inst& single, const LaunchDims& d, cudaStream_t s,
                           bool through_factors) {
   return launch_forward_events(single, nullptr, 1, d, s, nullptr, through_factors, -1);
+}
+
+int launch_vdiff(const Inst& single, const LaunchDims& d, cudaStream_t s) {
+  constexpr int B = 256;
+  auto xblocks = [&](int64_t lanes) {
+    return unsigned(std::max<int64_t>(1, (lanes + B - 1) / B));
+  };
+  const Inst* tab = nullptr;
+  const int n = 1;
+  const int c0 = 0, c1 = d.ntr;
+  FCT_STAGE(k_vdiff, d.max_nodes);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? FCT_OK : cuda_error(e, "vertical diffusion launch");
 }
 
 int launch_copy_dry(const Inst* tab, int n, int64_t max_dense, cudaStream_t s) {

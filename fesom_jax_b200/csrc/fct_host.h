@@ -35,6 +35,7 @@ struct LaunchDims {
   int per_thread = 8;  // most tracers one thread carries (8, 4, 2 or 1): the tuning knob
   bool any_wi;      // launch the implicit w_i stage
   bool copy_dry;    // launch the dry-level copy
+  bool any_vdiff = false;  // launch the implicit vertical diffusion after each chunk
   bool fused = true;  // fused stages (lean workspace); false: every stage kernel writes its
                       // intermediates (what the reverse pass reads)
 };
@@ -55,6 +56,8 @@ int launch_forward_stages(const Inst& single, const LaunchDims& d, cudaStream_t 
 
 // Copy T's dry levels into T_new for ``n`` instances of ``tab`` (ignores Inst::copy_dry).
 int launch_copy_dry(const Inst* tab, int n, int64_t max_dense, cudaStream_t s);
+// Implicit vertical diffusion alone (fct_vert_diff): single instance, tracer-major.
+int launch_vdiff(const Inst& single, const LaunchDims& d, cudaStream_t s);
 
 // Workspace of `ntr` tracers: every stage field (the unfused stages, which the reverse
 // pass recomputes and reads), or with `fused` only the fields the fused forward keeps.

@@ -115,6 +115,11 @@ struct Inst {
   int64_t tstride;
   int tg;
   int wtg;   // tracers held by the workspace (its interleave stride when interleaved)
+  // implicit vertical diffusion after the step (fesom_jax/tracer_diff.py:68-123; Kv NULL =
+  // off): input vd_T (the FCT result in the batched epilogue), output T_new
+  const double *Kv, *vd_T, *vd_Z3d, *bc_surf, *sw_3d;
+  int64_t bc_stride;   // doubles between tracers' bc_surf rows
+  int sw_tracer;       // tracer that takes the shortwave divergence (-1: none)
   const double *Z3d, *zbar3, *w_i;
   Workspace ws;
   double dt;

@@ -419,6 +419,46 @@ int fct_plan_set_fused(FctPlan* P, int fused) {
   return FCT_OK;
 }
 
+int fct_vert_diff(FctPlan* P, const FctVdiffFields* f, double dt, int ntr, fct_stream_t stream) {
+  if (!P || !f) return set_error(FCT_ERR_INVALID, "NULL plan or fields");
+  if (ntr < 1) return set_error(FCT_ERR_INVALID, "ntr must be >= 1");
+  if (ntr > P->max_tracers)
+    return set_error(FCT_ERR_CAPACITY, "ntr=%d exceeds reserved workspace (%d tracers); "
+                     "call fct_plan_reserve first", ntr, P->max_tracers);
+  if (!f->T || !f->T_new || !f->Kv || !f->hnode_new)
+    return set_error(FCT_ERR_INVALID, "a required field pointer is NULL");
+  if (!(dt > 0.0)) return set_error(FCT_ERR_INVALID, "dt must be positive");
+  int prev = -1;
+  cudaGetDevice(&prev);
+  if (prev != P->device) cudaSetDevice(P->device);
+  Inst in{};
+  in.m = P->d_mesh;
+  in.hnode_new = f->hnode_new;
+  in.T = f->T;
+  in.T_new = f->T_new;
+  in.vd_T = f->T;
+  in.Kv = f->Kv;
+  in.vd_Z3d = f->Z3d;
+  in.bc_surf = f->bc_surf;
+  in.bc_stride = P->N;
+  in.sw_3d = f->sw_3d;
+  in.sw_tracer = f->sw_3d ? f->sw_tracer : -1;
+  in.tstride = f->tracer_stride ? f->tracer_stride : int64_t(P->N) * P->L;
+  in.tg = 0;
+  in.wtg = ntr;
+  in.ws = P->ws;
+  in.dt = dt;
+  in.ntr = ntr;
+  LaunchDims dims{};
+  dims.max_nodes = P->N;
+  dims.ntr = ntr;
+  dims.chunk = 0;
+  dims.per_thread = 8;
+  const int st = launch_vdiff(in, dims, static_cast<cudaStream_t>(stream));
+  if (prev >= 0 && prev != P->device) cudaSetDevice(prev);
+  return st;
+}
+
 int fct_forward(FctPlan* P, const FctFields* f, double dt, int ntr, fct_stream_t stream) {
   if (!P || !f) return set_error(FCT_ERR_INVALID, "NULL plan or fields");
   if (ntr < 1) return set_error(FCT_ERR_INVALID, "ntr must be >= 1");

@@ -34,7 +34,8 @@ def _torch():
 class FctInstance(C.Structure):
     _fields_ = [("plan", C.c_void_p), ("uv", C.c_void_p), ("w_e", C.c_void_p),
                 ("helem", C.c_void_p), ("hnode", C.c_void_p), ("hnode_new", C.c_void_p),
-                ("buf", C.c_void_p * 3), ("ntr", C.c_int), ("dt", C.c_double)]
+                ("buf", C.c_void_p * 3), ("ntr", C.c_int), ("dt", C.c_double),
+                ("Kv", C.c_void_p)]
 
 
 def _bind_batch(L):
@@ -70,6 +71,7 @@ class Member:
     hnode: object
     hnode_new: object
     buf: object         # torch [3, N, nl, ntr] (tracers interleaved innermost)
+    Kv: object = None   # torch [N, nl] or None (no vertical diffusion)
 
 
 class Ensemble:
@@ -92,8 +94,11 @@ class Ensemble:
             p = self._plans[id(mesh)] = FctPlan(mesh, self.device, max_tracers=1)
         return p
 
-    def add_member(self, mesh: Mesh, uv, w_e, helem, hnode, hnode_new, T, T_old, dt: float) -> int:
-        """Add a member (host numpy or device tensors); ``T``/``T_old`` are ``[ntr, N, nl]``."""
+    def add_member(self, mesh: Mesh, uv, w_e, helem, hnode, hnode_new, T, T_old, dt: float,
+                   Kv=None) -> int:
+        """Add a member (host numpy or device tensors); ``T``/``T_old`` are ``[ntr, N, nl]``.
+        With ``Kv`` (``[N, nl]``) every step is followed by the implicit vertical diffusion
+        of fesom_jax/tracer_diff.py:68-123 (step.py:452), in the same graph."""
         if self._h is not None:
             raise RuntimeError("members must be added before the ensemble is built")
         t = self.torch
@@ -117,7 +122,7 @@ class Ensemble:
         buf[2].copy_(T.permute(1, 2, 0))
         self.plan(mesh)
         self.members.append(Member(mesh, ntr, float(dt), d(uv), d(w_e), d(helem), d(hnode),
-                                   d(hnode_new), buf))
+                                   d(hnode_new), buf, d(Kv) if Kv is not None else None))
         return len(self.members) - 1
 
     # ------------------------------------------------------------------ build
@@ -135,6 +140,7 @@ class Ensemble:
             for j in range(3):
                 q.buf[j] = mb.buf[j].data_ptr()
             q.ntr, q.dt = mb.ntr, mb.dt
+            q.Kv = mb.Kv.data_ptr() if mb.Kv is not None else None
         h = C.c_void_p()
         _lib.check(L.fct_batch_create(arr, n, self.workspace_budget, C.byref(h)))
         self._h = h

@@ -116,6 +116,27 @@ int fct_forward(FctPlan* plan, const FctFields* fields, double dt, int ntr,
                 fct_stream_t stream);
 
 /*
+ * Implicit vertical tracer diffusion (fesom_jax/tracer_diff.py:68-123 impl_vert_diff_one;
+ * :126-141 impl_vert_diff is two tracers with the shortwave on the first): per node
+ * column, the tridiagonal system of the diffusivity Kv solved by the Thomas algorithm
+ * (ops.py:121-168), the increment added to T on wet layers; dry levels keep T.
+ */
+typedef struct FctVdiffFields {
+  const double* T;          /* ntr x [nod2D, nl], tracer_stride apart */
+  double* T_new;            /* ntr x [nod2D, nl] (may equal T: in place) */
+  int64_t tracer_stride;    /* 0 = nod2D * nl */
+  const double* Kv;         /* [nod2D, nl] diffusivity on interfaces */
+  const double* hnode_new;  /* [nod2D, nl] */
+  const double* Z3d;        /* optional [nod2D, nl] mid-layer depths (NULL: the mesh's Z) */
+  const double* bc_surf;    /* optional ntr x [nod2D] surface-layer RHS increments */
+  const double* sw_3d;      /* optional [nod2D, nl] shortwave flux (divergence added) */
+  int sw_tracer;            /* which tracer takes sw_3d (the reference: T, 0) */
+} FctVdiffFields;
+/* Needs a workspace of ntr tracers (fct_plan_reserve); allocates nothing. */
+int fct_vert_diff(FctPlan* plan, const FctVdiffFields* fields, double dt, int ntr,
+                  fct_stream_t stream);
+
+/*
  * Reverse mode (the reference's autodiff surface: jax.grad through advect_one_fct,
  * fesom_jax/integrate.py:43-169 under jax.grad). Cotangents follow JAX's subgradient
  * conventions: maximum/minimum split equally at a tie, segment_max/min and max over an
@@ -179,6 +200,8 @@ typedef struct FctInstance {
   double* buf[3];           /* rotating tracer buffers, each [nod2D,nl,ntr] */
   int ntr;
   double dt;
+  const double* Kv;         /* optional [nod2D,nl]: implicit vertical diffusion after each
+                               step (tracer_diff.py:68-123, step.py:452; NULL = off) */
 } FctInstance;
 
 typedef struct FctBatch FctBatch;

@@ -85,3 +85,35 @@ def check_against_golden(m, g, name, case, T_new, rtol=RTOL):
     assert abs(dg[1] - dr[1]) <= rtol * dr[2] * 10, f"{name}: weighted sum"
     assert abs(dg[3] - dr[3]) <= rtol * dr[3] * 10, f"{name}: sum of squares"
     return err
+
+
+VDIFF_GOLDEN = Path(__file__).resolve().parent / "golden" / "fct_vdiff_golden.npz"
+
+
+def vdiff_cases(m):
+    """Implicit vertical diffusion cases on ``m``: name -> dict(T, Kv, hnode_new, kw)
+    (``kw``: bc_surf / sw_3d / Z3d of fesom_jax/tracer_diff.py:68)."""
+    rng = np.random.default_rng(77)
+    f = I.make_fields(m, seed=0)
+    lm, im = m.node_layer_mask, m.node_iface_mask
+    frac = I.layer_depth_fraction(m)[None, :]
+    Kv = np.where(im, 1e-5 + 1e-2 * np.exp(-5.0 * frac) * rng.uniform(0.5, 1.5, im.shape), 0.0)
+    k = np.arange(m.nl)[None, :]
+    zbar3 = np.broadcast_to(m.zbar, (m.nod2D, m.nl)).copy()
+    zbar3[:, 1:] *= 1.0 + 0.01 * np.sin(np.arange(m.nod2D))[:, None]
+    Z3d = np.concatenate([0.5 * (zbar3[:, :-1] + zbar3[:, 1:]),
+                          0.5 * (zbar3[:, -2:-1] + zbar3[:, -1:])], axis=1)
+    Zp = np.concatenate([m.Z, m.Z[-1:]])
+    sw = np.where(im, 2e-5 * np.exp(Zp[None, :] / 20.0) * rng.uniform(0.8, 1.2, im.shape), 0.0)
+    base = dict(Kv=Kv, hnode_new=f.hnode_new)
+    out = {
+        "T": dict(T=f.tracers[0], kw={}),
+        "S_bc": dict(T=f.tracers[1], kw=dict(bc_surf=rng.normal(0.0, 0.01, m.nod2D))),
+        "T_sw": dict(T=f.tracers[0], kw=dict(sw_3d=sw)),
+        "T_zstar": dict(T=f.tracers[0], kw=dict(Z3d=Z3d)),
+        "const": dict(T=np.where(lm, 20.0, 0.0), kw={}),
+        "grad": dict(T=np.where(lm, 10.0 + 0.5 * k, 0.0), kw={}),
+    }
+    for c in out.values():
+        c.update(base)
+    return out
