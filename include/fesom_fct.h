@@ -137,6 +137,26 @@ int fct_vert_diff(FctPlan* plan, const FctVdiffFields* fields, double dt, int nt
                   fct_stream_t stream);
 
 /*
+ * Sea-ice FCT advection (fesom_jax/ice_adv.py:175-194 fct_solve; fesom_ice_fct.c): one
+ * step of the three surface ice tracers with the element-based Taylor-Galerkin scheme,
+ * the consistent-mass low/high-order solves and the Zalesak limiter. The plan's mesh is
+ * used at its surface level; its workspace serves as scratch (allocates nothing).
+ */
+typedef struct FctIceFields {
+  const double* tracer[3];  /* a_ice, m_ice, m_snow: [nod2D] */
+  double* tracer_new[3];    /* advected tracers (before cut_off): [nod2D] */
+  const double* u_ice;      /* [nod2D] nodal ice velocity */
+  const double* v_ice;      /* [nod2D] */
+} FctIceFields;
+typedef struct FctIceConfig {
+  double dt;                /* IceConfig.ice_dt */
+  double gamma;             /* IceConfig.ice_gamma_fct (0.5) */
+  double diff;              /* IceConfig.ice_diff (10) */
+} FctIceConfig;
+int fct_ice_solve(FctPlan* plan, const FctIceFields* fields, const FctIceConfig* cfg,
+                  fct_stream_t stream);
+
+/*
  * Reverse mode (the reference's autodiff surface: jax.grad through advect_one_fct,
  * fesom_jax/integrate.py:43-169 under jax.grad). Cotangents follow JAX's subgradient
  * conventions: maximum/minimum split equally at a tie, segment_max/min and max over an

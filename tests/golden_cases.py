@@ -117,3 +117,25 @@ def vdiff_cases(m):
     for c in out.values():
         c.update(base)
     return out
+
+
+ICE_GOLDEN = Path(__file__).resolve().parent / "golden" / "fct_ice_golden.npz"
+
+
+def ice_cases(m, seed=0):
+    """Sea-ice FCT inputs on ``m``: name -> dict(a, m, ms, u, v, dt). A concentration
+    blob with a sharp edge (limiter active), ice/snow thickness, nodal ice velocity."""
+    rng = np.random.default_rng(seed)
+    N = m.nod2D
+    lon, lat = m.coord_nod2D[:, 0], m.coord_nod2D[:, 1]
+    d = np.hypot(lon - np.median(lon), lat - np.median(lat))
+    r = np.argsort(np.argsort(d)) / N          # distance rank in [0, 1)
+    a = np.clip(2.0 - 3.3 * r + 0.05 * rng.normal(size=N), 0.0, 1.0)
+    a = np.where(r < 0.3, 1.0, a)    # a flat top, a ramp, open water beyond r = 0.6
+    hi = a * (1.0 + 2.0 * rng.uniform(size=N))
+    hs = a * 0.3 * rng.uniform(size=N)
+    u, v = rng.normal(0.0, 0.1, N), rng.normal(0.0, 0.1, N)
+    return {
+        "step_500": dict(a=a, m=hi, ms=hs, u=u, v=v, dt=500.0),
+        "fast_3600": dict(a=a, m=hi, ms=hs, u=5.0 * u, v=5.0 * v, dt=3600.0),
+    }
