@@ -385,25 +385,42 @@ __global__ void __launch_bounds__(B) r_edge(Adj A) {
     const double diff = A2 - A1;
     const double Tm1 = A1 + (2.0 * diff + c1 * g0 + c2 * g2) / 6.0;
     const double Tm2 = A2 - (2.0 * diff + c1 * g1 + c2 * g3) / 6.0;
-    // HO = -0.5 ((vf + |vf|) Tm1 + (vf - |vf|) Tm2)
-    const double gTm1 = -0.5 * (vf + avf) * gHO, gTm2 = -0.5 * (vf - avf) * gHO;
+    // HO = -0.5 ((vf + |vf|) Tm1 + (vf - |vf|) Tm2); fl = -0.5 (T1 (vf + |vf|) + T2 (vf - |vf|));
+    // the per-end terms of Tm1/Tm2 and T1/T2 are re-derived by the consumers (edge_terms)
     double gvf = -0.5 * ((1.0 + s) * Tm1 + (1.0 - s) * Tm2) * gHO;
-    // fl = -0.5 (T1 (vf + |vf|) + T2 (vf - |vf|))
-    const double gT1 = -0.5 * (vf + avf) * gfl, gT2 = -0.5 * (vf - avf) * gfl;
     gvf += -0.5 * (T1 * (1.0 + s) + T2 * (1.0 - s)) * gfl;
-    // Tm1 = A1 + X1/6, Tm2 = A2 - X2/6, X = 2 (A2 - A1) + c1 g + c2 g'
-    const double gX1 = gTm1 / 6.0, gX2 = -gTm2 / 6.0;
-    const double gdiff = 2.0 * gX1 + 2.0 * gX2;
-    A.a.gA1[oe + qe] = gTm1 - gdiff;
-    A.a.gA2[oe + qe] = gTm2 + gdiff;
-    A.a.gT1[oe + qe] = gT1;
-    A.a.gT2[oe + qe] = gT2;
-    A.a.gg0[oe + qe] = c1 * gX1;
-    A.a.gg2[oe + qe] = c2 * gX1;
-    A.a.gg1[oe + qe] = c1 * gX2;
-    A.a.gg3[oe + qe] = c2 * gX2;
+    A.a.gHO[oe + qe] = gHO;
+    A.a.gfl[oe + qe] = gfl;
     A.a.gvf[oe + qe] = gvf;
   }
+}
+
+// The per-end cotangents of edge e at level k (tracer t), re-derived from the stored
+// gHO (of the MFCT flux) and gfl (of the upwind flux) with r_edge's expressions:
+//   T1/T2: through the upwind flux; A1/A2: through ttfAB in Tm1/Tm2;
+//   g0..g3: through the gradients in Tm1 (g0 = c1 gX1, g2 = c2 gX1) and Tm2 (g1, g3).
+struct EdgeTerms {
+  double gT1, gT2, gA1, gA2, gg0, gg1, gg2, gg3;
+};
+__device__ __forceinline__ EdgeTerms edge_terms(const Adj& A, int t, int e, int k) {
+  const DevMesh& m = *A.in.m;
+  const int64_t qe = int64_t(e) * m.L + k, oe = t * A.a.sEd;
+  const double vf = A.in.ws.vflux[qe], avf = fabs(vf);
+  const double gHO = A.a.gHO[oe + qe], gfl = A.a.gfl[oe + qe];
+  const double c1 = m.ecoef[2 * e], c2 = m.ecoef[2 * e + 1];
+  const double gTm1 = -0.5 * (vf + avf) * gHO, gTm2 = -0.5 * (vf - avf) * gHO;
+  EdgeTerms r;
+  r.gT1 = -0.5 * (vf + avf) * gfl;
+  r.gT2 = -0.5 * (vf - avf) * gfl;
+  const double gX1 = gTm1 / 6.0, gX2 = -gTm2 / 6.0;
+  const double gdiff = 2.0 * gX1 + 2.0 * gX2;
+  r.gA1 = gTm1 - gdiff;
+  r.gA2 = gTm2 + gdiff;
+  r.gg0 = c1 * gX1;
+  r.gg2 = c2 * gX1;
+  r.gg1 = c1 * gX2;
+  r.gg3 = c2 * gX2;
+  return r;
 }
 
 __device__ __forceinline__ bool use_tri_at(const DevMesh& m, int e, int k) {
@@ -424,14 +441,13 @@ __global__ void __launch_bounds__(B) r_gnode(Adj A) {
   const int n = lane_ent(lane), k = lane_lev(lane), L = m.L;
   const int64_t qn = int64_t(n) * L + k;
   for (int t = 0; t < in.ntr; ++t) {
-    const int64_t oe = t * A.a.sEd;
     double gx = 0.0, gy = 0.0;
     for (int j = m.ne_off[n]; j < m.ne_off[n + 1]; ++j) {
       const int idx = m.ne_idx[j], e = idx >> 1;
       if (!edge_on(m, e, k) || use_tri_at(m, e, k)) continue;
-      const int64_t qe = oe + int64_t(e) * L + k;
-      if (idx & 1) { gx += A.a.gg1[qe]; gy += A.a.gg3[qe]; }
-      else { gx += A.a.gg0[qe]; gy += A.a.gg2[qe]; }
+      const EdgeTerms et = edge_terms(A, t, e, k);
+      if (idx & 1) { gx += et.gg1; gy += et.gg3; }
+      else { gx += et.gg0; gy += et.gg2; }
     }
     A.a.ggnx[t * A.a.sN + qn] = gx;
     A.a.ggny[t * A.a.sN + qn] = gy;
@@ -448,14 +464,14 @@ __global__ void __launch_bounds__(B) r_tr(Adj A) {
   const int el = lane_ent(lane), k = lane_lev(lane), L = m.L;
   const double aw = m.earea[el];
   for (int t = 0; t < in.ntr; ++t) {
-    const int64_t oe = t * A.a.sEd, oa = t * A.a.sN;
+    const int64_t oa = t * A.a.sN;
     double gx = 0.0, gy = 0.0;
     for (int j = m.eud_off[el]; j < m.eud_off[el + 1]; ++j) {
       const int idx = m.eud_idx[j], e = idx >> 1;
       if (!edge_on(m, e, k) || !use_tri_at(m, e, k)) continue;
-      const int64_t qe = oe + int64_t(e) * L + k;
-      if (idx & 1) { gx += A.a.gg1[qe]; gy += A.a.gg3[qe]; }   // down triangle
-      else { gx += A.a.gg0[qe]; gy += A.a.gg2[qe]; }           // up triangle
+      const EdgeTerms et = edge_terms(A, t, e, k);
+      if (idx & 1) { gx += et.gg1; gy += et.gg3; }   // down triangle
+      else { gx += et.gg0; gy += et.gg2; }           // up triangle
     }
     for (int v = 0; v < 3; ++v) {   // gnode(n) = sum_e a_e tr_e / den(n)
       const int n = m.enodes[3 * el + v];
@@ -589,42 +605,42 @@ __global__ void __launch_bounds__(B) r_vert_b(Adj A) {
   const Inst& in = A.in;
   const DevMesh& m = *in.m;
   const int64_t i = lane_index();
-  const int64_t NL = int64_t(m.N) * m.L;
-  if (i >= NL) return;
-  const int L = m.L;
-  const int n = int(i / L), k = int(i - int64_t(n) * L);
+  if (i >= m.n_layer) return;
+  const uint32_t lane = m.layer_lanes[i];
+  const int n = lane_ent(lane), k = lane_lev(lane), L = m.L;
   const int nzmin = m.nzmin[n], nzmax = m.nzmax[n];
   const int64_t base = int64_t(n) * L;
-  const bool layer = k >= nzmin && k < nzmax;
-  // the upwind LO flux of interface j adds to gT[j] and gT[jm], jm = max(j - 1, 0), so
-  // level k takes interface k (layers only) and interface k+1 (also k = nzmin - 1, dry)
-  const bool below = k + 1 >= nzmin && k + 1 < nzmax;
+  // Wet layers only: the dry entries of gTv / gAv / gw stay zero from the workspace's
+  // one-time clear, except level nzmin - 1 (above a cavity's first layer), which the
+  // upwind flux of interface nzmin reaches through jm = nzmin - 1; its thread writes it.
   for (int t = 0; t < in.ntr; ++t) {
     const int64_t oa = t * A.a.sN;
     const double* ghi = A.a.gtmax + oa + base;
     const double* gfv = A.a.gtmin + oa + base;
     double gT = 0.0, gA = 0.0;
-    if (layer) {
+    {
       const double w = in.w_e[base + k], area = m.area[base + k];
       gT += -0.5 * (w + fabs(w)) * area * gfv[k];
       if (k == 0) gT += -0.5 * (w - fabs(w)) * area * gfv[k];
     }
-    if (below) {
+    if (k + 1 < nzmax) {
       const double w = in.w_e[base + k + 1], area = m.area[base + k + 1];
       gT += -0.5 * (w - fabs(w)) * area * gfv[k + 1];
     }
-    if (layer) {
-      // QR4C terms from interfaces k-1 .. k+2 in ascending j (a term that does not reach
-      // k is +0.0; gA starts at +0.0, so adding it changes no bit)
-      for (int j = k - 1; j <= k + 2; ++j) {
-        if (j < nzmin || j >= nzmax) continue;
-        gA += ga_term(in, m, base, j, k, nzmin, nzmax, ghi[j]);
-      }
-    } else {
-      A.a.gw[oa + i] = 0.0;
+    // QR4C terms from interfaces k-1 .. k+2 in ascending j (a term that does not reach
+    // k is +0.0; gA starts at +0.0, so adding it changes no bit)
+    for (int j = k - 1; j <= k + 2; ++j) {
+      if (j < nzmin || j >= nzmax) continue;
+      gA += ga_term(in, m, base, j, k, nzmin, nzmax, ghi[j]);
     }
-    A.a.gTv[oa + i] = gT;
-    A.a.gAv[oa + i] = gA;
+    A.a.gTv[oa + base + k] = gT;
+    A.a.gAv[oa + base + k] = gA;
+    if (k == nzmin && k > 0) {   // dry level above: only the (w - |w|) term of interface k
+      const double w = in.w_e[base + k], area = m.area[base + k];
+      double g = 0.0;
+      g += -0.5 * (w - fabs(w)) * area * gfv[k];
+      A.a.gTv[oa + base + k - 1] = g;
+    }
   }
 }
 
@@ -639,7 +655,7 @@ __global__ void __launch_bounds__(B) r_final(Adj A) {
   const int n = int(i / L), k = int(i - int64_t(n) * L);
   const bool layer = k >= m.nzmin[n] && k < m.nzmax[n];
   for (int t = 0; t < in.ntr; ++t) {
-    const int64_t oa = t * A.a.sN, oe = t * A.a.sEd;
+    const int64_t oa = t * A.a.sN;
     const double gv = A.a.gTv[oa + i];
     double gT, gA = A.a.gAv[oa + i];
     if (!layer) {
@@ -649,9 +665,9 @@ __global__ void __launch_bounds__(B) r_final(Adj A) {
       for (int j = m.ne_off[n]; j < m.ne_off[n + 1]; ++j) {
         const int idx = m.ne_idx[j], e = idx >> 1;
         if (!edge_on(m, e, k)) continue;
-        const int64_t qe = oe + int64_t(e) * L + k;
-        if (idx & 1) { gT += A.a.gT2[qe]; gA += A.a.gA2[qe]; }
-        else { gT += A.a.gT1[qe]; gA += A.a.gA1[qe]; }
+        const EdgeTerms et = edge_terms(A, t, e, k);
+        if (idx & 1) { gT += et.gT2; gA += et.gA2; }
+        else { gT += et.gT1; gA += et.gA1; }
       }
     }
     A.gT[t * in.tstride + i] = gT + kAbNew * gA;
@@ -774,6 +790,8 @@ int fct_plan_reserve_adjoint(FctPlan* P, int max_tracers) {
                                              kAdjElemFields * sE);
   double* p = nullptr;
   FCT_CUDA(cudaMalloc(&p, size_t(nd) * sizeof(double)));
+  // dry-level entries are never written by the reverse kernels and must read as zero
+  FCT_CUDA(cudaMemset(p, 0, size_t(nd) * sizeof(double)));
   if (P->d_adj) cudaFree(P->d_adj);
   P->d_adj = p;
   AdjWorkspace& a = P->aws;
@@ -784,7 +802,7 @@ int fct_plan_reserve_adjoint(FctPlan* P, int max_tracers) {
                      &a.ggnx, &a.ggny, &a.gTp, &a.gTtr, &a.gTv, &a.gAv, &a.gw};
   static_assert(sizeof(node) / sizeof(node[0]) == kAdjNodeFields, "node field count");
   for (double** f : node) *f = take(sN);
-  double** edge[] = {&a.gA1, &a.gA2, &a.gT1, &a.gT2, &a.gg0, &a.gg1, &a.gg2, &a.gg3, &a.gvf};
+  double** edge[] = {&a.gHO, &a.gfl, &a.gvf};
   static_assert(sizeof(edge) / sizeof(edge[0]) == kAdjEdgeFields, "edge field count");
   for (double** f : edge) *f = take(sEd);
   double** elem[] = {&a.gamax, &a.gamin, &a.gtrx, &a.gtry};
@@ -858,7 +876,7 @@ int fct_adjoint(FctPlan* P, const FctFields* f, const double* gT_new, double dt,
   r_tr<<<grid(hm.n_elem, B), B, 0, s>>>(A);
   r_grad_t<<<grid(hm.n_layer, B), B, 0, s>>>(A);
   r_vert_a<<<grid(hm.n_layer, B), B, 0, s>>>(A);
-  r_vert_b<<<grid(int64_t(P->N) * P->L, B), B, 0, s>>>(A);
+  r_vert_b<<<grid(hm.n_layer, B), B, 0, s>>>(A);
   r_final<<<grid(int64_t(P->N) * P->L, B), B, 0, s>>>(A);
   r_uv<<<grid(int64_t(P->E) * P->L, B), B, 0, s>>>(A);
   r_wsum<<<grid(int64_t(P->N) * P->L, B), B, 0, s>>>(A);

@@ -131,13 +131,14 @@ struct AdjWorkspace {
   // node [N, L] per tracer
   double *gdel, *gLOd, *gTd, *gpf, *gmf, *gtmax, *gtmin, *gplus, *gminus, *gLOl;
   double *gtvmax, *gtvmin, *gLOb, *gTb, *gdiv, *ggnx, *ggny, *gTp, *gTtr, *gTv, *gAv, *gw;
-  // edge [Ed, L] per tracer
-  double *gA1, *gA2, *gT1, *gT2, *gg0, *gg1, *gg2, *gg3, *gvf;
+  // edge [Ed, L] per tracer: cotangents of the edge's HO flux, LO flux and volume flux
+  // (the consumers re-derive the per-end terms from them)
+  double *gHO, *gfl, *gvf;
   // element [E, L] per tracer
   double *gamax, *gamin, *gtrx, *gtry;
   int64_t sN, sE, sEd;
 };
-constexpr int kAdjNodeFields = 22, kAdjEdgeFields = 9, kAdjElemFields = 4;
+constexpr int kAdjNodeFields = 22, kAdjEdgeFields = 3, kAdjElemFields = 4;
 
 }  // namespace fct
 
