@@ -33,6 +33,11 @@ sys.path.insert(0, str(ROOT))
 METRIC = "FCT node-level updates/s FP64, batched vs plain on 1 B200; serve p50/p99 ms"
 UNIT = "node-level updates/s"
 FALLBACK_HBM_GBS = 6650.0
+# DRAM bytes (read + write) per node-level update of the four fused tracer kernels, from
+# one ncu capture of the small case of the batched workload (2 members x 8 tracers of the
+# CORE2-size mesh: 12.41 GB per FCT step / 48.76 M updates); the tracer-independent volume
+# flux kernel (2.6% of the step) is not included. Scaled to a launch by the updates it does.
+TRAFFIC_B_PER_UPDATE = 254.6
 
 
 def peaks() -> dict:
@@ -253,7 +258,10 @@ def run_ours(args, D: Dist) -> dict | None:
                roofline=dict(bound="hbm", kernel="fused FCT step (vflux, node_lo, edge_adf, node_limit, node_final)",
                              achieved=achieved, peak=pk["hbm_gbs"], unit="GB/s",
                              frac=achieved / pk["hbm_gbs"], peak_source=pk["source"],
-                             traffic=None, alg_bytes_per_step=alg),
+                             traffic=TRAFFIC_B_PER_UPDATE * info["updates_per_step"],
+                             traffic_note="ncu DRAM bytes of the 4 tracer kernels, small-case "
+                                          "capture scaled by updates",
+                             alg_bytes_per_step=alg),
                gpu_launches=n_kernels * S * args.steps,
                tuning=dict(chunk=ens.chunk, candidates_ms_per_2_steps=tune))
 
