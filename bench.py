@@ -299,6 +299,7 @@ def run_ours(args, D: Dist) -> dict | None:
         tp = e0.elapsed_time(e1) / 1e3
         out["plain"] = dict(value=reps * cfg["ntr"] * mesh.n_wet_layers / tp, unit=UNIT,
                             how="fct_forward, 1 tracer per call, 1 FCT step per call")
+    tuned = ens.chunk
     ens.close()   # the end-to-end run below builds its own ensemble
     del ens
     torch.cuda.empty_cache()
@@ -310,51 +311,67 @@ def run_ours(args, D: Dist) -> dict | None:
         del inp
         torch.cuda.empty_cache()
         if not args.no_e2e:
-            out["e2e"] = e2e_host(args, mesh, cfg, dev)
+            out["e2e"] = e2e_host(args, mesh, cfg, dev, per_thread=tuned)
         if not args.no_cpu:
             out["cpu_baseline"] = cpu_oracle_rate(mesh, host, cfg["ntr"], cfg["dt"])
     return out
 
 
-def e2e_host(args, mesh, cfg, dev) -> dict:
+def e2e_host(args, mesh, cfg, dev, per_thread: int = 0) -> dict:
     """The same metric through the public ensemble API with HOST buffers: every bench step
     copies each member's inputs (T, T_old, uv, w_e) from pinned host memory, runs the
-    FCT steps and copies the final T back; copies are inside the timed region."""
+    FCT steps and copies the final T back; copies are inside the timed region. Members are
+    pipelined over three CUDA streams (one single-member ensemble each), so one member's
+    copies overlap another's FCT steps, as a user streaming members through the API would."""
     import torch
 
     from fesom_jax_b200 import workloads as W
     from fesom_jax_b200.ensemble import Ensemble
     nm = min(args.e2e_members, cfg["members"])
     thick = W.rest_thickness_gpu(mesh, dev)
-    ens = Ensemble(device=dev.index, workspace_budget=int(args.workspace_gb * (1 << 30)))
-    host = []
+    streams = [torch.cuda.Stream(dev) for _ in range(3)]
+    ens, host = [], []
     for i in range(nm):
         inp = W.member_inputs_gpu(mesh, seed=500000 + i, ntr=cfg["ntr"], device=dev,
                                   thickness=thick, sigma=cfg["sigma"], n_vortices=cfg["n_vortices"])
-        ens.add_member(mesh, inp["uv"], inp["w_e"], inp["helem"], inp["hnode"], inp["hnode_new"],
-                       inp["T"], inp["T_old"], cfg["dt"])
-        host.append({k: inp[k].cpu().pin_memory() for k in ("uv", "w_e")})
+        e = Ensemble(device=dev.index, workspace_budget=int(args.workspace_gb * (1 << 30)))
+        e.add_member(mesh, inp["uv"], inp["w_e"], inp["helem"], inp["hnode"], inp["hnode_new"],
+                     inp["T"], inp["T_old"], cfg["dt"])
+        h = {k: inp[k].cpu().pin_memory() for k in ("uv", "w_e")}
         # host state in the resident interleaved layout [N, nl, ntr]
         for k in ("T", "T_old"):
-            host[-1][k] = inp[k].permute(1, 2, 0).contiguous().cpu().pin_memory()
-        host[-1]["out"] = torch.empty_like(host[-1]["T"]).pin_memory()
+            h[k] = inp[k].permute(1, 2, 0).contiguous().cpu().pin_memory()
+        h["out"] = torch.empty_like(h["T"]).pin_memory()
+        ens.append(e)
+        host.append(h)
         del inp
     torch.cuda.empty_cache()
-    ens.build()
+    for e in ens:
+        e.build()
+        if per_thread:   # the main run's autotuned tracers per thread
+            e.set_chunk(per_thread)
     S = cfg["fct_steps"]
-    stream = torch.cuda.current_stream(dev)
+    main = torch.cuda.current_stream(dev)
     h2d = sum(h[k].numel() * 8 for h in host for k in ("T", "T_old", "uv", "w_e"))
     d2h = sum(h["out"].numel() * 8 for h in host)
 
     def one():
-        for i, h in enumerate(host):
-            mb = ens.members[i]
-            ens.set_state(i, h["T"], h["T_old"], non_blocking=True, interleaved=True)
-            mb.uv.copy_(h["uv"], non_blocking=True)
-            mb.w_e.copy_(h["w_e"], non_blocking=True)
-        ens.run(S)
-        for i, h in enumerate(host):
-            h["out"].copy_(ens.state_interleaved(i)[0], non_blocking=True)
+        start = torch.cuda.Event()
+        start.record(main)
+        for i, (e, h) in enumerate(zip(ens, host)):
+            st = streams[i % len(streams)]
+            st.wait_event(start)
+            with torch.cuda.stream(st):
+                mb = e.members[0]
+                e.set_state(0, h["T"], h["T_old"], non_blocking=True, interleaved=True)
+                mb.uv.copy_(h["uv"], non_blocking=True)
+                mb.w_e.copy_(h["w_e"], non_blocking=True)
+                e.run(S, stream=st.cuda_stream)
+                h["out"].copy_(e.state_interleaved(0)[0], non_blocking=True)
+        for st in streams:
+            done = torch.cuda.Event()
+            done.record(st)
+            main.wait_event(done)
 
     for _ in range(max(1, min(args.warmup, 2))):
         one()
@@ -362,149 +379,20 @@ def e2e_host(args, mesh, cfg, dev) -> dict:
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     reps = max(1, min(args.steps, 3))
     w0 = time.perf_counter()
-    e0.record(stream)
+    e0.record(main)
     for _ in range(reps):
         one()
-    e1.record(stream)
+    e1.record(main)
     torch.cuda.synchronize()
     wall = time.perf_counter() - w0
     t = max(e0.elapsed_time(e1) / 1e3, 1e-9)
-    upd = ens.info()["updates_per_step"] * S * reps
-    ens.close()
+    upd = sum(e.info()["updates_per_step"] for e in ens) * S * reps
+    for e in ens:
+        e.close()
     return dict(value=upd / t, unit=UNIT, h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h,
-                members=nm, steps=reps, wall_s=wall,
-                how="Ensemble API, pinned host buffers in/out every step")
-
-
-# ---------------------------------------------------------------- adjoint (config 3)
-def run_adjoint(args, D: Dist) -> dict:
-    """Gradient of loss = sum_n areasvol[n,0] (T_K[n,0] - target_n)^2 after K = 10 FCT
-    steps on the CORE2-size mesh, w.r.t. the initial T and uv, with w_e = compute_w(uv)
-    inside the loss (chain_loss_and_grad: per-step recomputation checkpointing). Reports
-    its cost against the forward alone (compute_w + K steps) and central finite
-    differences (eps = 1e-7) along 20 seeded directions (10 for T0, 10 for uv).
-
-    The velocities here are white noise (sigma 0.002 m/s, vertical CFL < 1): a
-    streamfunction flow is
-    discretely divergence-free, so w = compute_w(uv) is roundoff and the upwind |w| sits
-    at its kink, where central differences and any subgradient disagree."""
-    import torch
-
-    from fesom_jax_b200 import inputs as I
-    from fesom_jax_b200 import workloads as W
-    from fesom_jax_b200.adjoint import chain_loss_and_grad
-    from fesom_jax_b200.ale import compute_w
-    from fesom_jax_b200.tracer_adv import get_plan
-    torch.cuda.set_device(D.local_rank)
-    dev = torch.device("cuda", D.local_rank)
-    mesh = W.make_workload_mesh("batched", seed=0)
-    K, dt = 10, 1800.0
-    f = I.make_fields(mesh, seed=3 + D.rank, ab2=True, kind="white", sigma=0.002)
-    d = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev)  # noqa: E731
-    T0, To0, uv = d(f.tracers[0]), d(f.tracers_old[0]), d(f.uv)
-    helem, hn, hnn = d(f.helem), d(f.hnode), d(f.hnode_new)
-    target = torch.from_numpy(np.random.default_rng(7).normal(15.0, 3.0, mesh.nod2D))
-    plan = get_plan(mesh, D.local_rank)
-    stream = torch.cuda.current_stream(dev)
-
-    def forward():
-        w = compute_w(mesh, uv, helem)
-        T, To = T0, To0
-        for _ in range(K):
-            T, To = plan.forward(uv, w, helem, hn, hnn, T, To, dt), T
-        return T
-
-    def grad():
-        return chain_loss_and_grad(mesh, T0, uv, helem, hn, hnn, target, K, dt=dt, T_old0=To0)
-
-    def timed(fn, reps):
-        for _ in range(max(args.warmup, 1)):
-            fn()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(reps):
-            fn()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / reps / 1e3
-
-    D.barrier()
-    t_fwd = timed(forward, args.steps)
-    t_grad = timed(grad, args.steps)
-    t = D.max(t_grad, dev)
-    loss, gT0, guv = grad()
-    # central finite differences
-    rng = np.random.default_rng(2024)
-    lm = torch.from_numpy(mesh.node_layer_mask).to(dev)
-    em = torch.from_numpy(mesh.elem_layer_mask).to(dev)[:, :, None]
-    rel = []
-    eps = 1e-7
-    for j in range(0 if args.no_fd else 20):
-        if j < 10:
-            v = d(rng.normal(size=T0.shape)) * lm
-            Lp = chain_loss_and_grad(mesh, T0 + eps * v, uv, helem, hn, hnn, target, K, dt=dt,
-                                     T_old0=To0)[0]
-            Lm = chain_loss_and_grad(mesh, T0 - eps * v, uv, helem, hn, hnn, target, K, dt=dt,
-                                     T_old0=To0)[0]
-            ad = float((gT0 * v).sum())
-        else:
-            v = d(rng.normal(size=uv.shape)) * em
-            Lp = chain_loss_and_grad(mesh, T0, uv + eps * v, helem, hn, hnn, target, K, dt=dt,
-                                     T_old0=To0)[0]
-            Lm = chain_loss_and_grad(mesh, T0, uv - eps * v, helem, hn, hnn, target, K, dt=dt,
-                                     T_old0=To0)[0]
-            ad = float((guv * v).sum())
-        fd = (Lp - Lm) / (2 * eps)
-        rel.append(abs(fd - ad) / max(abs(ad), 1e-300))
-    upd = K * mesh.n_wet_layers * D.world
-    return dict(value=upd / t, t=t * args.steps, mesh=mesh, t_fwd=t_fwd, t_grad=t_grad,
-                cfg=dict(members=1, ntr=1, fct_steps=K, dt=dt),
-                adjoint=dict(forward_ms=t_fwd * 1e3, loss_and_grad_ms=t_grad * 1e3,
-                             ratio=t_grad / t_fwd, K=K, loss=loss,
-                             fd_rel_err_max=float(max(rel)) if rel else None,
-                             fd_rel_err_median=float(np.median(rel)) if rel else None,
-                             fd_directions=len(rel), fd_eps=eps, max_cfl_z=float(I.max_cfl_z(
-                                 mesh, f.w_e, f.hnode, dt)),
-                             how="chain_loss_and_grad (fct_forward x K, fct_adjoint x K, "
-                                 "fct_compute_w_adjoint) vs compute_w + fct_forward x K"))
-
-
-# ---------------------------------------------------------------- serving (config 5)
-def run_serve(args, D: Dist) -> dict:
-    """Continuous-batching serving (ServingEngine): Poisson arrivals at 200 req/s mixing
-    the pi, CORE2-size and 1.3M-node meshes (0.6/0.3/0.1), each request K ~ U{1..50} FCT
-    steps of a resident member (T, S), 20 % with the adjoint of the last step; admission
-    by a 150 GB HBM budget. The offered load is far above one GPU's capacity, so the
-    stream is bounded (``--serve-seconds`` of arrivals) and the run also reports a
-    sustainable-rate stream and the serial plain-launch baseline on the same requests."""
-    import torch
-
-    from fesom_jax_b200 import workloads as W
-    from fesom_jax_b200.mesh import pi_mesh
-    from fesom_jax_b200.serve import ServingEngine, poisson_requests
-    torch.cuda.set_device(D.local_rank)
-    meshes = {"pi": pi_mesh(), "core2": W.make_workload_mesh("batched", seed=0),
-              "large": W.make_workload_mesh("large", seed=0)}
-    dts = {"pi": 3600.0, "core2": 1800.0, "large": 600.0}
-    eng = ServingEngine(meshes, dts, budget_bytes=150e9, device=D.local_rank, ntr=2,
-                        workspace_bytes=45e9, sigma={"large": 0.2})
-    out = {}
-    reqs = poisson_requests(200.0, args.serve_seconds, seed=1 + D.rank)
-    clocks = ClockSampler(gpu_index(D.local_rank))
-    clocks.start()
-    sat = eng.run(reqs, time_limit=args.serve_limit)
-    out["clocks"] = clocks.stop()
-    out["saturated"] = dict(rate_req_s=200.0, arrivals_s=args.serve_seconds, **sat)
-    cap = sat["throughput_req_s"]
-    low = poisson_requests(max(0.5 * cap, 0.2), args.serve_seconds * 4, seed=100 + D.rank)
-    out["sustainable"] = dict(rate_req_s=max(0.5 * cap, 0.2),
-                              **eng.run(low, time_limit=args.serve_limit))
-    out["serial"] = eng.run_serial(reqs, time_limit=args.serve_limit / 2)
-    eng.close()
-    out["value"] = sat["updates_per_s"] * D.world
-    out["t"] = sat["wall_s"]
-    return out
+                members=nm, steps=reps, wall_s=wall, streams=len(streams),
+                how="Ensemble API, pinned host buffers in/out every step, members pipelined "
+                    "over 3 streams")
 
 
 # ------------------------------------------------------------------ reference arm
