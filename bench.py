@@ -221,7 +221,8 @@ def run_ours(args, D: Dist) -> dict | None:
                                   thickness=thick, sigma=cfg["sigma"],
                                   n_vortices=cfg["n_vortices"])
         ens.add_member(mesh, inp["uv"], inp["w_e"], inp["helem"], inp["hnode"],
-                       inp["hnode_new"], inp["T"], inp["T_old"], cfg["dt"], Kv=Kv)
+                       inp["hnode_new"], inp["T"], inp["T_old"], cfg["dt"], Kv=Kv,
+                       derive_w=args.derive_w)
         member_inputs.append(inp if i == 0 else None)
         del inp
     torch.cuda.empty_cache()   # hand the input temporaries back before the arena is allocated
@@ -491,6 +492,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fd", action="store_true", help="adjoint: skip the FD check")
+    ap.add_argument("--derive-w", action="store_true",
+                    help="batched/large: derive w_e = compute_w(uv) inside every step's graph")
     ap.add_argument("--vdiff", action="store_true",
                     help="batched/large: implicit vertical diffusion after every FCT step")
     args = ap.parse_args()
@@ -520,7 +523,8 @@ def main():
                 warmup=args.warmup, ms_per_step=r["t"] / args.steps * 1e3,
                 higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64",
                 data="synthetic (seeded mesh, velocities and tracers)",
-                config=dict(workload_config(args.config, cfg, mesh), vertical_diffusion=bool(args.vdiff)),
+                config=dict(workload_config(args.config, cfg, mesh), vertical_diffusion=bool(args.vdiff),
+                            derive_w=bool(args.derive_w)),
                 roofline=r["roofline"],
                 clocks=r["clocks"], gpu_launches=r["gpu_launches"],
                 fct_step_ms=r["fct_step_ms"], stage_ms=r["prof"], finite=r["finite"],

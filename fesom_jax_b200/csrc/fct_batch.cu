@@ -142,6 +142,11 @@ int fct_batch_create(const FctInstance* insts, int n, int64_t budget, FctBatch**
         in.ws = ws;
         in.dt = q.dt;
         in.ntr = q.ntr;
+        in.w_derived = q.w_derived;   // optional producer: w_e = compute_w(uv, helem)
+        if (q.w_derived) {
+          in.w_e = q.w_derived;
+          d.any_derive_w = true;
+        }
         in.Kv = q.Kv;   // optional diffusion epilogue, in place on T_new
         in.vd_T = in.T_new;
         in.sw_tracer = -1;
@@ -207,7 +212,7 @@ int fct_batch_info(const FctBatch* B, int64_t out[6]) {
     }
     const int stages = (g.dims.fused ? 4 : 7) + (g.dims.any_wi ? 1 : 0) +
                        (g.dims.any_vdiff ? 1 : 0);
-    launches += 1 + int64_t(stages) * per_chunk_launches;
+    launches += 1 + (g.dims.any_derive_w ? 1 : 0) + int64_t(stages) * per_chunk_launches;
   }
   out[4] = wmax;
   out[5] = launches;
@@ -430,6 +435,10 @@ int fct_serve_step(FctServe* S, const FctInstance* insts, const int32_t* phases,
     off += workspace_doubles_fused(P->N, P->Ed, P->L, q.ntr);
     in.dt = q.dt;
     in.ntr = q.ntr;
+    if (q.w_derived) {   // producer: w_e = compute_w(uv, helem) at this step
+      in.w_derived = q.w_derived;
+      in.w_e = q.w_derived;
+    }
   }
   cudaError_t e = cudaMemcpyAsync(S->d_tab, S->h_tab, size_t(n) * sizeof(Inst),
                                   cudaMemcpyHostToDevice, s);
@@ -455,6 +464,8 @@ int fct_serve_step(FctServe* S, const FctInstance* insts, const int32_t* phases,
     d.ntr = ntr;
     d.chunk = 0;
     d.per_thread = ntr >= 4 ? 4 : ntr;
+    for (int j = j0; j < j1; ++j)
+      if (insts[order[j]].w_derived) d.any_derive_w = true;
     d.any_wi = false;
     d.copy_dry = false;
     Inst dummy{};

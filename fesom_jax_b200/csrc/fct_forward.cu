@@ -1159,6 +1159,10 @@ int launch_forward_events(const Inst& single, const Inst* tab, int n, const Laun
       ++stage;
     };
     if (ci == 0) {   // the volume flux is shared by all tracers
+      if (tab && d.any_derive_w) {   // producer: w_e from continuity, in the same graph
+        const int st = launch_compute_w_tab(tab, n, d.max_nodes, s);
+        if (st) return st;
+      }
       if (tab) k_vflux_n<<<grid(d.max_edge), B, 0, s>>>(tab);
       else k_vflux_1<<<grid(d.max_edge), B, 0, s>>>(single);
     }

@@ -36,6 +36,7 @@ struct LaunchDims {
   bool any_wi;      // launch the implicit w_i stage
   bool copy_dry;    // launch the dry-level copy
   bool any_vdiff = false;  // launch the implicit vertical diffusion after each chunk
+  bool any_derive_w = false;  // derive w_e from uv (compute_w) before the step
   bool fused = true;  // fused stages (lean workspace); false: every stage kernel writes its
                       // intermediates (what the reverse pass reads)
 };
@@ -56,6 +57,8 @@ int launch_forward_stages(const Inst& single, const LaunchDims& d, cudaStream_t 
 
 // Copy T's dry levels into T_new for ``n`` instances of ``tab`` (ignores Inst::copy_dry).
 int launch_copy_dry(const Inst* tab, int n, int64_t max_dense, cudaStream_t s);
+// compute_w of every table instance with w_derived set (fct_producers.cu).
+int launch_compute_w_tab(const Inst* tab, int n, int64_t max_nodes, cudaStream_t s);
 // Implicit vertical diffusion alone (fct_vert_diff): single instance, tracer-major.
 int launch_vdiff(const Inst& single, const LaunchDims& d, cudaStream_t s);
 

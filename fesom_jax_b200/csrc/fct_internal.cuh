@@ -120,6 +120,7 @@ struct Inst {
   const double *Kv, *vd_T, *vd_Z3d, *bc_surf, *sw_3d;
   int64_t bc_stride;   // doubles between tracers' bc_surf rows
   int sw_tracer;       // tracer that takes the shortwave divergence (-1: none)
+  double* w_derived;   // batched producer: w_e = compute_w(uv, helem) written here first
   const double *Z3d, *zbar3, *w_i;
   Workspace ws;
   double dt;

@@ -35,7 +35,7 @@ class FctInstance(C.Structure):
     _fields_ = [("plan", C.c_void_p), ("uv", C.c_void_p), ("w_e", C.c_void_p),
                 ("helem", C.c_void_p), ("hnode", C.c_void_p), ("hnode_new", C.c_void_p),
                 ("buf", C.c_void_p * 3), ("ntr", C.c_int), ("dt", C.c_double),
-                ("Kv", C.c_void_p)]
+                ("Kv", C.c_void_p), ("w_derived", C.c_void_p)]
 
 
 def _bind_batch(L):
@@ -72,6 +72,7 @@ class Member:
     hnode_new: object
     buf: object         # torch [3, N, nl, ntr] (tracers interleaved innermost)
     Kv: object = None   # torch [N, nl] or None (no vertical diffusion)
+    derive_w: bool = False   # w_e recomputed from uv each step (into w_e)
 
 
 class Ensemble:
@@ -95,10 +96,12 @@ class Ensemble:
         return p
 
     def add_member(self, mesh: Mesh, uv, w_e, helem, hnode, hnode_new, T, T_old, dt: float,
-                   Kv=None) -> int:
+                   Kv=None, derive_w: bool = False) -> int:
         """Add a member (host numpy or device tensors); ``T``/``T_old`` are ``[ntr, N, nl]``.
         With ``Kv`` (``[N, nl]``) every step is followed by the implicit vertical diffusion
-        of fesom_jax/tracer_diff.py:68-123 (step.py:452), in the same graph."""
+        of fesom_jax/tracer_diff.py:68-123 (step.py:452), in the same graph. With
+        ``derive_w`` every step first derives ``w_e = compute_w(uv, helem)``
+        (fesom_jax/ale.py:309-365, step.py:367) on the GPU and ``w_e`` may be None."""
         if self._h is not None:
             raise RuntimeError("members must be added before the ensemble is built")
         t = self.torch
@@ -121,8 +124,11 @@ class Ensemble:
         buf[1].copy_(T.permute(1, 2, 0))
         buf[2].copy_(T.permute(1, 2, 0))
         self.plan(mesh)
+        if derive_w:
+            w_e = t.empty((N, nl), dtype=t.float64, device=dev)
         self.members.append(Member(mesh, ntr, float(dt), d(uv), d(w_e), d(helem), d(hnode),
-                                   d(hnode_new), buf, d(Kv) if Kv is not None else None))
+                                   d(hnode_new), buf, d(Kv) if Kv is not None else None,
+                                   derive_w))
         return len(self.members) - 1
 
     # ------------------------------------------------------------------ build
@@ -141,6 +147,7 @@ class Ensemble:
                 q.buf[j] = mb.buf[j].data_ptr()
             q.ntr, q.dt = mb.ntr, mb.dt
             q.Kv = mb.Kv.data_ptr() if mb.Kv is not None else None
+            q.w_derived = mb.w_e.data_ptr() if mb.derive_w else None
         h = C.c_void_p()
         _lib.check(L.fct_batch_create(arr, n, self.workspace_budget, C.byref(h)))
         self._h = h

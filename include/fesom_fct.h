@@ -222,6 +222,9 @@ typedef struct FctInstance {
   double dt;
   const double* Kv;         /* optional [nod2D,nl]: implicit vertical diffusion after each
                                step (tracer_diff.py:68-123, step.py:452; NULL = off) */
+  double* w_derived;        /* optional [nod2D,nl]: each step first derives w_e =
+                               compute_w(uv, helem) (ale.py:309-365, step.py:367) into this
+                               buffer and advects with it (w_e is then ignored); NULL = off */
 } FctInstance;
 
 typedef struct FctBatch FctBatch;

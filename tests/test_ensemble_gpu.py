@@ -125,3 +125,25 @@ def test_chunked_workspace_equals_plain(torch, pi, per_thread):
     prof = ens.profile_step()
     assert prof["node_final"] > 0.0
     ens.close()
+
+
+def test_derived_w_equals_compute_w_then_fct(torch, pi):
+    """A member with derive_w runs compute_w(uv, helem) inside every step's graph; it
+    equals the plain compute_w call followed by the plain FCT calls, bit for bit."""
+    from fesom_jax_b200.ale import compute_w
+    from fesom_jax_b200.ensemble import Ensemble
+    f = I.make_fields(pi, seed=31, n_passive=1, ab2=True)
+    ens = Ensemble(device=0)
+    ens.add_member(pi, f.uv, None, f.helem, f.hnode, f.hnode_new, f.tracers, f.tracers_old,
+                   DT, derive_w=True)
+    ens.build()
+    # compute_w + vflux + 4 fused stages x 2 launches (3 tracers: a 2-tracer and a 1-tracer split)
+    assert ens.info()["launches_per_step"] == 1 + 1 + 4 * 2
+    ens.run(STEPS)
+    torch.cuda.synchronize()
+    d = lambda x: torch.from_numpy(np.ascontiguousarray(x)).cuda()  # noqa: E731
+    w = compute_w(pi, d(f.uv), d(f.helem))
+    T, To = _plain(torch, pi, I.Fields(**{**f.__dict__, "w_e": w.cpu().numpy()}), STEPS)
+    Tb, Tob = ens.state(0)
+    assert np.array_equal(Tb.cpu().numpy(), T) and np.array_equal(Tob.cpu().numpy(), To)
+    ens.close()
