@@ -139,3 +139,40 @@ def ice_cases(m, seed=0):
         "step_500": dict(a=a, m=hi, ms=hs, u=u, v=v, dt=500.0),
         "fast_3600": dict(a=a, m=hi, ms=hs, u=5.0 * u, v=5.0 * v, dt=3600.0),
     }
+
+
+CAVITY_GOLDEN = Path(__file__).resolve().parent / "golden" / "fct_cavity_golden.npz"
+CAVITY_ARRAYS = ("ulevels", "ulevels_nod2D", "ulevels_nod2D_max", "area", "areasvol")
+
+
+def cavity_arrays(m):
+    """An ice-shelf cavity on ``m`` (a cavity-free mesh): the cells whose three nodes lie in
+    the northernmost ~15% of deep nodes start at level 3 (two dry layers on top); node
+    ``ulevels_nod2D`` is the min and ``ulevels_nod2D_max`` the max over a node's cells;
+    ``area``/``areasvol`` are zero above a node's first wet layer. Returns the five arrays."""
+    lat = m.coord_nod2D[:, 1]
+    deep = m.nlevels_nod2D >= 12
+    cav = deep & (lat >= np.quantile(lat[deep], 0.85))
+    en = m.elem_nodes
+    ul = np.where(cav[en].all(axis=1), 3, 1).astype(np.int32)
+    uln = np.full(m.nod2D, 10 ** 6, np.int64)
+    ulx = np.zeros(m.nod2D, np.int64)
+    for v in range(3):
+        np.minimum.at(uln, en[:, v], ul)
+        np.maximum.at(ulx, en[:, v], ul)
+    uln = uln.astype(np.int32)
+    ulx = ulx.astype(np.int32)
+    k = np.arange(m.nl)[None, :]
+    dry_top = k < (uln - 1)[:, None]
+    area = np.where(dry_top, 0.0, m.area)
+    areasvol = np.where(dry_top, 0.0, m.areasvol)
+    return dict(ulevels=ul, ulevels_nod2D=uln, ulevels_nod2D_max=ulx, area=area,
+                areasvol=areasvol)
+
+
+def cavity_mesh(m):
+    """``m`` with the cavity of :func:`cavity_arrays` (a new Mesh; masks re-derived)."""
+    from fesom_jax_b200.mesh import FCT_FIELDS, Mesh
+    fields = {f: getattr(m, f) for f in FCT_FIELDS}
+    fields.update(cavity_arrays(m))
+    return Mesh(**fields, name=m.name + "_cavity")
