@@ -165,6 +165,13 @@ int validate_desc(const FctMeshDesc* d) {
   for (int i = 0; i < nie; ++i)
     if (d->nod_in_elem2D[i] < 0 || d->nod_in_elem2D[i] >= E)
       return set_error(FCT_ERR_INVALID, "nod_in_elem2D[%d] out of range", i);
+  for (int n = 0; n < N; ++n)   // every listed cell has the node as a vertex
+    for (int j = d->nod_in_elem2D_offsets[n]; j < d->nod_in_elem2D_offsets[n + 1]; ++j) {
+      const int* en = d->elem_nodes + 3 * size_t(d->nod_in_elem2D[j]);
+      if (en[0] != n && en[1] != n && en[2] != n)
+        return set_error(FCT_ERR_INVALID, "nod_in_elem2D lists element %d for node %d, "
+                         "which is not one of its vertices", d->nod_in_elem2D[j], n);
+    }
   return FCT_OK;
 }
 

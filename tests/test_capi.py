@@ -4,6 +4,7 @@ import ctypes
 import re
 from pathlib import Path
 
+import numpy as np
 import pytest
 
 ROOT = Path(__file__).resolve().parents[1]
@@ -42,3 +43,43 @@ def test_plan_create_rejects_bad_mesh(pi):
     h = ctypes.c_void_p()
     st = _lib.lib().fct_plan_create(ctypes.byref(desc), 0, 1, ctypes.byref(h))
     assert st == -1 and b"out of range" in _lib.lib().fct_last_error()
+
+
+def _desc_with(pi, keep, field, mutate):
+    from fesom_jax_b200 import _lib
+    desc = _lib.mesh_desc(pi, keep)
+    names = [f for f, _ in _lib.FctMeshDesc._fields_[4:]]
+    arr = keep[names.index(field)].copy()
+    mutate(arr)
+    keep.append(arr)
+    ptype = _lib.i32p if arr.dtype == np.int32 else _lib.f64p
+    setattr(desc, field, arr.ctypes.data_as(ptype))
+    return desc
+
+
+@pytest.mark.parametrize("field,mutate,msg", [
+    ("elem_nodes", lambda a: a.__setitem__((3, 1), -1), b"elem_nodes"),
+    ("edge_tri", lambda a: a.__setitem__((2, 0), -1), b"edge_tri"),
+    ("nlevels", lambda a: a.__setitem__(5, 1000), b"level range"),
+    ("ulevels_nod2D", lambda a: a.__setitem__(7, 0), b"level range"),
+    ("nod_in_elem2D", lambda a: a.__setitem__(0, a[-1]), b"not one of its vertices"),
+])
+def test_plan_create_rejects_inconsistent_arrays(pi, field, mutate, msg):
+    """Host-side validation (before any CUDA call): indices in range, level ranges
+    consistent, node->element lists naming cells that contain the node."""
+    from fesom_jax_b200 import _lib
+    keep = []
+    desc = _desc_with(pi, keep, field, mutate)
+    h = ctypes.c_void_p()
+    st = _lib.lib().fct_plan_create(ctypes.byref(desc), 0, 1, ctypes.byref(h))
+    assert st == -1 and msg in _lib.lib().fct_last_error(), _lib.lib().fct_last_error()
+
+
+def test_plan_create_rejects_too_many_levels(pi):
+    from fesom_jax_b200 import _lib
+    keep = []
+    desc = _lib.mesh_desc(pi, keep)
+    desc.nl = 129
+    h = ctypes.c_void_p()
+    st = _lib.lib().fct_plan_create(ctypes.byref(desc), 0, 1, ctypes.byref(h))
+    assert st == -1 and b"nl=129" in _lib.lib().fct_last_error()
