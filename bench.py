@@ -396,6 +396,137 @@ def e2e_host(args, mesh, cfg, dev, per_thread: int = 0) -> dict:
                     "over 3 streams")
 
 
+# ---------------------------------------------------------------- adjoint (config 3)
+def run_adjoint(args, D: Dist) -> dict:
+    """Gradient of loss = sum_n areasvol[n,0] (T_K[n,0] - target_n)^2 after K = 10 FCT
+    steps on the CORE2-size mesh, w.r.t. the initial T and uv, with w_e = compute_w(uv)
+    inside the loss (chain_loss_and_grad: per-step recomputation checkpointing). Reports
+    its cost against the forward alone (compute_w + K steps) and central finite
+    differences (eps = 1e-7) along 20 seeded directions (10 for T0, 10 for uv).
+
+    The velocities here are white noise (sigma 0.002 m/s, vertical CFL < 1): a
+    streamfunction flow is
+    discretely divergence-free, so w = compute_w(uv) is roundoff and the upwind |w| sits
+    at its kink, where central differences and any subgradient disagree."""
+    import torch
+
+    from fesom_jax_b200 import inputs as I
+    from fesom_jax_b200 import workloads as W
+    from fesom_jax_b200.adjoint import chain_loss_and_grad
+    from fesom_jax_b200.ale import compute_w
+    from fesom_jax_b200.tracer_adv import get_plan
+    torch.cuda.set_device(D.local_rank)
+    dev = torch.device("cuda", D.local_rank)
+    mesh = W.make_workload_mesh("batched", seed=0)
+    K, dt = 10, 1800.0
+    f = I.make_fields(mesh, seed=3 + D.rank, ab2=True, kind="white", sigma=0.002)
+    d = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev)  # noqa: E731
+    T0, To0, uv = d(f.tracers[0]), d(f.tracers_old[0]), d(f.uv)
+    helem, hn, hnn = d(f.helem), d(f.hnode), d(f.hnode_new)
+    target = torch.from_numpy(np.random.default_rng(7).normal(15.0, 3.0, mesh.nod2D))
+    plan = get_plan(mesh, D.local_rank)
+    stream = torch.cuda.current_stream(dev)
+
+    def forward():
+        w = compute_w(mesh, uv, helem)
+        T, To = T0, To0
+        for _ in range(K):
+            T, To = plan.forward(uv, w, helem, hn, hnn, T, To, dt), T
+        return T
+
+    def grad():
+        return chain_loss_and_grad(mesh, T0, uv, helem, hn, hnn, target, K, dt=dt, T_old0=To0)
+
+    def timed(fn, reps):
+        for _ in range(max(args.warmup, 1)):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps / 1e3
+
+    D.barrier()
+    t_fwd = timed(forward, args.steps)
+    t_grad = timed(grad, args.steps)
+    t = D.max(t_grad, dev)
+    loss, gT0, guv = grad()
+    # central finite differences
+    rng = np.random.default_rng(2024)
+    lm = torch.from_numpy(mesh.node_layer_mask).to(dev)
+    em = torch.from_numpy(mesh.elem_layer_mask).to(dev)[:, :, None]
+    rel = []
+    eps = 1e-7
+    for j in range(0 if args.no_fd else 20):
+        if j < 10:
+            v = d(rng.normal(size=T0.shape)) * lm
+            Lp = chain_loss_and_grad(mesh, T0 + eps * v, uv, helem, hn, hnn, target, K, dt=dt,
+                                     T_old0=To0)[0]
+            Lm = chain_loss_and_grad(mesh, T0 - eps * v, uv, helem, hn, hnn, target, K, dt=dt,
+                                     T_old0=To0)[0]
+            ad = float((gT0 * v).sum())
+        else:
+            v = d(rng.normal(size=uv.shape)) * em
+            Lp = chain_loss_and_grad(mesh, T0, uv + eps * v, helem, hn, hnn, target, K, dt=dt,
+                                     T_old0=To0)[0]
+            Lm = chain_loss_and_grad(mesh, T0, uv - eps * v, helem, hn, hnn, target, K, dt=dt,
+                                     T_old0=To0)[0]
+            ad = float((guv * v).sum())
+        fd = (Lp - Lm) / (2 * eps)
+        rel.append(abs(fd - ad) / max(abs(ad), 1e-300))
+    upd = K * mesh.n_wet_layers * D.world
+    return dict(value=upd / t, t=t * args.steps, mesh=mesh, t_fwd=t_fwd, t_grad=t_grad,
+                cfg=dict(members=1, ntr=1, fct_steps=K, dt=dt),
+                adjoint=dict(forward_ms=t_fwd * 1e3, loss_and_grad_ms=t_grad * 1e3,
+                             ratio=t_grad / t_fwd, K=K, loss=loss,
+                             fd_rel_err_max=float(max(rel)) if rel else None,
+                             fd_rel_err_median=float(np.median(rel)) if rel else None,
+                             fd_directions=len(rel), fd_eps=eps, max_cfl_z=float(I.max_cfl_z(
+                                 mesh, f.w_e, f.hnode, dt)),
+                             how="chain_loss_and_grad (fct_forward x K, fct_adjoint x K, "
+                                 "fct_compute_w_adjoint) vs compute_w + fct_forward x K"))
+
+
+# ---------------------------------------------------------------- serving (config 5)
+def run_serve(args, D: Dist) -> dict:
+    """Continuous-batching serving (ServingEngine): Poisson arrivals at 200 req/s mixing
+    the pi, CORE2-size and 1.3M-node meshes (0.6/0.3/0.1), each request K ~ U{1..50} FCT
+    steps of a resident member (T, S), 20 % with the adjoint of the last step; admission
+    by a 150 GB HBM budget. The offered load is far above one GPU's capacity, so the
+    stream is bounded (``--serve-seconds`` of arrivals) and the run also reports a
+    sustainable-rate stream and the serial plain-launch baseline on the same requests."""
+    import torch
+
+    from fesom_jax_b200 import workloads as W
+    from fesom_jax_b200.mesh import pi_mesh
+    from fesom_jax_b200.serve import ServingEngine, poisson_requests
+    torch.cuda.set_device(D.local_rank)
+    meshes = {"pi": pi_mesh(), "core2": W.make_workload_mesh("batched", seed=0),
+              "large": W.make_workload_mesh("large", seed=0)}
+    dts = {"pi": 3600.0, "core2": 1800.0, "large": 600.0}
+    eng = ServingEngine(meshes, dts, budget_bytes=150e9, device=D.local_rank, ntr=2,
+                        workspace_bytes=45e9, sigma={"large": 0.2})
+    out = {}
+    reqs = poisson_requests(200.0, args.serve_seconds, seed=1 + D.rank)
+    clocks = ClockSampler(gpu_index(D.local_rank))
+    clocks.start()
+    sat = eng.run(reqs, time_limit=args.serve_limit)
+    out["clocks"] = clocks.stop()
+    out["saturated"] = dict(rate_req_s=200.0, arrivals_s=args.serve_seconds, **sat)
+    cap = sat["throughput_req_s"]
+    low = poisson_requests(max(0.5 * cap, 0.2), args.serve_seconds * 4, seed=100 + D.rank)
+    out["sustainable"] = dict(rate_req_s=max(0.5 * cap, 0.2),
+                              **eng.run(low, time_limit=args.serve_limit))
+    out["serial"] = eng.run_serial(reqs, time_limit=args.serve_limit / 2)
+    eng.close()
+    out["value"] = sat["updates_per_s"] * D.world
+    out["t"] = sat["wall_s"]
+    return out
+
+
 # ------------------------------------------------------------------ reference arm
 def run_reference(args, D: Dist):
     """CPU arm: the C restatement of the reference algorithm on the box's host cores
