@@ -400,9 +400,10 @@ def e2e_host(args, mesh, cfg, dev, per_thread: int = 0) -> dict:
 def run_adjoint(args, D: Dist) -> dict:
     """Gradient of loss = sum_n areasvol[n,0] (T_K[n,0] - target_n)^2 after K = 10 FCT
     steps on the CORE2-size mesh, w.r.t. the initial T and uv, with w_e = compute_w(uv)
-    inside the loss (chain_loss_and_grad: per-step recomputation checkpointing). Reports
-    its cost against the forward alone (compute_w + K steps) and central finite
-    differences (eps = 1e-7) along 20 seeded directions (10 for T0, 10 for uv).
+    inside the loss (chain_loss_and_grad with a forward tape; the per-step recomputation
+    variant is timed beside it). Reports its cost against the forward alone (compute_w +
+    K steps) and central finite differences (eps = 1e-7) along 20 seeded directions (10
+    for T0, 10 for uv).
 
     The velocities here are white noise (sigma 0.002 m/s, vertical CFL < 1): a
     streamfunction flow is
@@ -412,7 +413,7 @@ def run_adjoint(args, D: Dist) -> dict:
 
     from fesom_jax_b200 import inputs as I
     from fesom_jax_b200 import workloads as W
-    from fesom_jax_b200.adjoint import chain_loss_and_grad
+    from fesom_jax_b200.adjoint import Tape, chain_loss_and_grad
     from fesom_jax_b200.ale import compute_w
     from fesom_jax_b200.tracer_adv import get_plan
     torch.cuda.set_device(D.local_rank)
@@ -434,8 +435,9 @@ def run_adjoint(args, D: Dist) -> dict:
             T, To = plan.forward(uv, w, helem, hn, hnn, T, To, dt), T
         return T
 
-    def grad():
-        return chain_loss_and_grad(mesh, T0, uv, helem, hn, hnn, target, K, dt=dt, T_old0=To0)
+    def grad(checkpoint="tape"):
+        return chain_loss_and_grad(mesh, T0, uv, helem, hn, hnn, target, K, dt=dt, T_old0=To0,
+                                   checkpoint=checkpoint)
 
     def timed(fn, reps):
         for _ in range(max(args.warmup, 1)):
@@ -452,8 +454,11 @@ def run_adjoint(args, D: Dist) -> dict:
     D.barrier()
     t_fwd = timed(forward, args.steps)
     t_grad = timed(grad, args.steps)
+    t_grad_rc = timed(lambda: grad("recompute"), args.steps)
     t = D.max(t_grad, dev)
     loss, gT0, guv = grad()
+    _, gT0_rc, guv_rc = grad("recompute")
+    same_bits = bool(torch.equal(gT0, gT0_rc) and torch.equal(guv, guv_rc))
     # central finite differences
     rng = np.random.default_rng(2024)
     lm = torch.from_numpy(mesh.node_layer_mask).to(dev)
@@ -481,13 +486,18 @@ def run_adjoint(args, D: Dist) -> dict:
     return dict(value=upd / t, t=t * args.steps, mesh=mesh, t_fwd=t_fwd, t_grad=t_grad,
                 cfg=dict(members=1, ntr=1, fct_steps=K, dt=dt),
                 adjoint=dict(forward_ms=t_fwd * 1e3, loss_and_grad_ms=t_grad * 1e3,
-                             ratio=t_grad / t_fwd, K=K, loss=loss,
+                             ratio=t_grad / t_fwd, K=K, loss=loss, checkpoint="tape",
+                             tape_gb=Tape.nbytes(mesh, K, 1, D.local_rank) / 1e9,
+                             recompute_loss_and_grad_ms=t_grad_rc * 1e3,
+                             recompute_ratio=t_grad_rc / t_fwd,
+                             tape_equals_recompute=same_bits,
                              fd_rel_err_max=float(max(rel)) if rel else None,
                              fd_rel_err_median=float(np.median(rel)) if rel else None,
                              fd_directions=len(rel), fd_eps=eps, max_cfl_z=float(I.max_cfl_z(
                                  mesh, f.w_e, f.hnode, dt)),
-                             how="chain_loss_and_grad (fct_forward x K, fct_adjoint x K, "
-                                 "fct_compute_w_adjoint) vs compute_w + fct_forward x K"))
+                             how="chain_loss_and_grad (fct_forward_taped x K, "
+                                 "fct_adjoint_ex x K, fct_compute_w_adjoint) vs compute_w + "
+                                 "fct_forward x K"))
 
 
 # ---------------------------------------------------------------- serving (config 5)

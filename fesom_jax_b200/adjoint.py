@@ -9,9 +9,11 @@ and exposed three ways:
 * :class:`AdvectFCT` -- a ``torch.autograd.Function`` (forward = ``fct_forward``,
   backward = ``fct_adjoint``), the custom-VJP wrapper: ``loss.backward()`` through the
   CUDA step;
-* :func:`chain_loss_and_grad` -- a K-step loss with per-step recomputation
-  checkpointing: only the K+1 tracer states are stored; each step's intermediates are
-  recomputed inside its adjoint call.
+* :func:`chain_loss_and_grad` -- a K-step loss. Checkpointing is either a
+  :class:`Tape` (every step's forward intermediates are kept, as jax.grad keeps its
+  residuals, so the reverse pass only runs the reverse kernels) or per-step
+  recomputation (only the K+1 tracer states are kept; each step's intermediates are
+  recomputed inside its adjoint call). Both give the same bits.
 
 Subgradients follow JAX's conventions (equal split at max/min ties, even split over tied
 segment maxima, ``abs'(0) = 0``).
@@ -37,12 +39,120 @@ def _bind(L):
     L.fct_plan_reserve_adjoint.argtypes = [C.c_void_p, C.c_int]
     L.fct_adjoint.argtypes = [C.c_void_p, C.POINTER(_lib.FctFields), C.c_void_p, C.c_double,
                               C.c_int, C.POINTER(FctGrads), C.c_void_p]
+    L.fct_adjoint_ex.argtypes = [C.c_void_p, C.POINTER(_lib.FctFields), C.c_void_p,
+                                 C.c_double, C.c_int, C.POINTER(FctGrads), C.c_void_p, C.c_int,
+                                 C.c_int, C.c_void_p]
     L.fct_compute_w_adjoint.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_int, C.c_void_p]
-    for n in ("fct_plan_reserve_adjoint", "fct_adjoint", "fct_compute_w_adjoint"):
+    L.fct_tape_bytes.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int64)]
+    L.fct_tape_create.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int64,
+                                  C.POINTER(C.c_void_p)]
+    L.fct_tape_destroy.argtypes = [C.c_void_p]
+    L.fct_forward_taped.argtypes = [C.c_void_p, C.POINTER(_lib.FctFields), C.c_double, C.c_int,
+                                    C.c_void_p, C.c_int, C.c_void_p]
+    for n in ("fct_plan_reserve_adjoint", "fct_adjoint", "fct_adjoint_ex",
+              "fct_compute_w_adjoint", "fct_tape_bytes", "fct_tape_create", "fct_tape_destroy",
+              "fct_forward_taped"):
         getattr(L, n).restype = C.c_int
     L._adj_bound = True
     return L
+
+
+# accumulate bits of fct_adjoint_ex (include/fesom_fct.h)
+ACC_T, ACC_T_OLD, ACC_UV, ACC_W = 1, 2, 4, 8
+
+
+def _fields(mesh: Mesh, uv, w_e, helem, hnode, hnode_new, T, T_old, T_new=None, Z3d=None,
+            zbar3=None):
+    f = _lib.FctFields()
+    f.uv, f.w_e, f.helem = uv.data_ptr(), w_e.data_ptr(), helem.data_ptr()
+    f.hnode, f.hnode_new = hnode.data_ptr(), hnode_new.data_ptr()
+    f.T, f.T_old = T.data_ptr(), T_old.data_ptr()
+    f.T_new = T_new.data_ptr() if T_new is not None else None
+    f.tracer_stride = mesh.nod2D * mesh.nl
+    f.Z3d = Z3d.data_ptr() if Z3d is not None else None
+    f.zbar3 = zbar3.data_ptr() if zbar3 is not None else None
+    f.w_i = None
+    return f
+
+
+class Tape:
+    """Forward intermediates of up to ``steps`` FCT steps of one mesh (``fct_tape_*``):
+    :meth:`forward` runs a step and keeps its intermediates in a slot, and the adjoint of
+    that slot (``advect_one_fct_vjp(..., tape=, slot=)``) runs only the reverse kernels.
+    The memory (:meth:`nbytes`) comes from torch's caching allocator, so tapes of the same
+    size reuse it."""
+
+    def __init__(self, mesh: Mesh, steps: int, ntr: int = 1, device: int | None = None):
+        torch = _torch()
+        dev = torch.cuda.current_device() if device is None else int(device)
+        self.mesh, self.steps, self.ntr, self.device = mesh, int(steps), int(ntr), dev
+        self.plan = get_plan(mesh, dev)
+        L = _bind(_lib.lib())
+        nb = Tape.nbytes(mesh, steps, ntr, dev)
+        self._mem = torch.empty(max(nb // 8, 1), dtype=torch.float64,
+                                device=torch.device("cuda", dev))
+        h = C.c_void_p()
+        with self.plan._lock:
+            _lib.check(L.fct_tape_create(self.plan.handle, self.ntr, self.steps,
+                                         C.c_void_p(self._mem.data_ptr()), nb, C.byref(h)))
+        self._h = h
+
+    @staticmethod
+    def nbytes(mesh: Mesh, steps: int, ntr: int = 1, device: int = 0) -> int:
+        out = C.c_int64()
+        L = _bind(_lib.lib())
+        _lib.check(L.fct_tape_bytes(get_plan(mesh, device).handle, int(ntr), int(steps),
+                                    C.byref(out)))
+        return int(out.value)
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    def forward(self, slot: int, uv, w_e, helem, hnode, hnode_new, T, T_old, dt: float,
+                Z3d=None, zbar3=None, out=None):
+        """``fct_forward`` of one step, recorded in ``slot``; returns ``T_new``."""
+        torch = _torch()
+        ntr = 1 if T.dim() == 2 else int(T.shape[0])
+        T, T_old = T.contiguous(), T_old.contiguous()
+        if out is None:
+            out = torch.empty_like(T)
+        f = _fields(self.mesh, uv, w_e, helem, hnode, hnode_new, T, T_old, out, Z3d, zbar3)
+        with self.plan._lock:
+            _lib.check(_bind(_lib.lib()).fct_forward_taped(
+                self.plan.handle, C.byref(f), float(dt), ntr, self._h, int(slot),
+                _stream(torch, T.device)))
+        return out
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _lib.lib().fct_tape_destroy(self._h)
+            self._h = C.c_void_p()
+        self._mem = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _adjoint(plan, f, gT_new, dt, ntr, gT, gTo, guv, gw, tape=None, slot=0, acc=0, dev=None):
+    torch = _torch()
+    L = _bind(_lib.lib())
+    g = FctGrads(gT.data_ptr(), gTo.data_ptr(), guv.data_ptr(), gw.data_ptr())
+    with plan._lock:
+        _lib.check(L.fct_adjoint_ex(plan.handle, C.byref(f), C.c_void_p(gT_new.data_ptr()),
+                                    float(dt), ntr, C.byref(g),
+                                    tape.handle if tape is not None else None, int(slot),
+                                    int(acc), _stream(torch, dev)))
 
 
 def _stream(torch, dev):
@@ -50,31 +160,24 @@ def _stream(torch, dev):
 
 
 def advect_one_fct_vjp(mesh: Mesh, uv, w_e, helem, hnode, hnode_new, T, T_old, gT_new, *,
-                       dt: float, Z3d=None, zbar3=None):
+                       dt: float, Z3d=None, zbar3=None, tape: Tape | None = None,
+                       slot: int = 0):
     """Cotangents ``(gT, gT_old, guv, gw_e)`` of one FCT step for the output cotangent
     ``gT_new`` (CUDA float64 tensors; ``T`` may carry a leading tracer axis, in which case
-    ``guv``/``gw_e`` are summed over the tracers)."""
+    ``guv``/``gw_e`` are summed over the tracers). With ``tape``, the step recorded in
+    ``slot`` (by :meth:`Tape.forward` with the same inputs) is not recomputed."""
     torch = _torch()
     dev = T.device
     plan = get_plan(mesh, dev.index if dev.index is not None else torch.cuda.current_device())
     L = _bind(_lib.lib())
     ntr = 1 if T.dim() == 2 else int(T.shape[0])
-    _lib.check(L.fct_plan_reserve_adjoint(plan.handle, ntr))
+    if tape is None:
+        _lib.check(L.fct_plan_reserve_adjoint(plan.handle, ntr))
     T, T_old, gT_new = T.contiguous(), T_old.contiguous(), gT_new.contiguous()
-    f = _lib.FctFields()
-    f.uv, f.w_e, f.helem = uv.data_ptr(), w_e.data_ptr(), helem.data_ptr()
-    f.hnode, f.hnode_new = hnode.data_ptr(), hnode_new.data_ptr()
-    f.T, f.T_old, f.T_new = T.data_ptr(), T_old.data_ptr(), None
-    f.tracer_stride = mesh.nod2D * mesh.nl
-    f.Z3d = Z3d.data_ptr() if Z3d is not None else None
-    f.zbar3 = zbar3.data_ptr() if zbar3 is not None else None
-    f.w_i = None
+    f = _fields(mesh, uv, w_e, helem, hnode, hnode_new, T, T_old, None, Z3d, zbar3)
     gT, gTo = torch.empty_like(T), torch.empty_like(T)
     guv, gw = torch.empty_like(uv), torch.empty_like(w_e)
-    g = FctGrads(gT.data_ptr(), gTo.data_ptr(), guv.data_ptr(), gw.data_ptr())
-    with plan._lock:
-        _lib.check(L.fct_adjoint(plan.handle, C.byref(f), C.c_void_p(gT_new.data_ptr()),
-                                 float(dt), ntr, C.byref(g), _stream(torch, dev)))
+    _adjoint(plan, f, gT_new, dt, ntr, gT, gTo, guv, gw, tape, slot, 0, dev)
     return gT, gTo, guv, gw
 
 
@@ -150,39 +253,67 @@ def functions():
     return _FUNCS
 
 
+def _tape_fits(torch, mesh: Mesh, steps: int, dev) -> bool:
+    """A tape of ``steps`` one-tracer steps fits in half of the memory torch could hand out
+    (free device memory plus its cached, unused blocks)."""
+    need = Tape.nbytes(mesh, steps, 1, dev.index)
+    free, _ = torch.cuda.mem_get_info(dev)
+    cached = torch.cuda.memory_reserved(dev) - torch.cuda.memory_allocated(dev)
+    return need <= 0.5 * (free + cached)
+
+
 def chain_loss_and_grad(mesh: Mesh, T0, uv, helem, hnode, hnode_new, target, steps: int, *,
-                        dt: float, T_old0=None):
+                        dt: float, T_old0=None, checkpoint: str = "auto"):
     """Loss ``sum_n areasvol[n,0] * (T_K[n,0] - target_n)^2`` after ``steps`` FCT steps
     with ``w_e = compute_w(uv)`` inside the loss, and its gradients w.r.t. the initial
-    ``T0`` and ``uv``. Per-step recomputation checkpointing: the K+1 states are kept,
-    every step's intermediates are recomputed in its adjoint call.
+    ``T0`` and ``uv``. ``checkpoint``: ``"tape"`` keeps every step's intermediates
+    (:class:`Tape`), ``"recompute"`` keeps only the K+1 states and recomputes each step
+    inside its adjoint call, ``"auto"`` takes the tape when it fits in half the free
+    memory. The cotangents are accumulated in place (``fct_adjoint_ex``).
 
     Returns ``(loss, gT0, guv)``; ``T_old0`` defaults to ``T0`` (step-1 convention)."""
     torch = _torch()
     from .ale import compute_w
-    plan = get_plan(mesh, T0.device.index)
-    w = compute_w(mesh, uv, helem)
-    states = [T_old0 if T_old0 is not None else T0, T0]   # [T_{-1}, T_0, T_1, ...]
-    for _ in range(steps):
-        states.append(plan.forward(uv, w, helem, hnode, hnode_new, states[-1], states[-2], dt))
-    TK = states[-1]
-    av0 = torch.from_numpy(mesh.areasvol[:, 0].copy()).to(T0.device)
-    tgt = target.to(T0.device)
-    diff = TK[:, 0] - tgt
-    loss = float((av0 * diff * diff).sum().item())
-    lam = torch.zeros_like(TK)
-    lam[:, 0] = 2.0 * av0 * diff
-    guv = torch.zeros_like(uv)
-    gw = torch.zeros_like(w)
-    carry = torch.zeros_like(TK)   # cotangent reaching T_s through step s+1's T_old input
-    for s in range(steps - 1, -1, -1):
-        T_s, T_sm1 = states[s + 1], states[s]
-        gT, gTo, gu, gww = advect_one_fct_vjp(mesh, uv, w, helem, hnode, hnode_new, T_s, T_sm1,
-                                              lam, dt=dt)
-        guv += gu
-        gw += gww
-        lam = gT + carry
-        carry = gTo
-    gT0 = lam + (carry if T_old0 is None else 0.0)
-    compute_w_vjp(mesh, gw, helem, guv)
+    dev = T0.device
+    plan = get_plan(mesh, dev.index)
+    if checkpoint not in ("auto", "tape", "recompute"):
+        raise ValueError(f"checkpoint={checkpoint!r}: expected auto, tape or recompute")
+    if checkpoint == "auto":
+        checkpoint = "tape" if _tape_fits(torch, mesh, steps, dev) else "recompute"
+    tape = Tape(mesh, steps, 1, dev.index) if checkpoint == "tape" else None
+    if tape is None:
+        _lib.check(_bind(_lib.lib()).fct_plan_reserve_adjoint(plan.handle, 1))
+    try:
+        w = compute_w(mesh, uv, helem)
+        states = [T_old0 if T_old0 is not None else T0, T0]   # [T_{-1}, T_0, T_1, ...]
+        for s in range(steps):
+            if tape is not None:
+                states.append(tape.forward(s, uv, w, helem, hnode, hnode_new, states[-1],
+                                           states[-2], dt))
+            else:
+                states.append(plan.forward(uv, w, helem, hnode, hnode_new, states[-1],
+                                           states[-2], dt))
+        TK = states[-1]
+        av0 = torch.from_numpy(mesh.areasvol[:, 0].copy()).to(dev)
+        tgt = target.to(dev)
+        diff = TK[:, 0] - tgt
+        loss = float((av0 * diff * diff).sum().item())
+        lam = torch.zeros_like(TK)
+        lam[:, 0] = 2.0 * av0 * diff
+        guv = torch.zeros_like(uv)
+        gw = torch.zeros_like(w)
+        carry = torch.zeros_like(TK)   # cotangent reaching T_s through step s+1's T_old input
+        for s in range(steps - 1, -1, -1):
+            T_s, T_sm1 = states[s + 1], states[s]
+            f = _fields(mesh, uv, w, helem, hnode, hnode_new, T_s, T_sm1)
+            gTo = torch.empty_like(TK)
+            # gT accumulates into carry: the cotangent of T_s is gT + carry
+            _adjoint(plan, f, lam, dt, 1, carry, gTo, guv, gw, tape, s,
+                     ACC_T | ACC_UV | ACC_W, dev)
+            lam, carry = carry, gTo
+        gT0 = lam + (carry if T_old0 is None else 0.0)
+        compute_w_vjp(mesh, gw, helem, guv)
+    finally:
+        if tape is not None:
+            tape.close()
     return loss, gT0, guv

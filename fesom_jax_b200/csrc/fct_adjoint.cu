@@ -1,34 +1,49 @@
-// Reverse mode of the FCT step (fct_adjoint) and of compute_w (fct_compute_w_adjoint).
+// Reverse mode of the FCT step (fct_adjoint, fct_adjoint_ex) and of compute_w
+// (fct_compute_w_adjoint), plus the forward tape (fct_tape_*, fct_forward_taped).
 //
-// The forward step is recomputed first (the stage kernels of fct_forward write their
-// intermediates to the plan workspace); the reverse kernels below then walk the stages
-// backwards. Every transpose of a forward scatter is again a deterministic gather over a
-// CSR list, so cotangents are bit-identical run to run.
+// The reverse kernels read the forward step's intermediates: either recomputed first by
+// the unfused stage kernels into the plan workspace (per-step recomputation), or kept
+// from the forward call on a tape (one full workspace per recorded step). They walk the
+// stages backwards; every transpose of a forward scatter is again a deterministic gather
+// over a CSR list, so cotangents are bit-identical run to run, and taped and recomputed
+// cotangents are the same bits.
 //
 // Reverse stage map (forward function in fesom_jax/tracer_adv.py -> reverse kernel):
-//   ale_reconstruct (:142-151), flux2dtracer_fct (:469-484)       -> r_seed
-//   zalesak_limit b3 (:453-465)                                    -> r_factors
-//   zalesak_limit b2 (:441-451), a4 window minus LO (:417-418)     -> r_ratio
-//   zalesak_limit a4 vertical window max/min (:412-416)            -> r_window
-//   zalesak_limit a3 segment_max/min (:399-405)                    -> r_cluster
-//   zalesak_limit a1-a2 (:389-397)                                 -> r_bounds
-//   compute_fct_lo (:298-313)                                      -> r_lo
-//   adv_flux_hor_ho (:196-225), adv_flux_hor (:96-105), b1 edges   -> r_edge
-//   fill_up_dn_grad (:344-368), _node_avg_grad (:329-341)          -> r_gnode, r_tr
-//   tracer_gradient_elements (:316-326)                            -> r_grad_t
-//   adv_flux_ver_ho (:241-295), adv_flux_ver (:108-120), b1 vertical -> r_vert_a, r_vert_b
-//   tracer_ab (:59-66), assembly of dT, dT_old                    -> r_final
-//   edge_vflux (:69-93)                                            -> r_uv
-//   ale.compute_w (fesom_jax/ale.py:309-365)                       -> r_w_div, r_w_uv
+//   ale_reconstruct (:142-151), flux2dtracer_fct (:469-484)        -> r_seed (divergence),
+//                                                                     r_bounds_lo (T, LO)
+//   zalesak_limit b3 (:453-465)                                     -> r_factors
+//   zalesak_limit b2 (:441-451), a4 window (:407-418)               -> r_ratio_window
+//   zalesak_limit a2 (:393-397) over a3's per-cell shares            -> r_cluster
+//   zalesak_limit a1 (:389-391), compute_fct_lo (:298-313)          -> r_bounds_lo
+//   adv_flux_hor_ho (:196-225), adv_flux_hor (:96-105), b1 edges    -> r_edge
+//   fill_up_dn_grad (:344-368) node branch; adv_flux_ver_ho
+//     (:241-295), adv_flux_ver (:108-120), b1 vertical              -> r_gnode_vert
+//   fill_up_dn_grad triangle branch, _node_avg_grad (:329-341)      -> r_tr
+//   tracer_gradient_elements (:316-326), vertical fluxes on T and
+//     ttfAB, tracer_ab (:59-66), edge terms; w_e summed over tracers -> r_final
+//   edge_vflux (:69-93)                                             -> r_uv
+//   ale.compute_w (fesom_jax/ale.py:309-365)                        -> r_w_div, r_w_uv
 //
 // Subgradients follow JAX: maximum/minimum split the cotangent equally at a tie,
 // max over an element's vertices and segment_max/min spread it evenly over tied
 // entries, abs'(0) = 0 (so d max(x, 0)/dx = 1/2 at x = 0).
 #include <algorithm>
+#include <vector>
 
+#include "fct_div.cuh"
 #include "fct_host.h"
 
 using namespace fct;
+
+struct FctTape {
+  FctPlan* plan = nullptr;
+  int ntr = 0, steps = 0;
+  double* d = nullptr;
+  bool owned = false;   // allocated by fct_tape_create (else caller memory)
+  std::vector<Workspace> ws;
+  std::vector<char> recorded;
+  std::vector<double> dt;
+};
 
 namespace {
 
@@ -37,6 +52,8 @@ constexpr int B = 256;
 __device__ __forceinline__ int64_t lane_index() {
   return int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
 }
+template <class T>
+__device__ __forceinline__ T ld(const T* p) { return __ldg(p); }
 __device__ __forceinline__ double ab2(double T, double To) { return kAbOld * To + kAbNew * T; }
 __device__ __forceinline__ double safe_nz(double x) { return x == 0.0 ? 1.0 : x; }
 __device__ __forceinline__ double sgn(double x) { return x > 0.0 ? 1.0 : (x < 0.0 ? -1.0 : 0.0); }
@@ -48,58 +65,52 @@ __device__ __forceinline__ double smin_b(double a, double b) { return b < a ? 1.
 // d max(x, 0)/dx and d min(x, 0)/dx
 __device__ __forceinline__ double dmax0(double x) { return x > 0.0 ? 1.0 : (x == 0.0 ? 0.5 : 0.0); }
 __device__ __forceinline__ double dmin0(double x) { return x < 0.0 ? 1.0 : (x == 0.0 ? 0.5 : 0.0); }
+// k in [r & 255, (r >> 8) & 255) (packed level ranges of the mesh slots)
+__device__ __forceinline__ bool in_range(int k, unsigned r) {
+  return k >= int(r & 255u) && k < int((r >> 8) & 255u);
+}
+
+// accumulate flags of fct_adjoint_ex
+constexpr int kAccT = 1, kAccTo = 2, kAccUV = 4, kAccW = 8;
 
 struct Adj {
-  Inst in;               // forward fields + forward workspace (recomputed)
+  Inst in;               // forward fields + forward workspace (recomputed or taped)
   AdjWorkspace a;
   const double* gTn;     // cotangent of T_new (tracer-major, in.tstride)
   double *gT, *gTo, *guv, *gw;
+  int acc;               // kAcc* bits: add into the output instead of overwriting it
 };
 
-__device__ __forceinline__ bool edge_on(const DevMesh& m, int e, int k) {
-  return k >= m.ekmin[e] && k < m.ekmax[e];
-}
-__device__ __forceinline__ bool elem_on(const DevMesh& m, int el, int k) {
-  return k >= m.eul[el] && k < m.enl[el];
-}
-
-// cotangent reaching the limited vertical flux at interface j of node column `base`
-__device__ __forceinline__ double gvl_at(const DevMesh& m, const double* gdel, int64_t base,
-                                        int j, int nzmin, int nzmax, double dt) {
+// Cotangent reaching the limited vertical flux at interface j of a node column, from the
+// stored divergence cotangents ghsc = gdel * dt / sa (sa = areasvol, 1 where it is 0): the
+// flux enters layer j's update with +dt/areasvol and layer j-1's with -dt/areasvol, each
+// only where that layer exists and areasvol > 0 (flux2dtracer_fct, tracer_adv.py:476-479).
+__device__ __forceinline__ double gvl_at(const DevMesh& m, const double* ghsc, int64_t base,
+                                        int j, int nzmin, int nzmax) {
   double g = 0.0;
-  if (j >= nzmin && j < nzmax) {
-    const double av = m.areasvol[base + j];
-    if (av > 0.0) g += gdel[base + j] * dt / av;
-  }
-  if (j - 1 >= nzmin && j - 1 < nzmax) {
-    const double av = m.areasvol[base + j - 1];
-    if (av > 0.0) g -= gdel[base + j - 1] * dt / av;
-  }
+  if (j >= nzmin && j < nzmax && ld(m.areasvol + base + j) > 0.0) g += ghsc[base + j];
+  if (j - 1 >= nzmin && j - 1 < nzmax && ld(m.areasvol + base + j - 1) > 0.0)
+    g -= ghsc[base + j - 1];
   return g;
 }
 
 // ------------------------------------------------------------------ r_seed
+// T_new = T + d / hnn (d = del + T (hn - hnn)); del holds the flux divergence times
+// dt / areasvol. Stores the cotangent of a node's flux divergence, gdel * dt / sa.
 __global__ void __launch_bounds__(B) r_seed(Adj A) {
   const Inst& in = A.in;
   const DevMesh& m = *in.m;
   const int64_t i = lane_index();
   if (i >= m.n_layer) return;
-  const uint32_t lane = m.layer_lanes[i];
-  const int n = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const int64_t qn = int64_t(n) * L + k;
-  const double hn = in.hnode[qn], hnn = in.hnode_new[qn];
+  const uint32_t lane = ld(m.layer_lanes + i);
+  const int64_t qn = int64_t(lane_ent(lane)) * m.L + lane_lev(lane);
+  const double hnn = ld(in.hnode_new + qn), av = ld(m.areasvol + qn);
+  const double sa = av > 0.0 ? av : 1.0;
   for (int t = 0; t < in.ntr; ++t) {
-    const int64_t o = t * A.a.sN;
-    const double g = A.gTn[t * in.tstride + qn];
-    double gT = g, gdel = 0.0;
-    if (hnn > 0.0) {
-      gdel = g / hnn;                 // T_new = T + d / hnn
-      gT += gdel * (hn - hnn);        // d = del + T (hn - hnn)
-    }
-    gT += -gdel * hn;                 // lo_trans = -T hn + LO hnn
-    A.a.gdel[o + qn] = gdel;
-    A.a.gLOd[o + qn] = gdel * hnn;
-    A.a.gTd[o + qn] = gT;
+    const double g = ld(A.gTn + t * in.tstride + qn);
+    double gdel = 0.0;
+    if (hnn > 0.0) gdel = g / hnn;
+    A.a.ghsc[t * A.a.sN + qn] = gdel * in.dt / sa;
   }
 }
 
@@ -109,223 +120,259 @@ __global__ void __launch_bounds__(B) r_factors(Adj A) {
   const DevMesh& m = *in.m;
   const int64_t i = lane_index();
   if (i >= m.n_layer) return;
-  const uint32_t lane = m.layer_lanes[i];
+  const uint32_t lane = ld(m.layer_lanes + i);
   const int n = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const int nzmin = m.nzmin[n], nzmax = m.nzmax[n];
+  const int nzmin = ld(m.nzmin + n), nzmax = ld(m.nzmax + n);
   const int64_t base = int64_t(n) * L, qn = base + k;
-  const double dt = in.dt;
+  const int e0 = ld(m.ne_off + n), e1 = ld(m.ne_off + n + 1);
   for (int t = 0; t < in.ntr; ++t) {
     const int64_t o = t * in.ws.sN;
     const double* pf = in.ws.pf + o;
     const double* mf = in.ws.mf + o;
     const double* adfv = in.ws.adfv + o;
-    const double* gdel = A.a.gdel + t * A.a.sN;
+    const double* ghsc = A.a.ghsc + t * A.a.sN;
+    const double pfk = pf[qn], mfk = mf[qn];
     double gp = 0.0, gm = 0.0;
     // vertical limited flux at interface k (this node's own factors at k)
     {
       const double f = adfv[qn];
-      const double g_ae = gvl_at(m, gdel, base, k, nzmin, nzmax, dt) * f;
+      const double g_ae = gvl_at(m, ghsc, base, k, nzmin, nzmax) * f;
       if (k == nzmin) {
         if (f >= 0.0) gp += g_ae; else gm += g_ae;
       } else if (f >= 0.0) {
-        gp += g_ae * smin_b(mf[qn - 1], pf[qn]);
+        gp += g_ae * smin_b(mf[qn - 1], pfk);
       } else {
-        gm += g_ae * smin_b(pf[qn - 1], mf[qn]);
+        gm += g_ae * smin_b(pf[qn - 1], mfk);
       }
     }
     // vertical limited flux at interface k+1 (uses this node's factors as the k-1 ones)
     if (k + 1 < nzmax) {
       const double f = adfv[qn + 1];
-      const double g_ae = gvl_at(m, gdel, base, k + 1, nzmin, nzmax, dt) * f;
-      if (f >= 0.0) gm += g_ae * smin_a(mf[qn], pf[qn + 1]);
-      else gp += g_ae * smin_a(pf[qn], mf[qn + 1]);
+      const double g_ae = gvl_at(m, ghsc, base, k + 1, nzmin, nzmax) * f;
+      if (f >= 0.0) gm += g_ae * smin_a(mfk, pf[qn + 1]);
+      else gp += g_ae * smin_a(pfk, mf[qn + 1]);
     }
-    // horizontal limited fluxes of the incident edges
-    const double av0 = m.areasvol[qn];
-    const double ghsc0 = gdel[qn] * dt / (av0 > 0.0 ? av0 : 1.0);
-    for (int j = m.ne_off[n]; j < m.ne_off[n + 1]; ++j) {
-      const int idx = m.ne_idx[j], e = idx >> 1;
-      if (!edge_on(m, e, k)) continue;
-      const int64_t qo = int64_t(m.ne_oth[j]) * L + k;
-      const double avo = m.areasvol[qo];
-      const double ghsco = gdel[qo] * dt / (avo > 0.0 ? avo : 1.0);
-      const bool second = idx & 1;
+    // horizontal limited fluxes of the incident edges, ascending edge id; the loads are
+    // unconditional (all in bounds) and edges without a flux at k are selected away
+    const double ghsc0 = ghsc[qn];
+    const double* adfh = in.ws.adfh + t * in.ws.sEd;
+#pragma unroll 2
+    for (int j = e0; j < e1; ++j) {
+      const int4 sl = __ldg(m.ne4 + j);
+      const bool on = in_range(k, unsigned(sl.z));
+      const bool second = sl.x & 1;
+      const int64_t qo = int64_t(sl.y) * L + k;
+      const double ghsco = ghsc[qo];
       const double glim = second ? (ghsco - ghsc0) : (ghsc0 - ghsco);
-      const double a = in.ws.adfh[t * in.ws.sEd + int64_t(e) * L + k];
+      const double a = adfh[int64_t(sl.x >> 1) * L + k];
       const double g_ae = glim * a;
-      const double pf1 = second ? pf[qo] : pf[qn], mf1 = second ? mf[qo] : mf[qn];
-      const double pf2 = second ? pf[qn] : pf[qo], mf2 = second ? mf[qn] : mf[qo];
+      const double pfo = pf[qo], mfo = mf[qo];
+      const double pf1 = second ? pfo : pfk, mf1 = second ? mfo : mfk;
+      const double pf2 = second ? pfk : pfo, mf2 = second ? mfk : mfo;
+      double dp = 0.0, dm = 0.0;
+      bool tp = false, tm = false;
       if (a >= 0.0) {   // ae = min(pf[n1], mf[n2])
-        if (!second) gp += g_ae * smin_a(pf1, mf2); else gm += g_ae * smin_b(pf1, mf2);
+        if (!second) { dp = g_ae * smin_a(pf1, mf2); tp = true; }
+        else { dm = g_ae * smin_b(pf1, mf2); tm = true; }
       } else {          // ae = min(mf[n1], pf[n2])
-        if (!second) gm += g_ae * smin_a(mf1, pf2); else gp += g_ae * smin_b(mf1, pf2);
+        if (!second) { dm = g_ae * smin_a(mf1, pf2); tm = true; }
+        else { dp = g_ae * smin_b(mf1, pf2); tp = true; }
       }
+      gp = (on && tp) ? gp + dp : gp;
+      gm = (on && tm) ? gm + dm : gm;
     }
     A.a.gpf[t * A.a.sN + qn] = gp;
     A.a.gmf[t * A.a.sN + qn] = gm;
   }
 }
 
-// ------------------------------- r_ratio: pf = min(1, fmax_w / flux_pos), likewise mf
-__global__ void __launch_bounds__(B) r_ratio(Adj A) {
+// ---------------- r_ratio_window: pf = min(1, fmax_w / flux_pos), likewise mf, the a4
+// window (max/min over the cluster bounds at k-1, k, k+1 of the same column), and the a3
+// share of each cell that attains the node's cluster bound.
+// Blocks of B threads cover B - 2 lanes plus one halo lane on each side: every thread
+// computes its lane's window cotangents (gtmax, gtmin) into shared memory, and the core
+// lanes spread them back over the window's three levels (lanes i-1, i, i+1).
+__global__ void __launch_bounds__(B) r_ratio_window(Adj A) {
+  __shared__ double sx[B], sn[B];
   const Inst& in = A.in;
   const DevMesh& m = *in.m;
-  const int64_t i = lane_index();
-  if (i >= m.n_layer) return;
-  const uint32_t lane = m.layer_lanes[i];
-  const int n = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const int nzmin = m.nzmin[n], nzmax = m.nzmax[n];
-  const int64_t qn = int64_t(n) * L + k;
-  const double av = m.areasvol[qn], hnn = in.hnode_new[qn];
-  const bool valid = (av > 0.0) && (hnn > 0.0);
-  const double sa = av > 0.0 ? av : 1.0, sh = hnn > 0.0 ? hnn : 1.0;
+  const int tid = threadIdx.x;
+  const int64_t lane = int64_t(blockIdx.x) * (B - 2) + tid - 1;
+  const bool valid = lane >= 0 && lane < m.n_layer;
+  const bool core = valid && tid >= 1 && tid <= B - 2;
+  const int L = m.L;
+  int n = 0, k = 0, nzmin = 0, nzmax = 0;
+  int64_t base = 0, qn = 0;
+  bool valid_n = false, use_own = true;
+  Rcp rsa{1.0, 1.0, true}, rsh{1.0, 1.0, true};
+  if (valid) {
+    const uint32_t ln = ld(m.layer_lanes + lane);
+    n = lane_ent(ln);
+    k = lane_lev(ln);
+    nzmin = ld(m.nzmin + n);
+    nzmax = ld(m.nzmax + n);
+    base = int64_t(n) * L;
+    qn = base + k;
+    const double av = ld(m.areasvol + qn), hnn = ld(in.hnode_new + qn);
+    valid_n = (av > 0.0) && (hnn > 0.0);
+    rsa = rcp(av > 0.0 ? av : 1.0);
+    rsh = rcp(hnn > 0.0 ? hnn : 1.0);
+    use_own = (k == nzmin) || (k == nzmax - 1);
+  }
   const double dt = in.dt;
-  const bool use_own = (k == nzmin) || (k == nzmax - 1);
   for (int t = 0; t < in.ntr; ++t) {
     const int64_t o = t * in.ws.sN, oa = t * A.a.sN;
-    double gtmax = 0.0, gtmin = 0.0, gplus = 0.0, gminus = 0.0;
+    const double* tv = in.ws.tvmax + o;
+    const double* tn = in.ws.tvmin + o;
+    double gtmax = 0.0, gtmin = 0.0;
     if (valid) {
-      const double* tv = in.ws.tvmax + o;
-      const double* tn = in.ws.tvmin + o;
-      double tmax = tv[qn], tmin = tn[qn];
-      if (!use_own) {
-        tmax = fmax(fmax(tv[qn - 1], tv[qn]), tv[qn + 1]);
-        tmin = fmin(fmin(tn[qn - 1], tn[qn]), tn[qn + 1]);
+      double gplus = 0.0, gminus = 0.0;
+      if (valid_n) {
+        double tmax = tv[qn], tmin = tn[qn];
+        if (!use_own) {
+          tmax = fmax(fmax(tv[qn - 1], tv[qn]), tv[qn + 1]);
+          tmin = fmin(fmin(tn[qn - 1], tn[qn]), tn[qn + 1]);
+        }
+        const double lo = in.ws.lo[o + qn];
+        const double plus = in.ws.fplus[o + qn], minus = in.ws.fminus[o + qn];
+        const double fmax_w = tmax - lo, fmin_w = tmin - lo;
+        const double flux_pos = divr(divr(plus * dt, rsa), rsh) + kFluxEps;
+        const double flux_neg = divr(divr(minus * dt, rsa), rsh) - kFluxEps;
+        const Rcp rfp = rcp(flux_pos), rfn = rcp(flux_neg);
+        const double rp = divr(fmax_w, rfp), rm = divr(fmin_w, rfn);
+        const double grp = A.a.gpf[oa + qn] * smin_b(1.0, rp);
+        const double grm = A.a.gmf[oa + qn] * smin_b(1.0, rm);
+        gtmax = divr(grp, rfp);
+        gtmin = divr(grm, rfn);
+        gplus = divr(divr(-grp * fmax_w / (flux_pos * flux_pos) * dt, rsa), rsh);
+        gminus = divr(divr(-grm * fmin_w / (flux_neg * flux_neg) * dt, rsa), rsh);
       }
-      const double lo = in.ws.lo[o + qn];
-      const double plus = in.ws.fplus[o + qn], minus = in.ws.fminus[o + qn];
-      const double fmax_w = tmax - lo, fmin_w = tmin - lo;
-      const double flux_pos = plus * dt / sa / sh + kFluxEps;
-      const double flux_neg = minus * dt / sa / sh - kFluxEps;
-      const double rp = fmax_w / flux_pos, rm = fmin_w / flux_neg;
-      const double grp = A.a.gpf[oa + qn] * smin_b(1.0, rp);
-      const double grm = A.a.gmf[oa + qn] * smin_b(1.0, rm);
-      gtmax = grp / flux_pos;
-      gtmin = grm / flux_neg;
-      gplus = (-grp * fmax_w / (flux_pos * flux_pos)) * dt / sa / sh;
-      gminus = (-grm * fmin_w / (flux_neg * flux_neg)) * dt / sa / sh;
+      if (core) {
+        A.a.gplus[oa + qn] = gplus;
+        A.a.gminus[oa + qn] = gminus;
+        A.a.gLOl[oa + qn] = -(gtmax + gtmin);
+      }
     }
-    A.a.gtmax[oa + qn] = gtmax;
-    A.a.gtmin[oa + qn] = gtmin;
-    A.a.gplus[oa + qn] = gplus;
-    A.a.gminus[oa + qn] = gminus;
-    A.a.gLOl[oa + qn] = -(gtmax + gtmin);
+    sx[tid] = gtmax;
+    sn[tid] = gtmin;
+    __syncthreads();
+    if (core) {
+      const double* tvc = tv + base;
+      const double* tnc = tn + base;
+      double gvx = 0.0, gvn = 0.0;
+      for (int mm = k - 1; mm <= k + 1; ++mm) {
+        if (mm < nzmin || mm >= nzmax) continue;
+        const int sl = tid + (mm - k);   // lane of level mm (same column)
+        if (mm == nzmin || mm == nzmax - 1) {
+          if (mm == k) { gvx += sx[sl]; gvn += sn[sl]; }
+          continue;
+        }
+        {  // max(max(a, b), c) with a = tv[mm-1], b = tv[mm], c = tv[mm+1]
+          const double a = tvc[mm - 1], b = tvc[mm], c = tvc[mm + 1];
+          const double inner = fmax(a, b), go = sx[sl];
+          const double gi = go * smax_a(inner, c), gc = go * smax_b(inner, c);
+          if (k == mm - 1) gvx += gi * smax_a(a, b);
+          if (k == mm) gvx += gi * smax_b(a, b);
+          if (k == mm + 1) gvx += gc;
+        }
+        {
+          const double a = tnc[mm - 1], b = tnc[mm], c = tnc[mm + 1];
+          const double inner = fmin(a, b), go = sn[sl];
+          const double gi = go * smin_a(inner, c), gc = go * smin_b(inner, c);
+          if (k == mm - 1) gvn += gi * smin_a(a, b);
+          if (k == mm) gvn += gi * smin_b(a, b);
+          if (k == mm + 1) gvn += gc;
+        }
+      }
+      // one tied cell's share of the cluster bound (a3's even split over the cells that
+      // attain it; a node layer has at least one such cell)
+      const int cx = int(in.ws.ccx[o + qn]), cn = int(in.ws.ccn[o + qn]);
+      A.a.gqx[oa + qn] = cx > 0 ? divr(gvx, rcp(double(cx))) : 0.0;
+      A.a.gqn[oa + qn] = cn > 0 ? divr(gvn, rcp(double(cn))) : 0.0;
+    }
+    __syncthreads();
   }
 }
 
-// ------------------------ r_window: tmax(m) = max over tvert at m-1, m, m+1
-__global__ void __launch_bounds__(B) r_window(Adj A) {
-  const Inst& in = A.in;
-  const DevMesh& m = *in.m;
-  const int64_t i = lane_index();
-  if (i >= m.n_layer) return;
-  const uint32_t lane = m.layer_lanes[i];
-  const int n = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const int nzmin = m.nzmin[n], nzmax = m.nzmax[n];
-  const int64_t base = int64_t(n) * L;
-  for (int t = 0; t < in.ntr; ++t) {
-    const double* tv = in.ws.tvmax + t * in.ws.sN + base;
-    const double* tn = in.ws.tvmin + t * in.ws.sN + base;
-    const double* gx = A.a.gtmax + t * A.a.sN + base;
-    const double* gn = A.a.gtmin + t * A.a.sN + base;
-    double gvx = 0.0, gvn = 0.0;
-    for (int mm = k - 1; mm <= k + 1; ++mm) {
-      if (mm < nzmin || mm >= nzmax) continue;
-      if (mm == nzmin || mm == nzmax - 1) {
-        if (mm == k) { gvx += gx[mm]; gvn += gn[mm]; }
-        continue;
-      }
-      {  // max(max(a, b), c) with a = tv[mm-1], b = tv[mm], c = tv[mm+1]
-        const double a = tv[mm - 1], b = tv[mm], c = tv[mm + 1];
-        const double inner = fmax(a, b), go = gx[mm];
-        const double gi = go * smax_a(inner, c), gc = go * smax_b(inner, c);
-        if (k == mm - 1) gvx += gi * smax_a(a, b);
-        if (k == mm) gvx += gi * smax_b(a, b);
-        if (k == mm + 1) gvx += gc;
-      }
-      {
-        const double a = tn[mm - 1], b = tn[mm], c = tn[mm + 1];
-        const double inner = fmin(a, b), go = gn[mm];
-        const double gi = go * smin_a(inner, c), gc = go * smin_b(inner, c);
-        if (k == mm - 1) gvn += gi * smin_a(a, b);
-        if (k == mm) gvn += gi * smin_b(a, b);
-        if (k == mm + 1) gvn += gc;
-      }
-    }
-    A.a.gtvmax[t * A.a.sN + base + k] = gvx;
-    A.a.gtvmin[t * A.a.sN + base + k] = gvn;
-  }
-}
-
-// ------------------- r_cluster: segment_max/min over a node's elements (even split)
+// ------- r_cluster: a2 element max/min over its vertices, cotangent spread evenly over
+// the tied vertices, of the a3 shares of the vertices whose cluster bound the element
+// attains (tie counts come from the forward). Stored already divided by the element's
+// vertex tie count: the share of each attaining vertex.
 __global__ void __launch_bounds__(B) r_cluster(Adj A) {
   const Inst& in = A.in;
   const DevMesh& m = *in.m;
   const int64_t i = lane_index();
   if (i >= m.n_elem) return;
-  const uint32_t lane = m.elem_lanes[i];
+  const uint32_t lane = ld(m.elem_lanes + i);
   const int e = lane_ent(lane), k = lane_lev(lane), L = m.L;
+  const int64_t qe = int64_t(e) * L + k;
+  const int64_t qv[3] = {int64_t(ld(m.enodes + 3 * e)) * L + k,
+                         int64_t(ld(m.enodes + 3 * e + 1)) * L + k,
+                         int64_t(ld(m.enodes + 3 * e + 2)) * L + k};
   for (int t = 0; t < in.ntr; ++t) {
-    const double* amax = in.ws.amax + t * in.ws.sE;
-    const double* amin = in.ws.amin + t * in.ws.sE;
-    const double vx = amax[int64_t(e) * L + k], vn = amin[int64_t(e) * L + k];
-    double gx = 0.0, gn = 0.0;
-    for (int v = 0; v < 3; ++v) {   // tie counts come from the forward recompute
-      const int n = m.enodes[3 * e + v];
-      const int64_t qn = int64_t(n) * L + k, qt = t * in.ws.sN + qn;
-      if (vx == in.ws.tvmax[qt]) gx += A.a.gtvmax[t * A.a.sN + qn] / int(in.ws.ccx[qt]);
-      if (vn == in.ws.tvmin[qt]) gn += A.a.gtvmin[t * A.a.sN + qn] / int(in.ws.ccn[qt]);
+    const int64_t o = t * in.ws.sN, oa = t * A.a.sN, oe = t * in.ws.sE;
+    const double vx = in.ws.amax[oe + qe], vn = in.ws.amin[oe + qe];
+    double tx[3], tn[3], qx[3], qn[3];
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+      tx[v] = in.ws.tvmax[o + qv[v]];
+      tn[v] = in.ws.tvmin[o + qv[v]];
+      qx[v] = A.a.gqx[oa + qv[v]];
+      qn[v] = A.a.gqn[oa + qv[v]];
     }
-    A.a.gamax[t * A.a.sE + int64_t(e) * L + k] = gx;
-    A.a.gamin[t * A.a.sE + int64_t(e) * L + k] = gn;
+    double gx = 0.0, gn = 0.0;
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+      gx = vx == tx[v] ? gx + qx[v] : gx;
+      gn = vn == tn[v] ? gn + qn[v] : gn;
+    }
+    A.a.gax[t * A.a.sE + qe] = divr(gx, rcp(double(int(in.ws.ecx[oe + qe]))));
+    A.a.gan[t * A.a.sE + qe] = divr(gn, rcp(double(int(in.ws.ecn[oe + qe]))));
   }
 }
 
-// ------------- r_bounds: element max/min over its vertices of max/min(LO, T) (even split)
-__global__ void __launch_bounds__(B) r_bounds(Adj A) {
+// ------- r_bounds_lo: a1 (max/min of LO and T) gathering the element shares of the
+// node's cells whose bound this node attains, then LO = numer / hnn and the seed terms
+// of T and LO.
+__global__ void __launch_bounds__(B) r_bounds_lo(Adj A) {
   const Inst& in = A.in;
   const DevMesh& m = *in.m;
   const int64_t i = lane_index();
   if (i >= m.n_layer) return;
-  const uint32_t lane = m.layer_lanes[i];
+  const uint32_t lane = ld(m.layer_lanes + i);
   const int n = lane_ent(lane), k = lane_lev(lane), L = m.L;
   const int64_t qn = int64_t(n) * L + k;
-  for (int t = 0; t < in.ntr; ++t) {
-    const double* lo = in.ws.lo + t * in.ws.sN;
-    const double* T = in.T + t * in.tstride;
-    const double mxv = fmax(lo[qn], T[qn]), mnv = fmin(lo[qn], T[qn]);
-    double gx = 0.0, gn = 0.0;
-    for (int j = m.nel_off[n]; j < m.nel_off[n + 1]; ++j) {
-      const int el = m.nel_idx[j];
-      if (!elem_on(m, el, k)) continue;
-      const int64_t qe = int64_t(el) * L + k;
-      const double ex = in.ws.amax[t * in.ws.sE + qe], en = in.ws.amin[t * in.ws.sE + qe];
-      if (mxv != ex && mnv != en) continue;
-      const int64_t qc = t * in.ws.sE + qe;   // tie counts from the forward recompute
-      if (mxv == ex) gx += A.a.gamax[t * A.a.sE + qe] / int(in.ws.ecx[qc]);
-      if (mnv == en) gn += A.a.gamin[t * A.a.sE + qe] / int(in.ws.ecn[qc]);
-    }
-    const int64_t oa = t * A.a.sN;
-    A.a.gLOb[oa + qn] = gx * smax_a(lo[qn], T[qn]) + gn * smin_a(lo[qn], T[qn]);
-    A.a.gTb[oa + qn] = gx * smax_b(lo[qn], T[qn]) + gn * smin_b(lo[qn], T[qn]);
-  }
-}
-
-// ------------------------------------------------------ r_lo: LO = numer / hnn
-__global__ void __launch_bounds__(B) r_lo(Adj A) {
-  const Inst& in = A.in;
-  const DevMesh& m = *in.m;
-  const int64_t i = lane_index();
-  if (i >= m.n_layer) return;
-  const uint32_t lane = m.layer_lanes[i];
-  const int n = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const int64_t qn = int64_t(n) * L + k;
-  const double hn = in.hnode[qn], hnn = in.hnode_new[qn], av = m.areasvol[qn];
+  const double hn = ld(in.hnode + qn), hnn = ld(in.hnode_new + qn), av = ld(m.areasvol + qn);
   const bool valid = (hnn > 0.0) && (av > 0.0);
+  const int c0 = ld(m.nel_off + n), c1 = ld(m.nel_off + n + 1);
   for (int t = 0; t < in.ntr; ++t) {
-    const int64_t oa = t * A.a.sN;
-    const double gLO = A.a.gLOd[oa + qn] + A.a.gLOl[oa + qn] + A.a.gLOb[oa + qn];
-    double gdiv = 0.0, gT = A.a.gTd[oa + qn] + A.a.gTb[oa + qn];
+    const int64_t o = t * in.ws.sN, oa = t * A.a.sN, oe = t * in.ws.sE, ae = t * A.a.sE;
+    const double lo = in.ws.lo[o + qn], T = ld(in.T + t * in.tstride + qn);
+    const double mxv = fmax(lo, T), mnv = fmin(lo, T);
+    double gx = 0.0, gn = 0.0;
+    // the node's cells in nod_in_elem2D order; loads are unconditional (in bounds) and
+    // cells dry at k are selected away
+#pragma unroll 2
+    for (int j = c0; j < c1; ++j) {
+      const bool on = in_range(k, unsigned(ld(m.nelr + j)));
+      const int64_t qe = int64_t(ld(m.nel_idx + j)) * L + k;
+      const double ex = in.ws.amax[oe + qe], en = in.ws.amin[oe + qe];
+      const double sx = A.a.gax[ae + qe], sn = A.a.gan[ae + qe];
+      gx = (on && mxv == ex) ? gx + sx : gx;
+      gn = (on && mnv == en) ? gn + sn : gn;
+    }
+    const double gLOb = gx * smax_a(lo, T) + gn * smin_a(lo, T);
+    const double gTb = gx * smax_b(lo, T) + gn * smin_b(lo, T);
+    // seed: T_new = T + d / hnn, d = (-T hn + LO hnn) + fluxes + T (hn - hnn)
+    const double g = ld(A.gTn + t * in.tstride + qn);
+    double gTs = g, gdel = 0.0;
+    if (hnn > 0.0) {
+      gdel = g / hnn;
+      gTs += gdel * (hn - hnn);
+    }
+    gTs += -gdel * hn;
+    const double gLO = gdel * hnn + A.a.gLOl[oa + qn] + gLOb;
+    double gdiv = 0.0, gT = gTs + gTb;
     if (valid) {
       const double gnum = gLO / hnn;
       gT += gnum * hn;
@@ -337,32 +384,29 @@ __global__ void __launch_bounds__(B) r_lo(Adj A) {
 }
 
 // ------------------ r_edge: adf_h = HO - LO flux; cotangents of the edge inputs
-__global__ void __launch_bounds__(B) r_edge(Adj A) {
+__global__ void __launch_bounds__(B, 3) r_edge(Adj A) {
   const Inst& in = A.in;
   const DevMesh& m = *in.m;
   const int64_t i = lane_index();
   if (i >= m.n_edge) return;
-  const uint32_t lane = m.edge_lanes[i];
+  const uint32_t lane = ld(m.edge_lanes + i);
   const int e = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const int n1 = m.edges[2 * e], n2 = m.edges[2 * e + 1];
-  const int up = m.eupdn[2 * e], dn = m.eupdn[2 * e + 1];
-  const int kmin = max(m.ulmax[n1], m.ulmax[n2]) - 1;
-  const int kmax = min(m.nlmin[n1], m.nlmin[n2]) - 1;
-  const bool use_tri = (up >= 0) && (dn >= 0) && k >= kmin && k < kmax;
+  const int n1 = ld(m.edges + 2 * e), n2 = ld(m.edges + 2 * e + 1);
+  const bool use_tri = in_range(k, unsigned(ld(m.etr + e)));
   const int64_t qe = int64_t(e) * L + k, q1 = int64_t(n1) * L + k, q2 = int64_t(n2) * L + k;
-  const double vf = in.ws.vflux[qe], avf = fabs(vf), s = sgn(vf);
-  const double c1 = m.ecoef[2 * e], c2 = m.ecoef[2 * e + 1];
-  const double av1 = m.areasvol[q1], av2 = m.areasvol[q2];
-  const double dt = in.dt;
+  int64_t qa = q1, qb = q2;   // where the MFCT gradients are read
+  if (use_tri) {
+    qa = int64_t(ld(m.eupdn + 2 * e)) * L + k;
+    qb = int64_t(ld(m.eupdn + 2 * e + 1)) * L + k;
+  }
+  const double vf = ld(in.ws.vflux + qe), s = sgn(vf);
+  const double c1 = ld(m.ecoef + 2 * e), c2 = ld(m.ecoef + 2 * e + 1);
+  const Rcp r6{6.0, 1.0 / 6.0, true};
   for (int t = 0; t < in.ntr; ++t) {
     const int64_t o = t * in.ws.sN, oa = t * A.a.sN, oe = t * A.a.sEd;
-    const double* T = in.T + t * in.tstride;
-    const double* To = in.T_old + t * in.tstride;
     const double a = in.ws.adfh[t * in.ws.sEd + qe];
     // limited flux lim = ae * a, with hsc(n1) += lim, hsc(n2) -= lim
-    const double ghsc1 = A.a.gdel[oa + q1] * dt / (av1 > 0.0 ? av1 : 1.0);
-    const double ghsc2 = A.a.gdel[oa + q2] * dt / (av2 > 0.0 ? av2 : 1.0);
-    const double glim = ghsc1 - ghsc2;
+    const double glim = A.a.ghsc[oa + q1] - A.a.ghsc[oa + q2];
     const double pf1 = in.ws.pf[o + q1], mf1 = in.ws.mf[o + q1];
     const double pf2 = in.ws.pf[o + q2], mf2 = in.ws.mf[o + q2];
     const double ae = a >= 0.0 ? fmin(pf1, mf2) : fmin(mf1, pf2);
@@ -373,18 +417,17 @@ __global__ void __launch_bounds__(B) r_edge(Adj A) {
     // adf_h = HO - fl; fl also feeds LO through the divergence
     const double gHO = ga;
     const double gfl = -ga + (A.a.gdiv[oa + q1] - A.a.gdiv[oa + q2]);
-    const double T1 = T[q1], T2 = T[q2];
-    const double A1 = ab2(T1, To[q1]), A2 = ab2(T2, To[q2]);
-    double g0, g1, g2, g3;
-    if (use_tri) {
-      const int64_t qu = t * in.ws.sE + int64_t(up) * L + k, qd = t * in.ws.sE + int64_t(dn) * L + k;
-      g0 = in.ws.gx[qu]; g1 = in.ws.gx[qd]; g2 = in.ws.gy[qu]; g3 = in.ws.gy[qd];
-    } else {
-      g0 = in.ws.gnx[o + q1]; g1 = in.ws.gnx[o + q2]; g2 = in.ws.gny[o + q1]; g3 = in.ws.gny[o + q2];
-    }
+    const double* T = in.T + t * in.tstride;
+    const double* To = in.T_old + t * in.tstride;
+    const double T1 = ld(T + q1), T2 = ld(T + q2);
+    const double A1 = ab2(T1, ld(To + q1)), A2 = ab2(T2, ld(To + q2));
+    // MFCT gradients: the up/down cells' (use_tri) or the two nodes' averages
+    const double* gxp = use_tri ? in.ws.gx + t * in.ws.sE : in.ws.gnx + o;
+    const double* gyp = use_tri ? in.ws.gy + t * in.ws.sE : in.ws.gny + o;
+    const double g0 = gxp[qa], g1 = gxp[qb], g2 = gyp[qa], g3 = gyp[qb];
     const double diff = A2 - A1;
-    const double Tm1 = A1 + (2.0 * diff + c1 * g0 + c2 * g2) / 6.0;
-    const double Tm2 = A2 - (2.0 * diff + c1 * g1 + c2 * g3) / 6.0;
+    const double Tm1 = A1 + divr(2.0 * diff + c1 * g0 + c2 * g2, r6);
+    const double Tm2 = A2 - divr(2.0 * diff + c1 * g1 + c2 * g3, r6);
     // HO = -0.5 ((vf + |vf|) Tm1 + (vf - |vf|) Tm2); fl = -0.5 (T1 (vf + |vf|) + T2 (vf - |vf|));
     // the per-end terms of Tm1/Tm2 and T1/T2 are re-derived by the consumers (edge_terms)
     double gvf = -0.5 * ((1.0 + s) * Tm1 + (1.0 - s) * Tm2) * gHO;
@@ -405,14 +448,15 @@ struct EdgeTerms {
 __device__ __forceinline__ EdgeTerms edge_terms(const Adj& A, int t, int e, int k) {
   const DevMesh& m = *A.in.m;
   const int64_t qe = int64_t(e) * m.L + k, oe = t * A.a.sEd;
-  const double vf = A.in.ws.vflux[qe], avf = fabs(vf);
+  const double vf = ld(A.in.ws.vflux + qe), avf = fabs(vf);
   const double gHO = A.a.gHO[oe + qe], gfl = A.a.gfl[oe + qe];
-  const double c1 = m.ecoef[2 * e], c2 = m.ecoef[2 * e + 1];
+  const double c1 = ld(m.ecoef + 2 * e), c2 = ld(m.ecoef + 2 * e + 1);
   const double gTm1 = -0.5 * (vf + avf) * gHO, gTm2 = -0.5 * (vf - avf) * gHO;
+  const Rcp r6{6.0, 1.0 / 6.0, true};
   EdgeTerms r;
   r.gT1 = -0.5 * (vf + avf) * gfl;
   r.gT2 = -0.5 * (vf - avf) * gfl;
-  const double gX1 = gTm1 / 6.0, gX2 = -gTm2 / 6.0;
+  const double gX1 = divr(gTm1, r6), gX2 = divr(-gTm2, r6);
   const double gdiff = 2.0 * gX1 + 2.0 * gX2;
   r.gA1 = gTm1 - gdiff;
   r.gA2 = gTm2 + gdiff;
@@ -423,34 +467,117 @@ __device__ __forceinline__ EdgeTerms edge_terms(const Adj& A, int t, int e, int 
   return r;
 }
 
-__device__ __forceinline__ bool use_tri_at(const DevMesh& m, int e, int k) {
-  const int n1 = m.edges[2 * e], n2 = m.edges[2 * e + 1];
-  const int up = m.eupdn[2 * e], dn = m.eupdn[2 * e + 1];
-  const int kmin = max(m.ulmax[n1], m.ulmax[n2]) - 1;
-  const int kmax = min(m.nlmin[n1], m.nlmin[n2]) - 1;
-  return (up >= 0) && (dn >= 0) && k >= kmin && k < kmax;
+// QR4C stencil depths of interface j (tracer_adv.py:228-238, 265-273)
+__device__ __forceinline__ void qr4c_depths(const Inst& in, const DevMesh& m, int64_t base,
+                                            int j, double& Znz, double& Zm1, double& Zm2,
+                                            double& Zp1, double& zb) {
+  const int L = m.L;
+  if (in.Z3d) {
+    const double* Zc = in.Z3d + base;
+    Znz = ld(Zc + j); Zm1 = ld(Zc + j - 1); Zm2 = ld(Zc + j - 2);
+    Zp1 = ld(Zc + (j + 1 < L ? j + 1 : L - 1));
+    zb = ld(in.zbar3 + base + j);
+  } else {
+    Znz = ld(m.Zp + j); Zm1 = ld(m.Zp + j - 1); Zm2 = ld(m.Zp + j - 2);
+    Zp1 = ld(m.Zp + (j + 1 < L ? j + 1 : L - 1));
+    zb = ld(m.zbar + j);
+  }
 }
 
-// ------------- r_gnode: cotangent of the node-average gradient (fill_up_dn_grad else-branch)
-__global__ void __launch_bounds__(B) r_gnode(Adj A) {
+// ------- r_gnode_vert: cotangent of the node-average gradient (fill_up_dn_grad's node
+// branch, gathered over the node's edges), and of the vertical fluxes at interface
+// j = k: gf of adf_v[j] (limiter application and the plus/minus sums) reaches the QR4C
+// flux (ghi = gf) and the upwind flux (gfv = -gf + gdiv terms); gw[j] is complete here
+// (only interface j feeds it), and the QR4C flux's terms for ttfAB at levels j, j-1, j-2
+// and j+1 are stored for r_final to gather.
+__global__ void __launch_bounds__(B) r_gnode_vert(Adj A) {
   const Inst& in = A.in;
   const DevMesh& m = *in.m;
   const int64_t i = lane_index();
   if (i >= m.n_layer) return;
-  const uint32_t lane = m.layer_lanes[i];
-  const int n = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const int64_t qn = int64_t(n) * L + k;
+  const uint32_t lane = ld(m.layer_lanes + i);
+  const int n = lane_ent(lane), j = lane_lev(lane), L = m.L;
+  const int nzmin = ld(m.nzmin + n), nzmax = ld(m.nzmax + n);
+  const int64_t base = int64_t(n) * L, qn = base + j;
+  const int e0 = ld(m.ne_off + n), e1 = ld(m.ne_off + n + 1);
+  const double w = ld(in.w_e + qn), area = ld(m.area + qn);
+  const int jm = j > 0 ? j - 1 : 0;
+  const Rcp r3{3.0, 1.0 / 3.0, true};
+  const bool interior = j >= nzmin + 2 && j <= nzmax - 2 && j != nzmax - 1;
+  double Znz = 0.0, Zm1 = 0.0, Zm2 = 0.0, Zp1 = 0.0, zb = 0.0;
+  Rcp rdc{1.0, 1.0, true}, rdu{1.0, 1.0, true}, rdd{1.0, 1.0, true};
+  if (interior) {
+    qr4c_depths(in, m, base, j, Znz, Zm1, Zm2, Zp1, zb);
+    rdc = rcp(safe_nz(Zm1 - Znz));
+    rdu = rcp(safe_nz(Znz - Zp1));
+    rdd = rcp(safe_nz(Zm2 - Zm1));
+  }
   for (int t = 0; t < in.ntr; ++t) {
-    double gx = 0.0, gy = 0.0;
-    for (int j = m.ne_off[n]; j < m.ne_off[n + 1]; ++j) {
-      const int idx = m.ne_idx[j], e = idx >> 1;
-      if (!edge_on(m, e, k) || use_tri_at(m, e, k)) continue;
-      const EdgeTerms et = edge_terms(A, t, e, k);
-      if (idx & 1) { gx += et.gg1; gy += et.gg3; }
-      else { gx += et.gg0; gy += et.gg2; }
+    const int64_t o = t * in.ws.sN, oa = t * A.a.sN;
+    {   // node-average gradient, ascending edge id (loads unconditional, in bounds)
+      double gx = 0.0, gy = 0.0;
+#pragma unroll 2
+      for (int jj = e0; jj < e1; ++jj) {
+        const int4 sl = __ldg(m.ne4 + jj);
+        const int e = sl.x >> 1;
+        const bool on = in_range(j, unsigned(sl.z)) && !in_range(j, unsigned(ld(m.etr + e)));
+        const EdgeTerms et = edge_terms(A, t, e, j);
+        const bool second = sl.x & 1;
+        gx = on ? gx + (second ? et.gg1 : et.gg0) : gx;
+        gy = on ? gy + (second ? et.gg3 : et.gg2) : gy;
+      }
+      A.a.ggnx[oa + qn] = gx;
+      A.a.ggny[oa + qn] = gy;
     }
-    A.a.ggnx[t * A.a.sN + qn] = gx;
-    A.a.ggny[t * A.a.sN + qn] = gy;
+    const double* T = in.T + t * in.tstride + base;
+    const double* To = in.T_old + t * in.tstride + base;
+    const double* pf = in.ws.pf + o + base;
+    const double* mf = in.ws.mf + o + base;
+    const double* gplus = A.a.gplus + oa + base;
+    const double* gminus = A.a.gminus + oa + base;
+    const double* gdiv = A.a.gdiv + oa + base;
+    const double f = in.ws.adfv[o + qn];
+    double ae;
+    if (j == nzmin) ae = f >= 0.0 ? pf[j] : mf[j];
+    else ae = f >= 0.0 ? fmin(mf[j - 1], pf[j]) : fmin(pf[j - 1], mf[j]);
+    double gf = gvl_at(m, A.a.ghsc + oa, base, j, nzmin, nzmax) * ae;
+    gf += gplus[j] * dmax0(f) + gminus[j] * dmin0(f);
+    if (j - 1 >= nzmin) gf -= gplus[j - 1] * dmax0(-f) + gminus[j - 1] * dmin0(-f);
+    const double ghi = gf;
+    double gfv = -gf + gdiv[j];
+    if (j - 1 >= nzmin) gfv -= gdiv[j - 1];
+    A.a.gfv[oa + qn] = gfv;
+    double gw = 0.0;
+    gw += -0.5 * (ld(T + j) * (1.0 + sgn(w)) + ld(T + jm) * (1.0 - sgn(w))) * area * gfv;
+    // QR4C (tracer_adv.py:241-295): surface, next-to-surface / next-to-bottom, interior
+    double z0 = 0.0, zm1 = 0.0, zm2 = 0.0, zp1 = 0.0;
+    if (j == nzmin) {
+      gw += -ab2(ld(T + j), ld(To + j)) * area * ghi;
+      z0 = -w * area * ghi;
+    } else if (j == nzmin + 1 || j == nzmax - 1) {
+      gw += -0.5 * (ab2(ld(T + j - 1), ld(To + j - 1)) + ab2(ld(T + j), ld(To + j))) * area * ghi;
+      z0 = zm1 = -0.5 * w * area * ghi;
+    } else if (interior) {
+      const double A0 = ab2(ld(T + j), ld(To + j)), Am1 = ab2(ld(T + j - 1), ld(To + j - 1));
+      const double Am2 = ab2(ld(T + j - 2), ld(To + j - 2)), Ap1 = ab2(ld(T + j + 1), ld(To + j + 1));
+      const double qc = divr(Am1 - A0, rdc), qu = divr(A0 - Ap1, rdu), qd = divr(Am2 - Am1, rdd);
+      const double Tmean1 = A0 + divr((2.0 * qc + qu) * (zb - Znz), r3);
+      const double Tmean2 = Am1 + divr((2.0 * qc + qd) * (zb - Zm1), r3);
+      gw += -0.5 * (Tmean1 + Tmean2) * area * ghi;
+      // Tmean1 = A0 + (2 qc + qu) (zb - Z[j]) / 3, Tmean2 = Am1 + (2 qc + qd) (zb - Z[j-1]) / 3
+      const double gS = -0.5 * w * area * ghi;
+      const double gq1 = divr(gS * (zb - Znz), r3), gq2 = divr(gS * (zb - Zm1), r3);
+      const double gqc = 2.0 * gq1 + 2.0 * gq2, gqu = gq1, gqd = gq2;
+      z0 = gS - divr(gqc, rdc) + divr(gqu, rdu);
+      zm1 = gS + divr(gqc, rdc) - divr(gqd, rdd);
+      zm2 = divr(gqd, rdd);
+      zp1 = -divr(gqu, rdu);
+    }
+    A.a.gw[oa + qn] = gw;
+    A.a.gz0[oa + qn] = z0;
+    A.a.gzm1[oa + qn] = zm1;
+    A.a.gzm2[oa + qn] = zm2;
+    A.a.gzp1[oa + qn] = zp1;
   }
 }
 
@@ -460,191 +587,42 @@ __global__ void __launch_bounds__(B) r_tr(Adj A) {
   const DevMesh& m = *in.m;
   const int64_t i = lane_index();
   if (i >= m.n_elem) return;
-  const uint32_t lane = m.elem_lanes[i];
+  const uint32_t lane = ld(m.elem_lanes + i);
   const int el = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const double aw = m.earea[el];
+  const double aw = ld(m.earea + el);
+  const int u0 = ld(m.eud_off + el), u1 = ld(m.eud_off + el + 1);
+  const int64_t qv[3] = {int64_t(ld(m.enodes + 3 * el)) * L + k,
+                         int64_t(ld(m.enodes + 3 * el + 1)) * L + k,
+                         int64_t(ld(m.enodes + 3 * el + 2)) * L + k};
+  // the forward's (safe) node-average denominators of the three vertices
+  const Rcp rd[3] = {rcp(in.ws.nden[qv[0]]), rcp(in.ws.nden[qv[1]]), rcp(in.ws.nden[qv[2]])};
   for (int t = 0; t < in.ntr; ++t) {
     const int64_t oa = t * A.a.sN;
     double gx = 0.0, gy = 0.0;
-    for (int j = m.eud_off[el]; j < m.eud_off[el + 1]; ++j) {
-      const int idx = m.eud_idx[j], e = idx >> 1;
-      if (!edge_on(m, e, k) || !use_tri_at(m, e, k)) continue;
+    for (int j = u0; j < u1; ++j) {   // edges using el as up (slot 0) or down (1) cell
+      const int idx = ld(m.eud_idx + j), e = idx >> 1;
+      const bool on = in_range(k, unsigned(ld(m.etr + e)));
       const EdgeTerms et = edge_terms(A, t, e, k);
-      if (idx & 1) { gx += et.gg1; gy += et.gg3; }   // down triangle
-      else { gx += et.gg0; gy += et.gg2; }           // up triangle
+      gx = on ? gx + ((idx & 1) ? et.gg1 : et.gg0) : gx;   // down : up triangle
+      gy = on ? gy + ((idx & 1) ? et.gg3 : et.gg2) : gy;
     }
+#pragma unroll
     for (int v = 0; v < 3; ++v) {   // gnode(n) = sum_e a_e tr_e / den(n)
-      const int n = m.enodes[3 * el + v];
-      const int64_t qn = int64_t(n) * L + k;
-      const double dd = in.ws.nden[qn];   // the forward's (safe) denominator
-      gx += A.a.ggnx[oa + qn] * aw / dd;
-      gy += A.a.ggny[oa + qn] * aw / dd;
+      gx += divr(A.a.ggnx[oa + qv[v]] * aw, rd[v]);
+      gy += divr(A.a.ggny[oa + qv[v]] * aw, rd[v]);
     }
     A.a.gtrx[t * A.a.sE + int64_t(el) * L + k] = gx;
     A.a.gtry[t * A.a.sE + int64_t(el) * L + k] = gy;
   }
 }
 
-// ------------------------- r_grad_t: tracer_gradient_elements transposed (on T)
-__global__ void __launch_bounds__(B) r_grad_t(Adj A) {
-  const Inst& in = A.in;
-  const DevMesh& m = *in.m;
-  const int64_t i = lane_index();
-  if (i >= m.n_layer) return;
-  const uint32_t lane = m.layer_lanes[i];
-  const int n = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const int64_t qn = int64_t(n) * L + k;
-  for (int t = 0; t < in.ntr; ++t) {
-    double g = 0.0;
-    for (int j = m.nel_off[n]; j < m.nel_off[n + 1]; ++j) {
-      const int el = m.nel_idx[j];
-      if (!elem_on(m, el, k)) continue;
-      const int iv = m.enodes[3 * el] == n ? 0 : (m.enodes[3 * el + 1] == n ? 1 : 2);
-      const int64_t qe = t * A.a.sE + int64_t(el) * L + k;
-      g += m.gsca[6 * el + iv] * A.a.gtrx[qe] + m.gsca[6 * el + 3 + iv] * A.a.gtry[qe];
-    }
-    A.a.gTtr[t * A.a.sN + qn] = g;
-  }
-}
-
-// ------- r_vert_a / r_vert_b: vertical fluxes (QR4C HO, upwind LO) and their limiter terms.
-// r_vert_a (one thread per layer interface j of a node): the cotangent gf of adf_v[j]
-// (limiter application and the plus/minus sums), ghi = gf and gfv = -gf + gdiv terms,
-// stored in the dead r_ratio outputs gtmax / gtmin, and gw[j] complete (only interface
-// j feeds it). r_vert_b (one thread per node level k): gT[k] and gA[k] gathered from the
-// interfaces j = k-1 .. k+2 in ascending j (the order of a column loop over j that
-// scatters into gT / gA), so the per-level sums do not depend on the parallel split.
-__device__ __forceinline__ void qr4c_depths(const Inst& in, const DevMesh& m, int64_t base,
-                                            int j, double& Znz, double& Zm1, double& Zm2,
-                                            double& Zp1, double& zb) {
-  const int L = m.L;
-  if (in.Z3d) {
-    const double* Zc = in.Z3d + base;
-    Znz = Zc[j]; Zm1 = Zc[j - 1]; Zm2 = Zc[j - 2]; Zp1 = Zc[j + 1 < L ? j + 1 : L - 1];
-    zb = in.zbar3[base + j];
-  } else {
-    Znz = m.Zp[j]; Zm1 = m.Zp[j - 1]; Zm2 = m.Zp[j - 2]; Zp1 = m.Zp[j + 1 < L ? j + 1 : L - 1];
-    zb = m.zbar[j];
-  }
-}
-
-__global__ void __launch_bounds__(B) r_vert_a(Adj A) {
-  const Inst& in = A.in;
-  const DevMesh& m = *in.m;
-  const int64_t i = lane_index();
-  if (i >= m.n_layer) return;
-  const uint32_t lane = m.layer_lanes[i];
-  const int n = lane_ent(lane), j = lane_lev(lane), L = m.L;
-  const int nzmin = m.nzmin[n], nzmax = m.nzmax[n];
-  const int64_t base = int64_t(n) * L;
-  const double dt = in.dt;
-  const double w = in.w_e[base + j], area = m.area[base + j];
-  const int jm = j > 0 ? j - 1 : 0;
-  for (int t = 0; t < in.ntr; ++t) {
-    const double* T = in.T + t * in.tstride + base;
-    const double* To = in.T_old + t * in.tstride + base;
-    const int64_t o = t * in.ws.sN, oa = t * A.a.sN;
-    const double* pf = in.ws.pf + o + base;
-    const double* mf = in.ws.mf + o + base;
-    const double* gplus = A.a.gplus + oa + base;
-    const double* gminus = A.a.gminus + oa + base;
-    const double* gdiv = A.a.gdiv + oa + base;
-    const double f = in.ws.adfv[o + base + j];
-    double ae;
-    if (j == nzmin) ae = f >= 0.0 ? pf[j] : mf[j];
-    else ae = f >= 0.0 ? fmin(mf[j - 1], pf[j]) : fmin(pf[j - 1], mf[j]);
-    double gf = gvl_at(m, A.a.gdel + oa, base, j, nzmin, nzmax, dt) * ae;
-    gf += gplus[j] * dmax0(f) + gminus[j] * dmin0(f);
-    if (j - 1 >= nzmin) gf -= gplus[j - 1] * dmax0(-f) + gminus[j - 1] * dmin0(-f);
-    const double ghi = gf;
-    double gfv = -gf + gdiv[j];
-    if (j - 1 >= nzmin) gfv -= gdiv[j - 1];
-    A.a.gtmax[oa + base + j] = ghi;
-    A.a.gtmin[oa + base + j] = gfv;
-    double gw = 0.0;
-    gw += -0.5 * (T[j] * (1.0 + sgn(w)) + T[jm] * (1.0 - sgn(w))) * area * gfv;
-    if (j == nzmin) {
-      gw += -ab2(T[j], To[j]) * area * ghi;
-    } else if (j == nzmin + 1 || j == nzmax - 1) {
-      gw += -0.5 * (ab2(T[j - 1], To[j - 1]) + ab2(T[j], To[j])) * area * ghi;
-    } else if (j >= nzmin + 2 && j <= nzmax - 2) {
-      double Znz, Zm1, Zm2, Zp1, zb;
-      qr4c_depths(in, m, base, j, Znz, Zm1, Zm2, Zp1, zb);
-      const double dc = safe_nz(Zm1 - Znz), du = safe_nz(Znz - Zp1), dd = safe_nz(Zm2 - Zm1);
-      const double A0 = ab2(T[j], To[j]), Am1 = ab2(T[j - 1], To[j - 1]);
-      const double Am2 = ab2(T[j - 2], To[j - 2]), Ap1 = ab2(T[j + 1], To[j + 1]);
-      const double qc = (Am1 - A0) / dc, qu = (A0 - Ap1) / du, qd = (Am2 - Am1) / dd;
-      const double Tmean1 = A0 + (2.0 * qc + qu) * (zb - Znz) / 3.0;
-      const double Tmean2 = Am1 + (2.0 * qc + qd) * (zb - Zm1) / 3.0;
-      gw += -0.5 * (Tmean1 + Tmean2) * area * ghi;
-    }
-    A.a.gw[oa + base + j] = gw;
-  }
-}
-
-// contribution of interface j to gA[k] (QR4C on ttfAB)
-__device__ __forceinline__ double ga_term(const Inst& in, const DevMesh& m, int64_t base, int j,
-                                         int k, int nzmin, int nzmax, double ghi) {
-  const double w = in.w_e[base + j], area = m.area[base + j];
-  if (j == nzmin) return k == j ? -w * area * ghi : 0.0;
-  if (j == nzmin + 1 || j == nzmax - 1)
-    return (k == j - 1 || k == j) ? -0.5 * w * area * ghi : 0.0;
-  double Znz, Zm1, Zm2, Zp1, zb;
-  qr4c_depths(in, m, base, j, Znz, Zm1, Zm2, Zp1, zb);
-  const double dc = safe_nz(Zm1 - Znz), du = safe_nz(Znz - Zp1), dd = safe_nz(Zm2 - Zm1);
-  const double gS = -0.5 * w * area * ghi;
-  const double gq1 = gS * (zb - Znz) / 3.0, gq2 = gS * (zb - Zm1) / 3.0;
-  const double gqc = 2.0 * gq1 + 2.0 * gq2, gqu = gq1, gqd = gq2;
-  if (k == j) return gS - gqc / dc + gqu / du;
-  if (k == j - 1) return gS + gqc / dc - gqd / dd;
-  if (k == j - 2) return gqd / dd;
-  return -gqu / du;   // k == j + 1
-}
-
-__global__ void __launch_bounds__(B) r_vert_b(Adj A) {
-  const Inst& in = A.in;
-  const DevMesh& m = *in.m;
-  const int64_t i = lane_index();
-  if (i >= m.n_layer) return;
-  const uint32_t lane = m.layer_lanes[i];
-  const int n = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const int nzmin = m.nzmin[n], nzmax = m.nzmax[n];
-  const int64_t base = int64_t(n) * L;
-  // Wet layers only: the dry entries of gTv / gAv / gw stay zero from the workspace's
-  // one-time clear, except level nzmin - 1 (above a cavity's first layer), which the
-  // upwind flux of interface nzmin reaches through jm = nzmin - 1; its thread writes it.
-  for (int t = 0; t < in.ntr; ++t) {
-    const int64_t oa = t * A.a.sN;
-    const double* ghi = A.a.gtmax + oa + base;
-    const double* gfv = A.a.gtmin + oa + base;
-    double gT = 0.0, gA = 0.0;
-    {
-      const double w = in.w_e[base + k], area = m.area[base + k];
-      gT += -0.5 * (w + fabs(w)) * area * gfv[k];
-      if (k == 0) gT += -0.5 * (w - fabs(w)) * area * gfv[k];
-    }
-    if (k + 1 < nzmax) {
-      const double w = in.w_e[base + k + 1], area = m.area[base + k + 1];
-      gT += -0.5 * (w - fabs(w)) * area * gfv[k + 1];
-    }
-    // QR4C terms from interfaces k-1 .. k+2 in ascending j (a term that does not reach
-    // k is +0.0; gA starts at +0.0, so adding it changes no bit)
-    for (int j = k - 1; j <= k + 2; ++j) {
-      if (j < nzmin || j >= nzmax) continue;
-      gA += ga_term(in, m, base, j, k, nzmin, nzmax, ghi[j]);
-    }
-    A.a.gTv[oa + base + k] = gT;
-    A.a.gAv[oa + base + k] = gA;
-    if (k == nzmin && k > 0) {   // dry level above: only the (w - |w|) term of interface k
-      const double w = in.w_e[base + k], area = m.area[base + k];
-      double g = 0.0;
-      g += -0.5 * (w - fabs(w)) * area * gfv[k];
-      A.a.gTv[oa + base + k - 1] = g;
-    }
-  }
-}
-
-// --------------- r_final: assemble dT and dT_old (tracer_ab: ttfAB = -0.6 T_old + 1.6 T)
+// --------------- r_final: dT and dT_old at every node level (tracer_ab: ttfAB = -0.6 T_old
+// + 1.6 T). Wet layers gather: the seed/LO/bounds terms (gTp); the element gradients on T
+// over the node's cells (tracer_gradient_elements transposed); the vertical upwind flux of
+// interfaces k and k+1 on T, and the QR4C fluxes of interfaces k-1 .. k+2 on ttfAB in
+// ascending interface order; the edge terms in ascending edge id. Dry levels keep T
+// (T_new = T there), except level nzmin - 1 above a cavity's first layer, which the upwind
+// flux of interface nzmin reaches. Also sums gw_e over the tracers.
 __global__ void __launch_bounds__(B) r_final(Adj A) {
   const Inst& in = A.in;
   const DevMesh& m = *in.m;
@@ -653,26 +631,73 @@ __global__ void __launch_bounds__(B) r_final(Adj A) {
   if (i >= NL) return;
   const int L = m.L;
   const int n = int(i / L), k = int(i - int64_t(n) * L);
-  const bool layer = k >= m.nzmin[n] && k < m.nzmax[n];
+  const int nzmin = ld(m.nzmin + n), nzmax = ld(m.nzmax + n);
+  const bool layer = k >= nzmin && k < nzmax;
+  const int e0 = ld(m.ne_off + n), e1 = ld(m.ne_off + n + 1);
+  const int c0 = ld(m.nel_off + n), c1 = ld(m.nel_off + n + 1);
   for (int t = 0; t < in.ntr; ++t) {
     const int64_t oa = t * A.a.sN;
-    const double gv = A.a.gTv[oa + i];
-    double gT, gA = A.a.gAv[oa + i];
+    const double* gfv = A.a.gfv + oa;
+    double gT, gA = 0.0;
     if (!layer) {
-      gT = A.gTn[t * in.tstride + i] + gv;   // dry levels: T_new = T
+      double gv = 0.0;
+      if (k + 1 == nzmin && nzmin < nzmax) {   // above a cavity: the (w - |w|) term of
+                                               // interface nzmin only
+        const double w = ld(in.w_e + i + 1), area = ld(m.area + i + 1);
+        double g = 0.0;
+        g += -0.5 * (w - fabs(w)) * area * gfv[i + 1];
+        gv = g;
+      }
+      gT = ld(A.gTn + t * in.tstride + i) + gv;   // dry levels: T_new = T
     } else {
-      gT = A.a.gTp[oa + i] + A.a.gTtr[oa + i] + gv;
-      for (int j = m.ne_off[n]; j < m.ne_off[n + 1]; ++j) {
-        const int idx = m.ne_idx[j], e = idx >> 1;
-        if (!edge_on(m, e, k)) continue;
-        const EdgeTerms et = edge_terms(A, t, e, k);
-        if (idx & 1) { gT += et.gT2; gA += et.gA2; }
-        else { gT += et.gT1; gA += et.gA1; }
+      // vertical upwind fluxes of interfaces k and k+1
+      double gTv = 0.0;
+      {
+        const double w = ld(in.w_e + i), area = ld(m.area + i);
+        gTv += -0.5 * (w + fabs(w)) * area * gfv[i];
+        if (k == 0) gTv += -0.5 * (w - fabs(w)) * area * gfv[i];
+      }
+      if (k + 1 < nzmax) {
+        const double w = ld(in.w_e + i + 1), area = ld(m.area + i + 1);
+        gTv += -0.5 * (w - fabs(w)) * area * gfv[i + 1];
+      }
+      // QR4C terms of interfaces k-1 .. k+2 in ascending order (a term that does not
+      // reach k is +0.0; gA starts at +0.0, so adding it changes no bit)
+      if (k - 1 >= nzmin) gA += A.a.gzp1[oa + i - 1];
+      gA += A.a.gz0[oa + i];
+      if (k + 1 < nzmax) gA += A.a.gzm1[oa + i + 1];
+      if (k + 2 < nzmax) gA += A.a.gzm2[oa + i + 2];
+      // element gradients on T: the node's cells in nod_in_elem2D order
+      double gTtr = 0.0;
+#pragma unroll 2
+      for (int j = c0; j < c1; ++j) {
+        const unsigned r = unsigned(ld(m.nelr + j));
+        const bool on = in_range(k, r);
+        const int el = ld(m.nel_idx + j), iv = int((r >> 16) & 3u);
+        const int64_t qe = t * A.a.sE + int64_t(el) * L + k;
+        const double v = ld(m.gsca + 6 * el + iv) * A.a.gtrx[qe] +
+                         ld(m.gsca + 6 * el + 3 + iv) * A.a.gtry[qe];
+        gTtr = on ? gTtr + v : gTtr;
+      }
+      gT = A.a.gTp[oa + i] + gTtr + gTv;
+#pragma unroll 2
+      for (int j = e0; j < e1; ++j) {
+        const int4 sl = __ldg(m.ne4 + j);
+        const bool on = in_range(k, unsigned(sl.z));
+        const EdgeTerms et = edge_terms(A, t, sl.x >> 1, k);
+        const bool second = sl.x & 1;
+        gT = on ? gT + (second ? et.gT2 : et.gT1) : gT;
+        gA = on ? gA + (second ? et.gA2 : et.gA1) : gA;
       }
     }
-    A.gT[t * in.tstride + i] = gT + kAbNew * gA;
-    A.gTo[t * in.tstride + i] = kAbOld * gA;
+    const int64_t oT = t * in.tstride + i;
+    const double vT = gT + kAbNew * gA, vTo = kAbOld * gA;
+    A.gT[oT] = (A.acc & kAccT) ? A.gT[oT] + vT : vT;
+    A.gTo[oT] = (A.acc & kAccTo) ? A.gTo[oT] + vTo : vTo;
   }
+  double g = 0.0;   // dL/dw_e summed over tracers (dry levels hold the workspace's zeros)
+  for (int t = 0; t < in.ntr; ++t) g += A.a.gw[t * A.a.sN + i];
+  A.gw[i] = (A.acc & kAccW) ? A.gw[i] + g : g;
 }
 
 // -------------------------- r_uv: edge_vflux transposed, summed over tracers
@@ -684,37 +709,31 @@ __global__ void __launch_bounds__(B) r_uv(Adj A) {
   if (i >= int64_t(m.E) * L) return;
   const int el = int(i / L), k = int(i - int64_t(el) * L);
   double gU = 0.0, gV = 0.0;
-  if (elem_on(m, el, k)) {
-    const double h = in.helem[i];
+  if (k >= ld(m.eul + el) && k < ld(m.enl + el)) {
+    const double h = ld(in.helem + i);
     for (int r = 0; r < 3; ++r) {
-      const int ent = m.eedge[3 * el + r];
+      const int ent = ld(m.eedge + 3 * el + r);
       if (ent < 0) continue;
       const int e = ent >> 1;
       const double* cr = m.cross + 4 * int64_t(e);
       double gvf = 0.0;
       for (int t = 0; t < in.ntr; ++t) gvf += A.a.gvf[t * A.a.sEd + int64_t(e) * L + k];
       if (ent & 1) {   // t2 = (V dx2 - U dy2) h
-        gU += -gvf * cr[3] * h;
-        gV += gvf * cr[2] * h;
+        gU += -gvf * ld(cr + 3) * h;
+        gV += gvf * ld(cr + 2) * h;
       } else {         // t1 = (U dy1 - V dx1) h
-        gU += gvf * cr[1] * h;
-        gV += -gvf * cr[0] * h;
+        gU += gvf * ld(cr + 1) * h;
+        gV += -gvf * ld(cr + 0) * h;
       }
     }
   }
-  A.guv[2 * i] = gU;
-  A.guv[2 * i + 1] = gV;
-}
-
-// ---------------------------------------------- r_wsum: dL/dw_e summed over tracers
-__global__ void __launch_bounds__(B) r_wsum(Adj A) {
-  const Inst& in = A.in;
-  const DevMesh& m = *in.m;
-  const int64_t i = lane_index();
-  if (i >= int64_t(m.N) * m.L) return;
-  double g = 0.0;
-  for (int t = 0; t < in.ntr; ++t) g += A.a.gw[t * A.a.sN + i];
-  A.gw[i] = g;
+  if (A.acc & kAccUV) {
+    A.guv[2 * i] += gU;
+    A.guv[2 * i + 1] += gV;
+  } else {
+    A.guv[2 * i] = gU;
+    A.guv[2 * i + 1] = gV;
+  }
 }
 
 // --------------------------------- compute_w reverse: w = mask * suffix-sum(div) / area
@@ -747,7 +766,7 @@ __global__ void __launch_bounds__(B) r_w_uv(const DevMesh* __restrict__ mp,
   if (i >= int64_t(m.E) * L) return;
   const int el = int(i / L), k = int(i - int64_t(el) * L);
   double gU = 0.0, gV = 0.0;
-  if (elem_on(m, el, k)) {
+  if (k >= m.eul[el] && k < m.enl[el]) {
     const double h = helem[i];
     for (int r = 0; r < 3; ++r) {
       const int ent = m.eedge[3 * el + r];
@@ -774,6 +793,83 @@ __global__ void __launch_bounds__(B) r_w_uv(const DevMesh* __restrict__ mp,
   }
 }
 
+// Reverse-pass workspace of `max_tracers` tracers (zeroed: the dry-level entries are
+// never written by the reverse kernels and must read as zero).
+int reserve_adj_ws(FctPlan* P, int max_tracers) {
+  if (max_tracers <= P->adj_tracers) return FCT_OK;
+  FCT_CUDA(cudaSetDevice(P->device));
+  const int64_t sN = int64_t(P->N) * P->L, sE = int64_t(P->E) * P->L, sEd = int64_t(P->Ed) * P->L;
+  const int64_t nd = int64_t(max_tracers) * (kAdjNodeFields * sN + kAdjEdgeFields * sEd +
+                                             kAdjElemFields * sE);
+  double* p = nullptr;
+  FCT_CUDA(cudaMalloc(&p, size_t(nd) * sizeof(double)));
+  FCT_CUDA(cudaMemset(p, 0, size_t(nd) * sizeof(double)));
+  if (P->d_adj) cudaFree(P->d_adj);
+  P->d_adj = p;
+  AdjWorkspace& a = P->aws;
+  a.sN = sN; a.sE = sE; a.sEd = sEd;
+  auto take = [&](int64_t n) { double* q = p; p += n * max_tracers; return q; };
+  double** node[] = {&a.ghsc, &a.gpf, &a.gmf, &a.gplus, &a.gminus, &a.gLOl, &a.gqx,
+                     &a.gqn, &a.gdiv, &a.gTp, &a.ggnx, &a.ggny, &a.gfv, &a.gw, &a.gz0,
+                     &a.gzm1, &a.gzm2, &a.gzp1};
+  static_assert(sizeof(node) / sizeof(node[0]) == kAdjNodeFields, "node field count");
+  for (double** f : node) *f = take(sN);
+  double** edge[] = {&a.gHO, &a.gfl, &a.gvf};
+  static_assert(sizeof(edge) / sizeof(edge[0]) == kAdjEdgeFields, "edge field count");
+  for (double** f : edge) *f = take(sEd);
+  double** elem[] = {&a.gax, &a.gan, &a.gtrx, &a.gtry};
+  static_assert(sizeof(elem) / sizeof(elem[0]) == kAdjElemFields, "elem field count");
+  for (double** f : elem) *f = take(sE);
+  P->adj_tracers = max_tracers;
+  return FCT_OK;
+}
+
+int check_fields(const FctFields* f) {
+  if (!f->uv || !f->w_e || !f->helem || !f->hnode || !f->hnode_new || !f->T || !f->T_old)
+    return set_error(FCT_ERR_INVALID, "a required field pointer is NULL");
+  if (f->w_i) return set_error(FCT_ERR_UNSUPPORTED, "the adjoint does not differentiate w_i");
+  if ((f->Z3d == nullptr) != (f->zbar3 == nullptr))
+    return set_error(FCT_ERR_INVALID, "Z3d and zbar3 must be given together");
+  return FCT_OK;
+}
+
+Inst make_inst(const FctPlan* P, const FctFields* f, double dt, int ntr, const Workspace& ws) {
+  Inst in{};
+  in.m = P->d_mesh;
+  in.uv = f->uv; in.w_e = f->w_e; in.helem = f->helem;
+  in.hnode = f->hnode; in.hnode_new = f->hnode_new;
+  in.T = f->T; in.T_old = f->T_old;
+  in.T_new = f->T_new;
+  in.tstride = f->tracer_stride ? f->tracer_stride : int64_t(P->N) * P->L;
+  in.tg = 0;
+  in.wtg = ntr;
+  in.Z3d = f->Z3d; in.zbar3 = f->zbar3; in.w_i = nullptr;
+  in.ws = ws;
+  in.dt = dt;
+  in.ntr = ntr;
+  return in;
+}
+
+LaunchDims unfused_dims(const FctPlan* P, int ntr) {
+  LaunchDims d{};
+  d.max_iface = P->hm.n_iface; d.max_layer = P->hm.n_layer; d.max_edge = P->hm.n_edge;
+  d.max_elem = P->hm.n_elem; d.max_dense = int64_t(P->N) * P->L; d.max_nodes = P->N;
+  d.ntr = ntr; d.chunk = 0; d.per_thread = 8; d.any_wi = false; d.copy_dry = true;
+  d.fused = false;   // the reverse kernels read every stage's intermediates
+  return d;
+}
+
+struct DeviceGuard {
+  int prev = -1, dev;
+  explicit DeviceGuard(int d) : dev(d) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    if (prev >= 0 && prev != dev) cudaSetDevice(prev);
+  }
+};
+
 }  // namespace
 
 extern "C" {
@@ -781,108 +877,152 @@ extern "C" {
 int fct_plan_reserve_adjoint(FctPlan* P, int max_tracers) {
   if (!P) return set_error(FCT_ERR_INVALID, "plan is NULL");
   if (max_tracers < 1) return set_error(FCT_ERR_INVALID, "max_tracers must be >= 1");
-  if (max_tracers <= P->adj_tracers) return FCT_OK;
   int st = plan_reserve_ws(P, max_tracers, /*full=*/true);   // the recompute keeps every field
   if (st) return st;
-  FCT_CUDA(cudaSetDevice(P->device));
-  const int64_t sN = int64_t(P->N) * P->L, sE = int64_t(P->E) * P->L, sEd = int64_t(P->Ed) * P->L;
-  const int64_t nd = int64_t(max_tracers) * (kAdjNodeFields * sN + kAdjEdgeFields * sEd +
-                                             kAdjElemFields * sE);
-  double* p = nullptr;
-  FCT_CUDA(cudaMalloc(&p, size_t(nd) * sizeof(double)));
-  // dry-level entries are never written by the reverse kernels and must read as zero
-  FCT_CUDA(cudaMemset(p, 0, size_t(nd) * sizeof(double)));
-  if (P->d_adj) cudaFree(P->d_adj);
-  P->d_adj = p;
-  AdjWorkspace& a = P->aws;
-  a.sN = sN; a.sE = sE; a.sEd = sEd;
-  auto take = [&](int64_t n) { double* q = p; p += n * max_tracers; return q; };
-  double** node[] = {&a.gdel, &a.gLOd, &a.gTd, &a.gpf, &a.gmf, &a.gtmax, &a.gtmin, &a.gplus,
-                     &a.gminus, &a.gLOl, &a.gtvmax, &a.gtvmin, &a.gLOb, &a.gTb, &a.gdiv,
-                     &a.ggnx, &a.ggny, &a.gTp, &a.gTtr, &a.gTv, &a.gAv, &a.gw};
-  static_assert(sizeof(node) / sizeof(node[0]) == kAdjNodeFields, "node field count");
-  for (double** f : node) *f = take(sN);
-  double** edge[] = {&a.gHO, &a.gfl, &a.gvf};
-  static_assert(sizeof(edge) / sizeof(edge[0]) == kAdjEdgeFields, "edge field count");
-  for (double** f : edge) *f = take(sEd);
-  double** elem[] = {&a.gamax, &a.gamin, &a.gtrx, &a.gtry};
-  static_assert(sizeof(elem) / sizeof(elem[0]) == kAdjElemFields, "elem field count");
-  for (double** f : elem) *f = take(sE);
-  P->adj_tracers = max_tracers;
+  return reserve_adj_ws(P, max_tracers);
+}
+
+int fct_tape_bytes(const FctPlan* P, int ntr, int steps, int64_t* out) {
+  if (!P || !out) return set_error(FCT_ERR_INVALID, "NULL argument");
+  if (ntr < 1 || steps < 1) return set_error(FCT_ERR_INVALID, "ntr and steps must be >= 1");
+  *out = int64_t(steps) * workspace_doubles(P->N, P->E, P->Ed, P->L, ntr) * int64_t(sizeof(double));
   return FCT_OK;
 }
 
-int fct_adjoint(FctPlan* P, const FctFields* f, const double* gT_new, double dt, int ntr,
-                const FctGrads* g, fct_stream_t stream) {
+int fct_tape_create(FctPlan* P, int ntr, int steps, void* mem, int64_t bytes, FctTape** out) {
+  if (!P || !out) return set_error(FCT_ERR_INVALID, "NULL argument");
+  *out = nullptr;
+  if (ntr < 1 || steps < 1) return set_error(FCT_ERR_INVALID, "ntr and steps must be >= 1");
+  const int64_t per = workspace_doubles(P->N, P->E, P->Ed, P->L, ntr);
+  const int64_t need = per * int64_t(steps) * int64_t(sizeof(double));
+  if (mem) {
+    if (bytes < need)
+      return set_error(FCT_ERR_CAPACITY, "tape memory of %lld bytes < %lld needed",
+                       (long long)bytes, (long long)need);
+    if (reinterpret_cast<uintptr_t>(mem) % 256 != 0)
+      return set_error(FCT_ERR_INVALID, "tape memory must be 256-byte aligned");
+  }
+  DeviceGuard g(P->device);
+  int st = reserve_adj_ws(P, ntr);
+  if (st) return st;
+  double* d = static_cast<double*>(mem);
+  if (!d) {
+    const cudaError_t e = cudaMalloc(&d, size_t(need));
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return set_error(FCT_ERR_CUDA, "tape of %d steps x %d tracers (%.2f GB): %s", steps, ntr,
+                       double(need) * 1e-9, cudaGetErrorString(e));
+    }
+  }
+  FctTape* T = new FctTape();
+  T->plan = P;
+  T->ntr = ntr;
+  T->steps = steps;
+  T->d = d;
+  T->owned = mem == nullptr;
+  for (int s = 0; s < steps; ++s)
+    T->ws.push_back(carve_workspace(d + per * s, P->N, P->E, P->Ed, P->L, ntr));
+  T->recorded.assign(size_t(steps), 0);
+  T->dt.assign(size_t(steps), 0.0);
+  *out = T;
+  return FCT_OK;
+}
+
+int fct_tape_destroy(FctTape* T) {
+  if (!T) return FCT_OK;
+  DeviceGuard g(T->plan->device);
+  if (T->d && T->owned) cudaFree(T->d);
+  delete T;
+  return FCT_OK;
+}
+
+int fct_forward_taped(FctPlan* P, const FctFields* f, double dt, int ntr, FctTape* tape,
+                      int slot, fct_stream_t stream) {
+  if (!P || !f || !tape) return set_error(FCT_ERR_INVALID, "NULL argument");
+  if (tape->plan != P) return set_error(FCT_ERR_INVALID, "the tape belongs to another plan");
+  if (ntr < 1 || ntr > tape->ntr)
+    return set_error(FCT_ERR_CAPACITY, "ntr=%d outside the tape's [1, %d]", ntr, tape->ntr);
+  if (slot < 0 || slot >= tape->steps)
+    return set_error(FCT_ERR_INVALID, "slot %d outside the tape's [0, %d)", slot, tape->steps);
+  int st = check_fields(f);
+  if (st) return st;
+  if (!f->T_new) return set_error(FCT_ERR_INVALID, "T_new is NULL");
+  if (!(dt > 0.0)) return set_error(FCT_ERR_INVALID, "dt must be positive");
+  DeviceGuard g(P->device);
+  const Inst in = make_inst(P, f, dt, ntr, tape->ws[size_t(slot)]);
+  st = launch_forward(in, nullptr, 1, unfused_dims(P, ntr), static_cast<cudaStream_t>(stream));
+  if (st) return st;
+  tape->recorded[size_t(slot)] = 1;
+  tape->dt[size_t(slot)] = dt;
+  return FCT_OK;
+}
+
+int fct_adjoint_ex(FctPlan* P, const FctFields* f, const double* gT_new, double dt, int ntr,
+                   const FctGrads* g, const FctTape* tape, int slot, int accumulate,
+                   fct_stream_t stream) {
   if (!P || !f || !g || !gT_new) return set_error(FCT_ERR_INVALID, "NULL argument");
   if (ntr < 1) return set_error(FCT_ERR_INVALID, "ntr must be >= 1");
-  if (ntr > P->adj_tracers || ntr > P->max_tracers)
+  if (accumulate & ~(kAccT | kAccTo | kAccUV | kAccW))
+    return set_error(FCT_ERR_INVALID, "unknown accumulate bits 0x%x", accumulate);
+  if (ntr > P->adj_tracers)
     return set_error(FCT_ERR_CAPACITY, "ntr=%d exceeds the reserved adjoint workspace (%d); "
                      "call fct_plan_reserve_adjoint first", ntr, P->adj_tracers);
-  if (!f->uv || !f->w_e || !f->helem || !f->hnode || !f->hnode_new || !f->T || !f->T_old)
-    return set_error(FCT_ERR_INVALID, "a required field pointer is NULL");
+  if (tape) {
+    if (tape->plan != P) return set_error(FCT_ERR_INVALID, "the tape belongs to another plan");
+    if (slot < 0 || slot >= tape->steps)
+      return set_error(FCT_ERR_INVALID, "slot %d outside the tape's [0, %d)", slot, tape->steps);
+    if (!tape->recorded[size_t(slot)])
+      return set_error(FCT_ERR_INVALID, "tape slot %d holds no recorded step", slot);
+    if (ntr > tape->ntr)
+      return set_error(FCT_ERR_CAPACITY, "ntr=%d exceeds the tape's %d tracers", ntr, tape->ntr);
+    if (tape->dt[size_t(slot)] != dt)
+      return set_error(FCT_ERR_INVALID, "dt differs from the recorded step's");
+  } else if (ntr > P->max_tracers || !P->ws_full) {
+    return set_error(FCT_ERR_CAPACITY, "ntr=%d exceeds the reserved recompute workspace; "
+                     "call fct_plan_reserve_adjoint first", ntr);
+  }
+  int st = check_fields(f);
+  if (st) return st;
   if (!g->gT || !g->gT_old || !g->guv || !g->gw_e)
     return set_error(FCT_ERR_INVALID, "a gradient output pointer is NULL");
-  if (f->w_i) return set_error(FCT_ERR_UNSUPPORTED, "the adjoint does not differentiate w_i");
-  if ((f->Z3d == nullptr) != (f->zbar3 == nullptr))
-    return set_error(FCT_ERR_INVALID, "Z3d and zbar3 must be given together");
   if (!(dt > 0.0)) return set_error(FCT_ERR_INVALID, "dt must be positive");
-  int prev = -1;
-  cudaGetDevice(&prev);
-  if (prev != P->device) cudaSetDevice(P->device);
-  auto restore = [&](int st) {
-    if (prev >= 0 && prev != P->device) cudaSetDevice(prev);
-    return st;
-  };
+  DeviceGuard guard(P->device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   Adj A{};
-  Inst& in = A.in;
-  in.m = P->d_mesh;
-  in.uv = f->uv; in.w_e = f->w_e; in.helem = f->helem;
-  in.hnode = f->hnode; in.hnode_new = f->hnode_new;
-  in.T = f->T; in.T_old = f->T_old;
-  in.T_new = nullptr;
-  in.tstride = f->tracer_stride ? f->tracer_stride : int64_t(P->N) * P->L;
-  in.tg = 0;
-  in.wtg = ntr;
-  in.Z3d = f->Z3d; in.zbar3 = f->zbar3; in.w_i = nullptr;
-  in.ws = P->ws;
-  in.dt = dt;
-  in.ntr = ntr;
+  A.in = make_inst(P, f, dt, ntr, tape ? tape->ws[size_t(slot)] : P->ws);
+  A.in.T_new = nullptr;
   A.a = P->aws;
   A.gTn = gT_new;
   A.gT = g->gT; A.gTo = g->gT_old; A.guv = g->guv; A.gw = g->gw_e;
-  // forward recomputation: every stage except the final update (T_new is not needed)
-  LaunchDims d{};
-  d.max_iface = P->hm.n_iface; d.max_layer = P->hm.n_layer; d.max_edge = P->hm.n_edge;
-  d.max_elem = P->hm.n_elem; d.max_dense = int64_t(P->N) * P->L; d.max_nodes = P->N;
-  d.ntr = ntr; d.chunk = 0; d.per_thread = 8; d.any_wi = false; d.copy_dry = false;
-  d.fused = false;   // the reverse kernels read every stage's intermediates
-  int st = launch_forward_stages(in, d, s, /*through_factors=*/true);
-  if (st) return restore(st);
+  A.acc = accumulate;
+  if (!tape) {   // forward recomputation: every stage except the final update
+    LaunchDims d = unfused_dims(P, ntr);
+    d.copy_dry = false;
+    st = launch_forward_stages(A.in, d, s, /*through_factors=*/true);
+    if (st) return st;
+  }
   auto grid = [](int64_t lanes, int b) {
     return dim3(unsigned(std::max<int64_t>(1, (lanes + b - 1) / b)));
   };
   const DevMesh& hm = P->hm;
   r_seed<<<grid(hm.n_layer, B), B, 0, s>>>(A);
   r_factors<<<grid(hm.n_layer, B), B, 0, s>>>(A);
-  r_ratio<<<grid(hm.n_layer, B), B, 0, s>>>(A);
-  r_window<<<grid(hm.n_layer, B), B, 0, s>>>(A);
+  r_ratio_window<<<dim3(unsigned(std::max<int64_t>(1, (hm.n_layer + B - 3) / (B - 2)))), B, 0, s>>>(A);
   r_cluster<<<grid(hm.n_elem, B), B, 0, s>>>(A);
-  r_bounds<<<grid(hm.n_layer, B), B, 0, s>>>(A);
-  r_lo<<<grid(hm.n_layer, B), B, 0, s>>>(A);
+  r_bounds_lo<<<grid(hm.n_layer, B), B, 0, s>>>(A);
   r_edge<<<grid(hm.n_edge, B), B, 0, s>>>(A);
-  r_gnode<<<grid(hm.n_layer, B), B, 0, s>>>(A);
+  r_gnode_vert<<<grid(hm.n_layer, B), B, 0, s>>>(A);
   r_tr<<<grid(hm.n_elem, B), B, 0, s>>>(A);
-  r_grad_t<<<grid(hm.n_layer, B), B, 0, s>>>(A);
-  r_vert_a<<<grid(hm.n_layer, B), B, 0, s>>>(A);
-  r_vert_b<<<grid(hm.n_layer, B), B, 0, s>>>(A);
   r_final<<<grid(int64_t(P->N) * P->L, B), B, 0, s>>>(A);
   r_uv<<<grid(int64_t(P->E) * P->L, B), B, 0, s>>>(A);
-  r_wsum<<<grid(int64_t(P->N) * P->L, B), B, 0, s>>>(A);
   const cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return restore(cuda_error(e, "adjoint kernel launch"));
-  return restore(FCT_OK);
+  if (e != cudaSuccess) return cuda_error(e, "adjoint kernel launch");
+  return FCT_OK;
+}
+
+int fct_adjoint(FctPlan* P, const FctFields* f, const double* gT_new, double dt, int ntr,
+                const FctGrads* g, fct_stream_t stream) {
+  return fct_adjoint_ex(P, f, gT_new, dt, ntr, g, nullptr, 0, 0, stream);
 }
 
 int fct_compute_w_adjoint(FctPlan* P, const double* gw, const double* helem, double* guv,
@@ -890,16 +1030,13 @@ int fct_compute_w_adjoint(FctPlan* P, const double* gw, const double* helem, dou
   if (!P || !gw || !helem || !guv) return set_error(FCT_ERR_INVALID, "NULL argument");
   if (P->adj_tracers < 1)
     return set_error(FCT_ERR_CAPACITY, "call fct_plan_reserve_adjoint first");
-  int prev = -1;
-  cudaGetDevice(&prev);
-  if (prev != P->device) cudaSetDevice(P->device);
+  DeviceGuard guard(P->device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   double* gdiv = P->aws.gdiv;   // scratch: one node field
   r_w_div<<<unsigned((P->N + 127) / 128), 128, 0, s>>>(P->d_mesh, gw, gdiv);
   const int64_t EL = int64_t(P->E) * P->L;
   r_w_uv<<<unsigned((EL + B - 1) / B), B, 0, s>>>(P->d_mesh, gdiv, helem, guv, accumulate);
   const cudaError_t e = cudaGetLastError();
-  if (prev >= 0 && prev != P->device) cudaSetDevice(prev);
   return e == cudaSuccess ? FCT_OK : cuda_error(e, "compute_w adjoint launch");
 }
 

@@ -455,10 +455,7 @@ __device__ __forceinline__ void body_edge_adf(const Inst& in, int64_t i, int t0,
   const uint32_t lane = ld(m.edge_lanes + i);
   const int e = lane_ent(lane), k = lane_lev(lane), L = m.L;
   const int n1 = ld(m.edges + 2 * e), n2 = ld(m.edges + 2 * e + 1);
-  const int up = ld(m.eupdn + 2 * e), dn = ld(m.eupdn + 2 * e + 1);
-  const int kmin = max(ld(m.ulmax + n1), ld(m.ulmax + n2)) - 1;
-  const int kmax = min(ld(m.nlmin + n1), ld(m.nlmin + n2)) - 1;
-  const bool use_tri = (up >= 0) && (dn >= 0) && k >= kmin && k < kmax;
+  const bool use_tri = in_range(k, unsigned(ld(m.etr + e)));
   const double vf = ld(in.ws.vflux + int64_t(e) * L + k);
   const double avf = fabs(vf);
   const double c1 = ld(m.ecoef + 2 * e), c2 = ld(m.ecoef + 2 * e + 1);
@@ -472,6 +469,7 @@ __device__ __forceinline__ void body_edge_adf(const Inst& in, int64_t i, int t0,
   ldn<NTR, IL>(in.T_old, q2, t0, ts, tg, O2);
   if (use_tri) {
     // both cells are wet at k here (k is above every adjacent cell's bottom)
+    const int up = ld(m.eupdn + 2 * e), dn = ld(m.eupdn + 2 * e + 1);
     if constexpr (FUSED) {
       cell_grad<NTR, IL>(in, up, k, t0, g0, g2);
       cell_grad<NTR, IL>(in, dn, k, t0, g1, g3);

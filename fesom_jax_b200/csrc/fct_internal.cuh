@@ -65,6 +65,10 @@ struct DevMesh {
   const int* eud_idx;    //   entry = 2*edge + slot (edge_up_dn_tri[edge, slot] == element)
   const int* ekmin;      // [Ed] first level of the edge's lanes (union of its cells' layers)
   const int* ekmax;      // [Ed] one past the last such level
+  const int* etr;        // [Ed] levels where MFCT uses the up/down cells' gradients
+                         //   (fill_up_dn_grad, tracer_adv.py:344-368), packed
+                         //   kmin | kmax << 8 and clipped to [ekmin, ekmax); empty
+                         //   when a cell is missing
   // packed CSR slots for the fused stage kernels (one 16-byte load per neighbour)
   const int4* ne4;       // per node->edge slot: {2*edge + second, other node,
                          //   ekmin | ekmax << 8, cell layer ranges (see pack_tri)}
@@ -130,16 +134,24 @@ struct Inst {
 // Reverse-pass intermediates of one instance (tracer-major, dense [entity, L]).
 struct AdjWorkspace {
   // node [N, L] per tracer
-  double *gdel, *gLOd, *gTd, *gpf, *gmf, *gtmax, *gtmin, *gplus, *gminus, *gLOl;
-  double *gtvmax, *gtvmin, *gLOb, *gTb, *gdiv, *ggnx, *ggny, *gTp, *gTtr, *gTv, *gAv, *gw;
+  double* ghsc;               // cotangent of the node's flux divergence: gdel * dt / areasvol
+  double *gpf, *gmf;          // limiter factors
+  double *gplus, *gminus;     // limiter sums
+  double* gLOl;               // LO through the limiter window (-(gtmax + gtmin))
+  double *gqx, *gqn;          // cluster bounds divided by their tie counts (one cell's share)
+  double *gdiv, *gTp;         // LO's divergence; T through the seed, LO and the bounds
+  double *ggnx, *ggny;        // node-average gradients
+  double *gfv, *gw;           // vertical LO flux, w_e (per tracer)
+  double *gz0, *gzm1, *gzm2, *gzp1;  // interface j's QR4C flux into ttfAB at j, j-1, j-2, j+1
   // edge [Ed, L] per tracer: cotangents of the edge's HO flux, LO flux and volume flux
   // (the consumers re-derive the per-end terms from them)
   double *gHO, *gfl, *gvf;
-  // element [E, L] per tracer
-  double *gamax, *gamin, *gtrx, *gtry;
+  // element [E, L] per tracer: the element bounds' shares (divided by the vertex tie
+  // counts) and the element gradients
+  double *gax, *gan, *gtrx, *gtry;
   int64_t sN, sE, sEd;
 };
-constexpr int kAdjNodeFields = 22, kAdjEdgeFields = 3, kAdjElemFields = 4;
+constexpr int kAdjNodeFields = 18, kAdjEdgeFields = 3, kAdjElemFields = 4;
 
 }  // namespace fct
 

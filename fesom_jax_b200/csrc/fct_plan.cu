@@ -257,6 +257,19 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
     ekmin[e] = std::max(lo, 0);
     ekmax[e] = std::min(hi, L);
   }
+  // levels where MFCT takes the up/down cells' gradients (tracer_adv.py:344-368): both
+  // cells present and k in [max(ulevels_nod2D_max) - 1, min(nlevels_nod2D_min) - 1) of
+  // the two nodes, clipped to the edge's own levels
+  std::vector<int> etr(Ed, 0);
+  for (int e = 0; e < Ed; ++e) {
+    const int n1 = d->edges[2 * e], n2 = d->edges[2 * e + 1];
+    if (d->edge_up_dn_tri[2 * e] < 0 || d->edge_up_dn_tri[2 * e + 1] < 0) continue;
+    const int lo = std::max({d->ulevels_nod2D_max[n1] - 1, d->ulevels_nod2D_max[n2] - 1,
+                             ekmin[e]});
+    const int hi = std::min({d->nlevels_nod2D_min[n1] - 1, d->nlevels_nod2D_min[n2] - 1,
+                             ekmax[e]});
+    if (hi > lo) etr[e] = lo | (hi << 8);
+  }
   // packed slots for the fused kernels
   std::vector<int4> ne4(2 * size_t(Ed));
   for (int n = 0; n < N; ++n)
@@ -317,6 +330,7 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   size_t o_cross = b.add(d->edge_cross_dxdy, 4 * size_t(Ed));
   size_t o_ecoef = b.add(ecoef.data(), ecoef.size());
   size_t o_ekmin = b.add(ekmin.data(), Ed), o_ekmax = b.add(ekmax.data(), Ed);
+  size_t o_etr = b.add(etr.data(), Ed);
   size_t o_eedge = b.add(eedge.data(), eedge.size());
   size_t o_eudoff = b.add(eud_off.data(), eud_off.size());
   size_t o_eudidx = b.add(eud_idx.data(), std::max<size_t>(eud_idx.size(), 1));
@@ -358,6 +372,7 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   m.eud_off = (const int*)(base + o_eudoff);
   m.eud_idx = (const int*)(base + o_eudidx);
   m.ekmax = (const int*)(base + o_ekmax);
+  m.etr = (const int*)(base + o_etr);
   m.ne4 = (const int4*)(base + o_ne4);
   m.nel4 = (const int4*)(base + o_nel4);
   m.nelr = (const int*)(base + o_nelr);

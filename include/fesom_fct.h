@@ -179,6 +179,35 @@ int fct_plan_reserve_adjoint(FctPlan* plan, int max_tracers);
  * treated as constants. */
 int fct_adjoint(FctPlan* plan, const FctFields* fields, const double* gT_new, double dt,
                 int ntr, const FctGrads* grads, fct_stream_t stream);
+
+/* Forward tape: the intermediates of up to ``steps`` recorded FCT steps (one full stage
+ * workspace per step, fct_tape_bytes), so that the reverse pass of a recorded step skips
+ * the recomputation. The tape keeps intermediates only; the step's inputs (fields) must
+ * still be passed to fct_adjoint_ex unchanged. The reference saves its residuals the
+ * same way under jax.grad (fesom_jax/integrate.py:43-169). */
+typedef struct FctTape FctTape;
+int fct_tape_bytes(const FctPlan* plan, int ntr, int steps, int64_t* out);
+/* Creates a tape in ``mem`` (device memory of ``bytes`` >= fct_tape_bytes, 256-byte
+ * aligned, owned by the caller and kept alive until fct_tape_destroy), or allocates it when
+ * ``mem`` is NULL. Also reserves the plan's reverse-pass workspace for ``ntr`` tracers. */
+int fct_tape_create(FctPlan* plan, int ntr, int steps, void* mem, int64_t bytes,
+                    FctTape** out);
+int fct_tape_destroy(FctTape* tape);
+/* fct_forward that also records the step's intermediates in tape slot ``slot``
+ * (T_new is bit-identical to fct_forward's). w_i is not supported (not differentiated). */
+int fct_forward_taped(FctPlan* plan, const FctFields* fields, double dt, int ntr,
+                      FctTape* tape, int slot, fct_stream_t stream);
+/* Accumulate bits of fct_adjoint_ex: add into the output instead of overwriting it. */
+#define FCT_ACC_T 1
+#define FCT_ACC_T_OLD 2
+#define FCT_ACC_UV 4
+#define FCT_ACC_W 8
+/* fct_adjoint with options: ``tape`` (NULL: recompute the step; else the step recorded
+ * in ``slot`` with the same fields and dt) and ``accumulate`` (FCT_ACC_* bits). The
+ * cotangents are bit-identical to fct_adjoint's (plus the accumulated contents). */
+int fct_adjoint_ex(FctPlan* plan, const FctFields* fields, const double* gT_new, double dt,
+                   int ntr, const FctGrads* grads, const FctTape* tape, int slot,
+                   int accumulate, fct_stream_t stream);
 /* Vector-Jacobian product of fct_compute_w (fesom_jax/ale.py:309-365) w.r.t. uv:
  * guv (+)= J^T gw, [elem2D,nl,2]; ``accumulate`` = 0 overwrites, 1 adds. */
 int fct_compute_w_adjoint(FctPlan* plan, const double* gw, const double* helem,

@@ -127,3 +127,74 @@ def test_autograd_function_matches_vjp(torch, pi):
     from fesom_jax_b200.adjoint import compute_w_vjp
     guv_total = compute_w_vjp(pi, gw, helem, guv.clone())
     assert torch.allclose(uv.grad, guv_total, rtol=1e-12, atol=0)
+
+
+def test_tape_equals_recompute(torch, pi):
+    """A taped step's forward equals fct_forward and its adjoint equals the recomputing
+    adjoint, bit for bit; so does the K-step chain under both checkpoint modes."""
+    from fesom_jax_b200.adjoint import Tape, advect_one_fct_vjp, chain_loss_and_grad
+    from fesom_jax_b200.tracer_adv import get_plan
+    f = I.make_fields(pi, seed=5, ab2=True, kind="white", sigma=0.02, n_passive=1)
+    args = [_d(torch, x) for x in (f.uv, f.w_e, f.helem, f.hnode, f.hnode_new)]
+    T, To = _d(torch, f.tracers), _d(torch, f.tracers_old)
+    gTn = _d(torch, np.random.default_rng(3).normal(size=T.shape))
+    with Tape(pi, steps=2, ntr=3) as tape:
+        Tn = tape.forward(1, *args, T, To, DT)
+        assert torch.equal(Tn, get_plan(pi, 0).forward(*args, T, To, DT))
+        taped = advect_one_fct_vjp(pi, *args, T, To, gTn, dt=DT, tape=tape, slot=1)
+        again = advect_one_fct_vjp(pi, *args, T, To, gTn, dt=DT, tape=tape, slot=1)
+    plain = advect_one_fct_vjp(pi, *args, T, To, gTn, dt=DT)
+    for a, b, c in zip(taped, plain, again):
+        assert torch.equal(a, b) and torch.equal(a, c)
+    target = torch.from_numpy(np.random.default_rng(8).normal(15.0, 3.0, pi.nod2D))
+    c = [_d(torch, x) for x in (f.helem, f.hnode, f.hnode_new)]
+    T0, To0, uv = T[0].contiguous(), To[0].contiguous(), args[0]
+    r_tape = chain_loss_and_grad(pi, T0, uv, *c, target, 4, dt=DT, T_old0=To0,
+                                 checkpoint="tape")
+    r_rc = chain_loss_and_grad(pi, T0, uv, *c, target, 4, dt=DT, T_old0=To0,
+                               checkpoint="recompute")
+    assert r_tape[0] == r_rc[0]
+    assert torch.equal(r_tape[1], r_rc[1]) and torch.equal(r_tape[2], r_rc[2])
+
+
+def test_adjoint_accumulate_bits(torch, pi):
+    """fct_adjoint_ex's accumulate bits add the cotangents into the outputs' contents."""
+    from fesom_jax_b200.adjoint import (ACC_T, ACC_T_OLD, ACC_UV, ACC_W, _adjoint, _fields,
+                                        advect_one_fct_vjp)
+    from fesom_jax_b200.tracer_adv import get_plan
+    f = I.make_fields(pi, seed=6, ab2=True)
+    args = [_d(torch, x) for x in (f.uv, f.w_e, f.helem, f.hnode, f.hnode_new)]
+    T, To = _d(torch, f.tracers[0]), _d(torch, f.tracers_old[0])
+    gTn = _d(torch, np.random.default_rng(4).normal(size=T.shape))
+    ref = advect_one_fct_vjp(pi, *args, T, To, gTn, dt=DT)
+    rng = np.random.default_rng(5)
+    base = [_d(torch, rng.normal(size=x.shape)) for x in ref]
+    plan = get_plan(pi, 0)
+    for acc in (ACC_T | ACC_UV | ACC_W, ACC_T_OLD, ACC_T | ACC_T_OLD | ACC_UV | ACC_W):
+        outs = [b.clone() for b in base]
+        _adjoint(plan, _fields(pi, *args, T, To), gTn, DT, 1, *outs, None, 0, acc, T.device)
+        for bit, o, b, r in zip((ACC_T, ACC_T_OLD, ACC_UV, ACC_W), outs, base, ref):
+            assert torch.equal(o, b + r if acc & bit else r), (acc, bit)
+    with pytest.raises(RuntimeError, match="accumulate"):
+        _adjoint(plan, _fields(pi, *args, T, To), gTn, DT, 1, *[b.clone() for b in base],
+                 None, 0, 16, T.device)
+
+
+def test_tape_rejects_misuse(torch, pi):
+    """Unrecorded slots, another dt, slots out of range and too many tracers are errors."""
+    from fesom_jax_b200.adjoint import Tape, advect_one_fct_vjp
+    f = I.make_fields(pi, seed=7, ab2=True)
+    args = [_d(torch, x) for x in (f.uv, f.w_e, f.helem, f.hnode, f.hnode_new)]
+    T, To = _d(torch, f.tracers[0]), _d(torch, f.tracers_old[0])
+    gTn = torch.ones_like(T)
+    with Tape(pi, steps=2) as tape:
+        with pytest.raises(RuntimeError, match="no recorded step"):
+            advect_one_fct_vjp(pi, *args, T, To, gTn, dt=DT, tape=tape, slot=0)
+        tape.forward(0, *args, T, To, DT)
+        with pytest.raises(RuntimeError, match="dt differs"):
+            advect_one_fct_vjp(pi, *args, T, To, gTn, dt=DT / 2, tape=tape, slot=0)
+        with pytest.raises(RuntimeError, match="slot 2 outside"):
+            tape.forward(2, *args, T, To, DT)
+        T2, To2 = torch.stack([T, T]), torch.stack([To, To])
+        with pytest.raises(RuntimeError, match="outside the tape"):
+            tape.forward(1, *args, T2, To2, DT)
