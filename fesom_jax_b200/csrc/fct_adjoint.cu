@@ -95,23 +95,44 @@ __device__ __forceinline__ double gvl_at(const DevMesh& m, const double* ghsc, i
 }
 
 // ------------------------------------------------------------------ r_seed
-// T_new = T + d / hnn (d = del + T (hn - hnn)); del holds the flux divergence times
-// dt / areasvol. Stores the cotangent of a node's flux divergence, gdel * dt / sa.
+// Every node level. Wet layers: T_new = T + d / hnn (d = del + T (hn - hnn)) and del holds
+// the flux divergence times dt / areasvol; stores the cotangent of a node's flux
+// divergence, gdel * dt / sa. Dry levels keep T (T_new = T, ale_reconstruct), so their
+// outputs are final here, except dT at the level above a cavity's first layer, which the
+// upwind flux of interface nzmin also reaches (r_final writes it); gw_e is zero there.
 __global__ void __launch_bounds__(B) r_seed(Adj A) {
   const Inst& in = A.in;
   const DevMesh& m = *in.m;
   const int64_t i = lane_index();
-  if (i >= m.n_layer) return;
-  const uint32_t lane = ld(m.layer_lanes + i);
-  const int64_t qn = int64_t(lane_ent(lane)) * m.L + lane_lev(lane);
-  const double hnn = ld(in.hnode_new + qn), av = ld(m.areasvol + qn);
-  const double sa = av > 0.0 ? av : 1.0;
-  for (int t = 0; t < in.ntr; ++t) {
-    const double g = ld(A.gTn + t * in.tstride + qn);
-    double gdel = 0.0;
-    if (hnn > 0.0) gdel = g / hnn;
-    A.a.ghsc[t * A.a.sN + qn] = gdel * in.dt / sa;
+  const int L = m.L;
+  if (i >= int64_t(m.N) * L) return;
+  const int n = int(i / L), k = int(i - int64_t(n) * L);
+  const int nzmin = ld(m.nzmin + n), nzmax = ld(m.nzmax + n);
+  if (k >= nzmin && k < nzmax) {
+    const double hnn = ld(in.hnode_new + i), av = ld(m.areasvol + i);
+    const double sa = av > 0.0 ? av : 1.0;
+    for (int t = 0; t < in.ntr; ++t) {
+      const double g = ld(A.gTn + t * in.tstride + i);
+      double gdel = 0.0;
+      if (hnn > 0.0) gdel = g / hnn;
+      A.a.ghsc[t * A.a.sN + i] = gdel * in.dt / sa;
+    }
+    return;
   }
+  const bool above_cavity = k + 1 == nzmin && nzmin < nzmax;
+  const double gA = 0.0;
+  for (int t = 0; t < in.ntr; ++t) {
+    const int64_t oT = t * in.tstride + i;
+    if (!above_cavity) {
+      const double vT = (ld(A.gTn + oT) + 0.0) + kAbNew * gA;
+      A.gT[oT] = (A.acc & kAccT) ? A.gT[oT] + vT : vT;
+    }
+    const double vTo = kAbOld * gA;
+    A.gTo[oT] = (A.acc & kAccTo) ? A.gTo[oT] + vTo : vTo;
+  }
+  double g = 0.0;   // dL/dw_e summed over tracers (the workspace's zeros at dry levels)
+  for (int t = 0; t < in.ntr; ++t) g += A.a.gw[t * A.a.sN + i];
+  A.gw[i] = (A.acc & kAccW) ? A.gw[i] + g : g;
 }
 
 // --------------------------------------------- r_factors: cotangents of pf, mf
@@ -599,6 +620,7 @@ __global__ void __launch_bounds__(B) r_tr(Adj A) {
   for (int t = 0; t < in.ntr; ++t) {
     const int64_t oa = t * A.a.sN;
     double gx = 0.0, gy = 0.0;
+#pragma unroll 2
     for (int j = u0; j < u1; ++j) {   // edges using el as up (slot 0) or down (1) cell
       const int idx = ld(m.eud_idx + j), e = idx >> 1;
       const bool on = in_range(k, unsigned(ld(m.etr + e)));
@@ -616,86 +638,81 @@ __global__ void __launch_bounds__(B) r_tr(Adj A) {
   }
 }
 
-// --------------- r_final: dT and dT_old at every node level (tracer_ab: ttfAB = -0.6 T_old
-// + 1.6 T). Wet layers gather: the seed/LO/bounds terms (gTp); the element gradients on T
-// over the node's cells (tracer_gradient_elements transposed); the vertical upwind flux of
+// --------------- r_final: dT and dT_old at every wet layer (tracer_ab: ttfAB = -0.6 T_old
+// + 1.6 T), gathering: the seed/LO/bounds terms (gTp); the element gradients on T over
+// the node's cells (tracer_gradient_elements transposed); the vertical upwind flux of
 // interfaces k and k+1 on T, and the QR4C fluxes of interfaces k-1 .. k+2 on ttfAB in
-// ascending interface order; the edge terms in ascending edge id. Dry levels keep T
-// (T_new = T there), except level nzmin - 1 above a cavity's first layer, which the upwind
-// flux of interface nzmin reaches. Also sums gw_e over the tracers.
+// ascending interface order; the edge terms in ascending edge id. Also sums gw_e over the
+// tracers, and writes dT at the dry level above a cavity's first layer (only the
+// (w - |w|) upwind term of interface nzmin reaches it; r_seed wrote the other dry levels).
 __global__ void __launch_bounds__(B) r_final(Adj A) {
   const Inst& in = A.in;
   const DevMesh& m = *in.m;
-  const int64_t i = lane_index();
-  const int64_t NL = int64_t(m.N) * m.L;
-  if (i >= NL) return;
-  const int L = m.L;
-  const int n = int(i / L), k = int(i - int64_t(n) * L);
+  const int64_t li = lane_index();
+  if (li >= m.n_layer) return;
+  const uint32_t lane = ld(m.layer_lanes + li);
+  const int n = lane_ent(lane), k = lane_lev(lane), L = m.L;
+  const int64_t i = int64_t(n) * L + k;
   const int nzmin = ld(m.nzmin + n), nzmax = ld(m.nzmax + n);
-  const bool layer = k >= nzmin && k < nzmax;
   const int e0 = ld(m.ne_off + n), e1 = ld(m.ne_off + n + 1);
   const int c0 = ld(m.nel_off + n), c1 = ld(m.nel_off + n + 1);
   for (int t = 0; t < in.ntr; ++t) {
     const int64_t oa = t * A.a.sN;
     const double* gfv = A.a.gfv + oa;
-    double gT, gA = 0.0;
-    if (!layer) {
-      double gv = 0.0;
-      if (k + 1 == nzmin && nzmin < nzmax) {   // above a cavity: the (w - |w|) term of
-                                               // interface nzmin only
-        const double w = ld(in.w_e + i + 1), area = ld(m.area + i + 1);
-        double g = 0.0;
-        g += -0.5 * (w - fabs(w)) * area * gfv[i + 1];
-        gv = g;
-      }
-      gT = ld(A.gTn + t * in.tstride + i) + gv;   // dry levels: T_new = T
-    } else {
-      // vertical upwind fluxes of interfaces k and k+1
-      double gTv = 0.0;
-      {
-        const double w = ld(in.w_e + i), area = ld(m.area + i);
-        gTv += -0.5 * (w + fabs(w)) * area * gfv[i];
-        if (k == 0) gTv += -0.5 * (w - fabs(w)) * area * gfv[i];
-      }
-      if (k + 1 < nzmax) {
-        const double w = ld(in.w_e + i + 1), area = ld(m.area + i + 1);
-        gTv += -0.5 * (w - fabs(w)) * area * gfv[i + 1];
-      }
-      // QR4C terms of interfaces k-1 .. k+2 in ascending order (a term that does not
-      // reach k is +0.0; gA starts at +0.0, so adding it changes no bit)
-      if (k - 1 >= nzmin) gA += A.a.gzp1[oa + i - 1];
-      gA += A.a.gz0[oa + i];
-      if (k + 1 < nzmax) gA += A.a.gzm1[oa + i + 1];
-      if (k + 2 < nzmax) gA += A.a.gzm2[oa + i + 2];
-      // element gradients on T: the node's cells in nod_in_elem2D order
-      double gTtr = 0.0;
+    if (k == nzmin && k > 0) {   // the dry level above a cavity
+      const double w = ld(in.w_e + i), area = ld(m.area + i);
+      double g = 0.0;
+      g += -0.5 * (w - fabs(w)) * area * gfv[i];
+      const int64_t oT = t * in.tstride + i - 1;
+      const double vT = (ld(A.gTn + oT) + g) + kAbNew * 0.0;
+      A.gT[oT] = (A.acc & kAccT) ? A.gT[oT] + vT : vT;
+    }
+    double gA = 0.0;
+    // vertical upwind fluxes of interfaces k and k+1
+    double gTv = 0.0;
+    {
+      const double w = ld(in.w_e + i), area = ld(m.area + i);
+      gTv += -0.5 * (w + fabs(w)) * area * gfv[i];
+      if (k == 0) gTv += -0.5 * (w - fabs(w)) * area * gfv[i];
+    }
+    if (k + 1 < nzmax) {
+      const double w = ld(in.w_e + i + 1), area = ld(m.area + i + 1);
+      gTv += -0.5 * (w - fabs(w)) * area * gfv[i + 1];
+    }
+    // QR4C terms of interfaces k-1 .. k+2 in ascending order (a term that does not
+    // reach k is +0.0; gA starts at +0.0, so adding it changes no bit)
+    if (k - 1 >= nzmin) gA += A.a.gzp1[oa + i - 1];
+    gA += A.a.gz0[oa + i];
+    if (k + 1 < nzmax) gA += A.a.gzm1[oa + i + 1];
+    if (k + 2 < nzmax) gA += A.a.gzm2[oa + i + 2];
+    // element gradients on T: the node's cells in nod_in_elem2D order
+    double gTtr = 0.0;
 #pragma unroll 2
-      for (int j = c0; j < c1; ++j) {
-        const unsigned r = unsigned(ld(m.nelr + j));
-        const bool on = in_range(k, r);
-        const int el = ld(m.nel_idx + j), iv = int((r >> 16) & 3u);
-        const int64_t qe = t * A.a.sE + int64_t(el) * L + k;
-        const double v = ld(m.gsca + 6 * el + iv) * A.a.gtrx[qe] +
-                         ld(m.gsca + 6 * el + 3 + iv) * A.a.gtry[qe];
-        gTtr = on ? gTtr + v : gTtr;
-      }
-      gT = A.a.gTp[oa + i] + gTtr + gTv;
+    for (int j = c0; j < c1; ++j) {
+      const unsigned r = unsigned(ld(m.nelr + j));
+      const bool on = in_range(k, r);
+      const int el = ld(m.nel_idx + j), iv = int((r >> 16) & 3u);
+      const int64_t qe = t * A.a.sE + int64_t(el) * L + k;
+      const double v = ld(m.gsca + 6 * el + iv) * A.a.gtrx[qe] +
+                       ld(m.gsca + 6 * el + 3 + iv) * A.a.gtry[qe];
+      gTtr = on ? gTtr + v : gTtr;
+    }
+    double gT = A.a.gTp[oa + i] + gTtr + gTv;
 #pragma unroll 2
-      for (int j = e0; j < e1; ++j) {
-        const int4 sl = __ldg(m.ne4 + j);
-        const bool on = in_range(k, unsigned(sl.z));
-        const EdgeTerms et = edge_terms(A, t, sl.x >> 1, k);
-        const bool second = sl.x & 1;
-        gT = on ? gT + (second ? et.gT2 : et.gT1) : gT;
-        gA = on ? gA + (second ? et.gA2 : et.gA1) : gA;
-      }
+    for (int j = e0; j < e1; ++j) {
+      const int4 sl = __ldg(m.ne4 + j);
+      const bool on = in_range(k, unsigned(sl.z));
+      const EdgeTerms et = edge_terms(A, t, sl.x >> 1, k);
+      const bool second = sl.x & 1;
+      gT = on ? gT + (second ? et.gT2 : et.gT1) : gT;
+      gA = on ? gA + (second ? et.gA2 : et.gA1) : gA;
     }
     const int64_t oT = t * in.tstride + i;
     const double vT = gT + kAbNew * gA, vTo = kAbOld * gA;
     A.gT[oT] = (A.acc & kAccT) ? A.gT[oT] + vT : vT;
     A.gTo[oT] = (A.acc & kAccTo) ? A.gTo[oT] + vTo : vTo;
   }
-  double g = 0.0;   // dL/dw_e summed over tracers (dry levels hold the workspace's zeros)
+  double g = 0.0;   // dL/dw_e summed over tracers
   for (int t = 0; t < in.ntr; ++t) g += A.a.gw[t * A.a.sN + i];
   A.gw[i] = (A.acc & kAccW) ? A.gw[i] + g : g;
 }
@@ -798,6 +815,11 @@ __global__ void __launch_bounds__(B) r_w_uv(const DevMesh* __restrict__ mp,
 int reserve_adj_ws(FctPlan* P, int max_tracers) {
   if (max_tracers <= P->adj_tracers) return FCT_OK;
   FCT_CUDA(cudaSetDevice(P->device));
+  if (!P->adj_side) {
+    FCT_CUDA(cudaStreamCreateWithFlags(&P->adj_side, cudaStreamNonBlocking));
+    FCT_CUDA(cudaEventCreateWithFlags(&P->adj_fork, cudaEventDisableTiming));
+    FCT_CUDA(cudaEventCreateWithFlags(&P->adj_join, cudaEventDisableTiming));
+  }
   const int64_t sN = int64_t(P->N) * P->L, sE = int64_t(P->E) * P->L, sEd = int64_t(P->Ed) * P->L;
   const int64_t nd = int64_t(max_tracers) * (kAdjNodeFields * sN + kAdjEdgeFields * sEd +
                                              kAdjElemFields * sE);
@@ -1005,16 +1027,23 @@ int fct_adjoint_ex(FctPlan* P, const FctFields* f, const double* gT_new, double 
     return dim3(unsigned(std::max<int64_t>(1, (lanes + b - 1) / b)));
   };
   const DevMesh& hm = P->hm;
-  r_seed<<<grid(hm.n_layer, B), B, 0, s>>>(A);
+  const int64_t NL = int64_t(P->N) * P->L;
+  r_seed<<<grid(NL, B), B, 0, s>>>(A);
   r_factors<<<grid(hm.n_layer, B), B, 0, s>>>(A);
   r_ratio_window<<<dim3(unsigned(std::max<int64_t>(1, (hm.n_layer + B - 3) / (B - 2)))), B, 0, s>>>(A);
   r_cluster<<<grid(hm.n_elem, B), B, 0, s>>>(A);
   r_bounds_lo<<<grid(hm.n_layer, B), B, 0, s>>>(A);
   r_edge<<<grid(hm.n_edge, B), B, 0, s>>>(A);
+  // r_uv needs only r_edge's volume-flux cotangents: it runs on the plan's side stream
+  // beside the node/element chain (both are latency-bound gathers)
+  FCT_CUDA(cudaEventRecord(P->adj_fork, s));
+  FCT_CUDA(cudaStreamWaitEvent(P->adj_side, P->adj_fork, 0));
+  r_uv<<<grid(int64_t(P->E) * P->L, B), B, 0, P->adj_side>>>(A);
+  FCT_CUDA(cudaEventRecord(P->adj_join, P->adj_side));
   r_gnode_vert<<<grid(hm.n_layer, B), B, 0, s>>>(A);
   r_tr<<<grid(hm.n_elem, B), B, 0, s>>>(A);
-  r_final<<<grid(int64_t(P->N) * P->L, B), B, 0, s>>>(A);
-  r_uv<<<grid(int64_t(P->E) * P->L, B), B, 0, s>>>(A);
+  r_final<<<grid(hm.n_layer, B), B, 0, s>>>(A);
+  FCT_CUDA(cudaStreamWaitEvent(s, P->adj_join, 0));
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_error(e, "adjoint kernel launch");
   return FCT_OK;
