@@ -16,8 +16,8 @@
 //   zalesak_limit a2 (:393-397) over a3's per-cell shares            -> r_cluster
 //   zalesak_limit a1 (:389-391), compute_fct_lo (:298-313)          -> r_bounds_lo
 //   adv_flux_hor_ho (:196-225), adv_flux_hor (:96-105), b1 edges    -> r_edge
-//   fill_up_dn_grad (:344-368) node branch; adv_flux_ver_ho
-//     (:241-295), adv_flux_ver (:108-120), b1 vertical              -> r_gnode_vert
+//   fill_up_dn_grad (:344-368) node branch                          -> r_gnode
+//   adv_flux_ver_ho (:241-295), adv_flux_ver (:108-120), b1 vertical -> r_vert
 //   fill_up_dn_grad triangle branch, _node_avg_grad (:329-341)      -> r_tr
 //   tracer_gradient_elements (:316-326), vertical fluxes on T and
 //     ttfAB, tracer_ab (:59-66), edge terms; w_e summed over tracers -> r_final
@@ -505,13 +505,41 @@ __device__ __forceinline__ void qr4c_depths(const Inst& in, const DevMesh& m, in
   }
 }
 
-// ------- r_gnode_vert: cotangent of the node-average gradient (fill_up_dn_grad's node
-// branch, gathered over the node's edges), and of the vertical fluxes at interface
-// j = k: gf of adf_v[j] (limiter application and the plus/minus sums) reaches the QR4C
-// flux (ghi = gf) and the upwind flux (gfv = -gf + gdiv terms); gw[j] is complete here
-// (only interface j feeds it), and the QR4C flux's terms for ttfAB at levels j, j-1, j-2
-// and j+1 are stored for r_final to gather.
-__global__ void __launch_bounds__(B) r_gnode_vert(Adj A) {
+// ------- r_gnode: cotangent of the node-average gradient (fill_up_dn_grad's node branch),
+// gathered over the node's edges in ascending edge id.
+__global__ void __launch_bounds__(B) r_gnode(Adj A) {
+  const Inst& in = A.in;
+  const DevMesh& m = *in.m;
+  const int64_t i = lane_index();
+  if (i >= m.n_layer) return;
+  const uint32_t lane = ld(m.layer_lanes + i);
+  const int n = lane_ent(lane), k = lane_lev(lane), L = m.L;
+  const int64_t qn = int64_t(n) * L + k;
+  const int e0 = ld(m.ne_off + n), e1 = ld(m.ne_off + n + 1);
+  for (int t = 0; t < in.ntr; ++t) {
+    const int64_t oa = t * A.a.sN;
+    double gx = 0.0, gy = 0.0;
+#pragma unroll 2
+    for (int j = e0; j < e1; ++j) {   // loads unconditional (in bounds), off edges selected away
+      const int4 sl = __ldg(m.ne4 + j);
+      const int e = sl.x >> 1;
+      const bool on = in_range(k, unsigned(sl.z)) && !in_range(k, unsigned(ld(m.etr + e)));
+      const EdgeTerms et = edge_terms(A, t, e, k);
+      const bool second = sl.x & 1;
+      gx = on ? gx + (second ? et.gg1 : et.gg0) : gx;
+      gy = on ? gy + (second ? et.gg3 : et.gg2) : gy;
+    }
+    A.a.ggnx[oa + qn] = gx;
+    A.a.ggny[oa + qn] = gy;
+  }
+}
+
+// ------- r_vert: the vertical fluxes at interface j = k: gf of adf_v[j] (limiter
+// application and the plus/minus sums) reaches the QR4C flux (ghi = gf) and the upwind
+// flux (gfv = -gf + gdiv terms); gw[j] is complete here (only interface j feeds it), and
+// the QR4C flux's terms for ttfAB at levels j, j-1, j-2 and j+1 are stored for r_final to
+// gather. Independent of the edge chain (it runs beside r_edge).
+__global__ void __launch_bounds__(B) r_vert(Adj A) {
   const Inst& in = A.in;
   const DevMesh& m = *in.m;
   const int64_t i = lane_index();
@@ -520,11 +548,10 @@ __global__ void __launch_bounds__(B) r_gnode_vert(Adj A) {
   const int n = lane_ent(lane), j = lane_lev(lane), L = m.L;
   const int nzmin = ld(m.nzmin + n), nzmax = ld(m.nzmax + n);
   const int64_t base = int64_t(n) * L, qn = base + j;
-  const int e0 = ld(m.ne_off + n), e1 = ld(m.ne_off + n + 1);
   const double w = ld(in.w_e + qn), area = ld(m.area + qn);
   const int jm = j > 0 ? j - 1 : 0;
   const Rcp r3{3.0, 1.0 / 3.0, true};
-  const bool interior = j >= nzmin + 2 && j <= nzmax - 2 && j != nzmax - 1;
+  const bool interior = j >= nzmin + 2 && j <= nzmax - 2;
   double Znz = 0.0, Zm1 = 0.0, Zm2 = 0.0, Zp1 = 0.0, zb = 0.0;
   Rcp rdc{1.0, 1.0, true}, rdu{1.0, 1.0, true}, rdd{1.0, 1.0, true};
   if (interior) {
@@ -535,21 +562,6 @@ __global__ void __launch_bounds__(B) r_gnode_vert(Adj A) {
   }
   for (int t = 0; t < in.ntr; ++t) {
     const int64_t o = t * in.ws.sN, oa = t * A.a.sN;
-    {   // node-average gradient, ascending edge id (loads unconditional, in bounds)
-      double gx = 0.0, gy = 0.0;
-#pragma unroll 2
-      for (int jj = e0; jj < e1; ++jj) {
-        const int4 sl = __ldg(m.ne4 + jj);
-        const int e = sl.x >> 1;
-        const bool on = in_range(j, unsigned(sl.z)) && !in_range(j, unsigned(ld(m.etr + e)));
-        const EdgeTerms et = edge_terms(A, t, e, j);
-        const bool second = sl.x & 1;
-        gx = on ? gx + (second ? et.gg1 : et.gg0) : gx;
-        gy = on ? gy + (second ? et.gg3 : et.gg2) : gy;
-      }
-      A.a.ggnx[oa + qn] = gx;
-      A.a.ggny[oa + qn] = gy;
-    }
     const double* T = in.T + t * in.tstride + base;
     const double* To = in.T_old + t * in.tstride + base;
     const double* pf = in.ws.pf + o + base;
@@ -616,7 +628,7 @@ __global__ void __launch_bounds__(B) r_tr(Adj A) {
                          int64_t(ld(m.enodes + 3 * el + 1)) * L + k,
                          int64_t(ld(m.enodes + 3 * el + 2)) * L + k};
   // the forward's (safe) node-average denominators of the three vertices
-  const Rcp rd[3] = {rcp(in.ws.nden[qv[0]]), rcp(in.ws.nden[qv[1]]), rcp(in.ws.nden[qv[2]])};
+  const double dd[3] = {in.ws.nden[qv[0]], in.ws.nden[qv[1]], in.ws.nden[qv[2]]};
   for (int t = 0; t < in.ntr; ++t) {
     const int64_t oa = t * A.a.sN;
     double gx = 0.0, gy = 0.0;
@@ -630,8 +642,8 @@ __global__ void __launch_bounds__(B) r_tr(Adj A) {
     }
 #pragma unroll
     for (int v = 0; v < 3; ++v) {   // gnode(n) = sum_e a_e tr_e / den(n)
-      gx += divr(A.a.ggnx[oa + qv[v]] * aw, rd[v]);
-      gy += divr(A.a.ggny[oa + qv[v]] * aw, rd[v]);
+      gx += A.a.ggnx[oa + qv[v]] * aw / dd[v];
+      gy += A.a.ggny[oa + qv[v]] * aw / dd[v];
     }
     A.a.gtrx[t * A.a.sE + int64_t(el) * L + k] = gx;
     A.a.gtry[t * A.a.sE + int64_t(el) * L + k] = gy;
@@ -817,8 +829,8 @@ int reserve_adj_ws(FctPlan* P, int max_tracers) {
   FCT_CUDA(cudaSetDevice(P->device));
   if (!P->adj_side) {
     FCT_CUDA(cudaStreamCreateWithFlags(&P->adj_side, cudaStreamNonBlocking));
-    FCT_CUDA(cudaEventCreateWithFlags(&P->adj_fork, cudaEventDisableTiming));
-    FCT_CUDA(cudaEventCreateWithFlags(&P->adj_join, cudaEventDisableTiming));
+    for (cudaEvent_t& ev : P->adj_ev)
+      FCT_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   }
   const int64_t sN = int64_t(P->N) * P->L, sE = int64_t(P->E) * P->L, sEd = int64_t(P->Ed) * P->L;
   const int64_t nd = int64_t(max_tracers) * (kAdjNodeFields * sN + kAdjEdgeFields * sEd +
@@ -1033,17 +1045,23 @@ int fct_adjoint_ex(FctPlan* P, const FctFields* f, const double* gT_new, double 
   r_ratio_window<<<dim3(unsigned(std::max<int64_t>(1, (hm.n_layer + B - 3) / (B - 2)))), B, 0, s>>>(A);
   r_cluster<<<grid(hm.n_elem, B), B, 0, s>>>(A);
   r_bounds_lo<<<grid(hm.n_layer, B), B, 0, s>>>(A);
+  // Side stream: r_vert (needs the node kernels above) beside r_edge, then r_uv (needs
+  // r_edge's volume-flux cotangents) beside r_gnode / r_tr / r_final. All of them are
+  // latency-bound gathers, so the pairs share the SMs.
+  FCT_CUDA(cudaEventRecord(P->adj_ev[0], s));
+  FCT_CUDA(cudaStreamWaitEvent(P->adj_side, P->adj_ev[0], 0));
+  r_vert<<<grid(hm.n_layer, B), B, 0, P->adj_side>>>(A);
+  FCT_CUDA(cudaEventRecord(P->adj_ev[1], P->adj_side));
   r_edge<<<grid(hm.n_edge, B), B, 0, s>>>(A);
-  // r_uv needs only r_edge's volume-flux cotangents: it runs on the plan's side stream
-  // beside the node/element chain (both are latency-bound gathers)
-  FCT_CUDA(cudaEventRecord(P->adj_fork, s));
-  FCT_CUDA(cudaStreamWaitEvent(P->adj_side, P->adj_fork, 0));
+  FCT_CUDA(cudaEventRecord(P->adj_ev[2], s));
+  FCT_CUDA(cudaStreamWaitEvent(P->adj_side, P->adj_ev[2], 0));
   r_uv<<<grid(int64_t(P->E) * P->L, B), B, 0, P->adj_side>>>(A);
-  FCT_CUDA(cudaEventRecord(P->adj_join, P->adj_side));
-  r_gnode_vert<<<grid(hm.n_layer, B), B, 0, s>>>(A);
+  FCT_CUDA(cudaEventRecord(P->adj_ev[3], P->adj_side));
+  r_gnode<<<grid(hm.n_layer, B), B, 0, s>>>(A);
   r_tr<<<grid(hm.n_elem, B), B, 0, s>>>(A);
+  FCT_CUDA(cudaStreamWaitEvent(s, P->adj_ev[1], 0));
   r_final<<<grid(hm.n_layer, B), B, 0, s>>>(A);
-  FCT_CUDA(cudaStreamWaitEvent(s, P->adj_join, 0));
+  FCT_CUDA(cudaStreamWaitEvent(s, P->adj_ev[3], 0));
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_error(e, "adjoint kernel launch");
   return FCT_OK;

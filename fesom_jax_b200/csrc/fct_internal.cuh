@@ -169,7 +169,7 @@ struct FctPlan {
   int64_t n_wet_elem_layers = 0;
   double* d_adj = nullptr;         // reverse-pass workspace
   int adj_tracers = 0;
-  cudaStream_t adj_side = nullptr;  // reverse pass: a kernel independent of the main chain
-  cudaEvent_t adj_fork = nullptr, adj_join = nullptr;
+  cudaStream_t adj_side = nullptr;  // reverse pass: kernels independent of the main chain
+  cudaEvent_t adj_ev[4] = {};       //   and the events that fork and join it
   fct::AdjWorkspace aws{};
 };

@@ -398,8 +398,8 @@ int fct_plan_destroy(FctPlan* P) {
   cudaSetDevice(P->device);
   if (P->d_adj) cudaFree(P->d_adj);
   if (P->adj_side) cudaStreamDestroy(P->adj_side);
-  if (P->adj_fork) cudaEventDestroy(P->adj_fork);
-  if (P->adj_join) cudaEventDestroy(P->adj_join);
+  for (cudaEvent_t ev : P->adj_ev)
+    if (ev) cudaEventDestroy(ev);
   if (P->d_ws) cudaFree(P->d_ws);
   if (P->d_mesh) cudaFree(P->d_mesh);
   if (P->d_static) cudaFree(P->d_static);
