@@ -435,7 +435,10 @@ def run_adjoint(args, D: Dist) -> dict:
             T, To = plan.forward(uv, w, helem, hn, hnn, T, To, dt), T
         return T
 
-    def grad(checkpoint="tape"):
+    main_mode = args.checkpoint   # the headline checkpointing; the other is timed beside it
+    other = "recompute" if main_mode == "tape" else None
+
+    def grad(checkpoint=main_mode):
         return chain_loss_and_grad(mesh, T0, uv, helem, hn, hnn, target, K, dt=dt, T_old0=To0,
                                    checkpoint=checkpoint)
 
@@ -454,11 +457,13 @@ def run_adjoint(args, D: Dist) -> dict:
     D.barrier()
     t_fwd = timed(forward, args.steps)
     t_grad = timed(grad, args.steps)
-    t_grad_rc = timed(lambda: grad("recompute"), args.steps)
+    t_grad_rc = timed(lambda: grad(other), args.steps) if other else None
     t = D.max(t_grad, dev)
     loss, gT0, guv = grad()
-    _, gT0_rc, guv_rc = grad("recompute")
-    same_bits = bool(torch.equal(gT0, gT0_rc) and torch.equal(guv, guv_rc))
+    same_bits = None
+    if other:
+        _, gT0_rc, guv_rc = grad(other)
+        same_bits = bool(torch.equal(gT0, gT0_rc) and torch.equal(guv, guv_rc))
     # central finite differences
     rng = np.random.default_rng(2024)
     lm = torch.from_numpy(mesh.node_layer_mask).to(dev)
@@ -469,16 +474,16 @@ def run_adjoint(args, D: Dist) -> dict:
         if j < 10:
             v = d(rng.normal(size=T0.shape)) * lm
             Lp = chain_loss_and_grad(mesh, T0 + eps * v, uv, helem, hn, hnn, target, K, dt=dt,
-                                     T_old0=To0)[0]
+                                     T_old0=To0, checkpoint=main_mode)[0]
             Lm = chain_loss_and_grad(mesh, T0 - eps * v, uv, helem, hn, hnn, target, K, dt=dt,
-                                     T_old0=To0)[0]
+                                     T_old0=To0, checkpoint=main_mode)[0]
             ad = float((gT0 * v).sum())
         else:
             v = d(rng.normal(size=uv.shape)) * em
             Lp = chain_loss_and_grad(mesh, T0, uv + eps * v, helem, hn, hnn, target, K, dt=dt,
-                                     T_old0=To0)[0]
+                                     T_old0=To0, checkpoint=main_mode)[0]
             Lm = chain_loss_and_grad(mesh, T0, uv - eps * v, helem, hn, hnn, target, K, dt=dt,
-                                     T_old0=To0)[0]
+                                     T_old0=To0, checkpoint=main_mode)[0]
             ad = float((guv * v).sum())
         fd = (Lp - Lm) / (2 * eps)
         rel.append(abs(fd - ad) / max(abs(ad), 1e-300))
@@ -486,18 +491,18 @@ def run_adjoint(args, D: Dist) -> dict:
     return dict(value=upd / t, t=t * args.steps, mesh=mesh, t_fwd=t_fwd, t_grad=t_grad,
                 cfg=dict(members=1, ntr=1, fct_steps=K, dt=dt),
                 adjoint=dict(forward_ms=t_fwd * 1e3, loss_and_grad_ms=t_grad * 1e3,
-                             ratio=t_grad / t_fwd, K=K, loss=loss, checkpoint="tape",
+                             ratio=t_grad / t_fwd, K=K, loss=loss, checkpoint=main_mode,
                              tape_gb=Tape.nbytes(mesh, K, 1, D.local_rank) / 1e9,
-                             recompute_loss_and_grad_ms=t_grad_rc * 1e3,
-                             recompute_ratio=t_grad_rc / t_fwd,
+                             recompute_loss_and_grad_ms=(t_grad_rc * 1e3 if other else None),
+                             recompute_ratio=(t_grad_rc / t_fwd if other else None),
                              tape_equals_recompute=same_bits,
                              fd_rel_err_max=float(max(rel)) if rel else None,
                              fd_rel_err_median=float(np.median(rel)) if rel else None,
                              fd_directions=len(rel), fd_eps=eps, max_cfl_z=float(I.max_cfl_z(
                                  mesh, f.w_e, f.hnode, dt)),
-                             how="chain_loss_and_grad (fct_forward_taped x K, "
-                                 "fct_adjoint_ex x K, fct_compute_w_adjoint) vs compute_w + "
-                                 "fct_forward x K"))
+                             how="chain_loss_and_grad (forward x K with the chosen "
+                                 "checkpointing, fct_adjoint_ex x K, fct_compute_w_adjoint) vs "
+                                 "compute_w + fct_forward x K"))
 
 
 # ---------------------------------------------------------------- serving (config 5)
@@ -633,6 +638,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fd", action="store_true", help="adjoint: skip the FD check")
+    ap.add_argument("--checkpoint", choices=["tape", "recompute"], default="tape",
+                    help="adjoint: keep every step's intermediates (tape; the per-step "
+                         "recomputation is timed beside it) or recompute them only")
     ap.add_argument("--derive-w", action="store_true",
                     help="batched/large: derive w_e = compute_w(uv) inside every step's graph")
     ap.add_argument("--vdiff", action="store_true",

@@ -50,9 +50,10 @@ def _bind(L):
     L.fct_tape_destroy.argtypes = [C.c_void_p]
     L.fct_forward_taped.argtypes = [C.c_void_p, C.POINTER(_lib.FctFields), C.c_double, C.c_int,
                                     C.c_void_p, C.c_int, C.c_void_p]
+    L.fct_tape_mark_recorded.argtypes = [C.c_void_p, C.c_int, C.c_double]
     for n in ("fct_plan_reserve_adjoint", "fct_adjoint", "fct_adjoint_ex",
               "fct_compute_w_adjoint", "fct_tape_bytes", "fct_tape_create", "fct_tape_destroy",
-              "fct_forward_taped"):
+              "fct_forward_taped", "fct_tape_mark_recorded"):
         getattr(L, n).restype = C.c_int
     L._adj_bound = True
     return L

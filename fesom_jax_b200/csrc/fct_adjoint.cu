@@ -970,6 +970,16 @@ int fct_tape_destroy(FctTape* T) {
   return FCT_OK;
 }
 
+int fct_tape_mark_recorded(FctTape* T, int slot, double dt) {
+  if (!T) return set_error(FCT_ERR_INVALID, "tape is NULL");
+  if (slot < 0 || slot >= T->steps)
+    return set_error(FCT_ERR_INVALID, "slot %d outside the tape's [0, %d)", slot, T->steps);
+  if (!(dt > 0.0)) return set_error(FCT_ERR_INVALID, "dt must be positive");
+  T->recorded[size_t(slot)] = 1;
+  T->dt[size_t(slot)] = dt;
+  return FCT_OK;
+}
+
 int fct_forward_taped(FctPlan* P, const FctFields* f, double dt, int ntr, FctTape* tape,
                       int slot, fct_stream_t stream) {
   if (!P || !f || !tape) return set_error(FCT_ERR_INVALID, "NULL argument");

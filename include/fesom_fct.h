@@ -197,6 +197,10 @@ int fct_tape_destroy(FctTape* tape);
  * (T_new is bit-identical to fct_forward's). w_i is not supported (not differentiated). */
 int fct_forward_taped(FctPlan* plan, const FctFields* fields, double dt, int ntr,
                       FctTape* tape, int slot, fct_stream_t stream);
+/* Declares that ``slot`` of a tape created over caller memory already holds a step
+ * recorded by fct_forward_taped with ``dt`` (through another tape over the same memory,
+ * e.g. in a separate forward and backward call of a stateless custom-call handler). */
+int fct_tape_mark_recorded(FctTape* tape, int slot, double dt);
 /* Accumulate bits of fct_adjoint_ex: add into the output instead of overwriting it. */
 #define FCT_ACC_T 1
 #define FCT_ACC_T_OLD 2

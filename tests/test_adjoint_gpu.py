@@ -198,3 +198,42 @@ def test_tape_rejects_misuse(torch, pi):
         T2, To2 = torch.stack([T, T]), torch.stack([To, To])
         with pytest.raises(RuntimeError, match="outside the tape"):
             tape.forward(1, *args, T2, To2, DT)
+
+
+def test_tape_reopened_over_the_same_memory(torch, pi):
+    """The stateless-handler pattern: a step recorded through one tape is read back through
+    a second tape created over the same caller memory (fct_tape_mark_recorded)."""
+    import ctypes as C
+    from fesom_jax_b200 import _lib
+    from fesom_jax_b200.adjoint import Tape, _bind, advect_one_fct_vjp
+    f = I.make_fields(pi, seed=8, ab2=True, kind="white", sigma=0.02)
+    args = [_d(torch, x) for x in (f.uv, f.w_e, f.helem, f.hnode, f.hnode_new)]
+    T, To = _d(torch, f.tracers[0]), _d(torch, f.tracers_old[0])
+    gTn = _d(torch, np.random.default_rng(9).normal(size=T.shape))
+    L = _bind(_lib.lib())
+    first = Tape(pi, steps=1)
+    first.forward(0, *args, T, To, DT)
+    mem, nb = first._mem, Tape.nbytes(pi, 1)
+    L.fct_tape_destroy(first._h)
+    first._h = C.c_void_p()
+    second = Tape.__new__(Tape)
+    second.mesh, second.steps, second.ntr, second.device = pi, 1, 1, 0
+    second.plan, second._mem = first.plan, mem
+    h = C.c_void_p()
+    _lib.check(L.fct_tape_create(second.plan.handle, 1, 1, C.c_void_p(mem.data_ptr()), nb,
+                                 C.byref(h)))
+    second._h = h
+    with pytest.raises(RuntimeError, match="no recorded step"):
+        advect_one_fct_vjp(pi, *args, T, To, gTn, dt=DT, tape=second, slot=0)
+    _lib.check(L.fct_tape_mark_recorded(h, 0, DT))
+    got = advect_one_fct_vjp(pi, *args, T, To, gTn, dt=DT, tape=second, slot=0)
+    ref = advect_one_fct_vjp(pi, *args, T, To, gTn, dt=DT)
+    for a, b in zip(got, ref):
+        assert torch.equal(a, b)
+    second.close()
+    with pytest.raises(RuntimeError, match="256-byte aligned"):
+        _lib.check(L.fct_tape_create(second.plan.handle, 1, 1, C.c_void_p(mem.data_ptr() + 8),
+                                     nb, C.byref(h)))
+    with pytest.raises(RuntimeError, match="needed"):
+        _lib.check(L.fct_tape_create(second.plan.handle, 1, 1, C.c_void_p(mem.data_ptr()),
+                                     nb - 8, C.byref(h)))
