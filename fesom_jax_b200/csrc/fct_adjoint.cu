@@ -106,7 +106,8 @@ __global__ void __launch_bounds__(B) r_seed(Adj A) {
   const int64_t i = lane_index();
   const int L = m.L;
   if (i >= int64_t(m.N) * L) return;
-  const int n = int(i / L), k = int(i - int64_t(n) * L);
+  int n, k;
+  split_dense(i, L, n, k);
   const int nzmin = ld(m.nzmin + n), nzmax = ld(m.nzmax + n);
   if (k >= nzmin && k < nzmax) {
     const double hnn = ld(in.hnode_new + i), av = ld(m.areasvol + i);
@@ -420,7 +421,7 @@ __global__ void __launch_bounds__(B, 3) r_edge(Adj A) {
     qa = int64_t(ld(m.eupdn + 2 * e)) * L + k;
     qb = int64_t(ld(m.eupdn + 2 * e + 1)) * L + k;
   }
-  const double vf = ld(in.ws.vflux + qe), s = sgn(vf);
+  const double vf = ld(in.ws.vflux + qe), avf = fabs(vf), s = sgn(vf);
   const double c1 = ld(m.ecoef + 2 * e), c2 = ld(m.ecoef + 2 * e + 1);
   const Rcp r6{6.0, 1.0 / 6.0, true};
   for (int t = 0; t < in.ntr; ++t) {
@@ -449,43 +450,23 @@ __global__ void __launch_bounds__(B, 3) r_edge(Adj A) {
     const double diff = A2 - A1;
     const double Tm1 = A1 + divr(2.0 * diff + c1 * g0 + c2 * g2, r6);
     const double Tm2 = A2 - divr(2.0 * diff + c1 * g1 + c2 * g3, r6);
-    // HO = -0.5 ((vf + |vf|) Tm1 + (vf - |vf|) Tm2); fl = -0.5 (T1 (vf + |vf|) + T2 (vf - |vf|));
-    // the per-end terms of Tm1/Tm2 and T1/T2 are re-derived by the consumers (edge_terms)
+    // HO = -0.5 ((vf + |vf|) Tm1 + (vf - |vf|) Tm2); fl = -0.5 (T1 (vf + |vf|) + T2 (vf - |vf|))
     double gvf = -0.5 * ((1.0 + s) * Tm1 + (1.0 - s) * Tm2) * gHO;
     gvf += -0.5 * (T1 * (1.0 + s) + T2 * (1.0 - s)) * gfl;
-    A.a.gHO[oe + qe] = gHO;
-    A.a.gfl[oe + qe] = gfl;
     A.a.gvf[oe + qe] = gvf;
+    // per-end terms for the node and element gathers: T1/T2 through the upwind flux;
+    // ttfAB at the ends through Tm1 = A1 + X1 / 6 and Tm2 = A2 - X2 / 6 with
+    // X = 2 (A2 - A1) + c1 gx + c2 gy (so the gradients' factors are c1 gX, c2 gX)
+    const double gTm1 = -0.5 * (vf + avf) * gHO, gTm2 = -0.5 * (vf - avf) * gHO;
+    const double gX1 = divr(gTm1, r6), gX2 = divr(-gTm2, r6);
+    const double gdiff = 2.0 * gX1 + 2.0 * gX2;
+    A.a.gT1[oe + qe] = -0.5 * (vf + avf) * gfl;
+    A.a.gT2[oe + qe] = -0.5 * (vf - avf) * gfl;
+    A.a.gA1[oe + qe] = gTm1 - gdiff;
+    A.a.gA2[oe + qe] = gTm2 + gdiff;
+    A.a.gX1[oe + qe] = gX1;
+    A.a.gX2[oe + qe] = gX2;
   }
-}
-
-// The per-end cotangents of edge e at level k (tracer t), re-derived from the stored
-// gHO (of the MFCT flux) and gfl (of the upwind flux) with r_edge's expressions:
-//   T1/T2: through the upwind flux; A1/A2: through ttfAB in Tm1/Tm2;
-//   g0..g3: through the gradients in Tm1 (g0 = c1 gX1, g2 = c2 gX1) and Tm2 (g1, g3).
-struct EdgeTerms {
-  double gT1, gT2, gA1, gA2, gg0, gg1, gg2, gg3;
-};
-__device__ __forceinline__ EdgeTerms edge_terms(const Adj& A, int t, int e, int k) {
-  const DevMesh& m = *A.in.m;
-  const int64_t qe = int64_t(e) * m.L + k, oe = t * A.a.sEd;
-  const double vf = ld(A.in.ws.vflux + qe), avf = fabs(vf);
-  const double gHO = A.a.gHO[oe + qe], gfl = A.a.gfl[oe + qe];
-  const double c1 = ld(m.ecoef + 2 * e), c2 = ld(m.ecoef + 2 * e + 1);
-  const double gTm1 = -0.5 * (vf + avf) * gHO, gTm2 = -0.5 * (vf - avf) * gHO;
-  const Rcp r6{6.0, 1.0 / 6.0, true};
-  EdgeTerms r;
-  r.gT1 = -0.5 * (vf + avf) * gfl;
-  r.gT2 = -0.5 * (vf - avf) * gfl;
-  const double gX1 = divr(gTm1, r6), gX2 = divr(-gTm2, r6);
-  const double gdiff = 2.0 * gX1 + 2.0 * gX2;
-  r.gA1 = gTm1 - gdiff;
-  r.gA2 = gTm2 + gdiff;
-  r.gg0 = c1 * gX1;
-  r.gg2 = c2 * gX1;
-  r.gg1 = c1 * gX2;
-  r.gg3 = c2 * gX2;
-  return r;
 }
 
 // QR4C stencil depths of interface j (tracer_adv.py:228-238, 265-273)
@@ -517,17 +498,18 @@ __global__ void __launch_bounds__(B) r_gnode(Adj A) {
   const int64_t qn = int64_t(n) * L + k;
   const int e0 = ld(m.ne_off + n), e1 = ld(m.ne_off + n + 1);
   for (int t = 0; t < in.ntr; ++t) {
-    const int64_t oa = t * A.a.sN;
+    const int64_t oa = t * A.a.sN, oe = t * A.a.sEd;
     double gx = 0.0, gy = 0.0;
 #pragma unroll 2
     for (int j = e0; j < e1; ++j) {   // loads unconditional (in bounds), off edges selected away
       const int4 sl = __ldg(m.ne4 + j);
       const int e = sl.x >> 1;
       const bool on = in_range(k, unsigned(sl.z)) && !in_range(k, unsigned(ld(m.etr + e)));
-      const EdgeTerms et = edge_terms(A, t, e, k);
       const bool second = sl.x & 1;
-      gx = on ? gx + (second ? et.gg1 : et.gg0) : gx;
-      gy = on ? gy + (second ? et.gg3 : et.gg2) : gy;
+      const double x = (second ? A.a.gX2 : A.a.gX1)[oe + int64_t(e) * L + k];
+      const double c1 = ld(m.ecoef + 2 * e), c2 = ld(m.ecoef + 2 * e + 1);
+      gx = on ? gx + c1 * x : gx;
+      gy = on ? gy + c2 * x : gy;
     }
     A.a.ggnx[oa + qn] = gx;
     A.a.ggny[oa + qn] = gy;
@@ -630,15 +612,17 @@ __global__ void __launch_bounds__(B) r_tr(Adj A) {
   // the forward's (safe) node-average denominators of the three vertices
   const double dd[3] = {in.ws.nden[qv[0]], in.ws.nden[qv[1]], in.ws.nden[qv[2]]};
   for (int t = 0; t < in.ntr; ++t) {
-    const int64_t oa = t * A.a.sN;
+    const int64_t oa = t * A.a.sN, oe = t * A.a.sEd;
     double gx = 0.0, gy = 0.0;
 #pragma unroll 2
     for (int j = u0; j < u1; ++j) {   // edges using el as up (slot 0) or down (1) cell
       const int idx = ld(m.eud_idx + j), e = idx >> 1;
       const bool on = in_range(k, unsigned(ld(m.etr + e)));
-      const EdgeTerms et = edge_terms(A, t, e, k);
-      gx = on ? gx + ((idx & 1) ? et.gg1 : et.gg0) : gx;   // down : up triangle
-      gy = on ? gy + ((idx & 1) ? et.gg3 : et.gg2) : gy;
+      // the down (slot 1) / up (slot 0) cell's gradient enters Tm2 / Tm1
+      const double x = ((idx & 1) ? A.a.gX2 : A.a.gX1)[oe + int64_t(e) * L + k];
+      const double c1 = ld(m.ecoef + 2 * e), c2 = ld(m.ecoef + 2 * e + 1);
+      gx = on ? gx + c1 * x : gx;
+      gy = on ? gy + c2 * x : gy;
     }
 #pragma unroll
     for (int v = 0; v < 3; ++v) {   // gnode(n) = sum_e a_e tr_e / den(n)
@@ -714,10 +698,11 @@ __global__ void __launch_bounds__(B) r_final(Adj A) {
     for (int j = e0; j < e1; ++j) {
       const int4 sl = __ldg(m.ne4 + j);
       const bool on = in_range(k, unsigned(sl.z));
-      const EdgeTerms et = edge_terms(A, t, sl.x >> 1, k);
       const bool second = sl.x & 1;
-      gT = on ? gT + (second ? et.gT2 : et.gT1) : gT;
-      gA = on ? gA + (second ? et.gA2 : et.gA1) : gA;
+      const int64_t q = t * A.a.sEd + int64_t(sl.x >> 1) * L + k;
+      const double vT = (second ? A.a.gT2 : A.a.gT1)[q], vA = (second ? A.a.gA2 : A.a.gA1)[q];
+      gT = on ? gT + vT : gT;
+      gA = on ? gA + vA : gA;
     }
     const int64_t oT = t * in.tstride + i;
     const double vT = gT + kAbNew * gA, vTo = kAbOld * gA;
@@ -736,7 +721,8 @@ __global__ void __launch_bounds__(B) r_uv(Adj A) {
   const int64_t i = lane_index();
   const int L = m.L;
   if (i >= int64_t(m.E) * L) return;
-  const int el = int(i / L), k = int(i - int64_t(el) * L);
+  int el, k;
+  split_dense(i, L, el, k);
   double gU = 0.0, gV = 0.0;
   if (k >= ld(m.eul + el) && k < ld(m.enl + el)) {
     const double h = ld(in.helem + i);
@@ -793,7 +779,8 @@ __global__ void __launch_bounds__(B) r_w_uv(const DevMesh* __restrict__ mp,
   const int64_t i = lane_index();
   const int L = m.L;
   if (i >= int64_t(m.E) * L) return;
-  const int el = int(i / L), k = int(i - int64_t(el) * L);
+  int el, k;
+  split_dense(i, L, el, k);
   double gU = 0.0, gV = 0.0;
   if (k >= m.eul[el] && k < m.enl[el]) {
     const double h = helem[i];
@@ -848,7 +835,7 @@ int reserve_adj_ws(FctPlan* P, int max_tracers) {
                      &a.gzm1, &a.gzm2, &a.gzp1};
   static_assert(sizeof(node) / sizeof(node[0]) == kAdjNodeFields, "node field count");
   for (double** f : node) *f = take(sN);
-  double** edge[] = {&a.gHO, &a.gfl, &a.gvf};
+  double** edge[] = {&a.gT1, &a.gT2, &a.gA1, &a.gA2, &a.gX1, &a.gX2, &a.gvf};
   static_assert(sizeof(edge) / sizeof(edge[0]) == kAdjEdgeFields, "edge field count");
   for (double** f : edge) *f = take(sEd);
   double** elem[] = {&a.gax, &a.gan, &a.gtrx, &a.gtry};

@@ -989,7 +989,8 @@ __device__ __forceinline__ void body_copy_dry(const Inst& in, int64_t i) {
   const DevMesh& m = *in.m;
   const int64_t NL = int64_t(m.N) * m.L;
   if (i >= NL) return;
-  const int n = int(i / m.L), k = int(i - int64_t(n) * m.L);
+  int n, k;
+  split_dense(i, m.L, n, k);
   if (k >= m.nzmin[n] && k < m.nzmax[n]) return;
   for (int t = 0; t < in.ntr; ++t) {
     const int64_t a = tix<IL>(i, t, in.tstride, in.tg);

@@ -32,6 +32,14 @@ __host__ __device__ inline unsigned pack_tri(int ul1, int nl1, int ul2, int nl2)
   return unsigned(ul1) | (unsigned(nl1) << 8) | (unsigned(ul2) << 16) | (unsigned(nl2) << 24);
 }
 __host__ __device__ inline int lane_lev(uint32_t lane) { return int(lane & kLevelMask); }
+// (entity, level) of a dense [entity, L] index: entity counts are below 2^25 and L <= 128,
+// so the index fits 32 bits and one 32-bit division splits it (a 64-bit integer division
+// is a long emulated sequence on the GPU).
+__device__ __forceinline__ void split_dense(int64_t i, int L, int& ent, int& k) {
+  const uint32_t u = uint32_t(i), q = u / uint32_t(L);
+  ent = int(q);
+  k = int(u - q * uint32_t(L));
+}
 
 // Static mesh on the device (pointers into one plan allocation).
 struct DevMesh {
@@ -143,15 +151,16 @@ struct AdjWorkspace {
   double *ggnx, *ggny;        // node-average gradients
   double *gfv, *gw;           // vertical LO flux, w_e (per tracer)
   double *gz0, *gzm1, *gzm2, *gzp1;  // interface j's QR4C flux into ttfAB at j, j-1, j-2, j+1
-  // edge [Ed, L] per tracer: cotangents of the edge's HO flux, LO flux and volume flux
-  // (the consumers re-derive the per-end terms from them)
-  double *gHO, *gfl, *gvf;
+  // edge [Ed, L] per tracer: the per-end cotangents of the edge's fluxes (T at the first /
+  // second node through the upwind flux, ttfAB through MFCT, the MFCT gradient factor
+  // of each end) and of its volume flux
+  double *gT1, *gT2, *gA1, *gA2, *gX1, *gX2, *gvf;
   // element [E, L] per tracer: the element bounds' shares (divided by the vertex tie
   // counts) and the element gradients
   double *gax, *gan, *gtrx, *gtry;
   int64_t sN, sE, sEd;
 };
-constexpr int kAdjNodeFields = 18, kAdjEdgeFields = 3, kAdjElemFields = 4;
+constexpr int kAdjNodeFields = 18, kAdjEdgeFields = 7, kAdjElemFields = 4;
 
 }  // namespace fct
 
