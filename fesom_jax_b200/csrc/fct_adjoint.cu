@@ -10,7 +10,8 @@
 //
 // Reverse stage map (forward function in fesom_jax/tracer_adv.py -> reverse kernel):
 //   ale_reconstruct (:142-151), flux2dtracer_fct (:469-484)        -> r_seed (divergence),
-//                                                                     r_bounds_lo (T, LO)
+//                                                                     r_bounds_lo (T, LO),
+//                                                                     r_dry (dry levels)
 //   zalesak_limit b3 (:453-465)                                     -> r_factors
 //   zalesak_limit b2 (:441-451), a4 window (:407-418)               -> r_ratio_window
 //   zalesak_limit a2 (:393-397) over a3's per-cell shares            -> r_cluster
@@ -95,12 +96,30 @@ __device__ __forceinline__ double gvl_at(const DevMesh& m, const double* ghsc, i
 }
 
 // ------------------------------------------------------------------ r_seed
-// Every node level. Wet layers: T_new = T + d / hnn (d = del + T (hn - hnn)) and del holds
-// the flux divergence times dt / areasvol; stores the cotangent of a node's flux
-// divergence, gdel * dt / sa. Dry levels keep T (T_new = T, ale_reconstruct), so their
-// outputs are final here, except dT at the level above a cavity's first layer, which the
-// upwind flux of interface nzmin also reaches (r_final writes it); gw_e is zero there.
+// T_new = T + d / hnn (d = del + T (hn - hnn)) and del holds the flux divergence times
+// dt / areasvol: stores the cotangent of a node's flux divergence, gdel * dt / sa.
 __global__ void __launch_bounds__(B) r_seed(Adj A) {
+  const Inst& in = A.in;
+  const DevMesh& m = *in.m;
+  const int64_t li = lane_index();
+  if (li >= m.n_layer) return;
+  const uint32_t lane = ld(m.layer_lanes + li);
+  const int64_t i = int64_t(lane_ent(lane)) * m.L + lane_lev(lane);
+  const double hnn = ld(in.hnode_new + i), av = ld(m.areasvol + i);
+  const double sa = av > 0.0 ? av : 1.0;
+  for (int t = 0; t < in.ntr; ++t) {
+    const double g = ld(A.gTn + t * in.tstride + i);
+    double gdel = 0.0;
+    if (hnn > 0.0) gdel = g / hnn;
+    A.a.ghsc[t * A.a.sN + i] = gdel * in.dt / sa;
+  }
+}
+
+// ------------------------------------------------------------------ r_dry
+// Dry levels keep T (T_new = T, ale_reconstruct): their outputs depend only on dT_new and
+// are final here, except dT at the level above a cavity's first layer, which the upwind
+// flux of interface nzmin also reaches (r_final writes it); gw_e is zero there.
+__global__ void __launch_bounds__(B) r_dry(Adj A) {
   const Inst& in = A.in;
   const DevMesh& m = *in.m;
   const int64_t i = lane_index();
@@ -109,17 +128,7 @@ __global__ void __launch_bounds__(B) r_seed(Adj A) {
   int n, k;
   split_dense(i, L, n, k);
   const int nzmin = ld(m.nzmin + n), nzmax = ld(m.nzmax + n);
-  if (k >= nzmin && k < nzmax) {
-    const double hnn = ld(in.hnode_new + i), av = ld(m.areasvol + i);
-    const double sa = av > 0.0 ? av : 1.0;
-    for (int t = 0; t < in.ntr; ++t) {
-      const double g = ld(A.gTn + t * in.tstride + i);
-      double gdel = 0.0;
-      if (hnn > 0.0) gdel = g / hnn;
-      A.a.ghsc[t * A.a.sN + i] = gdel * in.dt / sa;
-    }
-    return;
-  }
+  if (k >= nzmin && k < nzmax) return;
   const bool above_cavity = k + 1 == nzmin && nzmin < nzmax;
   const double gA = 0.0;
   for (int t = 0; t < in.ntr; ++t) {
@@ -1036,17 +1045,20 @@ int fct_adjoint_ex(FctPlan* P, const FctFields* f, const double* gT_new, double 
     return dim3(unsigned(std::max<int64_t>(1, (lanes + b - 1) / b)));
   };
   const DevMesh& hm = P->hm;
-  const int64_t NL = int64_t(P->N) * P->L;
-  r_seed<<<grid(NL, B), B, 0, s>>>(A);
+  // Side stream: r_dry (dry levels, needs nothing) from the start; r_vert (needs the
+  // node kernels up to r_bounds_lo) beside r_edge; r_uv (needs r_edge's volume-flux
+  // cotangents) beside r_gnode / r_tr / r_final. All are latency-bound gathers, so the
+  // pairs share the SMs.
+  FCT_CUDA(cudaEventRecord(P->adj_ev[0], s));
+  FCT_CUDA(cudaStreamWaitEvent(P->adj_side, P->adj_ev[0], 0));
+  r_dry<<<grid(int64_t(P->N) * P->L, B), B, 0, P->adj_side>>>(A);
+  r_seed<<<grid(hm.n_layer, B), B, 0, s>>>(A);
   r_factors<<<grid(hm.n_layer, B), B, 0, s>>>(A);
   r_ratio_window<<<dim3(unsigned(std::max<int64_t>(1, (hm.n_layer + B - 3) / (B - 2)))), B, 0, s>>>(A);
   r_cluster<<<grid(hm.n_elem, B), B, 0, s>>>(A);
   r_bounds_lo<<<grid(hm.n_layer, B), B, 0, s>>>(A);
-  // Side stream: r_vert (needs the node kernels above) beside r_edge, then r_uv (needs
-  // r_edge's volume-flux cotangents) beside r_gnode / r_tr / r_final. All of them are
-  // latency-bound gathers, so the pairs share the SMs.
-  FCT_CUDA(cudaEventRecord(P->adj_ev[0], s));
-  FCT_CUDA(cudaStreamWaitEvent(P->adj_side, P->adj_ev[0], 0));
+  FCT_CUDA(cudaEventRecord(P->adj_ev[4], s));
+  FCT_CUDA(cudaStreamWaitEvent(P->adj_side, P->adj_ev[4], 0));
   r_vert<<<grid(hm.n_layer, B), B, 0, P->adj_side>>>(A);
   FCT_CUDA(cudaEventRecord(P->adj_ev[1], P->adj_side));
   r_edge<<<grid(hm.n_edge, B), B, 0, s>>>(A);

@@ -179,6 +179,6 @@ struct FctPlan {
   double* d_adj = nullptr;         // reverse-pass workspace
   int adj_tracers = 0;
   cudaStream_t adj_side = nullptr;  // reverse pass: kernels independent of the main chain
-  cudaEvent_t adj_ev[4] = {};       //   and the events that fork and join it
+  cudaEvent_t adj_ev[5] = {};       //   and the events that fork and join it
   fct::AdjWorkspace aws{};
 };
