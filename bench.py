@@ -203,7 +203,7 @@ def run_ours(args, D: Dist) -> dict | None:
         cfg["fct_steps"] = args.fct_steps
     if args.ntr:
         cfg["ntr"] = args.ntr
-    mesh = W.make_workload_mesh(args.config, seed=0)
+    mesh = W.make_workload_mesh(args.config, seed=0, node_order=args.node_order)
     thick = W.rest_thickness_gpu(mesh, dev)
     ens = Ensemble(device=D.local_rank, workspace_budget=int(args.workspace_gb * (1 << 30)))
     member_inputs = []
@@ -638,6 +638,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fd", action="store_true", help="adjoint: skip the FD check")
+    ap.add_argument("--node-order", choices=["rcm", "raw", "random"], default="rcm",
+                    help="synthetic meshes: node numbering (reverse Cuthill-McKee, the "
+                         "generator's Fibonacci order, or a seeded shuffle)")
     ap.add_argument("--checkpoint", choices=["tape", "recompute"], default="tape",
                     help="adjoint: keep every step's intermediates (tape; the per-step "
                          "recomputation is timed beside it) or recompute them only")

@@ -87,13 +87,18 @@ def _smooth_field(xyz: np.ndarray, rng: np.random.Generator, n_waves: int = 24,
 
 def generate_raw(n_nodes: int, zbar: np.ndarray, seed: int = 0, bottom=(5, None),
                  cap_deg: float = 80.0, n_land: int = 3, land_radius_deg=(8.0, 20.0),
-                 jitter: float = 0.25) -> dict:
+                 jitter: float = 0.25, node_order: str = "rcm") -> dict:
     """Raw mesh: geographic nodes (degrees), CW-agnostic triangles, and level counts.
 
     ``bottom=(lo, hi)`` bounds the per-node bottom level count (``hi`` defaults to
-    ``len(zbar)``); it is drawn from a seeded smooth field. Returns the dict consumed by
-    :func:`derive` (the same keys the reference preparation script reads).
+    ``len(zbar)``); it is drawn from a seeded smooth field. ``node_order``: ``"rcm"``
+    (reverse Cuthill-McKee, the default: neighbours are close in index), ``"raw"`` (the
+    Fibonacci point order: consecutive nodes are a golden angle apart) or ``"random"``
+    (a seeded shuffle); elements follow as ascending smallest vertex. Returns the dict
+    consumed by :func:`derive` (the same keys the reference preparation script reads).
     """
+    if node_order not in ("rcm", "raw", "random"):
+        raise ValueError(f"node_order={node_order!r}: expected rcm, raw or random")
     from scipy.spatial import ConvexHull
     from scipy.sparse import coo_matrix
     from scipy.sparse.csgraph import reverse_cuthill_mckee
@@ -141,12 +146,17 @@ def generate_raw(n_nodes: int, zbar: np.ndarray, seed: int = 0, bottom=(5, None)
     tri = remap[tri]
     xyz, glon, glat = xyz[used], glon[used], glat[used]
     N = used.size
-    # reverse Cuthill-McKee node order for locality
-    a, b = np.concatenate([tri[:, 0], tri[:, 1], tri[:, 2]]), np.concatenate(
-        [tri[:, 1], tri[:, 2], tri[:, 0]])
-    adj = coo_matrix((np.ones(a.size), (a, b)), shape=(N, N)).tocsr()
-    adj = adj + adj.T
-    perm = np.asarray(reverse_cuthill_mckee(adj, symmetric_mode=True))
+    # node order: reverse Cuthill-McKee for locality (default)
+    if node_order == "rcm":
+        a, b = np.concatenate([tri[:, 0], tri[:, 1], tri[:, 2]]), np.concatenate(
+            [tri[:, 1], tri[:, 2], tri[:, 0]])
+        adj = coo_matrix((np.ones(a.size), (a, b)), shape=(N, N)).tocsr()
+        adj = adj + adj.T
+        perm = np.asarray(reverse_cuthill_mckee(adj, symmetric_mode=True))
+    elif node_order == "random":
+        perm = np.random.default_rng(seed + 7919).permutation(N)
+    else:
+        perm = np.arange(N)
     inv = np.empty(N, np.int64)
     inv[perm] = np.arange(N)
     tri = inv[tri]

@@ -26,13 +26,16 @@ WORKLOADS = {
 }
 
 
-def make_workload_mesh(name: str, seed: int = 0) -> Mesh:
+def make_workload_mesh(name: str, seed: int = 0, node_order: str = "rcm") -> Mesh:
+    """The configuration's mesh; synthetic meshes in ``node_order`` (see
+    :func:`meshgen.generate_raw`; the pi mesh keeps its shipped order)."""
     from . import meshgen
     w = WORKLOADS[name]
     if w["n_nodes"] is None:
         return pi_mesh()
+    suffix = "" if node_order == "rcm" else f"_{node_order}"
     return meshgen.make_mesh(w["n_nodes"], nl=w["nl"], seed=seed, bottom=w["bottom"],
-                             name=f"{name}_{w['n_nodes']}")
+                             name=f"{name}_{w['n_nodes']}{suffix}", node_order=node_order)
 
 
 @dataclasses.dataclass
