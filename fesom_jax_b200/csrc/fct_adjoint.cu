@@ -12,8 +12,7 @@
 //   ale_reconstruct (:142-151), flux2dtracer_fct (:469-484)        -> r_seed (divergence),
 //                                                                     r_bounds_lo (T, LO),
 //                                                                     r_dry (dry levels)
-//   zalesak_limit b3 (:453-465)                                     -> r_factors
-//   zalesak_limit b2 (:441-451), a4 window (:407-418)               -> r_ratio_window
+//   zalesak_limit b3 (:453-465), b2 (:441-451), a4 window (:407-418) -> r_ratio_window
 //   zalesak_limit a2 (:393-397) over a3's per-cell shares            -> r_cluster
 //   zalesak_limit a1 (:389-391), compute_fct_lo (:298-313)          -> r_bounds_lo
 //   adv_flux_hor_ho (:196-225), adv_flux_hor (:96-105), b1 edges    -> r_edge
@@ -145,81 +144,78 @@ __global__ void __launch_bounds__(B) r_dry(Adj A) {
   A.gw[i] = (A.acc & kAccW) ? A.gw[i] + g : g;
 }
 
-// --------------------------------------------- r_factors: cotangents of pf, mf
-__global__ void __launch_bounds__(B) r_factors(Adj A) {
+// ------------------------------- cotangents of the limiter factors pf, mf at (n, k)
+// (zalesak_limit b3, tracer_adv.py:453-465): the limited vertical fluxes at interfaces k
+// and k+1 and the limited horizontal fluxes of the incident edges in ascending edge id.
+__device__ __forceinline__ void factor_cotangents(const Adj& A, int t, int n, int k, int nzmin,
+                                                  int nzmax, double& gp, double& gm) {
   const Inst& in = A.in;
   const DevMesh& m = *in.m;
-  const int64_t i = lane_index();
-  if (i >= m.n_layer) return;
-  const uint32_t lane = ld(m.layer_lanes + i);
-  const int n = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const int nzmin = ld(m.nzmin + n), nzmax = ld(m.nzmax + n);
+  const int L = m.L;
   const int64_t base = int64_t(n) * L, qn = base + k;
   const int e0 = ld(m.ne_off + n), e1 = ld(m.ne_off + n + 1);
-  for (int t = 0; t < in.ntr; ++t) {
-    const int64_t o = t * in.ws.sN;
-    const double* pf = in.ws.pf + o;
-    const double* mf = in.ws.mf + o;
-    const double* adfv = in.ws.adfv + o;
-    const double* ghsc = A.a.ghsc + t * A.a.sN;
-    const double pfk = pf[qn], mfk = mf[qn];
-    double gp = 0.0, gm = 0.0;
-    // vertical limited flux at interface k (this node's own factors at k)
-    {
-      const double f = adfv[qn];
-      const double g_ae = gvl_at(m, ghsc, base, k, nzmin, nzmax) * f;
-      if (k == nzmin) {
-        if (f >= 0.0) gp += g_ae; else gm += g_ae;
-      } else if (f >= 0.0) {
-        gp += g_ae * smin_b(mf[qn - 1], pfk);
-      } else {
-        gm += g_ae * smin_b(pf[qn - 1], mfk);
-      }
+  const int64_t o = t * in.ws.sN;
+  const double* pf = in.ws.pf + o;
+  const double* mf = in.ws.mf + o;
+  const double* adfv = in.ws.adfv + o;
+  const double* ghsc = A.a.ghsc + t * A.a.sN;
+  const double pfk = pf[qn], mfk = mf[qn];
+  gp = 0.0;
+  gm = 0.0;
+  // vertical limited flux at interface k (this node's own factors at k)
+  {
+    const double f = adfv[qn];
+    const double g_ae = gvl_at(m, ghsc, base, k, nzmin, nzmax) * f;
+    if (k == nzmin) {
+      if (f >= 0.0) gp += g_ae; else gm += g_ae;
+    } else if (f >= 0.0) {
+      gp += g_ae * smin_b(mf[qn - 1], pfk);
+    } else {
+      gm += g_ae * smin_b(pf[qn - 1], mfk);
     }
-    // vertical limited flux at interface k+1 (uses this node's factors as the k-1 ones)
-    if (k + 1 < nzmax) {
-      const double f = adfv[qn + 1];
-      const double g_ae = gvl_at(m, ghsc, base, k + 1, nzmin, nzmax) * f;
-      if (f >= 0.0) gm += g_ae * smin_a(mfk, pf[qn + 1]);
-      else gp += g_ae * smin_a(pfk, mf[qn + 1]);
-    }
-    // horizontal limited fluxes of the incident edges, ascending edge id; the loads are
-    // unconditional (all in bounds) and edges without a flux at k are selected away
-    const double ghsc0 = ghsc[qn];
-    const double* adfh = in.ws.adfh + t * in.ws.sEd;
+  }
+  // vertical limited flux at interface k+1 (uses this node's factors as the k-1 ones)
+  if (k + 1 < nzmax) {
+    const double f = adfv[qn + 1];
+    const double g_ae = gvl_at(m, ghsc, base, k + 1, nzmin, nzmax) * f;
+    if (f >= 0.0) gm += g_ae * smin_a(mfk, pf[qn + 1]);
+    else gp += g_ae * smin_a(pfk, mf[qn + 1]);
+  }
+  // horizontal limited fluxes of the incident edges, ascending edge id; the loads are
+  // unconditional (all in bounds) and edges without a flux at k are selected away
+  const double ghsc0 = ghsc[qn];
+  const double* adfh = in.ws.adfh + t * in.ws.sEd;
 #pragma unroll 2
-    for (int j = e0; j < e1; ++j) {
-      const int4 sl = __ldg(m.ne4 + j);
-      const bool on = in_range(k, unsigned(sl.z));
-      const bool second = sl.x & 1;
-      const int64_t qo = int64_t(sl.y) * L + k;
-      const double ghsco = ghsc[qo];
-      const double glim = second ? (ghsco - ghsc0) : (ghsc0 - ghsco);
-      const double a = adfh[int64_t(sl.x >> 1) * L + k];
-      const double g_ae = glim * a;
-      const double pfo = pf[qo], mfo = mf[qo];
-      const double pf1 = second ? pfo : pfk, mf1 = second ? mfo : mfk;
-      const double pf2 = second ? pfk : pfo, mf2 = second ? mfk : mfo;
-      double dp = 0.0, dm = 0.0;
-      bool tp = false, tm = false;
-      if (a >= 0.0) {   // ae = min(pf[n1], mf[n2])
-        if (!second) { dp = g_ae * smin_a(pf1, mf2); tp = true; }
-        else { dm = g_ae * smin_b(pf1, mf2); tm = true; }
-      } else {          // ae = min(mf[n1], pf[n2])
-        if (!second) { dm = g_ae * smin_a(mf1, pf2); tm = true; }
-        else { dp = g_ae * smin_b(mf1, pf2); tp = true; }
-      }
-      gp = (on && tp) ? gp + dp : gp;
-      gm = (on && tm) ? gm + dm : gm;
+  for (int j = e0; j < e1; ++j) {
+    const int4 sl = __ldg(m.ne4 + j);
+    const bool on = in_range(k, unsigned(sl.z));
+    const bool second = sl.x & 1;
+    const int64_t qo = int64_t(sl.y) * L + k;
+    const double ghsco = ghsc[qo];
+    const double glim = second ? (ghsco - ghsc0) : (ghsc0 - ghsco);
+    const double a = adfh[int64_t(sl.x >> 1) * L + k];
+    const double g_ae = glim * a;
+    const double pfo = pf[qo], mfo = mf[qo];
+    const double pf1 = second ? pfo : pfk, mf1 = second ? mfo : mfk;
+    const double pf2 = second ? pfk : pfo, mf2 = second ? mfk : mfo;
+    double dp = 0.0, dm = 0.0;
+    bool tp = false, tm = false;
+    if (a >= 0.0) {   // ae = min(pf[n1], mf[n2])
+      if (!second) { dp = g_ae * smin_a(pf1, mf2); tp = true; }
+      else { dm = g_ae * smin_b(pf1, mf2); tm = true; }
+    } else {          // ae = min(mf[n1], pf[n2])
+      if (!second) { dm = g_ae * smin_a(mf1, pf2); tm = true; }
+      else { dp = g_ae * smin_b(mf1, pf2); tp = true; }
     }
-    A.a.gpf[t * A.a.sN + qn] = gp;
-    A.a.gmf[t * A.a.sN + qn] = gm;
+    gp = (on && tp) ? gp + dp : gp;
+    gm = (on && tm) ? gm + dm : gm;
   }
 }
 
-// ---------------- r_ratio_window: pf = min(1, fmax_w / flux_pos), likewise mf, the a4
-// window (max/min over the cluster bounds at k-1, k, k+1 of the same column), and the a3
-// share of each cell that attains the node's cluster bound.
+// ---------------- r_ratio_window: the factor cotangents (b3), pf = min(1, fmax_w /
+// flux_pos) and likewise mf (b2), the a4 window (max/min over the cluster bounds at k-1, k,
+// k+1 of the same column), and the a3 share of each cell that attains the node's cluster
+// bound.
 // Blocks of B threads cover B - 2 lanes plus one halo lane on each side: every thread
 // computes its lane's window cotangents (gtmax, gtmin) into shared memory, and the core
 // lanes spread them back over the window's three levels (lanes i-1, i, i+1).
@@ -257,6 +253,8 @@ __global__ void __launch_bounds__(B) r_ratio_window(Adj A) {
     const double* tn = in.ws.tvmin + o;
     double gtmax = 0.0, gtmin = 0.0;
     if (valid) {
+      double gpf, gmf;
+      factor_cotangents(A, t, n, k, nzmin, nzmax, gpf, gmf);
       double gplus = 0.0, gminus = 0.0;
       if (valid_n) {
         double tmax = tv[qn], tmin = tn[qn];
@@ -271,8 +269,8 @@ __global__ void __launch_bounds__(B) r_ratio_window(Adj A) {
         const double flux_neg = divr(divr(minus * dt, rsa), rsh) - kFluxEps;
         const Rcp rfp = rcp(flux_pos), rfn = rcp(flux_neg);
         const double rp = divr(fmax_w, rfp), rm = divr(fmin_w, rfn);
-        const double grp = A.a.gpf[oa + qn] * smin_b(1.0, rp);
-        const double grm = A.a.gmf[oa + qn] * smin_b(1.0, rm);
+        const double grp = gpf * smin_b(1.0, rp);
+        const double grm = gmf * smin_b(1.0, rm);
         gtmax = divr(grp, rfp);
         gtmin = divr(grm, rfn);
         gplus = divr(divr(-grp * fmax_w / (flux_pos * flux_pos) * dt, rsa), rsh);
@@ -839,7 +837,7 @@ int reserve_adj_ws(FctPlan* P, int max_tracers) {
   AdjWorkspace& a = P->aws;
   a.sN = sN; a.sE = sE; a.sEd = sEd;
   auto take = [&](int64_t n) { double* q = p; p += n * max_tracers; return q; };
-  double** node[] = {&a.ghsc, &a.gpf, &a.gmf, &a.gplus, &a.gminus, &a.gLOl, &a.gqx,
+  double** node[] = {&a.ghsc, &a.gplus, &a.gminus, &a.gLOl, &a.gqx,
                      &a.gqn, &a.gdiv, &a.gTp, &a.ggnx, &a.ggny, &a.gfv, &a.gw, &a.gz0,
                      &a.gzm1, &a.gzm2, &a.gzp1};
   static_assert(sizeof(node) / sizeof(node[0]) == kAdjNodeFields, "node field count");
@@ -1053,7 +1051,6 @@ int fct_adjoint_ex(FctPlan* P, const FctFields* f, const double* gT_new, double 
   FCT_CUDA(cudaStreamWaitEvent(P->adj_side, P->adj_ev[0], 0));
   r_dry<<<grid(int64_t(P->N) * P->L, B), B, 0, P->adj_side>>>(A);
   r_seed<<<grid(hm.n_layer, B), B, 0, s>>>(A);
-  r_factors<<<grid(hm.n_layer, B), B, 0, s>>>(A);
   r_ratio_window<<<dim3(unsigned(std::max<int64_t>(1, (hm.n_layer + B - 3) / (B - 2)))), B, 0, s>>>(A);
   r_cluster<<<grid(hm.n_elem, B), B, 0, s>>>(A);
   r_bounds_lo<<<grid(hm.n_layer, B), B, 0, s>>>(A);

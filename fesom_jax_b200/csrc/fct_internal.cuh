@@ -143,7 +143,6 @@ struct Inst {
 struct AdjWorkspace {
   // node [N, L] per tracer
   double* ghsc;               // cotangent of the node's flux divergence: gdel * dt / areasvol
-  double *gpf, *gmf;          // limiter factors
   double *gplus, *gminus;     // limiter sums
   double* gLOl;               // LO through the limiter window (-(gtmax + gtmin))
   double *gqx, *gqn;          // cluster bounds divided by their tie counts (one cell's share)
@@ -160,7 +159,7 @@ struct AdjWorkspace {
   double *gax, *gan, *gtrx, *gtry;
   int64_t sN, sE, sEd;
 };
-constexpr int kAdjNodeFields = 18, kAdjEdgeFields = 7, kAdjElemFields = 4;
+constexpr int kAdjNodeFields = 16, kAdjEdgeFields = 7, kAdjElemFields = 4;
 
 }  // namespace fct
 

@@ -237,3 +237,31 @@ def test_tape_reopened_over_the_same_memory(torch, pi):
     with pytest.raises(RuntimeError, match="needed"):
         _lib.check(L.fct_tape_create(second.plan.handle, 1, 1, C.c_void_p(mem.data_ptr()),
                                      nb - 8, C.byref(h)))
+
+
+def test_tape_equals_recompute_on_cavity(torch, pi):
+    """The same on the cavity mesh (nzmin > 0 under ice shelves): the dry level above a
+    cavity's first layer receives the upwind term of interface nzmin in both modes."""
+    from fesom_jax_b200.adjoint import Tape, advect_one_fct_vjp
+    from tests.golden_cases import cavity_mesh
+    cav = cavity_mesh(pi)
+    assert (cav.ulevels_nod2D > 1).any()
+    f = I.make_fields(cav, seed=4, ab2=True, kind="white", sigma=0.02)
+    args = [_d(torch, x) for x in (f.uv, f.w_e, f.helem, f.hnode, f.hnode_new)]
+    T, To = _d(torch, f.tracers), _d(torch, f.tracers_old)
+    gTn = _d(torch, np.random.default_rng(12).normal(size=T.shape))
+    with Tape(cav, steps=1, ntr=2) as tape:
+        tape.forward(0, *args, T, To, DT)
+        taped = advect_one_fct_vjp(cav, *args, T, To, gTn, dt=DT, tape=tape, slot=0)
+    plain = advect_one_fct_vjp(cav, *args, T, To, gTn, dt=DT)
+    for a, b in zip(taped, plain):
+        assert torch.equal(a, b)
+    # the dry level above the first layer of cavity nodes with w < 0 at that interface
+    # carries more than dT_new (the upwind term); the other dry levels carry dT_new
+    nodes = np.nonzero(cav.ulevels_nod2D > 1)[0]
+    ks = cav.ulevels_nod2D[nodes] - 2
+    got = taped[0][0].cpu().numpy()[nodes, ks]
+    seed = gTn[0].cpu().numpy()[nodes, ks]
+    wtop = f.w_e[nodes, ks + 1]
+    assert np.any((got != seed) & (wtop < 0))
+    assert np.all(got[wtop > 0] == seed[wtop > 0] + 0.0)
