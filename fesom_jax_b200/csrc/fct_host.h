@@ -70,6 +70,8 @@ int64_t workspace_doubles(int64_t N, int64_t E, int64_t Ed, int64_t L, int ntr);
 int64_t workspace_doubles_fused(int64_t N, int64_t Ed, int64_t L, int ntr);
 // Grow the plan workspace to `ntr` tracers; `full` also makes it hold every stage field.
 int plan_reserve_ws(FctPlan* P, int ntr, bool full);
+// A plan created by fct_plan_create in this process and not destroyed yet.
+bool plan_alive(const FctPlan* P);
 
 // Launches one stage takes for `csz` tracers of a workspace chunk with at most
 // `per_thread` tracers per thread (the split rule of the stage launcher).

@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cstring>
 #include <mutex>
+#include <unordered_set>
 #include <vector>
 
 #include "fct_host.h"
@@ -19,6 +20,16 @@
 namespace fct {
 
 static thread_local std::string g_last_error;
+
+// Plans alive in this process: the custom-call handlers receive a plan as an integer in
+// their opaque bytes and check it here before use.
+static std::mutex g_plans_mu;
+static std::unordered_set<const FctPlan*> g_plans;
+
+bool plan_alive(const FctPlan* P) {
+  std::lock_guard<std::mutex> lk(g_plans_mu);
+  return g_plans.count(P) != 0;
+}
 
 int set_error(int status, const char* fmt, ...) {
   char buf[1024];
@@ -395,6 +406,10 @@ const char* fct_version(void) { return "fesom_fct 0.1.0 (sm_100a, fp64)"; }
 
 int fct_plan_destroy(FctPlan* P) {
   if (!P) return FCT_OK;
+  {
+    std::lock_guard<std::mutex> lk(fct::g_plans_mu);
+    fct::g_plans.erase(P);
+  }
   cudaSetDevice(P->device);
   if (P->d_adj) cudaFree(P->d_adj);
   if (P->adj_side) cudaStreamDestroy(P->adj_side);
@@ -422,6 +437,10 @@ int fct_plan_create(const FctMeshDesc* desc, int device, int max_tracers, FctPla
   st = plan_build(desc, device, P);
   if (!st) st = fct_plan_reserve(P, max_tracers < 1 ? 1 : max_tracers);
   if (st) { fct_plan_destroy(P); return st; }
+  {
+    std::lock_guard<std::mutex> lk(fct::g_plans_mu);
+    fct::g_plans.insert(P);
+  }
   *out = P;
   return FCT_OK;
 }

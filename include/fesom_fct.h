@@ -212,6 +212,32 @@ int fct_tape_mark_recorded(FctTape* tape, int slot, double dt);
 int fct_adjoint_ex(FctPlan* plan, const FctFields* fields, const double* gT_new, double dt,
                    int ntr, const FctGrads* grads, const FctTape* tape, int slot,
                    int accumulate, fct_stream_t stream);
+/*
+ * JAX/XLA custom-call handlers, legacy GPU ABI (jax.ffi.register_ffi_target(name,
+ * jax.ffi.pycapsule(fn), platform="CUDA", api_version=0)); they replace the reference's
+ * in-graph advect_one_fct (fesom_jax/tracer_adv.py:532-578) and its jax.grad.
+ * ``opaque`` holds an FctXlaOpaque. ``buffers`` has a fixed layout (absent optional
+ * operands are one-element placeholders, flagged absent):
+ *   forward: uv, w_e, helem, hnode, hnode_new, T, T_old, Z3d, zbar3, w_i | T_new, status
+ *   adjoint: uv, w_e, helem, hnode, hnode_new, T, T_old, Z3d, zbar3, gT_new |
+ *            gT, gT_old, guv, gw_e, status
+ * ``status`` is an int32 device scalar receiving the FctStatus (the ABI has no error
+ * return). No allocation: reserve the plan (fct_plan_reserve; fct_plan_reserve_adjoint for
+ * the adjoint) before the first call.
+ */
+typedef struct FctXlaOpaque {
+  uint64_t plan;   /* FctPlan* of this process, as an integer */
+  double dt;
+  int32_t ntr;     /* tracers in T (tracer-major, [ntr, nod2D, nl]) */
+  int32_t flags;   /* FCT_XLA_* */
+} FctXlaOpaque;
+#define FCT_XLA_Z3D 1   /* Z3d and zbar3 are real operands */
+#define FCT_XLA_WI 2    /* w_i is a real operand (forward only) */
+#define FCT_XLA_FWD_STATUS 11
+#define FCT_XLA_ADJ_STATUS 14
+void fct_xla_forward(void* stream, void** buffers, const char* opaque, size_t opaque_len);
+void fct_xla_adjoint(void* stream, void** buffers, const char* opaque, size_t opaque_len);
+
 /* Vector-Jacobian product of fct_compute_w (fesom_jax/ale.py:309-365) w.r.t. uv:
  * guv (+)= J^T gw, [elem2D,nl,2]; ``accumulate`` = 0 overwrites, 1 adds. */
 int fct_compute_w_adjoint(FctPlan* plan, const double* gw, const double* helem,
