@@ -48,6 +48,21 @@ static int batch_launch_step(FctBatch* b, int phase, cudaStream_t s) {
   return FCT_OK;
 }
 
+namespace {
+
+// The kernels index an interleaved array (entity-level x tracer slot) in 32 bits: every
+// such array of instance i must hold fewer than 2^32 elements.
+int check_interleave(const FctPlan* P, int tg, int wtg, int i) {
+  const int64_t ent = std::max({int64_t(P->N), int64_t(P->E), int64_t(P->Ed)});
+  if (ent * P->L * std::max(tg, wtg) >= (int64_t(1) << 32))
+    return set_error(FCT_ERR_CAPACITY, "instance %d: %lld entity levels x %d tracers exceed "
+                     "the 2^32-element interleaved arrays; use fewer tracers per instance", i,
+                     (long long)(ent * P->L), std::max(tg, wtg));
+  return FCT_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 int fct_batch_create(const FctInstance* insts, int n, int64_t budget, FctBatch** out) {
@@ -75,6 +90,8 @@ int fct_batch_create(const FctInstance* insts, int n, int64_t budget, FctBatch**
       wc = (wc + 1) / 2;
     wchunk[i] = wc;
     ws_doubles[i] = workspace_doubles_fused(P->N, P->Ed, P->L, wc);
+    const int st = check_interleave(P, q.ntr, wc, i);
+    if (st) return st;
   }
   FctBatch* B = new FctBatch();
   B->device = dev;
@@ -401,6 +418,8 @@ int fct_serve_step(FctServe* S, const FctInstance* insts, const int32_t* phases,
     if (!q.plan || q.plan->device != S->device || q.ntr < 1 || !q.buf[0] || !q.buf[1] ||
         !q.buf[2] || !q.uv || !q.w_e || !q.helem || !q.hnode || !q.hnode_new || !(q.dt > 0.0))
       return set_error(FCT_ERR_INVALID, "instance %d is invalid", i);
+    const int st = check_interleave(q.plan, q.ntr, q.ntr, i);
+    if (st) return st;
     need += workspace_doubles_fused(q.plan->N, q.plan->Ed, q.plan->L, q.ntr);
   }
   if (need > S->arena_doubles)

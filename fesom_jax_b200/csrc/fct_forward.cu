@@ -40,18 +40,25 @@ __device__ __forceinline__ int64_t lane_index() {
 template <class T>
 __device__ __forceinline__ T ld(const T* p) { return __ldg(p); }
 
-// Address of tracer t at entity-level q: interleaved q*tg + t, else t*stride + q.
+// Dense offset of entity-level (e, k): below 2^32 (entities < 2^25, L <= 128), so it is
+// computed in 32 bits (64-bit index products are multi-instruction sequences).
+__device__ __forceinline__ uint32_t lq(int e, int L, int k) {
+  return uint32_t(e) * uint32_t(L) + uint32_t(k);
+}
+
+// Address of tracer t at entity-level q: interleaved q*tg + t (below 2^32: the batch
+// engine checks every interleaved array against it), else t*stride + q.
 template <bool IL>
-__device__ __forceinline__ int64_t tix(int64_t q, int t, int64_t stride, int tg) {
-  return IL ? q * tg + t : int64_t(t) * stride + q;
+__device__ __forceinline__ int64_t tix(uint32_t q, int t, int64_t stride, int tg) {
+  return IL ? int64_t(q * uint32_t(tg) + uint32_t(t)) : int64_t(t) * stride + q;
 }
 
 // Tracers [t0, t0+NTR) of entity-level q.
 template <int NTR, bool IL>
-__device__ __forceinline__ void ldn(const double* __restrict__ p, int64_t q, int t0,
+__device__ __forceinline__ void ldn(const double* __restrict__ p, uint32_t q, int t0,
                                     int64_t stride, int tg, double (&v)[NTR]) {
   if constexpr (IL && (NTR % 2 == 0)) {
-    const double* b = p + q * tg + t0;
+    const double* b = p + (q * uint32_t(tg) + uint32_t(t0));
     if ((reinterpret_cast<uintptr_t>(b) & 15) == 0) {
 #pragma unroll
       for (int i = 0; i < NTR; i += 2) {
@@ -67,10 +74,10 @@ __device__ __forceinline__ void ldn(const double* __restrict__ p, int64_t q, int
 }
 
 template <int NTR, bool IL>
-__device__ __forceinline__ void stn(double* __restrict__ p, int64_t q, int t0, int64_t stride,
+__device__ __forceinline__ void stn(double* __restrict__ p, uint32_t q, int t0, int64_t stride,
                                     int tg, const double (&v)[NTR]) {
   if constexpr (IL && (NTR % 2 == 0)) {
-    double* b = p + q * tg + t0;
+    double* b = p + (q * uint32_t(tg) + uint32_t(t0));
     if ((reinterpret_cast<uintptr_t>(b) & 15) == 0) {
 #pragma unroll
       for (int i = 0; i < NTR; i += 2)
@@ -84,7 +91,7 @@ __device__ __forceinline__ void stn(double* __restrict__ p, int64_t q, int t0, i
 
 // tie counts (bytes) of tracers [t0, t0+NTR) at entity-level q
 template <int NTR, bool IL>
-__device__ __forceinline__ void stc(uint8_t* __restrict__ p, int64_t q, int t0, int64_t stride,
+__device__ __forceinline__ void stc(uint8_t* __restrict__ p, uint32_t q, int t0, int64_t stride,
                                     int tg, const int (&v)[NTR]) {
 #pragma unroll
   for (int i = 0; i < NTR; ++i) p[tix<IL>(q, t0 + i, stride, tg)] = uint8_t(v[i]);
@@ -100,16 +107,16 @@ __device__ __forceinline__ void body_vflux(const Inst& in, int64_t i) {
   const double* cr = m.cross + 4 * int64_t(e);
   double t1 = 0.0, t2 = 0.0;
   if (k >= ld(m.eul + el1) && k < ld(m.enl + el1)) {
-    const int64_t q = int64_t(el1) * L + k;
+    const uint32_t q = lq(el1, L, k);
     const double2 U = __ldg(reinterpret_cast<const double2*>(in.uv) + q);
     t1 = (U.x * ld(cr + 1) - U.y * ld(cr + 0)) * ld(in.helem + q);
   }
   if (el2 >= 0 && k >= ld(m.eul + el2) && k < ld(m.enl + el2)) {
-    const int64_t q = int64_t(el2) * L + k;
+    const uint32_t q = lq(el2, L, k);
     const double2 U = __ldg(reinterpret_cast<const double2*>(in.uv) + q);
     t2 = (U.y * ld(cr + 2) - U.x * ld(cr + 3)) * ld(in.helem + q);
   }
-  in.ws.vflux[int64_t(e) * L + k] = t1 + t2;
+  in.ws.vflux[lq(e, L, k)] = t1 + t2;
 }
 
 // ---------------------------------------------------- tracer_gradient_elements
@@ -135,9 +142,9 @@ __device__ __forceinline__ void cell_grad(const Inst& in, int el, int v0, int v1
                                           int t0, double (&gx)[NTR], double (&gy)[NTR]) {
   const int L = in.m->L;
   double a0[NTR], a1[NTR], a2[NTR];
-  ldn<NTR, IL>(in.T, int64_t(v0) * L + k, t0, in.tstride, in.tg, a0);
-  ldn<NTR, IL>(in.T, int64_t(v1) * L + k, t0, in.tstride, in.tg, a1);
-  ldn<NTR, IL>(in.T, int64_t(v2) * L + k, t0, in.tstride, in.tg, a2);
+  ldn<NTR, IL>(in.T, lq(v0, L, k), t0, in.tstride, in.tg, a0);
+  ldn<NTR, IL>(in.T, lq(v1, L, k), t0, in.tstride, in.tg, a1);
+  ldn<NTR, IL>(in.T, lq(v2, L, k), t0, in.tstride, in.tg, a2);
   cell_grad_vals<NTR>(in, el, a0, a1, a2, gx, gy);
 }
 
@@ -150,18 +157,18 @@ __device__ __forceinline__ void cell_grad_own(const Inst& in, int el, int v0, in
   const int L = in.m->L;
   double a0[NTR], a1[NTR], a2[NTR];
   if (pos == 0) {
-    ldn<NTR, IL>(in.T, int64_t(v1) * L + k, t0, in.tstride, in.tg, a1);
-    ldn<NTR, IL>(in.T, int64_t(v2) * L + k, t0, in.tstride, in.tg, a2);
+    ldn<NTR, IL>(in.T, lq(v1, L, k), t0, in.tstride, in.tg, a1);
+    ldn<NTR, IL>(in.T, lq(v2, L, k), t0, in.tstride, in.tg, a2);
 #pragma unroll
     for (int t = 0; t < NTR; ++t) a0[t] = own[t];
   } else if (pos == 1) {
-    ldn<NTR, IL>(in.T, int64_t(v0) * L + k, t0, in.tstride, in.tg, a0);
-    ldn<NTR, IL>(in.T, int64_t(v2) * L + k, t0, in.tstride, in.tg, a2);
+    ldn<NTR, IL>(in.T, lq(v0, L, k), t0, in.tstride, in.tg, a0);
+    ldn<NTR, IL>(in.T, lq(v2, L, k), t0, in.tstride, in.tg, a2);
 #pragma unroll
     for (int t = 0; t < NTR; ++t) a1[t] = own[t];
   } else {
-    ldn<NTR, IL>(in.T, int64_t(v0) * L + k, t0, in.tstride, in.tg, a0);
-    ldn<NTR, IL>(in.T, int64_t(v1) * L + k, t0, in.tstride, in.tg, a1);
+    ldn<NTR, IL>(in.T, lq(v0, L, k), t0, in.tstride, in.tg, a0);
+    ldn<NTR, IL>(in.T, lq(v1, L, k), t0, in.tstride, in.tg, a1);
 #pragma unroll
     for (int t = 0; t < NTR; ++t) a2[t] = own[t];
   }
@@ -188,7 +195,7 @@ __device__ __forceinline__ void body_elem_grad(const Inst& in, int64_t i, int t0
   const int e = lane_ent(lane), k = lane_lev(lane), L = m.L;
   double gx[NTR], gy[NTR];
   cell_grad<NTR, IL>(in, e, k, t0, gx, gy);
-  const int64_t q = int64_t(e) * L + k;
+  const uint32_t q = lq(e, L, k);
   stn<NTR, IL>(in.ws.gx, q, w0, in.ws.sE, in.wtg, gx);
   stn<NTR, IL>(in.ws.gy, q, w0, in.ws.sE, in.wtg, gy);
 }
@@ -210,7 +217,7 @@ __device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i, int t0, 
   const uint32_t lane = ld(m.iface_lanes + i);
   const int n = lane_ent(lane), k = lane_lev(lane), L = m.L;
   const int nzmin = ld(m.nzmin + n), nzmax = ld(m.nzmax + n);
-  const int64_t base = int64_t(n) * L, qn = base + k;
+  const uint32_t base = lq(n, L, 0), qn = base + uint32_t(k);
   const bool layer = k < nzmax;
   const bool layer1 = (k + 1) < nzmax;
   const int km1 = k > 0 ? k - 1 : 0;
@@ -256,10 +263,10 @@ __device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i, int t0, 
         const int4 sl = __ldg(m.ne4 + j);
         const bool on = in_range(k, unsigned(sl.z));
         const bool second = sl.x & 1;
-        const double vf = ld(in.ws.vflux + int64_t(sl.x >> 1) * L + k);
+        const double vf = ld(in.ws.vflux + lq(sl.x >> 1, L, k));
         const double avf = fabs(vf);
         double To[NTR];
-        ldn<NTR, IL>(in.T, int64_t(sl.y) * L + k, t0, ts, tg, To);
+        ldn<NTR, IL>(in.T, lq(sl.y, L, k), t0, ts, tg, To);
 #pragma unroll
         for (int t = 0; t < NTR; ++t) {
           const double T1 = second ? To[t] : Tc[t], T2 = second ? Tc[t] : To[t];
@@ -272,10 +279,10 @@ __device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i, int t0, 
         const int idx = ld(m.ne_idx + j), e = idx >> 1;
         if (k < ld(m.ekmin + e) || k >= ld(m.ekmax + e)) continue;   // vflux == 0 there
         const int oth = ld(m.ne_oth + j);
-        const double vf = ld(in.ws.vflux + int64_t(e) * L + k);
+        const double vf = ld(in.ws.vflux + lq(e, L, k));
         const double avf = fabs(vf);
         double To[NTR];
-        ldn<NTR, IL>(in.T, int64_t(oth) * L + k, t0, ts, tg, To);
+        ldn<NTR, IL>(in.T, lq(oth, L, k), t0, ts, tg, To);
 #pragma unroll
         for (int t = 0; t < NTR; ++t) {
           const double T1 = (idx & 1) ? To[t] : Tc[t], T2 = (idx & 1) ? Tc[t] : To[t];
@@ -317,7 +324,7 @@ __device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i, int t0, 
         const int el = ld(m.nel_idx + j);
         if (k >= ld(m.eul + el) && k < ld(m.enl + el)) {
           const double a = ld(m.earea + el);
-          const int64_t qe = int64_t(el) * L + k;
+          const uint32_t qe = lq(el, L, k);
           double gx[NTR], gy[NTR];
           ldn<NTR, IL>(in.ws.gx, qe, w0, in.ws.sE, in.wtg, gx);
           ldn<NTR, IL>(in.ws.gy, qe, w0, in.ws.sE, in.wtg, gy);
@@ -410,7 +417,7 @@ __device__ __forceinline__ void body_vert_impl(const Inst& in, int64_t n, int t0
   const int L = m.L;
   const int nzmin = m.nzmin[n], nzmax = m.nzmax[n];
   if (nzmax <= nzmin) return;
-  const int64_t base = n * L;
+  const uint32_t base = lq(int(n), L, 0);
   const double dt = in.dt;
   double cp[kMaxLevels], dp[kMaxLevels];
   for (int tw = w0; tw < w0 + NTR; ++tw) {
@@ -456,10 +463,10 @@ __device__ __forceinline__ void body_edge_adf(const Inst& in, int64_t i, int t0,
   const int e = lane_ent(lane), k = lane_lev(lane), L = m.L;
   const int n1 = ld(m.edges + 2 * e), n2 = ld(m.edges + 2 * e + 1);
   const bool use_tri = in_range(k, unsigned(ld(m.etr + e)));
-  const double vf = ld(in.ws.vflux + int64_t(e) * L + k);
+  const double vf = ld(in.ws.vflux + lq(e, L, k));
   const double avf = fabs(vf);
   const double c1 = ld(m.ecoef + 2 * e), c2 = ld(m.ecoef + 2 * e + 1);
-  const int64_t q1 = int64_t(n1) * L + k, q2 = int64_t(n2) * L + k;
+  const uint32_t q1 = lq(n1, L, k), q2 = lq(n2, L, k);
   const int64_t ts = in.tstride;
   const int tg = in.tg;
   double T1[NTR], T2[NTR], O1[NTR], O2[NTR], g0[NTR], g1[NTR], g2[NTR], g3[NTR];
@@ -474,7 +481,7 @@ __device__ __forceinline__ void body_edge_adf(const Inst& in, int64_t i, int t0,
       cell_grad<NTR, IL>(in, up, k, t0, g0, g2);
       cell_grad<NTR, IL>(in, dn, k, t0, g1, g3);
     } else {
-      const int64_t qu = int64_t(up) * L + k, qd = int64_t(dn) * L + k;
+      const uint32_t qu = lq(up, L, k), qd = lq(dn, L, k);
       ldn<NTR, IL>(in.ws.gx, qu, w0, in.ws.sE, in.wtg, g0);
       ldn<NTR, IL>(in.ws.gx, qd, w0, in.ws.sE, in.wtg, g1);
       ldn<NTR, IL>(in.ws.gy, qu, w0, in.ws.sE, in.wtg, g2);
@@ -498,7 +505,7 @@ __device__ __forceinline__ void body_edge_adf(const Inst& in, int64_t i, int t0,
     const double ho = -0.5 * ((vf + avf) * Tm1 + (vf - avf) * Tm2);
     adf[t] = ho - fl;
   }
-  stn<NTR, IL>(in.ws.adfh, int64_t(e) * L + k, w0, in.ws.sEd, in.wtg, adf);
+  stn<NTR, IL>(in.ws.adfh, lq(e, L, k), w0, in.ws.sEd, in.wtg, adf);
 }
 
 // ------------------------ zalesak a2: element max/min of the LO/T window
@@ -508,9 +515,9 @@ __device__ __forceinline__ void body_elem_bounds(const Inst& in, int64_t i, int 
   if (i >= m.n_elem) return;
   const uint32_t lane = ld(m.elem_lanes + i);
   const int e = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const int64_t q[3] = {int64_t(ld(m.enodes + 3 * e)) * L + k,
-                        int64_t(ld(m.enodes + 3 * e + 1)) * L + k,
-                        int64_t(ld(m.enodes + 3 * e + 2)) * L + k};
+  const uint32_t q[3] = {lq(ld(m.enodes + 3 * e), L, k),
+                        lq(ld(m.enodes + 3 * e + 1), L, k),
+                        lq(ld(m.enodes + 3 * e + 2), L, k)};
   double mx[NTR], mn[NTR], hi[3][NTR], lw[3][NTR];
 #pragma unroll
   for (int t = 0; t < NTR; ++t) { mx[t] = -INFINITY; mn[t] = INFINITY; }
@@ -527,7 +534,7 @@ __device__ __forceinline__ void body_elem_bounds(const Inst& in, int64_t i, int 
       mn[t] = fmin(mn[t], lw[v][t]);
     }
   }
-  const int64_t qe = int64_t(e) * L + k;
+  const uint32_t qe = lq(e, L, k);
   {   // vertices attaining the bounds (the reverse pass splits cotangents evenly over them)
     int cx[NTR], cn[NTR];
 #pragma unroll
@@ -556,7 +563,7 @@ __device__ __forceinline__ void body_node_cluster(const Inst& in, int64_t i, int
   for (int j = c0; j < c1; ++j) {
     const int el = ld(m.nel_idx + j);
     if (k >= ld(m.eul + el) && k < ld(m.enl + el)) {
-      const int64_t q = int64_t(el) * L + k;
+      const uint32_t q = lq(el, L, k);
       double a[NTR], b[NTR];
       ldn<NTR, IL>(in.ws.amax, q, w0, in.ws.sE, in.wtg, a);
       ldn<NTR, IL>(in.ws.amin, q, w0, in.ws.sE, in.wtg, b);
@@ -573,7 +580,7 @@ __device__ __forceinline__ void body_node_cluster(const Inst& in, int64_t i, int
       }
     }
   }
-  const int64_t qn = int64_t(n) * L + k;
+  const uint32_t qn = lq(n, L, k);
   stn<NTR, IL>(in.ws.tvmax, qn, w0, in.ws.sN, in.wtg, mx);
   stn<NTR, IL>(in.ws.tvmin, qn, w0, in.ws.sN, in.wtg, mn);
   // cells attaining the cluster bounds (padded values included), for the reverse pass
@@ -584,7 +591,7 @@ __device__ __forceinline__ void body_node_cluster(const Inst& in, int64_t i, int
     const int el = ld(m.nel_idx + j);
     double a[NTR], b[NTR];
     if (k >= ld(m.eul + el) && k < ld(m.enl + el)) {
-      const int64_t q = int64_t(el) * L + k;
+      const uint32_t q = lq(el, L, k);
       ldn<NTR, IL>(in.ws.amax, q, w0, in.ws.sE, in.wtg, a);
       ldn<NTR, IL>(in.ws.amin, q, w0, in.ws.sE, in.wtg, b);
     } else {
@@ -609,7 +616,7 @@ __device__ __forceinline__ void body_node_factors(const Inst& in, int64_t i, int
   const uint32_t lane = ld(m.layer_lanes + i);
   const int n = lane_ent(lane), k = lane_lev(lane), L = m.L;
   const int nzmin = ld(m.nzmin + n), nzmax = ld(m.nzmax + n);
-  const int64_t base = int64_t(n) * L, qn = base + k;
+  const uint32_t base = lq(n, L, 0), qn = base + uint32_t(k);
   const bool use_own = (k == nzmin) || (k == nzmax - 1);
   const double av = ld(m.areasvol + qn), hnn = ld(in.hnode_new + qn);
   const bool valid = (av > 0.0) && (hnn > 0.0);
@@ -644,7 +651,7 @@ __device__ __forceinline__ void body_node_factors(const Inst& in, int64_t i, int
     const int idx = ld(m.ne_idx + j), e = idx >> 1;
     if (k < ld(m.ekmin + e) || k >= ld(m.ekmax + e)) continue;   // no flux on this level
     double a[NTR];
-    ldn<NTR, IL>(in.ws.adfh, int64_t(e) * L + k, w0, in.ws.sEd, in.wtg, a);
+    ldn<NTR, IL>(in.ws.adfh, lq(e, L, k), w0, in.ws.sEd, in.wtg, a);
 #pragma unroll
     for (int t = 0; t < NTR; ++t) {
       const double s = (idx & 1) ? -a[t] : a[t];
@@ -692,13 +699,13 @@ __device__ __forceinline__ void node_limit(const Inst& in, int64_t lane, bool co
   const int L = m.L;
   const int64_t sN = in.ws.sN;
   int n = 0, k = 0;
-  int64_t qn = 0;
+  uint32_t qn = 0;
   double mx[NTR], mn[NTR], sp[NTR], sm[NTR], lo[NTR];
   if (valid) {
     const uint32_t ln = ld(m.layer_lanes + lane);
     n = lane_ent(ln);
     k = lane_lev(ln);
-    qn = int64_t(n) * L + k;
+    qn = lq(n, L, k);
 #pragma unroll
     for (int t = 0; t < NTR; ++t) {
       mx[t] = -INFINITY; mn[t] = INFINITY; sp[t] = 0.0; sm[t] = 0.0;
@@ -717,9 +724,9 @@ __device__ __forceinline__ void node_limit(const Inst& in, int64_t lane, bool co
       off = off || !c1 || (has2 && !c2);
       const bool on = in_range(k, unsigned(sl.z));
       const bool second = sl.x & 1;
-      const int64_t qo = int64_t(sl.y) * L + k;
+      const uint32_t qo = lq(sl.y, L, k);
       double a[NTR], lv[NTR], tv[NTR];
-      ldn<NTR, IL>(in.ws.adfh, int64_t(sl.x >> 1) * L + k, w0, in.ws.sEd, in.wtg, a);
+      ldn<NTR, IL>(in.ws.adfh, lq(sl.x >> 1, L, k), w0, in.ws.sEd, in.wtg, a);
       ldn<NTR, IL>(in.ws.lo, qo, w0, sN, in.wtg, lv);
       ldn<NTR, IL>(in.T, qo, t0, in.tstride, in.tg, tv);
 #pragma unroll
@@ -792,7 +799,7 @@ __device__ __forceinline__ void body_node_final(const Inst& in, int64_t i, int t
   const uint32_t lane = ld(m.layer_lanes + i);
   const int n = lane_ent(lane), k = lane_lev(lane), L = m.L;
   const int nzmin = ld(m.nzmin + n), nzmax = ld(m.nzmax + n);
-  const int64_t base = int64_t(n) * L, qn = base + k;
+  const uint32_t base = lq(n, L, 0), qn = base + uint32_t(k);
   const double av = ld(m.areasvol + qn);
   const double sa = av > 0.0 ? av : 1.0;
   const double hn = ld(in.hnode + qn), hnn = ld(in.hnode_new + qn);
@@ -843,9 +850,9 @@ __device__ __forceinline__ void body_node_final(const Inst& in, int64_t i, int t
       const int4 sl = __ldg(m.ne4 + j);
       const bool on = in_range(k, unsigned(sl.z));
       const bool second = sl.x & 1;
-      const int64_t qo = int64_t(sl.y) * L + k;
+      const uint32_t qo = lq(sl.y, L, k);
       double a[NTR], pfo[NTR], mfo[NTR];
-      ldn<NTR, IL>(in.ws.adfh, int64_t(sl.x >> 1) * L + k, w0, in.ws.sEd, in.wtg, a);
+      ldn<NTR, IL>(in.ws.adfh, lq(sl.x >> 1, L, k), w0, in.ws.sEd, in.wtg, a);
       ldn<NTR, IL>(in.ws.pf, qo, w0, sN, in.wtg, pfo);
       ldn<NTR, IL>(in.ws.mf, qo, w0, sN, in.wtg, mfo);
 #pragma unroll
@@ -861,9 +868,9 @@ __device__ __forceinline__ void body_node_final(const Inst& in, int64_t i, int t
     for (int j = e0; j < e1; ++j) {
       const int idx = ld(m.ne_idx + j), e = idx >> 1;
       if (k < ld(m.ekmin + e) || k >= ld(m.ekmax + e)) continue;   // no flux on this level
-      const int64_t qo = int64_t(ld(m.ne_oth + j)) * L + k;
+      const uint32_t qo = lq(ld(m.ne_oth + j), L, k);
       double a[NTR], pfo[NTR], mfo[NTR];
-      ldn<NTR, IL>(in.ws.adfh, int64_t(e) * L + k, w0, in.ws.sEd, in.wtg, a);
+      ldn<NTR, IL>(in.ws.adfh, lq(e, L, k), w0, in.ws.sEd, in.wtg, a);
       ldn<NTR, IL>(in.ws.pf, qo, w0, sN, in.wtg, pfo);
       ldn<NTR, IL>(in.ws.mf, qo, w0, sN, in.wtg, mfo);
 #pragma unroll
@@ -904,7 +911,7 @@ __device__ __forceinline__ void body_vdiff(const Inst& in, int64_t n, int t0, in
   if (n >= m.N || !in.Kv) return;
   const int L = m.L;
   const int nzmin = ld(m.nzmin + n), nzmax = ld(m.nzmax + n);
-  const int64_t base = n * L;
+  const uint32_t base = lq(int(n), L, 0);
   const int64_t ts = in.tstride, sN = in.ws.sN;
   const int tg = in.tg;
   const double* Tin = in.vd_T;
@@ -925,7 +932,7 @@ __device__ __forceinline__ void body_vdiff(const Inst& in, int64_t n, int t0, in
   ldn<NTR, IL>(Tin, base + nzmin, t0, ts, tg, Tc);
   ldn<NTR, IL>(Tin, base + (nzmin > 0 ? nzmin - 1 : 0), t0, ts, tg, Tm);
   for (int k = nzmin; k < nzmax; ++k) {
-    const int64_t q = base + k;
+    const uint32_t q = base + uint32_t(k);
     const bool last = k + 1 >= L;
     if (last) {
 #pragma unroll
@@ -969,7 +976,7 @@ __device__ __forceinline__ void body_vdiff(const Inst& in, int64_t n, int t0, in
 #pragma unroll
   for (int t = 0; t < NTR; ++t) x[t] = 0.0;
   for (int k = nzmax - 1; k >= nzmin; --k) {
-    const int64_t q = base + k;
+    const uint32_t q = base + uint32_t(k);
     const double cp = in.ws.gnx[tix<IL>(q, w0, sN, in.wtg)];
     double dp[NTR], Tv[NTR];
     ldn<NTR, IL>(in.ws.lo, q, w0, sN, in.wtg, dp);
@@ -993,7 +1000,7 @@ __device__ __forceinline__ void body_copy_dry(const Inst& in, int64_t i) {
   split_dense(i, m.L, n, k);
   if (k >= m.nzmin[n] && k < m.nzmax[n]) return;
   for (int t = 0; t < in.ntr; ++t) {
-    const int64_t a = tix<IL>(i, t, in.tstride, in.tg);
+    const int64_t a = tix<IL>(uint32_t(i), t, in.tstride, in.tg);
     in.T_new[a] = in.T[a];
   }
 }
