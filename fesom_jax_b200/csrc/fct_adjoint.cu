@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(B) r_seed(Adj A) {
   const int64_t li = lane_index();
   if (li >= m.n_layer) return;
   const uint32_t lane = ld(m.layer_lanes + li);
-  const int64_t i = int64_t(lane_ent(lane)) * m.L + lane_lev(lane);
+  const uint32_t i = lq(lane_ent(lane), m.L, lane_lev(lane));
   const double hnn = ld(in.hnode_new + i), av = ld(m.areasvol + i);
   const double sa = av > 0.0 ? av : 1.0;
   for (int t = 0; t < in.ntr; ++t) {
@@ -152,7 +152,7 @@ __device__ __forceinline__ void factor_cotangents(const Adj& A, int t, int n, in
   const Inst& in = A.in;
   const DevMesh& m = *in.m;
   const int L = m.L;
-  const int64_t base = int64_t(n) * L, qn = base + k;
+  const uint32_t base = lq(n, L, 0), qn = base + uint32_t(k);
   const int e0 = ld(m.ne_off + n), e1 = ld(m.ne_off + n + 1);
   const int64_t o = t * in.ws.sN;
   const double* pf = in.ws.pf + o;
@@ -190,10 +190,10 @@ __device__ __forceinline__ void factor_cotangents(const Adj& A, int t, int n, in
     const int4 sl = __ldg(m.ne4 + j);
     const bool on = in_range(k, unsigned(sl.z));
     const bool second = sl.x & 1;
-    const int64_t qo = int64_t(sl.y) * L + k;
+    const uint32_t qo = lq(sl.y, L, k);
     const double ghsco = ghsc[qo];
     const double glim = second ? (ghsco - ghsc0) : (ghsc0 - ghsco);
-    const double a = adfh[int64_t(sl.x >> 1) * L + k];
+    const double a = adfh[lq(sl.x >> 1, L, k)];
     const double g_ae = glim * a;
     const double pfo = pf[qo], mfo = mf[qo];
     const double pf1 = second ? pfo : pfk, mf1 = second ? mfo : mfk;
@@ -229,7 +229,7 @@ __global__ void __launch_bounds__(B) r_ratio_window(Adj A) {
   const bool core = valid && tid >= 1 && tid <= B - 2;
   const int L = m.L;
   int n = 0, k = 0, nzmin = 0, nzmax = 0;
-  int64_t base = 0, qn = 0;
+  uint32_t base = 0, qn = 0;
   bool valid_n = false, use_own = true;
   Rcp rsa{1.0, 1.0, true}, rsh{1.0, 1.0, true};
   if (valid) {
@@ -238,8 +238,8 @@ __global__ void __launch_bounds__(B) r_ratio_window(Adj A) {
     k = lane_lev(ln);
     nzmin = ld(m.nzmin + n);
     nzmax = ld(m.nzmax + n);
-    base = int64_t(n) * L;
-    qn = base + k;
+    base = lq(n, L, 0);
+    qn = base + uint32_t(k);
     const double av = ld(m.areasvol + qn), hnn = ld(in.hnode_new + qn);
     valid_n = (av > 0.0) && (hnn > 0.0);
     rsa = rcp(av > 0.0 ? av : 1.0);
@@ -334,10 +334,10 @@ __global__ void __launch_bounds__(B) r_cluster(Adj A) {
   if (i >= m.n_elem) return;
   const uint32_t lane = ld(m.elem_lanes + i);
   const int e = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const int64_t qe = int64_t(e) * L + k;
-  const int64_t qv[3] = {int64_t(ld(m.enodes + 3 * e)) * L + k,
-                         int64_t(ld(m.enodes + 3 * e + 1)) * L + k,
-                         int64_t(ld(m.enodes + 3 * e + 2)) * L + k};
+  const uint32_t qe = lq(e, L, k);
+  const uint32_t qv[3] = {lq(ld(m.enodes + 3 * e), L, k),
+                         lq(ld(m.enodes + 3 * e + 1), L, k),
+                         lq(ld(m.enodes + 3 * e + 2), L, k)};
   for (int t = 0; t < in.ntr; ++t) {
     const int64_t o = t * in.ws.sN, oa = t * A.a.sN, oe = t * in.ws.sE;
     const double vx = in.ws.amax[oe + qe], vn = in.ws.amin[oe + qe];
@@ -370,7 +370,7 @@ __global__ void __launch_bounds__(B) r_bounds_lo(Adj A) {
   if (i >= m.n_layer) return;
   const uint32_t lane = ld(m.layer_lanes + i);
   const int n = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const int64_t qn = int64_t(n) * L + k;
+  const uint32_t qn = lq(n, L, k);
   const double hn = ld(in.hnode + qn), hnn = ld(in.hnode_new + qn), av = ld(m.areasvol + qn);
   const bool valid = (hnn > 0.0) && (av > 0.0);
   const int c0 = ld(m.nel_off + n), c1 = ld(m.nel_off + n + 1);
@@ -384,7 +384,7 @@ __global__ void __launch_bounds__(B) r_bounds_lo(Adj A) {
 #pragma unroll 2
     for (int j = c0; j < c1; ++j) {
       const bool on = in_range(k, unsigned(ld(m.nelr + j)));
-      const int64_t qe = int64_t(ld(m.nel_idx + j)) * L + k;
+      const uint32_t qe = lq(ld(m.nel_idx + j), L, k);
       const double ex = in.ws.amax[oe + qe], en = in.ws.amin[oe + qe];
       const double sx = A.a.gax[ae + qe], sn = A.a.gan[ae + qe];
       gx = (on && mxv == ex) ? gx + sx : gx;
@@ -422,11 +422,11 @@ __global__ void __launch_bounds__(B, 3) r_edge(Adj A) {
   const int e = lane_ent(lane), k = lane_lev(lane), L = m.L;
   const int n1 = ld(m.edges + 2 * e), n2 = ld(m.edges + 2 * e + 1);
   const bool use_tri = in_range(k, unsigned(ld(m.etr + e)));
-  const int64_t qe = int64_t(e) * L + k, q1 = int64_t(n1) * L + k, q2 = int64_t(n2) * L + k;
-  int64_t qa = q1, qb = q2;   // where the MFCT gradients are read
+  const uint32_t qe = lq(e, L, k), q1 = lq(n1, L, k), q2 = lq(n2, L, k);
+  uint32_t qa = q1, qb = q2;   // where the MFCT gradients are read
   if (use_tri) {
-    qa = int64_t(ld(m.eupdn + 2 * e)) * L + k;
-    qb = int64_t(ld(m.eupdn + 2 * e + 1)) * L + k;
+    qa = lq(ld(m.eupdn + 2 * e), L, k);
+    qb = lq(ld(m.eupdn + 2 * e + 1), L, k);
   }
   const double vf = ld(in.ws.vflux + qe), avf = fabs(vf), s = sgn(vf);
   const double c1 = ld(m.ecoef + 2 * e), c2 = ld(m.ecoef + 2 * e + 1);
@@ -502,7 +502,7 @@ __global__ void __launch_bounds__(B) r_gnode(Adj A) {
   if (i >= m.n_layer) return;
   const uint32_t lane = ld(m.layer_lanes + i);
   const int n = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const int64_t qn = int64_t(n) * L + k;
+  const uint32_t qn = lq(n, L, k);
   const int e0 = ld(m.ne_off + n), e1 = ld(m.ne_off + n + 1);
   for (int t = 0; t < in.ntr; ++t) {
     const int64_t oa = t * A.a.sN, oe = t * A.a.sEd;
@@ -513,7 +513,7 @@ __global__ void __launch_bounds__(B) r_gnode(Adj A) {
       const int e = sl.x >> 1;
       const bool on = in_range(k, unsigned(sl.z)) && !in_range(k, unsigned(ld(m.etr + e)));
       const bool second = sl.x & 1;
-      const double x = (second ? A.a.gX2 : A.a.gX1)[oe + int64_t(e) * L + k];
+      const double x = (second ? A.a.gX2 : A.a.gX1)[oe + lq(e, L, k)];
       const double c1 = ld(m.ecoef + 2 * e), c2 = ld(m.ecoef + 2 * e + 1);
       gx = on ? gx + c1 * x : gx;
       gy = on ? gy + c2 * x : gy;
@@ -536,7 +536,7 @@ __global__ void __launch_bounds__(B) r_vert(Adj A) {
   const uint32_t lane = ld(m.layer_lanes + i);
   const int n = lane_ent(lane), j = lane_lev(lane), L = m.L;
   const int nzmin = ld(m.nzmin + n), nzmax = ld(m.nzmax + n);
-  const int64_t base = int64_t(n) * L, qn = base + j;
+  const uint32_t base = lq(n, L, 0), qn = base + uint32_t(j);
   const double w = ld(in.w_e + qn), area = ld(m.area + qn);
   const int jm = j > 0 ? j - 1 : 0;
   const Rcp r3{3.0, 1.0 / 3.0, true};
@@ -613,9 +613,9 @@ __global__ void __launch_bounds__(B) r_tr(Adj A) {
   const int el = lane_ent(lane), k = lane_lev(lane), L = m.L;
   const double aw = ld(m.earea + el);
   const int u0 = ld(m.eud_off + el), u1 = ld(m.eud_off + el + 1);
-  const int64_t qv[3] = {int64_t(ld(m.enodes + 3 * el)) * L + k,
-                         int64_t(ld(m.enodes + 3 * el + 1)) * L + k,
-                         int64_t(ld(m.enodes + 3 * el + 2)) * L + k};
+  const uint32_t qv[3] = {lq(ld(m.enodes + 3 * el), L, k),
+                         lq(ld(m.enodes + 3 * el + 1), L, k),
+                         lq(ld(m.enodes + 3 * el + 2), L, k)};
   // the forward's (safe) node-average denominators of the three vertices
   const double dd[3] = {in.ws.nden[qv[0]], in.ws.nden[qv[1]], in.ws.nden[qv[2]]};
   for (int t = 0; t < in.ntr; ++t) {
@@ -626,7 +626,7 @@ __global__ void __launch_bounds__(B) r_tr(Adj A) {
       const int idx = ld(m.eud_idx + j), e = idx >> 1;
       const bool on = in_range(k, unsigned(ld(m.etr + e)));
       // the down (slot 1) / up (slot 0) cell's gradient enters Tm2 / Tm1
-      const double x = ((idx & 1) ? A.a.gX2 : A.a.gX1)[oe + int64_t(e) * L + k];
+      const double x = ((idx & 1) ? A.a.gX2 : A.a.gX1)[oe + lq(e, L, k)];
       const double c1 = ld(m.ecoef + 2 * e), c2 = ld(m.ecoef + 2 * e + 1);
       gx = on ? gx + c1 * x : gx;
       gy = on ? gy + c2 * x : gy;
@@ -636,8 +636,8 @@ __global__ void __launch_bounds__(B) r_tr(Adj A) {
       gx += A.a.ggnx[oa + qv[v]] * aw / dd[v];
       gy += A.a.ggny[oa + qv[v]] * aw / dd[v];
     }
-    A.a.gtrx[t * A.a.sE + int64_t(el) * L + k] = gx;
-    A.a.gtry[t * A.a.sE + int64_t(el) * L + k] = gy;
+    A.a.gtrx[t * A.a.sE + lq(el, L, k)] = gx;
+    A.a.gtry[t * A.a.sE + lq(el, L, k)] = gy;
   }
 }
 
@@ -655,7 +655,7 @@ __global__ void __launch_bounds__(B) r_final(Adj A) {
   if (li >= m.n_layer) return;
   const uint32_t lane = ld(m.layer_lanes + li);
   const int n = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const int64_t i = int64_t(n) * L + k;
+  const int64_t i = lq(n, L, k);
   const int nzmin = ld(m.nzmin + n), nzmax = ld(m.nzmax + n);
   const int e0 = ld(m.ne_off + n), e1 = ld(m.ne_off + n + 1);
   const int c0 = ld(m.nel_off + n), c1 = ld(m.nel_off + n + 1);
@@ -695,7 +695,7 @@ __global__ void __launch_bounds__(B) r_final(Adj A) {
       const unsigned r = unsigned(ld(m.nelr + j));
       const bool on = in_range(k, r);
       const int el = ld(m.nel_idx + j), iv = int((r >> 16) & 3u);
-      const int64_t qe = t * A.a.sE + int64_t(el) * L + k;
+      const int64_t qe = t * A.a.sE + lq(el, L, k);
       const double v = ld(m.gsca + 6 * el + iv) * A.a.gtrx[qe] +
                        ld(m.gsca + 6 * el + 3 + iv) * A.a.gtry[qe];
       gTtr = on ? gTtr + v : gTtr;
@@ -706,7 +706,7 @@ __global__ void __launch_bounds__(B) r_final(Adj A) {
       const int4 sl = __ldg(m.ne4 + j);
       const bool on = in_range(k, unsigned(sl.z));
       const bool second = sl.x & 1;
-      const int64_t q = t * A.a.sEd + int64_t(sl.x >> 1) * L + k;
+      const int64_t q = t * A.a.sEd + lq(sl.x >> 1, L, k);
       const double vT = (second ? A.a.gT2 : A.a.gT1)[q], vA = (second ? A.a.gA2 : A.a.gA1)[q];
       gT = on ? gT + vT : gT;
       gA = on ? gA + vA : gA;
@@ -739,7 +739,7 @@ __global__ void __launch_bounds__(B) r_uv(Adj A) {
       const int e = ent >> 1;
       const double* cr = m.cross + 4 * int64_t(e);
       double gvf = 0.0;
-      for (int t = 0; t < in.ntr; ++t) gvf += A.a.gvf[t * A.a.sEd + int64_t(e) * L + k];
+      for (int t = 0; t < in.ntr; ++t) gvf += A.a.gvf[t * A.a.sEd + lq(e, L, k)];
       if (ent & 1) {   // t2 = (V dx2 - U dy2) h
         gU += -gvf * ld(cr + 3) * h;
         gV += gvf * ld(cr + 2) * h;
@@ -797,7 +797,7 @@ __global__ void __launch_bounds__(B) r_w_uv(const DevMesh* __restrict__ mp,
       const int e = ent >> 1;
       const double* cr = m.cross + 4 * int64_t(e);
       // c = t1 - t2 is added to div at n1 and subtracted at n2
-      const double gc = gdiv[int64_t(m.edges[2 * e]) * L + k] - gdiv[int64_t(m.edges[2 * e + 1]) * L + k];
+      const double gc = gdiv[lq(m.edges[2 * e], L, k)] - gdiv[lq(m.edges[2 * e + 1], L, k)];
       if (ent & 1) {   // t2 = (V dx2 - U dy2) h enters c with a minus sign
         gV += -gc * cr[2] * h;
         gU += gc * cr[3] * h;

@@ -40,12 +40,6 @@ __device__ __forceinline__ int64_t lane_index() {
 template <class T>
 __device__ __forceinline__ T ld(const T* p) { return __ldg(p); }
 
-// Dense offset of entity-level (e, k): below 2^32 (entities < 2^25, L <= 128), so it is
-// computed in 32 bits (64-bit index products are multi-instruction sequences).
-__device__ __forceinline__ uint32_t lq(int e, int L, int k) {
-  return uint32_t(e) * uint32_t(L) + uint32_t(k);
-}
-
 // Address of tracer t at entity-level q: interleaved q*tg + t (below 2^32: the batch
 // engine checks every interleaved array against it), else t*stride + q.
 template <bool IL>

@@ -32,6 +32,12 @@ __host__ __device__ inline unsigned pack_tri(int ul1, int nl1, int ul2, int nl2)
   return unsigned(ul1) | (unsigned(nl1) << 8) | (unsigned(ul2) << 16) | (unsigned(nl2) << 24);
 }
 __host__ __device__ inline int lane_lev(uint32_t lane) { return int(lane & kLevelMask); }
+// Dense offset of entity-level (e, k): below 2^32 (entities < 2^25, L <= 128), so it is
+// computed in 32 bits (64-bit index products are multi-instruction sequences).
+__device__ __forceinline__ uint32_t lq(int e, int L, int k) {
+  return uint32_t(e) * uint32_t(L) + uint32_t(k);
+}
+
 // (entity, level) of a dense [entity, L] index: entity counts are below 2^25 and L <= 128,
 // so the index fits 32 bits and one 32-bit division splits it (a 64-bit integer division
 // is a long emulated sequence on the GPU).
