@@ -208,9 +208,10 @@ template <int NTR, bool IL, bool FUSED>
 __device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i, int t0, int w0) {
   const DevMesh& m = *in.m;
   if (i >= m.n_iface) return;
-  const uint32_t lane = ld(m.iface_lanes + i);
-  const int n = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const int nzmin = ld(m.nzmin + n), nzmax = ld(m.nzmax + n);
+  const int4 rec = __ldg(m.iface4 + i);
+  const unsigned pk = unsigned(rec.w);
+  const int n = lane_ent(uint32_t(rec.x)), k = lane_lev(uint32_t(rec.x)), L = m.L;
+  const int nzmin = int(pk & 255u), nzmax = int((pk >> 8) & 255u);
   const uint32_t base = lq(n, L, 0), qn = base + uint32_t(k);
   const bool layer = k < nzmax;
   const bool layer1 = (k + 1) < nzmax;
@@ -248,7 +249,7 @@ __device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i, int t0, 
     double div[NTR];
 #pragma unroll
     for (int t = 0; t < NTR; ++t) div[t] = 0.0;
-    const int e0 = ld(m.ne_off + n), e1 = ld(m.ne_off + n + 1);
+    const int e0 = rec.y, e1 = rec.y + int((pk >> 16) & 255u);
     if constexpr (FUSED) {
       // loads are unconditional (all in bounds) and inactive edges are selected away,
       // so consecutive slots' loads overlap
@@ -296,7 +297,7 @@ __device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i, int t0, 
     double nx[NTR], ny[NTR], den = 0.0;
 #pragma unroll
     for (int t = 0; t < NTR; ++t) nx[t] = ny[t] = 0.0;
-    const int c0 = ld(m.nel_off + n), c1 = ld(m.nel_off + n + 1);
+    const int c0 = rec.z, c1 = rec.z + int(pk >> 24);
     if constexpr (FUSED) {
       for (int j = c0; j < c1; ++j) {
         const unsigned r = unsigned(ld(m.nelr + j));
@@ -453,10 +454,10 @@ template <int NTR, bool IL, bool FUSED>
 __device__ __forceinline__ void body_edge_adf(const Inst& in, int64_t i, int t0, int w0) {
   const DevMesh& m = *in.m;
   if (i >= m.n_edge) return;
-  const uint32_t lane = ld(m.edge_lanes + i);
-  const int e = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const int n1 = ld(m.edges + 2 * e), n2 = ld(m.edges + 2 * e + 1);
-  const bool use_tri = in_range(k, unsigned(ld(m.etr + e)));
+  const int4 rec = __ldg(m.edge4 + i);
+  const int e = lane_ent(uint32_t(rec.x)), k = lane_lev(uint32_t(rec.x)), L = m.L;
+  const int n1 = rec.y, n2 = rec.z;
+  const bool use_tri = in_range(k, unsigned(rec.w));
   const double vf = ld(in.ws.vflux + lq(e, L, k));
   const double avf = fabs(vf);
   const double c1 = ld(m.ecoef + 2 * e), c2 = ld(m.ecoef + 2 * e + 1);
@@ -694,18 +695,20 @@ __device__ __forceinline__ void node_limit(const Inst& in, int64_t lane, bool co
   const int64_t sN = in.ws.sN;
   int n = 0, k = 0;
   uint32_t qn = 0;
+  unsigned pk = 0;
   double mx[NTR], mn[NTR], sp[NTR], sm[NTR], lo[NTR];
   if (valid) {
-    const uint32_t ln = ld(m.layer_lanes + lane);
-    n = lane_ent(ln);
-    k = lane_lev(ln);
+    const int4 rec = __ldg(m.layer4 + lane);
+    pk = unsigned(rec.w);
+    n = lane_ent(uint32_t(rec.x));
+    k = lane_lev(uint32_t(rec.x));
     qn = lq(n, L, k);
 #pragma unroll
     for (int t = 0; t < NTR; ++t) {
       mx[t] = -INFINITY; mn[t] = INFINITY; sp[t] = 0.0; sm[t] = 0.0;
     }
     bool own = false, off = false;
-    const int e0 = ld(m.ne_off + n), e1 = ld(m.ne_off + n + 1);
+    const int e0 = rec.y, e1 = rec.y + int((pk >> 16) & 255u);
 #pragma unroll 2
     for (int j = e0; j < e1; ++j) {
       const int4 sl = __ldg(m.ne4 + j);
@@ -751,7 +754,7 @@ __device__ __forceinline__ void node_limit(const Inst& in, int64_t lane, bool co
   }
   __syncthreads();
   if (!valid || !core) return;
-  const int nzmin = ld(m.nzmin + n), nzmax = ld(m.nzmax + n);
+  const int nzmin = int(pk & 255u), nzmax = int((pk >> 8) & 255u);
   if (k != nzmin && k != nzmax - 1) {   // interior: window over k-1, k, k+1 (lanes +-1)
 #pragma unroll
     for (int t = 0; t < NTR; ++t) {
@@ -790,9 +793,10 @@ template <int NTR, bool IL, bool FUSED>
 __device__ __forceinline__ void body_node_final(const Inst& in, int64_t i, int t0, int w0) {
   const DevMesh& m = *in.m;
   if (i >= m.n_layer) return;
-  const uint32_t lane = ld(m.layer_lanes + i);
-  const int n = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const int nzmin = ld(m.nzmin + n), nzmax = ld(m.nzmax + n);
+  const int4 rec = __ldg(m.layer4 + i);
+  const unsigned pk = unsigned(rec.w);
+  const int n = lane_ent(uint32_t(rec.x)), k = lane_lev(uint32_t(rec.x)), L = m.L;
+  const int nzmin = int(pk & 255u), nzmax = int((pk >> 8) & 255u);
   const uint32_t base = lq(n, L, 0), qn = base + uint32_t(k);
   const double av = ld(m.areasvol + qn);
   const double sa = av > 0.0 ? av : 1.0;
@@ -837,7 +841,7 @@ __device__ __forceinline__ void body_node_final(const Inst& in, int64_t i, int t
   double hsc[NTR];
 #pragma unroll
   for (int t = 0; t < NTR; ++t) hsc[t] = 0.0;
-  const int e0 = ld(m.ne_off + n), e1 = ld(m.ne_off + n + 1);
+  const int e0 = rec.y, e1 = rec.y + int((pk >> 16) & 255u);
   if constexpr (FUSED) {
 #pragma unroll 2
     for (int j = e0; j < e1; ++j) {

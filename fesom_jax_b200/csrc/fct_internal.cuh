@@ -96,6 +96,13 @@ struct DevMesh {
   const uint32_t* layer_lanes;  int64_t n_layer;   // nodes, k in [nzmin, nzmax)
   const uint32_t* edge_lanes;   int64_t n_edge;    // edges, k in the union of cell layers
   const uint32_t* elem_lanes;   int64_t n_elem;    // elements, k in [eul, enl)
+  // lane records of the fused kernels, one 16-byte load per thread:
+  //   node lanes {lane, first edge slot, first cell slot,
+  //               nzmin | nzmax << 8 | edge count << 16 | cell count << 24}
+  //   edge lanes {lane, n1, n2, etr of the edge}
+  const int4* iface4;
+  const int4* layer4;
+  const int4* edge4;
 };
 
 // Per-tracer intermediates of one instance (dense [entity, L]; tracer t at +t*stride).

@@ -323,6 +323,29 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
     for (int k = ekmin[e]; k < ekmax[e]; ++k)
       edgel.push_back((uint32_t(e) << kLevelBits) | uint32_t(k));
   P->n_wet_elem_layers = wet_elem;
+  // lane records (fct_internal.cuh): level range, CSR starts and degrees of a node lane,
+  // and the end nodes and triangle range of an edge lane, in one 16-byte word
+  auto node_rec = [&](uint32_t ln) -> int4 {
+    const int n = int(ln >> kLevelBits);
+    const int ed = ne_off[n + 1] - ne_off[n];
+    const int cd = d->nod_in_elem2D_offsets[n + 1] - d->nod_in_elem2D_offsets[n];
+    return make_int4(int(ln), ne_off[n], d->nod_in_elem2D_offsets[n],
+                     int(unsigned(nzmin[n]) | (unsigned(nzmax[n]) << 8) | (unsigned(ed) << 16) |
+                         (unsigned(cd) << 24)));
+  };
+  for (int n = 0; n < N; ++n) {
+    if (ne_off[n + 1] - ne_off[n] > 255 ||
+        d->nod_in_elem2D_offsets[n + 1] - d->nod_in_elem2D_offsets[n] > 255)
+      return set_error(FCT_ERR_INVALID, "node %d has more than 255 edges or cells", n);
+  }
+  std::vector<int4> iface4(std::max<size_t>(iface.size(), 1)), layer4(std::max<size_t>(layer.size(), 1));
+  for (size_t i = 0; i < iface.size(); ++i) iface4[i] = node_rec(iface[i]);
+  for (size_t i = 0; i < layer.size(); ++i) layer4[i] = node_rec(layer[i]);
+  std::vector<int4> edge4(std::max<size_t>(edgel.size(), 1));
+  for (size_t i = 0; i < edgel.size(); ++i) {
+    const int e = int(edgel[i] >> kLevelBits);
+    edge4[i] = make_int4(int(edgel[i]), d->edges[2 * e], d->edges[2 * e + 1], etr[e]);
+  }
 
   Blob b;
   const int nie = d->nod_in_elem2D_offsets[N];
@@ -350,6 +373,8 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   size_t o_Zp = b.add(Zp.data(), L), o_zbar = b.add(d->zbar, L);
   size_t o_if = b.add(iface.data(), iface.size()), o_ly = b.add(layer.data(), layer.size());
   size_t o_ed = b.add(edgel.data(), edgel.size()), o_el = b.add(eleml.data(), eleml.size());
+  size_t o_if4 = b.add(iface4.data(), iface4.size()), o_ly4 = b.add(layer4.data(), layer4.size());
+  size_t o_ed4 = b.add(edge4.data(), edge4.size());
 
   FCT_CUDA(cudaSetDevice(device));
   FCT_CUDA(cudaMalloc(&P->d_static, b.bytes.size()));
@@ -393,6 +418,9 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   m.layer_lanes = (const uint32_t*)(base + o_ly);  m.n_layer = int64_t(layer.size());
   m.edge_lanes = (const uint32_t*)(base + o_ed);   m.n_edge = int64_t(edgel.size());
   m.elem_lanes = (const uint32_t*)(base + o_el);   m.n_elem = int64_t(eleml.size());
+  m.iface4 = (const int4*)(base + o_if4);
+  m.layer4 = (const int4*)(base + o_ly4);
+  m.edge4 = (const int4*)(base + o_ed4);
   FCT_CUDA(cudaMalloc(&P->d_mesh, sizeof(DevMesh)));
   FCT_CUDA(cudaMemcpy(P->d_mesh, &m, sizeof(DevMesh), cudaMemcpyHostToDevice));
   return FCT_OK;
