@@ -148,12 +148,12 @@ __global__ void __launch_bounds__(B) r_dry(Adj A) {
 // (zalesak_limit b3, tracer_adv.py:453-465): the limited vertical fluxes at interfaces k
 // and k+1 and the limited horizontal fluxes of the incident edges in ascending edge id.
 __device__ __forceinline__ void factor_cotangents(const Adj& A, int t, int n, int k, int nzmin,
-                                                  int nzmax, double& gp, double& gm) {
+                                                  int nzmax, int e0, int e1, double& gp,
+                                                  double& gm) {
   const Inst& in = A.in;
   const DevMesh& m = *in.m;
   const int L = m.L;
   const uint32_t base = lq(n, L, 0), qn = base + uint32_t(k);
-  const int e0 = ld(m.ne_off + n), e1 = ld(m.ne_off + n + 1);
   const int64_t o = t * in.ws.sN;
   const double* pf = in.ws.pf + o;
   const double* mf = in.ws.mf + o;
@@ -228,16 +228,19 @@ __global__ void __launch_bounds__(B) r_ratio_window(Adj A) {
   const bool valid = lane >= 0 && lane < m.n_layer;
   const bool core = valid && tid >= 1 && tid <= B - 2;
   const int L = m.L;
-  int n = 0, k = 0, nzmin = 0, nzmax = 0;
+  int n = 0, k = 0, nzmin = 0, nzmax = 0, e0 = 0, e1 = 0;
   uint32_t base = 0, qn = 0;
   bool valid_n = false, use_own = true;
   Rcp rsa{1.0, 1.0, true}, rsh{1.0, 1.0, true};
   if (valid) {
-    const uint32_t ln = ld(m.layer_lanes + lane);
-    n = lane_ent(ln);
-    k = lane_lev(ln);
-    nzmin = ld(m.nzmin + n);
-    nzmax = ld(m.nzmax + n);
+    const int4 rec = __ldg(m.layer4 + lane);
+    const unsigned pk = unsigned(rec.w);
+    n = lane_ent(uint32_t(rec.x));
+    k = lane_lev(uint32_t(rec.x));
+    nzmin = int(pk & 255u);
+    nzmax = int((pk >> 8) & 255u);
+    e0 = rec.y;
+    e1 = rec.y + int((pk >> 16) & 255u);
     base = lq(n, L, 0);
     qn = base + uint32_t(k);
     const double av = ld(m.areasvol + qn), hnn = ld(in.hnode_new + qn);
@@ -254,7 +257,7 @@ __global__ void __launch_bounds__(B) r_ratio_window(Adj A) {
     double gtmax = 0.0, gtmin = 0.0;
     if (valid) {
       double gpf, gmf;
-      factor_cotangents(A, t, n, k, nzmin, nzmax, gpf, gmf);
+      factor_cotangents(A, t, n, k, nzmin, nzmax, e0, e1, gpf, gmf);
       double gplus = 0.0, gminus = 0.0;
       if (valid_n) {
         double tmax = tv[qn], tmin = tn[qn];
@@ -368,12 +371,13 @@ __global__ void __launch_bounds__(B) r_bounds_lo(Adj A) {
   const DevMesh& m = *in.m;
   const int64_t i = lane_index();
   if (i >= m.n_layer) return;
-  const uint32_t lane = ld(m.layer_lanes + i);
-  const int n = lane_ent(lane), k = lane_lev(lane), L = m.L;
+  const int4 rec = __ldg(m.layer4 + i);
+  const unsigned pk = unsigned(rec.w);
+  const int n = lane_ent(uint32_t(rec.x)), k = lane_lev(uint32_t(rec.x)), L = m.L;
   const uint32_t qn = lq(n, L, k);
   const double hn = ld(in.hnode + qn), hnn = ld(in.hnode_new + qn), av = ld(m.areasvol + qn);
   const bool valid = (hnn > 0.0) && (av > 0.0);
-  const int c0 = ld(m.nel_off + n), c1 = ld(m.nel_off + n + 1);
+  const int c0 = rec.z, c1 = rec.z + int(pk >> 24);
   for (int t = 0; t < in.ntr; ++t) {
     const int64_t o = t * in.ws.sN, oa = t * A.a.sN, oe = t * in.ws.sE, ae = t * A.a.sE;
     const double lo = in.ws.lo[o + qn], T = ld(in.T + t * in.tstride + qn);
@@ -418,10 +422,10 @@ __global__ void __launch_bounds__(B, 3) r_edge(Adj A) {
   const DevMesh& m = *in.m;
   const int64_t i = lane_index();
   if (i >= m.n_edge) return;
-  const uint32_t lane = ld(m.edge_lanes + i);
-  const int e = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const int n1 = ld(m.edges + 2 * e), n2 = ld(m.edges + 2 * e + 1);
-  const bool use_tri = in_range(k, unsigned(ld(m.etr + e)));
+  const int4 rec = __ldg(m.edge4 + i);
+  const int e = lane_ent(uint32_t(rec.x)), k = lane_lev(uint32_t(rec.x)), L = m.L;
+  const int n1 = rec.y, n2 = rec.z;
+  const bool use_tri = in_range(k, unsigned(rec.w));
   const uint32_t qe = lq(e, L, k), q1 = lq(n1, L, k), q2 = lq(n2, L, k);
   uint32_t qa = q1, qb = q2;   // where the MFCT gradients are read
   if (use_tri) {
@@ -500,10 +504,11 @@ __global__ void __launch_bounds__(B) r_gnode(Adj A) {
   const DevMesh& m = *in.m;
   const int64_t i = lane_index();
   if (i >= m.n_layer) return;
-  const uint32_t lane = ld(m.layer_lanes + i);
-  const int n = lane_ent(lane), k = lane_lev(lane), L = m.L;
+  const int4 rec = __ldg(m.layer4 + i);
+  const unsigned pk = unsigned(rec.w);
+  const int n = lane_ent(uint32_t(rec.x)), k = lane_lev(uint32_t(rec.x)), L = m.L;
   const uint32_t qn = lq(n, L, k);
-  const int e0 = ld(m.ne_off + n), e1 = ld(m.ne_off + n + 1);
+  const int e0 = rec.y, e1 = rec.y + int((pk >> 16) & 255u);
   for (int t = 0; t < in.ntr; ++t) {
     const int64_t oa = t * A.a.sN, oe = t * A.a.sEd;
     double gx = 0.0, gy = 0.0;
@@ -533,9 +538,10 @@ __global__ void __launch_bounds__(B) r_vert(Adj A) {
   const DevMesh& m = *in.m;
   const int64_t i = lane_index();
   if (i >= m.n_layer) return;
-  const uint32_t lane = ld(m.layer_lanes + i);
-  const int n = lane_ent(lane), j = lane_lev(lane), L = m.L;
-  const int nzmin = ld(m.nzmin + n), nzmax = ld(m.nzmax + n);
+  const int4 rec = __ldg(m.layer4 + i);
+  const unsigned pk = unsigned(rec.w);
+  const int n = lane_ent(uint32_t(rec.x)), j = lane_lev(uint32_t(rec.x)), L = m.L;
+  const int nzmin = int(pk & 255u), nzmax = int((pk >> 8) & 255u);
   const uint32_t base = lq(n, L, 0), qn = base + uint32_t(j);
   const double w = ld(in.w_e + qn), area = ld(m.area + qn);
   const int jm = j > 0 ? j - 1 : 0;
@@ -653,12 +659,13 @@ __global__ void __launch_bounds__(B) r_final(Adj A) {
   const DevMesh& m = *in.m;
   const int64_t li = lane_index();
   if (li >= m.n_layer) return;
-  const uint32_t lane = ld(m.layer_lanes + li);
-  const int n = lane_ent(lane), k = lane_lev(lane), L = m.L;
+  const int4 rec = __ldg(m.layer4 + li);
+  const unsigned pk = unsigned(rec.w);
+  const int n = lane_ent(uint32_t(rec.x)), k = lane_lev(uint32_t(rec.x)), L = m.L;
   const int64_t i = lq(n, L, k);
-  const int nzmin = ld(m.nzmin + n), nzmax = ld(m.nzmax + n);
-  const int e0 = ld(m.ne_off + n), e1 = ld(m.ne_off + n + 1);
-  const int c0 = ld(m.nel_off + n), c1 = ld(m.nel_off + n + 1);
+  const int nzmin = int(pk & 255u), nzmax = int((pk >> 8) & 255u);
+  const int e0 = rec.y, e1 = rec.y + int((pk >> 16) & 255u);
+  const int c0 = rec.z, c1 = rec.z + int(pk >> 24);
   for (int t = 0; t < in.ntr; ++t) {
     const int64_t oa = t * A.a.sN;
     const double* gfv = A.a.gfv + oa;

@@ -549,9 +549,9 @@ template <int NTR, bool IL>
 __device__ __forceinline__ void body_node_cluster(const Inst& in, int64_t i, int t0, int w0) {
   const DevMesh& m = *in.m;
   if (i >= m.n_layer) return;
-  const uint32_t lane = ld(m.layer_lanes + i);
-  const int n = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const int c0 = ld(m.nel_off + n), c1 = ld(m.nel_off + n + 1);
+  const int4 rec = __ldg(m.layer4 + i);
+  const int n = lane_ent(uint32_t(rec.x)), k = lane_lev(uint32_t(rec.x)), L = m.L;
+  const int c0 = rec.z, c1 = rec.z + int(unsigned(rec.w) >> 24);
   double mx[NTR], mn[NTR];
 #pragma unroll
   for (int t = 0; t < NTR; ++t) { mx[t] = -INFINITY; mn[t] = INFINITY; }
@@ -608,9 +608,10 @@ template <int NTR, bool IL>
 __device__ __forceinline__ void body_node_factors(const Inst& in, int64_t i, int t0, int w0) {
   const DevMesh& m = *in.m;
   if (i >= m.n_layer) return;
-  const uint32_t lane = ld(m.layer_lanes + i);
-  const int n = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const int nzmin = ld(m.nzmin + n), nzmax = ld(m.nzmax + n);
+  const int4 rec = __ldg(m.layer4 + i);
+  const unsigned pk = unsigned(rec.w);
+  const int n = lane_ent(uint32_t(rec.x)), k = lane_lev(uint32_t(rec.x)), L = m.L;
+  const int nzmin = int(pk & 255u), nzmax = int((pk >> 8) & 255u);
   const uint32_t base = lq(n, L, 0), qn = base + uint32_t(k);
   const bool use_own = (k == nzmin) || (k == nzmax - 1);
   const double av = ld(m.areasvol + qn), hnn = ld(in.hnode_new + qn);
@@ -641,7 +642,7 @@ __device__ __forceinline__ void body_node_factors(const Inst& in, int64_t i, int
   double sp[NTR], sm[NTR];
 #pragma unroll
   for (int t = 0; t < NTR; ++t) sp[t] = sm[t] = 0.0;
-  const int e0 = ld(m.ne_off + n), e1 = ld(m.ne_off + n + 1);
+  const int e0 = rec.y, e1 = rec.y + int((pk >> 16) & 255u);
   for (int j = e0; j < e1; ++j) {
     const int idx = ld(m.ne_idx + j), e = idx >> 1;
     if (k < ld(m.ekmin + e) || k >= ld(m.ekmax + e)) continue;   // no flux on this level
