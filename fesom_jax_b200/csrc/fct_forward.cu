@@ -471,11 +471,12 @@ __device__ __forceinline__ void body_edge_adf(const Inst& in, int64_t i, int t0,
   ldn<NTR, IL>(in.T_old, q2, t0, ts, tg, O2);
   if (use_tri) {
     // both cells are wet at k here (k is above every adjacent cell's bottom)
-    const int up = ld(m.eupdn + 2 * e), dn = ld(m.eupdn + 2 * e + 1);
     if constexpr (FUSED) {
-      cell_grad<NTR, IL>(in, up, k, t0, g0, g2);
-      cell_grad<NTR, IL>(in, dn, k, t0, g1, g3);
+      const int4 cu = __ldg(m.eud4 + 2 * e), cd = __ldg(m.eud4 + 2 * e + 1);
+      cell_grad<NTR, IL>(in, cu.x, cu.y, cu.z, cu.w, k, t0, g0, g2);
+      cell_grad<NTR, IL>(in, cd.x, cd.y, cd.z, cd.w, k, t0, g1, g3);
     } else {
+      const int up = ld(m.eupdn + 2 * e), dn = ld(m.eupdn + 2 * e + 1);
       const uint32_t qu = lq(up, L, k), qd = lq(dn, L, k);
       ldn<NTR, IL>(in.ws.gx, qu, w0, in.ws.sE, in.wtg, g0);
       ldn<NTR, IL>(in.ws.gx, qd, w0, in.ws.sE, in.wtg, g1);

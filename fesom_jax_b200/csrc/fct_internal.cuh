@@ -103,6 +103,9 @@ struct DevMesh {
   const int4* iface4;
   const int4* layer4;
   const int4* edge4;
+  // per edge, its MFCT up and down cells with their vertices: [2e] = {up, v0, v1, v2},
+  // [2e+1] = {dn, v0, v1, v2} (zeros where the cell is missing)
+  const int4* eud4;
 };
 
 // Per-tracer intermediates of one instance (dense [entity, L]; tracer t at +t*stride).

@@ -341,6 +341,13 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   std::vector<int4> iface4(std::max<size_t>(iface.size(), 1)), layer4(std::max<size_t>(layer.size(), 1));
   for (size_t i = 0; i < iface.size(); ++i) iface4[i] = node_rec(iface[i]);
   for (size_t i = 0; i < layer.size(); ++i) layer4[i] = node_rec(layer[i]);
+  std::vector<int4> eud4(2 * size_t(Ed));
+  for (int e = 0; e < Ed; ++e)
+    for (int r = 0; r < 2; ++r) {
+      const int el = d->edge_up_dn_tri[2 * e + r];
+      const int* en = d->elem_nodes + 3 * size_t(el >= 0 ? el : 0);
+      eud4[2 * size_t(e) + r] = el >= 0 ? make_int4(el, en[0], en[1], en[2]) : make_int4(0, 0, 0, 0);
+    }
   std::vector<int4> edge4(std::max<size_t>(edgel.size(), 1));
   for (size_t i = 0; i < edgel.size(); ++i) {
     const int e = int(edgel[i] >> kLevelBits);
@@ -375,6 +382,7 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   size_t o_ed = b.add(edgel.data(), edgel.size()), o_el = b.add(eleml.data(), eleml.size());
   size_t o_if4 = b.add(iface4.data(), iface4.size()), o_ly4 = b.add(layer4.data(), layer4.size());
   size_t o_ed4 = b.add(edge4.data(), edge4.size());
+  size_t o_eud4 = b.add(eud4.data(), eud4.size());
 
   FCT_CUDA(cudaSetDevice(device));
   FCT_CUDA(cudaMalloc(&P->d_static, b.bytes.size()));
@@ -421,6 +429,7 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   m.iface4 = (const int4*)(base + o_if4);
   m.layer4 = (const int4*)(base + o_ly4);
   m.edge4 = (const int4*)(base + o_ed4);
+  m.eud4 = (const int4*)(base + o_eud4);
   FCT_CUDA(cudaMalloc(&P->d_mesh, sizeof(DevMesh)));
   FCT_CUDA(cudaMemcpy(P->d_mesh, &m, sizeof(DevMesh), cudaMemcpyHostToDevice));
   return FCT_OK;
