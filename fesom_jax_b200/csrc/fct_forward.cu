@@ -91,22 +91,28 @@ __device__ __forceinline__ void stc(uint8_t* __restrict__ p, uint32_t q, int t0,
   for (int i = 0; i < NTR; ++i) p[tix<IL>(q, t0 + i, stride, tg)] = uint8_t(v[i]);
 }
 
+// k in [r & 255, (r >> 8) & 255): the packed level ranges of the fused stages' slots
+__device__ __forceinline__ bool in_range(int k, unsigned r) {
+  return k >= int(r & 255u) && k < int((r >> 8) & 255u);
+}
+
 // ---------------------------------------------------------------- edge_vflux
 __device__ __forceinline__ void body_vflux(const Inst& in, int64_t i) {
   const DevMesh& m = *in.m;
   if (i >= m.n_edge) return;
   const uint32_t lane = ld(m.edge_lanes + i);
   const int e = lane_ent(lane), k = lane_lev(lane), L = m.L;
-  const int el1 = ld(m.etri + 2 * e), el2 = ld(m.etri + 2 * e + 1);
+  const int4 ec = __ldg(m.ecell4 + e);   // cells and their layer ranges in one load
+  const unsigned tr = unsigned(ec.z);
   const double* cr = m.cross + 4 * int64_t(e);
   double t1 = 0.0, t2 = 0.0;
-  if (k >= ld(m.eul + el1) && k < ld(m.enl + el1)) {
-    const uint32_t q = lq(el1, L, k);
+  if (in_range(k, tr & 0xffffu)) {
+    const uint32_t q = lq(ec.x, L, k);
     const double2 U = __ldg(reinterpret_cast<const double2*>(in.uv) + q);
     t1 = (U.x * ld(cr + 1) - U.y * ld(cr + 0)) * ld(in.helem + q);
   }
-  if (el2 >= 0 && k >= ld(m.eul + el2) && k < ld(m.enl + el2)) {
-    const uint32_t q = lq(el2, L, k);
+  if (((tr >> 16) & 255u) != kNoCell && in_range(k, tr >> 16)) {
+    const uint32_t q = lq(ec.y, L, k);
     const double2 U = __ldg(reinterpret_cast<const double2*>(in.uv) + q);
     t2 = (U.y * ld(cr + 2) - U.x * ld(cr + 3)) * ld(in.helem + q);
   }
@@ -176,10 +182,6 @@ __device__ __forceinline__ void cell_grad(const Inst& in, int el, int k, int t0,
   cell_grad<NTR, IL>(in, el, ld(en), ld(en + 1), ld(en + 2), k, t0, gx, gy);
 }
 
-// k in [r & 255, (r >> 8) & 255): the packed level ranges of the fused stages' slots
-__device__ __forceinline__ bool in_range(int k, unsigned r) {
-  return k >= int(r & 255u) && k < int((r >> 8) & 255u);
-}
 
 template <int NTR, bool IL>
 __device__ __forceinline__ void body_elem_grad(const Inst& in, int64_t i, int t0, int w0) {
@@ -301,8 +303,8 @@ __device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i, int t0, 
     if constexpr (FUSED) {
       for (int j = c0; j < c1; ++j) {
         const unsigned r = unsigned(ld(m.nelr + j));
+        const int4 sl = __ldg(m.nel4 + j);   // in bounds: issued beside the range word
         if (!in_range(k, r)) continue;
-        const int4 sl = __ldg(m.nel4 + j);
         const double a = ld(m.earea + sl.x);
         double gx[NTR], gy[NTR];
         cell_grad_own<NTR, IL>(in, sl.x, sl.y, sl.z, sl.w, int((r >> 16) & 3u), Tc, k, t0, gx,

@@ -106,6 +106,9 @@ struct DevMesh {
   // per edge, its MFCT up and down cells with their vertices: [2e] = {up, v0, v1, v2},
   // [2e+1] = {dn, v0, v1, v2} (zeros where the cell is missing)
   const int4* eud4;
+  // per edge, its two cells and their layer ranges: {el1, el2 (-1 on a coast),
+  // ranges packed as in the node->edge slots (pack_tri), 0}
+  const int4* ecell4;
 };
 
 // Per-tracer intermediates of one instance (dense [entity, L]; tracer t at +t*stride).

@@ -348,6 +348,13 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
       const int* en = d->elem_nodes + 3 * size_t(el >= 0 ? el : 0);
       eud4[2 * size_t(e) + r] = el >= 0 ? make_int4(el, en[0], en[1], en[2]) : make_int4(0, 0, 0, 0);
     }
+  std::vector<int4> ecell4(static_cast<size_t>(Ed));
+  for (int e = 0; e < Ed; ++e) {
+    const int el1 = d->edge_tri[2 * e], el2 = d->edge_tri[2 * e + 1];
+    const unsigned tri = el2 >= 0 ? pack_tri(eul[el1], enl[el1], eul[el2], enl[el2])
+                                  : pack_tri(eul[el1], enl[el1], int(kNoCell), 0);
+    ecell4[e] = make_int4(el1, el2, int(tri), 0);
+  }
   std::vector<int4> edge4(std::max<size_t>(edgel.size(), 1));
   for (size_t i = 0; i < edgel.size(); ++i) {
     const int e = int(edgel[i] >> kLevelBits);
@@ -383,6 +390,7 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   size_t o_if4 = b.add(iface4.data(), iface4.size()), o_ly4 = b.add(layer4.data(), layer4.size());
   size_t o_ed4 = b.add(edge4.data(), edge4.size());
   size_t o_eud4 = b.add(eud4.data(), eud4.size());
+  size_t o_ecell4 = b.add(ecell4.data(), ecell4.size());
 
   FCT_CUDA(cudaSetDevice(device));
   FCT_CUDA(cudaMalloc(&P->d_static, b.bytes.size()));
@@ -430,6 +438,7 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   m.layer4 = (const int4*)(base + o_ly4);
   m.edge4 = (const int4*)(base + o_ed4);
   m.eud4 = (const int4*)(base + o_eud4);
+  m.ecell4 = (const int4*)(base + o_ecell4);
   FCT_CUDA(cudaMalloc(&P->d_mesh, sizeof(DevMesh)));
   FCT_CUDA(cudaMemcpy(P->d_mesh, &m, sizeof(DevMesh), cudaMemcpyHostToDevice));
   return FCT_OK;
