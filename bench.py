@@ -35,9 +35,9 @@ UNIT = "node-level updates/s"
 FALLBACK_HBM_GBS = 6650.0
 # DRAM bytes (read + write) per node-level update of the four fused tracer kernels, from
 # one ncu capture of the small case of the batched workload (2 members x 8 tracers of the
-# CORE2-size mesh: 12.41 GB per FCT step / 48.76 M updates); the tracer-independent volume
-# flux kernel (2.6% of the step) is not included. Scaled to a launch by the updates it does.
-TRAFFIC_B_PER_UPDATE = 254.6
+# CORE2-size mesh: 12.81 GB per FCT step / 48.76 M updates); the tracer-independent volume
+# flux kernel (1.9% of the step) is not included. Scaled to a launch by the updates it does.
+TRAFFIC_B_PER_UPDATE = 262.6
 
 
 def peaks() -> dict:
