@@ -290,7 +290,9 @@ typedef struct FctBatch FctBatch;
 
 /* Group the instances so that each group's workspace fits ``workspace_budget_bytes``
  * (at least one instance per group), allocate one workspace arena (reused by the groups
- * in turn) and the per-phase device instance tables. */
+ * in turn) and the per-phase device instance tables. An instance's interleaved arrays
+ * (max(nod2D, elem2D, edge2D) x nl x ntr elements) must hold fewer than 2^32 elements
+ * (FCT_ERR_CAPACITY otherwise; the same holds for fct_serve_step). */
 int fct_batch_create(const FctInstance* insts, int n, int64_t workspace_budget_bytes,
                      FctBatch** out);
 int fct_batch_destroy(FctBatch* b);

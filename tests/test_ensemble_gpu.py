@@ -147,3 +147,23 @@ def test_derived_w_equals_compute_w_then_fct(torch, pi):
     Tb, Tob = ens.state(0)
     assert np.array_equal(Tb.cpu().numpy(), T) and np.array_equal(Tob.cpu().numpy(), To)
     ens.close()
+
+
+def test_batch_rejects_interleaved_arrays_beyond_2_32(torch, pi):
+    """The kernels index interleaved [entity, nl, tracers] arrays in 32 bits: a batch whose
+    instance would need 2^32 or more elements in one is refused while validating (the
+    placeholder field pointers are never dereferenced)."""
+    import ctypes as C
+    from fesom_jax_b200 import _lib
+    from fesom_jax_b200.ensemble import FctInstance, _bind_batch
+    from fesom_jax_b200.tracer_adv import get_plan
+    L = _bind_batch(_lib.lib())
+    plan = get_plan(pi, 0)
+    p = 1 << 20
+    ntr = 10000   # 8986 edges x 48 levels x 10000 tracers > 2^32
+    arr = (FctInstance * 1)(FctInstance(plan.handle.value, p, p, p, p, p,
+                                        (C.c_void_p * 3)(p, p, p), ntr, 1800.0, None, None))
+    h = C.c_void_p()
+    st = L.fct_batch_create(arr, 1, 1 << 34, C.byref(h))
+    assert st == -3 and not h.value
+    assert "2^32" in L.fct_last_error().decode()
