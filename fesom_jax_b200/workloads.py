@@ -16,7 +16,7 @@ from . import inputs as I
 from .mesh import Mesh, pi_mesh
 
 WORKLOADS = {
-    # name: mesh + member layout
+    # name: mesh + member layout of each benchmark workload
     "pi": dict(n_nodes=None, nl=48, members=1, ntr=2, fct_steps=1, dt=3600.0, sigma=0.1,
                n_vortices=0, bottom=None),
     "batched": dict(n_nodes=127000, nl=48, members=32, ntr=8, fct_steps=30, dt=1800.0,
