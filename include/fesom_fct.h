@@ -14,7 +14,8 @@
  *
  * Every entry point returns FCT_OK (0) or a negative FctStatus; the message of the
  * last failure on the calling thread is returned by fct_last_error().
- * No entry point except fct_plan_create / fct_plan_reserve / fct_batch_create
+ * No entry point except fct_plan_create / fct_plan_reserve / fct_plan_reserve_adjoint /
+ * fct_batch_create / fct_serve_create / fct_tape_create (without caller memory)
  * allocates device memory, and none synchronises the stream it is given.
  */
 #ifndef FESOM_FCT_H
