@@ -83,3 +83,30 @@ def test_plan_create_rejects_too_many_levels(pi):
     h = ctypes.c_void_p()
     st = _lib.lib().fct_plan_create(ctypes.byref(desc), 0, 1, ctypes.byref(h))
     assert st == -1 and b"nl=129" in _lib.lib().fct_last_error()
+
+
+def _header_define(name):
+    text = (ROOT / "include" / "fesom_fct.h").read_text()
+    m = re.search(r"^#define\s+" + name + r"\s+(\d+)", text, re.M)
+    assert m, name
+    return int(m.group(1))
+
+
+def test_xla_opaque_and_buffer_layout_agree_with_the_header():
+    """The custom-call opaque struct (uint64 plan, double dt, int32 ntr, int32 flags) is 24
+    bytes in the header, in fesom_jax_b200.xla and in the struct.pack format a JAX binding
+    uses; the status result indices and flags match the header's."""
+    import struct
+    from fesom_jax_b200 import xla
+    assert ctypes.sizeof(xla.FctXlaOpaque) == 24 == struct.calcsize("<Qdii")
+    o = xla.FctXlaOpaque(0x1234, 1800.0, 3, xla.Z3D | xla.WI)
+    assert bytes(memoryview(o)) == struct.pack("<Qdii", 0x1234, 1800.0, 3, 3)
+    assert xla.FWD_STATUS == _header_define("FCT_XLA_FWD_STATUS") == 11
+    assert xla.ADJ_STATUS == _header_define("FCT_XLA_ADJ_STATUS") == 14
+    assert (xla.Z3D, xla.WI) == (_header_define("FCT_XLA_Z3D"), _header_define("FCT_XLA_WI"))
+
+
+def test_adjoint_accumulate_bits_agree_with_the_header():
+    from fesom_jax_b200.adjoint import ACC_T, ACC_T_OLD, ACC_UV, ACC_W
+    assert (ACC_T, ACC_T_OLD, ACC_UV, ACC_W) == tuple(
+        _header_define(n) for n in ("FCT_ACC_T", "FCT_ACC_T_OLD", "FCT_ACC_UV", "FCT_ACC_W"))
