@@ -66,3 +66,21 @@ def test_stretched_zbar():
     assert z.shape == (70,) and z[0] == 0.0 and abs(z[-1] + 6000.0) < 1e-6
     dz = -np.diff(z)
     assert np.all(dz > 0) and np.all(np.diff(dz) > 0) and abs(dz[0] - 5.0) < 0.5
+
+
+def test_node_orders_renumber_the_same_mesh():
+    """rcm, raw and random orders number the same ocean: the same counts and wet layers, a
+    valid mesh each, local neighbours for rcm and the Fibonacci order, not for a shuffle."""
+    import numpy as np
+    from fesom_jax_b200.meshgen import make_mesh
+    spans = {}
+    meshes = {}
+    for order in ("rcm", "raw", "random"):
+        m = make_mesh(3000, nl=12, seed=4, bottom=(4, None), node_order=order)
+        meshes[order] = m
+        spans[order] = float(np.median(np.abs(m.edges[:, 0] - m.edges[:, 1])))
+    counts = {(m.nod2D, m.elem2D, m.edge2D, m.n_wet_layers) for m in meshes.values()}
+    assert len(counts) == 1
+    assert spans["rcm"] < 0.1 * spans["random"] and spans["raw"] < 0.1 * spans["random"]
+    with pytest.raises(ValueError, match="node_order"):
+        make_mesh(300, nl=12, seed=4, node_order="hilbert")
