@@ -38,6 +38,12 @@ FALLBACK_HBM_GBS = 6650.0
 # CORE2-size mesh: 12.81 GB per FCT step / 48.76 M updates); the tracer-independent volume
 # flux kernel (1.9% of the step) is not included. Scaled to a launch by the updates it does.
 TRAFFIC_B_PER_UPDATE = 262.6
+# Warp-instructions per node-level update of the same four kernels in the same capture
+# (smsp__inst_executed.sum / updates). The kernels are latency- and issue-limited rather
+# than HBM-bound, so the line also reports this issue-rate fraction beside the HBM one:
+# achieved warp-instructions/s against 148 SMs x 4 schedulers x the sampled SM clock.
+WARP_INST_PER_UPDATE = 99.2
+B200_SMS, SCHEDULERS_PER_SM = 148, 4
 
 
 def peaks() -> dict:
@@ -46,6 +52,20 @@ def peaks() -> dict:
         d = json.loads(p.read_text())
         return dict(hbm_gbs=float(d["hbm_gbs"]), source="measured")
     return dict(hbm_gbs=FALLBACK_HBM_GBS, source="fallback")
+
+
+def issue_roofline(updates_per_s: float, clk) -> dict:
+    """Instruction-issue fraction of the batched step: warp-instructions per update (ncu
+    capture constant) x updates/s against every scheduler issuing one per cycle at the
+    median SM clock sampled in the timed region (max clock when unsampled). The step
+    time includes the tracer-independent volume-flux kernel, so this is a slight
+    underestimate."""
+    mhz = (clk or {}).get("sm_mhz") or (clk or {}).get("sm_max_mhz") or 1965.0
+    peak = B200_SMS * SCHEDULERS_PER_SM * float(mhz) * 1e6 / 1e9
+    achieved = WARP_INST_PER_UPDATE * updates_per_s / 1e9
+    return dict(achieved=achieved, peak=peak, unit="G warp-instructions/s",
+                frac=achieved / peak, warp_inst_per_update=WARP_INST_PER_UPDATE,
+                sm_mhz=float(mhz))
 
 
 # ------------------------------------------------------------------------- clocks
@@ -273,7 +293,8 @@ def run_ours(args, D: Dist) -> dict | None:
                              traffic=TRAFFIC_B_PER_UPDATE * info["updates_per_step"],
                              traffic_note="ncu DRAM bytes of the 4 tracer kernels, small-case "
                                           "capture scaled by updates",
-                             alg_bytes_per_step=alg),
+                             alg_bytes_per_step=alg,
+                             issue=issue_roofline(value / D.world, clk)),
                gpu_launches=n_kernels * S * args.steps,
                tuning=dict(chunk=ens.chunk, candidates_ms_per_2_steps=tune))
 
