@@ -202,6 +202,69 @@ def cpu_oracle_rate(mesh, fields_host, ntr: int, dt: float, min_seconds: float =
                        f"FCT step) on {mesh.name}, {t_total:.1f} s")
 
 
+# ------------------------------------------------------------------ correctness gates
+# per-step parity of the CUDA path against the oracle (max-norm over wet lanes, relative)
+GATE_RTOL = 1e-12
+# budget closure residual relative to the tracer content
+GATE_CLOSURE_RTOL = 1e-13
+
+
+def run_gates(ens, mesh, cfg, plan, member: int = 0) -> dict:
+    """The per-run correctness gates on one member, after the timed region: one more
+    batched FCT step of every member, then on ``member``:
+    (i) every tracer against the C oracle (fct_ref.c, all host threads) at <= 1e-12
+        (max-norm over wet lanes, relative to max|T_oracle|);
+    (ii) budget closure of tracer 0 (content change = dt x surface fluxes, from the numpy
+        oracle's intermediates) to 1e-13 of the content;
+    (iii) no value of tracer 0 outside the limiter's window (fesom_jax/tracer_adv.py:389-418),
+        4 ulp slack;
+    (iv) bitwise determinism: the single-instance fused call twice on the same inputs, and
+        the batched result of tracer 0 against it.
+    The oracle serves as the checker only; nothing here is timed."""
+    import torch
+
+    from oracle import fct_c, fct_np
+    from oracle.gates import closure_residual, window_violations
+    mb = ens.members[member]
+    T, To = (x.cpu().numpy() for x in ens.state(member))
+    host = {k: getattr(mb, k).cpu().numpy() for k in ("uv", "w_e", "helem", "hnode",
+                                                      "hnode_new")}
+    ens.step()
+    torch.cuda.synchronize()
+    Tn = ens.state(member)[0].cpu().numpy()
+    lm = mesh.node_layer_mask
+    keep = []
+    from fesom_jax_b200 import _lib as fl
+    desc = fl.mesh_desc(mesh, keep)
+    worst, dry_equal = 0.0, True
+    for t in range(mb.ntr):
+        ref, _ = fct_c.advect_one_fct(mesh, host["uv"], host["w_e"], host["helem"],
+                                      host["hnode"], host["hnode_new"], T[t], To[t],
+                                      dt=mb.dt, desc=desc)
+        worst = max(worst, float(np.max(np.abs(Tn[t][lm] - ref[lm])) /
+                                 np.max(np.abs(ref[lm]))))
+        dry_equal = dry_equal and bool(np.array_equal(Tn[t][~lm], T[t][~lm]))
+    inter = {}
+    ref0, _ = fct_np.advect_one_fct(mesh, host["uv"], host["w_e"], host["helem"],
+                                    host["hnode"], host["hnode_new"], T[0], To[0], dt=mb.dt,
+                                    intermediates=inter)
+    closure = closure_residual(mesh, T[0], host["hnode"], host["hnode_new"], Tn[0], inter,
+                               mb.dt)
+    viol = int(len(window_violations(mesh, T[0], host["hnode_new"], Tn[0], inter)))
+    d = lambda x: torch.from_numpy(np.ascontiguousarray(x)).cuda()  # noqa: E731
+    args = [d(host[k]) for k in ("uv", "w_e", "helem", "hnode", "hnode_new")]
+    a = plan.forward(*args, d(T[0]), d(To[0]), mb.dt)
+    b = plan.forward(*args, d(T[0]), d(To[0]), mb.dt)
+    det = bool(torch.equal(a, b))
+    batched_eq = bool(np.array_equal(a.cpu().numpy(), Tn[0]))
+    out = dict(member=member, tracers=mb.ntr, max_rel_err=worst, rtol=GATE_RTOL,
+               dry_levels_equal=dry_equal, closure_rel=closure, closure_rtol=GATE_CLOSURE_RTOL,
+               window_violations=viol, deterministic=det, batched_equals_plain=batched_eq)
+    out["passed"] = bool(worst <= GATE_RTOL and dry_equal and closure <= GATE_CLOSURE_RTOL
+                         and viol == 0 and det)
+    return out
+
+
 # ------------------------------------------------------------------------ our arm
 def member_seed(rank: int, i: int) -> int:
     """Seed of member ``i`` on ``rank``: replicas advance different members."""
@@ -239,7 +302,7 @@ def run_ours(args, D: Dist) -> dict | None:
     for i in range(cfg["members"]):
         inp = W.member_inputs_gpu(mesh, seed=member_seed(D.rank, i), ntr=cfg["ntr"], device=dev,
                                   thickness=thick, sigma=cfg["sigma"],
-                                  n_vortices=cfg["n_vortices"])
+                                  n_vortices=cfg["n_vortices"], kind=cfg["velocity"])
         ens.add_member(mesh, inp["uv"], inp["w_e"], inp["helem"], inp["hnode"],
                        inp["hnode_new"], inp["T"], inp["T_old"], cfg["dt"], Kv=Kv,
                        derive_w=args.derive_w)
@@ -273,20 +336,30 @@ def run_ours(args, D: Dist) -> dict | None:
     upd_rank = info["updates_per_step"] * S * args.steps
     value, t = D.weak_value(upd_rank, t_local, dev)
 
+    # health: non-finite T_new values written by any member since the build (device
+    # counters of the final stage), and the finiteness of every member's state
+    nonfinite = ens.health()
+    finite = (sum(nonfinite) == 0 and
+              all(bool(torch.isfinite(ens.state(i)[0]).all().item())
+                  for i in range(len(ens.members))))
     # per-stage breakdown (events on the launching stream, one step, synchronised)
     prof = {}
     for _ in range(3):
         for k, v in ens.profile_step().items():
             prof[k] = prof.get(k, 0.0) + v / 3
     fct_step_ms = t_local / (S * args.steps) * 1e3
-    finite = bool(torch.isfinite(ens.state(0)[0]).all().item())
     alg = W.algorithmic_bytes(mesh, cfg["ntr"], cfg["members"])
     pk = peaks()
     achieved = alg / (fct_step_ms / 1e3) / 1e9
     info = ens.info()   # after tuning: launches per step depend on tracers per thread
     n_kernels = info["launches_per_step"]
+    gates = None
+    if D.rank == 0 and not args.no_gates:
+        from fesom_jax_b200.tracer_adv import get_plan
+        gates = run_gates(ens, mesh, cfg, get_plan(mesh, D.local_rank))
     out = dict(value=value, t=t, info=info, clocks=clk, prof=prof, fct_step_ms=fct_step_ms,
-               finite=finite, mesh=mesh, cfg=cfg, alg_bytes=alg,
+               finite=finite, nonfinite=int(sum(nonfinite)), gates=gates, mesh=mesh, cfg=cfg,
+               alg_bytes=alg,
                roofline=dict(bound="hbm", kernel="fused FCT step (vflux, node_lo, edge_adf, node_limit, node_final)",
                              achieved=achieved, peak=pk["hbm_gbs"], unit="GB/s",
                              frac=achieved / pk["hbm_gbs"], peak_source=pk["source"],
@@ -355,7 +428,8 @@ def e2e_host(args, mesh, cfg, dev, per_thread: int = 0) -> dict:
     ens, host = [], []
     for i in range(nm):
         inp = W.member_inputs_gpu(mesh, seed=500000 + i, ntr=cfg["ntr"], device=dev,
-                                  thickness=thick, sigma=cfg["sigma"], n_vortices=cfg["n_vortices"])
+                                  thickness=thick, sigma=cfg["sigma"], n_vortices=cfg["n_vortices"],
+                                  kind=cfg["velocity"])
         e = Ensemble(device=dev.index, workspace_budget=int(args.workspace_gb * (1 << 30)))
         e.add_member(mesh, inp["uv"], inp["w_e"], inp["helem"], inp["hnode"], inp["hnode_new"],
                      inp["T"], inp["T_old"], cfg["dt"])
@@ -576,7 +650,7 @@ def run_reference(args, D: Dist):
     cfg = dict(W.WORKLOADS[args.config])
     mesh = W.make_workload_mesh(args.config, seed=0)
     f = I.make_fields(mesh, seed=1, n_passive=max(cfg["ntr"] - 2, 0), ab2=True,
-                      sigma=cfg["sigma"])
+                      sigma=cfg["sigma"], n_vortices=cfg["n_vortices"], kind=cfg["velocity"])
     ntr = cfg["ntr"]
     keep = []
     from fesom_jax_b200 import _lib as fl
@@ -630,10 +704,12 @@ def side_line(args, D: Dist, r: dict) -> dict:
 
 
 def workload_config(name, cfg, mesh) -> dict:
+    from fesom_jax_b200 import workloads as W
     return dict(workload=f"{name}: FCT tracer advection, {mesh.name} mesh", nod2D=mesh.nod2D,
                 elem2D=mesh.elem2D, edge2D=mesh.edge2D, nl=mesh.nl,
                 wet_node_layers=mesh.n_wet_layers, members=cfg["members"], tracers=cfg["ntr"],
                 fct_steps_per_bench_step=cfg["fct_steps"], dt=cfg["dt"],
+                velocity=W.velocity_note(name),
                 l2="inputs larger than L2 (resident state >> 126 MB)",
                 parallelism="replicas: members per GPU, no collective")
 
@@ -659,6 +735,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fd", action="store_true", help="adjoint: skip the FD check")
+    ap.add_argument("--no-gates", action="store_true",
+                    help="skip the per-run correctness gates (oracle parity, closure, window)")
     ap.add_argument("--node-order", choices=["rcm", "raw", "random"], default="rcm",
                     help="synthetic meshes: node numbering (reverse Cuthill-McKee, the "
                          "generator's Fibonacci order, or a seeded shuffle)")
@@ -701,11 +779,17 @@ def main():
                 roofline=r["roofline"],
                 clocks=r["clocks"], gpu_launches=r["gpu_launches"],
                 fct_step_ms=r["fct_step_ms"], stage_ms=r["prof"], finite=r["finite"],
-                batch=r["info"], tuning=r["tuning"])
+                nonfinite=r["nonfinite"], gates=r["gates"], batch=r["info"], tuning=r["tuning"])
     for k in ("plain", "e2e", "cpu_baseline"):
         if k in r:
             line[k] = r[k]
+    failed = not r["finite"] or (r["gates"] is not None and not r["gates"]["passed"])
+    if failed:   # a state that went non-finite or failed a gate gives no throughput
+        line["value"] = None
+        line["error"] = ("non-finite state" if not r["finite"] else "correctness gate failed")
     print(json.dumps(line), flush=True)
+    if failed:
+        sys.exit(1)
 
 
 if __name__ == "__main__":

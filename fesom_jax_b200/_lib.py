@@ -43,6 +43,15 @@ class FctFields(C.Structure):
     ]
 
 
+FCT_ERR_NONFINITE = -5
+
+
+def health_status(status: int) -> None:
+    """Raise for a failed health call; FCT_ERR_NONFINITE is a result, not a failure."""
+    if status not in (FCT_OK, FCT_ERR_NONFINITE):
+        check(status)
+
+
 class FctError(RuntimeError):
     def __init__(self, status: int, msg: str):
         super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
@@ -72,8 +81,9 @@ def lib() -> C.CDLL:
     L.fct_plan_set_fused.argtypes = [C.c_void_p, C.c_int]
     L.fct_forward.argtypes = [C.c_void_p, C.POINTER(FctFields), C.c_double, C.c_int, C.c_void_p]
     L.fct_compute_w.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.fct_plan_health.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_int64)]
     for name in ("fct_plan_create", "fct_plan_destroy", "fct_plan_reserve", "fct_plan_info",
-                 "fct_plan_set_fused", "fct_forward", "fct_compute_w"):
+                 "fct_plan_set_fused", "fct_forward", "fct_compute_w", "fct_plan_health"):
         getattr(L, name).restype = C.c_int
     _lib = L
     return L

@@ -994,8 +994,15 @@ int fct_forward_taped(FctPlan* P, const FctFields* f, double dt, int ntr, FctTap
   if (!f->T_new) return set_error(FCT_ERR_INVALID, "T_new is NULL");
   if (!(dt > 0.0)) return set_error(FCT_ERR_INVALID, "dt must be positive");
   DeviceGuard g(P->device);
-  const Inst in = make_inst(P, f, dt, ntr, tape->ws[size_t(slot)]);
-  st = launch_forward(in, nullptr, 1, unfused_dims(P, ntr), static_cast<cudaStream_t>(stream));
+  Inst in = make_inst(P, f, dt, ntr, tape->ws[size_t(slot)]);
+  in.nonfinite = P->d_health;
+  {
+    PlanUse use(P, static_cast<cudaStream_t>(stream));
+    st = use.status();
+    if (!st) st = launch_forward(in, nullptr, 1, unfused_dims(P, ntr),
+                                 static_cast<cudaStream_t>(stream));
+    if (!st) st = use.release();
+  }
   if (st) return st;
   tape->recorded[size_t(slot)] = 1;
   tape->dt[size_t(slot)] = dt;
@@ -1033,6 +1040,8 @@ int fct_adjoint_ex(FctPlan* P, const FctFields* f, const double* gT_new, double 
   if (!(dt > 0.0)) return set_error(FCT_ERR_INVALID, "dt must be positive");
   DeviceGuard guard(P->device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  PlanUse use(P, s);
+  if (use.status()) return use.status();
   Adj A{};
   A.in = make_inst(P, f, dt, ntr, tape ? tape->ws[size_t(slot)] : P->ws);
   A.in.T_new = nullptr;
@@ -1077,7 +1086,7 @@ int fct_adjoint_ex(FctPlan* P, const FctFields* f, const double* gT_new, double 
   FCT_CUDA(cudaStreamWaitEvent(s, P->adj_ev[3], 0));
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_error(e, "adjoint kernel launch");
-  return FCT_OK;
+  return use.release();
 }
 
 int fct_adjoint(FctPlan* P, const FctFields* f, const double* gT_new, double dt, int ntr,
@@ -1092,12 +1101,14 @@ int fct_compute_w_adjoint(FctPlan* P, const double* gw, const double* helem, dou
     return set_error(FCT_ERR_CAPACITY, "call fct_plan_reserve_adjoint first");
   DeviceGuard guard(P->device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  PlanUse use(P, s);
+  if (use.status()) return use.status();
   double* gdiv = P->aws.gdiv;   // scratch: one node field
   r_w_div<<<unsigned((P->N + 127) / 128), 128, 0, s>>>(P->d_mesh, gw, gdiv);
   const int64_t EL = int64_t(P->E) * P->L;
   r_w_uv<<<unsigned((EL + B - 1) / B), B, 0, s>>>(P->d_mesh, gdiv, helem, guv, accumulate);
   const cudaError_t e = cudaGetLastError();
-  return e == cudaSuccess ? FCT_OK : cuda_error(e, "compute_w adjoint launch");
+  return e == cudaSuccess ? use.release() : cuda_error(e, "compute_w adjoint launch");
 }
 
 }  // extern "C"

@@ -33,6 +33,7 @@ struct FctBatch {
   double* arena = nullptr;
   int64_t arena_bytes = 0;
   Inst* d_tables = nullptr;
+  unsigned long long* d_health = nullptr;   // per-instance non-finite counters
   int64_t total_updates = 0;     // sum over instances of ntr * wet node layers
   std::mutex graph_mu;
   std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
@@ -175,7 +176,13 @@ int fct_batch_create(const FctInstance* insts, int n, int64_t budget, FctBatch**
     d.per_thread = d.chunk < 8 ? d.chunk : 8;
     gr.dims = d;
   }
-  e = cudaMalloc(&B->d_tables, tab.size() * sizeof(Inst));
+  e = cudaMalloc(&B->d_health, size_t(n) * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMemset(B->d_health, 0, size_t(n) * sizeof(unsigned long long));
+  for (int i = 0; i < n && e == cudaSuccess; ++i)
+    for (int p = 0; p < 3; ++p)
+      tab[size_t(p) * n + i].nonfinite = insts[i].nonfinite ? insts[i].nonfinite
+                                                           : B->d_health + i;
+  if (e == cudaSuccess) e = cudaMalloc(&B->d_tables, tab.size() * sizeof(Inst));
   if (e == cudaSuccess)
     e = cudaMemcpy(B->d_tables, tab.data(), tab.size() * sizeof(Inst), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&B->cap_stream, cudaStreamNonBlocking);
@@ -195,6 +202,7 @@ int fct_batch_destroy(FctBatch* B) {
   for (auto& kv : B->graphs) cudaGraphExecDestroy(kv.second);
   if (B->cap_stream) cudaStreamDestroy(B->cap_stream);
   if (B->d_tables) cudaFree(B->d_tables);
+  if (B->d_health) cudaFree(B->d_health);
   if (B->arena) cudaFree(B->arena);
   if (prev >= 0) cudaSetDevice(prev);
   delete B;
@@ -296,6 +304,44 @@ int fct_batch_run(FctBatch* B, int first_phase, int steps, fct_stream_t stream) 
   return restore(FCT_OK);
 }
 
+int fct_batch_fill_workspace(FctBatch* B, int byte, fct_stream_t stream) {
+  if (!B) return set_error(FCT_ERR_INVALID, "batch is NULL");
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(B->device);
+  const cudaError_t e = cudaMemsetAsync(B->arena, byte & 0xff, size_t(B->arena_bytes),
+                                        static_cast<cudaStream_t>(stream));
+  if (prev >= 0) cudaSetDevice(prev);
+  return e == cudaSuccess ? FCT_OK : cuda_error(e, "batch workspace fill");
+}
+
+int fct_batch_health(FctBatch* B, fct_stream_t stream, int64_t* counts) {
+  if (!B) return set_error(FCT_ERR_INVALID, "batch is NULL");
+  const int n = int(B->insts.size());
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(B->device);
+  auto restore = [&](int st) { if (prev >= 0) cudaSetDevice(prev); return st; };
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  std::vector<unsigned long long> h(size_t(n), 0ull);
+  cudaError_t e = cudaMemcpyAsync(h.data(), B->d_health, size_t(n) * sizeof(h[0]),
+                                  cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(B->d_health, 0, size_t(n) * sizeof(h[0]), s);
+  if (e != cudaSuccess) return restore(cuda_error(e, "batch health read"));
+  unsigned long long total = 0;
+  int first = -1;
+  for (int i = 0; i < n; ++i) {
+    if (counts) counts[i] = int64_t(h[size_t(i)]);
+    if (h[size_t(i)] && first < 0) first = i;
+    total += h[size_t(i)];
+  }
+  if (total)
+    return restore(set_error(FCT_ERR_NONFINITE, "%llu non-finite T_new values since the last "
+                             "check (first in instance %d)", total, first));
+  return restore(FCT_OK);
+}
+
 int fct_batch_profile(FctBatch* B, int phase, double* stage_ms, int max_stages,
                       fct_stream_t stream) {
   if (!B || !stage_ms) return set_error(FCT_ERR_INVALID, "NULL argument");
@@ -341,6 +387,7 @@ struct FctServe {
   int64_t arena_doubles = 0;
   Inst* d_tab = nullptr;      // device instance table
   Inst* h_tab = nullptr;      // pinned staging
+  unsigned long long* d_health = nullptr;   // non-finite counter of instances without one
   cudaEvent_t uploaded = nullptr;
   bool pending = false;       // an upload from h_tab may still be in flight
 };
@@ -374,6 +421,9 @@ int fct_serve_create(int device, int max_instances, int64_t workspace_bytes, Fct
     return fail(e, "serve staging cudaMallocHost");
   if ((e = cudaEventCreateWithFlags(&S->uploaded, cudaEventDisableTiming)) != cudaSuccess)
     return fail(e, "cudaEventCreate");
+  if ((e = cudaMalloc(&S->d_health, sizeof(unsigned long long))) != cudaSuccess ||
+      (e = cudaMemset(S->d_health, 0, sizeof(unsigned long long))) != cudaSuccess)
+    return fail(e, "serve health counter");
   if (prev >= 0) cudaSetDevice(prev);
   *out = S;
   return FCT_OK;
@@ -390,6 +440,7 @@ int fct_serve_destroy(FctServe* S) {
   }
   if (S->h_tab) cudaFreeHost(S->h_tab);
   if (S->d_tab) cudaFree(S->d_tab);
+  if (S->d_health) cudaFree(S->d_health);
   if (S->arena) cudaFree(S->arena);
   if (prev >= 0) cudaSetDevice(prev);
   delete S;
@@ -454,6 +505,7 @@ int fct_serve_step(FctServe* S, const FctInstance* insts, const int32_t* phases,
     off += workspace_doubles_fused(P->N, P->Ed, P->L, q.ntr);
     in.dt = q.dt;
     in.ntr = q.ntr;
+    in.nonfinite = q.nonfinite ? q.nonfinite : S->d_health;
     if (q.w_derived) {   // producer: w_e = compute_w(uv, helem) at this step
       in.w_derived = q.w_derived;
       in.w_e = q.w_derived;
@@ -493,6 +545,16 @@ int fct_serve_step(FctServe* S, const FctInstance* insts, const int32_t* phases,
     j0 = j1;
   }
   return restore(FCT_OK);
+}
+
+int fct_serve_health(FctServe* S, fct_stream_t stream, int64_t* n_nonfinite) {
+  if (!S) return set_error(FCT_ERR_INVALID, "serve engine is NULL");
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(S->device);
+  const int st = read_health(S->d_health, 1, static_cast<cudaStream_t>(stream), n_nonfinite);
+  if (prev >= 0) cudaSetDevice(prev);
+  return st;
 }
 
 const char* fct_stage_name(int i) {

@@ -91,6 +91,19 @@ __device__ __forceinline__ void stc(uint8_t* __restrict__ p, uint32_t q, int t0,
   for (int i = 0; i < NTR; ++i) p[tix<IL>(q, t0 + i, stride, tg)] = uint8_t(v[i]);
 }
 
+// Health counter (the reference's finiteness gate, fesom_jax/diagnostics.py:31-101): add
+// the number of non-finite values among ``v`` to ``*counter``. Finite results cost a test
+// per value and no atomic.
+template <int NTR>
+__device__ __forceinline__ void count_nonfinite(unsigned long long* counter,
+                                                const double (&v)[NTR]) {
+  if (!counter) return;
+  unsigned bad = 0;
+#pragma unroll
+  for (int t = 0; t < NTR; ++t) bad += isfinite(v[t]) ? 0u : 1u;
+  if (bad) atomicAdd(counter, static_cast<unsigned long long>(bad));
+}
+
 // k in [r & 255, (r >> 8) & 255): the packed level ranges of the fused stages' slots
 __device__ __forceinline__ bool in_range(int k, unsigned r) {
   return k >= int(r & 255u) && k < int((r >> 8) & 255u);
@@ -898,6 +911,7 @@ __device__ __forceinline__ void body_node_final(const Inst& in, int64_t i, int t
     out[t] = Tv[t] + (hnn > 0.0 ? divr(d, rhn) : 0.0);
   }
   stn<NTR, IL>(in.T_new, qn, t0, in.tstride, tg, out);
+  count_nonfinite<NTR>(in.nonfinite, out);
 }
 
 // ------------- implicit vertical diffusion (tracer_diff.py:68-123, ops.py:121-168)

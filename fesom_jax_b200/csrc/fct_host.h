@@ -73,6 +73,29 @@ int plan_reserve_ws(FctPlan* P, int ntr, bool full);
 // A plan created by fct_plan_create in this process and not destroyed yet.
 bool plan_alive(const FctPlan* P);
 
+// Ordering of the calls that use a plan's workspace: hold ``P->mu`` (PlanUse does), wait
+// on stream ``s`` for the previous user, launch, then record the release on ``s``. Both
+// are skipped while ``s`` is being captured into a CUDA graph (an event from outside a
+// capture cannot be waited on inside it): captured calls are ordered by their graph.
+class PlanUse {
+ public:
+  PlanUse(FctPlan* P, cudaStream_t s);
+  // record the release event (call after the launches; returns a status)
+  int release();
+  int status() const { return st_; }
+
+ private:
+  std::lock_guard<std::mutex> lk_;
+  FctPlan* P_;
+  cudaStream_t s_;
+  bool capturing_ = false;
+  int st_ = 0;
+};
+
+// Copy a device counter to the host on ``s``, wait, zero it, and return FCT_ERR_NONFINITE
+// when it was non-zero (``out`` receives the count when not NULL).
+int read_health(unsigned long long* d_counter, int n, cudaStream_t s, int64_t* out);
+
 // Launches one stage takes for `csz` tracers of a workspace chunk with at most
 // `per_thread` tracers per thread (the split rule of the stage launcher).
 inline int stage_launches(int csz, int per_thread) {

@@ -241,12 +241,20 @@ extern "C" int fct_ice_solve(FctPlan* P, const FctIceFields* f, const FctIceConf
   A.dt = cfg->dt; A.gamma = cfg->gamma; A.diff = cfg->diff;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const unsigned g = unsigned((N + B - 1) / B);
-  k_ice_rhs<<<g, B, 0, s>>>(A);
-  k_ice_hi<<<g, B, 0, s>>>(A, A.d0, A.d1);   // two residual corrections (ice_adv.py:104)
-  k_ice_hi<<<g, B, 0, s>>>(A, A.d1, A.d0);
-  k_ice_limit<<<g, B, 0, s>>>(A, A.d0);
-  k_ice_apply<<<g, B, 0, s>>>(A, A.d0);
-  const cudaError_t e = cudaGetLastError();
+  int st;
+  {
+    PlanUse use(P, s);
+    st = use.status();
+    if (!st) {
+      k_ice_rhs<<<g, B, 0, s>>>(A);
+      k_ice_hi<<<g, B, 0, s>>>(A, A.d0, A.d1);   // two residual corrections (ice_adv.py:104)
+      k_ice_hi<<<g, B, 0, s>>>(A, A.d1, A.d0);
+      k_ice_limit<<<g, B, 0, s>>>(A, A.d0);
+      k_ice_apply<<<g, B, 0, s>>>(A, A.d0);
+      const cudaError_t e = cudaGetLastError();
+      st = e == cudaSuccess ? use.release() : cuda_error(e, "ice FCT launch");
+    }
+  }
   if (prev >= 0 && prev != P->device) cudaSetDevice(prev);
-  return e == cudaSuccess ? FCT_OK : cuda_error(e, "ice FCT launch");
+  return st;
 }

@@ -7,6 +7,8 @@
 #pragma once
 
 #include <cstdint>
+#include <mutex>
+
 #include <cuda_runtime.h>
 
 #include "../../include/fesom_fct.h"
@@ -153,6 +155,9 @@ struct Inst {
   int sw_tracer;       // tracer that takes the shortwave divergence (-1: none)
   double* w_derived;   // batched producer: w_e = compute_w(uv, helem) written here first
   const double *Z3d, *zbar3, *w_i;
+  // health counter: the final stage adds the number of non-finite T_new values it writes
+  // (NULL: not counted)
+  unsigned long long* nonfinite;
   Workspace ws;
   double dt;
   int ntr;
@@ -184,6 +189,15 @@ constexpr int kAdjNodeFields = 16, kAdjEdgeFields = 7, kAdjElemFields = 4;
 
 struct FctPlan {
   int device = 0;
+  // the workspace's last user: every call that writes the plan workspace waits for this
+  // event on its own stream and records it afterwards, so calls on different streams do
+  // not overlap on the workspace (host threads are serialised by ``mu``)
+  std::mutex mu;
+  cudaEvent_t ws_ev = nullptr;
+  bool ws_used = false;
+  unsigned long long* d_health = nullptr;   // non-finite T_new values written since the last
+                                            // fct_plan_health
+
   int N = 0, E = 0, Ed = 0, L = 0;
   fct::DevMesh hm{};               // device pointers (host copy)
   fct::DevMesh* d_mesh = nullptr;  // device copy

@@ -3,17 +3,16 @@
 // Who needs it: code that runs where device allocation is not allowed or not safe.
 // An XLA/JAX custom-call handler executes inside a runtime that owns (and usually
 // preallocates) the GPU's memory, so a cudaMalloc there competes with or fails under
-// that pool; a stream being captured into a CUDA graph must not allocate; and a
-// latency-bound serving loop should never block on the allocator. Such callers can
-// create a plan once at set-up time, but at call time they can only hand over the
-// inputs and outputs they were given.
+// that pool; a latency-bound serving loop should never block on the allocator. Such
+// callers can create a plan once at set-up time, but at call time they can only hand
+// over the inputs and outputs they were given.
 //
-// This entry point runs the same stage kernels as fct_forward, but their intermediates
-// live in ``g_fct_static_scratch``, a file-scope __device__ array of
-// kStaticScratchDoubles doubles (64 MiB) that every GPU which loads the library holds
-// until the process exits. Nothing here calls cudaMalloc, cudaFree or any allocating
-// library routine. Sizes whose scratch need exceeds the array are rejected with
-// FCT_ERR_CAPACITY.
+// This entry point runs the fused stage kernels of fct_forward (always the fused ones,
+// whatever fct_plan_set_fused chose for the plan), but their intermediates live in
+// ``g_fct_static_scratch``, a file-scope __device__ array of kStaticScratchDoubles
+// doubles (64 MiB) that every GPU which loads the library holds until the process exits.
+// Nothing here calls cudaMalloc, cudaFree or any allocating library routine. Sizes whose
+// scratch need exceeds the array are rejected with FCT_ERR_CAPACITY.
 //
 // The array's name is only a host-side stand-in in host code, so its device address is
 // looked up once per device (cudaGetSymbolAddress, with that device current) on the
@@ -88,6 +87,7 @@ extern "C" int fct_forward_noalloc(FctPlan* P, const FctFields* f, double dt, in
   in.ws = carve_workspace(scratch, P->N, P->E, P->Ed, P->L, ntr, /*fused=*/true);
   in.dt = dt;
   in.ntr = ntr;
+  in.nonfinite = P->d_health;   // allocated with the plan
   LaunchDims dims{};
   dims.max_iface = P->hm.n_iface;
   dims.max_layer = P->hm.n_layer;

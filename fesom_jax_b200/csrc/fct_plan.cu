@@ -31,6 +31,42 @@ bool plan_alive(const FctPlan* P) {
   return g_plans.count(P) != 0;
 }
 
+PlanUse::PlanUse(FctPlan* P, cudaStream_t s) : lk_(P->mu), P_(P), s_(s) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaError_t e = cudaStreamIsCapturing(s, &cs);
+  if (e != cudaSuccess) {   // the legacy stream while another stream captures: treat as
+    cudaGetLastError();     // captured (no event work)
+    cs = cudaStreamCaptureStatusActive;
+  }
+  capturing_ = cs != cudaStreamCaptureStatusNone;
+  if (!capturing_ && P->ws_used) {
+    e = cudaStreamWaitEvent(s, P->ws_ev, 0);
+    if (e != cudaSuccess) st_ = cuda_error(e, "workspace order wait");
+  }
+}
+
+int PlanUse::release() {
+  if (st_ || capturing_) return st_;
+  const cudaError_t e = cudaEventRecord(P_->ws_ev, s_);
+  if (e != cudaSuccess) return cuda_error(e, "workspace order record");
+  P_->ws_used = true;
+  return FCT_OK;
+}
+
+int read_health(unsigned long long* d, int n, cudaStream_t s, int64_t* out) {
+  std::vector<unsigned long long> h(size_t(n > 0 ? n : 1), 0ull);
+  FCT_CUDA(cudaMemcpyAsync(h.data(), d, size_t(n) * sizeof(*d), cudaMemcpyDeviceToHost, s));
+  FCT_CUDA(cudaStreamSynchronize(s));
+  FCT_CUDA(cudaMemsetAsync(d, 0, size_t(n) * sizeof(*d), s));
+  unsigned long long total = 0;
+  for (int i = 0; i < n; ++i) total += h[size_t(i)];
+  if (out) *out = int64_t(total);
+  if (total)
+    return set_error(FCT_ERR_NONFINITE, "%llu non-finite T_new values since the last check",
+                     total);
+  return FCT_OK;
+}
+
 int set_error(int status, const char* fmt, ...) {
   char buf[1024];
   va_list ap;
@@ -441,6 +477,9 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   m.ecell4 = (const int4*)(base + o_ecell4);
   FCT_CUDA(cudaMalloc(&P->d_mesh, sizeof(DevMesh)));
   FCT_CUDA(cudaMemcpy(P->d_mesh, &m, sizeof(DevMesh), cudaMemcpyHostToDevice));
+  FCT_CUDA(cudaMalloc(&P->d_health, sizeof(unsigned long long)));
+  FCT_CUDA(cudaMemset(P->d_health, 0, sizeof(unsigned long long)));
+  FCT_CUDA(cudaEventCreateWithFlags(&P->ws_ev, cudaEventDisableTiming));
   return FCT_OK;
 }
 
@@ -461,6 +500,11 @@ int fct_plan_destroy(FctPlan* P) {
   if (P->adj_side) cudaStreamDestroy(P->adj_side);
   for (cudaEvent_t ev : P->adj_ev)
     if (ev) cudaEventDestroy(ev);
+  if (P->ws_ev) {
+    cudaEventSynchronize(P->ws_ev);
+    cudaEventDestroy(P->ws_ev);
+  }
+  if (P->d_health) cudaFree(P->d_health);
   if (P->d_ws) cudaFree(P->d_ws);
   if (P->d_mesh) cudaFree(P->d_mesh);
   if (P->d_static) cudaFree(P->d_static);
@@ -544,7 +588,13 @@ int fct_vert_diff(FctPlan* P, const FctVdiffFields* f, double dt, int ntr, fct_s
   dims.ntr = ntr;
   dims.chunk = 0;
   dims.per_thread = 8;
-  const int st = launch_vdiff(in, dims, static_cast<cudaStream_t>(stream));
+  int st;
+  {
+    PlanUse use(P, static_cast<cudaStream_t>(stream));
+    st = use.status();
+    if (!st) st = launch_vdiff(in, dims, static_cast<cudaStream_t>(stream));
+    if (!st) st = use.release();
+  }
   if (prev >= 0 && prev != P->device) cudaSetDevice(prev);
   return st;
 }
@@ -573,6 +623,7 @@ int fct_forward(FctPlan* P, const FctFields* f, double dt, int ntr, fct_stream_t
   in.ws = P->ws;
   in.dt = dt;
   in.ntr = ntr;
+  in.nonfinite = P->d_health;
   LaunchDims dims{};
   dims.max_iface = P->hm.n_iface;
   dims.max_layer = P->hm.n_layer;
@@ -589,7 +640,45 @@ int fct_forward(FctPlan* P, const FctFields* f, double dt, int ntr, fct_stream_t
   int prev = -1;
   cudaGetDevice(&prev);
   if (prev != P->device) cudaSetDevice(P->device);
-  const int st = launch_forward(in, nullptr, 1, dims, static_cast<cudaStream_t>(stream));
+  int st;
+  {
+    PlanUse use(P, static_cast<cudaStream_t>(stream));
+    st = use.status();
+    if (!st) st = launch_forward(in, nullptr, 1, dims, static_cast<cudaStream_t>(stream));
+    if (!st) st = use.release();
+  }
+  if (prev >= 0 && prev != P->device) cudaSetDevice(prev);
+  return st;
+}
+
+int fct_plan_fill_workspace(FctPlan* P, int byte, fct_stream_t stream) {
+  if (!P) return set_error(FCT_ERR_INVALID, "NULL plan");
+  if (!P->d_ws) return FCT_OK;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  if (prev != P->device) cudaSetDevice(P->device);
+  const int64_t nd = P->ws_full ? workspace_doubles(P->N, P->E, P->Ed, P->L, P->max_tracers)
+                                : workspace_doubles_fused(P->N, P->Ed, P->L, P->max_tracers);
+  int st;
+  {
+    PlanUse use(P, static_cast<cudaStream_t>(stream));
+    st = use.status();
+    if (!st) {
+      const cudaError_t e = cudaMemsetAsync(P->d_ws, byte & 0xff, size_t(nd) * sizeof(double),
+                                            static_cast<cudaStream_t>(stream));
+      st = e == cudaSuccess ? use.release() : cuda_error(e, "workspace fill");
+    }
+  }
+  if (prev >= 0 && prev != P->device) cudaSetDevice(prev);
+  return st;
+}
+
+int fct_plan_health(FctPlan* P, fct_stream_t stream, int64_t* n_nonfinite) {
+  if (!P) return set_error(FCT_ERR_INVALID, "NULL plan");
+  int prev = -1;
+  cudaGetDevice(&prev);
+  if (prev != P->device) cudaSetDevice(P->device);
+  const int st = read_health(P->d_health, 1, static_cast<cudaStream_t>(stream), n_nonfinite);
   if (prev >= 0 && prev != P->device) cudaSetDevice(prev);
   return st;
 }

@@ -35,7 +35,7 @@ class FctInstance(C.Structure):
     _fields_ = [("plan", C.c_void_p), ("uv", C.c_void_p), ("w_e", C.c_void_p),
                 ("helem", C.c_void_p), ("hnode", C.c_void_p), ("hnode_new", C.c_void_p),
                 ("buf", C.c_void_p * 3), ("ntr", C.c_int), ("dt", C.c_double),
-                ("Kv", C.c_void_p), ("w_derived", C.c_void_p)]
+                ("Kv", C.c_void_p), ("w_derived", C.c_void_p), ("nonfinite", C.c_void_p)]
 
 
 def _bind_batch(L):
@@ -51,8 +51,11 @@ def _bind_batch(L):
                                     C.c_void_p]
     L.fct_stage_name.restype = C.c_char_p
     L.fct_batch_set_chunk.argtypes = [C.c_void_p, C.c_int]
+    L.fct_batch_health.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_int64)]
+    L.fct_batch_fill_workspace.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
     for n in ("fct_batch_create", "fct_batch_destroy", "fct_batch_info", "fct_batch_prepare",
-              "fct_batch_step", "fct_batch_run", "fct_batch_profile", "fct_batch_set_chunk"):
+              "fct_batch_step", "fct_batch_run", "fct_batch_profile", "fct_batch_set_chunk",
+              "fct_batch_health", "fct_batch_fill_workspace"):
         getattr(L, n).restype = C.c_int
     L._batch_bound = True
     return L
@@ -180,6 +183,21 @@ class Ensemble:
         _lib.check(_bind_batch(_lib.lib()).fct_batch_run(self._h, self.phase % 3, int(steps),
                                                          self._stream(stream)))
         self.phase += int(steps)
+
+    def health(self, stream=None) -> list:
+        """Per-member counts of non-finite ``T_new`` values written since the previous
+        check (``fct_batch_health``; synchronises the stream). All zeros for a healthy
+        ensemble; the reference's finiteness gate (fesom_jax/diagnostics.py:31-101)."""
+        n = len(self.members)
+        out = (C.c_int64 * n)()
+        _lib.health_status(_bind_batch(_lib.lib()).fct_batch_health(
+            self._h, self._stream(stream), out))
+        return [int(v) for v in out]
+
+    def fill_workspace(self, byte: int = 0xFF, stream=None) -> None:
+        """Debug aid: fill the workspace arena with ``byte`` (0xFF: NaN doubles)."""
+        _lib.check(_bind_batch(_lib.lib()).fct_batch_fill_workspace(self._h, int(byte),
+                                                                    self._stream(stream)))
 
     def set_chunk(self, chunk: int) -> None:
         _lib.check(_bind_batch(_lib.lib()).fct_batch_set_chunk(self._h, int(chunk)))

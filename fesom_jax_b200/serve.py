@@ -37,7 +37,8 @@ def _bind(L):
     L.fct_serve_destroy.argtypes = [C.c_void_p]
     L.fct_serve_step.argtypes = [C.c_void_p, C.POINTER(FctInstance), C.POINTER(C.c_int32),
                                  C.c_int, C.c_void_p]
-    for n in ("fct_serve_create", "fct_serve_destroy", "fct_serve_step"):
+    L.fct_serve_health.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_int64)]
+    for n in ("fct_serve_create", "fct_serve_destroy", "fct_serve_step", "fct_serve_health"):
         getattr(L, n).restype = C.c_int
     L._serve_bound = True
     return L
@@ -60,6 +61,8 @@ class Request:
     done_event: object = None
     result: object = None
     grad: object = None
+    health: object = None   # device counter of non-finite T_new values of this request
+    nonfinite: int = 0      # its value after the run
 
 
 def poisson_requests(rate: float, duration: float, mix=(("pi", 0.6), ("core2", 0.3),
@@ -206,6 +209,7 @@ class ServingEngine:
         for j in range(3):
             q.buf[j] = r.state[j].data_ptr()
         q.ntr, q.dt = self.ntr, e.dt
+        q.nonfinite = r.health.data_ptr() if r.health is not None else None
         return q
 
     def _adjoint(self, r: Request, stream, after_event):
@@ -247,6 +251,10 @@ class ServingEngine:
         mem = self.static_bytes
         ws_active = 0
         iters, inst_total = 0, 0
+        # one non-finite counter per request (read after the run: no host sync per step)
+        counters = torch.zeros(max(len(requests), 1), dtype=torch.int64, device=self.dev)
+        for i, r in enumerate(requests):
+            r.health = counters[i:i + 1]
         torch.cuda.synchronize(self.dev)
         start = torch.cuda.Event(enable_timing=True)
         start.record(stream)
@@ -317,6 +325,9 @@ class ServingEngine:
                 time.sleep(max(0.0, min(0.01, pending[0].arrival - (time.perf_counter() - t0))))
         torch.cuda.synchronize(self.dev)
         wall = time.perf_counter() - t0
+        counts = counters.cpu().tolist()
+        for i, r in enumerate(requests):
+            r.nonfinite, r.health = int(counts[i]), None
         done = [r for r in requests if r.done is not None]
         lat = np.array([r.done - r.arrival for r in done]) * 1e3
         upd = sum(r.K * self.ntr * self.meshes[r.mesh].mesh.n_wet_layers for r in done)
@@ -324,7 +335,8 @@ class ServingEngine:
                     mean_batch=inst_total / max(iters, 1),
                     p50_ms=float(np.percentile(lat, 50)) if len(lat) else None,
                     p99_ms=float(np.percentile(lat, 99)) if len(lat) else None,
-                    throughput_req_s=len(done) / wall, updates_per_s=upd / wall)
+                    throughput_req_s=len(done) / wall, updates_per_s=upd / wall,
+                    nonfinite_requests=sum(1 for r in requests if r.nonfinite))
 
     def run_serial(self, requests: list[Request], time_limit: float | None = None) -> dict:
         """Baseline: the same requests one at a time through the single-instance C ABI

@@ -69,6 +69,25 @@ class FctPlan:
     def reserve(self, ntr: int) -> None:
         _lib.check(_lib.lib().fct_plan_reserve(self._h, int(ntr)))
 
+    def health(self, stream=None) -> int:
+        """Non-finite ``T_new`` values this plan's forward calls wrote since the previous
+        check (``fct_plan_health``; synchronises the stream). The finiteness gate of the
+        reference's diagnostics (fesom_jax/diagnostics.py:31-101)."""
+        torch = _torch()
+        s = stream if stream is not None else torch.cuda.current_stream(self.device).cuda_stream
+        n = C.c_int64(0)
+        _lib.health_status(_lib.lib().fct_plan_health(self._h, C.c_void_p(int(s)), C.byref(n)))
+        return int(n.value)
+
+    def fill_workspace(self, byte: int = 0xFF, stream=None) -> None:
+        """Debug aid: fill the plan workspace with ``byte`` (0xFF: NaN doubles)."""
+        torch = _torch()
+        s = stream if stream is not None else torch.cuda.current_stream(self.device).cuda_stream
+        L = _lib.lib()
+        L.fct_plan_fill_workspace.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        L.fct_plan_fill_workspace.restype = C.c_int
+        _lib.check(L.fct_plan_fill_workspace(self._h, int(byte), C.c_void_p(int(s))))
+
     def set_fused(self, fused: bool) -> None:
         """Fused stage kernels (default) or one kernel per reference stage; same bits."""
         _lib.check(_lib.lib().fct_plan_set_fused(self._h, int(bool(fused))))
@@ -123,7 +142,9 @@ class FctPlan:
         f.zbar3 = zbar3.data_ptr() if zbar3 is not None else None
         f.w_i = w_i.data_ptr() if w_i is not None else None
         s = stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
-        with self._lock:   # one workspace per plan: calls on a plan are serialised
+        # the library orders calls on one plan on the GPU; the lock keeps the host-side
+        # enqueue of concurrent Python threads whole
+        with self._lock:
             _lib.check(_lib.lib().fct_forward(self._h, C.byref(f), float(dt), ntr,
                                               C.c_void_p(int(s))))
         return out

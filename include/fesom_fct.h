@@ -16,7 +16,8 @@
  * last failure on the calling thread is returned by fct_last_error().
  * No entry point except fct_plan_create / fct_plan_reserve / fct_plan_reserve_adjoint /
  * fct_batch_create / fct_serve_create / fct_tape_create (without caller memory)
- * allocates device memory, and none synchronises the stream it is given.
+ * allocates device memory, and none but the health checks (fct_*_health) synchronises
+ * the stream it is given.
  */
 #ifndef FESOM_FCT_H
 #define FESOM_FCT_H
@@ -112,9 +113,27 @@ int fct_plan_info(const FctPlan* plan, int64_t out[8]);
 int fct_plan_set_fused(FctPlan* plan, int fused);
 
 /* One FCT step for ``ntr`` tracers: fesom_jax/tracer_adv.py:532-578 (advect_one_fct),
- * with exch=None. Writes T_new; T_old_new is T itself (the caller keeps the alias). */
+ * with exch=None. Writes T_new; T_old_new is T itself (the caller keeps the alias).
+ * Calls on one plan that use its workspace (fct_forward, fct_forward_taped, fct_adjoint*,
+ * fct_vert_diff, fct_ice_solve, fct_compute_w_adjoint, the XLA handlers) are ordered on
+ * the GPU even when issued on different streams or host threads: each waits on its stream
+ * for the previous one (a plan-owned event; nothing waits on the host). Calls issued while
+ * their stream is captured into a CUDA graph skip that ordering. */
 int fct_forward(FctPlan* plan, const FctFields* fields, double dt, int ntr,
                 fct_stream_t stream);
+
+/* Health check, the finiteness gate of the reference's diagnostics
+ * (fesom_jax/diagnostics.py:31-101 state_diagnostics/verdict): the number of non-finite
+ * T_new values that fct_forward, fct_forward_taped, fct_forward_noalloc and the XLA
+ * forward handler wrote with this plan since the previous check. Synchronises ``stream``
+ * (call it between steps, not in a hot loop), resets the counter, stores the count in
+ * ``*n_nonfinite`` (may be NULL) and returns FCT_ERR_NONFINITE when it is non-zero. */
+int fct_plan_health(FctPlan* plan, fct_stream_t stream, int64_t* n_nonfinite);
+/* Debug aid (no reference counterpart): fill the plan's workspace with the byte ``byte``
+ * (0xFF makes every double a NaN), ordered like the compute calls. The stage kernels read
+ * only workspace entries written earlier in the same step, so a step after a fill gives
+ * the same result; tests use it to show that. */
+int fct_plan_fill_workspace(FctPlan* plan, int byte, fct_stream_t stream);
 
 /*
  * Implicit vertical tracer diffusion (fesom_jax/tracer_diff.py:68-123 impl_vert_diff_one;
@@ -244,15 +263,15 @@ void fct_xla_adjoint(void* stream, void** buffers, const char* opaque, size_t op
 int fct_compute_w_adjoint(FctPlan* plan, const double* gw, const double* helem,
                           double* guv, int accumulate, fct_stream_t stream);
 
-/* The same step as fct_forward for callers that cannot allocate device memory at call
- * time (an XLA/JAX custom-call handler running inside a runtime that owns the GPU's
- * memory, a stream under CUDA-graph capture, a serving loop that must not block on the
- * allocator). Its scratch is a 64 MiB file-scope device array instead of the plan's
+/* The step of fct_forward (its fused stage kernels, whatever fct_plan_set_fused chose) for
+ * callers that cannot allocate device memory at call time (an XLA/JAX custom-call handler
+ * running inside a runtime that owns the GPU's memory, a serving loop that must not block
+ * on the allocator). Its scratch is a 64 MiB file-scope device array instead of the plan's
  * workspace, so the plan may have been created with any max_tracers; sizes whose scratch
  * exceeds the array return FCT_ERR_CAPACITY. No reference counterpart: the reference
  * lets XLA allocate its temporaries. The first call on a device looks up the array's
- * address (make it before any stream capture); all calls share the array, so calls that
- * overlap on the GPU race. */
+ * address (make it before any stream capture); all calls share the array, which keeps
+ * the last call's contents, so calls that overlap on the GPU race. */
 int fct_forward_noalloc(FctPlan* plan, const FctFields* fields, double dt, int ntr,
                         fct_stream_t stream);
 
@@ -285,6 +304,9 @@ typedef struct FctInstance {
   double* w_derived;        /* optional [nod2D,nl]: each step first derives w_e =
                                compute_w(uv, helem) (ale.py:309-365, step.py:367) into this
                                buffer and advects with it (w_e is then ignored); NULL = off */
+  unsigned long long* nonfinite; /* optional DEVICE counter: each step adds the number of
+                               non-finite T_new values it writes (NULL: the batch's own
+                               per-instance counter, or the serve engine's counter) */
 } FctInstance;
 
 typedef struct FctBatch FctBatch;
@@ -313,6 +335,15 @@ int fct_batch_step(FctBatch* b, int phase, fct_stream_t stream);
  * holds T after the run is buf[(first_phase + steps + 1) % 3]. */
 int fct_batch_run(FctBatch* b, int first_phase, int steps, fct_stream_t stream);
 
+/* Health check of a batch (as fct_plan_health): per-instance counts of non-finite T_new
+ * values written since the previous check into ``counts`` (n entries; may be NULL; 0 for
+ * instances that count into their own FctInstance.nonfinite). Synchronises ``stream``,
+ * resets the counters and returns FCT_ERR_NONFINITE when any count is non-zero. */
+int fct_batch_health(FctBatch* b, fct_stream_t stream, int64_t* counts);
+/* Debug aid (no reference counterpart), as fct_plan_fill_workspace for the batch's
+ * workspace arena, on ``stream``. */
+int fct_batch_fill_workspace(FctBatch* b, int byte, fct_stream_t stream);
+
 /*
  * Continuous batching: one FCT step for an arbitrary set of instances that changes from
  * call to call (requests joining and leaving), on any meshes. ``FctServe`` owns a
@@ -327,6 +358,9 @@ int fct_serve_create(int device, int max_instances, int64_t workspace_bytes, Fct
 int fct_serve_destroy(FctServe* s);
 int fct_serve_step(FctServe* s, const FctInstance* insts, const int32_t* phases, int n,
                    fct_stream_t stream);
+/* Health check of the serve engine's own counter (instances without a counter of their
+ * own), as fct_plan_health. */
+int fct_serve_health(FctServe* s, fct_stream_t stream, int64_t* n_nonfinite);
 
 /* Self-check of the division the kernels use for quotients that share a divisor (the
  * divisor's reciprocal computed once, then an FMA correction per quotient; see

@@ -1,5 +1,5 @@
-"""Per-step correctness gates beyond the max-norm tolerance, on the oracle (CPU) and on
-the CUDA result (GPU):
+"""Per-step correctness gates beyond the max-norm tolerance (``oracle/gates.py``), on the
+oracle (CPU) and on the CUDA result (GPU):
 
 * budget closure: sum(areasvol * (hnode_new * T_new - hnode * T)) equals
   dt * sum over nodes of the surface fluxes (LO vertical flux + limited antidiffusive
@@ -19,7 +19,7 @@ is checked against them because it equals the oracle's T_new to 1e-12."""
 import numpy as np
 import pytest
 
-from oracle import fct_np
+from oracle import fct_np, gates
 from tests.golden_cases import DT, cases
 
 CASES = ["T_step1", "S_step1", "T_ab2", "sharp_x5", "const"]
@@ -36,38 +36,15 @@ def _oracle(m, c):
 
 
 def closure_residual(m, c, T_new, inter):
-    lm = m.node_layer_mask
-    av = m.areasvol
-    content = np.where(lm, av * c["hnode"] * c["T"], 0.0)
-    lhs = np.sum(np.where(lm, av * c["hnode_new"] * T_new, 0.0)) - np.sum(content)
-    n = np.arange(m.nod2D)
-    top = m.ulevels_nod2D - 1
-    rhs = DT * np.sum(inter["flux_v_lo"][n, top] + inter["adf_v_lim"][n, top])
-    return abs(lhs - rhs) / np.sum(np.abs(content))
+    return gates.closure_residual(m, c["T"], c["hnode"], c["hnode_new"], T_new, inter, DT)
 
 
 def window(m, inter):
-    """The limiter's admissible window per node-layer (a4, tracer_adv.py:407-418)."""
-    k = np.arange(m.nl)[None, :]
-    nzmin = (m.ulevels_nod2D - 1)[:, None]
-    nzmax = (m.nlevels_nod2D - 1)[:, None]
-    own = (k == nzmin) | (k == nzmax - 1)
-    tv_max, tv_min = inter["tvert_max"], inter["tvert_min"]
-    w_max = np.where(own, tv_max, np.maximum(np.maximum(fct_np.shift_down(tv_max), tv_max),
-                                             fct_np.shift_up(tv_max)))
-    w_min = np.where(own, tv_min, np.minimum(np.minimum(fct_np.shift_down(tv_min), tv_min),
-                                             fct_np.shift_up(tv_min)))
-    return w_max, w_min
+    return gates.window(m, inter)
 
 
 def window_violations(m, c, T_new, inter):
-    w_max, w_min = window(m, inter)
-    valid = m.node_layer_mask & (m.areasvol > 0.0) & (c["hnode_new"] > 0.0)
-    scale = np.maximum(np.abs(c["T"]), np.abs(inter["LO"]))
-    with np.errstate(invalid="ignore"):
-        hi = w_max + 4.0 * np.spacing(np.maximum(np.abs(w_max), scale))
-        lo = w_min - 4.0 * np.spacing(np.maximum(np.abs(w_min), scale))
-    return np.argwhere(valid & ((T_new > hi) | (T_new < lo)))
+    return gates.window_violations(m, c["T"], c["hnode_new"], T_new, inter)
 
 
 @pytest.mark.parametrize("name", CASES)
