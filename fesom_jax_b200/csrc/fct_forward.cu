@@ -447,7 +447,9 @@ __device__ __forceinline__ void body_vert_impl(const Inst& in, int64_t n, int t0
       const double c = (bot ? 0.0 : -fmax(0.0, wd)) * v_bot;
       const double b_adv = b_top + b_bot;
       const double b = in.hnode_new[base + k] + b_adv;
-      const double Tm = LO(k > 0 ? k - 1 : 0), T0 = LO(k), Tp = k + 1 < L ? LO(k + 1) : 0.0;
+      // the neighbours above the surface and below the bottom enter with a zero
+      // coefficient; LO is 0 there in the reference, and this step never wrote them
+      const double Tm = surf ? 0.0 : LO(k - 1), T0 = LO(k), Tp = bot ? 0.0 : LO(k + 1);
       const double rhs = -(a * Tm + b_adv * T0 + c * Tp);
       const double md = b - a * cprev;
       cprev = c / md;

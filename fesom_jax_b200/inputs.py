@@ -188,11 +188,11 @@ def basin_taper(rings, nl: int, xp=np):
     nearest wall on that layer (:func:`wall_rings`, ``R = len(rings)``), 1 beyond ``R - 1``
     hops. ``xp`` is numpy or torch (the ring arrays must be of that kind)."""
     R = len(rings)
-    k = xp.arange(nl).reshape(1, -1)
     nlmin0 = rings[0][0]
+    k = xp.arange(nl).reshape(1, -1)
     taper = xp.ones((nlmin0.shape[0], nl), dtype=xp.float64)
     if xp is not np:
-        taper = taper.to(nlmin0.device)
+        k, taper = k.to(nlmin0.device), taper.to(nlmin0.device)
     for r in range(R - 1, -1, -1):
         nlmin, ulmax, coast = rings[r]
         wall = (coast.reshape(-1, 1) | (k < ulmax.reshape(-1, 1) - 1)

@@ -165,3 +165,26 @@ def test_serving_counts_nonfinite_requests(torch, pi):
     st = eng.run(reqs)
     assert st["completed"] == 3 and st["nonfinite_requests"] == 0
     eng.close()
+
+
+@pytest.mark.parametrize("fused", [True, False])
+def test_every_option_ignores_a_poisoned_workspace(torch, pi, fused):
+    """The step with every option (w_split w_i, zstar Z3d/zbar3), fused and one kernel per
+    stage, gives the same bits on a plan whose workspace was filled with NaN bytes as on a
+    fresh plan: no stage reads a workspace entry it did not write in the same call."""
+    from fesom_jax_b200.tracer_adv import FctPlan
+    from tests.golden_cases import cases
+    c = cases(pi)["T_wsplit_zstar"]
+    d = lambda x: _dev(torch, x)  # noqa: E731
+    args = [d(c[k]) for k in ("uv", "w_e", "helem", "hnode", "hnode_new", "T", "T_old")]
+    kw = {k: d(v) for k, v in c["kw"].items()}
+    outs = []
+    for poison in (False, True):
+        plan = FctPlan(pi, 0, max_tracers=1)
+        plan.set_fused(fused)
+        if poison:
+            plan.fill_workspace(0xFF)
+        outs.append(plan.forward(*args, 3600.0, **kw).cpu().numpy())
+        assert plan.health() == 0
+        plan.close()
+    assert np.array_equal(outs[0], outs[1])
