@@ -313,9 +313,10 @@ def run_ours(args, D: Dist) -> dict | None:
     info = ens.info()
     S = cfg["fct_steps"]
     stream = torch.cuda.current_stream(dev)
-    tune = ens.autotune(steps=2) if not args.chunk else None
-    if args.chunk:
-        ens.set_chunk(args.chunk)
+    fixed = bool(args.chunk or args.levels)
+    tune = ens.autotune(steps=2) if not fixed else None
+    if fixed:
+        ens.set_mapping(args.chunk or ens.chunk, args.levels or ens.levels)
     torch.cuda.synchronize()
     for _ in range(args.warmup):
         ens.run(S)
@@ -369,7 +370,8 @@ def run_ours(args, D: Dist) -> dict | None:
                              alg_bytes_per_step=alg,
                              issue=issue_roofline(value / D.world, clk)),
                gpu_launches=n_kernels * S * args.steps,
-               tuning=dict(chunk=ens.chunk, candidates_ms_per_2_steps=tune))
+               tuning=dict(tracers_per_thread=ens.chunk, levels_per_thread=ens.levels,
+                           candidates_ms_per_2_steps=tune))
 
     # plain one-instance-per-launch comparison (the reference's call granularity:
     # one tracer per advect_one_fct call), member 0, one FCT step per call
@@ -394,7 +396,7 @@ def run_ours(args, D: Dist) -> dict | None:
         tp = e0.elapsed_time(e1) / 1e3
         out["plain"] = dict(value=reps * cfg["ntr"] * mesh.n_wet_layers / tp, unit=UNIT,
                             how="fct_forward, 1 tracer per call, 1 FCT step per call")
-    tuned = ens.chunk
+    tuned = (ens.chunk, ens.levels)
     ens.close()   # the end-to-end run below builds its own ensemble
     del ens
     torch.cuda.empty_cache()
@@ -412,7 +414,7 @@ def run_ours(args, D: Dist) -> dict | None:
     return out
 
 
-def e2e_host(args, mesh, cfg, dev, per_thread: int = 0) -> dict:
+def e2e_host(args, mesh, cfg, dev, per_thread=None) -> dict:
     """The same metric through the public ensemble API with HOST buffers: every bench step
     copies each member's inputs (T, T_old, uv, w_e) from pinned host memory, runs the
     FCT steps and copies the final T back; copies are inside the timed region. Members are
@@ -444,8 +446,8 @@ def e2e_host(args, mesh, cfg, dev, per_thread: int = 0) -> dict:
     torch.cuda.empty_cache()
     for e in ens:
         e.build()
-        if per_thread:   # the main run's autotuned tracers per thread
-            e.set_chunk(per_thread)
+        if per_thread:   # the main run's autotuned thread mapping
+            e.set_mapping(*per_thread)
     S = cfg["fct_steps"]
     main = torch.cuda.current_stream(dev)
     h2d = sum(h[k].numel() * 8 for h in host for k in ("T", "T_old", "uv", "w_e"))
@@ -729,7 +731,10 @@ def main():
     ap.add_argument("--members", type=int, default=0)
     ap.add_argument("--fct-steps", type=int, default=0)
     ap.add_argument("--ntr", type=int, default=0, help="override tracers per member")
-    ap.add_argument("--chunk", type=int, default=0, help="fix the tracer chunk (no autotune)")
+    ap.add_argument("--chunk", type=int, default=0,
+                    help="fix the tracers per thread (no autotune)")
+    ap.add_argument("--levels", type=int, default=0,
+                    help="fix the levels per thread (no autotune)")
     ap.add_argument("--workspace-gb", type=float, default=40.0)
     ap.add_argument("--e2e-members", type=int, default=8)
     ap.add_argument("--no-e2e", action="store_true")

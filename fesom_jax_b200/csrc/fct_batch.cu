@@ -136,12 +136,7 @@ int fct_batch_create(const FctInstance* insts, int n, int64_t budget, FctBatch**
       const Workspace ws =
           carve_workspace(B->arena + off, P->N, P->E, P->Ed, P->L, wchunk[i], /*fused=*/true);
       off += ws_doubles[i];
-      d.max_iface = std::max(d.max_iface, P->hm.n_iface);
-      d.max_layer = std::max(d.max_layer, P->hm.n_layer);
-      d.max_edge = std::max(d.max_edge, P->hm.n_edge);
-      d.max_elem = std::max(d.max_elem, P->hm.n_elem);
-      d.max_dense = std::max(d.max_dense, int64_t(P->N) * P->L);
-      d.max_nodes = std::max(d.max_nodes, int64_t(P->N));
+      dims_cover(d, P);
       d.ntr = q.ntr;
       d.chunk = wchunk[i];
       B->total_updates += int64_t(q.ntr) * P->hm.n_layer;
@@ -173,7 +168,8 @@ int fct_batch_create(const FctInstance* insts, int n, int64_t budget, FctBatch**
     }
     d.any_wi = false;
     d.copy_dry = false;
-    d.per_thread = d.chunk < 8 ? d.chunk : 8;
+    d.per_thread = std::min(d.chunk, 2);
+    d.lpt = 4;
     gr.dims = d;
   }
   e = cudaMalloc(&B->d_health, size_t(n) * sizeof(unsigned long long));
@@ -209,15 +205,25 @@ int fct_batch_destroy(FctBatch* B) {
   return FCT_OK;
 }
 
-int fct_batch_set_chunk(FctBatch* B, int chunk) {
+int fct_batch_set_mapping(FctBatch* B, int tracers_per_thread, int levels_per_thread) {
   if (!B) return set_error(FCT_ERR_INVALID, "batch is NULL");
-  if (chunk != 1 && chunk != 2 && chunk != 4 && chunk != 8)
-    return set_error(FCT_ERR_INVALID, "chunk must be 1, 2, 4 or 8");
+  const int t = tracers_per_thread, l = levels_per_thread;
+  if ((t != 1 && t != 2 && t != 4 && t != 8) || (l != 1 && l != 2 && l != 4 && l != 8))
+    return set_error(FCT_ERR_INVALID, "tracers and levels per thread must be 1, 2, 4 or 8");
   std::lock_guard<std::mutex> lk(B->graph_mu);
-  for (auto& g : B->groups) g.dims.per_thread = chunk;
-  for (auto& kv : B->graphs) cudaGraphExecDestroy(kv.second);   // recapture with the new chunk
+  for (auto& g : B->groups) {
+    g.dims.per_thread = t;
+    g.dims.lpt = l;
+  }
+  for (auto& kv : B->graphs) cudaGraphExecDestroy(kv.second);   // recapture with the mapping
   B->graphs.clear();
   return FCT_OK;
+}
+
+int fct_batch_set_chunk(FctBatch* B, int chunk) {
+  if (!B) return set_error(FCT_ERR_INVALID, "batch is NULL");
+  const int lpt = B->groups.empty() ? 4 : B->groups[0].dims.lpt;
+  return fct_batch_set_mapping(B, chunk, lpt);
 }
 
 int fct_batch_info(const FctBatch* B, int64_t out[6]) {
@@ -235,7 +241,7 @@ int fct_batch_info(const FctBatch* B, int64_t out[6]) {
       const int csz = std::min(chunk, g.dims.ntr - c0);
       per_chunk_launches += stage_launches(csz, g.dims.per_thread);
     }
-    const int stages = (g.dims.fused ? 4 : 7) + (g.dims.any_wi ? 1 : 0) +
+    const int stages = (g.dims.fused ? 5 : 7) + (g.dims.any_wi ? 1 : 0) +
                        (g.dims.any_vdiff ? 1 : 0);
     launches += 1 + (g.dims.any_derive_w ? 1 : 0) + int64_t(stages) * per_chunk_launches;
   }
@@ -523,18 +529,13 @@ int fct_serve_step(FctServe* S, const FctInstance* insts, const int32_t* phases,
     const int ntr = insts[order[j0]].ntr;
     const FctPlan* P0 = insts[order[j0]].plan;
     while (j1 < n && insts[order[j1]].ntr == ntr && insts[order[j1]].plan == P0) {
-      const FctPlan* P = insts[order[j1]].plan;
-      d.max_iface = std::max(d.max_iface, P->hm.n_iface);
-      d.max_layer = std::max(d.max_layer, P->hm.n_layer);
-      d.max_edge = std::max(d.max_edge, P->hm.n_edge);
-      d.max_elem = std::max(d.max_elem, P->hm.n_elem);
-      d.max_dense = std::max(d.max_dense, int64_t(P->N) * P->L);
-      d.max_nodes = std::max(d.max_nodes, int64_t(P->N));
+      dims_cover(d, insts[order[j1]].plan);
       ++j1;
     }
     d.ntr = ntr;
     d.chunk = 0;
-    d.per_thread = ntr >= 4 ? 4 : ntr;
+    d.per_thread = P0->per_thread;
+    d.lpt = P0->lpt;
     for (int j = j0; j < j1; ++j)
       if (insts[order[j]].w_derived) d.any_derive_w = true;
     d.any_wi = false;

@@ -23,91 +23,11 @@
 // contiguous chunk in the interleaved layout), so the gathers overlap.
 #include <algorithm>
 
-#include "fct_div.cuh"
-#include "fct_host.h"
+#include "fct_device.cuh"
 
 namespace fct {
 
 namespace {
-
-__device__ __forceinline__ double ab2(double T, double To) { return kAbOld * To + kAbNew * T; }
-__device__ __forceinline__ double safe_nz(double x) { return x == 0.0 ? 1.0 : x; }
-
-__device__ __forceinline__ int64_t lane_index() {
-  return int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-}
-
-template <class T>
-__device__ __forceinline__ T ld(const T* p) { return __ldg(p); }
-
-// Address of tracer t at entity-level q: interleaved q*tg + t (below 2^32: the batch
-// engine checks every interleaved array against it), else t*stride + q.
-template <bool IL>
-__device__ __forceinline__ int64_t tix(uint32_t q, int t, int64_t stride, int tg) {
-  return IL ? int64_t(q * uint32_t(tg) + uint32_t(t)) : int64_t(t) * stride + q;
-}
-
-// Tracers [t0, t0+NTR) of entity-level q.
-template <int NTR, bool IL>
-__device__ __forceinline__ void ldn(const double* __restrict__ p, uint32_t q, int t0,
-                                    int64_t stride, int tg, double (&v)[NTR]) {
-  if constexpr (IL && (NTR % 2 == 0)) {
-    const double* b = p + (q * uint32_t(tg) + uint32_t(t0));
-    if ((reinterpret_cast<uintptr_t>(b) & 15) == 0) {
-#pragma unroll
-      for (int i = 0; i < NTR; i += 2) {
-        const double2 x = __ldg(reinterpret_cast<const double2*>(b + i));
-        v[i] = x.x;
-        v[i + 1] = x.y;
-      }
-      return;
-    }
-  }
-#pragma unroll
-  for (int i = 0; i < NTR; ++i) v[i] = __ldg(p + tix<IL>(q, t0 + i, stride, tg));
-}
-
-template <int NTR, bool IL>
-__device__ __forceinline__ void stn(double* __restrict__ p, uint32_t q, int t0, int64_t stride,
-                                    int tg, const double (&v)[NTR]) {
-  if constexpr (IL && (NTR % 2 == 0)) {
-    double* b = p + (q * uint32_t(tg) + uint32_t(t0));
-    if ((reinterpret_cast<uintptr_t>(b) & 15) == 0) {
-#pragma unroll
-      for (int i = 0; i < NTR; i += 2)
-        *reinterpret_cast<double2*>(b + i) = make_double2(v[i], v[i + 1]);
-      return;
-    }
-  }
-#pragma unroll
-  for (int i = 0; i < NTR; ++i) p[tix<IL>(q, t0 + i, stride, tg)] = v[i];
-}
-
-// tie counts (bytes) of tracers [t0, t0+NTR) at entity-level q
-template <int NTR, bool IL>
-__device__ __forceinline__ void stc(uint8_t* __restrict__ p, uint32_t q, int t0, int64_t stride,
-                                    int tg, const int (&v)[NTR]) {
-#pragma unroll
-  for (int i = 0; i < NTR; ++i) p[tix<IL>(q, t0 + i, stride, tg)] = uint8_t(v[i]);
-}
-
-// Health counter (the reference's finiteness gate, fesom_jax/diagnostics.py:31-101): add
-// the number of non-finite values among ``v`` to ``*counter``. Finite results cost a test
-// per value and no atomic.
-template <int NTR>
-__device__ __forceinline__ void count_nonfinite(unsigned long long* counter,
-                                                const double (&v)[NTR]) {
-  if (!counter) return;
-  unsigned bad = 0;
-#pragma unroll
-  for (int t = 0; t < NTR; ++t) bad += isfinite(v[t]) ? 0u : 1u;
-  if (bad) atomicAdd(counter, static_cast<unsigned long long>(bad));
-}
-
-// k in [r & 255, (r >> 8) & 255): the packed level ranges of the fused stages' slots
-__device__ __forceinline__ bool in_range(int k, unsigned r) {
-  return k >= int(r & 255u) && k < int((r >> 8) & 255u);
-}
 
 // ---------------------------------------------------------------- edge_vflux
 __device__ __forceinline__ void body_vflux(const Inst& in, int64_t i) {
@@ -132,70 +52,6 @@ __device__ __forceinline__ void body_vflux(const Inst& in, int64_t i) {
   in.ws.vflux[lq(e, L, k)] = t1 + t2;
 }
 
-// ---------------------------------------------------- tracer_gradient_elements
-// Gradient of T on cell `el` (nodes v0, v1, v2) at level k; the stored (elem_grad) and the
-// recomputed (fused stages) gradients both come from here, so they are the same bits.
-template <int NTR>
-__device__ __forceinline__ void cell_grad_vals(const Inst& in, int el, const double (&a0)[NTR],
-                                               const double (&a1)[NTR], const double (&a2)[NTR],
-                                               double (&gx)[NTR], double (&gy)[NTR]) {
-  // gradient_sca row of the cell: 48 bytes, 16-byte aligned (3 double2 loads)
-  const double2* g = reinterpret_cast<const double2*>(in.m->gsca + 6 * int64_t(el));
-  const double2 p = __ldg(g), q = __ldg(g + 1), r = __ldg(g + 2);
-  const double g0 = p.x, g1 = p.y, g2 = q.x, g3 = q.y, g4 = r.x, g5 = r.y;
-#pragma unroll
-  for (int t = 0; t < NTR; ++t) {
-    gx[t] = g0 * a0[t] + g1 * a1[t] + g2 * a2[t];
-    gy[t] = g3 * a0[t] + g4 * a1[t] + g5 * a2[t];
-  }
-}
-
-template <int NTR, bool IL>
-__device__ __forceinline__ void cell_grad(const Inst& in, int el, int v0, int v1, int v2, int k,
-                                          int t0, double (&gx)[NTR], double (&gy)[NTR]) {
-  const int L = in.m->L;
-  double a0[NTR], a1[NTR], a2[NTR];
-  ldn<NTR, IL>(in.T, lq(v0, L, k), t0, in.tstride, in.tg, a0);
-  ldn<NTR, IL>(in.T, lq(v1, L, k), t0, in.tstride, in.tg, a1);
-  ldn<NTR, IL>(in.T, lq(v2, L, k), t0, in.tstride, in.tg, a2);
-  cell_grad_vals<NTR>(in, el, a0, a1, a2, gx, gy);
-}
-
-// The same gradient when the tracer values at the lane's own node (vertex `pos` of the
-// cell) are already in registers: only the other two vertices are gathered.
-template <int NTR, bool IL>
-__device__ __forceinline__ void cell_grad_own(const Inst& in, int el, int v0, int v1, int v2,
-                                              int pos, const double (&own)[NTR], int k, int t0,
-                                              double (&gx)[NTR], double (&gy)[NTR]) {
-  const int L = in.m->L;
-  double a0[NTR], a1[NTR], a2[NTR];
-  if (pos == 0) {
-    ldn<NTR, IL>(in.T, lq(v1, L, k), t0, in.tstride, in.tg, a1);
-    ldn<NTR, IL>(in.T, lq(v2, L, k), t0, in.tstride, in.tg, a2);
-#pragma unroll
-    for (int t = 0; t < NTR; ++t) a0[t] = own[t];
-  } else if (pos == 1) {
-    ldn<NTR, IL>(in.T, lq(v0, L, k), t0, in.tstride, in.tg, a0);
-    ldn<NTR, IL>(in.T, lq(v2, L, k), t0, in.tstride, in.tg, a2);
-#pragma unroll
-    for (int t = 0; t < NTR; ++t) a1[t] = own[t];
-  } else {
-    ldn<NTR, IL>(in.T, lq(v0, L, k), t0, in.tstride, in.tg, a0);
-    ldn<NTR, IL>(in.T, lq(v1, L, k), t0, in.tstride, in.tg, a1);
-#pragma unroll
-    for (int t = 0; t < NTR; ++t) a2[t] = own[t];
-  }
-  cell_grad_vals<NTR>(in, el, a0, a1, a2, gx, gy);
-}
-
-template <int NTR, bool IL>
-__device__ __forceinline__ void cell_grad(const Inst& in, int el, int k, int t0,
-                                          double (&gx)[NTR], double (&gy)[NTR]) {
-  const int* en = in.m->enodes + 3 * int64_t(el);
-  cell_grad<NTR, IL>(in, el, ld(en), ld(en + 1), ld(en + 2), k, t0, gx, gy);
-}
-
-
 template <int NTR, bool IL>
 __device__ __forceinline__ void body_elem_grad(const Inst& in, int64_t i, int t0, int w0) {
   const DevMesh& m = *in.m;
@@ -209,17 +65,8 @@ __device__ __forceinline__ void body_elem_grad(const Inst& in, int64_t i, int t0
   stn<NTR, IL>(in.ws.gy, q, w0, in.ws.sE, in.wtg, gy);
 }
 
-// Upwind vertical flux at interface j (layer-masked), tracer_adv.py:108-120, given the
-// tracer below (Tb = T[j]) and above (Ta = T[j-1], edge-replicated at j = 0).
-__device__ __forceinline__ double vflux_up(double Tb, double Ta, double w, double area) {
-  const double aw = fabs(w);
-  return -0.5 * (Tb * (w + aw) + Ta * (w - aw)) * area;
-}
-
 // -------------------------------- LO solution, node-average gradient, adf_v
-// FUSED: packed edge slots, and the cell gradients recomputed from T instead of read
-// from the elem_grad stage.
-template <int NTR, bool IL, bool FUSED>
+template <int NTR, bool IL>
 __device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i, int t0, int w0) {
   const DevMesh& m = *in.m;
   if (i >= m.n_iface) return;
@@ -265,42 +112,22 @@ __device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i, int t0, 
 #pragma unroll
     for (int t = 0; t < NTR; ++t) div[t] = 0.0;
     const int e0 = rec.y, e1 = rec.y + int((pk >> 16) & 255u);
-    if constexpr (FUSED) {
-      // loads are unconditional (all in bounds) and inactive edges are selected away,
-      // so consecutive slots' loads overlap
-#pragma unroll 2
-      for (int j = e0; j < e1; ++j) {
-        const int4 sl = __ldg(m.ne4 + j);
-        const bool on = in_range(k, unsigned(sl.z));
-        const bool second = sl.x & 1;
-        const double vf = ld(in.ws.vflux + lq(sl.x >> 1, L, k));
-        const double avf = fabs(vf);
-        double To[NTR];
-        ldn<NTR, IL>(in.T, lq(sl.y, L, k), t0, ts, tg, To);
+    for (int j = e0; j < e1; ++j) {
+      const int idx = ld(m.ne_idx + j), e = idx >> 1;
+      if (k < ld(m.ekmin + e) || k >= ld(m.ekmax + e)) continue;   // vflux == 0 there
+      const int oth = ld(m.ne_oth + j);
+      const double vf = ld(in.ws.vflux + lq(e, L, k));
+      const double avf = fabs(vf);
+      double To[NTR];
+      ldn<NTR, IL>(in.T, lq(oth, L, k), t0, ts, tg, To);
 #pragma unroll
-        for (int t = 0; t < NTR; ++t) {
-          const double T1 = second ? To[t] : Tc[t], T2 = second ? Tc[t] : To[t];
-          const double fl = -0.5 * (T1 * (vf + avf) + T2 * (vf - avf));
-          div[t] = on ? div[t] + (second ? -fl : fl) : div[t];
-        }
-      }
-    } else {
-      for (int j = e0; j < e1; ++j) {
-        const int idx = ld(m.ne_idx + j), e = idx >> 1;
-        if (k < ld(m.ekmin + e) || k >= ld(m.ekmax + e)) continue;   // vflux == 0 there
-        const int oth = ld(m.ne_oth + j);
-        const double vf = ld(in.ws.vflux + lq(e, L, k));
-        const double avf = fabs(vf);
-        double To[NTR];
-        ldn<NTR, IL>(in.T, lq(oth, L, k), t0, ts, tg, To);
-#pragma unroll
-        for (int t = 0; t < NTR; ++t) {
-          const double T1 = (idx & 1) ? To[t] : Tc[t], T2 = (idx & 1) ? Tc[t] : To[t];
-          const double fl = -0.5 * (T1 * (vf + avf) + T2 * (vf - avf));
-          div[t] += (idx & 1) ? -fl : fl;
-        }
+      for (int t = 0; t < NTR; ++t) {
+        const double T1 = (idx & 1) ? To[t] : Tc[t], T2 = (idx & 1) ? Tc[t] : To[t];
+        const double fl = -0.5 * (T1 * (vf + avf) + T2 * (vf - avf));
+        div[t] += (idx & 1) ? -fl : fl;
       }
     }
+  
     const bool valid = (hnn > 0.0) && (av > 0.0);
     double lo[NTR];
 #pragma unroll
@@ -313,15 +140,14 @@ __device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i, int t0, 
 #pragma unroll
     for (int t = 0; t < NTR; ++t) nx[t] = ny[t] = 0.0;
     const int c0 = rec.z, c1 = rec.z + int(pk >> 24);
-    if constexpr (FUSED) {
-      for (int j = c0; j < c1; ++j) {
-        const unsigned r = unsigned(ld(m.nelr + j));
-        const int4 sl = __ldg(m.nel4 + j);   // in bounds: issued beside the range word
-        if (!in_range(k, r)) continue;
-        const double a = ld(m.earea + sl.x);
+    for (int j = c0; j < c1; ++j) {
+      const int el = ld(m.nel_idx + j);
+      if (k >= ld(m.eul + el) && k < ld(m.enl + el)) {
+        const double a = ld(m.earea + el);
+        const uint32_t qe = lq(el, L, k);
         double gx[NTR], gy[NTR];
-        cell_grad_own<NTR, IL>(in, sl.x, sl.y, sl.z, sl.w, int((r >> 16) & 3u), Tc, k, t0, gx,
-                               gy);
+        ldn<NTR, IL>(in.ws.gx, qe, w0, in.ws.sE, in.wtg, gx);
+        ldn<NTR, IL>(in.ws.gy, qe, w0, in.ws.sE, in.wtg, gy);
 #pragma unroll
         for (int t = 0; t < NTR; ++t) {
           nx[t] += gx[t] * a;
@@ -329,28 +155,10 @@ __device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i, int t0, 
         }
         den += a;
       }
-    } else {
-      for (int j = c0; j < c1; ++j) {
-        const int el = ld(m.nel_idx + j);
-        if (k >= ld(m.eul + el) && k < ld(m.enl + el)) {
-          const double a = ld(m.earea + el);
-          const uint32_t qe = lq(el, L, k);
-          double gx[NTR], gy[NTR];
-          ldn<NTR, IL>(in.ws.gx, qe, w0, in.ws.sE, in.wtg, gx);
-          ldn<NTR, IL>(in.ws.gy, qe, w0, in.ws.sE, in.wtg, gy);
-#pragma unroll
-          for (int t = 0; t < NTR; ++t) {
-            nx[t] += gx[t] * a;
-            ny[t] += gy[t] * a;
-          }
-          den += a;
-        }
-      }
     }
+  
     const Rcp rdd = rcp(den > 0.0 ? den : 1.0);
-    if constexpr (!FUSED) {   // kept for the reverse pass (tracer independent)
-      if (w0 == 0) in.ws.nden[qn] = rdd.y;
-    }
+    if (w0 == 0) in.ws.nden[qn] = rdd.y;   // kept for the reverse pass (tracer independent)
 #pragma unroll
     for (int t = 0; t < NTR; ++t) {
       nx[t] = divr(nx[t], rdd);
@@ -467,7 +275,7 @@ __device__ __forceinline__ void body_vert_impl(const Inst& in, int64_t n, int t0
 }
 
 // -------------------------- fill_up_dn_grad + adv_flux_hor_ho - LO flux = adf_h
-template <int NTR, bool IL, bool FUSED>
+template <int NTR, bool IL>
 __device__ __forceinline__ void body_edge_adf(const Inst& in, int64_t i, int t0, int w0) {
   const DevMesh& m = *in.m;
   if (i >= m.n_edge) return;
@@ -488,18 +296,13 @@ __device__ __forceinline__ void body_edge_adf(const Inst& in, int64_t i, int t0,
   ldn<NTR, IL>(in.T_old, q2, t0, ts, tg, O2);
   if (use_tri) {
     // both cells are wet at k here (k is above every adjacent cell's bottom)
-    if constexpr (FUSED) {
-      const int4 cu = __ldg(m.eud4 + 2 * e), cd = __ldg(m.eud4 + 2 * e + 1);
-      cell_grad<NTR, IL>(in, cu.x, cu.y, cu.z, cu.w, k, t0, g0, g2);
-      cell_grad<NTR, IL>(in, cd.x, cd.y, cd.z, cd.w, k, t0, g1, g3);
-    } else {
-      const int up = ld(m.eupdn + 2 * e), dn = ld(m.eupdn + 2 * e + 1);
-      const uint32_t qu = lq(up, L, k), qd = lq(dn, L, k);
-      ldn<NTR, IL>(in.ws.gx, qu, w0, in.ws.sE, in.wtg, g0);
-      ldn<NTR, IL>(in.ws.gx, qd, w0, in.ws.sE, in.wtg, g1);
-      ldn<NTR, IL>(in.ws.gy, qu, w0, in.ws.sE, in.wtg, g2);
-      ldn<NTR, IL>(in.ws.gy, qd, w0, in.ws.sE, in.wtg, g3);
-    }
+    const int up = ld(m.eupdn + 2 * e), dn = ld(m.eupdn + 2 * e + 1);
+    const uint32_t qu = lq(up, L, k), qd = lq(dn, L, k);
+    ldn<NTR, IL>(in.ws.gx, qu, w0, in.ws.sE, in.wtg, g0);
+    ldn<NTR, IL>(in.ws.gx, qd, w0, in.ws.sE, in.wtg, g1);
+    ldn<NTR, IL>(in.ws.gy, qu, w0, in.ws.sE, in.wtg, g2);
+    ldn<NTR, IL>(in.ws.gy, qd, w0, in.ws.sE, in.wtg, g3);
+  
   } else {
     ldn<NTR, IL>(in.ws.gnx, q1, w0, in.ws.sN, in.wtg, g0);
     ldn<NTR, IL>(in.ws.gnx, q2, w0, in.ws.sN, in.wtg, g1);
@@ -695,120 +498,8 @@ __device__ __forceinline__ void body_node_factors(const Inst& in, int64_t i, int
   stn<NTR, IL>(in.ws.fminus, qn, w0, sN, in.wtg, mi);
 }
 
-// ------- fused zalesak a2 + a3 + a4 + b1 + b2: cluster bounds, window, factors
-// The cluster bound of node n at level k is the max (min) of max(LO, T) (min(LO, T)) over
-// the nodes of n's cells that are wet at k, padded with -BIG (+BIG) when one of n's cells
-// is dry at k (tracer_adv.py:389-405). Every cell of n has two edges at n, so those nodes
-// are n itself (when any cell is wet at k) and the edge neighbours with a wet cell at k:
-// one gather over the packed edge slots, which also sums the antidiffusive fluxes (b1).
-// max/min are exact, so the result equals the per-cell evaluation bit for bit.
-// The a4 window (k-1, k, k+1 of the same column) comes from the neighbouring lanes'
-// cluster bounds in shared memory: a block computes bounds for its lanes plus one halo
-// lane on each side, and finishes the factors for its core lanes only.
-template <int NTR, bool IL>
-__device__ __forceinline__ void node_limit(const Inst& in, int64_t lane, bool core, int t0,
-                                           int w0, int tid, int nb, double* smx, double* smn) {
-  const DevMesh& m = *in.m;
-  const bool valid = lane >= 0 && lane < m.n_layer;
-  const int L = m.L;
-  const int64_t sN = in.ws.sN;
-  int n = 0, k = 0;
-  uint32_t qn = 0;
-  unsigned pk = 0;
-  double mx[NTR], mn[NTR], sp[NTR], sm[NTR], lo[NTR];
-  if (valid) {
-    const int4 rec = __ldg(m.layer4 + lane);
-    pk = unsigned(rec.w);
-    n = lane_ent(uint32_t(rec.x));
-    k = lane_lev(uint32_t(rec.x));
-    qn = lq(n, L, k);
-#pragma unroll
-    for (int t = 0; t < NTR; ++t) {
-      mx[t] = -INFINITY; mn[t] = INFINITY; sp[t] = 0.0; sm[t] = 0.0;
-    }
-    bool own = false, off = false;
-    const int e0 = rec.y, e1 = rec.y + int((pk >> 16) & 255u);
-#pragma unroll 2
-    for (int j = e0; j < e1; ++j) {
-      const int4 sl = __ldg(m.ne4 + j);
-      const unsigned tr = unsigned(sl.w);
-      const bool c1 = in_range(k, tr & 0xffffu);
-      const bool has2 = ((tr >> 16) & 255u) != kNoCell;
-      const bool c2 = has2 && in_range(k, tr >> 16);
-      const bool wet = c1 || c2;
-      own = own || wet;
-      off = off || !c1 || (has2 && !c2);
-      const bool on = in_range(k, unsigned(sl.z));
-      const bool second = sl.x & 1;
-      const uint32_t qo = lq(sl.y, L, k);
-      double a[NTR], lv[NTR], tv[NTR];
-      ldn<NTR, IL>(in.ws.adfh, lq(sl.x >> 1, L, k), w0, in.ws.sEd, in.wtg, a);
-      ldn<NTR, IL>(in.ws.lo, qo, w0, sN, in.wtg, lv);
-      ldn<NTR, IL>(in.T, qo, t0, in.tstride, in.tg, tv);
-#pragma unroll
-      for (int t = 0; t < NTR; ++t) {
-        mx[t] = wet ? fmax(mx[t], fmax(lv[t], tv[t])) : mx[t];
-        mn[t] = wet ? fmin(mn[t], fmin(lv[t], tv[t])) : mn[t];
-        const double sv = second ? -a[t] : a[t];
-        sp[t] = on ? sp[t] + fmax(sv, 0.0) : sp[t];
-        sm[t] = on ? sm[t] + fmin(sv, 0.0) : sm[t];
-      }
-    }
-    double tv[NTR];
-    ldn<NTR, IL>(in.ws.lo, qn, w0, sN, in.wtg, lo);
-    ldn<NTR, IL>(in.T, qn, t0, in.tstride, in.tg, tv);
-#pragma unroll
-    for (int t = 0; t < NTR; ++t) {
-      if (own) {
-        mx[t] = fmax(mx[t], fmax(lo[t], tv[t]));
-        mn[t] = fmin(mn[t], fmin(lo[t], tv[t]));
-      }
-      if (off) {
-        mx[t] = fmax(mx[t], -kBig);
-        mn[t] = fmin(mn[t], kBig);
-      }
-      smx[t * 256 + tid] = mx[t];
-      smn[t * 256 + tid] = mn[t];
-    }
-  }
-  __syncthreads();
-  if (!valid || !core) return;
-  const int nzmin = int(pk & 255u), nzmax = int((pk >> 8) & 255u);
-  if (k != nzmin && k != nzmax - 1) {   // interior: window over k-1, k, k+1 (lanes +-1)
-#pragma unroll
-    for (int t = 0; t < NTR; ++t) {
-      mx[t] = fmax(fmax(smx[t * 256 + tid - nb], mx[t]), smx[t * 256 + tid + nb]);
-      mn[t] = fmin(fmin(smn[t * 256 + tid - nb], mn[t]), smn[t * 256 + tid + nb]);
-    }
-  }
-  const double av = ld(m.areasvol + qn), hnn = ld(in.hnode_new + qn);
-  const bool valid_n = (av > 0.0) && (hnn > 0.0);
-  const double sa = av > 0.0 ? av : 1.0, sh = hnn > 0.0 ? hnn : 1.0;
-  const Rcp rsa = rcp(sa), rsh = rcp(sh);
-  const double dt = in.dt;
-  double ft[NTR], fb[NTR];
-  ldn<NTR, IL>(in.ws.adfv, qn, w0, sN, in.wtg, ft);
-  ldn<NTR, IL>(in.ws.adfv, qn + 1, w0, sN, in.wtg, fb);   // k+1 <= nzmax < L
-  double pf[NTR], mf[NTR];
-#pragma unroll
-  for (int t = 0; t < NTR; ++t) {
-    const double plus = (fmax(ft[t], 0.0) + fmax(-fb[t], 0.0)) + sp[t];
-    const double minus = (fmin(ft[t], 0.0) + fmin(-fb[t], 0.0)) + sm[t];
-    pf[t] = 1.0;
-    mf[t] = 1.0;
-    if (valid_n) {
-      const double flux_pos = divr(divr(plus * dt, rsa), rsh) + kFluxEps;
-      const double flux_neg = divr(divr(minus * dt, rsa), rsh) - kFluxEps;
-      pf[t] = fmin(1.0, (mx[t] - lo[t]) / flux_pos);
-      mf[t] = fmin(1.0, (mn[t] - lo[t]) / flux_neg);
-    }
-  }
-  stn<NTR, IL>(in.ws.pf, qn, w0, sN, in.wtg, pf);
-  stn<NTR, IL>(in.ws.mf, qn, w0, sN, in.wtg, mf);
-}
-
 // ---------- zalesak b3 + flux2dtracer_fct + ale_reconstruct: T_new on layers
-template <int NTR, bool IL, bool FUSED>
+template <int NTR, bool IL>
 __device__ __forceinline__ void body_node_final(const Inst& in, int64_t i, int t0, int w0) {
   const DevMesh& m = *in.m;
   if (i >= m.n_layer) return;
@@ -861,44 +552,22 @@ __device__ __forceinline__ void body_node_final(const Inst& in, int64_t i, int t
 #pragma unroll
   for (int t = 0; t < NTR; ++t) hsc[t] = 0.0;
   const int e0 = rec.y, e1 = rec.y + int((pk >> 16) & 255u);
-  if constexpr (FUSED) {
-#pragma unroll 2
-    for (int j = e0; j < e1; ++j) {
-      const int4 sl = __ldg(m.ne4 + j);
-      const bool on = in_range(k, unsigned(sl.z));
-      const bool second = sl.x & 1;
-      const uint32_t qo = lq(sl.y, L, k);
-      double a[NTR], pfo[NTR], mfo[NTR];
-      ldn<NTR, IL>(in.ws.adfh, lq(sl.x >> 1, L, k), w0, in.ws.sEd, in.wtg, a);
-      ldn<NTR, IL>(in.ws.pf, qo, w0, sN, in.wtg, pfo);
-      ldn<NTR, IL>(in.ws.mf, qo, w0, sN, in.wtg, mfo);
+  for (int j = e0; j < e1; ++j) {
+    const int idx = ld(m.ne_idx + j), e = idx >> 1;
+    if (k < ld(m.ekmin + e) || k >= ld(m.ekmax + e)) continue;   // no flux on this level
+    const uint32_t qo = lq(ld(m.ne_oth + j), L, k);
+    double a[NTR], pfo[NTR], mfo[NTR];
+    ldn<NTR, IL>(in.ws.adfh, lq(e, L, k), w0, in.ws.sEd, in.wtg, a);
+    ldn<NTR, IL>(in.ws.pf, qo, w0, sN, in.wtg, pfo);
+    ldn<NTR, IL>(in.ws.mf, qo, w0, sN, in.wtg, mfo);
 #pragma unroll
-      for (int t = 0; t < NTR; ++t) {
-        const double pf1 = second ? pfo[t] : pf0[t], mf1 = second ? mfo[t] : mf0[t];
-        const double pf2 = second ? pf0[t] : pfo[t], mf2 = second ? mf0[t] : mfo[t];
-        const double ae = a[t] >= 0.0 ? fmin(pf1, mf2) : fmin(mf1, pf2);
-        const double lim = ae * a[t];
-        hsc[t] = on ? hsc[t] + (second ? -lim : lim) : hsc[t];
-      }
-    }
-  } else {
-    for (int j = e0; j < e1; ++j) {
-      const int idx = ld(m.ne_idx + j), e = idx >> 1;
-      if (k < ld(m.ekmin + e) || k >= ld(m.ekmax + e)) continue;   // no flux on this level
-      const uint32_t qo = lq(ld(m.ne_oth + j), L, k);
-      double a[NTR], pfo[NTR], mfo[NTR];
-      ldn<NTR, IL>(in.ws.adfh, lq(e, L, k), w0, in.ws.sEd, in.wtg, a);
-      ldn<NTR, IL>(in.ws.pf, qo, w0, sN, in.wtg, pfo);
-      ldn<NTR, IL>(in.ws.mf, qo, w0, sN, in.wtg, mfo);
-#pragma unroll
-      for (int t = 0; t < NTR; ++t) {
-        // (pf, mf) at the edge's first node n1 and second node n2
-        const double pf1 = (idx & 1) ? pfo[t] : pf0[t], mf1 = (idx & 1) ? mfo[t] : mf0[t];
-        const double pf2 = (idx & 1) ? pf0[t] : pfo[t], mf2 = (idx & 1) ? mf0[t] : mfo[t];
-        const double ae = a[t] >= 0.0 ? fmin(pf1, mf2) : fmin(mf1, pf2);
-        const double lim = ae * a[t];
-        hsc[t] += (idx & 1) ? -lim : lim;
-      }
+    for (int t = 0; t < NTR; ++t) {
+      // (pf, mf) at the edge's first node n1 and second node n2
+      const double pf1 = (idx & 1) ? pfo[t] : pf0[t], mf1 = (idx & 1) ? mfo[t] : mf0[t];
+      const double pf2 = (idx & 1) ? pf0[t] : pfo[t], mf2 = (idx & 1) ? mf0[t] : mfo[t];
+      const double ae = a[t] >= 0.0 ? fmin(pf1, mf2) : fmin(mf1, pf2);
+      const double lim = ae * a[t];
+      hsc[t] += (idx & 1) ? -lim : lim;
     }
   }
   double Tv[NTR], lo[NTR], out[NTR];
@@ -921,7 +590,7 @@ __device__ __forceinline__ void body_node_final(const Inst& in, int64_t i, int t
 // layers [nzmin, nzmax) (the reference's padded rows above and below solve to exactly 0,
 // so starting and ending the recursions there gives the same numbers). The elimination
 // factors m and cp do not depend on the tracer: one reciprocal of m serves c/m and every
-// tracer's dp/m. cp goes to workspace slot w0 of gnx, dp to the tracer's slots of lo
+// tracer's dp/m. cp goes to workspace slot w0 of adfv, dp to the tracer's slots of lo
 // (both free after the FCT stages); the back substitution reads them in reverse.
 template <int NTR, bool IL>
 __device__ __forceinline__ void body_vdiff(const Inst& in, int64_t n, int t0, int w0) {
@@ -973,7 +642,7 @@ __device__ __forceinline__ void body_vdiff(const Inst& in, int64_t n, int t0, in
     const double b = -a - c + ld(in.hnode_new + q);
     const Rcp rm = rcp(b - a * cprev);
     cprev = divr(c, rm);
-    in.ws.gnx[tix<IL>(q, w0, sN, in.wtg)] = cprev;
+    in.ws.adfv[tix<IL>(q, w0, sN, in.wtg)] = cprev;
     double swd = 0.0;
     if (in.sw_3d) {
       const double sw = ld(in.sw_3d + q), swp = last ? 0.0 : ld(in.sw_3d + q + 1);
@@ -995,7 +664,7 @@ __device__ __forceinline__ void body_vdiff(const Inst& in, int64_t n, int t0, in
   for (int t = 0; t < NTR; ++t) x[t] = 0.0;
   for (int k = nzmax - 1; k >= nzmin; --k) {
     const uint32_t q = base + uint32_t(k);
-    const double cp = in.ws.gnx[tix<IL>(q, w0, sN, in.wtg)];
+    const double cp = in.ws.adfv[tix<IL>(q, w0, sN, in.wtg)];
     double dp[NTR], Tv[NTR];
     ldn<NTR, IL>(in.ws.lo, q, w0, sN, in.wtg, dp);
     ldn<NTR, IL>(Tin, q, t0, ts, tg, Tv);
@@ -1051,58 +720,18 @@ constexpr int kMinBlocks = NTR == 1 ? 6 : NTR == 2 ? 4 : NTR == 4 ? 3 : 1;
     body<NTR, true>(tab[blockIdx.y], g >> lg, t0 + sub, w0 + sub);                      \
   }
 
-#define FCT_BODY_VARIANT(name, body, fused)                                             \
-  template <int NTR, bool IL>                                                           \
-  __device__ __forceinline__ void name(const Inst& in, int64_t i, int t0, int w0) {     \
-    body<NTR, IL, fused>(in, i, t0, w0);                                                \
-  }
-FCT_BODY_VARIANT(body_node_lo_u, body_node_lo, false)
-FCT_BODY_VARIANT(body_node_lo_f, body_node_lo, true)
-FCT_BODY_VARIANT(body_edge_adf_u, body_edge_adf, false)
-FCT_BODY_VARIANT(body_edge_adf_f, body_edge_adf, true)
-FCT_BODY_VARIANT(body_node_final_u, body_node_final, false)
-FCT_BODY_VARIANT(body_node_final_f, body_node_final, true)
 
 // unfused stages (every intermediate in the workspace; the reverse pass reads them)
 FCT_KERNEL_T(k_elem_grad, body_elem_grad)
-FCT_KERNEL_T(k_node_lo, body_node_lo_u)
+FCT_KERNEL_T(k_node_lo, body_node_lo)
 FCT_KERNEL_T(k_vert_impl, body_vert_impl)
-FCT_KERNEL_T(k_edge_adf, body_edge_adf_u)
+FCT_KERNEL_T(k_edge_adf, body_edge_adf)
 FCT_KERNEL_T(k_elem_bounds, body_elem_bounds)
 FCT_KERNEL_T(k_node_cluster, body_node_cluster)
 FCT_KERNEL_T(k_node_factors, body_node_factors)
-FCT_KERNEL_T(k_node_final, body_node_final_u)
-// fused stages
-FCT_KERNEL_T(k_node_lo_f, body_node_lo_f)
-FCT_KERNEL_T(k_edge_adf_f, body_edge_adf_f)
-FCT_KERNEL_T(k_node_final_f, body_node_final_f)
+FCT_KERNEL_T(k_node_final, body_node_final)
+// implicit vertical diffusion (the epilogue of the batched step and fct_vert_diff)
 FCT_KERNEL_T(k_vdiff, body_vdiff)
-
-// node_limit blocks hold 256 threads: `_1` one lane per thread (slice = blockIdx.y),
-// `_n` 256 >> lg lanes of 2^lg adjacent slice threads; the first and last lane of a
-// block are halo lanes.
-template <int NTR>
-__global__ void __launch_bounds__(256, kMinBlocks<NTR>) k_node_limit_1(Inst in, int t0,
-                                                                      int w0) {
-  __shared__ double smx[NTR * 256], smn[NTR * 256];
-  const int tid = threadIdx.x;
-  const int64_t lane = int64_t(blockIdx.x) * 254 + tid - 1;
-  const int sub = int(blockIdx.y) * NTR;
-  node_limit<NTR, false>(in, lane, tid >= 1 && tid <= 254, t0 + sub, w0 + sub, tid, 1, smx,
-                         smn);
-}
-template <int NTR>
-__global__ void __launch_bounds__(256, kMinBlocks<NTR>) k_node_limit_n(const Inst* __restrict__ tab,
-                                                                      int t0,
-                                                      int w0, int lg) {
-  __shared__ double smx[NTR * 256], smn[NTR * 256];
-  const int tid = threadIdx.x;
-  const int ll = tid >> lg, bl = 256 >> lg;
-  const int64_t lane = int64_t(blockIdx.x) * (bl - 2) + ll - 1;
-  const int sub = (tid & ((1 << lg) - 1)) * NTR;
-  node_limit<NTR, true>(tab[blockIdx.y], lane, ll >= 1 && ll <= bl - 2, t0 + sub, w0 + sub,
-                        tid, 1 << lg, smx, smn);
-}
 
 __global__ void __launch_bounds__(256) k_vflux_1(Inst in) { body_vflux(in, lane_index()); }
 __global__ void __launch_bounds__(256) k_vflux_n(const Inst* __restrict__ tab) {
@@ -1134,17 +763,6 @@ const char* const kStageNames[kNumStages] = {
       name##_1<P><<<dim3(xblocks(lanes), 1u << lg), B, 0, s>>>(single, t0, w0);          \
   } while (0)
 
-#define FCT_LIMIT_AS(name, lanes, P)                                                    \
-  do {                                                                                  \
-    if (tab)                                                                            \
-      k_node_limit_n<P><<<dim3(unsigned(std::max<int64_t>(                              \
-                               1, (int64_t(lanes) + (B >> lg) - 3) / ((B >> lg) - 2))), \
-                           unsigned(n)), B, 0, s>>>(tab, t0, w0, lg);                   \
-    else                                                                                \
-      k_node_limit_1<P><<<dim3(unsigned(std::max<int64_t>(1, (int64_t(lanes) + 253) / 254)), \
-                           1u << lg), B, 0, s>>>(single, t0, w0);                       \
-  } while (0)
-
 #define FCT_SPLIT(AS, name, lanes)                                                      \
   do {                                                                                  \
     for (int t0 = c0; t0 < c1;) {                                                       \
@@ -1162,7 +780,6 @@ const char* const kStageNames[kNumStages] = {
     }                                                                                   \
   } while (0)
 #define FCT_STAGE(name, lanes) FCT_SPLIT(FCT_STAGE_AS, name, lanes)
-#define FCT_LIMIT(lanes) FCT_SPLIT(FCT_LIMIT_AS, k_node_limit, lanes)
 
 int launch_forward_events(const Inst& single, const Inst* tab, int n, const LaunchDims& d,
                           cudaStream_t s, cudaEvent_t* after, bool stop_before_final,
@@ -1192,22 +809,25 @@ int launch_forward_events(const Inst& single, const Inst* tab, int n, const Laun
     }
     mark();
     if (d.fused) {
-      // 4 launches per chunk; the stages folded into others record empty intervals
-      // (elem_grad into node_lo and edge_adf, elem_bounds and node_cluster into the
-      // factors stage, k_node_limit)
+      // segment kernels (fct_seg_*.cu), 5 launches per chunk; the stages folded into
+      // others record empty intervals (elem_grad: the node gradients are evaluated only
+      // where MFCT needs them, in the edge stage; elem_bounds and node_cluster: the factors
+      // stage)
       mark();
-      FCT_STAGE(k_node_lo_f, d.max_iface);
+      int st = launch_seg_lo(single, tab, n, d, c0, c1, s);
+      if (st) return st;
       mark();
       if (d.any_wi) FCT_STAGE(k_vert_impl, d.max_nodes);
       mark();
-      FCT_STAGE(k_edge_adf_f, d.max_edge);
+      if ((st = launch_seg_edge(single, tab, n, d, c0, c1, s))) return st;
+      if ((st = launch_edge_fix(single, tab, n, d, c0, c1, s))) return st;
       mark();
       mark();
       mark();
-      FCT_LIMIT(d.max_layer);
+      if ((st = launch_seg_limit(single, tab, n, d, c0, c1, s))) return st;
       mark();
       if (stop_before_final) continue;
-      FCT_STAGE(k_node_final_f, d.max_layer);
+      if ((st = launch_seg_final(single, tab, n, d, c0, c1, s))) return st;
       if (d.any_vdiff) {   // epilogue: implicit vertical diffusion of this chunk, in place
         if (d.copy_dry) {  // the dry levels of T_new must hold T before it runs
           if (tab) k_copy_dry_n<<<grid(d.max_dense), B, 0, s>>>(tab);

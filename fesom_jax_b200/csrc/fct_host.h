@@ -1,6 +1,7 @@
 // Host-side helpers shared by the libfesom_fct translation units.
 #pragma once
 
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <string>
@@ -39,7 +40,41 @@ struct LaunchDims {
   bool any_derive_w = false;  // derive w_e from uv (compute_w) before the step
   bool fused = true;  // fused stages (lean workspace); false: every stage kernel writes its
                       // intermediates (what the reverse pass reads)
+  // fused (segment) stages: levels per thread (1, 2, 4 or 8: a tuning knob) and the
+  // largest segment counts over the launch's instances
+  int lpt = 4;
+  int64_t max_nseg[kSegVariants] = {0, 0, 0, 0};
+  int64_t max_eseg[kSegVariants] = {0, 0, 0, 0};
+  int64_t max_efix = 0;
 };
+
+// Grow ``d``'s lane and segment counts to cover a plan's mesh.
+inline void dims_cover(LaunchDims& d, const FctPlan* P) {
+  const DevMesh& m = P->hm;
+  d.max_iface = std::max(d.max_iface, m.n_iface);
+  d.max_layer = std::max(d.max_layer, m.n_layer);
+  d.max_edge = std::max(d.max_edge, m.n_edge);
+  d.max_elem = std::max(d.max_elem, m.n_elem);
+  d.max_dense = std::max(d.max_dense, int64_t(P->N) * P->L);
+  d.max_nodes = std::max(d.max_nodes, int64_t(P->N));
+  for (int v = 0; v < kSegVariants; ++v) {
+    d.max_nseg[v] = std::max(d.max_nseg[v], m.n_nseg[v]);
+    d.max_eseg[v] = std::max(d.max_eseg[v], m.n_eseg[v]);
+  }
+  d.max_efix = std::max(d.max_efix, m.n_efix);
+}
+
+// The fused stages over the tracers [c0, c1) of a workspace chunk (fct_seg_*.cu).
+int launch_seg_lo(const Inst& single, const Inst* tab, int n, const LaunchDims& d, int c0,
+                  int c1, cudaStream_t s);
+int launch_seg_edge(const Inst& single, const Inst* tab, int n, const LaunchDims& d, int c0,
+                    int c1, cudaStream_t s);
+int launch_edge_fix(const Inst& single, const Inst* tab, int n, const LaunchDims& d, int c0,
+                    int c1, cudaStream_t s);
+int launch_seg_limit(const Inst& single, const Inst* tab, int n, const LaunchDims& d, int c0,
+                     int c1, cudaStream_t s);
+int launch_seg_final(const Inst& single, const Inst* tab, int n, const LaunchDims& d, int c0,
+                     int c1, cudaStream_t s);
 int launch_forward(const Inst& single, const Inst* tab, int n, const LaunchDims& d,
                    cudaStream_t s);
 // Same, recording ``after[i]`` on ``s`` after stage i of a chunk (skipped stages record

@@ -224,8 +224,9 @@ extern "C" int fct_ice_solve(FctPlan* P, const FctIceFields* f, const FctIceConf
   if (!(cfg->dt > 0.0)) return set_error(FCT_ERR_INVALID, "dt must be positive");
   const int64_t N = P->N;
   // scratch: 6 fields of 3 x nod2D doubles, carved from the plan workspace's node fields
-  // (LO onwards: at least 6 x nod2D x nl doubles, contiguous in both workspace layouts)
-  if (18 * N > 6 * N * P->L * int64_t(P->max_tracers))
+  // (LO onwards: at least kFusedNodeFields x nod2D x nl doubles per tracer, contiguous in
+  // both workspace layouts)
+  if (18 * N > kFusedNodeFields * N * P->L * int64_t(P->max_tracers))
     return set_error(FCT_ERR_CAPACITY, "plan workspace too small for the ice step");
   int prev = -1;
   cudaGetDevice(&prev);

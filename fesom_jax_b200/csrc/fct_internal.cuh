@@ -49,6 +49,15 @@ __device__ __forceinline__ void split_dense(int64_t i, int L, int& ent, int& k) 
   k = int(u - q * uint32_t(L));
 }
 
+// Segment kernels: a thread takes a run of up to kSegLevels[v] consecutive levels of one
+// node or edge (variant v), so the entity's neighbour lists and static data are decoded
+// once per run instead of once per level.
+constexpr int kSegVariants = 4;
+constexpr int kSegLevels[kSegVariants] = {1, 2, 4, 8};
+__host__ __device__ constexpr int seg_variant(int lpt) {
+  return lpt == 1 ? 0 : lpt == 2 ? 1 : lpt == 4 ? 2 : 3;
+}
+
 // Static mesh on the device (pointers into one plan allocation).
 struct DevMesh {
   int N, E, Ed, L;
@@ -111,12 +120,31 @@ struct DevMesh {
   // per edge, its two cells and their layer ranges: {el1, el2 (-1 on a coast),
   // ranges packed as in the node->edge slots (pack_tri), 0}
   const int4* ecell4;
+  // segment kernels:
+  //   nrec per node {first edge slot, first cell slot,
+  //                  nzmin | nzmax << 8 | edge count << 16 | cell count << 24, 0}
+  //   erec per edge {n1, n2, lo | hi << 8, 0}: [lo, hi) the levels where MFCT takes the up
+  //     and down cells' gradients and the up cell holds n1, the down cell n2 (else empty)
+  //   nseg[v] node segments (node << 7 | first layer), runs of kSegLevels[v] layers
+  //   eseg[v] edge segments (edge << 7 | first level), runs within [lo, hi)
+  //   efix    the edge lanes outside [lo, hi) (node-average gradients, or a mesh whose
+  //     up/down cells do not hold the edge's nodes)
+  const int4* nrec;
+  const int4* erec;
+  const uint32_t* nseg[kSegVariants];
+  int64_t n_nseg[kSegVariants];
+  const uint32_t* eseg[kSegVariants];
+  int64_t n_eseg[kSegVariants];
+  const uint32_t* efix;
+  int64_t n_efix;
 };
 
 // Per-tracer intermediates of one instance (dense [entity, L]; tracer t at +t*stride).
 // Kernels read only entries written earlier in the same step (every reader masks by the
 // level range of the entity it reads), so a workspace needs no initial values and may be
 // shared by instances of different meshes that run one after another.
+// node fields per tracer of the fused workspace: LO, adf_v, the two limiter factors
+constexpr int kFusedNodeFields = 4;
 struct Workspace {
   double* vflux;                 // [Ed,L] shared by all tracers of the instance
   double *gx, *gy;               // [E,L] element gradients
@@ -204,6 +232,8 @@ struct FctPlan {
   void* d_static = nullptr;        // one allocation for all static arrays
   int max_tracers = 0;
   bool fused = true;               // fct_forward runs the fused stage kernels
+  int per_thread = 2;              // fused stages: most tracers per thread
+  int lpt = 4;                     //   and levels per thread
   bool ws_full = false;            // workspace holds every stage field (unfused / adjoint)
   double* d_ws = nullptr;          // workspace allocation
   fct::Workspace ws{};

@@ -89,15 +89,11 @@ extern "C" int fct_forward_noalloc(FctPlan* P, const FctFields* f, double dt, in
   in.ntr = ntr;
   in.nonfinite = P->d_health;   // allocated with the plan
   LaunchDims dims{};
-  dims.max_iface = P->hm.n_iface;
-  dims.max_layer = P->hm.n_layer;
-  dims.max_edge = P->hm.n_edge;
-  dims.max_elem = P->hm.n_elem;
-  dims.max_dense = int64_t(P->N) * P->L;
-  dims.max_nodes = P->N;
+  dims_cover(dims, P);
   dims.ntr = ntr;
   dims.chunk = 0;
-  dims.per_thread = 8;
+  dims.per_thread = P->per_thread;
+  dims.lpt = P->lpt;
   dims.any_wi = f->w_i != nullptr;
   dims.copy_dry = true;
   return restore(launch_forward(in, nullptr, 1, dims, static_cast<cudaStream_t>(stream)));

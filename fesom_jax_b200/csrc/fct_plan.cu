@@ -84,7 +84,7 @@ int64_t workspace_doubles(int64_t N, int64_t E, int64_t Ed, int64_t L, int ntr) 
 }
 
 int64_t workspace_doubles_fused(int64_t N, int64_t Ed, int64_t L, int ntr) {
-  return Ed * L + int64_t(ntr) * (6 * N * L + Ed * L);
+  return Ed * L + int64_t(ntr) * (kFusedNodeFields * N * L + Ed * L);
 }
 
 Workspace carve_workspace(double* base, int64_t N, int64_t E, int64_t Ed, int64_t L, int ntr,
@@ -96,10 +96,8 @@ Workspace carve_workspace(double* base, int64_t N, int64_t E, int64_t Ed, int64_
   double* p = base;
   auto take = [&](int64_t n) { double* q = p; p += n; return q; };
   w.vflux = take(Ed * L);
-  if (fused) {   // the fused stages keep no element fields and no cluster bounds
+  if (fused) {   // the fused stages keep no element fields, node gradients or cluster bounds
     w.lo = take(ntr * w.sN);
-    w.gnx = take(ntr * w.sN);
-    w.gny = take(ntr * w.sN);
     w.adfv = take(ntr * w.sN);
     w.pf = take(ntr * w.sN);
     w.mf = take(ntr * w.sN);
@@ -396,6 +394,46 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
     const int e = int(edgel[i] >> kLevelBits);
     edge4[i] = make_int4(int(edgel[i]), d->edges[2 * e], d->edges[2 * e + 1], etr[e]);
   }
+  // segment kernels (fct_segments.cu): node records, runs of up to kSegLevels[i]
+  // consecutive layers of a node, runs of consecutive MFCT up/down-cell levels of an edge
+  // (those whose up cell holds the edge's first node and whose down cell its second), and
+  // the remaining edge lanes
+  std::vector<int4> nrec(static_cast<size_t>(N));
+  for (int n = 0; n < N; ++n) {
+    const int ed = ne_off[n + 1] - ne_off[n];
+    const int cd = d->nod_in_elem2D_offsets[n + 1] - d->nod_in_elem2D_offsets[n];
+    nrec[n] = make_int4(ne_off[n], d->nod_in_elem2D_offsets[n],
+                        int(unsigned(nzmin[n]) | (unsigned(nzmax[n]) << 8) |
+                            (unsigned(ed) << 16) | (unsigned(cd) << 24)), 0);
+  }
+  std::vector<int4> erec(static_cast<size_t>(Ed));
+  std::vector<uint32_t> efix;
+  std::vector<int> tlo(Ed, 0), thi(Ed, 0);
+  for (int e = 0; e < Ed; ++e) {
+    const int n1 = d->edges[2 * e], n2 = d->edges[2 * e + 1];
+    const int up = d->edge_up_dn_tri[2 * e], dn = d->edge_up_dn_tri[2 * e + 1];
+    auto holds = [&](int el, int n) {
+      const int* en = d->elem_nodes + 3 * size_t(el);
+      return en[0] == n || en[1] == n || en[2] == n;
+    };
+    if (etr[e] && holds(up, n1) && holds(dn, n2)) {
+      tlo[e] = etr[e] & 255;
+      thi[e] = (etr[e] >> 8) & 255;
+    }
+    erec[e] = make_int4(n1, n2, tlo[e] | (thi[e] << 8), 0);
+    for (int k = ekmin[e]; k < ekmax[e]; ++k)
+      if (k < tlo[e] || k >= thi[e]) efix.push_back((uint32_t(e) << kLevelBits) | uint32_t(k));
+  }
+  std::vector<uint32_t> nseg[kSegVariants], eseg[kSegVariants];
+  for (int v = 0; v < kSegVariants; ++v) {
+    const int lpt = kSegLevels[v];
+    for (int n = 0; n < N; ++n)
+      for (int k = std::max(nzmin[n], 0); k < std::min(nzmax[n], L); k += lpt)
+        nseg[v].push_back((uint32_t(n) << kLevelBits) | uint32_t(k));
+    for (int e = 0; e < Ed; ++e)
+      for (int k = tlo[e]; k < thi[e]; k += lpt)
+        eseg[v].push_back((uint32_t(e) << kLevelBits) | uint32_t(k));
+  }
 
   Blob b;
   const int nie = d->nod_in_elem2D_offsets[N];
@@ -427,6 +465,13 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   size_t o_ed4 = b.add(edge4.data(), edge4.size());
   size_t o_eud4 = b.add(eud4.data(), eud4.size());
   size_t o_ecell4 = b.add(ecell4.data(), ecell4.size());
+  size_t o_nrec = b.add(nrec.data(), nrec.size()), o_erec = b.add(erec.data(), erec.size());
+  size_t o_efix = b.add(efix.data(), std::max<size_t>(efix.size(), 1));
+  size_t o_nseg[kSegVariants], o_eseg[kSegVariants];
+  for (int v = 0; v < kSegVariants; ++v) {
+    o_nseg[v] = b.add(nseg[v].data(), std::max<size_t>(nseg[v].size(), 1));
+    o_eseg[v] = b.add(eseg[v].data(), std::max<size_t>(eseg[v].size(), 1));
+  }
 
   FCT_CUDA(cudaSetDevice(device));
   FCT_CUDA(cudaMalloc(&P->d_static, b.bytes.size()));
@@ -475,6 +520,16 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   m.edge4 = (const int4*)(base + o_ed4);
   m.eud4 = (const int4*)(base + o_eud4);
   m.ecell4 = (const int4*)(base + o_ecell4);
+  m.nrec = (const int4*)(base + o_nrec);
+  m.erec = (const int4*)(base + o_erec);
+  m.efix = (const uint32_t*)(base + o_efix);
+  m.n_efix = int64_t(efix.size());
+  for (int v = 0; v < kSegVariants; ++v) {
+    m.nseg[v] = (const uint32_t*)(base + o_nseg[v]);
+    m.n_nseg[v] = int64_t(nseg[v].size());
+    m.eseg[v] = (const uint32_t*)(base + o_eseg[v]);
+    m.n_eseg[v] = int64_t(eseg[v].size());
+  }
   FCT_CUDA(cudaMalloc(&P->d_mesh, sizeof(DevMesh)));
   FCT_CUDA(cudaMemcpy(P->d_mesh, &m, sizeof(DevMesh), cudaMemcpyHostToDevice));
   FCT_CUDA(cudaMalloc(&P->d_health, sizeof(unsigned long long)));
@@ -540,6 +595,16 @@ int fct_plan_info(const FctPlan* P, int64_t out[8]) {
   out[0] = P->N; out[1] = P->E; out[2] = P->Ed; out[3] = P->L;
   out[4] = P->hm.n_layer; out[5] = P->n_wet_elem_layers; out[6] = P->hm.n_edge;
   out[7] = P->max_tracers;
+  return FCT_OK;
+}
+
+int fct_plan_set_mapping(FctPlan* P, int tracers_per_thread, int levels_per_thread) {
+  if (!P) return set_error(FCT_ERR_INVALID, "NULL plan");
+  const int t = tracers_per_thread, l = levels_per_thread;
+  if ((t != 1 && t != 2 && t != 4 && t != 8) || (l != 1 && l != 2 && l != 4 && l != 8))
+    return set_error(FCT_ERR_INVALID, "tracers and levels per thread must be 1, 2, 4 or 8");
+  P->per_thread = t;
+  P->lpt = l;
   return FCT_OK;
 }
 
@@ -625,15 +690,11 @@ int fct_forward(FctPlan* P, const FctFields* f, double dt, int ntr, fct_stream_t
   in.ntr = ntr;
   in.nonfinite = P->d_health;
   LaunchDims dims{};
-  dims.max_iface = P->hm.n_iface;
-  dims.max_layer = P->hm.n_layer;
-  dims.max_edge = P->hm.n_edge;
-  dims.max_elem = P->hm.n_elem;
-  dims.max_dense = int64_t(P->N) * P->L;
-  dims.max_nodes = P->N;
+  dims_cover(dims, P);
   dims.ntr = ntr;
   dims.chunk = 0;       // one workspace chunk: all ntr tracers
-  dims.per_thread = 8;
+  dims.per_thread = P->per_thread;
+  dims.lpt = P->lpt;
   dims.any_wi = f->w_i != nullptr;
   dims.copy_dry = true;   // a fresh T_new: dry levels keep T (tracer_adv.py:147-151)
   dims.fused = P->fused;

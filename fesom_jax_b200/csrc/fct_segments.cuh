@@ -1,0 +1,636 @@
+// Segment kernels of the fused forward step: the product path of fct_forward, the
+// batched engine and the serving engine (fesom_jax/tracer_adv.py:532-578).
+//
+// A thread takes a *segment*: a run of up to LPT consecutive levels of one node (or one
+// edge) and NTR tracers. The entity's neighbour slots, level range and static geometry
+// are decoded once per segment and every neighbour gather issues LPT x NTR independent
+// loads (consecutive levels of one column), instead of one level per thread re-decoding
+// the same lists. The arithmetic of every quantity is the reference's, in the reference's
+// order (the same expressions as the one-kernel-per-stage path), so the results are the
+// same bits as that path's.
+//
+// Stages (kernels over the plan's segment lists, fct_internal.cuh DevMesh):
+//   seg_node_lo     node layers: LO (compute_fct_lo with adv_flux_hor/ver, :96-120,
+//                   :298-313) and adf_v (adv_flux_ver_ho minus the LO vertical flux,
+//                   :241-295, :568) on the tops of the layers; the bottom interface's
+//                   adf_v is 0 and not stored (readers take 0 there)
+//   seg_edge_adf    edge levels where MFCT takes the up/down cells' gradients
+//                   (fill_up_dn_grad :344-368, adv_flux_hor_ho :196-225): adf_h
+//   edge_fix        the other edge lanes: the node-average gradients (:329-341) of the
+//                   two end nodes computed on the fly; at 1-2 % of the edge lanes of an
+//                   open-ocean mesh this is cheaper than storing node gradients everywhere
+//   seg_node_limit  zalesak_limit a1-a4, b1, b2 (:371-451): cluster bounds over the edge
+//                   neighbours, the k-1/k/k+1 window (the run's bounds plus one level above
+//                   and below), the antidiffusive sums and the limiter factors
+//   seg_node_final  b3, flux2dtracer_fct, ale_reconstruct (:453-484, :142-151): T_new
+#pragma once
+
+#include <algorithm>
+
+#include "fct_device.cuh"
+
+namespace fct {
+namespace {
+
+// a level clamped into [0, L - 1]: loads at clamped levels are in bounds and their values
+// are discarded by the predicates that follow
+__device__ __forceinline__ int kclamp(int k, int L) { return k < 0 ? 0 : (k >= L ? L - 1 : k); }
+
+// ----------------------------------------------------------- LO and adf_v, node runs
+template <int NTR, int LPT, bool IL>
+__device__ __forceinline__ void seg_node_lo(const Inst& in, int64_t si, int t0, int w0) {
+  const DevMesh& m = *in.m;
+  constexpr int V = seg_variant(LPT);
+  if (si >= m.n_nseg[V]) return;
+  const uint32_t sg = __ldg(m.nseg[V] + si);
+  const int n = lane_ent(sg), k0 = lane_lev(sg), L = m.L;
+  const int4 rec = __ldg(m.nrec + n);
+  const unsigned pk = unsigned(rec.z);
+  const int nzmin = int(pk & 255u), nzmax = int((pk >> 8) & 255u);
+  const int nk = min(LPT, nzmax - k0);   // layers of this run
+  const uint32_t base = lq(n, L, 0);
+  const int64_t ts = in.tstride;
+  const int tg = in.tg;
+  const double dt = in.dt;
+  // T of the column at levels k0-2 .. k0+LPT (Tw[i] <-> level k0-2+i; the level above
+  // the surface reads T[0], the reference's edge-replicated top)
+  double Tw[LPT + 3][NTR];
+#pragma unroll
+  for (int i = 0; i < LPT + 3; ++i)
+    ldn<NTR, IL>(in.T, base + uint32_t(kclamp(k0 - 2 + i, L)), t0, ts, tg, Tw[i]);
+
+  // compute_fct_lo: edge->node upwind divergence in ascending edge id
+  double div[LPT][NTR];
+#pragma unroll
+  for (int l = 0; l < LPT; ++l)
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) div[l][t] = 0.0;
+  const int e0 = rec.x, e1 = rec.x + int((pk >> 16) & 255u);
+  for (int j = e0; j < e1; ++j) {
+    const int4 sl = __ldg(m.ne4 + j);
+    const unsigned rg = unsigned(sl.z);
+    const bool second = sl.x & 1;
+    const uint32_t qe = lq(sl.x >> 1, L, 0), qo = lq(sl.y, L, 0);
+#pragma unroll
+    for (int l = 0; l < LPT; ++l) {
+      const int k = k0 + l, kc = kclamp(k, L);
+      const bool on = l < nk && in_range(k, rg);
+      const double vf = __ldg(in.ws.vflux + qe + kc);
+      const double avf = fabs(vf);
+      double To[NTR];
+      ldn<NTR, IL>(in.T, qo + uint32_t(kc), t0, ts, tg, To);
+#pragma unroll
+      for (int t = 0; t < NTR; ++t) {
+        const double Tc = Tw[l + 2][t];
+        const double T1 = second ? To[t] : Tc, T2 = second ? Tc : To[t];
+        const double fl = -0.5 * (T1 * (vf + avf) + T2 * (vf - avf));
+        div[l][t] = on ? div[l][t] + (second ? -fl : fl) : div[l][t];
+      }
+    }
+  }
+
+  // upwind vertical flux at the interfaces k0 .. k0+LPT (layer-masked, tracer_adv.py:108-120)
+  double fv[LPT + 1][NTR];
+#pragma unroll
+  for (int i = 0; i <= LPT; ++i) {
+    const int k = k0 + i, kc = kclamp(k, L);
+    const bool layer = i <= nk && k < nzmax;
+    const double w = __ldg(in.w_e + base + kc), ar = __ldg(m.area + base + kc);
+#pragma unroll
+    for (int t = 0; t < NTR; ++t)
+      fv[i][t] = layer ? vflux_up(Tw[i + 2][t], Tw[i + 1][t], w, ar) : 0.0;
+  }
+  // LO on the run's layers
+#pragma unroll
+  for (int l = 0; l < LPT; ++l) {
+    if (l >= nk) break;
+    const uint32_t qn = base + uint32_t(k0 + l);
+    const double hn = __ldg(in.hnode + qn), hnn = __ldg(in.hnode_new + qn);
+    const double av = __ldg(m.areasvol + qn);
+    const Rcp rav = rcp(av), rhn = rcp(hnn);
+    const bool valid = (hnn > 0.0) && (av > 0.0);
+    double lo[NTR];
+#pragma unroll
+    for (int t = 0; t < NTR; ++t)
+      lo[t] = valid ? divr(Tw[l + 2][t] * hn +
+                               divr((div[l][t] + (fv[l][t] - fv[l + 1][t])) * dt, rav), rhn)
+                    : 0.0;
+    stn<NTR, IL>(in.ws.lo, qn, w0, in.ws.sN, in.wtg, lo);
+  }
+
+  // adv_flux_ver_ho (QR4C on ttfAB) minus the LO vertical flux at the layer tops
+  double To[LPT + 3][NTR];   // T_old at levels k0-2 .. k0+LPT
+#pragma unroll
+  for (int i = 0; i < LPT + 3; ++i)
+    ldn<NTR, IL>(in.T_old, base + uint32_t(kclamp(k0 - 2 + i, L)), t0, ts, tg, To[i]);
+#pragma unroll
+  for (int l = 0; l < LPT; ++l) {
+    if (l >= nk) break;
+    const int k = k0 + l;
+    const uint32_t qn = base + uint32_t(k);
+    const double w = __ldg(in.w_e + qn);
+    const double Wf = in.w_i ? w + __ldg(in.w_i + qn) : w;
+    const double area_k = __ldg(m.area + qn);
+    double hi[NTR];
+    if (k == nzmin) {
+#pragma unroll
+      for (int t = 0; t < NTR; ++t) hi[t] = -ab2(Tw[l + 2][t], To[l + 2][t]) * Wf * area_k;
+    } else if (k == nzmin + 1 || k == nzmax - 1) {
+#pragma unroll
+      for (int t = 0; t < NTR; ++t)
+        hi[t] = -0.5 * (ab2(Tw[l + 1][t], To[l + 1][t]) + ab2(Tw[l + 2][t], To[l + 2][t])) *
+                Wf * area_k;
+    } else {   // nzmin + 2 <= k <= nzmax - 2
+      double Znz, Zm1, Zm2, Zp1, zb;   // QR4C stencil depths (tracer_adv.py:228-238, 265-273)
+      if (in.Z3d) {
+        const double* Zc = in.Z3d + base;
+        Znz = __ldg(Zc + k); Zm1 = __ldg(Zc + k - 1); Zm2 = __ldg(Zc + k - 2);
+        Zp1 = __ldg(Zc + (k + 1 < L ? k + 1 : L - 1)); zb = __ldg(in.zbar3 + qn);
+      } else {
+        Znz = __ldg(m.Zp + k); Zm1 = __ldg(m.Zp + k - 1); Zm2 = __ldg(m.Zp + k - 2);
+        Zp1 = __ldg(m.Zp + (k + 1 < L ? k + 1 : L - 1)); zb = __ldg(m.zbar + k);
+      }
+      const Rcp rdc = rcp(safe_nz(Zm1 - Znz)), rdu = rcp(safe_nz(Znz - Zp1)),
+                rdd = rcp(safe_nz(Zm2 - Zm1));
+      const Rcp r3{3.0, 1.0 / 3.0, true};
+#pragma unroll
+      for (int t = 0; t < NTR; ++t) {
+        const double A0 = ab2(Tw[l + 2][t], To[l + 2][t]);
+        const double Am1 = ab2(Tw[l + 1][t], To[l + 1][t]);
+        const double Am2 = ab2(Tw[l][t], To[l][t]);
+        const double Ap1 = ab2(Tw[l + 3][t], To[l + 3][t]);
+        const double qc = divr(Am1 - A0, rdc);
+        const double qu = divr(A0 - Ap1, rdu);
+        const double qd = divr(Am2 - Am1, rdd);
+        const double Tmean1 = A0 + divr((2.0 * qc + qu) * (zb - Znz), r3);
+        const double Tmean2 = Am1 + divr((2.0 * qc + qd) * (zb - Zm1), r3);
+        hi[t] = -0.5 * (Tmean1 + Tmean2) * Wf * area_k;
+      }
+    }
+    double adf[NTR];
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) {
+      const double lo_v = in.w_i ? vflux_up(Tw[l + 2][t], Tw[l + 1][t], Wf, area_k) : fv[l][t];
+      adf[t] = hi[t] - lo_v;
+    }
+    stn<NTR, IL>(in.ws.adfv, qn, w0, in.ws.sN, in.wtg, adf);
+  }
+}
+
+// ---------------------------------------------- adf_h on a run of up/down-cell levels
+template <int NTR, int LPT, bool IL>
+__device__ __forceinline__ void seg_edge_adf(const Inst& in, int64_t si, int t0, int w0) {
+  const DevMesh& m = *in.m;
+  constexpr int V = seg_variant(LPT);
+  if (si >= m.n_eseg[V]) return;
+  const uint32_t sg = __ldg(m.eseg[V] + si);
+  const int e = lane_ent(sg), k0 = lane_lev(sg), L = m.L;
+  const int4 er = __ldg(m.erec + e);
+  const int nk = min(LPT, int((unsigned(er.z) >> 8) & 255u) - k0);
+  const int4 cu = __ldg(m.eud4 + 2 * e), cd = __ldg(m.eud4 + 2 * e + 1);
+  const double2 ec = __ldg(reinterpret_cast<const double2*>(m.ecoef) + e);
+  const double c1 = ec.x, c2 = ec.y;
+  const double2* gu = reinterpret_cast<const double2*>(m.gsca + 6 * int64_t(cu.x));
+  const double2* gd = reinterpret_cast<const double2*>(m.gsca + 6 * int64_t(cd.x));
+  const double2 up0 = __ldg(gu), up1 = __ldg(gu + 1), up2 = __ldg(gu + 2);
+  const double2 dn0 = __ldg(gd), dn1 = __ldg(gd + 1), dn2 = __ldg(gd + 2);
+  const uint32_t q1 = lq(er.x, L, 0), q2 = lq(er.y, L, 0), qe = lq(e, L, 0);
+  const uint32_t qu0 = lq(cu.y, L, 0), qu1 = lq(cu.z, L, 0), qu2 = lq(cu.w, L, 0);
+  const uint32_t qd0 = lq(cd.y, L, 0), qd1 = lq(cd.z, L, 0), qd2 = lq(cd.w, L, 0);
+  const int64_t ts = in.tstride;
+  const int tg = in.tg;
+  const Rcp r6{6.0, 1.0 / 6.0, true};
+#pragma unroll
+  for (int l = 0; l < LPT; ++l) {
+    const int kc = kclamp(k0 + l, L);
+    const double vf = __ldg(in.ws.vflux + qe + kc);
+    const double avf = fabs(vf);
+    double T1[NTR], T2[NTR], O1[NTR], O2[NTR];
+    ldn<NTR, IL>(in.T, q1 + kc, t0, ts, tg, T1);
+    ldn<NTR, IL>(in.T, q2 + kc, t0, ts, tg, T2);
+    ldn<NTR, IL>(in.T_old, q1 + kc, t0, ts, tg, O1);
+    ldn<NTR, IL>(in.T_old, q2 + kc, t0, ts, tg, O2);
+    double a0[NTR], a1[NTR], a2[NTR], b0[NTR], b1[NTR], b2[NTR];
+    ldn<NTR, IL>(in.T, qu0 + kc, t0, ts, tg, a0);
+    ldn<NTR, IL>(in.T, qu1 + kc, t0, ts, tg, a1);
+    ldn<NTR, IL>(in.T, qu2 + kc, t0, ts, tg, a2);
+    ldn<NTR, IL>(in.T, qd0 + kc, t0, ts, tg, b0);
+    ldn<NTR, IL>(in.T, qd1 + kc, t0, ts, tg, b1);
+    ldn<NTR, IL>(in.T, qd2 + kc, t0, ts, tg, b2);
+    double adf[NTR];
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) {
+      // the up and down cells' gradients, as tracer_gradient_elements evaluates them
+      const double g0 = up0.x * a0[t] + up0.y * a1[t] + up1.x * a2[t];
+      const double g2 = up1.y * a0[t] + up2.x * a1[t] + up2.y * a2[t];
+      const double g1 = dn0.x * b0[t] + dn0.y * b1[t] + dn1.x * b2[t];
+      const double g3 = dn1.y * b0[t] + dn2.x * b1[t] + dn2.y * b2[t];
+      const double fl = -0.5 * (T1[t] * (vf + avf) + T2[t] * (vf - avf));
+      const double A1 = ab2(T1[t], O1[t]), A2 = ab2(T2[t], O2[t]);
+      const double diff = A2 - A1;
+      const double Tm1 = A1 + divr(2.0 * diff + c1 * g0 + c2 * g2, r6);
+      const double Tm2 = A2 - divr(2.0 * diff + c1 * g1 + c2 * g3, r6);
+      const double ho = -0.5 * ((vf + avf) * Tm1 + (vf - avf) * Tm2);
+      adf[t] = ho - fl;
+    }
+    if (l < nk) stn<NTR, IL>(in.ws.adfh, qe + uint32_t(kc), w0, in.ws.sEd, in.wtg, adf);
+  }
+}
+
+// node-average gradient of T at node n, level k (_node_avg_grad, tracer_adv.py:329-341):
+// the area-weighted mean over n's cells wet at k, in the node's cell order
+template <int NTR, bool IL>
+__device__ __forceinline__ void node_avg_grad(const Inst& in, int n, int k, int t0,
+                                              double (&nx)[NTR], double (&ny)[NTR]) {
+  const DevMesh& m = *in.m;
+  const int4 rec = __ldg(m.nrec + n);
+  double den = 0.0;
+#pragma unroll
+  for (int t = 0; t < NTR; ++t) nx[t] = ny[t] = 0.0;
+  const int c0 = rec.y, c1 = rec.y + int(unsigned(rec.z) >> 24);
+  for (int j = c0; j < c1; ++j) {
+    const unsigned r = unsigned(__ldg(m.nelr + j));
+    const int4 sl = __ldg(m.nel4 + j);
+    if (!in_range(k, r)) continue;
+    const double a = __ldg(m.earea + sl.x);
+    double gx[NTR], gy[NTR];
+    cell_grad<NTR, IL>(in, sl.x, sl.y, sl.z, sl.w, k, t0, gx, gy);
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) {
+      nx[t] += gx[t] * a;
+      ny[t] += gy[t] * a;
+    }
+    den += a;
+  }
+  const Rcp rdd = rcp(den > 0.0 ? den : 1.0);
+#pragma unroll
+  for (int t = 0; t < NTR; ++t) {
+    nx[t] = divr(nx[t], rdd);
+    ny[t] = divr(ny[t], rdd);
+  }
+}
+
+// ----------------------------------------------- adf_h on the remaining edge lanes
+template <int NTR, bool IL>
+__device__ __forceinline__ void body_edge_fix(const Inst& in, int64_t i, int t0, int w0) {
+  const DevMesh& m = *in.m;
+  if (i >= m.n_efix) return;
+  const uint32_t lane = __ldg(m.efix + i);
+  const int e = lane_ent(lane), k = lane_lev(lane), L = m.L;
+  const int4 er = __ldg(m.erec + e);
+  const int n1 = er.x, n2 = er.y;
+  const bool use_tri = in_range(k, unsigned(__ldg(m.etr + e)));
+  const double vf = __ldg(in.ws.vflux + lq(e, L, k));
+  const double avf = fabs(vf);
+  const double c1 = __ldg(m.ecoef + 2 * e), c2 = __ldg(m.ecoef + 2 * e + 1);
+  const uint32_t q1 = lq(n1, L, k), q2 = lq(n2, L, k);
+  const int64_t ts = in.tstride;
+  const int tg = in.tg;
+  double T1[NTR], T2[NTR], O1[NTR], O2[NTR], g0[NTR], g1[NTR], g2[NTR], g3[NTR];
+  ldn<NTR, IL>(in.T, q1, t0, ts, tg, T1);
+  ldn<NTR, IL>(in.T, q2, t0, ts, tg, T2);
+  ldn<NTR, IL>(in.T_old, q1, t0, ts, tg, O1);
+  ldn<NTR, IL>(in.T_old, q2, t0, ts, tg, O2);
+  if (use_tri) {   // a mesh whose up/down cells do not hold the edge's nodes
+    const int4 cu = __ldg(m.eud4 + 2 * e), cd = __ldg(m.eud4 + 2 * e + 1);
+    cell_grad<NTR, IL>(in, cu.x, cu.y, cu.z, cu.w, k, t0, g0, g2);
+    cell_grad<NTR, IL>(in, cd.x, cd.y, cd.z, cd.w, k, t0, g1, g3);
+  } else {
+    node_avg_grad<NTR, IL>(in, n1, k, t0, g0, g2);
+    node_avg_grad<NTR, IL>(in, n2, k, t0, g1, g3);
+  }
+  double adf[NTR];
+  const Rcp r6{6.0, 1.0 / 6.0, true};
+#pragma unroll
+  for (int t = 0; t < NTR; ++t) {
+    const double fl = -0.5 * (T1[t] * (vf + avf) + T2[t] * (vf - avf));
+    const double A1 = ab2(T1[t], O1[t]), A2 = ab2(T2[t], O2[t]);
+    const double diff = A2 - A1;
+    const double Tm1 = A1 + divr(2.0 * diff + c1 * g0[t] + c2 * g2[t], r6);
+    const double Tm2 = A2 - divr(2.0 * diff + c1 * g1[t] + c2 * g3[t], r6);
+    const double ho = -0.5 * ((vf + avf) * Tm1 + (vf - avf) * Tm2);
+    adf[t] = ho - fl;
+  }
+  stn<NTR, IL>(in.ws.adfh, lq(e, L, k), w0, in.ws.sEd, in.wtg, adf);
+}
+
+// ---------------------------------------- limiter factors on a node's layer run
+// The cluster bound of node n at level k is the max (min) of max(LO, T) (min(LO, T)) over
+// the nodes of n's cells that are wet at k, padded with -BIG (+BIG) when one of n's cells
+// is dry at k (tracer_adv.py:389-405). Every cell of n has two edges at n, so those nodes
+// are n itself (when any cell is wet at k) and the edge neighbours with a wet cell at k;
+// max/min are exact, so this equals the per-cell evaluation bit for bit. The a4 window
+// needs the bounds one level above and below the run: the run evaluates them too.
+template <int NTR, int LPT, bool IL>
+__device__ __forceinline__ void seg_node_limit(const Inst& in, int64_t si, int t0, int w0) {
+  const DevMesh& m = *in.m;
+  constexpr int V = seg_variant(LPT);
+  constexpr int NB = LPT + 2;   // bound levels k0-1 .. k0+LPT
+  if (si >= m.n_nseg[V]) return;
+  const uint32_t sg = __ldg(m.nseg[V] + si);
+  const int n = lane_ent(sg), k0 = lane_lev(sg), L = m.L;
+  const int4 rec = __ldg(m.nrec + n);
+  const unsigned pk = unsigned(rec.z);
+  const int nzmin = int(pk & 255u), nzmax = int((pk >> 8) & 255u);
+  const int nk = min(LPT, nzmax - k0);
+  const uint32_t base = lq(n, L, 0);
+  const int64_t sN = in.ws.sN;
+  double mx[NB][NTR], mn[NB][NTR], sp[LPT][NTR], sm[LPT][NTR];
+#pragma unroll
+  for (int b = 0; b < NB; ++b)
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) { mx[b][t] = -INFINITY; mn[b][t] = INFINITY; }
+#pragma unroll
+  for (int l = 0; l < LPT; ++l)
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) sp[l][t] = sm[l][t] = 0.0;
+  unsigned own = 0u, off = 0u;   // bit b: a cell of n is wet / dry at level k0-1+b
+  const int e0 = rec.x, e1 = rec.x + int((pk >> 16) & 255u);
+  for (int j = e0; j < e1; ++j) {
+    const int4 sl = __ldg(m.ne4 + j);
+    const unsigned tr = unsigned(sl.w), rg = unsigned(sl.z);
+    const bool has2 = ((tr >> 16) & 255u) != kNoCell;
+    const bool second = sl.x & 1;
+    const uint32_t qo = lq(sl.y, L, 0), qe = lq(sl.x >> 1, L, 0);
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+      const int k = k0 - 1 + b, kc = kclamp(k, L);
+      const bool c1 = in_range(k, tr & 0xffffu);
+      const bool c2 = has2 && in_range(k, tr >> 16);
+      const bool wet = c1 || c2;
+      own |= unsigned(wet) << b;
+      off |= unsigned(!c1 || (has2 && !c2)) << b;
+      double lv[NTR], tv[NTR];
+      ldn<NTR, IL>(in.ws.lo, qo + uint32_t(kc), w0, sN, in.wtg, lv);
+      ldn<NTR, IL>(in.T, qo + uint32_t(kc), t0, in.tstride, in.tg, tv);
+#pragma unroll
+      for (int t = 0; t < NTR; ++t) {
+        mx[b][t] = wet ? fmax(mx[b][t], fmax(lv[t], tv[t])) : mx[b][t];
+        mn[b][t] = wet ? fmin(mn[b][t], fmin(lv[t], tv[t])) : mn[b][t];
+      }
+      if (b >= 1 && b <= LPT) {   // the run's own levels: antidiffusive sums (b1)
+        const int l = b - 1;
+        const bool on = l < nk && in_range(k, rg);
+        double a[NTR];
+        ldn<NTR, IL>(in.ws.adfh, qe + uint32_t(kc), w0, in.ws.sEd, in.wtg, a);
+#pragma unroll
+        for (int t = 0; t < NTR; ++t) {
+          const double sv = second ? -a[t] : a[t];
+          sp[l][t] = on ? sp[l][t] + fmax(sv, 0.0) : sp[l][t];
+          sm[l][t] = on ? sm[l][t] + fmin(sv, 0.0) : sm[l][t];
+        }
+      }
+    }
+  }
+  // the node itself, and the padding of dry cells
+  double lo[NB][NTR];
+#pragma unroll
+  for (int b = 0; b < NB; ++b) {
+    const int kc = kclamp(k0 - 1 + b, L);
+    double tv[NTR];
+    ldn<NTR, IL>(in.ws.lo, base + uint32_t(kc), w0, sN, in.wtg, lo[b]);
+    ldn<NTR, IL>(in.T, base + uint32_t(kc), t0, in.tstride, in.tg, tv);
+    const bool ow = (own >> b) & 1u, of = (off >> b) & 1u;
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) {
+      if (ow) {
+        mx[b][t] = fmax(mx[b][t], fmax(lo[b][t], tv[t]));
+        mn[b][t] = fmin(mn[b][t], fmin(lo[b][t], tv[t]));
+      }
+      if (of) {
+        mx[b][t] = fmax(mx[b][t], -kBig);
+        mn[b][t] = fmin(mn[b][t], kBig);
+      }
+    }
+  }
+  const double dt = in.dt;
+#pragma unroll
+  for (int l = 0; l < LPT; ++l) {
+    if (l >= nk) break;
+    const int k = k0 + l;
+    const uint32_t qn = base + uint32_t(k);
+    const bool interior = k != nzmin && k != nzmax - 1;   // a4: window over k-1, k, k+1
+    const double av = __ldg(m.areasvol + qn), hnn = __ldg(in.hnode_new + qn);
+    const bool valid_n = (av > 0.0) && (hnn > 0.0);
+    const double sa = av > 0.0 ? av : 1.0, sh = hnn > 0.0 ? hnn : 1.0;
+    const Rcp rsa = rcp(sa), rsh = rcp(sh);
+    double ft[NTR], fb[NTR];
+    ldn<NTR, IL>(in.ws.adfv, qn, w0, sN, in.wtg, ft);
+    if (k + 1 < nzmax) {
+      ldn<NTR, IL>(in.ws.adfv, qn + 1, w0, sN, in.wtg, fb);
+    } else {   // the bottom interface carries no flux
+#pragma unroll
+      for (int t = 0; t < NTR; ++t) fb[t] = 0.0;
+    }
+    double pf[NTR], mf[NTR];
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) {
+      const double wmx = interior ? fmax(fmax(mx[l][t], mx[l + 1][t]), mx[l + 2][t]) : mx[l + 1][t];
+      const double wmn = interior ? fmin(fmin(mn[l][t], mn[l + 1][t]), mn[l + 2][t]) : mn[l + 1][t];
+      const double plus = (fmax(ft[t], 0.0) + fmax(-fb[t], 0.0)) + sp[l][t];
+      const double minus = (fmin(ft[t], 0.0) + fmin(-fb[t], 0.0)) + sm[l][t];
+      pf[t] = 1.0;
+      mf[t] = 1.0;
+      if (valid_n) {
+        const double flux_pos = divr(divr(plus * dt, rsa), rsh) + kFluxEps;
+        const double flux_neg = divr(divr(minus * dt, rsa), rsh) - kFluxEps;
+        pf[t] = fmin(1.0, (wmx - lo[l + 1][t]) / flux_pos);
+        mf[t] = fmin(1.0, (wmn - lo[l + 1][t]) / flux_neg);
+      }
+    }
+    stn<NTR, IL>(in.ws.pf, qn, w0, sN, in.wtg, pf);
+    stn<NTR, IL>(in.ws.mf, qn, w0, sN, in.wtg, mf);
+  }
+}
+
+// ------------------- zalesak b3 + flux2dtracer_fct + ale_reconstruct on a layer run
+template <int NTR, int LPT, bool IL>
+__device__ __forceinline__ void seg_node_final(const Inst& in, int64_t si, int t0, int w0) {
+  const DevMesh& m = *in.m;
+  constexpr int V = seg_variant(LPT);
+  constexpr int NB = LPT + 2;   // factor levels k0-1 .. k0+LPT
+  if (si >= m.n_nseg[V]) return;
+  const uint32_t sg = __ldg(m.nseg[V] + si);
+  const int n = lane_ent(sg), k0 = lane_lev(sg), L = m.L;
+  const int4 rec = __ldg(m.nrec + n);
+  const unsigned pk = unsigned(rec.z);
+  const int nzmin = int(pk & 255u), nzmax = int((pk >> 8) & 255u);
+  const int nk = min(LPT, nzmax - k0);
+  const uint32_t base = lq(n, L, 0);
+  const int64_t sN = in.ws.sN;
+  const int tg = in.tg;
+  // limited horizontal fluxes, ascending edge id
+  double hsc[LPT][NTR];
+#pragma unroll
+  for (int l = 0; l < LPT; ++l)
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) hsc[l][t] = 0.0;
+  double pfw[NB][NTR], mfw[NB][NTR];   // own factors at levels k0-1 .. k0+LPT
+#pragma unroll
+  for (int b = 0; b < NB; ++b) {
+    const uint32_t q = base + uint32_t(kclamp(k0 - 1 + b, L));
+    ldn<NTR, IL>(in.ws.pf, q, w0, sN, in.wtg, pfw[b]);
+    ldn<NTR, IL>(in.ws.mf, q, w0, sN, in.wtg, mfw[b]);
+  }
+  const int e0 = rec.x, e1 = rec.x + int((pk >> 16) & 255u);
+  for (int j = e0; j < e1; ++j) {
+    const int4 sl = __ldg(m.ne4 + j);
+    const unsigned rg = unsigned(sl.z);
+    const bool second = sl.x & 1;
+    const uint32_t qo = lq(sl.y, L, 0), qe = lq(sl.x >> 1, L, 0);
+#pragma unroll
+    for (int l = 0; l < LPT; ++l) {
+      const int k = k0 + l, kc = kclamp(k, L);
+      const bool on = l < nk && in_range(k, rg);
+      double a[NTR], pfo[NTR], mfo[NTR];
+      ldn<NTR, IL>(in.ws.adfh, qe + uint32_t(kc), w0, in.ws.sEd, in.wtg, a);
+      ldn<NTR, IL>(in.ws.pf, qo + uint32_t(kc), w0, sN, in.wtg, pfo);
+      ldn<NTR, IL>(in.ws.mf, qo + uint32_t(kc), w0, sN, in.wtg, mfo);
+#pragma unroll
+      for (int t = 0; t < NTR; ++t) {
+        const double pf0 = pfw[l + 1][t], mf0 = mfw[l + 1][t];
+        const double pf1 = second ? pfo[t] : pf0, mf1 = second ? mfo[t] : mf0;
+        const double pf2 = second ? pf0 : pfo[t], mf2 = second ? mf0 : mfo[t];
+        const double ae = a[t] >= 0.0 ? fmin(pf1, mf2) : fmin(mf1, pf2);
+        const double lim = ae * a[t];
+        hsc[l][t] = on ? hsc[l][t] + (second ? -lim : lim) : hsc[l][t];
+      }
+    }
+  }
+  const double dt = in.dt;
+#pragma unroll
+  for (int l = 0; l < LPT; ++l) {
+    if (l >= nk) break;
+    const int k = k0 + l;
+    const uint32_t qn = base + uint32_t(k);
+    const double av = __ldg(m.areasvol + qn);
+    const double sa = av > 0.0 ? av : 1.0;
+    const double hn = __ldg(in.hnode + qn), hnn = __ldg(in.hnode_new + qn);
+    const Rcp rsa = rcp(sa), rhn = rcp(hnn);
+    double ft[NTR], vt[NTR], vb[NTR];
+    ldn<NTR, IL>(in.ws.adfv, qn, w0, sN, in.wtg, ft);
+    // limited vertical flux at the top interface k (tracer_adv.py:453-459)
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) {
+      const double pf0 = pfw[l + 1][t], mf0 = mfw[l + 1][t];
+      vt[t] = k == nzmin ? (ft[t] >= 0.0 ? pf0 : mf0) * ft[t]
+                         : (ft[t] >= 0.0 ? fmin(mfw[l][t], pf0) : fmin(pfw[l][t], mf0)) * ft[t];
+    }
+    // limited vertical flux at the bottom interface k+1 (0 at the node's bottom)
+    if (k + 1 >= nzmax) {
+#pragma unroll
+      for (int t = 0; t < NTR; ++t) vb[t] = 0.0;
+    } else {
+      double fb[NTR];
+      ldn<NTR, IL>(in.ws.adfv, qn + 1, w0, sN, in.wtg, fb);
+#pragma unroll
+      for (int t = 0; t < NTR; ++t)
+        vb[t] = (fb[t] >= 0.0 ? fmin(mfw[l + 1][t], pfw[l + 2][t])
+                              : fmin(pfw[l + 1][t], mfw[l + 2][t])) * fb[t];
+    }
+    double Tv[NTR], lo[NTR], out[NTR];
+    ldn<NTR, IL>(in.T, qn, t0, in.tstride, tg, Tv);
+    ldn<NTR, IL>(in.ws.lo, qn, w0, sN, in.wtg, lo);
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) {
+      const double lo_trans = -Tv[t] * hn + lo[t] * hnn;
+      const double vdiv = av > 0.0 ? divr((vt[t] - vb[t]) * dt, rsa) : 0.0;
+      double d = divr(hsc[l][t] * dt, rsa) + (lo_trans + vdiv);
+      d = d + Tv[t] * (hn - hnn);
+      out[t] = Tv[t] + (hnn > 0.0 ? divr(d, rhn) : 0.0);
+    }
+    stn<NTR, IL>(in.T_new, qn, t0, in.tstride, tg, out);
+    count_nonfinite<NTR>(in.nonfinite, out);
+  }
+}
+
+// ------------------------------------------------------------- kernels and launchers
+// Kernel wrappers: ``_1`` takes one instance by value (tracer-major layout, the
+// single-call path; tracer slice = blockIdx.y), ``_n`` instance blockIdx.y of a device
+// table (interleaved layout; 2^lg adjacent threads of a segment take adjacent tracer
+// slices, so together they read whole interleaved lines).
+#define FCT_SEG_KERNEL(name, body)                                                       \
+  template <int NTR, int LPT>                                                            \
+  __global__ void __launch_bounds__(256) name##_1(Inst in, int t0, int w0) {             \
+    const int sub = int(blockIdx.y) * NTR;                                               \
+    body<NTR, LPT, false>(in, lane_index(), t0 + sub, w0 + sub);                         \
+  }                                                                                      \
+  template <int NTR, int LPT>                                                            \
+  __global__ void __launch_bounds__(256) name##_n(const Inst* __restrict__ tab, int t0,  \
+                                                  int w0, int lg) {                      \
+    const int64_t g = lane_index();                                                      \
+    const int sub = int(g & ((int64_t(1) << lg) - 1)) * NTR;                             \
+    body<NTR, LPT, true>(tab[blockIdx.y], g >> lg, t0 + sub, w0 + sub);                  \
+  }
+
+inline unsigned seg_blocks(int64_t lanes) {
+  return unsigned(std::max<int64_t>(1, (lanes + 255) / 256));
+}
+
+// Tracers per thread of one launch: the largest of the compiled set (1, 2, 4 with any
+// levels per thread, 8 with at most 2, in the interleaved layout; 1 or 2 tracer-major)
+// that is at most ``rem`` and ``per_thread``.
+inline int seg_tracers(int rem, int per_thread, bool interleaved, int lpt) {
+  const int lim = std::min(rem, per_thread);
+  if (interleaved && lim >= 8 && lpt <= 2) return 8;
+  if (interleaved && lim >= 4) return 4;
+  return lim >= 2 ? 2 : 1;
+}
+
+#define FCT_SEG_CASE_N(kern, P, V)                                                       \
+  case P * 16 + V:                                                                       \
+    kern##_n<P, V><<<g, 256, 0, s>>>(tab, t0, w0, lg);                                   \
+    break;
+#define FCT_SEG_CASE_1(kern, P, V)                                                       \
+  case P * 16 + V:                                                                       \
+    kern##_1<P, V><<<g, 256, 0, s>>>(single, t0, w0);                                    \
+    break;
+
+// One segment stage over the tracers [c0, c1) of a workspace chunk (workspace index of
+// tracer t is t - c0): launches of P tracers x 2^lg slices. ``COUNT(V)`` is the largest
+// segment count of the variant over the launch's instances.
+#define FCT_SEG_LAUNCHER(fn, kern, COUNT)                                                \
+  int fn(const Inst& single, const Inst* tab, int n, const LaunchDims& d, int c0, int c1, \
+         cudaStream_t s) {                                                               \
+    const int V = seg_variant(d.lpt);                                                    \
+    const int64_t lanes = COUNT(V);                                                      \
+    for (int t0 = c0; t0 < c1;) {                                                        \
+      const int rem = c1 - t0;                                                           \
+      const int P = seg_tracers(rem, d.per_thread, tab != nullptr, d.lpt);               \
+      int lg = 0;                                                                        \
+      while (lg < 3 && (P << (lg + 1)) <= rem) ++lg;                                     \
+      const int w0 = t0 - c0;                                                            \
+      if (tab) {                                                                         \
+        const dim3 g(seg_blocks(lanes << lg), unsigned(n));                              \
+        switch (P * 16 + d.lpt) {                                                        \
+          FCT_SEG_CASE_N(kern, 1, 1) FCT_SEG_CASE_N(kern, 1, 2)                          \
+          FCT_SEG_CASE_N(kern, 1, 4) FCT_SEG_CASE_N(kern, 1, 8)                          \
+          FCT_SEG_CASE_N(kern, 2, 1) FCT_SEG_CASE_N(kern, 2, 2)                          \
+          FCT_SEG_CASE_N(kern, 2, 4) FCT_SEG_CASE_N(kern, 2, 8)                          \
+          FCT_SEG_CASE_N(kern, 4, 1) FCT_SEG_CASE_N(kern, 4, 2)                          \
+          FCT_SEG_CASE_N(kern, 4, 4) FCT_SEG_CASE_N(kern, 4, 8)                          \
+          FCT_SEG_CASE_N(kern, 8, 1) FCT_SEG_CASE_N(kern, 8, 2)                          \
+          default:                                                                       \
+            return set_error(FCT_ERR_INVALID, "no segment kernel for %d tracers x %d "  \
+                             "levels per thread", P, d.lpt);                            \
+        }                                                                                \
+      } else {                                                                           \
+        const dim3 g(seg_blocks(lanes), 1u << lg);                                       \
+        switch (P * 16 + d.lpt) {                                                        \
+          FCT_SEG_CASE_1(kern, 1, 1) FCT_SEG_CASE_1(kern, 1, 2)                          \
+          FCT_SEG_CASE_1(kern, 1, 4) FCT_SEG_CASE_1(kern, 1, 8)                          \
+          FCT_SEG_CASE_1(kern, 2, 1) FCT_SEG_CASE_1(kern, 2, 2)                          \
+          FCT_SEG_CASE_1(kern, 2, 4) FCT_SEG_CASE_1(kern, 2, 8)                          \
+          default:                                                                       \
+            return set_error(FCT_ERR_INVALID, "no segment kernel for %d tracers x %d "  \
+                             "levels per thread", P, d.lpt);                            \
+        }                                                                                \
+      }                                                                                  \
+      t0 += P << lg;                                                                     \
+    }                                                                                    \
+    const cudaError_t e = cudaGetLastError();                                            \
+    return e == cudaSuccess ? FCT_OK : cuda_error(e, #fn);                               \
+  }
+
+}  // namespace
+}  // namespace fct

@@ -51,11 +51,12 @@ def _bind_batch(L):
                                     C.c_void_p]
     L.fct_stage_name.restype = C.c_char_p
     L.fct_batch_set_chunk.argtypes = [C.c_void_p, C.c_int]
+    L.fct_batch_set_mapping.argtypes = [C.c_void_p, C.c_int, C.c_int]
     L.fct_batch_health.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_int64)]
     L.fct_batch_fill_workspace.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
     for n in ("fct_batch_create", "fct_batch_destroy", "fct_batch_info", "fct_batch_prepare",
               "fct_batch_step", "fct_batch_run", "fct_batch_profile", "fct_batch_set_chunk",
-              "fct_batch_health", "fct_batch_fill_workspace"):
+              "fct_batch_health", "fct_batch_fill_workspace", "fct_batch_set_mapping"):
         getattr(L, n).restype = C.c_int
     L._batch_bound = True
     return L
@@ -89,7 +90,8 @@ class Ensemble:
         self._plans: dict[int, FctPlan] = {}
         self._h = None
         self.phase = 0
-        self.chunk = 8
+        self.chunk = 2          # tracers per thread of the fused stages
+        self.levels = 4         # levels per thread
 
     # ---------------------------------------------------------------- members
     def plan(self, mesh: Mesh) -> FctPlan:
@@ -200,19 +202,32 @@ class Ensemble:
                                                                     self._stream(stream)))
 
     def set_chunk(self, chunk: int) -> None:
-        _lib.check(_bind_batch(_lib.lib()).fct_batch_set_chunk(self._h, int(chunk)))
-        self.chunk = int(chunk)
+        """Tracers per thread of the fused stages (1, 2, 4 or 8)."""
+        self.set_mapping(chunk, self.levels)
 
-    def autotune(self, steps: int = 2, candidates=(8, 4, 2, 1), reps: int = 2) -> dict:
-        """Time ``steps``-step graph runs for each tracer-chunk candidate (the member state
-        advances while tuning) and keep the fastest; returns ``{chunk: ms}``."""
+    def set_mapping(self, tracers_per_thread: int, levels_per_thread: int) -> None:
+        """Thread mapping of the fused stages: tracers and column levels per thread (each
+        1, 2, 4 or 8; 8 tracers with at most 2 levels). Results do not depend on it."""
+        _lib.check(_bind_batch(_lib.lib()).fct_batch_set_mapping(
+            self._h, int(tracers_per_thread), int(levels_per_thread)))
+        self.chunk, self.levels = int(tracers_per_thread), int(levels_per_thread)
+
+    # (tracers per thread, levels per thread) tried by autotune
+    MAPPINGS = ((1, 2), (1, 4), (1, 8), (2, 1), (2, 2), (2, 4), (2, 8), (4, 1), (4, 2),
+                (4, 4), (8, 1))
+
+    def autotune(self, steps: int = 2, candidates=None, reps: int = 2) -> dict:
+        """Time ``steps``-step graph runs for each (tracers, levels) per-thread mapping (the
+        member state advances while tuning) and keep the fastest; returns
+        ``{"TxL": ms}``."""
         t = self.torch
         stream = t.cuda.current_stream(self.device)
+        ntr_max = max(m.ntr for m in self.members)
         times = {}
-        for c in candidates:
-            if c > max(m.ntr for m in self.members) and c != min(candidates):
+        for c, lv in (candidates or self.MAPPINGS):
+            if c > ntr_max and c != 1:
                 continue
-            self.set_chunk(c)
+            self.set_mapping(c, lv)
             self.run(steps)                      # capture + warm
             e0, e1 = t.cuda.Event(enable_timing=True), t.cuda.Event(enable_timing=True)
             e0.record(stream)
@@ -220,10 +235,10 @@ class Ensemble:
                 self.run(steps)
             e1.record(stream)
             e1.synchronize()
-            times[c] = e0.elapsed_time(e1) / reps
+            times[(c, lv)] = e0.elapsed_time(e1) / reps
         best = min(times, key=times.get)
-        self.set_chunk(best)
-        return times
+        self.set_mapping(*best)
+        return {f"{c}x{lv}": v for (c, lv), v in times.items()}
 
     def profile_step(self, stream=None) -> dict:
         """Run one step stage by stage (synchronising) and return ``{stage: ms}``."""

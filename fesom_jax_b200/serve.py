@@ -165,7 +165,7 @@ class ServingEngine:
         """Doubles of the fused-stage workspace one instance takes in the arena."""
         m = self.meshes[r.mesh].mesh
         N, Ed, L = m.nod2D, m.edge2D, m.nl
-        return Ed * L + self.ntr * (6 * N * L + Ed * L)
+        return Ed * L + self.ntr * (4 * N * L + Ed * L)
 
     def state_bytes(self, r: Request) -> int:
         m = self.meshes[r.mesh].mesh

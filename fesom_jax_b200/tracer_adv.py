@@ -88,6 +88,15 @@ class FctPlan:
         L.fct_plan_fill_workspace.restype = C.c_int
         _lib.check(L.fct_plan_fill_workspace(self._h, int(byte), C.c_void_p(int(s))))
 
+    def set_mapping(self, tracers_per_thread: int, levels_per_thread: int) -> None:
+        """Thread mapping of the fused stages (tracers and column levels per thread, each
+        1, 2, 4 or 8); a tuning knob, the results do not depend on it."""
+        L = _lib.lib()
+        L.fct_plan_set_mapping.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        L.fct_plan_set_mapping.restype = C.c_int
+        _lib.check(L.fct_plan_set_mapping(self._h, int(tracers_per_thread),
+                                          int(levels_per_thread)))
+
     def set_fused(self, fused: bool) -> None:
         """Fused stage kernels (default) or one kernel per reference stage; same bits."""
         _lib.check(_lib.lib().fct_plan_set_fused(self._h, int(bool(fused))))

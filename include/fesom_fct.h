@@ -106,11 +106,18 @@ int fct_plan_reserve(FctPlan* plan, int max_tracers);
 /* Counts: [nod2D, elem2D, edge2D, nl, wet node layers, wet element layers, wet edge
  * layers, max_tracers]. */
 int fct_plan_info(const FctPlan* plan, int64_t out[8]);
-/* Which stage kernels fct_forward runs: fused (1, the default: 4 launches per tracer
- * chunk, element gradients and cluster bounds recomputed instead of stored) or one kernel
- * per reference stage (0: 7 launches, every intermediate written to the workspace, the
- * form the reverse pass recomputes). Both give the same T_new bit for bit. */
+/* Which stage kernels fct_forward runs: fused (1, the default: 5 launches per tracer
+ * chunk over runs of consecutive levels, element gradients and cluster bounds recomputed
+ * instead of stored) or one kernel per reference stage (0: 7 launches, every intermediate
+ * written to the workspace, the form the reverse pass recomputes). Both give the same
+ * T_new bit for bit. */
 int fct_plan_set_fused(FctPlan* plan, int fused);
+/* Thread mapping of the fused stages of this plan's fct_forward / fct_forward_noalloc and
+ * of its instances in fct_serve_step: the most tracers one thread carries and the levels
+ * of one node or edge column it takes (each 1, 2, 4 or 8; default 2 and 4). A tuning knob:
+ * the results do not depend on it. No reference counterpart (XLA picks its own loop
+ * mapping). */
+int fct_plan_set_mapping(FctPlan* plan, int tracers_per_thread, int levels_per_thread);
 
 /* One FCT step for ``ntr`` tracers: fesom_jax/tracer_adv.py:532-578 (advect_one_fct),
  * with exch=None. Writes T_new; T_old_new is T itself (the caller keeps the alias).
@@ -323,6 +330,9 @@ int fct_batch_destroy(FctBatch* b);
  * chunk, at most 8). Fewer use fewer registers (higher occupancy), more share each
  * gather's index work. Drops cached graphs. */
 int fct_batch_set_chunk(FctBatch* b, int chunk);
+/* Tuning: tracers per thread (1, 2, 4 or 8) and levels per thread (1, 2, 4 or 8) of the
+ * fused stages (8 tracers per thread run with at most 2 levels). Drops cached graphs. */
+int fct_batch_set_mapping(FctBatch* b, int tracers_per_thread, int levels_per_thread);
 /* [instances, groups, workspace bytes, total wet node layers x tracers,
  *  tracers per workspace chunk (largest over groups), kernel launches per step] */
 int fct_batch_info(const FctBatch* b, int64_t out[6]);

@@ -99,7 +99,7 @@ def test_profile_step_reports_every_stage(torch, members):
 
 def _ws_bytes(m, ntr):
     L = m.nl
-    return 8 * (m.edge2D * L + ntr * (6 * m.nod2D * L + m.edge2D * L))   # fused workspace
+    return 8 * (m.edge2D * L + ntr * (4 * m.nod2D * L + m.edge2D * L))   # fused workspace
 
 
 @pytest.mark.parametrize("per_thread", [8, 2, 1])
@@ -117,7 +117,7 @@ def test_chunked_workspace_equals_plain(torch, pi, per_thread):
     torch.cuda.synchronize()
     launches = ens.info()["launches_per_step"]
     # one launch per stage per chunk: S slices x per_thread tracers cover each chunk
-    assert launches == 1 + 4 * 3   # vflux + 4 fused stages per chunk
+    assert launches == 1 + 5 * 3   # vflux + 5 fused stages per chunk
     T, To = ens.state(0)
     Tp, Top = _plain(torch, pi, f, STEPS)
     assert np.array_equal(T.cpu().numpy(), Tp)

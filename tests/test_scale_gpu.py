@@ -57,7 +57,7 @@ def _members(torch, mesh, cfg, n, ntr):
 
 def _ws_bytes(mesh, chunk):
     N, Ed, L = mesh.nod2D, mesh.edge2D, mesh.nl
-    return 8 * (Ed * L + chunk * (6 * N * L + Ed * L))
+    return 8 * (Ed * L + chunk * (4 * N * L + Ed * L))
 
 
 def test_core2_batched_tuned_mapping_30_steps(torch):
