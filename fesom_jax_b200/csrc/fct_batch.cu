@@ -241,8 +241,8 @@ int fct_batch_info(const FctBatch* B, int64_t out[6]) {
       const int csz = std::min(chunk, g.dims.ntr - c0);
       per_chunk_launches += stage_launches(csz, g.dims.per_thread);
     }
-    const int stages = (g.dims.fused ? 5 : 7) + (g.dims.any_wi ? 1 : 0) +
-                       (g.dims.any_vdiff ? 1 : 0);
+    const int stages = (g.dims.fused ? 4 + (g.dims.max_efix > 0 ? 1 : 0) : 7) +
+                       (g.dims.any_wi ? 1 : 0) + (g.dims.any_vdiff ? 1 : 0);
     launches += 1 + (g.dims.any_derive_w ? 1 : 0) + int64_t(stages) * per_chunk_launches;
   }
   out[4] = wmax;

@@ -34,8 +34,7 @@ int launch_edge_fix(const Inst& single, const Inst* tab, int n, const LaunchDims
     const int w0 = t0 - c0;
     if (tab) {
       const dim3 g(seg_blocks(d.max_efix << lg), unsigned(n));
-      if (P == 8) k_edge_fix_n<8><<<g, 256, 0, s>>>(tab, t0, w0, lg);
-      else if (P == 4) k_edge_fix_n<4><<<g, 256, 0, s>>>(tab, t0, w0, lg);
+      if (P == 4) k_edge_fix_n<4><<<g, 256, 0, s>>>(tab, t0, w0, lg);
       else if (P == 2) k_edge_fix_n<2><<<g, 256, 0, s>>>(tab, t0, w0, lg);
       else k_edge_fix_n<1><<<g, 256, 0, s>>>(tab, t0, w0, lg);
     } else {
@@ -52,7 +51,7 @@ int launch_edge_fix(const Inst& single, const Inst* tab, int n, const LaunchDims
 namespace {
 
 #define FCT_COUNT(V) d.max_eseg[V]
-FCT_SEG_LAUNCHER(launch_impl, k_seg_edge, FCT_COUNT)
+FCT_SEG_LAUNCHER(launch_impl, k_seg_edge, FCT_COUNT, FCT_GRID_N, FCT_GRID_1)
 #undef FCT_COUNT
 
 }  // namespace

@@ -319,90 +319,109 @@ __device__ __forceinline__ void body_edge_fix(const Inst& in, int64_t i, int t0,
 // the nodes of n's cells that are wet at k, padded with -BIG (+BIG) when one of n's cells
 // is dry at k (tracer_adv.py:389-405). Every cell of n has two edges at n, so those nodes
 // are n itself (when any cell is wet at k) and the edge neighbours with a wet cell at k;
-// max/min are exact, so this equals the per-cell evaluation bit for bit. The a4 window
-// needs the bounds one level above and below the run: the run evaluates them too.
+// max/min are exact, so this equals the per-cell evaluation bit for bit.
+// The a4 window (k-1, k, k+1 of the same column) crosses a run's ends: each thread leaves
+// the bounds of its run's first and last level in shared memory, and the neighbouring
+// runs of the column (the adjacent segment slots of the block: a column's runs are
+// consecutive) read them. A block's first and last slot are halo runs that only publish
+// their bounds; ``sh`` holds [4][NTR][256] doubles (first-level max, min, last-level max,
+// min) and ``S`` is the distance between adjacent slots in threads.
 template <int NTR, int LPT, bool IL>
-__device__ __forceinline__ void seg_node_limit(const Inst& in, int64_t si, int t0, int w0) {
+__device__ __forceinline__ void seg_node_limit(const Inst& in, int64_t si, bool core, int t0,
+                                               int w0, int tid, int S, double* sh) {
   const DevMesh& m = *in.m;
   constexpr int V = seg_variant(LPT);
-  constexpr int NB = LPT + 2;   // bound levels k0-1 .. k0+LPT
-  if (si >= m.n_nseg[V]) return;
-  const uint32_t sg = __ldg(m.nseg[V] + si);
-  const int n = lane_ent(sg), k0 = lane_lev(sg), L = m.L;
-  const int4 rec = __ldg(m.nrec + n);
-  const unsigned pk = unsigned(rec.z);
-  const int nzmin = int(pk & 255u), nzmax = int((pk >> 8) & 255u);
-  const int nk = min(LPT, nzmax - k0);
-  const uint32_t base = lq(n, L, 0);
+  const bool valid = si >= 0 && si < m.n_nseg[V];
+  const int L = m.L;
   const int64_t sN = in.ws.sN;
-  double mx[NB][NTR], mn[NB][NTR], sp[LPT][NTR], sm[LPT][NTR];
-#pragma unroll
-  for (int b = 0; b < NB; ++b)
-#pragma unroll
-    for (int t = 0; t < NTR; ++t) { mx[b][t] = -INFINITY; mn[b][t] = INFINITY; }
+  int n = 0, k0 = 0, nzmin = 0, nzmax = 1, nk = 1;
+  uint32_t base = 0;
+  double mx[LPT][NTR], mn[LPT][NTR], sp[LPT][NTR], sm[LPT][NTR], lo[LPT][NTR];
 #pragma unroll
   for (int l = 0; l < LPT; ++l)
 #pragma unroll
-    for (int t = 0; t < NTR; ++t) sp[l][t] = sm[l][t] = 0.0;
-  unsigned own = 0u, off = 0u;   // bit b: a cell of n is wet / dry at level k0-1+b
-  const int e0 = rec.x, e1 = rec.x + int((pk >> 16) & 255u);
-  for (int j = e0; j < e1; ++j) {
-    const int4 sl = __ldg(m.ne4 + j);
-    const unsigned tr = unsigned(sl.w), rg = unsigned(sl.z);
-    const bool has2 = ((tr >> 16) & 255u) != kNoCell;
-    const bool second = sl.x & 1;
-    const uint32_t qo = lq(sl.y, L, 0), qe = lq(sl.x >> 1, L, 0);
+    for (int t = 0; t < NTR; ++t) {
+      mx[l][t] = -INFINITY; mn[l][t] = INFINITY; sp[l][t] = 0.0; sm[l][t] = 0.0;
+      lo[l][t] = 0.0;
+    }
+  if (valid) {
+    const uint32_t sg = __ldg(m.nseg[V] + si);
+    n = lane_ent(sg);
+    k0 = lane_lev(sg);
+    const int4 rec = __ldg(m.nrec + n);
+    const unsigned pk = unsigned(rec.z);
+    nzmin = int(pk & 255u);
+    nzmax = int((pk >> 8) & 255u);
+    nk = min(LPT, nzmax - k0);
+    base = lq(n, L, 0);
+    unsigned own = 0u, off = 0u;   // bit l: a cell of n is wet / dry at level k0+l
+    const int e0 = rec.x, e1 = rec.x + int((pk >> 16) & 255u);
+    for (int j = e0; j < e1; ++j) {
+      const int4 sl = __ldg(m.ne4 + j);
+      const unsigned tr = unsigned(sl.w), rg = unsigned(sl.z);
+      const bool has2 = ((tr >> 16) & 255u) != kNoCell;
+      const bool second = sl.x & 1;
+      const uint32_t qo = lq(sl.y, L, 0), qe = lq(sl.x >> 1, L, 0);
 #pragma unroll
-    for (int b = 0; b < NB; ++b) {
-      const int k = k0 - 1 + b, kc = kclamp(k, L);
-      const bool c1 = in_range(k, tr & 0xffffu);
-      const bool c2 = has2 && in_range(k, tr >> 16);
-      const bool wet = c1 || c2;
-      own |= unsigned(wet) << b;
-      off |= unsigned(!c1 || (has2 && !c2)) << b;
-      double lv[NTR], tv[NTR];
-      ldn<NTR, IL>(in.ws.lo, qo + uint32_t(kc), w0, sN, in.wtg, lv);
-      ldn<NTR, IL>(in.T, qo + uint32_t(kc), t0, in.tstride, in.tg, tv);
-#pragma unroll
-      for (int t = 0; t < NTR; ++t) {
-        mx[b][t] = wet ? fmax(mx[b][t], fmax(lv[t], tv[t])) : mx[b][t];
-        mn[b][t] = wet ? fmin(mn[b][t], fmin(lv[t], tv[t])) : mn[b][t];
-      }
-      if (b >= 1 && b <= LPT) {   // the run's own levels: antidiffusive sums (b1)
-        const int l = b - 1;
+      for (int l = 0; l < LPT; ++l) {
+        const int k = k0 + l, kc = kclamp(k, L);
+        const bool c1 = in_range(k, tr & 0xffffu);
+        const bool c2 = has2 && in_range(k, tr >> 16);
+        const bool wet = c1 || c2;
+        own |= unsigned(wet) << l;
+        off |= unsigned(!c1 || (has2 && !c2)) << l;
         const bool on = l < nk && in_range(k, rg);
-        double a[NTR];
+        double lv[NTR], tv[NTR], a[NTR];
+        ldn<NTR, IL>(in.ws.lo, qo + uint32_t(kc), w0, sN, in.wtg, lv);
+        ldn<NTR, IL>(in.T, qo + uint32_t(kc), t0, in.tstride, in.tg, tv);
         ldn<NTR, IL>(in.ws.adfh, qe + uint32_t(kc), w0, in.ws.sEd, in.wtg, a);
 #pragma unroll
         for (int t = 0; t < NTR; ++t) {
+          mx[l][t] = wet ? fmax(mx[l][t], fmax(lv[t], tv[t])) : mx[l][t];
+          mn[l][t] = wet ? fmin(mn[l][t], fmin(lv[t], tv[t])) : mn[l][t];
           const double sv = second ? -a[t] : a[t];
           sp[l][t] = on ? sp[l][t] + fmax(sv, 0.0) : sp[l][t];
           sm[l][t] = on ? sm[l][t] + fmin(sv, 0.0) : sm[l][t];
         }
       }
     }
-  }
-  // the node itself, and the padding of dry cells
-  double lo[NB][NTR];
+    // the node itself, and the padding of dry cells
 #pragma unroll
-  for (int b = 0; b < NB; ++b) {
-    const int kc = kclamp(k0 - 1 + b, L);
-    double tv[NTR];
-    ldn<NTR, IL>(in.ws.lo, base + uint32_t(kc), w0, sN, in.wtg, lo[b]);
-    ldn<NTR, IL>(in.T, base + uint32_t(kc), t0, in.tstride, in.tg, tv);
-    const bool ow = (own >> b) & 1u, of = (off >> b) & 1u;
+    for (int l = 0; l < LPT; ++l) {
+      const int kc = kclamp(k0 + l, L);
+      double tv[NTR];
+      ldn<NTR, IL>(in.ws.lo, base + uint32_t(kc), w0, sN, in.wtg, lo[l]);
+      ldn<NTR, IL>(in.T, base + uint32_t(kc), t0, in.tstride, in.tg, tv);
+      const bool ow = (own >> l) & 1u, of = (off >> l) & 1u;
 #pragma unroll
-    for (int t = 0; t < NTR; ++t) {
-      if (ow) {
-        mx[b][t] = fmax(mx[b][t], fmax(lo[b][t], tv[t]));
-        mn[b][t] = fmin(mn[b][t], fmin(lo[b][t], tv[t]));
-      }
-      if (of) {
-        mx[b][t] = fmax(mx[b][t], -kBig);
-        mn[b][t] = fmin(mn[b][t], kBig);
+      for (int t = 0; t < NTR; ++t) {
+        if (ow) {
+          mx[l][t] = fmax(mx[l][t], fmax(lo[l][t], tv[t]));
+          mn[l][t] = fmin(mn[l][t], fmin(lo[l][t], tv[t]));
+        }
+        if (of) {
+          mx[l][t] = fmax(mx[l][t], -kBig);
+          mn[l][t] = fmin(mn[l][t], kBig);
+        }
       }
     }
+    // publish the first and last level's bounds for the neighbouring runs
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) {
+      sh[(0 * NTR + t) * 256 + tid] = mx[0][t];
+      sh[(1 * NTR + t) * 256 + tid] = mn[0][t];
+    }
+#pragma unroll
+    for (int l = 0; l < LPT; ++l)
+      if (l == nk - 1)
+#pragma unroll
+        for (int t = 0; t < NTR; ++t) {
+          sh[(2 * NTR + t) * 256 + tid] = mx[l][t];
+          sh[(3 * NTR + t) * 256 + tid] = mn[l][t];
+        }
   }
+  __syncthreads();
+  if (!valid || !core) return;
   const double dt = in.dt;
 #pragma unroll
   for (int l = 0; l < LPT; ++l) {
@@ -412,8 +431,8 @@ __device__ __forceinline__ void seg_node_limit(const Inst& in, int64_t si, int t
     const bool interior = k != nzmin && k != nzmax - 1;   // a4: window over k-1, k, k+1
     const double av = __ldg(m.areasvol + qn), hnn = __ldg(in.hnode_new + qn);
     const bool valid_n = (av > 0.0) && (hnn > 0.0);
-    const double sa = av > 0.0 ? av : 1.0, sh = hnn > 0.0 ? hnn : 1.0;
-    const Rcp rsa = rcp(sa), rsh = rcp(sh);
+    const double sa = av > 0.0 ? av : 1.0, sh_ = hnn > 0.0 ? hnn : 1.0;
+    const Rcp rsa = rcp(sa), rsh = rcp(sh_);
     double ft[NTR], fb[NTR];
     ldn<NTR, IL>(in.ws.adfv, qn, w0, sN, in.wtg, ft);
     if (k + 1 < nzmax) {
@@ -425,8 +444,17 @@ __device__ __forceinline__ void seg_node_limit(const Inst& in, int64_t si, int t
     double pf[NTR], mf[NTR];
 #pragma unroll
     for (int t = 0; t < NTR; ++t) {
-      const double wmx = interior ? fmax(fmax(mx[l][t], mx[l + 1][t]), mx[l + 2][t]) : mx[l + 1][t];
-      const double wmn = interior ? fmin(fmin(mn[l][t], mn[l + 1][t]), mn[l + 2][t]) : mn[l + 1][t];
+      double wmx = mx[l][t], wmn = mn[l][t];
+      if (interior) {
+        const double ax = l > 0 ? mx[l - 1][t] : sh[(2 * NTR + t) * 256 + tid - S];
+        const double an = l > 0 ? mn[l - 1][t] : sh[(3 * NTR + t) * 256 + tid - S];
+        const double bx = l + 1 < nk ? mx[l + 1 < LPT ? l + 1 : l][t]
+                                     : sh[(0 * NTR + t) * 256 + tid + S];
+        const double bn = l + 1 < nk ? mn[l + 1 < LPT ? l + 1 : l][t]
+                                     : sh[(1 * NTR + t) * 256 + tid + S];
+        wmx = fmax(fmax(ax, wmx), bx);
+        wmn = fmin(fmin(an, wmn), bn);
+      }
       const double plus = (fmax(ft[t], 0.0) + fmax(-fb[t], 0.0)) + sp[l][t];
       const double minus = (fmin(ft[t], 0.0) + fmin(-fb[t], 0.0)) + sm[l][t];
       pf[t] = 1.0;
@@ -434,8 +462,8 @@ __device__ __forceinline__ void seg_node_limit(const Inst& in, int64_t si, int t
       if (valid_n) {
         const double flux_pos = divr(divr(plus * dt, rsa), rsh) + kFluxEps;
         const double flux_neg = divr(divr(minus * dt, rsa), rsh) - kFluxEps;
-        pf[t] = fmin(1.0, (wmx - lo[l + 1][t]) / flux_pos);
-        mf[t] = fmin(1.0, (wmn - lo[l + 1][t]) / flux_neg);
+        pf[t] = fmin(1.0, (wmx - lo[l][t]) / flux_pos);
+        mf[t] = fmin(1.0, (wmn - lo[l][t]) / flux_neg);
       }
     }
     stn<NTR, IL>(in.ws.pf, qn, w0, sN, in.wtg, pf);
@@ -549,30 +577,68 @@ __device__ __forceinline__ void seg_node_final(const Inst& in, int64_t si, int t
 // single-call path; tracer slice = blockIdx.y), ``_n`` instance blockIdx.y of a device
 // table (interleaved layout; 2^lg adjacent threads of a segment take adjacent tracer
 // slices, so together they read whole interleaved lines).
+// Resident 256-thread blocks per SM the compiler must fit, by the updates a thread
+// carries (registers capped accordingly: the gathers are latency-bound, so resident warps
+// pay more than the spills a cap may cost)
+__host__ __device__ constexpr int seg_min_blocks(int ntr, int lpt) {
+  return ntr * lpt <= 1 ? 6 : ntr * lpt <= 2 ? 4 : ntr * lpt <= 4 ? 3 : ntr * lpt <= 8 ? 2 : 1;
+}
+
 #define FCT_SEG_KERNEL(name, body)                                                       \
   template <int NTR, int LPT>                                                            \
-  __global__ void __launch_bounds__(256) name##_1(Inst in, int t0, int w0) {             \
+  __global__ void __launch_bounds__(256, seg_min_blocks(NTR, LPT))                       \
+      name##_1(Inst in, int t0, int w0) {                                                \
     const int sub = int(blockIdx.y) * NTR;                                               \
     body<NTR, LPT, false>(in, lane_index(), t0 + sub, w0 + sub);                         \
   }                                                                                      \
   template <int NTR, int LPT>                                                            \
-  __global__ void __launch_bounds__(256) name##_n(const Inst* __restrict__ tab, int t0,  \
-                                                  int w0, int lg) {                      \
+  __global__ void __launch_bounds__(256, seg_min_blocks(NTR, LPT))                       \
+      name##_n(const Inst* __restrict__ tab, int t0, int w0, int lg) {                   \
     const int64_t g = lane_index();                                                      \
     const int sub = int(g & ((int64_t(1) << lg) - 1)) * NTR;                             \
     body<NTR, LPT, true>(tab[blockIdx.y], g >> lg, t0 + sub, w0 + sub);                  \
   }
 
+// The limiter stage: 256-thread blocks of 256/S segment slots (S = 2^lg tracer-slice
+// threads per slot in ``_n``, 1 in ``_1``), the first and last slot halo runs.
+#define FCT_SEG_LIMIT_KERNEL(name)                                                       \
+  template <int NTR, int LPT>                                                            \
+  __global__ void __launch_bounds__(256, seg_min_blocks(NTR, LPT))                       \
+      name##_1(Inst in, int t0, int w0) {                                                \
+    __shared__ double sh[4 * NTR * 256];                                                 \
+    const int tid = threadIdx.x;                                                         \
+    const int64_t si = int64_t(blockIdx.x) * 254 + tid - 1;                              \
+    const int sub = int(blockIdx.y) * NTR;                                               \
+    seg_node_limit<NTR, LPT, false>(in, si, tid >= 1 && tid <= 254, t0 + sub, w0 + sub,  \
+                                    tid, 1, sh);                                         \
+  }                                                                                      \
+  template <int NTR, int LPT>                                                            \
+  __global__ void __launch_bounds__(256, seg_min_blocks(NTR, LPT))                       \
+      name##_n(const Inst* __restrict__ tab, int t0, int w0, int lg) {                   \
+    __shared__ double sh[4 * NTR * 256];                                                 \
+    const int tid = threadIdx.x;                                                         \
+    const int slot = tid >> lg, slots = 256 >> lg;                                       \
+    const int64_t si = int64_t(blockIdx.x) * (slots - 2) + slot - 1;                     \
+    const int sub = (tid & ((1 << lg) - 1)) * NTR;                                       \
+    seg_node_limit<NTR, LPT, true>(tab[blockIdx.y], si, slot >= 1 && slot <= slots - 2,  \
+                                   t0 + sub, w0 + sub, tid, 1 << lg, sh);                \
+  }
+
 inline unsigned seg_blocks(int64_t lanes) {
   return unsigned(std::max<int64_t>(1, (lanes + 255) / 256));
 }
+// grids: one thread per segment and slice; the limiter's blocks hold 256/S - 2 core slots
+#define FCT_GRID_N(lanes, lg) seg_blocks((lanes) << (lg))
+#define FCT_GRID_1(lanes) seg_blocks(lanes)
+#define FCT_LIMIT_GRID_N(lanes, lg) \
+  unsigned(std::max<int64_t>(1, ((lanes) + (256 >> (lg)) - 3) / ((256 >> (lg)) - 2)))
+#define FCT_LIMIT_GRID_1(lanes) unsigned(std::max<int64_t>(1, ((lanes) + 253) / 254))
 
-// Tracers per thread of one launch: the largest of the compiled set (1, 2, 4 with any
-// levels per thread, 8 with at most 2, in the interleaved layout; 1 or 2 tracer-major)
-// that is at most ``rem`` and ``per_thread``.
+// Tracers per thread of one launch: the largest of the compiled set (1, 2 or 4 in the
+// interleaved layout; 1 or 2 tracer-major) that is at most ``rem`` and ``per_thread``.
 inline int seg_tracers(int rem, int per_thread, bool interleaved, int lpt) {
+  (void)lpt;
   const int lim = std::min(rem, per_thread);
-  if (interleaved && lim >= 8 && lpt <= 2) return 8;
   if (interleaved && lim >= 4) return 4;
   return lim >= 2 ? 2 : 1;
 }
@@ -589,7 +655,7 @@ inline int seg_tracers(int rem, int per_thread, bool interleaved, int lpt) {
 // One segment stage over the tracers [c0, c1) of a workspace chunk (workspace index of
 // tracer t is t - c0): launches of P tracers x 2^lg slices. ``COUNT(V)`` is the largest
 // segment count of the variant over the launch's instances.
-#define FCT_SEG_LAUNCHER(fn, kern, COUNT)                                                \
+#define FCT_SEG_LAUNCHER(fn, kern, COUNT, GRID_N, GRID_1)                                \
   int fn(const Inst& single, const Inst* tab, int n, const LaunchDims& d, int c0, int c1, \
          cudaStream_t s) {                                                               \
     const int V = seg_variant(d.lpt);                                                    \
@@ -601,7 +667,7 @@ inline int seg_tracers(int rem, int per_thread, bool interleaved, int lpt) {
       while (lg < 3 && (P << (lg + 1)) <= rem) ++lg;                                     \
       const int w0 = t0 - c0;                                                            \
       if (tab) {                                                                         \
-        const dim3 g(seg_blocks(lanes << lg), unsigned(n));                              \
+        const dim3 g(GRID_N(lanes, lg), unsigned(n));                                    \
         switch (P * 16 + d.lpt) {                                                        \
           FCT_SEG_CASE_N(kern, 1, 1) FCT_SEG_CASE_N(kern, 1, 2)                          \
           FCT_SEG_CASE_N(kern, 1, 4) FCT_SEG_CASE_N(kern, 1, 8)                          \
@@ -609,13 +675,12 @@ inline int seg_tracers(int rem, int per_thread, bool interleaved, int lpt) {
           FCT_SEG_CASE_N(kern, 2, 4) FCT_SEG_CASE_N(kern, 2, 8)                          \
           FCT_SEG_CASE_N(kern, 4, 1) FCT_SEG_CASE_N(kern, 4, 2)                          \
           FCT_SEG_CASE_N(kern, 4, 4) FCT_SEG_CASE_N(kern, 4, 8)                          \
-          FCT_SEG_CASE_N(kern, 8, 1) FCT_SEG_CASE_N(kern, 8, 2)                          \
           default:                                                                       \
             return set_error(FCT_ERR_INVALID, "no segment kernel for %d tracers x %d "  \
                              "levels per thread", P, d.lpt);                            \
         }                                                                                \
       } else {                                                                           \
-        const dim3 g(seg_blocks(lanes), 1u << lg);                                       \
+        const dim3 g(GRID_1(lanes), 1u << lg);                                           \
         switch (P * 16 + d.lpt) {                                                        \
           FCT_SEG_CASE_1(kern, 1, 1) FCT_SEG_CASE_1(kern, 1, 2)                          \
           FCT_SEG_CASE_1(kern, 1, 4) FCT_SEG_CASE_1(kern, 1, 8)                          \

@@ -213,8 +213,7 @@ class Ensemble:
         self.chunk, self.levels = int(tracers_per_thread), int(levels_per_thread)
 
     # (tracers per thread, levels per thread) tried by autotune
-    MAPPINGS = ((1, 2), (1, 4), (1, 8), (2, 1), (2, 2), (2, 4), (2, 8), (4, 1), (4, 2),
-                (4, 4), (8, 1))
+    MAPPINGS = ((1, 1), (1, 2), (1, 4), (1, 8), (2, 1), (2, 2), (2, 4), (4, 1), (4, 2))
 
     def autotune(self, steps: int = 2, candidates=None, reps: int = 2) -> dict:
         """Time ``steps``-step graph runs for each (tracers, levels) per-thread mapping (the

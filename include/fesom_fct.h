@@ -330,8 +330,8 @@ int fct_batch_destroy(FctBatch* b);
  * chunk, at most 8). Fewer use fewer registers (higher occupancy), more share each
  * gather's index work. Drops cached graphs. */
 int fct_batch_set_chunk(FctBatch* b, int chunk);
-/* Tuning: tracers per thread (1, 2, 4 or 8) and levels per thread (1, 2, 4 or 8) of the
- * fused stages (8 tracers per thread run with at most 2 levels). Drops cached graphs. */
+/* Tuning: tracers per thread (1, 2, 4 or 8; the fused stages carry at most 4) and levels
+ * per thread (1, 2, 4 or 8) of the fused stages. Drops cached graphs. */
 int fct_batch_set_mapping(FctBatch* b, int tracers_per_thread, int levels_per_thread);
 /* [instances, groups, workspace bytes, total wet node layers x tracers,
  *  tracers per workspace chunk (largest over groups), kernel launches per step] */

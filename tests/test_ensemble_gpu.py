@@ -137,8 +137,8 @@ def test_derived_w_equals_compute_w_then_fct(torch, pi):
     ens.add_member(pi, f.uv, None, f.helem, f.hnode, f.hnode_new, f.tracers, f.tracers_old,
                    DT, derive_w=True)
     ens.build()
-    # compute_w + vflux + 4 fused stages x 2 launches (3 tracers: a 2-tracer and a 1-tracer split)
-    assert ens.info()["launches_per_step"] == 1 + 1 + 4 * 2
+    # compute_w + vflux + 5 fused stages x 2 launches (3 tracers: a 2-tracer and a 1-tracer split)
+    assert ens.info()["launches_per_step"] == 1 + 1 + 5 * 2
     ens.run(STEPS)
     torch.cuda.synchronize()
     d = lambda x: torch.from_numpy(np.ascontiguousarray(x)).cuda()  # noqa: E731
