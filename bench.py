@@ -370,8 +370,9 @@ def run_ours(args, D: Dist) -> dict | None:
                              alg_bytes_per_step=alg,
                              issue=issue_roofline(value / D.world, clk)),
                gpu_launches=n_kernels * S * args.steps,
-               tuning=dict(tracers_per_thread=ens.chunk, levels_per_thread=ens.levels,
-                           candidates_ms_per_2_steps=tune))
+               tuning=dict(stage_mapping={st: f"{c}x{lv}" for st, (c, lv) in
+                                          zip(ens.STAGES, ens.stage_map)},
+                           autotune=tune))
 
     # plain one-instance-per-launch comparison (the reference's call granularity:
     # one tracer per advect_one_fct call), member 0, one FCT step per call
@@ -396,7 +397,7 @@ def run_ours(args, D: Dist) -> dict | None:
         tp = e0.elapsed_time(e1) / 1e3
         out["plain"] = dict(value=reps * cfg["ntr"] * mesh.n_wet_layers / tp, unit=UNIT,
                             how="fct_forward, 1 tracer per call, 1 FCT step per call")
-    tuned = (ens.chunk, ens.levels)
+    tuned = list(ens.stage_map)
     ens.close()   # the end-to-end run below builds its own ensemble
     del ens
     torch.cuda.empty_cache()
@@ -446,8 +447,9 @@ def e2e_host(args, mesh, cfg, dev, per_thread=None) -> dict:
     torch.cuda.empty_cache()
     for e in ens:
         e.build()
-        if per_thread:   # the main run's autotuned thread mapping
-            e.set_mapping(*per_thread)
+        if per_thread:   # the main run's autotuned thread mapping, stage by stage
+            for st, m in enumerate(per_thread):
+                e.set_stage_mapping(st, *m)
     S = cfg["fct_steps"]
     main = torch.cuda.current_stream(dev)
     h2d = sum(h[k].numel() * 8 for h in host for k in ("T", "T_old", "uv", "w_e"))

@@ -169,7 +169,7 @@ int fct_batch_create(const FctInstance* insts, int n, int64_t budget, FctBatch**
     d.any_wi = false;
     d.copy_dry = false;
     d.per_thread = std::min(d.chunk, 2);
-    d.lpt = 4;
+    d.set_map(d.per_thread, 4);
     gr.dims = d;
   }
   e = cudaMalloc(&B->d_health, size_t(n) * sizeof(unsigned long long));
@@ -213,7 +213,7 @@ int fct_batch_set_mapping(FctBatch* B, int tracers_per_thread, int levels_per_th
   std::lock_guard<std::mutex> lk(B->graph_mu);
   for (auto& g : B->groups) {
     g.dims.per_thread = t;
-    g.dims.lpt = l;
+    g.dims.set_map(t, l);
   }
   for (auto& kv : B->graphs) cudaGraphExecDestroy(kv.second);   // recapture with the mapping
   B->graphs.clear();
@@ -222,8 +222,27 @@ int fct_batch_set_mapping(FctBatch* B, int tracers_per_thread, int levels_per_th
 
 int fct_batch_set_chunk(FctBatch* B, int chunk) {
   if (!B) return set_error(FCT_ERR_INVALID, "batch is NULL");
-  const int lpt = B->groups.empty() ? 4 : B->groups[0].dims.lpt;
+  const int lpt = B->groups.empty() ? 4 : B->groups[0].dims.smap_levels[0];
   return fct_batch_set_mapping(B, chunk, lpt);
+}
+
+int fct_batch_set_stage_mapping(FctBatch* B, int stage, int tracers_per_thread,
+                                int levels_per_thread) {
+  if (!B) return set_error(FCT_ERR_INVALID, "batch is NULL");
+  if (stage < 0 || stage >= kFusedStages)
+    return set_error(FCT_ERR_INVALID, "stage must be 0 (LO), 1 (edge), 2 (limiter) or 3 "
+                     "(final)");
+  const int t = tracers_per_thread, l = levels_per_thread;
+  if ((t != 1 && t != 2 && t != 4 && t != 8) || (l != 1 && l != 2 && l != 4 && l != 8))
+    return set_error(FCT_ERR_INVALID, "tracers and levels per thread must be 1, 2, 4 or 8");
+  std::lock_guard<std::mutex> lk(B->graph_mu);
+  for (auto& g : B->groups) {
+    g.dims.smap_tracers[stage] = t;
+    g.dims.smap_levels[stage] = l;
+  }
+  for (auto& kv : B->graphs) cudaGraphExecDestroy(kv.second);   // recapture with the mapping
+  B->graphs.clear();
+  return FCT_OK;
 }
 
 int fct_batch_info(const FctBatch* B, int64_t out[6]) {
@@ -535,7 +554,7 @@ int fct_serve_step(FctServe* S, const FctInstance* insts, const int32_t* phases,
     d.ntr = ntr;
     d.chunk = 0;
     d.per_thread = P0->per_thread;
-    d.lpt = P0->lpt;
+    d.set_map(P0->per_thread, P0->lpt);
     for (int j = j0; j < j1; ++j)
       if (insts[order[j]].w_derived) d.any_derive_w = true;
     d.any_wi = false;

@@ -46,6 +46,39 @@ __device__ __forceinline__ void ldn(const double* __restrict__ p, uint32_t q, in
   for (int i = 0; i < NTR; ++i) v[i] = __ldg(p + tix<IL>(q, t0 + i, stride, tg));
 }
 
+// ldn/stn for the segment kernels: in the interleaved layout with an even NTR the host
+// guarantees 16-byte alignment (even tracer strides and offsets, workspace fields on
+// 256-byte boundaries), so the tracer pairs load and store as double2 without a test.
+template <int NTR, bool IL>
+__device__ __forceinline__ void ldv(const double* __restrict__ p, uint32_t q, int t0,
+                                    int64_t stride, int tg, double (&v)[NTR]) {
+  if constexpr (IL && (NTR % 2 == 0)) {
+    const double2* b = reinterpret_cast<const double2*>(p + (q * uint32_t(tg) + uint32_t(t0)));
+#pragma unroll
+    for (int i = 0; i < NTR; i += 2) {
+      const double2 x = __ldg(b + i / 2);
+      v[i] = x.x;
+      v[i + 1] = x.y;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < NTR; ++i) v[i] = __ldg(p + tix<IL>(q, t0 + i, stride, tg));
+  }
+}
+
+template <int NTR, bool IL>
+__device__ __forceinline__ void stv(double* __restrict__ p, uint32_t q, int t0, int64_t stride,
+                                    int tg, const double (&v)[NTR]) {
+  if constexpr (IL && (NTR % 2 == 0)) {
+    double2* b = reinterpret_cast<double2*>(p + (q * uint32_t(tg) + uint32_t(t0)));
+#pragma unroll
+    for (int i = 0; i < NTR; i += 2) b[i / 2] = make_double2(v[i], v[i + 1]);
+  } else {
+#pragma unroll
+    for (int i = 0; i < NTR; ++i) p[tix<IL>(q, t0 + i, stride, tg)] = v[i];
+  }
+}
+
 template <int NTR, bool IL>
 __device__ __forceinline__ void stn(double* __restrict__ p, uint32_t q, int t0, int64_t stride,
                                     int tg, const double (&v)[NTR]) {

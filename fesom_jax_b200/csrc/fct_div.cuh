@@ -41,6 +41,11 @@ __device__ __forceinline__ Rcp rcp(double y) {
   return c;
 }
 
+// The native division for the operands the fast path does not take. Kept out of line so
+// that the compiler branches around it instead of evaluating it under a predicate at
+// every call site.
+static __device__ __noinline__ double div_slow(double x, double y) { return x / y; }
+
 // x / c.y, correctly rounded (IEEE round-to-nearest-even)
 __device__ __forceinline__ double divr(double x, const Rcp& c) {
   if (c.ok) {
@@ -51,7 +56,7 @@ __device__ __forceinline__ double divr(double x, const Rcp& c) {
       return fma(fma(-c.y, q1, x), c.r, q1);
     }
   }
-  return x / c.y;
+  return div_slow(x, c.y);
 }
 
 }  // namespace fct

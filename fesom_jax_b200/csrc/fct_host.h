@@ -25,6 +25,10 @@ inline int cuda_error(cudaError_t e, const char* what) {
     if (e_ != cudaSuccess) return ::fct::cuda_error(e_, #call); \
   } while (0)
 
+// fused stages with their own thread mapping: LO, edge, limiter, final
+constexpr int kFusedStages = 4;
+enum { kStageLo = 0, kStageEdge = 1, kStageLimit = 2, kStageFinal = 3 };
+
 // Launch the forward kernel sequence for ``n`` instances. ``single`` is used when
 // ``tab`` is null (n == 1), otherwise ``tab`` is a device array of ``n`` instances
 // whose lane counts are bounded by the ``max_*`` arguments.
@@ -40,9 +44,17 @@ struct LaunchDims {
   bool any_derive_w = false;  // derive w_e from uv (compute_w) before the step
   bool fused = true;  // fused stages (lean workspace); false: every stage kernel writes its
                       // intermediates (what the reverse pass reads)
-  // fused (segment) stages: levels per thread (1, 2, 4 or 8: a tuning knob) and the
-  // largest segment counts over the launch's instances
-  int lpt = 4;
+  // fused (segment) stages: per stage (LO, edge, limiter, final) the most tracers and the
+  // levels a thread takes (tuning knobs), and the largest segment counts over the launch's
+  // instances
+  int smap_tracers[kFusedStages] = {2, 2, 2, 2};
+  int smap_levels[kFusedStages] = {4, 4, 4, 4};
+  void set_map(int tracers, int levels) {
+    for (int i = 0; i < kFusedStages; ++i) {
+      smap_tracers[i] = tracers;
+      smap_levels[i] = levels;
+    }
+  }
   int64_t max_nseg[kSegVariants] = {0, 0, 0, 0};
   int64_t max_eseg[kSegVariants] = {0, 0, 0, 0};
   int64_t max_efix = 0;

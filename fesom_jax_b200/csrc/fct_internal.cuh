@@ -53,6 +53,11 @@ __device__ __forceinline__ void split_dense(int64_t i, int L, int& ent, int& k) 
 // node or edge (variant v), so the entity's neighbour lists and static data are decoded
 // once per run instead of once per level.
 constexpr int kSegVariants = 4;
+// node-layer flag words of the segment kernels (DevMesh::nflags)
+constexpr int kMaxSlots = 24;      // edges per node
+constexpr int kSlotWet = 24;       // bits 24..47: a cell of the slot's edge is wet
+constexpr int kOwnBit = 48;        // some cell of the node is wet at the level
+constexpr int kOffBit = 49;        // some cell of the node is dry at the level
 constexpr int kSegLevels[kSegVariants] = {1, 2, 4, 8};
 __host__ __device__ constexpr int seg_variant(int lpt) {
   return lpt == 1 ? 0 : lpt == 2 ? 1 : lpt == 4 ? 2 : 3;
@@ -122,7 +127,8 @@ struct DevMesh {
   const int4* ecell4;
   // segment kernels:
   //   nrec per node {first edge slot, first cell slot,
-  //                  nzmin | nzmax << 8 | edge count << 16 | cell count << 24, 0}
+  //                  nzmin | nzmax << 8 | edge count << 16 | cell count << 24,
+  //                  index of its first layer in nflags}
   //   erec per edge {n1, n2, lo | hi << 8, 0}: [lo, hi) the levels where MFCT takes the up
   //     and down cells' gradients and the up cell holds n1, the down cell n2 (else empty)
   //   nseg[v] node segments (node << 7 | first layer), runs of kSegLevels[v] layers
@@ -130,6 +136,9 @@ struct DevMesh {
   //   efix    the edge lanes outside [lo, hi) (node-average gradients, or a mesh whose
   //     up/down cells do not hold the edge's nodes)
   const int4* nrec;
+  const unsigned long long* nflags;   // per node layer, at nrec.w + (k - nzmin): bit j the
+                                      // slot's edge has level k, bit kSlotWet + j a cell of
+                                      // that edge is wet at k, kOwnBit / kOffBit
   const int4* erec;
   const uint32_t* nseg[kSegVariants];
   int64_t n_nseg[kSegVariants];

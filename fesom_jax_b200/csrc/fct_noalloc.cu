@@ -92,8 +92,7 @@ extern "C" int fct_forward_noalloc(FctPlan* P, const FctFields* f, double dt, in
   dims_cover(dims, P);
   dims.ntr = ntr;
   dims.chunk = 0;
-  dims.per_thread = P->per_thread;
-  dims.lpt = P->lpt;
+  dims.set_map(P->per_thread, P->lpt);
   dims.any_wi = f->w_i != nullptr;
   dims.copy_dry = true;
   return restore(launch_forward(in, nullptr, 1, dims, static_cast<cudaStream_t>(stream)));

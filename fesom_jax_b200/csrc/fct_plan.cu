@@ -77,14 +77,19 @@ int set_error(int status, const char* fmt, ...) {
   return status;
 }
 
+// Every workspace field starts on a 256-byte boundary (whole 32-double blocks), so the
+// segment kernels' double2 accesses are aligned.
+static int64_t pad32(int64_t n) { return (n + 31) & ~int64_t(31); }
+
 int64_t workspace_doubles(int64_t N, int64_t E, int64_t Ed, int64_t L, int ntr) {
-  const int64_t count_bytes = int64_t(ntr) * 2 * (N * L + E * L);
-  return Ed * L + N * L + int64_t(ntr) * (4 * E * L + 11 * N * L + Ed * L) +
-         (count_bytes + 7) / 8;
+  const int64_t t = ntr;
+  return pad32(Ed * L) + 4 * pad32(t * E * L) + 8 * pad32(t * N * L) + pad32(t * Ed * L) +
+         pad32(N * L) + 2 * pad32(t * N * L) + pad32((2 * t * (N * L + E * L) + 7) / 8);
 }
 
 int64_t workspace_doubles_fused(int64_t N, int64_t Ed, int64_t L, int ntr) {
-  return Ed * L + int64_t(ntr) * (kFusedNodeFields * N * L + Ed * L);
+  const int64_t t = ntr;
+  return pad32(Ed * L) + kFusedNodeFields * pad32(t * N * L) + pad32(t * Ed * L);
 }
 
 Workspace carve_workspace(double* base, int64_t N, int64_t E, int64_t Ed, int64_t L, int ntr,
@@ -94,7 +99,7 @@ Workspace carve_workspace(double* base, int64_t N, int64_t E, int64_t Ed, int64_
   w.sE = E * L;
   w.sEd = Ed * L;
   double* p = base;
-  auto take = [&](int64_t n) { double* q = p; p += n; return q; };
+  auto take = [&](int64_t n) { double* q = p; p += pad32(n); return q; };
   w.vflux = take(Ed * L);
   if (fused) {   // the fused stages keep no element fields, node gradients or cluster bounds
     w.lo = take(ntr * w.sN);
@@ -398,13 +403,41 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   // consecutive layers of a node, runs of consecutive MFCT up/down-cell levels of an edge
   // (those whose up cell holds the edge's first node and whose down cell its second), and
   // the remaining edge lanes
+  // and, per node layer, the flags of the node's edge slots at that level: bit j (slot j
+  // has the level: its flux is counted), bit kSlotWet + j (a cell of slot j is wet there),
+  // kOwnBit (some cell of the node is wet) and kOffBit (some cell of the node is dry)
   std::vector<int4> nrec(static_cast<size_t>(N));
+  std::vector<unsigned long long> nflags;
   for (int n = 0; n < N; ++n) {
     const int ed = ne_off[n + 1] - ne_off[n];
     const int cd = d->nod_in_elem2D_offsets[n + 1] - d->nod_in_elem2D_offsets[n];
+    if (ed > kMaxSlots)
+      return set_error(FCT_ERR_INVALID, "node %d has %d edges; at most %d are supported", n,
+                       ed, kMaxSlots);
     nrec[n] = make_int4(ne_off[n], d->nod_in_elem2D_offsets[n],
                         int(unsigned(nzmin[n]) | (unsigned(nzmax[n]) << 8) |
-                            (unsigned(ed) << 16) | (unsigned(cd) << 24)), 0);
+                            (unsigned(ed) << 16) | (unsigned(cd) << 24)),
+                        int(nflags.size()));
+    for (int k = std::max(nzmin[n], 0); k < std::min(nzmax[n], L); ++k) {
+      unsigned long long f = 0;
+      bool own = false, off = false;
+      for (int j = ne_off[n]; j < ne_off[n + 1]; ++j) {
+        const int4 sl = ne4[j];
+        const unsigned rg = unsigned(sl.z), tr = unsigned(sl.w);
+        const bool on = k >= int(rg & 255u) && k < int((rg >> 8) & 255u);
+        const bool has2 = ((tr >> 16) & 255u) != kNoCell;
+        const bool c1 = k >= int(tr & 255u) && k < int((tr >> 8) & 255u);
+        const bool c2 = has2 && k >= int((tr >> 16) & 255u) && k < int((tr >> 24) & 255u);
+        const int jj = j - ne_off[n];
+        f |= (unsigned long long)(on) << jj;
+        f |= (unsigned long long)(c1 || c2) << (kSlotWet + jj);
+        own = own || c1 || c2;
+        off = off || !c1 || (has2 && !c2);
+      }
+      f |= (unsigned long long)(own) << kOwnBit;
+      f |= (unsigned long long)(off) << kOffBit;
+      nflags.push_back(f);
+    }
   }
   std::vector<int4> erec(static_cast<size_t>(Ed));
   std::vector<uint32_t> efix;
@@ -466,6 +499,7 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   size_t o_eud4 = b.add(eud4.data(), eud4.size());
   size_t o_ecell4 = b.add(ecell4.data(), ecell4.size());
   size_t o_nrec = b.add(nrec.data(), nrec.size()), o_erec = b.add(erec.data(), erec.size());
+  size_t o_nflags = b.add(nflags.data(), std::max<size_t>(nflags.size(), 1));
   size_t o_efix = b.add(efix.data(), std::max<size_t>(efix.size(), 1));
   size_t o_nseg[kSegVariants], o_eseg[kSegVariants];
   for (int v = 0; v < kSegVariants; ++v) {
@@ -521,6 +555,7 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   m.eud4 = (const int4*)(base + o_eud4);
   m.ecell4 = (const int4*)(base + o_ecell4);
   m.nrec = (const int4*)(base + o_nrec);
+  m.nflags = (const unsigned long long*)(base + o_nflags);
   m.erec = (const int4*)(base + o_erec);
   m.efix = (const uint32_t*)(base + o_efix);
   m.n_efix = int64_t(efix.size());
@@ -693,8 +728,7 @@ int fct_forward(FctPlan* P, const FctFields* f, double dt, int ntr, fct_stream_t
   dims_cover(dims, P);
   dims.ntr = ntr;
   dims.chunk = 0;       // one workspace chunk: all ntr tracers
-  dims.per_thread = P->per_thread;
-  dims.lpt = P->lpt;
+  dims.set_map(P->per_thread, P->lpt);
   dims.any_wi = f->w_i != nullptr;
   dims.copy_dry = true;   // a fresh T_new: dry levels keep T (tracer_adv.py:147-151)
   dims.fused = P->fused;

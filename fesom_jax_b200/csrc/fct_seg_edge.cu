@@ -28,7 +28,7 @@ int launch_edge_fix(const Inst& single, const Inst* tab, int n, const LaunchDims
   if (d.max_efix == 0) return FCT_OK;
   for (int t0 = c0; t0 < c1;) {
     const int rem = c1 - t0;
-    const int P = seg_tracers(rem, d.per_thread, tab != nullptr, 1);
+    const int P = seg_tracers(rem, d.smap_tracers[kStageEdge], tab != nullptr, 1, seg_even(d));
     int lg = 0;
     while (lg < 3 && (P << (lg + 1)) <= rem) ++lg;
     const int w0 = t0 - c0;
@@ -51,7 +51,7 @@ int launch_edge_fix(const Inst& single, const Inst* tab, int n, const LaunchDims
 namespace {
 
 #define FCT_COUNT(V) d.max_eseg[V]
-FCT_SEG_LAUNCHER(launch_impl, k_seg_edge, FCT_COUNT, FCT_GRID_N, FCT_GRID_1)
+FCT_SEG_LAUNCHER(launch_impl, k_seg_edge, FCT_COUNT, FCT_GRID_N, FCT_GRID_1, kStageEdge)
 #undef FCT_COUNT
 
 }  // namespace

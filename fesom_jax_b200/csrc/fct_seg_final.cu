@@ -8,7 +8,7 @@ namespace {
 FCT_SEG_KERNEL(k_seg_final, seg_node_final)
 
 #define FCT_COUNT(V) d.max_nseg[V]
-FCT_SEG_LAUNCHER(launch_impl, k_seg_final, FCT_COUNT, FCT_GRID_N, FCT_GRID_1)
+FCT_SEG_LAUNCHER(launch_impl, k_seg_final, FCT_COUNT, FCT_GRID_N, FCT_GRID_1, kStageFinal)
 #undef FCT_COUNT
 
 }  // namespace

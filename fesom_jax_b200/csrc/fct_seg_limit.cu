@@ -8,7 +8,7 @@ namespace {
 FCT_SEG_LIMIT_KERNEL(k_seg_limit)
 
 #define FCT_COUNT(V) d.max_nseg[V]
-FCT_SEG_LAUNCHER(launch_impl, k_seg_limit, FCT_COUNT, FCT_LIMIT_GRID_N, FCT_LIMIT_GRID_1)
+FCT_SEG_LAUNCHER(launch_impl, k_seg_limit, FCT_COUNT, FCT_LIMIT_GRID_N, FCT_LIMIT_GRID_1, kStageLimit)
 #undef FCT_COUNT
 
 }  // namespace

@@ -8,7 +8,7 @@ namespace {
 FCT_SEG_KERNEL(k_seg_lo, seg_node_lo)
 
 #define FCT_COUNT(V) d.max_nseg[V]
-FCT_SEG_LAUNCHER(launch_impl, k_seg_lo, FCT_COUNT, FCT_GRID_N, FCT_GRID_1)
+FCT_SEG_LAUNCHER(launch_impl, k_seg_lo, FCT_COUNT, FCT_GRID_N, FCT_GRID_1, kStageLo)
 #undef FCT_COUNT
 
 }  // namespace

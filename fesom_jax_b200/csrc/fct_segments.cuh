@@ -57,7 +57,7 @@ __device__ __forceinline__ void seg_node_lo(const Inst& in, int64_t si, int t0, 
   double Tw[LPT + 3][NTR];
 #pragma unroll
   for (int i = 0; i < LPT + 3; ++i)
-    ldn<NTR, IL>(in.T, base + uint32_t(kclamp(k0 - 2 + i, L)), t0, ts, tg, Tw[i]);
+    ldv<NTR, IL>(in.T, base + uint32_t(kclamp(k0 - 2 + i, L)), t0, ts, tg, Tw[i]);
 
   // compute_fct_lo: edge->node upwind divergence in ascending edge id
   double div[LPT][NTR];
@@ -65,26 +65,31 @@ __device__ __forceinline__ void seg_node_lo(const Inst& in, int64_t si, int t0, 
   for (int l = 0; l < LPT; ++l)
 #pragma unroll
     for (int t = 0; t < NTR; ++t) div[l][t] = 0.0;
+  unsigned long long fl_[LPT];   // the run's node-layer flags (0 beyond the run)
+#pragma unroll
+  for (int l = 0; l < LPT; ++l) fl_[l] = l < nk ? __ldg(m.nflags + rec.w + (k0 + l - nzmin)) : 0ull;
   const int e0 = rec.x, e1 = rec.x + int((pk >> 16) & 255u);
   for (int j = e0; j < e1; ++j) {
     const int4 sl = __ldg(m.ne4 + j);
-    const unsigned rg = unsigned(sl.z);
+    const int jj = j - e0;
     const bool second = sl.x & 1;
+    const double sg1 = second ? -1.0 : 1.0;   // the flux leaves the edge's first node
     const uint32_t qe = lq(sl.x >> 1, L, 0), qo = lq(sl.y, L, 0);
 #pragma unroll
     for (int l = 0; l < LPT; ++l) {
-      const int k = k0 + l, kc = kclamp(k, L);
-      const bool on = l < nk && in_range(k, rg);
+      const int kc = kclamp(k0 + l, L);
+      const bool on = (fl_[l] >> jj) & 1ull;
       const double vf = __ldg(in.ws.vflux + qe + kc);
       const double avf = fabs(vf);
+      // the reference's face flux -0.5*(T1*(vf+|vf|) + T2*(vf-|vf|)) with the node's own
+      // value first (a + b == b + a exactly): the same bits for either end of the edge
+      const double cown = second ? vf - avf : vf + avf, coth = second ? vf + avf : vf - avf;
       double To[NTR];
-      ldn<NTR, IL>(in.T, qo + uint32_t(kc), t0, ts, tg, To);
+      ldv<NTR, IL>(in.T, qo + uint32_t(kc), t0, ts, tg, To);
 #pragma unroll
       for (int t = 0; t < NTR; ++t) {
-        const double Tc = Tw[l + 2][t];
-        const double T1 = second ? To[t] : Tc, T2 = second ? Tc : To[t];
-        const double fl = -0.5 * (T1 * (vf + avf) + T2 * (vf - avf));
-        div[l][t] = on ? div[l][t] + (second ? -fl : fl) : div[l][t];
+        const double f = -0.5 * (Tw[l + 2][t] * cown + To[t] * coth);
+        div[l][t] = on ? div[l][t] + sg1 * f : div[l][t];
       }
     }
   }
@@ -115,14 +120,14 @@ __device__ __forceinline__ void seg_node_lo(const Inst& in, int64_t si, int t0, 
       lo[t] = valid ? divr(Tw[l + 2][t] * hn +
                                divr((div[l][t] + (fv[l][t] - fv[l + 1][t])) * dt, rav), rhn)
                     : 0.0;
-    stn<NTR, IL>(in.ws.lo, qn, w0, in.ws.sN, in.wtg, lo);
+    stv<NTR, IL>(in.ws.lo, qn, w0, in.ws.sN, in.wtg, lo);
   }
 
   // adv_flux_ver_ho (QR4C on ttfAB) minus the LO vertical flux at the layer tops
   double To[LPT + 3][NTR];   // T_old at levels k0-2 .. k0+LPT
 #pragma unroll
   for (int i = 0; i < LPT + 3; ++i)
-    ldn<NTR, IL>(in.T_old, base + uint32_t(kclamp(k0 - 2 + i, L)), t0, ts, tg, To[i]);
+    ldv<NTR, IL>(in.T_old, base + uint32_t(kclamp(k0 - 2 + i, L)), t0, ts, tg, To[i]);
 #pragma unroll
   for (int l = 0; l < LPT; ++l) {
     if (l >= nk) break;
@@ -173,7 +178,7 @@ __device__ __forceinline__ void seg_node_lo(const Inst& in, int64_t si, int t0, 
       const double lo_v = in.w_i ? vflux_up(Tw[l + 2][t], Tw[l + 1][t], Wf, area_k) : fv[l][t];
       adf[t] = hi[t] - lo_v;
     }
-    stn<NTR, IL>(in.ws.adfv, qn, w0, in.ws.sN, in.wtg, adf);
+    stv<NTR, IL>(in.ws.adfv, qn, w0, in.ws.sN, in.wtg, adf);
   }
 }
 
@@ -206,17 +211,17 @@ __device__ __forceinline__ void seg_edge_adf(const Inst& in, int64_t si, int t0,
     const double vf = __ldg(in.ws.vflux + qe + kc);
     const double avf = fabs(vf);
     double T1[NTR], T2[NTR], O1[NTR], O2[NTR];
-    ldn<NTR, IL>(in.T, q1 + kc, t0, ts, tg, T1);
-    ldn<NTR, IL>(in.T, q2 + kc, t0, ts, tg, T2);
-    ldn<NTR, IL>(in.T_old, q1 + kc, t0, ts, tg, O1);
-    ldn<NTR, IL>(in.T_old, q2 + kc, t0, ts, tg, O2);
+    ldv<NTR, IL>(in.T, q1 + kc, t0, ts, tg, T1);
+    ldv<NTR, IL>(in.T, q2 + kc, t0, ts, tg, T2);
+    ldv<NTR, IL>(in.T_old, q1 + kc, t0, ts, tg, O1);
+    ldv<NTR, IL>(in.T_old, q2 + kc, t0, ts, tg, O2);
     double a0[NTR], a1[NTR], a2[NTR], b0[NTR], b1[NTR], b2[NTR];
-    ldn<NTR, IL>(in.T, qu0 + kc, t0, ts, tg, a0);
-    ldn<NTR, IL>(in.T, qu1 + kc, t0, ts, tg, a1);
-    ldn<NTR, IL>(in.T, qu2 + kc, t0, ts, tg, a2);
-    ldn<NTR, IL>(in.T, qd0 + kc, t0, ts, tg, b0);
-    ldn<NTR, IL>(in.T, qd1 + kc, t0, ts, tg, b1);
-    ldn<NTR, IL>(in.T, qd2 + kc, t0, ts, tg, b2);
+    ldv<NTR, IL>(in.T, qu0 + kc, t0, ts, tg, a0);
+    ldv<NTR, IL>(in.T, qu1 + kc, t0, ts, tg, a1);
+    ldv<NTR, IL>(in.T, qu2 + kc, t0, ts, tg, a2);
+    ldv<NTR, IL>(in.T, qd0 + kc, t0, ts, tg, b0);
+    ldv<NTR, IL>(in.T, qd1 + kc, t0, ts, tg, b1);
+    ldv<NTR, IL>(in.T, qd2 + kc, t0, ts, tg, b2);
     double adf[NTR];
 #pragma unroll
     for (int t = 0; t < NTR; ++t) {
@@ -233,7 +238,7 @@ __device__ __forceinline__ void seg_edge_adf(const Inst& in, int64_t si, int t0,
       const double ho = -0.5 * ((vf + avf) * Tm1 + (vf - avf) * Tm2);
       adf[t] = ho - fl;
     }
-    if (l < nk) stn<NTR, IL>(in.ws.adfh, qe + uint32_t(kc), w0, in.ws.sEd, in.wtg, adf);
+    if (l < nk) stv<NTR, IL>(in.ws.adfh, qe + uint32_t(kc), w0, in.ws.sEd, in.wtg, adf);
   }
 }
 
@@ -354,32 +359,30 @@ __device__ __forceinline__ void seg_node_limit(const Inst& in, int64_t si, bool 
     nzmax = int((pk >> 8) & 255u);
     nk = min(LPT, nzmax - k0);
     base = lq(n, L, 0);
-    unsigned own = 0u, off = 0u;   // bit l: a cell of n is wet / dry at level k0+l
+    unsigned long long fl_[LPT];   // the run's node-layer flags (0 beyond the run)
+#pragma unroll
+    for (int l = 0; l < LPT; ++l)
+      fl_[l] = l < nk ? __ldg(m.nflags + rec.w + (k0 + l - nzmin)) : 0ull;
     const int e0 = rec.x, e1 = rec.x + int((pk >> 16) & 255u);
     for (int j = e0; j < e1; ++j) {
       const int4 sl = __ldg(m.ne4 + j);
-      const unsigned tr = unsigned(sl.w), rg = unsigned(sl.z);
-      const bool has2 = ((tr >> 16) & 255u) != kNoCell;
-      const bool second = sl.x & 1;
+      const int jj = j - e0;
+      const double sg1 = (sl.x & 1) ? -1.0 : 1.0;   // adf_h leaves the edge's first node
       const uint32_t qo = lq(sl.y, L, 0), qe = lq(sl.x >> 1, L, 0);
 #pragma unroll
       for (int l = 0; l < LPT; ++l) {
-        const int k = k0 + l, kc = kclamp(k, L);
-        const bool c1 = in_range(k, tr & 0xffffu);
-        const bool c2 = has2 && in_range(k, tr >> 16);
-        const bool wet = c1 || c2;
-        own |= unsigned(wet) << l;
-        off |= unsigned(!c1 || (has2 && !c2)) << l;
-        const bool on = l < nk && in_range(k, rg);
+        const int kc = kclamp(k0 + l, L);
+        const bool wet = (fl_[l] >> (kSlotWet + jj)) & 1ull;
+        const bool on = (fl_[l] >> jj) & 1ull;
         double lv[NTR], tv[NTR], a[NTR];
-        ldn<NTR, IL>(in.ws.lo, qo + uint32_t(kc), w0, sN, in.wtg, lv);
-        ldn<NTR, IL>(in.T, qo + uint32_t(kc), t0, in.tstride, in.tg, tv);
-        ldn<NTR, IL>(in.ws.adfh, qe + uint32_t(kc), w0, in.ws.sEd, in.wtg, a);
+        ldv<NTR, IL>(in.ws.lo, qo + uint32_t(kc), w0, sN, in.wtg, lv);
+        ldv<NTR, IL>(in.T, qo + uint32_t(kc), t0, in.tstride, in.tg, tv);
+        ldv<NTR, IL>(in.ws.adfh, qe + uint32_t(kc), w0, in.ws.sEd, in.wtg, a);
 #pragma unroll
         for (int t = 0; t < NTR; ++t) {
           mx[l][t] = wet ? fmax(mx[l][t], fmax(lv[t], tv[t])) : mx[l][t];
           mn[l][t] = wet ? fmin(mn[l][t], fmin(lv[t], tv[t])) : mn[l][t];
-          const double sv = second ? -a[t] : a[t];
+          const double sv = sg1 * a[t];
           sp[l][t] = on ? sp[l][t] + fmax(sv, 0.0) : sp[l][t];
           sm[l][t] = on ? sm[l][t] + fmin(sv, 0.0) : sm[l][t];
         }
@@ -390,9 +393,9 @@ __device__ __forceinline__ void seg_node_limit(const Inst& in, int64_t si, bool 
     for (int l = 0; l < LPT; ++l) {
       const int kc = kclamp(k0 + l, L);
       double tv[NTR];
-      ldn<NTR, IL>(in.ws.lo, base + uint32_t(kc), w0, sN, in.wtg, lo[l]);
-      ldn<NTR, IL>(in.T, base + uint32_t(kc), t0, in.tstride, in.tg, tv);
-      const bool ow = (own >> l) & 1u, of = (off >> l) & 1u;
+      ldv<NTR, IL>(in.ws.lo, base + uint32_t(kc), w0, sN, in.wtg, lo[l]);
+      ldv<NTR, IL>(in.T, base + uint32_t(kc), t0, in.tstride, in.tg, tv);
+      const bool ow = (fl_[l] >> kOwnBit) & 1ull, of = (fl_[l] >> kOffBit) & 1ull;
 #pragma unroll
       for (int t = 0; t < NTR; ++t) {
         if (ow) {
@@ -434,9 +437,9 @@ __device__ __forceinline__ void seg_node_limit(const Inst& in, int64_t si, bool 
     const double sa = av > 0.0 ? av : 1.0, sh_ = hnn > 0.0 ? hnn : 1.0;
     const Rcp rsa = rcp(sa), rsh = rcp(sh_);
     double ft[NTR], fb[NTR];
-    ldn<NTR, IL>(in.ws.adfv, qn, w0, sN, in.wtg, ft);
+    ldv<NTR, IL>(in.ws.adfv, qn, w0, sN, in.wtg, ft);
     if (k + 1 < nzmax) {
-      ldn<NTR, IL>(in.ws.adfv, qn + 1, w0, sN, in.wtg, fb);
+      ldv<NTR, IL>(in.ws.adfv, qn + 1, w0, sN, in.wtg, fb);
     } else {   // the bottom interface carries no flux
 #pragma unroll
       for (int t = 0; t < NTR; ++t) fb[t] = 0.0;
@@ -462,12 +465,13 @@ __device__ __forceinline__ void seg_node_limit(const Inst& in, int64_t si, bool 
       if (valid_n) {
         const double flux_pos = divr(divr(plus * dt, rsa), rsh) + kFluxEps;
         const double flux_neg = divr(divr(minus * dt, rsa), rsh) - kFluxEps;
-        pf[t] = fmin(1.0, (wmx - lo[l][t]) / flux_pos);
-        mf[t] = fmin(1.0, (wmn - lo[l][t]) / flux_neg);
+        // correctly rounded quotients (the same bits as '/')
+        pf[t] = fmin(1.0, divr(wmx - lo[l][t], rcp(flux_pos)));
+        mf[t] = fmin(1.0, divr(wmn - lo[l][t], rcp(flux_neg)));
       }
     }
-    stn<NTR, IL>(in.ws.pf, qn, w0, sN, in.wtg, pf);
-    stn<NTR, IL>(in.ws.mf, qn, w0, sN, in.wtg, mf);
+    stv<NTR, IL>(in.ws.pf, qn, w0, sN, in.wtg, pf);
+    stv<NTR, IL>(in.ws.mf, qn, w0, sN, in.wtg, mf);
   }
 }
 
@@ -497,31 +501,36 @@ __device__ __forceinline__ void seg_node_final(const Inst& in, int64_t si, int t
 #pragma unroll
   for (int b = 0; b < NB; ++b) {
     const uint32_t q = base + uint32_t(kclamp(k0 - 1 + b, L));
-    ldn<NTR, IL>(in.ws.pf, q, w0, sN, in.wtg, pfw[b]);
-    ldn<NTR, IL>(in.ws.mf, q, w0, sN, in.wtg, mfw[b]);
+    ldv<NTR, IL>(in.ws.pf, q, w0, sN, in.wtg, pfw[b]);
+    ldv<NTR, IL>(in.ws.mf, q, w0, sN, in.wtg, mfw[b]);
   }
+  unsigned long long fl_[LPT];   // the run's node-layer flags (0 beyond the run)
+#pragma unroll
+  for (int l = 0; l < LPT; ++l) fl_[l] = l < nk ? __ldg(m.nflags + rec.w + (k0 + l - nzmin)) : 0ull;
   const int e0 = rec.x, e1 = rec.x + int((pk >> 16) & 255u);
   for (int j = e0; j < e1; ++j) {
     const int4 sl = __ldg(m.ne4 + j);
-    const unsigned rg = unsigned(sl.z);
+    const int jj = j - e0;
     const bool second = sl.x & 1;
+    const double sg1 = second ? -1.0 : 1.0;   // adf_h leaves the edge's first node
     const uint32_t qo = lq(sl.y, L, 0), qe = lq(sl.x >> 1, L, 0);
 #pragma unroll
     for (int l = 0; l < LPT; ++l) {
-      const int k = k0 + l, kc = kclamp(k, L);
-      const bool on = l < nk && in_range(k, rg);
+      const int kc = kclamp(k0 + l, L);
+      const bool on = (fl_[l] >> jj) & 1ull;
       double a[NTR], pfo[NTR], mfo[NTR];
-      ldn<NTR, IL>(in.ws.adfh, qe + uint32_t(kc), w0, in.ws.sEd, in.wtg, a);
-      ldn<NTR, IL>(in.ws.pf, qo + uint32_t(kc), w0, sN, in.wtg, pfo);
-      ldn<NTR, IL>(in.ws.mf, qo + uint32_t(kc), w0, sN, in.wtg, mfo);
+      ldv<NTR, IL>(in.ws.adfh, qe + uint32_t(kc), w0, in.ws.sEd, in.wtg, a);
+      ldv<NTR, IL>(in.ws.pf, qo + uint32_t(kc), w0, sN, in.wtg, pfo);
+      ldv<NTR, IL>(in.ws.mf, qo + uint32_t(kc), w0, sN, in.wtg, mfo);
 #pragma unroll
       for (int t = 0; t < NTR; ++t) {
-        const double pf0 = pfw[l + 1][t], mf0 = mfw[l + 1][t];
-        const double pf1 = second ? pfo[t] : pf0, mf1 = second ? mfo[t] : mf0;
-        const double pf2 = second ? pf0 : pfo[t], mf2 = second ? mf0 : mfo[t];
-        const double ae = a[t] >= 0.0 ? fmin(pf1, mf2) : fmin(mf1, pf2);
+        // b3 (tracer_adv.py:461-465): adf >= 0 ? min(plus(n1), minus(n2)) : min(minus(n1),
+        // plus(n2)); min is exact and symmetric, so in the node's own terms the factor is
+        // min(own plus, other minus) when the flux leaves the node, else the other pair
+        const double x1 = fmin(pfw[l + 1][t], mfo[t]), x2 = fmin(mfw[l + 1][t], pfo[t]);
+        const double ae = ((a[t] >= 0.0) != second) ? x1 : x2;
         const double lim = ae * a[t];
-        hsc[l][t] = on ? hsc[l][t] + (second ? -lim : lim) : hsc[l][t];
+        hsc[l][t] = on ? hsc[l][t] + sg1 * lim : hsc[l][t];
       }
     }
   }
@@ -536,7 +545,7 @@ __device__ __forceinline__ void seg_node_final(const Inst& in, int64_t si, int t
     const double hn = __ldg(in.hnode + qn), hnn = __ldg(in.hnode_new + qn);
     const Rcp rsa = rcp(sa), rhn = rcp(hnn);
     double ft[NTR], vt[NTR], vb[NTR];
-    ldn<NTR, IL>(in.ws.adfv, qn, w0, sN, in.wtg, ft);
+    ldv<NTR, IL>(in.ws.adfv, qn, w0, sN, in.wtg, ft);
     // limited vertical flux at the top interface k (tracer_adv.py:453-459)
 #pragma unroll
     for (int t = 0; t < NTR; ++t) {
@@ -550,15 +559,15 @@ __device__ __forceinline__ void seg_node_final(const Inst& in, int64_t si, int t
       for (int t = 0; t < NTR; ++t) vb[t] = 0.0;
     } else {
       double fb[NTR];
-      ldn<NTR, IL>(in.ws.adfv, qn + 1, w0, sN, in.wtg, fb);
+      ldv<NTR, IL>(in.ws.adfv, qn + 1, w0, sN, in.wtg, fb);
 #pragma unroll
       for (int t = 0; t < NTR; ++t)
         vb[t] = (fb[t] >= 0.0 ? fmin(mfw[l + 1][t], pfw[l + 2][t])
                               : fmin(pfw[l + 1][t], mfw[l + 2][t])) * fb[t];
     }
     double Tv[NTR], lo[NTR], out[NTR];
-    ldn<NTR, IL>(in.T, qn, t0, in.tstride, tg, Tv);
-    ldn<NTR, IL>(in.ws.lo, qn, w0, sN, in.wtg, lo);
+    ldv<NTR, IL>(in.T, qn, t0, in.tstride, tg, Tv);
+    ldv<NTR, IL>(in.ws.lo, qn, w0, sN, in.wtg, lo);
 #pragma unroll
     for (int t = 0; t < NTR; ++t) {
       const double lo_trans = -Tv[t] * hn + lo[t] * hnn;
@@ -567,7 +576,7 @@ __device__ __forceinline__ void seg_node_final(const Inst& in, int64_t si, int t
       d = d + Tv[t] * (hn - hnn);
       out[t] = Tv[t] + (hnn > 0.0 ? divr(d, rhn) : 0.0);
     }
-    stn<NTR, IL>(in.T_new, qn, t0, in.tstride, tg, out);
+    stv<NTR, IL>(in.T_new, qn, t0, in.tstride, tg, out);
     count_nonfinite<NTR>(in.nonfinite, out);
   }
 }
@@ -635,12 +644,19 @@ inline unsigned seg_blocks(int64_t lanes) {
 #define FCT_LIMIT_GRID_1(lanes) unsigned(std::max<int64_t>(1, ((lanes) + 253) / 254))
 
 // Tracers per thread of one launch: the largest of the compiled set (1, 2 or 4 in the
-// interleaved layout; 1 or 2 tracer-major) that is at most ``rem`` and ``per_thread``.
-inline int seg_tracers(int rem, int per_thread, bool interleaved, int lpt) {
+// interleaved layout, 1 when its strides are odd; 1 or 2 tracer-major) that is at most
+// ``rem`` and ``per_thread``.
+inline int seg_tracers(int rem, int per_thread, bool interleaved, int lpt, bool even) {
   (void)lpt;
   const int lim = std::min(rem, per_thread);
+  if (interleaved && !even) return 1;   // tracer pairs would not be 16-byte aligned
   if (interleaved && lim >= 4) return 4;
   return lim >= 2 ? 2 : 1;
+}
+// the interleaved tracer and workspace strides are even (tracer pairs 16-byte aligned)
+inline bool seg_even(const LaunchDims& d) {
+  const int chunk = d.chunk > 0 ? d.chunk : d.ntr;
+  return d.ntr % 2 == 0 && chunk % 2 == 0;
 }
 
 #define FCT_SEG_CASE_N(kern, P, V)                                                       \
@@ -655,20 +671,21 @@ inline int seg_tracers(int rem, int per_thread, bool interleaved, int lpt) {
 // One segment stage over the tracers [c0, c1) of a workspace chunk (workspace index of
 // tracer t is t - c0): launches of P tracers x 2^lg slices. ``COUNT(V)`` is the largest
 // segment count of the variant over the launch's instances.
-#define FCT_SEG_LAUNCHER(fn, kern, COUNT, GRID_N, GRID_1)                                \
+#define FCT_SEG_LAUNCHER(fn, kern, COUNT, GRID_N, GRID_1, STAGE)                         \
   int fn(const Inst& single, const Inst* tab, int n, const LaunchDims& d, int c0, int c1, \
          cudaStream_t s) {                                                               \
-    const int V = seg_variant(d.lpt);                                                    \
+    const int lpt = d.smap_levels[STAGE], per_thread = d.smap_tracers[STAGE];            \
+    const int V = seg_variant(lpt);                                                      \
     const int64_t lanes = COUNT(V);                                                      \
     for (int t0 = c0; t0 < c1;) {                                                        \
       const int rem = c1 - t0;                                                           \
-      const int P = seg_tracers(rem, d.per_thread, tab != nullptr, d.lpt);               \
+      const int P = seg_tracers(rem, per_thread, tab != nullptr, lpt, seg_even(d));      \
       int lg = 0;                                                                        \
       while (lg < 3 && (P << (lg + 1)) <= rem) ++lg;                                     \
       const int w0 = t0 - c0;                                                            \
       if (tab) {                                                                         \
         const dim3 g(GRID_N(lanes, lg), unsigned(n));                                    \
-        switch (P * 16 + d.lpt) {                                                        \
+        switch (P * 16 + lpt) {                                                          \
           FCT_SEG_CASE_N(kern, 1, 1) FCT_SEG_CASE_N(kern, 1, 2)                          \
           FCT_SEG_CASE_N(kern, 1, 4) FCT_SEG_CASE_N(kern, 1, 8)                          \
           FCT_SEG_CASE_N(kern, 2, 1) FCT_SEG_CASE_N(kern, 2, 2)                          \
@@ -677,18 +694,18 @@ inline int seg_tracers(int rem, int per_thread, bool interleaved, int lpt) {
           FCT_SEG_CASE_N(kern, 4, 4) FCT_SEG_CASE_N(kern, 4, 8)                          \
           default:                                                                       \
             return set_error(FCT_ERR_INVALID, "no segment kernel for %d tracers x %d "  \
-                             "levels per thread", P, d.lpt);                            \
+                             "levels per thread", P, lpt);                              \
         }                                                                                \
       } else {                                                                           \
         const dim3 g(GRID_1(lanes), 1u << lg);                                           \
-        switch (P * 16 + d.lpt) {                                                        \
+        switch (P * 16 + lpt) {                                                          \
           FCT_SEG_CASE_1(kern, 1, 1) FCT_SEG_CASE_1(kern, 1, 2)                          \
           FCT_SEG_CASE_1(kern, 1, 4) FCT_SEG_CASE_1(kern, 1, 8)                          \
           FCT_SEG_CASE_1(kern, 2, 1) FCT_SEG_CASE_1(kern, 2, 2)                          \
           FCT_SEG_CASE_1(kern, 2, 4) FCT_SEG_CASE_1(kern, 2, 8)                          \
           default:                                                                       \
             return set_error(FCT_ERR_INVALID, "no segment kernel for %d tracers x %d "  \
-                             "levels per thread", P, d.lpt);                            \
+                             "levels per thread", P, lpt);                              \
         }                                                                                \
       }                                                                                  \
       t0 += P << lg;                                                                     \

@@ -52,11 +52,13 @@ def _bind_batch(L):
     L.fct_stage_name.restype = C.c_char_p
     L.fct_batch_set_chunk.argtypes = [C.c_void_p, C.c_int]
     L.fct_batch_set_mapping.argtypes = [C.c_void_p, C.c_int, C.c_int]
+    L.fct_batch_set_stage_mapping.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
     L.fct_batch_health.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_int64)]
     L.fct_batch_fill_workspace.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
     for n in ("fct_batch_create", "fct_batch_destroy", "fct_batch_info", "fct_batch_prepare",
               "fct_batch_step", "fct_batch_run", "fct_batch_profile", "fct_batch_set_chunk",
-              "fct_batch_health", "fct_batch_fill_workspace", "fct_batch_set_mapping"):
+              "fct_batch_health", "fct_batch_fill_workspace", "fct_batch_set_mapping",
+              "fct_batch_set_stage_mapping"):
         getattr(L, n).restype = C.c_int
     L._batch_bound = True
     return L
@@ -92,6 +94,7 @@ class Ensemble:
         self.phase = 0
         self.chunk = 2          # tracers per thread of the fused stages
         self.levels = 4         # levels per thread
+        self.stage_map = [(2, 4)] * 4   # per fused stage (LO, edge, limiter, final)
 
     # ---------------------------------------------------------------- members
     def plan(self, mesh: Mesh) -> FctPlan:
@@ -211,33 +214,59 @@ class Ensemble:
         _lib.check(_bind_batch(_lib.lib()).fct_batch_set_mapping(
             self._h, int(tracers_per_thread), int(levels_per_thread)))
         self.chunk, self.levels = int(tracers_per_thread), int(levels_per_thread)
+        self.stage_map = [(self.chunk, self.levels)] * 4
+
+    def set_stage_mapping(self, stage: int, tracers_per_thread: int,
+                          levels_per_thread: int) -> None:
+        """The mapping of one fused stage (0 LO, 1 edge, 2 limiter, 3 final)."""
+        _lib.check(_bind_batch(_lib.lib()).fct_batch_set_stage_mapping(
+            self._h, int(stage), int(tracers_per_thread), int(levels_per_thread)))
+        self.stage_map[int(stage)] = (int(tracers_per_thread), int(levels_per_thread))
 
     # (tracers per thread, levels per thread) tried by autotune
     MAPPINGS = ((1, 1), (1, 2), (1, 4), (1, 8), (2, 1), (2, 2), (2, 4), (4, 1), (4, 2))
+    # the fused stages as profile_step names them, in mapping order
+    STAGES = ("node_lo", "edge_adf", "node_factors", "node_final")
 
-    def autotune(self, steps: int = 2, candidates=None, reps: int = 2) -> dict:
-        """Time ``steps``-step graph runs for each (tracers, levels) per-thread mapping (the
-        member state advances while tuning) and keep the fastest; returns
-        ``{"TxL": ms}``."""
+    def _graph_ms(self, steps: int, reps: int) -> float:
         t = self.torch
         stream = t.cuda.current_stream(self.device)
+        self.run(steps)                      # capture + warm
+        e0, e1 = t.cuda.Event(enable_timing=True), t.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            self.run(steps)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    def autotune(self, steps: int = 2, candidates=None, reps: int = 2) -> dict:
+        """Pick the thread mapping of every fused stage: each (tracers, levels) per-thread
+        candidate is timed stage by stage (profile_step) and each stage keeps its fastest;
+        the per-stage choice is then timed against the best single mapping for all stages
+        as ``steps``-step graph runs, and the faster stays (the member state advances while
+        tuning). Returns the per-candidate stage times and the choice."""
         ntr_max = max(m.ntr for m in self.members)
-        times = {}
-        for c, lv in (candidates or self.MAPPINGS):
-            if c > ntr_max and c != 1:
-                continue
+        cands = [(c, lv) for c, lv in (candidates or self.MAPPINGS) if c <= ntr_max or c == 1]
+        prof = {}
+        for c, lv in cands:
             self.set_mapping(c, lv)
-            self.run(steps)                      # capture + warm
-            e0, e1 = t.cuda.Event(enable_timing=True), t.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            for _ in range(reps):
-                self.run(steps)
-            e1.record(stream)
-            e1.synchronize()
-            times[(c, lv)] = e0.elapsed_time(e1) / reps
-        best = min(times, key=times.get)
-        self.set_mapping(*best)
-        return {f"{c}x{lv}": v for (c, lv), v in times.items()}
+            p = [self.profile_step() for _ in range(2)]
+            prof[(c, lv)] = {st: min(q[st] for q in p) for st in self.STAGES}
+        best_stage = [min(cands, key=lambda m: prof[m][st]) for st in self.STAGES]
+        uniform = min(cands, key=lambda m: sum(prof[m].values()))
+        self.set_mapping(*uniform)
+        t_uniform = self._graph_ms(steps, reps)
+        for i, m in enumerate(best_stage):
+            self.set_stage_mapping(i, *m)
+        t_stage = self._graph_ms(steps, reps)
+        if t_uniform < t_stage:
+            self.set_mapping(*uniform)
+        return dict(stage_ms={f"{c}x{lv}": prof[(c, lv)] for c, lv in cands},
+                    per_stage={st: f"{m[0]}x{m[1]}" for st, m in zip(self.STAGES, best_stage)},
+                    per_stage_ms=t_stage, uniform=f"{uniform[0]}x{uniform[1]}",
+                    uniform_ms=t_uniform,
+                    chosen="per_stage" if t_stage <= t_uniform else "uniform")
 
     def profile_step(self, stream=None) -> dict:
         """Run one step stage by stage (synchronising) and return ``{stage: ms}``."""

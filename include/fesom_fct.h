@@ -333,6 +333,10 @@ int fct_batch_set_chunk(FctBatch* b, int chunk);
 /* Tuning: tracers per thread (1, 2, 4 or 8; the fused stages carry at most 4) and levels
  * per thread (1, 2, 4 or 8) of the fused stages. Drops cached graphs. */
 int fct_batch_set_mapping(FctBatch* b, int tracers_per_thread, int levels_per_thread);
+/* The same for one fused stage: 0 LO and adf_v, 1 adf_h, 2 limiter factors, 3 T_new (the
+ * stages are separate kernels, so each may take its own mapping). Drops cached graphs. */
+int fct_batch_set_stage_mapping(FctBatch* b, int stage, int tracers_per_thread,
+                                int levels_per_thread);
 /* [instances, groups, workspace bytes, total wet node layers x tracers,
  *  tracers per workspace chunk (largest over groups), kernel launches per step] */
 int fct_batch_info(const FctBatch* b, int64_t out[6]);
