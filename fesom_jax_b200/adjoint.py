@@ -291,9 +291,9 @@ def chain_loss_and_grad(mesh: Mesh, T0, uv, helem, hnode, hnode_new, target, ste
             if tape is not None:
                 states.append(tape.forward(s, uv, w, helem, hnode, hnode_new, states[-1],
                                            states[-2], dt))
-            else:
+            else:   # the stage-by-stage kernels: the trajectory the tape would record
                 states.append(plan.forward(uv, w, helem, hnode, hnode_new, states[-1],
-                                           states[-2], dt))
+                                           states[-2], dt, stagewise=True))
         TK = states[-1]
         av0 = torch.from_numpy(mesh.areasvol[:, 0].copy()).to(dev)
         tgt = target.to(dev)

@@ -700,6 +700,16 @@ int fct_vert_diff(FctPlan* P, const FctVdiffFields* f, double dt, int ntr, fct_s
 }
 
 int fct_forward(FctPlan* P, const FctFields* f, double dt, int ntr, fct_stream_t stream) {
+  return fct_forward_ex(P, f, dt, ntr, 0, stream);
+}
+
+int fct_forward_ex(FctPlan* P, const FctFields* f, double dt, int ntr, int flags,
+                   fct_stream_t stream) {
+  if (flags & ~FCT_FWD_STAGEWISE) return set_error(FCT_ERR_INVALID, "unknown flags 0x%x", flags);
+  const bool stagewise = (flags & FCT_FWD_STAGEWISE) || !P || !P->fused;
+  if (P && stagewise && !P->ws_full)
+    return set_error(FCT_ERR_CAPACITY, "the stage-by-stage kernels need the full workspace: "
+                     "call fct_plan_set_fused(plan, 0) or fct_plan_reserve_adjoint first");
   if (!P || !f) return set_error(FCT_ERR_INVALID, "NULL plan or fields");
   if (ntr < 1) return set_error(FCT_ERR_INVALID, "ntr must be >= 1");
   if (ntr > P->max_tracers)
@@ -731,7 +741,7 @@ int fct_forward(FctPlan* P, const FctFields* f, double dt, int ntr, fct_stream_t
   dims.set_map(P->per_thread, P->lpt);
   dims.any_wi = f->w_i != nullptr;
   dims.copy_dry = true;   // a fresh T_new: dry levels keep T (tracer_adv.py:147-151)
-  dims.fused = P->fused;
+  dims.fused = !stagewise;
   int prev = -1;
   cudaGetDevice(&prev);
   if (prev != P->device) cudaSetDevice(P->device);

@@ -32,6 +32,22 @@
 namespace fct {
 namespace {
 
+// Arithmetic of the segment kernels. Quotients multiply by the divisor's correctly rounded
+// reciprocal (within 1.5 ulp of the quotient; the one-kernel-per-stage path rounds every
+// quotient correctly instead), products that feed a sum fuse into FMAs written out in the
+// source (--fmad=false keeps the compiler from contracting anything else, so every
+// template instantiation rounds alike), and max/min are plain comparisons (the same values
+// as fmax/fmin on the finite numbers the scheme carries).
+struct Rcq {
+  double r;
+};
+__device__ __forceinline__ Rcq rcpq(double y) { return Rcq{__drcp_rn(y)}; }
+__device__ __forceinline__ double divq(double x, const Rcq& c) { return x * c.r; }
+__device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : b; }
+__device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : b; }
+// AB2 extrapolation ttfAB = -0.6*T_old + 1.6*T (tracer_adv.py:59-66)
+__device__ __forceinline__ double ab2f(double T, double To) { return fma(kAbNew, T, kAbOld * To); }
+
 // a level clamped into [0, L - 1]: loads at clamped levels are in bounds and their values
 // are discarded by the predicates that follow
 __device__ __forceinline__ int kclamp(int k, int L) { return k < 0 ? 0 : (k >= L ? L - 1 : k); }
@@ -88,7 +104,7 @@ __device__ __forceinline__ void seg_node_lo(const Inst& in, int64_t si, int t0, 
       ldv<NTR, IL>(in.T, qo + uint32_t(kc), t0, ts, tg, To);
 #pragma unroll
       for (int t = 0; t < NTR; ++t) {
-        const double f = -0.5 * (Tw[l + 2][t] * cown + To[t] * coth);
+        const double f = -0.5 * fma(Tw[l + 2][t], cown, To[t] * coth);
         div[l][t] = on ? div[l][t] + sg1 * f : div[l][t];
       }
     }
@@ -112,13 +128,14 @@ __device__ __forceinline__ void seg_node_lo(const Inst& in, int64_t si, int t0, 
     const uint32_t qn = base + uint32_t(k0 + l);
     const double hn = __ldg(in.hnode + qn), hnn = __ldg(in.hnode_new + qn);
     const double av = __ldg(m.areasvol + qn);
-    const Rcp rav = rcp(av), rhn = rcp(hnn);
+    const double fdt = dt * __drcp_rn(av);   // dt / areasvol
+    const Rcq rhn = rcpq(hnn);
     const bool valid = (hnn > 0.0) && (av > 0.0);
     double lo[NTR];
 #pragma unroll
     for (int t = 0; t < NTR; ++t)
-      lo[t] = valid ? divr(Tw[l + 2][t] * hn +
-                               divr((div[l][t] + (fv[l][t] - fv[l + 1][t])) * dt, rav), rhn)
+      lo[t] = valid ? divq(fma(Tw[l + 2][t], hn, (div[l][t] + (fv[l][t] - fv[l + 1][t])) * fdt),
+                           rhn)
                     : 0.0;
     stv<NTR, IL>(in.ws.lo, qn, w0, in.ws.sN, in.wtg, lo);
   }
@@ -139,11 +156,11 @@ __device__ __forceinline__ void seg_node_lo(const Inst& in, int64_t si, int t0, 
     double hi[NTR];
     if (k == nzmin) {
 #pragma unroll
-      for (int t = 0; t < NTR; ++t) hi[t] = -ab2(Tw[l + 2][t], To[l + 2][t]) * Wf * area_k;
+      for (int t = 0; t < NTR; ++t) hi[t] = -ab2f(Tw[l + 2][t], To[l + 2][t]) * Wf * area_k;
     } else if (k == nzmin + 1 || k == nzmax - 1) {
 #pragma unroll
       for (int t = 0; t < NTR; ++t)
-        hi[t] = -0.5 * (ab2(Tw[l + 1][t], To[l + 1][t]) + ab2(Tw[l + 2][t], To[l + 2][t])) *
+        hi[t] = -0.5 * (ab2f(Tw[l + 1][t], To[l + 1][t]) + ab2f(Tw[l + 2][t], To[l + 2][t])) *
                 Wf * area_k;
     } else {   // nzmin + 2 <= k <= nzmax - 2
       double Znz, Zm1, Zm2, Zp1, zb;   // QR4C stencil depths (tracer_adv.py:228-238, 265-273)
@@ -155,21 +172,22 @@ __device__ __forceinline__ void seg_node_lo(const Inst& in, int64_t si, int t0, 
         Znz = __ldg(m.Zp + k); Zm1 = __ldg(m.Zp + k - 1); Zm2 = __ldg(m.Zp + k - 2);
         Zp1 = __ldg(m.Zp + (k + 1 < L ? k + 1 : L - 1)); zb = __ldg(m.zbar + k);
       }
-      const Rcp rdc = rcp(safe_nz(Zm1 - Znz)), rdu = rcp(safe_nz(Znz - Zp1)),
-                rdd = rcp(safe_nz(Zm2 - Zm1));
-      const Rcp r3{3.0, 1.0 / 3.0, true};
+      const Rcq rdc = rcpq(safe_nz(Zm1 - Znz)), rdu = rcpq(safe_nz(Znz - Zp1)),
+                rdd = rcpq(safe_nz(Zm2 - Zm1));
+      const double d1 = (zb - Znz) * (1.0 / 3.0), d2 = (zb - Zm1) * (1.0 / 3.0);
+      const double wa = -0.5 * Wf * area_k;
 #pragma unroll
       for (int t = 0; t < NTR; ++t) {
-        const double A0 = ab2(Tw[l + 2][t], To[l + 2][t]);
-        const double Am1 = ab2(Tw[l + 1][t], To[l + 1][t]);
-        const double Am2 = ab2(Tw[l][t], To[l][t]);
-        const double Ap1 = ab2(Tw[l + 3][t], To[l + 3][t]);
-        const double qc = divr(Am1 - A0, rdc);
-        const double qu = divr(A0 - Ap1, rdu);
-        const double qd = divr(Am2 - Am1, rdd);
-        const double Tmean1 = A0 + divr((2.0 * qc + qu) * (zb - Znz), r3);
-        const double Tmean2 = Am1 + divr((2.0 * qc + qd) * (zb - Zm1), r3);
-        hi[t] = -0.5 * (Tmean1 + Tmean2) * Wf * area_k;
+        const double A0 = ab2f(Tw[l + 2][t], To[l + 2][t]);
+        const double Am1 = ab2f(Tw[l + 1][t], To[l + 1][t]);
+        const double Am2 = ab2f(Tw[l][t], To[l][t]);
+        const double Ap1 = ab2f(Tw[l + 3][t], To[l + 3][t]);
+        const double qc = divq(Am1 - A0, rdc);
+        const double qu = divq(A0 - Ap1, rdu);
+        const double qd = divq(Am2 - Am1, rdd);
+        const double Tmean1 = fma(fma(2.0, qc, qu), d1, A0);
+        const double Tmean2 = fma(fma(2.0, qc, qd), d2, Am1);
+        hi[t] = (Tmean1 + Tmean2) * wa;
       }
     }
     double adf[NTR];
@@ -204,7 +222,6 @@ __device__ __forceinline__ void seg_edge_adf(const Inst& in, int64_t si, int t0,
   const uint32_t qd0 = lq(cd.y, L, 0), qd1 = lq(cd.z, L, 0), qd2 = lq(cd.w, L, 0);
   const int64_t ts = in.tstride;
   const int tg = in.tg;
-  const Rcp r6{6.0, 1.0 / 6.0, true};
 #pragma unroll
   for (int l = 0; l < LPT; ++l) {
     const int kc = kclamp(k0 + l, L);
@@ -226,17 +243,16 @@ __device__ __forceinline__ void seg_edge_adf(const Inst& in, int64_t si, int t0,
 #pragma unroll
     for (int t = 0; t < NTR; ++t) {
       // the up and down cells' gradients, as tracer_gradient_elements evaluates them
-      const double g0 = up0.x * a0[t] + up0.y * a1[t] + up1.x * a2[t];
-      const double g2 = up1.y * a0[t] + up2.x * a1[t] + up2.y * a2[t];
-      const double g1 = dn0.x * b0[t] + dn0.y * b1[t] + dn1.x * b2[t];
-      const double g3 = dn1.y * b0[t] + dn2.x * b1[t] + dn2.y * b2[t];
-      const double fl = -0.5 * (T1[t] * (vf + avf) + T2[t] * (vf - avf));
-      const double A1 = ab2(T1[t], O1[t]), A2 = ab2(T2[t], O2[t]);
-      const double diff = A2 - A1;
-      const double Tm1 = A1 + divr(2.0 * diff + c1 * g0 + c2 * g2, r6);
-      const double Tm2 = A2 - divr(2.0 * diff + c1 * g1 + c2 * g3, r6);
-      const double ho = -0.5 * ((vf + avf) * Tm1 + (vf - avf) * Tm2);
-      adf[t] = ho - fl;
+      const double g0 = fma(up1.x, a2[t], fma(up0.y, a1[t], up0.x * a0[t]));
+      const double g2 = fma(up2.y, a2[t], fma(up2.x, a1[t], up1.y * a0[t]));
+      const double g1 = fma(dn1.x, b2[t], fma(dn0.y, b1[t], dn0.x * b0[t]));
+      const double g3 = fma(dn2.y, b2[t], fma(dn2.x, b1[t], dn1.y * b0[t]));
+      const double A1 = ab2f(T1[t], O1[t]), A2 = ab2f(T2[t], O2[t]);
+      const double diff2 = 2.0 * (A2 - A1);
+      const double Tm1 = fma(fma(c2, g2, fma(c1, g0, diff2)), 1.0 / 6.0, A1);
+      const double Tm2 = fma(fma(c2, g3, fma(c1, g1, diff2)), -1.0 / 6.0, A2);
+      // HO - LO = -0.5*((vf+|vf|)*(Tm1 - T1) + (vf-|vf|)*(Tm2 - T2))
+      adf[t] = -0.5 * fma(vf + avf, Tm1 - T1[t], (vf - avf) * (Tm2 - T2[t]));
     }
     if (l < nk) stv<NTR, IL>(in.ws.adfh, qe + uint32_t(kc), w0, in.ws.sEd, in.wtg, adf);
   }
@@ -380,11 +396,11 @@ __device__ __forceinline__ void seg_node_limit(const Inst& in, int64_t si, bool 
         ldv<NTR, IL>(in.ws.adfh, qe + uint32_t(kc), w0, in.ws.sEd, in.wtg, a);
 #pragma unroll
         for (int t = 0; t < NTR; ++t) {
-          mx[l][t] = wet ? fmax(mx[l][t], fmax(lv[t], tv[t])) : mx[l][t];
-          mn[l][t] = wet ? fmin(mn[l][t], fmin(lv[t], tv[t])) : mn[l][t];
+          mx[l][t] = wet ? dmax(mx[l][t], dmax(lv[t], tv[t])) : mx[l][t];
+          mn[l][t] = wet ? dmin(mn[l][t], dmin(lv[t], tv[t])) : mn[l][t];
           const double sv = sg1 * a[t];
-          sp[l][t] = on ? sp[l][t] + fmax(sv, 0.0) : sp[l][t];
-          sm[l][t] = on ? sm[l][t] + fmin(sv, 0.0) : sm[l][t];
+          sp[l][t] = on ? sp[l][t] + dmax(sv, 0.0) : sp[l][t];
+          sm[l][t] = on ? sm[l][t] + dmin(sv, 0.0) : sm[l][t];
         }
       }
     }
@@ -399,12 +415,12 @@ __device__ __forceinline__ void seg_node_limit(const Inst& in, int64_t si, bool 
 #pragma unroll
       for (int t = 0; t < NTR; ++t) {
         if (ow) {
-          mx[l][t] = fmax(mx[l][t], fmax(lo[l][t], tv[t]));
-          mn[l][t] = fmin(mn[l][t], fmin(lo[l][t], tv[t]));
+          mx[l][t] = dmax(mx[l][t], dmax(lo[l][t], tv[t]));
+          mn[l][t] = dmin(mn[l][t], dmin(lo[l][t], tv[t]));
         }
         if (of) {
-          mx[l][t] = fmax(mx[l][t], -kBig);
-          mn[l][t] = fmin(mn[l][t], kBig);
+          mx[l][t] = dmax(mx[l][t], -kBig);
+          mn[l][t] = dmin(mn[l][t], kBig);
         }
       }
     }
@@ -435,7 +451,7 @@ __device__ __forceinline__ void seg_node_limit(const Inst& in, int64_t si, bool 
     const double av = __ldg(m.areasvol + qn), hnn = __ldg(in.hnode_new + qn);
     const bool valid_n = (av > 0.0) && (hnn > 0.0);
     const double sa = av > 0.0 ? av : 1.0, sh_ = hnn > 0.0 ? hnn : 1.0;
-    const Rcp rsa = rcp(sa), rsh = rcp(sh_);
+    const double fdt = dt * __drcp_rn(sa * sh_);   // dt / (areasvol * hnode_new)
     double ft[NTR], fb[NTR];
     ldv<NTR, IL>(in.ws.adfv, qn, w0, sN, in.wtg, ft);
     if (k + 1 < nzmax) {
@@ -455,19 +471,18 @@ __device__ __forceinline__ void seg_node_limit(const Inst& in, int64_t si, bool 
                                      : sh[(0 * NTR + t) * 256 + tid + S];
         const double bn = l + 1 < nk ? mn[l + 1 < LPT ? l + 1 : l][t]
                                      : sh[(1 * NTR + t) * 256 + tid + S];
-        wmx = fmax(fmax(ax, wmx), bx);
-        wmn = fmin(fmin(an, wmn), bn);
+        wmx = dmax(dmax(ax, wmx), bx);
+        wmn = dmin(dmin(an, wmn), bn);
       }
-      const double plus = (fmax(ft[t], 0.0) + fmax(-fb[t], 0.0)) + sp[l][t];
-      const double minus = (fmin(ft[t], 0.0) + fmin(-fb[t], 0.0)) + sm[l][t];
+      const double plus = (dmax(ft[t], 0.0) + dmax(-fb[t], 0.0)) + sp[l][t];
+      const double minus = (dmin(ft[t], 0.0) + dmin(-fb[t], 0.0)) + sm[l][t];
       pf[t] = 1.0;
       mf[t] = 1.0;
       if (valid_n) {
-        const double flux_pos = divr(divr(plus * dt, rsa), rsh) + kFluxEps;
-        const double flux_neg = divr(divr(minus * dt, rsa), rsh) - kFluxEps;
-        // correctly rounded quotients (the same bits as '/')
-        pf[t] = fmin(1.0, divr(wmx - lo[l][t], rcp(flux_pos)));
-        mf[t] = fmin(1.0, divr(wmn - lo[l][t], rcp(flux_neg)));
+        const double flux_pos = fma(plus, fdt, kFluxEps);
+        const double flux_neg = fma(minus, fdt, -kFluxEps);
+        pf[t] = dmin(1.0, (wmx - lo[l][t]) * __drcp_rn(flux_pos));
+        mf[t] = dmin(1.0, (wmn - lo[l][t]) * __drcp_rn(flux_neg));
       }
     }
     stv<NTR, IL>(in.ws.pf, qn, w0, sN, in.wtg, pf);
@@ -527,7 +542,7 @@ __device__ __forceinline__ void seg_node_final(const Inst& in, int64_t si, int t
         // b3 (tracer_adv.py:461-465): adf >= 0 ? min(plus(n1), minus(n2)) : min(minus(n1),
         // plus(n2)); min is exact and symmetric, so in the node's own terms the factor is
         // min(own plus, other minus) when the flux leaves the node, else the other pair
-        const double x1 = fmin(pfw[l + 1][t], mfo[t]), x2 = fmin(mfw[l + 1][t], pfo[t]);
+        const double x1 = dmin(pfw[l + 1][t], mfo[t]), x2 = dmin(mfw[l + 1][t], pfo[t]);
         const double ae = ((a[t] >= 0.0) != second) ? x1 : x2;
         const double lim = ae * a[t];
         hsc[l][t] = on ? hsc[l][t] + sg1 * lim : hsc[l][t];
@@ -543,7 +558,8 @@ __device__ __forceinline__ void seg_node_final(const Inst& in, int64_t si, int t
     const double av = __ldg(m.areasvol + qn);
     const double sa = av > 0.0 ? av : 1.0;
     const double hn = __ldg(in.hnode + qn), hnn = __ldg(in.hnode_new + qn);
-    const Rcp rsa = rcp(sa), rhn = rcp(hnn);
+    const double fdt = dt * __drcp_rn(sa);   // dt / areasvol
+    const Rcq rhn = rcpq(hnn);
     double ft[NTR], vt[NTR], vb[NTR];
     ldv<NTR, IL>(in.ws.adfv, qn, w0, sN, in.wtg, ft);
     // limited vertical flux at the top interface k (tracer_adv.py:453-459)
@@ -551,7 +567,7 @@ __device__ __forceinline__ void seg_node_final(const Inst& in, int64_t si, int t
     for (int t = 0; t < NTR; ++t) {
       const double pf0 = pfw[l + 1][t], mf0 = mfw[l + 1][t];
       vt[t] = k == nzmin ? (ft[t] >= 0.0 ? pf0 : mf0) * ft[t]
-                         : (ft[t] >= 0.0 ? fmin(mfw[l][t], pf0) : fmin(pfw[l][t], mf0)) * ft[t];
+                         : (ft[t] >= 0.0 ? dmin(mfw[l][t], pf0) : dmin(pfw[l][t], mf0)) * ft[t];
     }
     // limited vertical flux at the bottom interface k+1 (0 at the node's bottom)
     if (k + 1 >= nzmax) {
@@ -562,19 +578,19 @@ __device__ __forceinline__ void seg_node_final(const Inst& in, int64_t si, int t
       ldv<NTR, IL>(in.ws.adfv, qn + 1, w0, sN, in.wtg, fb);
 #pragma unroll
       for (int t = 0; t < NTR; ++t)
-        vb[t] = (fb[t] >= 0.0 ? fmin(mfw[l + 1][t], pfw[l + 2][t])
-                              : fmin(pfw[l + 1][t], mfw[l + 2][t])) * fb[t];
+        vb[t] = (fb[t] >= 0.0 ? dmin(mfw[l + 1][t], pfw[l + 2][t])
+                              : dmin(pfw[l + 1][t], mfw[l + 2][t])) * fb[t];
     }
     double Tv[NTR], lo[NTR], out[NTR];
     ldv<NTR, IL>(in.T, qn, t0, in.tstride, tg, Tv);
     ldv<NTR, IL>(in.ws.lo, qn, w0, sN, in.wtg, lo);
 #pragma unroll
     for (int t = 0; t < NTR; ++t) {
-      const double lo_trans = -Tv[t] * hn + lo[t] * hnn;
-      const double vdiv = av > 0.0 ? divr((vt[t] - vb[t]) * dt, rsa) : 0.0;
-      double d = divr(hsc[l][t] * dt, rsa) + (lo_trans + vdiv);
-      d = d + Tv[t] * (hn - hnn);
-      out[t] = Tv[t] + (hnn > 0.0 ? divr(d, rhn) : 0.0);
+      const double lo_trans = fma(lo[t], hnn, -Tv[t] * hn);
+      const double vdiv = av > 0.0 ? (vt[t] - vb[t]) * fdt : 0.0;
+      double d = fma(hsc[l][t], fdt, lo_trans + vdiv);
+      d = fma(Tv[t], hn - hnn, d);
+      out[t] = Tv[t] + (hnn > 0.0 ? divq(d, rhn) : 0.0);
     }
     stv<NTR, IL>(in.T_new, qn, t0, in.tstride, tg, out);
     count_nonfinite<NTR>(in.nonfinite, out);

@@ -113,8 +113,10 @@ class FctPlan:
             pass
 
     def forward(self, uv, w_e, helem, hnode, hnode_new, T, T_old, dt: float, out=None,
-                Z3d=None, zbar3=None, w_i=None, stream=None):
-        """One FCT step on device tensors; returns ``T_new`` (same shape as ``T``)."""
+                Z3d=None, zbar3=None, w_i=None, stream=None, stagewise: bool = False):
+        """One FCT step on device tensors; returns ``T_new`` (same shape as ``T``).
+        ``stagewise`` runs one kernel per reference stage (``fct_forward_ex``), the kernels
+        the reverse pass recomputes with (needs the plan's adjoint reservation)."""
         torch = _torch()
         m = self.mesh
         N, E, nl = m.nod2D, m.elem2D, m.nl
@@ -153,9 +155,17 @@ class FctPlan:
         s = stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
         # the library orders calls on one plan on the GPU; the lock keeps the host-side
         # enqueue of concurrent Python threads whole
+        L = _lib.lib()
         with self._lock:
-            _lib.check(_lib.lib().fct_forward(self._h, C.byref(f), float(dt), ntr,
-                                              C.c_void_p(int(s))))
+            if stagewise:
+                L.fct_forward_ex.argtypes = [C.c_void_p, C.POINTER(_lib.FctFields), C.c_double,
+                                             C.c_int, C.c_int, C.c_void_p]
+                L.fct_forward_ex.restype = C.c_int
+                _lib.check(L.fct_forward_ex(self._h, C.byref(f), float(dt), ntr, 1,
+                                            C.c_void_p(int(s))))
+            else:
+                _lib.check(L.fct_forward(self._h, C.byref(f), float(dt), ntr,
+                                         C.c_void_p(int(s))))
         return out
 
 

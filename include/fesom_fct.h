@@ -108,9 +108,10 @@ int fct_plan_reserve(FctPlan* plan, int max_tracers);
 int fct_plan_info(const FctPlan* plan, int64_t out[8]);
 /* Which stage kernels fct_forward runs: fused (1, the default: 5 launches per tracer
  * chunk over runs of consecutive levels, element gradients and cluster bounds recomputed
- * instead of stored) or one kernel per reference stage (0: 7 launches, every intermediate
- * written to the workspace, the form the reverse pass recomputes). Both give the same
- * T_new bit for bit. */
+ * instead of stored, quotients by reciprocals and explicit FMAs) or one kernel per
+ * reference stage (0: 7 launches, every intermediate written to the workspace, every
+ * quotient correctly rounded; the form the reverse pass recomputes). The two give the same
+ * T_new to rounding (a few ulp per step). */
 int fct_plan_set_fused(FctPlan* plan, int fused);
 /* Thread mapping of the fused stages of this plan's fct_forward / fct_forward_noalloc and
  * of its instances in fct_serve_step: the most tracers one thread carries and the levels
@@ -128,6 +129,15 @@ int fct_plan_set_mapping(FctPlan* plan, int tracers_per_thread, int levels_per_t
  * their stream is captured into a CUDA graph skip that ordering. */
 int fct_forward(FctPlan* plan, const FctFields* fields, double dt, int ntr,
                 fct_stream_t stream);
+
+/* fct_forward with options. FCT_FWD_STAGEWISE runs one kernel per reference stage (the
+ * kernels the reverse pass recomputes with, which round every quotient correctly), so a
+ * trajectory stepped with it is the one fct_adjoint differentiates bit for bit; it needs
+ * the full workspace (fct_plan_reserve_adjoint or fct_plan_set_fused(plan, 0)). The
+ * default fused kernels give the same T_new to rounding (a few ulp). */
+#define FCT_FWD_STAGEWISE 1
+int fct_forward_ex(FctPlan* plan, const FctFields* fields, double dt, int ntr, int flags,
+                   fct_stream_t stream);
 
 /* Health check, the finiteness gate of the reference's diagnostics
  * (fesom_jax/diagnostics.py:31-101 state_diagnostics/verdict): the number of non-finite
@@ -220,8 +230,9 @@ int fct_tape_bytes(const FctPlan* plan, int ntr, int steps, int64_t* out);
 int fct_tape_create(FctPlan* plan, int ntr, int steps, void* mem, int64_t bytes,
                     FctTape** out);
 int fct_tape_destroy(FctTape* tape);
-/* fct_forward that also records the step's intermediates in tape slot ``slot``
- * (T_new is bit-identical to fct_forward's). w_i is not supported (not differentiated). */
+/* fct_forward that also records the step's intermediates in tape slot ``slot`` (with the
+ * stage-by-stage kernels: T_new is bit-identical to fct_forward_ex with
+ * FCT_FWD_STAGEWISE). w_i is not supported (not differentiated). */
 int fct_forward_taped(FctPlan* plan, const FctFields* fields, double dt, int ntr,
                       FctTape* tape, int slot, fct_stream_t stream);
 /* Declares that ``slot`` of a tape created over caller memory already holds a step

@@ -130,8 +130,9 @@ def test_autograd_function_matches_vjp(torch, pi):
 
 
 def test_tape_equals_recompute(torch, pi):
-    """A taped step's forward equals fct_forward and its adjoint equals the recomputing
-    adjoint, bit for bit; so does the K-step chain under both checkpoint modes."""
+    """A taped step's forward (the stage-by-stage kernels) equals fct_forward (the fused
+    kernels) to rounding, and its adjoint equals the recomputing adjoint bit for bit; so
+    does the K-step chain under both checkpoint modes."""
     from fesom_jax_b200.adjoint import Tape, advect_one_fct_vjp, chain_loss_and_grad
     from fesom_jax_b200.tracer_adv import get_plan
     f = I.make_fields(pi, seed=5, ab2=True, kind="white", sigma=0.02, n_passive=1)
@@ -140,7 +141,8 @@ def test_tape_equals_recompute(torch, pi):
     gTn = _d(torch, np.random.default_rng(3).normal(size=T.shape))
     with Tape(pi, steps=2, ntr=3) as tape:
         Tn = tape.forward(1, *args, T, To, DT)
-        assert torch.equal(Tn, get_plan(pi, 0).forward(*args, T, To, DT))
+        Tf = get_plan(pi, 0).forward(*args, T, To, DT)
+        assert float((Tn - Tf).abs().max()) <= 1e-13 * float(Tf.abs().max())
         taped = advect_one_fct_vjp(pi, *args, T, To, gTn, dt=DT, tape=tape, slot=1)
         again = advect_one_fct_vjp(pi, *args, T, To, gTn, dt=DT, tape=tape, slot=1)
     plain = advect_one_fct_vjp(pi, *args, T, To, gTn, dt=DT)

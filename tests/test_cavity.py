@@ -75,7 +75,9 @@ def test_gpu_fused_and_unfused_on_cavity(cav, golden, name):
         ref = advect_one_fct(cav, *args, dt=DT)[0].cpu().numpy()
     finally:
         plan.set_fused(True)
-    assert np.array_equal(got, ref)
+    # the fused stages divide by reciprocals and fuse multiply-adds: equal to rounding
+    assert np.max(np.abs(got - ref)) <= 1e-13 * np.max(np.abs(ref))
+    assert np.array_equal(got[~cav.node_layer_mask], ref[~cav.node_layer_mask])
 
 
 @pytest.mark.gpu

@@ -7,6 +7,8 @@ from oracle import fct_np
 from tests.golden_cases import DT, RTOL, cases, check_against_golden, load_golden
 
 pytestmark = pytest.mark.gpu
+# fused stages against the one-kernel-per-stage path: max|difference| / max|T| per step
+FUSED_RTOL = 1e-13
 
 NAMES = ["T_step1", "S_step1", "T_ab2", "sharp_x5", "const", "T_wsplit_zstar"]
 
@@ -134,7 +136,8 @@ def test_dry_levels_keep_T_exactly(torch, pi, pi_cases):
 @pytest.mark.parametrize("name", NAMES)
 def test_fused_equals_unfused(torch, pi, pi_cases, name):
     """The fused stage kernels (the default) and one kernel per reference stage give the
-    same T_new (equal values; max/min of +-0 may differ in the sign of a zero)."""
+    same T_new to rounding (the fused stages multiply by reciprocals and fuse
+    multiply-adds; the stage-by-stage path rounds every quotient correctly)."""
     from fesom_jax_b200.tracer_adv import get_plan
     plan = get_plan(pi, 0)
     c = pi_cases[name]
@@ -144,7 +147,8 @@ def test_fused_equals_unfused(torch, pi, pi_cases, name):
     finally:
         plan.set_fused(True)
     got = run_gpu(torch, pi, c)
-    assert np.array_equal(got, ref)
+    assert np.max(np.abs(got - ref)) <= FUSED_RTOL * np.max(np.abs(ref))
+    assert np.array_equal(got[~pi.node_layer_mask], ref[~pi.node_layer_mask])
 
 
 def test_fused_equals_unfused_generated_mesh(torch):
@@ -162,4 +166,4 @@ def test_fused_equals_unfused_generated_mesh(torch):
     finally:
         plan.set_fused(True)
     got = advect_one_fct(m, *args, dt=DT)[0].cpu().numpy()
-    assert np.array_equal(got, ref)
+    assert np.max(np.abs(got - ref)) <= FUSED_RTOL * np.max(np.abs(ref))
