@@ -5,9 +5,10 @@
 // edge) and NTR tracers. The entity's neighbour slots, level range and static geometry
 // are decoded once per segment and every neighbour gather issues LPT x NTR independent
 // loads (consecutive levels of one column), instead of one level per thread re-decoding
-// the same lists. The arithmetic of every quantity is the reference's, in the reference's
-// order (the same expressions as the one-kernel-per-stage path), so the results are the
-// same bits as that path's.
+// the same lists. Every quantity is the reference's expression; the arithmetic (below)
+// trades correctly rounded quotients for reciprocal products and fused multiply-adds, so
+// the results equal the one-kernel-per-stage path's to rounding (a few ulp per step), and
+// every mapping and layout of these kernels gives the same bits.
 //
 // Stages (kernels over the plan's segment lists, fct_internal.cuh DevMesh):
 //   seg_node_lo     node layers: LO (compute_fct_lo with adv_flux_hor/ver, :96-120,
@@ -20,8 +21,8 @@
 //                   two end nodes computed on the fly; at 1-2 % of the edge lanes of an
 //                   open-ocean mesh this is cheaper than storing node gradients everywhere
 //   seg_node_limit  zalesak_limit a1-a4, b1, b2 (:371-451): cluster bounds over the edge
-//                   neighbours, the k-1/k/k+1 window (the run's bounds plus one level above
-//                   and below), the antidiffusive sums and the limiter factors
+//                   neighbours, the k-1/k/k+1 window (across runs through shared memory),
+//                   the antidiffusive sums and the limiter factors
 //   seg_node_final  b3, flux2dtracer_fct, ale_reconstruct (:453-484, :142-151): T_new
 #pragma once
 

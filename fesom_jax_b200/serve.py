@@ -165,7 +165,8 @@ class ServingEngine:
         """Doubles of the fused-stage workspace one instance takes in the arena."""
         m = self.meshes[r.mesh].mesh
         N, Ed, L = m.nod2D, m.edge2D, m.nl
-        return Ed * L + self.ntr * (4 * N * L + Ed * L)
+        pad = lambda n: (n + 31) // 32 * 32  # noqa: E731  (fields on 256-byte boundaries)
+        return pad(Ed * L) + 4 * pad(self.ntr * N * L) + pad(self.ntr * Ed * L)
 
     def state_bytes(self, r: Request) -> int:
         m = self.meshes[r.mesh].mesh

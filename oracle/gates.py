@@ -7,10 +7,11 @@ intermediates (test infrastructure: the checker of the CUDA results, never measu
   fluxes telescope (fesom_jax/tracer_adv.py:298-313, 469-484), so a step changes the
   tracer content only through the surface;
 * monotonicity against the Zalesak window (fesom_jax/tracer_adv.py:389-418): every
-  updated lane stays inside ``[window_min, window_max]`` with a slack of 4 ulp of the
-  largest magnitude the update combines (the bound, T and LO): ``T_new = T + ((LO *
-  hnode_new - T * hnode) + fluxes + T * (hnode - hnode_new)) / hnode_new`` cancels T
-  against LO-sized terms, so its rounding is relative to those.
+  updated lane stays inside ``[window_min, window_max]`` with a slack of 4 ulp (16 for the
+  CUDA path's results, GPU_WINDOW_ULPS) of the largest magnitude the update combines (the
+  bound, T and LO): ``T_new = T + ((LO * hnode_new - T * hnode) + fluxes + T * (hnode -
+  hnode_new)) / hnode_new`` cancels T against LO-sized terms, so its rounding is relative
+  to those.
 """
 
 from __future__ import annotations
@@ -46,12 +47,19 @@ def window(m, inter):
     return w_max, w_min
 
 
-def window_violations(m, T, hnode_new, T_new, inter):
-    """``[(node, layer)]`` of valid lanes outside the window (4 ulp slack)."""
+# Slack of the window check for results of the CUDA path: its fused kernels form every
+# quotient as a product with the divisor's reciprocal (up to 1.5 ulp each) and evaluate
+# LO, the bounds and the factors themselves, so their update may land a few ulp further
+# past the oracle's window than the oracle's own update does.
+GPU_WINDOW_ULPS = 16.0
+
+
+def window_violations(m, T, hnode_new, T_new, inter, ulps: float = 4.0):
+    """``[(node, layer)]`` of valid lanes outside the window (``ulps`` slack)."""
     w_max, w_min = window(m, inter)
     valid = m.node_layer_mask & (m.areasvol > 0.0) & (hnode_new > 0.0)
     scale = np.maximum(np.abs(T), np.abs(inter["LO"]))
     with np.errstate(invalid="ignore"):
-        hi = w_max + 4.0 * np.spacing(np.maximum(np.abs(w_max), scale))
-        lo = w_min - 4.0 * np.spacing(np.maximum(np.abs(w_min), scale))
+        hi = w_max + ulps * np.spacing(np.maximum(np.abs(w_max), scale))
+        lo = w_min - ulps * np.spacing(np.maximum(np.abs(w_min), scale))
     return np.argwhere(valid & ((T_new > hi) | (T_new < lo)))

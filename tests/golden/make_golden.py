@@ -21,6 +21,7 @@ from __future__ import annotations
 
 import ast
 import hashlib
+import os
 import sys
 import tempfile
 import textwrap
@@ -28,7 +29,10 @@ from pathlib import Path
 
 import numpy as np
 
-REF = Path("/root/reference")
+# the reference checkout (koldunovn/fesom_jax): the FESOM_JAX_REFERENCE environment
+# variable, else a ``reference`` directory beside this repository
+REF = Path(os.environ.get("FESOM_JAX_REFERENCE",
+                          str(Path(__file__).resolve().parents[3] / "reference")))
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parents[1]
 sys.path.insert(0, str(REPO))

@@ -1,11 +1,14 @@
-"""Build ``mesh_pi.npz`` from the reference's pi mesh export directory.
+"""Build ``fesom_jax_b200/data/mesh_pi.npz`` from the reference's pi mesh export directory.
 
 The pi mesh (3140 nodes) ships with the reference as one ``.npy`` per array
 (fesom_jax/data/mesh_pi, layout in docs/MESH_EXPORT_LAYOUT.md). This script keeps the
 arrays the FCT path reads and writes them, unchanged, into one compressed bundle so the
 mesh travels with this package:
 
-    python fesom_jax_b200/data/make_pi_bundle.py /root/reference/fesom_jax/data/mesh_pi
+    python tests/golden/make_pi_bundle.py [<reference checkout>/fesom_jax/data/mesh_pi]
+
+Without an argument it reads the checkout named by FESOM_JAX_REFERENCE (or a
+``reference`` directory beside this repository), as the golden generators do.
 """
 
 import sys
@@ -14,6 +17,7 @@ from pathlib import Path
 import numpy as np
 
 sys.path.insert(0, str(Path(__file__).resolve().parents[2]))
+sys.path.insert(0, str(Path(__file__).resolve().parent))
 from fesom_jax_b200.mesh import PI_BUNDLE, load_mesh, save_bundle  # noqa: E402
 
 
@@ -27,4 +31,8 @@ def main(src: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1])
+    if len(sys.argv) > 1:
+        main(sys.argv[1])
+    else:
+        from make_golden import REF
+        main(str(REF / "fesom_jax/data/mesh_pi"))

@@ -99,7 +99,8 @@ def test_profile_step_reports_every_stage(torch, members):
 
 def _ws_bytes(m, ntr):
     L = m.nl
-    return 8 * (m.edge2D * L + ntr * (4 * m.nod2D * L + m.edge2D * L))   # fused workspace
+    pad = lambda n: (n + 31) // 32 * 32  # noqa: E731  (fields on 256-byte boundaries)
+    return 8 * (pad(m.edge2D * L) + 4 * pad(ntr * m.nod2D * L) + pad(ntr * m.edge2D * L))
 
 
 @pytest.mark.parametrize("per_thread", [8, 2, 1])

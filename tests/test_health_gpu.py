@@ -147,7 +147,8 @@ def test_900_steps_from_poisoned_memory(torch, pi, mesh_name):
             inter = {}
             fct_np.advect_one_fct(m, f.uv, f.w_e, f.helem, f.hnode, f.hnode_new, T[0], To[0],
                                   dt=dt, intermediates=inter)
-            assert len(gates.window_violations(m, T[0], f.hnode_new, g[0], inter)) == 0
+            assert len(gates.window_violations(m, T[0], f.hnode_new, g[0], inter,
+                                              gates.GPU_WINDOW_ULPS)) == 0
     # passive tracers started in [0, 1]: a bounded scheme keeps them there
     T = ens.state(0)[0].cpu().numpy()
     assert T[2][lmn].min() >= -1e-12 and T[2][lmn].max() <= 1.0 + 1e-12

@@ -43,8 +43,8 @@ def window(m, inter):
     return gates.window(m, inter)
 
 
-def window_violations(m, c, T_new, inter):
-    return gates.window_violations(m, c["T"], c["hnode_new"], T_new, inter)
+def window_violations(m, c, T_new, inter, ulps=4.0):
+    return gates.window_violations(m, c["T"], c["hnode_new"], T_new, inter, ulps)
 
 
 @pytest.mark.parametrize("name", CASES)
@@ -76,4 +76,4 @@ def test_gpu_closure_and_window(pi, name):
     _, inter = _oracle(pi, c)
     T_gpu = run_gpu(torch, pi, c)
     assert closure_residual(pi, c, T_gpu, inter) <= CLOSURE_RTOL
-    assert len(window_violations(pi, c, T_gpu, inter)) == 0
+    assert len(window_violations(pi, c, T_gpu, inter, gates.GPU_WINDOW_ULPS)) == 0
