@@ -58,6 +58,7 @@ constexpr int kMaxSlots = 24;      // edges per node
 constexpr int kSlotWet = 24;       // bits 24..47: a cell of the slot's edge is wet
 constexpr int kOwnBit = 48;        // some cell of the node is wet at the level
 constexpr int kOffBit = 49;        // some cell of the node is dry at the level
+constexpr int kAllBit = 50;        // every slot has the level and a wet cell, none dry
 constexpr int kSegLevels[kSegVariants] = {1, 2, 4, 8};
 __host__ __device__ constexpr int seg_variant(int lpt) {
   return lpt == 1 ? 0 : lpt == 2 ? 1 : lpt == 4 ? 2 : 3;
@@ -140,6 +141,11 @@ struct DevMesh {
                                       // slot's edge has level k, bit kSlotWet + j a cell of
                                       // that edge is wet at k, kOwnBit / kOffBit
   const int4* erec;
+  // per edge with up/down-cell levels: the up cell's two vertices besides n1 and the down
+  // cell's two besides n2, {ua, ub, da, db}, and [8 e ..] the MFCT weights of (n1, ua, ub)
+  // and (n2, da, db): (edx*a*gsca_x + edy*R*gsca_y) / 6 of each vertex
+  const int4* emf4;
+  const double* emfw;
   const uint32_t* nseg[kSegVariants];
   int64_t n_nseg[kSegVariants];
   const uint32_t* eseg[kSegVariants];

@@ -436,10 +436,14 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
       }
       f |= (unsigned long long)(own) << kOwnBit;
       f |= (unsigned long long)(off) << kOffBit;
+      const unsigned long long slots = (1ull << ed) - 1ull;
+      const bool all = (f & slots) == slots && ((f >> kSlotWet) & slots) == slots && !off;
+      f |= (unsigned long long)(all) << kAllBit;
       nflags.push_back(f);
     }
   }
-  std::vector<int4> erec(static_cast<size_t>(Ed));
+  std::vector<int4> erec(static_cast<size_t>(Ed)), emf4(static_cast<size_t>(Ed));
+  std::vector<double> emfw(8 * size_t(Ed), 0.0);
   std::vector<uint32_t> efix;
   std::vector<int> tlo(Ed, 0), thi(Ed, 0);
   for (int e = 0; e < Ed; ++e) {
@@ -454,6 +458,27 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
       thi[e] = (etr[e] >> 8) & 255;
     }
     erec[e] = make_int4(n1, n2, tlo[e] | (thi[e] << 8), 0);
+    if (thi[e] > tlo[e]) {
+      // MFCT with the up cell's gradient at n1 and the down cell's at n2
+      // (tracer_adv.py:196-225): edx*a*gx + edy*R*gy of a cell is one weighted sum of its
+      // vertex values, sum_i (c1*gsca[i] + c2*gsca[3+i]) T_i, scaled here by the scheme's
+      // 1/6; vertex order: the edge's own node, then the cell's other two
+      const double c1 = ecoef[2 * e], c2 = ecoef[2 * e + 1];
+      int other[4];
+      for (int r = 0; r < 2; ++r) {
+        const int el = d->edge_up_dn_tri[2 * e + r], own = r == 0 ? n1 : n2;
+        const int* en = d->elem_nodes + 3 * size_t(el);
+        const double* g = d->gradient_sca + 6 * size_t(el);
+        const int p = en[0] == own ? 0 : (en[1] == own ? 1 : 2);
+        const int a = (p + 1) % 3, bb = (p + 2) % 3;
+        const int idx[3] = {p, a, bb};
+        for (int i = 0; i < 3; ++i)
+          emfw[8 * size_t(e) + 3 * r + i] = (c1 * g[idx[i]] + c2 * g[3 + idx[i]]) / 6.0;
+        other[2 * r] = en[a];
+        other[2 * r + 1] = en[bb];
+      }
+      emf4[e] = make_int4(other[0], other[1], other[2], other[3]);
+    }
     for (int k = ekmin[e]; k < ekmax[e]; ++k)
       if (k < tlo[e] || k >= thi[e]) efix.push_back((uint32_t(e) << kLevelBits) | uint32_t(k));
   }
@@ -499,6 +524,7 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   size_t o_eud4 = b.add(eud4.data(), eud4.size());
   size_t o_ecell4 = b.add(ecell4.data(), ecell4.size());
   size_t o_nrec = b.add(nrec.data(), nrec.size()), o_erec = b.add(erec.data(), erec.size());
+  size_t o_emf4 = b.add(emf4.data(), emf4.size()), o_emfw = b.add(emfw.data(), emfw.size());
   size_t o_nflags = b.add(nflags.data(), std::max<size_t>(nflags.size(), 1));
   size_t o_efix = b.add(efix.data(), std::max<size_t>(efix.size(), 1));
   size_t o_nseg[kSegVariants], o_eseg[kSegVariants];
@@ -557,6 +583,8 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   m.nrec = (const int4*)(base + o_nrec);
   m.nflags = (const unsigned long long*)(base + o_nflags);
   m.erec = (const int4*)(base + o_erec);
+  m.emf4 = (const int4*)(base + o_emf4);
+  m.emfw = (const double*)(base + o_emfw);
   m.efix = (const uint32_t*)(base + o_efix);
   m.n_efix = int64_t(efix.size());
   for (int v = 0; v < kSegVariants; ++v) {

@@ -27,6 +27,7 @@
 #pragma once
 
 #include <algorithm>
+#include <type_traits>
 
 #include "fct_device.cuh"
 
@@ -48,6 +49,19 @@ __device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : 
 __device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : b; }
 // AB2 extrapolation ttfAB = -0.6*T_old + 1.6*T (tracer_adv.py:59-66)
 __device__ __forceinline__ double ab2f(double T, double To) { return fma(kAbNew, T, kAbOld * To); }
+
+// Every level of the run has all its edge slots counted and wet and no dry cell (the
+// common case away from coasts and bathymetry steps): the slot loops then take a body
+// without the per-slot selects (``std::integral_constant`` picks it at compile time).
+template <int LPT>
+__device__ __forceinline__ bool run_all(const unsigned long long (&fl)[LPT], int nk) {
+  bool all = true;
+#pragma unroll
+  for (int l = 0; l < LPT; ++l) all = all && (l >= nk || ((fl[l] >> kAllBit) & 1ull));
+  return all;
+}
+using AllWet = std::integral_constant<bool, true>;
+using SomeDry = std::integral_constant<bool, false>;
 
 // a level clamped into [0, L - 1]: loads at clamped levels are in bounds and their values
 // are discarded by the predicates that follow
@@ -86,6 +100,7 @@ __device__ __forceinline__ void seg_node_lo(const Inst& in, int64_t si, int t0, 
 #pragma unroll
   for (int l = 0; l < LPT; ++l) fl_[l] = l < nk ? __ldg(m.nflags + rec.w + (k0 + l - nzmin)) : 0ull;
   const int e0 = rec.x, e1 = rec.x + int((pk >> 16) & 255u);
+  auto slots = [&](auto all_wet) {
   for (int j = e0; j < e1; ++j) {
     const int4 sl = __ldg(m.ne4 + j);
     const int jj = j - e0;
@@ -95,7 +110,7 @@ __device__ __forceinline__ void seg_node_lo(const Inst& in, int64_t si, int t0, 
 #pragma unroll
     for (int l = 0; l < LPT; ++l) {
       const int kc = kclamp(k0 + l, L);
-      const bool on = (fl_[l] >> jj) & 1ull;
+      const bool on = decltype(all_wet)::value || ((fl_[l] >> jj) & 1ull);
       const double vf = __ldg(in.ws.vflux + qe + kc);
       const double avf = fabs(vf);
       // the reference's face flux -0.5*(T1*(vf+|vf|) + T2*(vf-|vf|)) with the node's own
@@ -110,6 +125,9 @@ __device__ __forceinline__ void seg_node_lo(const Inst& in, int64_t si, int t0, 
       }
     }
   }
+  };
+  if (run_all<LPT>(fl_, nk)) slots(AllWet{});
+  else slots(SomeDry{});
 
   // upwind vertical flux at the interfaces k0 .. k0+LPT (layer-masked, tracer_adv.py:108-120)
   double fv[LPT + 1][NTR];
@@ -211,16 +229,12 @@ __device__ __forceinline__ void seg_edge_adf(const Inst& in, int64_t si, int t0,
   const int e = lane_ent(sg), k0 = lane_lev(sg), L = m.L;
   const int4 er = __ldg(m.erec + e);
   const int nk = min(LPT, int((unsigned(er.z) >> 8) & 255u) - k0);
-  const int4 cu = __ldg(m.eud4 + 2 * e), cd = __ldg(m.eud4 + 2 * e + 1);
-  const double2 ec = __ldg(reinterpret_cast<const double2*>(m.ecoef) + e);
-  const double c1 = ec.x, c2 = ec.y;
-  const double2* gu = reinterpret_cast<const double2*>(m.gsca + 6 * int64_t(cu.x));
-  const double2* gd = reinterpret_cast<const double2*>(m.gsca + 6 * int64_t(cd.x));
-  const double2 up0 = __ldg(gu), up1 = __ldg(gu + 1), up2 = __ldg(gu + 2);
-  const double2 dn0 = __ldg(gd), dn1 = __ldg(gd + 1), dn2 = __ldg(gd + 2);
+  const int4 ov = __ldg(m.emf4 + e);
+  const double2* wp = reinterpret_cast<const double2*>(m.emfw + 8 * int64_t(e));
+  const double2 w01 = __ldg(wp), w23 = __ldg(wp + 1), w45 = __ldg(wp + 2);
   const uint32_t q1 = lq(er.x, L, 0), q2 = lq(er.y, L, 0), qe = lq(e, L, 0);
-  const uint32_t qu0 = lq(cu.y, L, 0), qu1 = lq(cu.z, L, 0), qu2 = lq(cu.w, L, 0);
-  const uint32_t qd0 = lq(cd.y, L, 0), qd1 = lq(cd.z, L, 0), qd2 = lq(cd.w, L, 0);
+  const uint32_t qua = lq(ov.x, L, 0), qub = lq(ov.y, L, 0);
+  const uint32_t qda = lq(ov.z, L, 0), qdb = lq(ov.w, L, 0);
   const int64_t ts = in.tstride;
   const int tg = in.tg;
 #pragma unroll
@@ -228,30 +242,26 @@ __device__ __forceinline__ void seg_edge_adf(const Inst& in, int64_t si, int t0,
     const int kc = kclamp(k0 + l, L);
     const double vf = __ldg(in.ws.vflux + qe + kc);
     const double avf = fabs(vf);
-    double T1[NTR], T2[NTR], O1[NTR], O2[NTR];
+    double T1[NTR], T2[NTR], O1[NTR], O2[NTR], ua[NTR], ub[NTR], da[NTR], db[NTR];
     ldv<NTR, IL>(in.T, q1 + kc, t0, ts, tg, T1);
     ldv<NTR, IL>(in.T, q2 + kc, t0, ts, tg, T2);
     ldv<NTR, IL>(in.T_old, q1 + kc, t0, ts, tg, O1);
     ldv<NTR, IL>(in.T_old, q2 + kc, t0, ts, tg, O2);
-    double a0[NTR], a1[NTR], a2[NTR], b0[NTR], b1[NTR], b2[NTR];
-    ldv<NTR, IL>(in.T, qu0 + kc, t0, ts, tg, a0);
-    ldv<NTR, IL>(in.T, qu1 + kc, t0, ts, tg, a1);
-    ldv<NTR, IL>(in.T, qu2 + kc, t0, ts, tg, a2);
-    ldv<NTR, IL>(in.T, qd0 + kc, t0, ts, tg, b0);
-    ldv<NTR, IL>(in.T, qd1 + kc, t0, ts, tg, b1);
-    ldv<NTR, IL>(in.T, qd2 + kc, t0, ts, tg, b2);
+    ldv<NTR, IL>(in.T, qua + kc, t0, ts, tg, ua);
+    ldv<NTR, IL>(in.T, qub + kc, t0, ts, tg, ub);
+    ldv<NTR, IL>(in.T, qda + kc, t0, ts, tg, da);
+    ldv<NTR, IL>(in.T, qdb + kc, t0, ts, tg, db);
     double adf[NTR];
 #pragma unroll
     for (int t = 0; t < NTR; ++t) {
-      // the up and down cells' gradients, as tracer_gradient_elements evaluates them
-      const double g0 = fma(up1.x, a2[t], fma(up0.y, a1[t], up0.x * a0[t]));
-      const double g2 = fma(up2.y, a2[t], fma(up2.x, a1[t], up1.y * a0[t]));
-      const double g1 = fma(dn1.x, b2[t], fma(dn0.y, b1[t], dn0.x * b0[t]));
-      const double g3 = fma(dn2.y, b2[t], fma(dn2.x, b1[t], dn1.y * b0[t]));
+      // Tm1 = A1 + (2*(A2 - A1) + edx*a*g_up_x + edy*R*g_up_y)/6 with the up cell's
+      // gradient as one weighted vertex sum; Tm2 likewise with the down cell's, minus
       const double A1 = ab2f(T1[t], O1[t]), A2 = ab2f(T2[t], O2[t]);
-      const double diff2 = 2.0 * (A2 - A1);
-      const double Tm1 = fma(fma(c2, g2, fma(c1, g0, diff2)), 1.0 / 6.0, A1);
-      const double Tm2 = fma(fma(c2, g3, fma(c1, g1, diff2)), -1.0 / 6.0, A2);
+      const double dA = A2 - A1;
+      const double su = fma(w01.y, ua[t], fma(w23.x, ub[t], w01.x * T1[t]));
+      const double sd = fma(w23.y, T2[t], fma(w45.x, da[t], w45.y * db[t]));
+      const double Tm1 = fma(dA, 1.0 / 3.0, A1) + su;
+      const double Tm2 = fma(dA, -1.0 / 3.0, A2) - sd;
       // HO - LO = -0.5*((vf+|vf|)*(Tm1 - T1) + (vf-|vf|)*(Tm2 - T2))
       adf[t] = -0.5 * fma(vf + avf, Tm1 - T1[t], (vf - avf) * (Tm2 - T2[t]));
     }
@@ -381,6 +391,7 @@ __device__ __forceinline__ void seg_node_limit(const Inst& in, int64_t si, bool 
     for (int l = 0; l < LPT; ++l)
       fl_[l] = l < nk ? __ldg(m.nflags + rec.w + (k0 + l - nzmin)) : 0ull;
     const int e0 = rec.x, e1 = rec.x + int((pk >> 16) & 255u);
+    auto slots = [&](auto all_wet) {
     for (int j = e0; j < e1; ++j) {
       const int4 sl = __ldg(m.ne4 + j);
       const int jj = j - e0;
@@ -389,8 +400,8 @@ __device__ __forceinline__ void seg_node_limit(const Inst& in, int64_t si, bool 
 #pragma unroll
       for (int l = 0; l < LPT; ++l) {
         const int kc = kclamp(k0 + l, L);
-        const bool wet = (fl_[l] >> (kSlotWet + jj)) & 1ull;
-        const bool on = (fl_[l] >> jj) & 1ull;
+        const bool wet = decltype(all_wet)::value || ((fl_[l] >> (kSlotWet + jj)) & 1ull);
+        const bool on = decltype(all_wet)::value || ((fl_[l] >> jj) & 1ull);
         double lv[NTR], tv[NTR], a[NTR];
         ldv<NTR, IL>(in.ws.lo, qo + uint32_t(kc), w0, sN, in.wtg, lv);
         ldv<NTR, IL>(in.T, qo + uint32_t(kc), t0, in.tstride, in.tg, tv);
@@ -405,6 +416,9 @@ __device__ __forceinline__ void seg_node_limit(const Inst& in, int64_t si, bool 
         }
       }
     }
+    };
+    if (run_all<LPT>(fl_, nk)) slots(AllWet{});
+    else slots(SomeDry{});
     // the node itself, and the padding of dry cells
 #pragma unroll
     for (int l = 0; l < LPT; ++l) {
@@ -524,6 +538,7 @@ __device__ __forceinline__ void seg_node_final(const Inst& in, int64_t si, int t
 #pragma unroll
   for (int l = 0; l < LPT; ++l) fl_[l] = l < nk ? __ldg(m.nflags + rec.w + (k0 + l - nzmin)) : 0ull;
   const int e0 = rec.x, e1 = rec.x + int((pk >> 16) & 255u);
+  auto slots = [&](auto all_wet) {
   for (int j = e0; j < e1; ++j) {
     const int4 sl = __ldg(m.ne4 + j);
     const int jj = j - e0;
@@ -533,7 +548,7 @@ __device__ __forceinline__ void seg_node_final(const Inst& in, int64_t si, int t
 #pragma unroll
     for (int l = 0; l < LPT; ++l) {
       const int kc = kclamp(k0 + l, L);
-      const bool on = (fl_[l] >> jj) & 1ull;
+      const bool on = decltype(all_wet)::value || ((fl_[l] >> jj) & 1ull);
       double a[NTR], pfo[NTR], mfo[NTR];
       ldv<NTR, IL>(in.ws.adfh, qe + uint32_t(kc), w0, in.ws.sEd, in.wtg, a);
       ldv<NTR, IL>(in.ws.pf, qo + uint32_t(kc), w0, sN, in.wtg, pfo);
@@ -550,6 +565,9 @@ __device__ __forceinline__ void seg_node_final(const Inst& in, int64_t si, int t
       }
     }
   }
+  };
+  if (run_all<LPT>(fl_, nk)) slots(AllWet{});
+  else slots(SomeDry{});
   const double dt = in.dt;
 #pragma unroll
   for (int l = 0; l < LPT; ++l) {
