@@ -643,6 +643,63 @@ def run_serve(args, D: Dist) -> dict:
     return out
 
 
+# ------------------------------------------------------- side measurements (default run)
+def run_side(args, D: Dist) -> dict:
+    """Short measurements of the other configurations beside the headline, so a default
+    run covers them: config 1 (pi, plain fct_forward, T and S, one step, u, v ~ N(0, 0.1),
+    T_old = T) with its parity against the C oracle and the oracle's own rate, and config 3
+    (the 10-step adjoint loss gradient on the CORE2-size mesh, its cost against the
+    forward; no FD directions here). Each takes a few seconds."""
+    import copy
+
+    import torch
+
+    from fesom_jax_b200 import inputs as I
+    from fesom_jax_b200.mesh import pi_mesh
+    from fesom_jax_b200.tracer_adv import get_plan
+    from oracle import fct_c
+    out = {}
+    dev = torch.device("cuda", D.local_rank)
+    m = pi_mesh()
+    f = I.make_fields(m, seed=0, kind="white", sigma=0.1)
+    d = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev)  # noqa: E731
+    a = [d(x) for x in (f.uv, f.w_e, f.helem, f.hnode, f.hnode_new, f.tracers, f.tracers_old)]
+    plan = get_plan(m, D.local_rank)
+    outb = torch.empty_like(a[5])
+    for _ in range(20):
+        plan.forward(*a, 3600.0, out=outb)
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 500
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        plan.forward(*a, 3600.0, out=outb)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3 / reps
+    got = outb.cpu().numpy()
+    lm = m.node_layer_mask
+    worst, t_cpu = 0.0, 0.0
+    for tr in range(2):
+        c0 = time.perf_counter()
+        ref, _ = fct_c.advect_one_fct(m, f.uv, f.w_e, f.helem, f.hnode, f.hnode_new,
+                                      f.tracers[tr], f.tracers_old[tr], dt=3600.0)
+        t_cpu += time.perf_counter() - c0
+        worst = max(worst, float(np.max(np.abs(got[tr][lm] - ref[lm])) / np.max(np.abs(ref[lm]))))
+    upd = 2 * m.n_wet_layers
+    out["pi_plain"] = dict(value=upd / t, unit=UNIT, ms_per_step=t * 1e3, max_rel_err=worst,
+                           cpu_value=upd / t_cpu, cpu_cores=fct_c.max_threads(),
+                           how="fct_forward, T and S in one call, one FCT step, dt 3600")
+    a2 = copy.copy(args)
+    a2.no_fd, a2.steps, a2.warmup = True, 2, 1
+    r = run_adjoint(a2, D)["adjoint"]
+    out["adjoint"] = {k: r[k] for k in ("forward_ms", "loss_and_grad_ms", "ratio", "K",
+                                        "checkpoint", "recompute_loss_and_grad_ms",
+                                        "recompute_ratio", "tape_equals_recompute")}
+    return out
+
+
 # ------------------------------------------------------------------ reference arm
 def run_reference(args, D: Dist):
     """CPU arm: the C restatement of the reference algorithm on the box's host cores
@@ -744,6 +801,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fd", action="store_true", help="adjoint: skip the FD check")
+    ap.add_argument("--no-side", action="store_true",
+                    help="batched: skip the side measurements of the pi and adjoint configs")
     ap.add_argument("--no-gates", action="store_true",
                     help="skip the per-run correctness gates (oracle parity, closure, window)")
     ap.add_argument("--node-order", choices=["rcm", "raw", "random"], default="rcm",
@@ -771,6 +830,8 @@ def main():
             r = run_serve(args, D)
         else:
             r = run_ours(args, D)
+            if r is not None and args.config == "batched" and D.world == 1 and not args.no_side:
+                r["side"] = run_side(args, D)
     finally:
         D.close()
     if D.rank != 0 or r is None:
@@ -789,7 +850,7 @@ def main():
                 clocks=r["clocks"], gpu_launches=r["gpu_launches"],
                 fct_step_ms=r["fct_step_ms"], stage_ms=r["prof"], finite=r["finite"],
                 nonfinite=r["nonfinite"], gates=r["gates"], batch=r["info"], tuning=r["tuning"])
-    for k in ("plain", "e2e", "cpu_baseline"):
+    for k in ("plain", "e2e", "cpu_baseline", "side"):
         if k in r:
             line[k] = r[k]
     failed = not r["finite"] or (r["gates"] is not None and not r["gates"]["passed"])
