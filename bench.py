@@ -382,6 +382,8 @@ def run_ours(args, D: Dist) -> dict | None:
         from fesom_jax_b200.tracer_adv import get_plan
         inp = member_inputs[0]
         plan = get_plan(mesh, D.local_rank)
+        plan.autotune([inp[k] for k in ("uv", "w_e", "helem", "hnode", "hnode_new")] +
+                      [inp["T"][0], inp["T_old"][0]], cfg["dt"], reps=3)
         outb = torch.empty_like(inp["T"][0])
         for _ in range(2):
             plan.forward(inp["uv"], inp["w_e"], inp["helem"], inp["hnode"], inp["hnode_new"],
@@ -665,6 +667,7 @@ def run_side(args, D: Dist) -> dict:
     d = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev)  # noqa: E731
     a = [d(x) for x in (f.uv, f.w_e, f.helem, f.hnode, f.hnode_new, f.tracers, f.tracers_old)]
     plan = get_plan(m, D.local_rank)
+    tune = plan.autotune(a, 3600.0)
     outb = torch.empty_like(a[5])
     for _ in range(20):
         plan.forward(*a, 3600.0, out=outb)
@@ -690,6 +693,7 @@ def run_side(args, D: Dist) -> dict:
     upd = 2 * m.n_wet_layers
     out["pi_plain"] = dict(value=upd / t, unit=UNIT, ms_per_step=t * 1e3, max_rel_err=worst,
                            cpu_value=upd / t_cpu, cpu_cores=fct_c.max_threads(),
+                           tuning_ms=tune,
                            how="fct_forward, T and S in one call, one FCT step, dt 3600")
     a2 = copy.copy(args)
     a2.no_fd, a2.steps, a2.warmup = True, 2, 1

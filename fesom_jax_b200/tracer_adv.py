@@ -97,6 +97,30 @@ class FctPlan:
         _lib.check(L.fct_plan_set_mapping(self._h, int(tracers_per_thread),
                                           int(levels_per_thread)))
 
+    def autotune(self, args, dt: float, candidates=((1, 1), (1, 2), (1, 4), (2, 1), (2, 2),
+                                                    (2, 4)), reps: int = 20) -> dict:
+        """Time ``forward(*args, dt)`` (device tensors, the call to be tuned for) under each
+        (tracers, levels) per-thread mapping and keep the fastest; returns ``{"TxL": ms}``."""
+        torch = _torch()
+        dev = torch.device("cuda", self.device)
+        stream = torch.cuda.current_stream(dev)
+        out = torch.empty_like(args[5])
+        times = {}
+        for c, lv in candidates:
+            self.set_mapping(c, lv)
+            for _ in range(3):
+                self.forward(*args, dt, out=out)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                self.forward(*args, dt, out=out)
+            e1.record(stream)
+            e1.synchronize()
+            times[(c, lv)] = e0.elapsed_time(e1) / reps
+        best = min(times, key=times.get)
+        self.set_mapping(*best)
+        return {f"{c}x{lv}": v for (c, lv), v in times.items()}
+
     def set_fused(self, fused: bool) -> None:
         """Fused stage kernels (default) or one kernel per reference stage; same bits."""
         _lib.check(_lib.lib().fct_plan_set_fused(self._h, int(bool(fused))))
