@@ -436,9 +436,6 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
       }
       f |= (unsigned long long)(own) << kOwnBit;
       f |= (unsigned long long)(off) << kOffBit;
-      const unsigned long long slots = (1ull << ed) - 1ull;
-      const bool all = (f & slots) == slots && ((f >> kSlotWet) & slots) == slots && !off;
-      f |= (unsigned long long)(all) << kAllBit;
       nflags.push_back(f);
     }
   }

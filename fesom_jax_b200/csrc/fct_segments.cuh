@@ -27,7 +27,6 @@
 #pragma once
 
 #include <algorithm>
-#include <type_traits>
 
 #include "fct_device.cuh"
 
@@ -49,19 +48,6 @@ __device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : 
 __device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : b; }
 // AB2 extrapolation ttfAB = -0.6*T_old + 1.6*T (tracer_adv.py:59-66)
 __device__ __forceinline__ double ab2f(double T, double To) { return fma(kAbNew, T, kAbOld * To); }
-
-// Every level of the run has all its edge slots counted and wet and no dry cell (the
-// common case away from coasts and bathymetry steps): the slot loops then take a body
-// without the per-slot selects (``std::integral_constant`` picks it at compile time).
-template <int LPT>
-__device__ __forceinline__ bool run_all(const unsigned long long (&fl)[LPT], int nk) {
-  bool all = true;
-#pragma unroll
-  for (int l = 0; l < LPT; ++l) all = all && (l >= nk || ((fl[l] >> kAllBit) & 1ull));
-  return all;
-}
-using AllWet = std::integral_constant<bool, true>;
-using SomeDry = std::integral_constant<bool, false>;
 
 // a level clamped into [0, L - 1]: loads at clamped levels are in bounds and their values
 // are discarded by the predicates that follow
@@ -100,34 +86,30 @@ __device__ __forceinline__ void seg_node_lo(const Inst& in, int64_t si, int t0, 
 #pragma unroll
   for (int l = 0; l < LPT; ++l) fl_[l] = l < nk ? __ldg(m.nflags + rec.w + (k0 + l - nzmin)) : 0ull;
   const int e0 = rec.x, e1 = rec.x + int((pk >> 16) & 255u);
-  auto slots = [&](auto all_wet) {
-    for (int j = e0; j < e1; ++j) {
-      const int4 sl = __ldg(m.ne4 + j);
-      const int jj = j - e0;
-      const bool second = sl.x & 1;
-      const double sg1 = second ? -1.0 : 1.0;   // the flux leaves the edge's first node
-      const uint32_t qe = lq(sl.x >> 1, L, 0), qo = lq(sl.y, L, 0);
+  for (int j = e0; j < e1; ++j) {
+    const int4 sl = __ldg(m.ne4 + j);
+    const int jj = j - e0;
+    const bool second = sl.x & 1;
+    const double sg1 = second ? -1.0 : 1.0;   // the flux leaves the edge's first node
+    const uint32_t qe = lq(sl.x >> 1, L, 0), qo = lq(sl.y, L, 0);
 #pragma unroll
-      for (int l = 0; l < LPT; ++l) {
-        const int kc = kclamp(k0 + l, L);
-        const bool on = decltype(all_wet)::value || ((fl_[l] >> jj) & 1ull);
-        const double vf = __ldg(in.ws.vflux + qe + kc);
-        const double avf = fabs(vf);
-        // the reference's face flux -0.5*(T1*(vf+|vf|) + T2*(vf-|vf|)) with the node's own
-        // value first (a + b == b + a exactly): the same bits for either end of the edge
-        const double cown = second ? vf - avf : vf + avf, coth = second ? vf + avf : vf - avf;
-        double To[NTR];
-        ldv<NTR, IL>(in.T, qo + uint32_t(kc), t0, ts, tg, To);
+    for (int l = 0; l < LPT; ++l) {
+      const int kc = kclamp(k0 + l, L);
+      const bool on = ((fl_[l] >> jj) & 1ull);
+      const double vf = __ldg(in.ws.vflux + qe + kc);
+      const double avf = fabs(vf);
+      // the reference's face flux -0.5*(T1*(vf+|vf|) + T2*(vf-|vf|)) with the node's own
+      // value first (a + b == b + a exactly): the same bits for either end of the edge
+      const double cown = second ? vf - avf : vf + avf, coth = second ? vf + avf : vf - avf;
+      double To[NTR];
+      ldv<NTR, IL>(in.T, qo + uint32_t(kc), t0, ts, tg, To);
 #pragma unroll
-        for (int t = 0; t < NTR; ++t) {
-          const double f = -0.5 * fma(Tw[l + 2][t], cown, To[t] * coth);
-          div[l][t] = on ? div[l][t] + sg1 * f : div[l][t];
-        }
+      for (int t = 0; t < NTR; ++t) {
+        const double f = -0.5 * fma(Tw[l + 2][t], cown, To[t] * coth);
+        div[l][t] = on ? div[l][t] + sg1 * f : div[l][t];
       }
     }
-  };
-  if (run_all<LPT>(fl_, nk)) slots(AllWet{});
-  else slots(SomeDry{});
+  }
 
   // upwind vertical flux at the interfaces k0 .. k0+LPT (layer-masked, tracer_adv.py:108-120)
   double fv[LPT + 1][NTR];
@@ -391,34 +373,30 @@ __device__ __forceinline__ void seg_node_limit(const Inst& in, int64_t si, bool 
     for (int l = 0; l < LPT; ++l)
       fl_[l] = l < nk ? __ldg(m.nflags + rec.w + (k0 + l - nzmin)) : 0ull;
     const int e0 = rec.x, e1 = rec.x + int((pk >> 16) & 255u);
-    auto slots = [&](auto all_wet) {
-      for (int j = e0; j < e1; ++j) {
-        const int4 sl = __ldg(m.ne4 + j);
-        const int jj = j - e0;
-        const double sg1 = (sl.x & 1) ? -1.0 : 1.0;   // adf_h leaves the edge's first node
-        const uint32_t qo = lq(sl.y, L, 0), qe = lq(sl.x >> 1, L, 0);
+    for (int j = e0; j < e1; ++j) {
+      const int4 sl = __ldg(m.ne4 + j);
+      const int jj = j - e0;
+      const double sg1 = (sl.x & 1) ? -1.0 : 1.0;   // adf_h leaves the edge's first node
+      const uint32_t qo = lq(sl.y, L, 0), qe = lq(sl.x >> 1, L, 0);
 #pragma unroll
-        for (int l = 0; l < LPT; ++l) {
-          const int kc = kclamp(k0 + l, L);
-          const bool wet = decltype(all_wet)::value || ((fl_[l] >> (kSlotWet + jj)) & 1ull);
-          const bool on = decltype(all_wet)::value || ((fl_[l] >> jj) & 1ull);
-          double lv[NTR], tv[NTR], a[NTR];
-          ldv<NTR, IL>(in.ws.lo, qo + uint32_t(kc), w0, sN, in.wtg, lv);
-          ldv<NTR, IL>(in.T, qo + uint32_t(kc), t0, in.tstride, in.tg, tv);
-          ldv<NTR, IL>(in.ws.adfh, qe + uint32_t(kc), w0, in.ws.sEd, in.wtg, a);
+      for (int l = 0; l < LPT; ++l) {
+        const int kc = kclamp(k0 + l, L);
+        const bool wet = ((fl_[l] >> (kSlotWet + jj)) & 1ull);
+        const bool on = ((fl_[l] >> jj) & 1ull);
+        double lv[NTR], tv[NTR], a[NTR];
+        ldv<NTR, IL>(in.ws.lo, qo + uint32_t(kc), w0, sN, in.wtg, lv);
+        ldv<NTR, IL>(in.T, qo + uint32_t(kc), t0, in.tstride, in.tg, tv);
+        ldv<NTR, IL>(in.ws.adfh, qe + uint32_t(kc), w0, in.ws.sEd, in.wtg, a);
 #pragma unroll
-          for (int t = 0; t < NTR; ++t) {
-            mx[l][t] = wet ? dmax(mx[l][t], dmax(lv[t], tv[t])) : mx[l][t];
-            mn[l][t] = wet ? dmin(mn[l][t], dmin(lv[t], tv[t])) : mn[l][t];
-            const double sv = sg1 * a[t];
-            sp[l][t] = on ? sp[l][t] + dmax(sv, 0.0) : sp[l][t];
-            sm[l][t] = on ? sm[l][t] + dmin(sv, 0.0) : sm[l][t];
-          }
+        for (int t = 0; t < NTR; ++t) {
+          mx[l][t] = wet ? dmax(mx[l][t], dmax(lv[t], tv[t])) : mx[l][t];
+          mn[l][t] = wet ? dmin(mn[l][t], dmin(lv[t], tv[t])) : mn[l][t];
+          const double sv = sg1 * a[t];
+          sp[l][t] = on ? sp[l][t] + dmax(sv, 0.0) : sp[l][t];
+          sm[l][t] = on ? sm[l][t] + dmin(sv, 0.0) : sm[l][t];
         }
       }
-    };
-    if (run_all<LPT>(fl_, nk)) slots(AllWet{});
-    else slots(SomeDry{});
+    }
     // the node itself, and the padding of dry cells
 #pragma unroll
     for (int l = 0; l < LPT; ++l) {
@@ -538,36 +516,32 @@ __device__ __forceinline__ void seg_node_final(const Inst& in, int64_t si, int t
 #pragma unroll
   for (int l = 0; l < LPT; ++l) fl_[l] = l < nk ? __ldg(m.nflags + rec.w + (k0 + l - nzmin)) : 0ull;
   const int e0 = rec.x, e1 = rec.x + int((pk >> 16) & 255u);
-  auto slots = [&](auto all_wet) {
-    for (int j = e0; j < e1; ++j) {
-      const int4 sl = __ldg(m.ne4 + j);
-      const int jj = j - e0;
-      const bool second = sl.x & 1;
-      const double sg1 = second ? -1.0 : 1.0;   // adf_h leaves the edge's first node
-      const uint32_t qo = lq(sl.y, L, 0), qe = lq(sl.x >> 1, L, 0);
+  for (int j = e0; j < e1; ++j) {
+    const int4 sl = __ldg(m.ne4 + j);
+    const int jj = j - e0;
+    const bool second = sl.x & 1;
+    const double sg1 = second ? -1.0 : 1.0;   // adf_h leaves the edge's first node
+    const uint32_t qo = lq(sl.y, L, 0), qe = lq(sl.x >> 1, L, 0);
 #pragma unroll
-      for (int l = 0; l < LPT; ++l) {
-        const int kc = kclamp(k0 + l, L);
-        const bool on = decltype(all_wet)::value || ((fl_[l] >> jj) & 1ull);
-        double a[NTR], pfo[NTR], mfo[NTR];
-        ldv<NTR, IL>(in.ws.adfh, qe + uint32_t(kc), w0, in.ws.sEd, in.wtg, a);
-        ldv<NTR, IL>(in.ws.pf, qo + uint32_t(kc), w0, sN, in.wtg, pfo);
-        ldv<NTR, IL>(in.ws.mf, qo + uint32_t(kc), w0, sN, in.wtg, mfo);
+    for (int l = 0; l < LPT; ++l) {
+      const int kc = kclamp(k0 + l, L);
+      const bool on = ((fl_[l] >> jj) & 1ull);
+      double a[NTR], pfo[NTR], mfo[NTR];
+      ldv<NTR, IL>(in.ws.adfh, qe + uint32_t(kc), w0, in.ws.sEd, in.wtg, a);
+      ldv<NTR, IL>(in.ws.pf, qo + uint32_t(kc), w0, sN, in.wtg, pfo);
+      ldv<NTR, IL>(in.ws.mf, qo + uint32_t(kc), w0, sN, in.wtg, mfo);
 #pragma unroll
-        for (int t = 0; t < NTR; ++t) {
-          // b3 (tracer_adv.py:461-465): adf >= 0 ? min(plus(n1), minus(n2)) : min(minus(n1),
-          // plus(n2)); min is exact and symmetric, so in the node's own terms the factor is
-          // min(own plus, other minus) when the flux leaves the node, else the other pair
-          const double x1 = dmin(pfw[l + 1][t], mfo[t]), x2 = dmin(mfw[l + 1][t], pfo[t]);
-          const double ae = ((a[t] >= 0.0) != second) ? x1 : x2;
-          const double lim = ae * a[t];
-          hsc[l][t] = on ? hsc[l][t] + sg1 * lim : hsc[l][t];
-        }
+      for (int t = 0; t < NTR; ++t) {
+        // b3 (tracer_adv.py:461-465): adf >= 0 ? min(plus(n1), minus(n2)) : min(minus(n1),
+        // plus(n2)); min is exact and symmetric, so in the node's own terms the factor is
+        // min(own plus, other minus) when the flux leaves the node, else the other pair
+        const double x1 = dmin(pfw[l + 1][t], mfo[t]), x2 = dmin(mfw[l + 1][t], pfo[t]);
+        const double ae = ((a[t] >= 0.0) != second) ? x1 : x2;
+        const double lim = ae * a[t];
+        hsc[l][t] = on ? hsc[l][t] + sg1 * lim : hsc[l][t];
       }
     }
-  };
-  if (run_all<LPT>(fl_, nk)) slots(AllWet{});
-  else slots(SomeDry{});
+  }
   const double dt = in.dt;
 #pragma unroll
   for (int l = 0; l < LPT; ++l) {
