@@ -315,9 +315,12 @@ def run_ours(args, D: Dist) -> dict | None:
     info = ens.info()
     S = cfg["fct_steps"]
     stream = torch.cuda.current_stream(dev)
-    fixed = bool(args.chunk or args.levels)
+    fixed = bool(args.chunk or args.levels or args.stage_mapping)
     tune = ens.autotune(steps=2) if not fixed else None
-    if fixed:
+    if args.stage_mapping:
+        for st, m in enumerate(parse_stage_mapping(args.stage_mapping)):
+            ens.set_stage_mapping(st, *m)
+    elif fixed:
         ens.set_mapping(args.chunk or ens.chunk, args.levels or ens.levels)
     torch.cuda.synchronize()
     for _ in range(args.warmup):
@@ -781,6 +784,14 @@ def workload_config(name, cfg, mesh) -> dict:
                 parallelism="replicas: members per GPU, no collective")
 
 
+def parse_stage_mapping(text):
+    """'4x2,2x2,2x1,4x1' -> [(4, 2), (2, 2), (2, 1), (4, 1)] (one pair per fused stage)."""
+    out = [tuple(int(v) for v in part.split("x")) for part in text.split(",")]
+    if len(out) != 4 or any(len(m) != 2 for m in out):
+        raise SystemExit(f"--stage-mapping wants four TRACERSxLEVELS pairs, got {text!r}")
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -800,6 +811,9 @@ def main():
                     help="fix the tracers per thread (no autotune)")
     ap.add_argument("--levels", type=int, default=0,
                     help="fix the levels per thread (no autotune)")
+    ap.add_argument("--stage-mapping", default="",
+                    help="fix the mapping stage by stage (no autotune): tracers x levels per "
+                         "thread for LO, edge, limiter, final, e.g. 4x2,2x2,2x1,4x1")
     ap.add_argument("--workspace-gb", type=float, default=40.0)
     ap.add_argument("--e2e-members", type=int, default=8)
     ap.add_argument("--no-e2e", action="store_true")
