@@ -33,16 +33,17 @@ sys.path.insert(0, str(ROOT))
 METRIC = "FCT node-level updates/s FP64, batched vs plain on 1 B200; serve p50/p99 ms"
 UNIT = "node-level updates/s"
 FALLBACK_HBM_GBS = 6650.0
-# DRAM bytes (read + write) per node-level update of the four fused tracer kernels, from
-# one ncu capture of the small case of the batched workload (2 members x 8 tracers of the
-# CORE2-size mesh: 12.81 GB per FCT step / 48.76 M updates); the tracer-independent volume
-# flux kernel (1.9% of the step) is not included. Scaled to a launch by the updates it does.
-TRAFFIC_B_PER_UPDATE = 262.6
-# Warp-instructions per node-level update of the same four kernels in the same capture
+# DRAM bytes (read + write) per node-level update of the six kernels of the fused FCT step
+# (volume fluxes, LO, edge fluxes and their node-gradient lanes, limiter, final), from one
+# ncu capture of the small case of the batched workload (2 members x 8 tracers of the
+# CORE2-size mesh: 12.35 GB per FCT step / 48.76 M updates). Scaled to a launch by the
+# updates it does.
+TRAFFIC_B_PER_UPDATE = 253.4
+# Warp-instructions per node-level update of the same six kernels in the same capture
 # (smsp__inst_executed.sum / updates). The kernels are latency- and issue-limited rather
 # than HBM-bound, so the line also reports this issue-rate fraction beside the HBM one:
 # achieved warp-instructions/s against 148 SMs x 4 schedulers x the sampled SM clock.
-WARP_INST_PER_UPDATE = 99.2
+WARP_INST_PER_UPDATE = 40.5
 B200_SMS, SCHEDULERS_PER_SM = 148, 4
 
 
@@ -57,9 +58,7 @@ def peaks() -> dict:
 def issue_roofline(updates_per_s: float, clk) -> dict:
     """Instruction-issue fraction of the batched step: warp-instructions per update (ncu
     capture constant) x updates/s against every scheduler issuing one per cycle at the
-    median SM clock sampled in the timed region (max clock when unsampled). The step
-    time includes the tracer-independent volume-flux kernel, so this is a slight
-    underestimate."""
+    median SM clock sampled in the timed region (max clock when unsampled)."""
     mhz = (clk or {}).get("sm_mhz") or (clk or {}).get("sm_max_mhz") or 1965.0
     peak = B200_SMS * SCHEDULERS_PER_SM * float(mhz) * 1e6 / 1e9
     achieved = WARP_INST_PER_UPDATE * updates_per_s / 1e9
@@ -366,11 +365,12 @@ def run_ours(args, D: Dist) -> dict | None:
     out = dict(value=value, t=t, info=info, clocks=clk, prof=prof, fct_step_ms=fct_step_ms,
                finite=finite, nonfinite=int(sum(nonfinite)), gates=gates, mesh=mesh, cfg=cfg,
                alg_bytes=alg,
-               roofline=dict(bound="hbm", kernel="fused FCT step (vflux, node_lo, edge_adf, node_limit, node_final)",
+               roofline=dict(bound="hbm", kernel="fused FCT step (k_vflux, k_seg_lo, k_seg_edge, "
+                                                 "k_edge_fix, k_seg_limit, k_seg_final)",
                              achieved=achieved, peak=pk["hbm_gbs"], unit="GB/s",
                              frac=achieved / pk["hbm_gbs"], peak_source=pk["source"],
                              traffic=TRAFFIC_B_PER_UPDATE * info["updates_per_step"],
-                             traffic_note="ncu DRAM bytes of the 4 tracer kernels, small-case "
+                             traffic_note="ncu DRAM bytes of the step's 6 kernels, small-case "
                                           "capture scaled by updates",
                              alg_bytes_per_step=alg,
                              issue=issue_roofline(value / D.world, clk)),
@@ -508,13 +508,10 @@ def run_adjoint(args, D: Dist) -> dict:
     steps on the CORE2-size mesh, w.r.t. the initial T and uv, with w_e = compute_w(uv)
     inside the loss (chain_loss_and_grad with a forward tape; the per-step recomputation
     variant is timed beside it). Reports its cost against the forward alone (compute_w +
-    K steps) and central finite differences (eps = 1e-7) along 20 seeded directions (10
-    for T0, 10 for uv).
+    K steps), a dot-product test of the T gradients and a Taylor test of the uv gradient.
 
-    The velocities here are white noise (sigma 0.002 m/s, vertical CFL < 1): a
-    streamfunction flow is
-    discretely divergence-free, so w = compute_w(uv) is roundoff and the upwind |w| sits
-    at its kink, where central differences and any subgradient disagree."""
+    The velocities here are white noise (sigma 0.002 m/s, vertical CFL < 1), so w is far
+    from the upwind kink at 0 and the gradient is taken at a differentiable point."""
     import torch
 
     from fesom_jax_b200 import inputs as I
@@ -570,29 +567,33 @@ def run_adjoint(args, D: Dist) -> dict:
     if other:
         _, gT0_rc, guv_rc = grad(other)
         same_bits = bool(torch.equal(gT0, gT0_rc) and torch.equal(guv, guv_rc))
-    # central finite differences
-    rng = np.random.default_rng(2024)
-    lm = torch.from_numpy(mesh.node_layer_mask).to(dev)
-    em = torch.from_numpy(mesh.elem_layer_mask).to(dev)[:, :, None]
-    rel = []
-    eps = 1e-7
-    for j in range(0 if args.no_fd else 20):
-        if j < 10:
-            v = d(rng.normal(size=T0.shape)) * lm
-            Lp = chain_loss_and_grad(mesh, T0 + eps * v, uv, helem, hn, hnn, target, K, dt=dt,
+    # gradient checks that hold at this size (central differences are lost in the
+    # round-off of a ~1e15 loss): (1) a dot-product test along x = (T0, T_old0): the K-step
+    # map is positively homogeneous of degree 1 in its tracer inputs, so its tangent along
+    # x is T_K itself and <gT0, T0> + <gT_old0, T_old0> = <dL/dT_K, T_K>; (2) a Taylor test
+    # in uv: r(h) = |L(uv + h v) - L - h <guv, v>| falls as h^2 for the right gradient
+    checks = None
+    if not args.no_fd:
+        _, gT, gU, gTo = chain_loss_and_grad(mesh, T0, uv, helem, hn, hnn, target, K, dt=dt,
+                                             T_old0=To0, checkpoint=main_mode,
+                                             return_gT_old=True)
+        TK = forward()[:, 0]
+        av0 = torch.from_numpy(mesh.areasvol[:, 0].copy()).to(dev)
+        terms = 2.0 * av0 * (TK - target.to(dev)) * TK
+        lhs = float((gT * T0).sum() + (gTo * To0).sum())
+        rhs = float(terms.sum())
+        em = torch.from_numpy(mesh.elem_layer_mask).to(dev)[:, :, None]
+        v = d(np.random.default_rng(11).normal(0.0, 0.002, uv.shape)) * em
+        gv = float((gU * v).sum())
+        rem = {}
+        for h in (1e-1, 1e-2):
+            Lh = chain_loss_and_grad(mesh, T0, uv + h * v, helem, hn, hnn, target, K, dt=dt,
                                      T_old0=To0, checkpoint=main_mode)[0]
-            Lm = chain_loss_and_grad(mesh, T0 - eps * v, uv, helem, hn, hnn, target, K, dt=dt,
-                                     T_old0=To0, checkpoint=main_mode)[0]
-            ad = float((gT0 * v).sum())
-        else:
-            v = d(rng.normal(size=uv.shape)) * em
-            Lp = chain_loss_and_grad(mesh, T0, uv + eps * v, helem, hn, hnn, target, K, dt=dt,
-                                     T_old0=To0, checkpoint=main_mode)[0]
-            Lm = chain_loss_and_grad(mesh, T0, uv - eps * v, helem, hn, hnn, target, K, dt=dt,
-                                     T_old0=To0, checkpoint=main_mode)[0]
-            ad = float((guv * v).sum())
-        fd = (Lp - Lm) / (2 * eps)
-        rel.append(abs(fd - ad) / max(abs(ad), 1e-300))
+            rem[h] = abs(Lh - loss - h * gv)
+        checks = dict(dot_T_rel_err=abs(lhs - rhs) / float(terms.abs().sum()),
+                      taylor_uv=dict(h=[1e-1, 1e-2], remainder=[rem[1e-1], rem[1e-2]],
+                                     first_order=[abs(1e-1 * gv), abs(1e-2 * gv)],
+                                     order=float(np.log10(rem[1e-1] / max(rem[1e-2], 1e-300)))))
     upd = K * mesh.n_wet_layers * D.world
     return dict(value=upd / t, t=t * args.steps, mesh=mesh, t_fwd=t_fwd, t_grad=t_grad,
                 cfg=dict(members=1, ntr=1, fct_steps=K, dt=dt),
@@ -602,9 +603,7 @@ def run_adjoint(args, D: Dist) -> dict:
                              recompute_loss_and_grad_ms=(t_grad_rc * 1e3 if other else None),
                              recompute_ratio=(t_grad_rc / t_fwd if other else None),
                              tape_equals_recompute=same_bits,
-                             fd_rel_err_max=float(max(rel)) if rel else None,
-                             fd_rel_err_median=float(np.median(rel)) if rel else None,
-                             fd_directions=len(rel), fd_eps=eps, max_cfl_z=float(I.max_cfl_z(
+                             gradient_checks=checks, max_cfl_z=float(I.max_cfl_z(
                                  mesh, f.w_e, f.hnode, dt)),
                              how="chain_loss_and_grad (forward x K with the chosen "
                                  "checkpointing, fct_adjoint_ex x K, fct_compute_w_adjoint) vs "
@@ -654,7 +653,7 @@ def run_side(args, D: Dist) -> dict:
     run covers them: config 1 (pi, plain fct_forward, T and S, one step, u, v ~ N(0, 0.1),
     T_old = T) with its parity against the C oracle and the oracle's own rate, and config 3
     (the 10-step adjoint loss gradient on the CORE2-size mesh, its cost against the
-    forward; no FD directions here). Each takes a few seconds."""
+    forward; no gradient checks here). Each takes a few seconds."""
     import copy
 
     import torch
@@ -818,7 +817,8 @@ def main():
     ap.add_argument("--e2e-members", type=int, default=8)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--no-fd", action="store_true", help="adjoint: skip the FD check")
+    ap.add_argument("--no-checks", "--no-fd", dest="no_fd", action="store_true",
+                    help="adjoint: skip the gradient checks (dot-product and Taylor tests)")
     ap.add_argument("--no-side", action="store_true",
                     help="batched: skip the side measurements of the pi and adjoint configs")
     ap.add_argument("--no-gates", action="store_true",

@@ -264,7 +264,8 @@ def _tape_fits(torch, mesh: Mesh, steps: int, dev) -> bool:
 
 
 def chain_loss_and_grad(mesh: Mesh, T0, uv, helem, hnode, hnode_new, target, steps: int, *,
-                        dt: float, T_old0=None, checkpoint: str = "auto"):
+                        dt: float, T_old0=None, checkpoint: str = "auto",
+                        return_gT_old: bool = False):
     """Loss ``sum_n areasvol[n,0] * (T_K[n,0] - target_n)^2`` after ``steps`` FCT steps
     with ``w_e = compute_w(uv)`` inside the loss, and its gradients w.r.t. the initial
     ``T0`` and ``uv``. ``checkpoint``: ``"tape"`` keeps every step's intermediates
@@ -272,7 +273,9 @@ def chain_loss_and_grad(mesh: Mesh, T0, uv, helem, hnode, hnode_new, target, ste
     inside its adjoint call, ``"auto"`` takes the tape when it fits in half the free
     memory. The cotangents are accumulated in place (``fct_adjoint_ex``).
 
-    Returns ``(loss, gT0, guv)``; ``T_old0`` defaults to ``T0`` (step-1 convention)."""
+    Returns ``(loss, gT0, guv)``; ``T_old0`` defaults to ``T0`` (step-1 convention), and
+    then ``gT0`` is the gradient through both inputs. With ``return_gT_old`` and an explicit
+    ``T_old0`` the gradient w.r.t. ``T_old0`` is appended: ``(loss, gT0, guv, gT_old0)``."""
     torch = _torch()
     from .ale import compute_w
     dev = T0.device
@@ -317,4 +320,8 @@ def chain_loss_and_grad(mesh: Mesh, T0, uv, helem, hnode, hnode_new, target, ste
     finally:
         if tape is not None:
             tape.close()
+    if return_gT_old:
+        if T_old0 is None:
+            raise ValueError("return_gT_old needs an explicit T_old0")
+        return loss, gT0, guv, carry
     return loss, gT0, guv

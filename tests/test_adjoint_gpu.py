@@ -267,3 +267,74 @@ def test_tape_equals_recompute_on_cavity(torch, pi):
     wtop = f.w_e[nodes, ks + 1]
     assert np.any((got != seed) & (wtop < 0))
     assert np.all(got[wtop > 0] == seed[wtop > 0] + 0.0)
+
+
+def _core2_chain_inputs(torch):
+    from fesom_jax_b200 import workloads as W
+    mesh = W.make_workload_mesh("batched", seed=0)
+    f = I.make_fields(mesh, seed=3, ab2=True, kind="white", sigma=0.002)
+    d = [_d(torch, x) for x in (f.tracers[0], f.tracers_old[0], f.uv, f.helem, f.hnode,
+                                f.hnode_new)]
+    target = torch.from_numpy(np.random.default_rng(7).normal(15.0, 3.0, mesh.nod2D))
+    return mesh, f, d, target
+
+
+def test_chain_grad_dot_product_core2(torch):
+    """Dot-product test of the 10-step reverse pass on the CORE2-size mesh (126,990 nodes,
+    48 levels) against the oracle's tangent along x = (T0, T_old0).
+
+    The FCT step is positively homogeneous of degree 1 in its tracer inputs: the LO and HO
+    fluxes are linear in T, the limiter's bounds are max/min of T-linear values and its
+    factors are ratios of T-linear values (the 1e-16 ratio guard and the +-1e3 pads below
+    a cell's bottom never decide a max/min for these fields), and every subgradient
+    convention (equal split at ties, abs'(0) = 0) is a convex combination of degree-1
+    branches. So the tangent of the K-step map along x is the trajectory itself,
+    J x = T_K, and for L = sum_n a_n (T_K[n,0] - target_n)^2 the identity
+
+        <gT0, T0> + <gT_old0, T_old0> = sum_n 2 a_n (T_K[n,0] - target_n) T_K[n,0]
+
+    holds exactly; T_K comes from 10 steps of the C oracle. (Central differences at this
+    size are lost in the round-off of a loss near 1e15.)"""
+    from fesom_jax_b200.adjoint import chain_loss_and_grad
+    from fesom_jax_b200.ale import compute_w
+    from oracle import fct_c
+    mesh, f, (T0, To0, uv, helem, hn, hnn), target = _core2_chain_inputs(torch)
+    K, dt = 10, 1800.0
+    loss, gT0, guv, gTo0 = chain_loss_and_grad(mesh, T0, uv, helem, hn, hnn, target, K,
+                                               dt=dt, T_old0=To0, return_gT_old=True)
+    lhs = float((gT0 * T0).sum() + (gTo0 * To0).sum())
+    w = compute_w(mesh, uv, helem).cpu().numpy()
+    T, To = f.tracers[0], f.tracers_old[0]
+    for _ in range(K):
+        T, To = fct_c.advect_one_fct(mesh, f.uv, w, f.helem, f.hnode, f.hnode_new, T, To,
+                                     dt=dt)
+    terms = 2.0 * mesh.areasvol[:, 0] * (T[:, 0] - target.numpy()) * T[:, 0]
+    rhs = float(terms.sum())
+    assert abs(lhs - rhs) <= 1e-11 * float(np.abs(terms).sum()), (lhs, rhs)
+    assert abs(loss - float((mesh.areasvol[:, 0] * (T[:, 0] - target.numpy()) ** 2).sum())) \
+        <= 1e-11 * loss
+
+
+def test_chain_grad_uv_taylor_core2(torch):
+    """The uv gradient of the same 10-step loss on the CORE2-size mesh by a Taylor test:
+    along a seeded direction v (the size of uv), the remainder
+    r(h) = |L(uv + h v) - L(uv) - h <guv, v>| must fall as h^2 (second order: a wrong
+    gradient leaves a first-order remainder); kinks crossed by the perturbation (upwind
+    sign of w, limiter min/max switches) add O(h) x O(h) in expectation."""
+    from fesom_jax_b200.adjoint import chain_loss_and_grad
+    mesh, f, (T0, To0, uv, helem, hn, hnn), target = _core2_chain_inputs(torch)
+    K, dt = 10, 1800.0
+    L0, gT0, guv = chain_loss_and_grad(mesh, T0, uv, helem, hn, hnn, target, K, dt=dt,
+                                       T_old0=To0)
+    em = torch.from_numpy(mesh.elem_layer_mask).cuda()[:, :, None]
+    v = _d(torch, np.random.default_rng(11).normal(0.0, 0.002, uv.shape)) * em
+    gv = float((guv * v).sum())
+    r = {}
+    for h in (1e-1, 3e-2, 1e-2):
+        Lh = chain_loss_and_grad(mesh, T0, uv + h * v, helem, hn, hnn, target, K, dt=dt,
+                                 T_old0=To0)[0]
+        r[h] = abs(Lh - L0 - h * gv)
+        print(f"h={h:g} L(h)-L0={Lh - L0:.6e} h<g,v>={h * gv:.6e} r={r[h]:.3e}")
+    assert abs(gv) > 0
+    assert r[1e-2] <= 0.1 * abs(1e-2 * gv), r
+    assert r[1e-2] <= r[1e-1] / 30.0, r
