@@ -38,6 +38,7 @@ struct FctBatch {
   std::mutex graph_mu;
   std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
   cudaStream_t cap_stream = nullptr;
+  Fork fork{};   // the edge stage beside the LO stage (graph capture and fct_batch_step)
 };
 
 static int batch_launch_step(FctBatch* b, int phase, cudaStream_t s) {
@@ -182,8 +183,14 @@ int fct_batch_create(const FctInstance* insts, int n, int64_t budget, FctBatch**
   if (e == cudaSuccess)
     e = cudaMemcpy(B->d_tables, tab.data(), tab.size() * sizeof(Inst), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&B->cap_stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    if (prev >= 0) cudaSetDevice(prev);
+    return fail(cuda_error(e, "batch table setup"));
+  }
+  const int fst = fork_create(B->fork);
   if (prev >= 0) cudaSetDevice(prev);
-  if (e != cudaSuccess) return fail(cuda_error(e, "batch table setup"));
+  if (fst) return fail(fst);
+  for (auto& gr : B->groups) gr.dims.fork = &B->fork;
   for (auto& gr : B->groups)
     for (int p = 0; p < 3; ++p) gr.d_tab[p] = B->d_tables + size_t(p) * n + gr.first;
   *out = B;
@@ -197,6 +204,7 @@ int fct_batch_destroy(FctBatch* B) {
   cudaSetDevice(B->device);
   for (auto& kv : B->graphs) cudaGraphExecDestroy(kv.second);
   if (B->cap_stream) cudaStreamDestroy(B->cap_stream);
+  fork_destroy(B->fork);
   if (B->d_tables) cudaFree(B->d_tables);
   if (B->d_health) cudaFree(B->d_health);
   if (B->arena) cudaFree(B->arena);

@@ -781,6 +781,25 @@ const char* const kStageNames[kNumStages] = {
   } while (0)
 #define FCT_STAGE(name, lanes) FCT_SPLIT(FCT_STAGE_AS, name, lanes)
 
+// the fused step's edge stage beside its LO stage when the caller provides a fork
+constexpr bool kForkEdge = true;
+
+int fork_create(Fork& f) {
+  FCT_CUDA(cudaStreamCreateWithFlags(&f.side, cudaStreamNonBlocking));
+  for (auto& e : f.ev) FCT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  return FCT_OK;
+}
+
+void fork_destroy(Fork& f) {
+  if (f.side) {
+    cudaStreamSynchronize(f.side);
+    cudaStreamDestroy(f.side);
+  }
+  for (auto& e : f.ev)
+    if (e) cudaEventDestroy(e);
+  f = Fork{};
+}
+
 int launch_forward_events(const Inst& single, const Inst* tab, int n, const LaunchDims& d,
                           cudaStream_t s, cudaEvent_t* after, bool stop_before_final,
                           int chunk_sel) {
@@ -812,15 +831,28 @@ int launch_forward_events(const Inst& single, const Inst* tab, int n, const Laun
       // segment kernels (fct_seg_*.cu), 5 launches per chunk; the stages folded into
       // others record empty intervals (elem_grad: the node gradients are evaluated only
       // where MFCT needs them, in the edge stage; elem_bounds and node_cluster: the factors
-      // stage)
+      // stage). With a fork (and no stage timing) the edge stage runs on the side stream
+      // beside the LO stage and the limiter waits for both.
+      const Fork* fk = (kForkEdge && d.fork && !after) ? d.fork : nullptr;
       mark();
-      int st = launch_seg_lo(single, tab, n, d, c0, c1, s);
-      if (st) return st;
+      int st;
+      if (fk) {
+        FCT_CUDA(cudaEventRecord(fk->ev[0], s));
+        FCT_CUDA(cudaStreamWaitEvent(fk->side, fk->ev[0], 0));
+        if ((st = launch_seg_edge(single, tab, n, d, c0, c1, fk->side))) return st;
+        if ((st = launch_edge_fix(single, tab, n, d, c0, c1, fk->side))) return st;
+        FCT_CUDA(cudaEventRecord(fk->ev[1], fk->side));
+      }
+      if ((st = launch_seg_lo(single, tab, n, d, c0, c1, s))) return st;
       mark();
       if (d.any_wi) FCT_STAGE(k_vert_impl, d.max_nodes);
       mark();
-      if ((st = launch_seg_edge(single, tab, n, d, c0, c1, s))) return st;
-      if ((st = launch_edge_fix(single, tab, n, d, c0, c1, s))) return st;
+      if (fk) {
+        FCT_CUDA(cudaStreamWaitEvent(s, fk->ev[1], 0));
+      } else {
+        if ((st = launch_seg_edge(single, tab, n, d, c0, c1, s))) return st;
+        if ((st = launch_edge_fix(single, tab, n, d, c0, c1, s))) return st;
+      }
       mark();
       mark();
       mark();

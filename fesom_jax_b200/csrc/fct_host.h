@@ -58,7 +58,13 @@ struct LaunchDims {
   int64_t max_nseg[kSegVariants] = {0, 0, 0, 0};
   int64_t max_eseg[kSegVariants] = {0, 0, 0, 0};
   int64_t max_efix = 0;
+  // fused path: run the edge stage on fork->side beside the LO stage (null: one stream)
+  const Fork* fork = nullptr;
 };
+
+// Create / release a Fork on the current device.
+int fork_create(Fork& f);
+void fork_destroy(Fork& f);
 
 // Grow ``d``'s lane and segment counts to cover a plan's mesh.
 inline void dims_cover(LaunchDims& d, const FctPlan* P) {

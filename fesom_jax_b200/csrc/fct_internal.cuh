@@ -153,6 +153,15 @@ struct DevMesh {
   int64_t n_efix;
 };
 
+// A side stream and two events (fork, join) with which the fused step runs its edge stage
+// beside the LO stage: both read only the step's inputs and the volume fluxes, and they
+// write disjoint workspace fields (adf_h; LO and adf_v), so the two latency-bound kernels
+// can share the SMs. Owned by a plan or a batch and used under its lock.
+struct Fork {
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+};
+
 // Per-tracer intermediates of one instance (dense [entity, L]; tracer t at +t*stride).
 // Kernels read only entries written earlier in the same step (every reader masks by the
 // level range of the entity it reads), so a workspace needs no initial values and may be
@@ -256,5 +265,6 @@ struct FctPlan {
   int adj_tracers = 0;
   cudaStream_t adj_side = nullptr;  // reverse pass: kernels independent of the main chain
   cudaEvent_t adj_ev[5] = {};       //   and the events that fork and join it
+  fct::Fork fork{};                 // fused forward: the edge stage beside the LO stage
   fct::AdjWorkspace aws{};
 };

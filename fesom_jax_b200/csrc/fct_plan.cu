@@ -595,7 +595,7 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   FCT_CUDA(cudaMalloc(&P->d_health, sizeof(unsigned long long)));
   FCT_CUDA(cudaMemset(P->d_health, 0, sizeof(unsigned long long)));
   FCT_CUDA(cudaEventCreateWithFlags(&P->ws_ev, cudaEventDisableTiming));
-  return FCT_OK;
+  return fork_create(P->fork);
 }
 
 extern "C" {
@@ -619,6 +619,7 @@ int fct_plan_destroy(FctPlan* P) {
     cudaEventSynchronize(P->ws_ev);
     cudaEventDestroy(P->ws_ev);
   }
+  fork_destroy(P->fork);
   if (P->d_health) cudaFree(P->d_health);
   if (P->d_ws) cudaFree(P->d_ws);
   if (P->d_mesh) cudaFree(P->d_mesh);
@@ -767,6 +768,7 @@ int fct_forward_ex(FctPlan* P, const FctFields* f, double dt, int ntr, int flags
   dims.any_wi = f->w_i != nullptr;
   dims.copy_dry = true;   // a fresh T_new: dry levels keep T (tracer_adv.py:147-151)
   dims.fused = !stagewise;
+  dims.fork = &P->fork;   // used under the plan lock (PlanUse)
   int prev = -1;
   cudaGetDevice(&prev);
   if (prev != P->device) cudaSetDevice(P->device);
