@@ -332,12 +332,25 @@ class ServingEngine:
         done = [r for r in requests if r.done is not None]
         lat = np.array([r.done - r.arrival for r in done]) * 1e3
         upd = sum(r.K * self.ntr * self.meshes[r.mesh].mesh.n_wet_layers for r in done)
+        # per mesh class: latency, the wait for admission (arrival -> admitted) and the
+        # latency per step of the request (what K steps of that mesh take in the mix)
+        by_mesh = {}
+        for name in sorted({r.mesh for r in done}):
+            rs = [r for r in done if r.mesh == name]
+            lm = np.array([r.done - r.arrival for r in rs]) * 1e3
+            wait = np.array([r.admitted - r.arrival for r in rs]) * 1e3
+            per_step = np.array([(r.done - r.admitted) / r.K for r in rs]) * 1e3
+            by_mesh[name] = dict(completed=len(rs), p50_ms=float(np.percentile(lm, 50)),
+                                 p99_ms=float(np.percentile(lm, 99)),
+                                 wait_p99_ms=float(np.percentile(wait, 99)),
+                                 ms_per_step_p50=float(np.percentile(per_step, 50)))
         return dict(requests=n_total, completed=len(done), wall_s=wall, iterations=iters,
                     mean_batch=inst_total / max(iters, 1),
                     p50_ms=float(np.percentile(lat, 50)) if len(lat) else None,
                     p99_ms=float(np.percentile(lat, 99)) if len(lat) else None,
                     throughput_req_s=len(done) / wall, updates_per_s=upd / wall,
-                    nonfinite_requests=sum(1 for r in requests if r.nonfinite))
+                    nonfinite_requests=sum(1 for r in requests if r.nonfinite),
+                    by_mesh=by_mesh)
 
     def run_serial(self, requests: list[Request], time_limit: float | None = None) -> dict:
         """Baseline: the same requests one at a time through the single-instance C ABI

@@ -330,11 +330,14 @@ def test_chain_grad_uv_taylor_core2(torch):
     v = _d(torch, np.random.default_rng(11).normal(0.0, 0.002, uv.shape)) * em
     gv = float((guv * v).sum())
     r = {}
-    for h in (1e-1, 3e-2, 1e-2):
+    for h in (1e-2, 3e-3, 1e-3):
         Lh = chain_loss_and_grad(mesh, T0, uv + h * v, helem, hn, hnn, target, K, dt=dt,
                                  T_old0=To0)[0]
         r[h] = abs(Lh - L0 - h * gv)
         print(f"h={h:g} L(h)-L0={Lh - L0:.6e} h<g,v>={h * gv:.6e} r={r[h]:.3e}")
     assert abs(gv) > 0
-    assert r[1e-2] <= 0.1 * abs(1e-2 * gv), r
-    assert r[1e-2] <= r[1e-1] / 30.0, r
+    # measured on B200: r/|h<g,v>| = 14% at h = 1e-2 (v is as large as uv itself: at
+    # h = 1e-1 the remainder is 73%), falling with an observed order of 1.7-1.8; a wrong
+    # gradient leaves r/|h<g,v>| constant as h -> 0 (order 1)
+    assert r[1e-3] <= 0.05 * abs(1e-3 * gv), r
+    assert r[1e-3] <= r[1e-2] / 20.0, r
