@@ -49,6 +49,15 @@ __device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : 
 // AB2 extrapolation ttfAB = -0.6*T_old + 1.6*T (tracer_adv.py:59-66)
 __device__ __forceinline__ double ab2f(double T, double To) { return fma(kAbNew, T, kAbOld * To); }
 
+// The node kernels' neighbour loops load each slot record one slot ahead, so the next
+// slot's gathers do not wait behind its record (2-4% faster per node kernel on the
+// CORE2-size batched step)
+#define FCT_SLOT_BEGIN(e0, e1) \
+  int4 sl_nx = (e0) < (e1) ? __ldg(m.ne4 + (e0)) : make_int4(0, 0, 0, 0);
+#define FCT_SLOT_GET(j, e1) \
+  const int4 sl = sl_nx;    \
+  if ((j) + 1 < (e1)) sl_nx = __ldg(m.ne4 + (j) + 1);
+
 // a level clamped into [0, L - 1]: loads at clamped levels are in bounds and their values
 // are discarded by the predicates that follow
 __device__ __forceinline__ int kclamp(int k, int L) { return k < 0 ? 0 : (k >= L ? L - 1 : k); }
@@ -86,8 +95,9 @@ __device__ __forceinline__ void seg_node_lo(const Inst& in, int64_t si, int t0, 
 #pragma unroll
   for (int l = 0; l < LPT; ++l) fl_[l] = l < nk ? __ldg(m.nflags + rec.w + (k0 + l - nzmin)) : 0ull;
   const int e0 = rec.x, e1 = rec.x + int((pk >> 16) & 255u);
+  FCT_SLOT_BEGIN(e0, e1)
   for (int j = e0; j < e1; ++j) {
-    const int4 sl = __ldg(m.ne4 + j);
+    FCT_SLOT_GET(j, e1)
     const int jj = j - e0;
     const bool second = sl.x & 1;
     const double sg1 = second ? -1.0 : 1.0;   // the flux leaves the edge's first node
@@ -373,8 +383,9 @@ __device__ __forceinline__ void seg_node_limit(const Inst& in, int64_t si, bool 
     for (int l = 0; l < LPT; ++l)
       fl_[l] = l < nk ? __ldg(m.nflags + rec.w + (k0 + l - nzmin)) : 0ull;
     const int e0 = rec.x, e1 = rec.x + int((pk >> 16) & 255u);
+    FCT_SLOT_BEGIN(e0, e1)
     for (int j = e0; j < e1; ++j) {
-      const int4 sl = __ldg(m.ne4 + j);
+      FCT_SLOT_GET(j, e1)
       const int jj = j - e0;
       const double sg1 = (sl.x & 1) ? -1.0 : 1.0;   // adf_h leaves the edge's first node
       const uint32_t qo = lq(sl.y, L, 0), qe = lq(sl.x >> 1, L, 0);
@@ -516,8 +527,9 @@ __device__ __forceinline__ void seg_node_final(const Inst& in, int64_t si, int t
 #pragma unroll
   for (int l = 0; l < LPT; ++l) fl_[l] = l < nk ? __ldg(m.nflags + rec.w + (k0 + l - nzmin)) : 0ull;
   const int e0 = rec.x, e1 = rec.x + int((pk >> 16) & 255u);
+  FCT_SLOT_BEGIN(e0, e1)
   for (int j = e0; j < e1; ++j) {
-    const int4 sl = __ldg(m.ne4 + j);
+    FCT_SLOT_GET(j, e1)
     const int jj = j - e0;
     const bool second = sl.x & 1;
     const double sg1 = second ? -1.0 : 1.0;   // adf_h leaves the edge's first node
@@ -597,9 +609,11 @@ __device__ __forceinline__ void seg_node_final(const Inst& in, int64_t si, int t
 // slices, so together they read whole interleaved lines).
 // Resident 256-thread blocks per SM the compiler must fit, by the updates a thread
 // carries (registers capped accordingly: the gathers are latency-bound, so resident warps
-// pay more than the spills a cap may cost)
+// pay more than the spills a cap may cost). Measured on the CORE2-size batched step: one
+// block more per SM than 6/4/3/2/1 made it 5.5% faster (the autotuner then picks other
+// mappings), two more 1-9% slower.
 __host__ __device__ constexpr int seg_min_blocks(int ntr, int lpt) {
-  return ntr * lpt <= 1 ? 6 : ntr * lpt <= 2 ? 4 : ntr * lpt <= 4 ? 3 : ntr * lpt <= 8 ? 2 : 1;
+  return ntr * lpt <= 1 ? 7 : ntr * lpt <= 2 ? 5 : ntr * lpt <= 4 ? 4 : ntr * lpt <= 8 ? 3 : 2;
 }
 
 #define FCT_SEG_KERNEL(name, body)                                                       \
