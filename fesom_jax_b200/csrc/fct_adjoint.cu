@@ -48,6 +48,13 @@ struct FctTape {
 namespace {
 
 constexpr int B = 256;
+// Resident 256-thread blocks per SM the reverse kernels' register allocation must allow
+// (40 registers; 48 for r_edge). The kernels are latency-bound gathers, so resident warps
+// pay more than the spills the cap costs: on the CORE2-size 10-step chain the reverse
+// passes took 28.7 ms unconstrained (r_edge at 3 blocks), 23.3 ms at 4 blocks, 20.2 ms at
+// 6 (r_edge 5) and 20.0 ms at 8.
+constexpr int kRevMinBlocks = 6;
+constexpr int kRevEdgeMinBlocks = 5;
 
 __device__ __forceinline__ int64_t lane_index() {
   return int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -97,7 +104,7 @@ __device__ __forceinline__ double gvl_at(const DevMesh& m, const double* ghsc, i
 // ------------------------------------------------------------------ r_seed
 // T_new = T + d / hnn (d = del + T (hn - hnn)) and del holds the flux divergence times
 // dt / areasvol: stores the cotangent of a node's flux divergence, gdel * dt / sa.
-__global__ void __launch_bounds__(B) r_seed(Adj A) {
+__global__ void __launch_bounds__(B, kRevMinBlocks) r_seed(Adj A) {
   const Inst& in = A.in;
   const DevMesh& m = *in.m;
   const int64_t li = lane_index();
@@ -118,7 +125,7 @@ __global__ void __launch_bounds__(B) r_seed(Adj A) {
 // Dry levels keep T (T_new = T, ale_reconstruct): their outputs depend only on dT_new and
 // are final here, except dT at the level above a cavity's first layer, which the upwind
 // flux of interface nzmin also reaches (r_final writes it); gw_e is zero there.
-__global__ void __launch_bounds__(B) r_dry(Adj A) {
+__global__ void __launch_bounds__(B, kRevMinBlocks) r_dry(Adj A) {
   const Inst& in = A.in;
   const DevMesh& m = *in.m;
   const int64_t i = lane_index();
@@ -219,7 +226,7 @@ __device__ __forceinline__ void factor_cotangents(const Adj& A, int t, int n, in
 // Blocks of B threads cover B - 2 lanes plus one halo lane on each side: every thread
 // computes its lane's window cotangents (gtmax, gtmin) into shared memory, and the core
 // lanes spread them back over the window's three levels (lanes i-1, i, i+1).
-__global__ void __launch_bounds__(B) r_ratio_window(Adj A) {
+__global__ void __launch_bounds__(B, kRevMinBlocks) r_ratio_window(Adj A) {
   __shared__ double sx[B], sn[B];
   const Inst& in = A.in;
   const DevMesh& m = *in.m;
@@ -330,7 +337,7 @@ __global__ void __launch_bounds__(B) r_ratio_window(Adj A) {
 // the tied vertices, of the a3 shares of the vertices whose cluster bound the element
 // attains (tie counts come from the forward). Stored already divided by the element's
 // vertex tie count: the share of each attaining vertex.
-__global__ void __launch_bounds__(B) r_cluster(Adj A) {
+__global__ void __launch_bounds__(B, kRevMinBlocks) r_cluster(Adj A) {
   const Inst& in = A.in;
   const DevMesh& m = *in.m;
   const int64_t i = lane_index();
@@ -366,7 +373,7 @@ __global__ void __launch_bounds__(B) r_cluster(Adj A) {
 // ------- r_bounds_lo: a1 (max/min of LO and T) gathering the element shares of the
 // node's cells whose bound this node attains, then LO = numer / hnn and the seed terms
 // of T and LO.
-__global__ void __launch_bounds__(B) r_bounds_lo(Adj A) {
+__global__ void __launch_bounds__(B, kRevMinBlocks) r_bounds_lo(Adj A) {
   const Inst& in = A.in;
   const DevMesh& m = *in.m;
   const int64_t i = lane_index();
@@ -417,7 +424,7 @@ __global__ void __launch_bounds__(B) r_bounds_lo(Adj A) {
 }
 
 // ------------------ r_edge: adf_h = HO - LO flux; cotangents of the edge inputs
-__global__ void __launch_bounds__(B, 3) r_edge(Adj A) {
+__global__ void __launch_bounds__(B, kRevEdgeMinBlocks) r_edge(Adj A) {
   const Inst& in = A.in;
   const DevMesh& m = *in.m;
   const int64_t i = lane_index();
@@ -499,7 +506,7 @@ __device__ __forceinline__ void qr4c_depths(const Inst& in, const DevMesh& m, in
 
 // ------- r_gnode: cotangent of the node-average gradient (fill_up_dn_grad's node branch),
 // gathered over the node's edges in ascending edge id.
-__global__ void __launch_bounds__(B) r_gnode(Adj A) {
+__global__ void __launch_bounds__(B, kRevMinBlocks) r_gnode(Adj A) {
   const Inst& in = A.in;
   const DevMesh& m = *in.m;
   const int64_t i = lane_index();
@@ -533,7 +540,7 @@ __global__ void __launch_bounds__(B) r_gnode(Adj A) {
 // flux (gfv = -gf + gdiv terms); gw[j] is complete here (only interface j feeds it), and
 // the QR4C flux's terms for ttfAB at levels j, j-1, j-2 and j+1 are stored for r_final to
 // gather. Independent of the edge chain (it runs beside r_edge).
-__global__ void __launch_bounds__(B) r_vert(Adj A) {
+__global__ void __launch_bounds__(B, kRevMinBlocks) r_vert(Adj A) {
   const Inst& in = A.in;
   const DevMesh& m = *in.m;
   const int64_t i = lane_index();
@@ -610,7 +617,7 @@ __global__ void __launch_bounds__(B) r_vert(Adj A) {
 }
 
 // ---------------- r_tr: cotangent of the element gradients (up/dn use + node average)
-__global__ void __launch_bounds__(B) r_tr(Adj A) {
+__global__ void __launch_bounds__(B, kRevMinBlocks) r_tr(Adj A) {
   const Inst& in = A.in;
   const DevMesh& m = *in.m;
   const int64_t i = lane_index();
@@ -654,7 +661,7 @@ __global__ void __launch_bounds__(B) r_tr(Adj A) {
 // ascending interface order; the edge terms in ascending edge id. Also sums gw_e over the
 // tracers, and writes dT at the dry level above a cavity's first layer (only the
 // (w - |w|) upwind term of interface nzmin reaches it; r_seed wrote the other dry levels).
-__global__ void __launch_bounds__(B) r_final(Adj A) {
+__global__ void __launch_bounds__(B, kRevMinBlocks) r_final(Adj A) {
   const Inst& in = A.in;
   const DevMesh& m = *in.m;
   const int64_t li = lane_index();
@@ -729,7 +736,7 @@ __global__ void __launch_bounds__(B) r_final(Adj A) {
 }
 
 // -------------------------- r_uv: edge_vflux transposed, summed over tracers
-__global__ void __launch_bounds__(B) r_uv(Adj A) {
+__global__ void __launch_bounds__(B, kRevMinBlocks) r_uv(Adj A) {
   const Inst& in = A.in;
   const DevMesh& m = *in.m;
   const int64_t i = lane_index();

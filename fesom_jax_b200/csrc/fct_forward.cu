@@ -699,10 +699,11 @@ __device__ __forceinline__ void body_copy_dry(const Inst& in, int64_t i) {
 // read one contiguous run of S*NTR interleaved tracers together; in ``_1`` the slice is
 // blockIdx.y, so lanes stay contiguous along x within each tracer plane.
 // Resident 256-thread blocks per SM the compiler must fit (registers capped
-// accordingly): latency hiding pays more than the spills it costs (measured on the
-// CORE2-size batched step: +9% over the register-unconstrained build).
+// accordingly): latency hiding pays more than the spills it costs (one tracer, the
+// adjoint's taped forward on the CORE2-size mesh: 11.1 ms for 10 steps at 6 blocks,
+// 10.6 ms at 7, no gain at 8).
 template <int NTR>
-constexpr int kMinBlocks = NTR == 1 ? 6 : NTR == 2 ? 4 : NTR == 4 ? 3 : 1;
+constexpr int kMinBlocks = NTR == 1 ? 7 : NTR == 2 ? 5 : NTR == 4 ? 4 : 2;
 
 #define FCT_KERNEL_T(name, body)                                                        \
   template <int NTR>                                                                    \
