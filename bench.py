@@ -628,7 +628,8 @@ def run_serve(args, D: Dist) -> dict:
               "large": W.make_workload_mesh("large", seed=0)}
     dts = {"pi": 3600.0, "core2": 1800.0, "large": 600.0}
     eng = ServingEngine(meshes, dts, budget_bytes=150e9, device=D.local_rank, ntr=2,
-                        workspace_bytes=45e9, sigma={"large": 0.2})
+                        workspace_bytes=45e9, sigma={"large": 0.2},
+                        max_rounds=args.serve_rounds)
     out = {}
     reqs = poisson_requests(200.0, args.serve_seconds, seed=1 + D.rank)
     clocks = ClockSampler(gpu_index(D.local_rank))
@@ -766,7 +767,8 @@ def side_line(args, D: Dist, r: dict) -> dict:
     else:
         line["config"] = dict(workload="serve: Poisson 200 req/s, pi/CORE2/1.3M mix 0.6/0.3/0.1, "
                                        "K~U{1..50}, 20% adjoint, 150 GB budget, T+S",
-                              value_is="node-level updates/s served (saturated stream)")
+                              value_is="node-level updates/s served (saturated stream)",
+                              max_steps_per_iteration=args.serve_rounds)
         for k in ("saturated", "sustainable", "serial", "clocks"):
             line[k] = r[k]
     return line
@@ -801,6 +803,8 @@ def main():
                     default="batched")
     ap.add_argument("--serve-seconds", type=float, default=2.0,
                     help="serve: seconds of Poisson arrivals at 200 req/s")
+    ap.add_argument("--serve-rounds", type=int, default=16,
+                    help="serve: most steps a request takes per iteration (1 = lockstep)")
     ap.add_argument("--serve-limit", type=float, default=90.0,
                     help="serve: wall-clock cap per stream")
     ap.add_argument("--members", type=int, default=0)

@@ -418,11 +418,15 @@ struct FctServe {
   int max_instances = 0;
   double* arena = nullptr;
   int64_t arena_doubles = 0;
-  Inst* d_tab = nullptr;      // device instance table
-  Inst* h_tab = nullptr;      // pinned staging
+  Inst* d_tab = nullptr;      // device instance table (rewritten in stream order per call)
+  // pinned staging ring: a call fills the next slot and waits only for that slot's previous
+  // upload, so the host can enqueue several calls ahead of the GPU
+  static constexpr int kRing = 16;
+  Inst* h_tab[kRing] = {};
+  cudaEvent_t uploaded[kRing] = {};
+  bool pending[kRing] = {};   // an upload from h_tab[i] may still be in flight
+  int next = 0;
   unsigned long long* d_health = nullptr;   // non-finite counter of instances without one
-  cudaEvent_t uploaded = nullptr;
-  bool pending = false;       // an upload from h_tab may still be in flight
 };
 
 extern "C" {
@@ -450,10 +454,12 @@ int fct_serve_create(int device, int max_instances, int64_t workspace_bytes, Fct
     return fail(e, "serve workspace cudaMalloc");
   if ((e = cudaMalloc(&S->d_tab, size_t(max_instances) * sizeof(Inst))) != cudaSuccess)
     return fail(e, "serve table cudaMalloc");
-  if ((e = cudaMallocHost(&S->h_tab, size_t(max_instances) * sizeof(Inst))) != cudaSuccess)
-    return fail(e, "serve staging cudaMallocHost");
-  if ((e = cudaEventCreateWithFlags(&S->uploaded, cudaEventDisableTiming)) != cudaSuccess)
-    return fail(e, "cudaEventCreate");
+  for (int i = 0; i < FctServe::kRing; ++i) {
+    if ((e = cudaMallocHost(&S->h_tab[i], size_t(max_instances) * sizeof(Inst))) != cudaSuccess)
+      return fail(e, "serve staging cudaMallocHost");
+    if ((e = cudaEventCreateWithFlags(&S->uploaded[i], cudaEventDisableTiming)) != cudaSuccess)
+      return fail(e, "cudaEventCreate");
+  }
   if ((e = cudaMalloc(&S->d_health, sizeof(unsigned long long))) != cudaSuccess ||
       (e = cudaMemset(S->d_health, 0, sizeof(unsigned long long))) != cudaSuccess)
     return fail(e, "serve health counter");
@@ -467,11 +473,13 @@ int fct_serve_destroy(FctServe* S) {
   int prev = -1;
   cudaGetDevice(&prev);
   cudaSetDevice(S->device);
-  if (S->uploaded) {
-    cudaEventSynchronize(S->uploaded);
-    cudaEventDestroy(S->uploaded);
+  for (int i = 0; i < FctServe::kRing; ++i) {
+    if (S->uploaded[i]) {
+      cudaEventSynchronize(S->uploaded[i]);
+      cudaEventDestroy(S->uploaded[i]);
+    }
+    if (S->h_tab[i]) cudaFreeHost(S->h_tab[i]);
   }
-  if (S->h_tab) cudaFreeHost(S->h_tab);
   if (S->d_tab) cudaFree(S->d_tab);
   if (S->d_health) cudaFree(S->d_health);
   if (S->arena) cudaFree(S->arena);
@@ -514,8 +522,10 @@ int fct_serve_step(FctServe* S, const FctInstance* insts, const int32_t* phases,
   cudaSetDevice(S->device);
   auto restore = [&](int st) { if (prev >= 0) cudaSetDevice(prev); return st; };
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (S->pending) {   // the previous call's upload must have left the staging buffer
-    cudaError_t e = cudaEventSynchronize(S->uploaded);
+  const int slot = S->next;
+  Inst* h_tab = S->h_tab[slot];
+  if (S->pending[slot]) {   // that slot's previous upload must have left the staging buffer
+    cudaError_t e = cudaEventSynchronize(S->uploaded[slot]);
     if (e != cudaSuccess) return restore(cuda_error(e, "serve staging wait"));
   }
   int64_t off = 0;
@@ -523,7 +533,7 @@ int fct_serve_step(FctServe* S, const FctInstance* insts, const int32_t* phases,
     const FctInstance& q = insts[order[j]];
     const FctPlan* P = q.plan;
     const int p = ((phases[order[j]] % 3) + 3) % 3;
-    Inst& in = S->h_tab[j];
+    Inst& in = h_tab[j];
     in = Inst{};
     in.m = P->d_mesh;
     in.uv = q.uv; in.w_e = q.w_e; in.helem = q.helem;
@@ -544,12 +554,13 @@ int fct_serve_step(FctServe* S, const FctInstance* insts, const int32_t* phases,
       in.w_e = q.w_derived;
     }
   }
-  cudaError_t e = cudaMemcpyAsync(S->d_tab, S->h_tab, size_t(n) * sizeof(Inst),
+  cudaError_t e = cudaMemcpyAsync(S->d_tab, h_tab, size_t(n) * sizeof(Inst),
                                   cudaMemcpyHostToDevice, s);
   if (e != cudaSuccess) return restore(cuda_error(e, "serve table upload"));
-  e = cudaEventRecord(S->uploaded, s);
+  e = cudaEventRecord(S->uploaded[slot], s);
   if (e != cudaSuccess) return restore(cuda_error(e, "serve event record"));
-  S->pending = true;
+  S->pending[slot] = true;
+  S->next = (slot + 1) % FctServe::kRing;
   for (int j0 = 0; j0 < n;) {
     int j1 = j0;
     LaunchDims d{};

@@ -2,9 +2,11 @@
 
 Requests ask to advance one ensemble member, started from a seeded state on a given mesh,
 by K FCT steps (optionally followed by an adjoint). The engine keeps every admitted
-member's state resident in HBM and runs *iterations*: each iteration is ONE batched FCT
+member's state resident in HBM and runs *iterations*: each iteration is one batched FCT
 step (``fct_serve_step``: one launch per stage for all admitted members, any meshes)
-over every request still in flight. Requests that arrive while others are on the GPU are
+over every request still in flight, followed by extra rounds for the requests whose
+meshes are much cheaper per step than the largest one in flight (up to ``max_rounds``
+steps per iteration), so small requests are not held to the pace of the largest. Requests that arrive while others are on the GPU are
 admitted as soon as the HBM budget allows (FIFO), so their steps join the next iteration;
 a request leaves the batch after its K-th step and its memory is released once the GPU
 has finished with it. Adjoint requests then run the vector-Jacobian product of their last
@@ -62,6 +64,7 @@ class Request:
     result: object = None
     grad: object = None
     health: object = None   # device counter of non-finite T_new values of this request
+    inst: object = None     # its FctInstance while admitted
     nonfinite: int = 0      # its value after the run
 
 
@@ -105,7 +108,8 @@ class ServingEngine:
 
     def __init__(self, meshes: dict, dts: dict, budget_bytes: float = 150e9, device: int = 0,
                  ntr: int = 2, workspace_bytes: float | None = None, velocity_pool: int = 2,
-                 max_instances: int = 2048, adjoint_meshes=None, sigma: dict | None = None):
+                 max_instances: int = 2048, adjoint_meshes=None, sigma: dict | None = None,
+                 max_rounds: int = 16):
         from . import workloads as W
         torch = self.torch = _torch()
         self.device = device
@@ -140,6 +144,7 @@ class ServingEngine:
         _lib.check(self.L.fct_serve_create(device, max_instances, self.ws_bytes, C.byref(h)))
         self._h = h
         self.max_instances = max_instances
+        self.max_rounds = max(1, int(max_rounds))
         self.budget = int(budget_bytes)
         self.static_bytes = used + self.ws_bytes
         self.adj_stream = torch.cuda.Stream(self.dev)
@@ -236,6 +241,14 @@ class ServingEngine:
             ev.record(stream)
         return ev
 
+    def _rounds(self, active: list[Request]) -> list[int]:
+        """Steps each active request takes in this iteration: the ratio of the largest
+        active mesh's wet node layers to its own (the step cost scales with them), at
+        least 1, at most ``max_rounds`` and the steps it has left."""
+        wl = [self.meshes[r.mesh].mesh.n_wet_layers for r in active]
+        top = max(wl)
+        return [max(1, min(self.max_rounds, top // w, r.K - r.steps)) for r, w in zip(active, wl)]
+
     # ------------------------------------------------------------------ run
     def run(self, requests: list[Request], keep_results: bool = False, max_run_ahead: int = 2,
             time_limit: float | None = None) -> dict:
@@ -251,7 +264,7 @@ class ServingEngine:
         inflight: deque = deque()
         mem = self.static_bytes
         ws_active = 0
-        iters, inst_total = 0, 0
+        iters, inst_total, multi = 0, 0, 0
         # one non-finite counter per request (read after the run: no host sync per step)
         counters = torch.zeros(max(len(requests), 1), dtype=torch.int64, device=self.dev)
         for i, r in enumerate(requests):
@@ -277,6 +290,7 @@ class ServingEngine:
                     break
                 waiting.popleft()
                 r.state = self.init_state(r)
+                r.inst = self._instance(r)   # its buffers stay put until it leaves
                 r.nbytes, r.admitted = nb, now
                 mem += nb
                 ws_active += ws
@@ -289,24 +303,33 @@ class ServingEngine:
                     if keep_results:
                         p = r.K
                         r.result = r.state[(p + 1) % 3].permute(2, 0, 1).cpu().numpy()
-                    r.state = None
+                    r.state, r.inst = None, None
                     mem -= r.nbytes
                     n_done += 1
                 else:
                     keep.append(r)
             finishing = keep
             if active:
-                insts = (FctInstance * len(active))(*[self._instance(r) for r in active])
-                phases = (C.c_int32 * len(active))(*[r.steps for r in active])
-                _lib.check(self.L.fct_serve_step(self._h, insts, phases, len(active),
-                                                 C.c_void_p(int(stream.cuda_stream))))
+                # every active request advances one step; requests on meshes far cheaper
+                # per step than the dearest active one advance up to ``max_rounds`` steps
+                # (one fct_serve_step per round), so a pi-size request does not move at
+                # the pace of a 1.3M-node one sharing the iteration
+                rounds = self._rounds(active)
+                multi += max(rounds) > 1
+                for rd in range(max(rounds)):
+                    sub = [r for r, n in zip(active, rounds) if n > rd]
+                    insts = (FctInstance * len(sub))(*[r.inst for r in sub])
+                    phases = (C.c_int32 * len(sub))(*[r.steps for r in sub])
+                    _lib.check(self.L.fct_serve_step(self._h, insts, phases, len(sub),
+                                                     C.c_void_p(int(stream.cuda_stream))))
+                    for r in sub:
+                        r.steps += 1
+                    inst_total += len(sub)
                 ev = torch.cuda.Event(enable_timing=True)
                 ev.record(stream)
                 iters += 1
-                inst_total += len(active)
                 still = []
                 for r in active:
-                    r.steps += 1
                     if r.steps == r.K:
                         ws_active -= self.ws_need(r)
                         if r.adjoint and r.mesh in self.adjoint_meshes:
@@ -345,7 +368,7 @@ class ServingEngine:
                                  wait_p99_ms=float(np.percentile(wait, 99)),
                                  ms_per_step_p50=float(np.percentile(per_step, 50)))
         return dict(requests=n_total, completed=len(done), wall_s=wall, iterations=iters,
-                    mean_batch=inst_total / max(iters, 1),
+                    mean_batch=inst_total / max(iters, 1), multi_round_iterations=multi,
                     p50_ms=float(np.percentile(lat, 50)) if len(lat) else None,
                     p99_ms=float(np.percentile(lat, 99)) if len(lat) else None,
                     throughput_req_s=len(done) / wall, updates_per_s=upd / wall,

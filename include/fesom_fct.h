@@ -373,10 +373,11 @@ int fct_batch_fill_workspace(FctBatch* b, int byte, fct_stream_t stream);
  * Continuous batching: one FCT step for an arbitrary set of instances that changes from
  * call to call (requests joining and leaving), on any meshes. ``FctServe`` owns a
  * workspace arena (carved per call in instance order; a call whose instances need more
- * returns FCT_ERR_CAPACITY) and a device instance table uploaded from pinned host memory.
- * Instance i steps with rotation phase ``phases[i]`` (same convention as fct_batch_step).
- * Instances are launched in groups of one ntr and one mesh (each group's grid is sized
- * for its mesh). Calls on one FctServe must be ordered on one stream.
+ * returns FCT_ERR_CAPACITY) and a device instance table uploaded from pinned host memory
+ * (a ring of 16 staging buffers: a call waits on the host only for the upload of the call
+ * sixteen calls back). Instance i steps with rotation phase ``phases[i]`` (same convention as
+ * fct_batch_step). Instances are launched in groups of one ntr and one mesh (each group's
+ * grid is sized for its mesh). Calls on one FctServe must be ordered on one stream.
  */
 typedef struct FctServe FctServe;
 int fct_serve_create(int device, int max_instances, int64_t workspace_bytes, FctServe** out);

@@ -41,6 +41,8 @@ def test_results_same_alone_and_in_the_mix(engine):
     stats = engine.run(reqs, keep_results=True)
     assert stats["completed"] == len(reqs)
     assert stats["mean_batch"] > 1.5          # requests really shared iterations
+    # the 600-node requests took extra steps in iterations led by a pi-size request
+    assert stats["multi_round_iterations"] > 0
     for r in reqs:
         alone = _alone(engine, r)
         err = np.max(np.abs(r.result - alone)) / np.max(np.abs(alone))
