@@ -240,12 +240,37 @@ class Ensemble:
         e1.synchronize()
         return e0.elapsed_time(e1) / reps
 
-    def autotune(self, steps: int = 2, candidates=None, reps: int = 2) -> dict:
+    def autotune(self, steps: int = 2, candidates=None, reps: int = 2, cache=None) -> dict:
         """Pick the thread mapping of every fused stage: each (tracers, levels) per-thread
         candidate is timed stage by stage (profile_step) and each stage keeps its fastest;
         the per-stage choice is then timed against the best single mapping for all stages
         as ``steps``-step graph runs, and the faster stays (the member state advances while
-        tuning). Returns the per-candidate stage times and the choice."""
+        tuning). Returns the per-candidate stage times and the choice.
+
+        ``cache``: a :class:`fesom_jax_b200.tuning.TuningCache` (or ``True`` for the default
+        file). An entry for this GPU model, these meshes and this batch shape is applied
+        without timing; otherwise the choice is stored there."""
+        from . import tuning
+        if cache is True:
+            cache = tuning.TuningCache()
+        ck = None
+        if cache is not None:
+            ck = tuning.key("ensemble", tuning.gpu_name(self.device),
+                            {id(m.mesh): m.mesh for m in self.members}.values(),
+                            members=len(self.members),
+                            ntr=",".join(str(m.ntr) for m in self.members))
+            hit = cache.get(ck)
+            if hit:
+                for i, (c, lv) in enumerate(hit["stage_map"]):
+                    self.set_stage_mapping(i, c, lv)
+                return dict(cached=True, key=ck, stage_map=hit["stage_map"])
+        out = self._autotune(steps, candidates, reps)
+        if cache is not None:
+            cache.put(ck, dict(stage_map=[list(m) for m in self.stage_map],
+                               per_stage_ms=out["per_stage_ms"], uniform_ms=out["uniform_ms"]))
+        return out
+
+    def _autotune(self, steps: int, candidates, reps: int) -> dict:
         ntr_max = max(m.ntr for m in self.members)
         cands = [(c, lv) for c, lv in (candidates or self.MAPPINGS) if c <= ntr_max or c == 1]
         prof = {}

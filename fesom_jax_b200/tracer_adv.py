@@ -98,9 +98,24 @@ class FctPlan:
                                           int(levels_per_thread)))
 
     def autotune(self, args, dt: float, candidates=((1, 1), (1, 2), (1, 4), (2, 1), (2, 2),
-                                                    (2, 4)), reps: int = 20) -> dict:
+                                                    (2, 4)), reps: int = 20, cache=None) -> dict:
         """Time ``forward(*args, dt)`` (device tensors, the call to be tuned for) under each
-        (tracers, levels) per-thread mapping and keep the fastest; returns ``{"TxL": ms}``."""
+        (tracers, levels) per-thread mapping and keep the fastest; returns ``{"TxL": ms}``.
+        ``cache`` (a :class:`fesom_jax_b200.tuning.TuningCache`, or ``True`` for the default
+        file): an entry for this GPU model, mesh and tracer count is applied without
+        timing (returns ``{"cached": "TxL"}``); otherwise the choice is stored."""
+        from . import tuning
+        if cache is True:
+            cache = tuning.TuningCache()
+        ck = None
+        if cache is not None:
+            T = args[5]
+            ck = tuning.key("plan", tuning.gpu_name(self.device), [self.mesh],
+                            ntr=int(T.shape[0]) if T.dim() == 3 else 1)
+            hit = cache.get(ck)
+            if hit:
+                self.set_mapping(*hit["mapping"])
+                return {"cached": f"{hit['mapping'][0]}x{hit['mapping'][1]}"}
         torch = _torch()
         dev = torch.device("cuda", self.device)
         stream = torch.cuda.current_stream(dev)
@@ -119,6 +134,8 @@ class FctPlan:
             times[(c, lv)] = e0.elapsed_time(e1) / reps
         best = min(times, key=times.get)
         self.set_mapping(*best)
+        if cache is not None:
+            cache.put(ck, dict(mapping=list(best), ms=times[best]))
         return {f"{c}x{lv}": v for (c, lv), v in times.items()}
 
     def set_fused(self, fused: bool) -> None:

@@ -168,3 +168,19 @@ def test_batch_rejects_interleaved_arrays_beyond_2_32(torch, pi):
     st = L.fct_batch_create(arr, 1, 1 << 34, C.byref(h))
     assert st == -3 and not h.value
     assert "2^32" in L.fct_last_error().decode()
+
+
+def test_autotune_cache_applies_the_stored_mapping(torch, members, tmp_path):
+    """The first tuning of a batch shape stores its per-stage mapping; a second ensemble of
+    the same meshes and shape applies it without timing, and steps to the same bits."""
+    from fesom_jax_b200.tuning import TuningCache
+    cache = TuningCache(tmp_path / "tuning.json")
+    a = _ensemble(torch, members, 24 << 30)
+    first = a.autotune(steps=1, reps=1, cache=cache)
+    assert "cached" not in first
+    b = _ensemble(torch, members, 24 << 30)
+    second = b.autotune(steps=1, reps=1, cache=cache)
+    assert second["cached"] and [tuple(m) for m in second["stage_map"]] == list(a.stage_map)
+    assert b.stage_map == a.stage_map
+    a.close()
+    b.close()
