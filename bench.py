@@ -36,14 +36,14 @@ FALLBACK_HBM_GBS = 6650.0
 # DRAM bytes (read + write) per node-level update of the six kernels of the fused FCT step
 # (volume fluxes, LO, edge fluxes and their node-gradient lanes, limiter, final), from one
 # ncu capture of the small case of the batched workload (2 members x 8 tracers of the
-# CORE2-size mesh: 12.35 GB per FCT step / 48.76 M updates). Scaled to a launch by the
+# CORE2-size mesh: 12.53 GB per FCT step / 48.76 M updates). Scaled to a launch by the
 # updates it does.
-TRAFFIC_B_PER_UPDATE = 253.4
+TRAFFIC_B_PER_UPDATE = 257.0
 # Warp-instructions per node-level update of the same six kernels in the same capture
 # (smsp__inst_executed.sum / updates). The kernels are latency- and issue-limited rather
 # than HBM-bound, so the line also reports this issue-rate fraction beside the HBM one:
 # achieved warp-instructions/s against 148 SMs x 4 schedulers x the sampled SM clock.
-WARP_INST_PER_UPDATE = 40.5
+WARP_INST_PER_UPDATE = 46.0
 B200_SMS, SCHEDULERS_PER_SM = 148, 4
 
 
@@ -541,9 +541,13 @@ def run_adjoint(args, D: Dist) -> dict:
     main_mode = args.checkpoint   # the headline checkpointing; the other is timed beside it
     other = "recompute" if main_mode == "tape" else None
 
+    torch.cuda.empty_cache()   # hand back what earlier measurements left cached
+    tape = Tape(mesh, K, 1, D.local_rank) if main_mode == "tape" else None
+
     def grad(checkpoint=main_mode):
         return chain_loss_and_grad(mesh, T0, uv, helem, hn, hnn, target, K, dt=dt, T_old0=To0,
-                                   checkpoint=checkpoint)
+                                   checkpoint=checkpoint,
+                                   tape=tape if checkpoint == "tape" else None)
 
     def timed(fn, reps):
         for _ in range(max(args.warmup, 1)):
@@ -576,7 +580,8 @@ def run_adjoint(args, D: Dist) -> dict:
     if not args.no_fd:
         _, gT, gU, gTo = chain_loss_and_grad(mesh, T0, uv, helem, hn, hnn, target, K, dt=dt,
                                              T_old0=To0, checkpoint=main_mode,
-                                             return_gT_old=True)
+                                             return_gT_old=True,
+                                             tape=tape if main_mode == "tape" else None)
         TK = forward()[:, 0]
         av0 = torch.from_numpy(mesh.areasvol[:, 0].copy()).to(dev)
         terms = 2.0 * av0 * (TK - target.to(dev)) * TK
@@ -586,14 +591,17 @@ def run_adjoint(args, D: Dist) -> dict:
         v = d(np.random.default_rng(11).normal(0.0, 0.002, uv.shape)) * em
         gv = float((gU * v).sum())
         rem = {}
-        for h in (1e-1, 1e-2):
+        for h in (1e-2, 1e-3):
             Lh = chain_loss_and_grad(mesh, T0, uv + h * v, helem, hn, hnn, target, K, dt=dt,
-                                     T_old0=To0, checkpoint=main_mode)[0]
+                                     T_old0=To0, checkpoint=main_mode,
+                                     tape=tape if main_mode == "tape" else None)[0]
             rem[h] = abs(Lh - loss - h * gv)
         checks = dict(dot_T_rel_err=abs(lhs - rhs) / float(terms.abs().sum()),
-                      taylor_uv=dict(h=[1e-1, 1e-2], remainder=[rem[1e-1], rem[1e-2]],
-                                     first_order=[abs(1e-1 * gv), abs(1e-2 * gv)],
-                                     order=float(np.log10(rem[1e-1] / max(rem[1e-2], 1e-300)))))
+                      taylor_uv=dict(h=[1e-2, 1e-3], remainder=[rem[1e-2], rem[1e-3]],
+                                     first_order=[abs(1e-2 * gv), abs(1e-3 * gv)],
+                                     order=float(np.log10(rem[1e-2] / max(rem[1e-3], 1e-300)))))
+    if tape is not None:
+        tape.close()
     upd = K * mesh.n_wet_layers * D.world
     return dict(value=upd / t, t=t * args.steps, mesh=mesh, t_fwd=t_fwd, t_grad=t_grad,
                 cfg=dict(members=1, ntr=1, fct_steps=K, dt=dt),

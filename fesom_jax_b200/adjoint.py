@@ -44,6 +44,8 @@ def _bind(L):
                                  C.c_int, C.c_void_p]
     L.fct_compute_w_adjoint.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_int, C.c_void_p]
+    L.fct_adjoint_flush_uv.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                       C.c_void_p]
     L.fct_tape_bytes.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int64)]
     L.fct_tape_create.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int64,
                                   C.POINTER(C.c_void_p)]
@@ -52,15 +54,17 @@ def _bind(L):
                                     C.c_void_p, C.c_int, C.c_void_p]
     L.fct_tape_mark_recorded.argtypes = [C.c_void_p, C.c_int, C.c_double]
     for n in ("fct_plan_reserve_adjoint", "fct_adjoint", "fct_adjoint_ex",
-              "fct_compute_w_adjoint", "fct_tape_bytes", "fct_tape_create", "fct_tape_destroy",
+              "fct_compute_w_adjoint", "fct_adjoint_flush_uv", "fct_tape_bytes",
+              "fct_tape_create", "fct_tape_destroy",
               "fct_forward_taped", "fct_tape_mark_recorded"):
         getattr(L, n).restype = C.c_int
     L._adj_bound = True
     return L
 
 
-# accumulate bits of fct_adjoint_ex (include/fesom_fct.h)
-ACC_T, ACC_T_OLD, ACC_UV, ACC_W = 1, 2, 4, 8
+# accumulate bits of fct_adjoint_ex (include/fesom_fct.h); DEFER_UV: the step's volume-flux
+# cotangents go into the plan's running sum (fct_adjoint_flush_uv transposes it once)
+ACC_T, ACC_T_OLD, ACC_UV, ACC_W, DEFER_UV = 1, 2, 4, 8, 16
 
 
 def _fields(mesh: Mesh, uv, w_e, helem, hnode, hnode_new, T, T_old, T_new=None, Z3d=None,
@@ -148,7 +152,8 @@ class Tape:
 def _adjoint(plan, f, gT_new, dt, ntr, gT, gTo, guv, gw, tape=None, slot=0, acc=0, dev=None):
     torch = _torch()
     L = _bind(_lib.lib())
-    g = FctGrads(gT.data_ptr(), gTo.data_ptr(), guv.data_ptr(), gw.data_ptr())
+    g = FctGrads(gT.data_ptr(), gTo.data_ptr(), guv.data_ptr() if guv is not None else None,
+                 gw.data_ptr())
     with plan._lock:
         _lib.check(L.fct_adjoint_ex(plan.handle, C.byref(f), C.c_void_p(gT_new.data_ptr()),
                                     float(dt), ntr, C.byref(g),
@@ -265,13 +270,18 @@ def _tape_fits(torch, mesh: Mesh, steps: int, dev) -> bool:
 
 def chain_loss_and_grad(mesh: Mesh, T0, uv, helem, hnode, hnode_new, target, steps: int, *,
                         dt: float, T_old0=None, checkpoint: str = "auto",
-                        return_gT_old: bool = False):
+                        return_gT_old: bool = False, defer_uv: bool = True, tape=None):
     """Loss ``sum_n areasvol[n,0] * (T_K[n,0] - target_n)^2`` after ``steps`` FCT steps
     with ``w_e = compute_w(uv)`` inside the loss, and its gradients w.r.t. the initial
     ``T0`` and ``uv``. ``checkpoint``: ``"tape"`` keeps every step's intermediates
     (:class:`Tape`), ``"recompute"`` keeps only the K+1 states and recomputes each step
     inside its adjoint call, ``"auto"`` takes the tape when it fits in half the free
-    memory. The cotangents are accumulated in place (``fct_adjoint_ex``).
+    memory. The cotangents are accumulated in place (``fct_adjoint_ex``). With
+    ``defer_uv`` (the default) the steps' volume-flux cotangents are summed on the device
+    and transposed into the uv gradient once after the last step (uv and helem are the
+    same at every step), instead of once per step; the result agrees to rounding.
+    ``tape``: a :class:`Tape` of this mesh with at least ``steps`` slots, reused across
+    calls (it stays open); by default tape mode allocates one per call.
 
     Returns ``(loss, gT0, guv)``; ``T_old0`` defaults to ``T0`` (step-1 convention), and
     then ``gT0`` is the gradient through both inputs. With ``return_gT_old`` and an explicit
@@ -282,9 +292,15 @@ def chain_loss_and_grad(mesh: Mesh, T0, uv, helem, hnode, hnode_new, target, ste
     plan = get_plan(mesh, dev.index)
     if checkpoint not in ("auto", "tape", "recompute"):
         raise ValueError(f"checkpoint={checkpoint!r}: expected auto, tape or recompute")
-    if checkpoint == "auto":
+    own_tape = False
+    if tape is not None:
+        if tape.mesh is not mesh or tape.steps < steps or tape.device != dev.index:
+            raise ValueError("tape: needs this mesh, this device and >= steps slots")
+        checkpoint = "tape"
+    elif checkpoint == "auto":
         checkpoint = "tape" if _tape_fits(torch, mesh, steps, dev) else "recompute"
-    tape = Tape(mesh, steps, 1, dev.index) if checkpoint == "tape" else None
+    if tape is None and checkpoint == "tape":
+        tape, own_tape = Tape(mesh, steps, 1, dev.index), True
     if tape is None:
         _lib.check(_bind(_lib.lib()).fct_plan_reserve_adjoint(plan.handle, 1))
     try:
@@ -312,13 +328,18 @@ def chain_loss_and_grad(mesh: Mesh, T0, uv, helem, hnode, hnode_new, target, ste
             f = _fields(mesh, uv, w, helem, hnode, hnode_new, T_s, T_sm1)
             gTo = torch.empty_like(TK)
             # gT accumulates into carry: the cotangent of T_s is gT + carry
-            _adjoint(plan, f, lam, dt, 1, carry, gTo, guv, gw, tape, s,
-                     ACC_T | ACC_UV | ACC_W, dev)
+            _adjoint(plan, f, lam, dt, 1, carry, gTo, None if defer_uv else guv, gw, tape, s,
+                     ACC_T | ACC_W | (DEFER_UV if defer_uv else ACC_UV), dev)
             lam, carry = carry, gTo
         gT0 = lam + (carry if T_old0 is None else 0.0)
+        if defer_uv:
+            with plan._lock:
+                _lib.check(_bind(_lib.lib()).fct_adjoint_flush_uv(
+                    plan.handle, C.c_void_p(helem.data_ptr()), C.c_void_p(guv.data_ptr()), 1,
+                    _stream(torch, dev)))
         compute_w_vjp(mesh, gw, helem, guv)
     finally:
-        if tape is not None:
+        if own_tape:
             tape.close()
     if return_gT_old:
         if T_old0 is None:

@@ -79,6 +79,9 @@ __device__ __forceinline__ bool in_range(int k, unsigned r) {
 
 // accumulate flags of fct_adjoint_ex
 constexpr int kAccT = 1, kAccTo = 2, kAccUV = 4, kAccW = 8;
+// FCT_ADJ_DEFER_UV: the volume-flux cotangents go into the plan's running sum instead of
+// being transposed into guv by this call
+constexpr int kDeferUV = 16;
 
 struct Adj {
   Inst in;               // forward fields + forward workspace (recomputed or taped)
@@ -442,6 +445,7 @@ __global__ void __launch_bounds__(B, kRevEdgeMinBlocks) r_edge(Adj A) {
   const double vf = ld(in.ws.vflux + qe), avf = fabs(vf), s = sgn(vf);
   const double c1 = ld(m.ecoef + 2 * e), c2 = ld(m.ecoef + 2 * e + 1);
   const Rcp r6{6.0, 1.0 / 6.0, true};
+  double gvf_t = 0.0;   // summed over tracers in tracer order, as r_uv sums them
   for (int t = 0; t < in.ntr; ++t) {
     const int64_t o = t * in.ws.sN, oa = t * A.a.sN, oe = t * A.a.sEd;
     const double a = in.ws.adfh[t * in.ws.sEd + qe];
@@ -472,6 +476,7 @@ __global__ void __launch_bounds__(B, kRevEdgeMinBlocks) r_edge(Adj A) {
     double gvf = -0.5 * ((1.0 + s) * Tm1 + (1.0 - s) * Tm2) * gHO;
     gvf += -0.5 * (T1 * (1.0 + s) + T2 * (1.0 - s)) * gfl;
     A.a.gvf[oe + qe] = gvf;
+    gvf_t += gvf;
     // per-end terms for the node and element gathers: T1/T2 through the upwind flux;
     // ttfAB at the ends through Tm1 = A1 + X1 / 6 and Tm2 = A2 - X2 / 6 with
     // X = 2 (A2 - A1) + c1 gx + c2 gy (so the gradients' factors are c1 gX, c2 gX)
@@ -485,6 +490,7 @@ __global__ void __launch_bounds__(B, kRevEdgeMinBlocks) r_edge(Adj A) {
     A.a.gX1[oe + qe] = gX1;
     A.a.gX2[oe + qe] = gX2;
   }
+  if (A.acc & kDeferUV) A.a.gvf_sum[qe] += gvf_t;   // one thread per edge level: no race
 }
 
 // QR4C stencil depths of interface j (tracer_adv.py:228-238, 265-273)
@@ -736,24 +742,25 @@ __global__ void __launch_bounds__(B, kRevMinBlocks) r_final(Adj A) {
 }
 
 // -------------------------- r_uv: edge_vflux transposed, summed over tracers
-__global__ void __launch_bounds__(B, kRevMinBlocks) r_uv(Adj A) {
-  const Inst& in = A.in;
-  const DevMesh& m = *in.m;
-  const int64_t i = lane_index();
+// guv at element level i (= el * L + k) from volume-flux cotangents gvf [ntr x Ed*L, sEd
+// apart]: the element's three edges in its edge order
+__device__ __forceinline__ void uv_transpose(const DevMesh& m, const double* __restrict__ helem,
+                                             const double* __restrict__ gvfs, int ntr,
+                                             int64_t sEd, double* __restrict__ guv, int acc,
+                                             int64_t i) {
   const int L = m.L;
-  if (i >= int64_t(m.E) * L) return;
   int el, k;
   split_dense(i, L, el, k);
   double gU = 0.0, gV = 0.0;
   if (k >= ld(m.eul + el) && k < ld(m.enl + el)) {
-    const double h = ld(in.helem + i);
+    const double h = ld(helem + i);
     for (int r = 0; r < 3; ++r) {
       const int ent = ld(m.eedge + 3 * el + r);
       if (ent < 0) continue;
       const int e = ent >> 1;
       const double* cr = m.cross + 4 * int64_t(e);
       double gvf = 0.0;
-      for (int t = 0; t < in.ntr; ++t) gvf += A.a.gvf[t * A.a.sEd + lq(e, L, k)];
+      for (int t = 0; t < ntr; ++t) gvf += gvfs[t * sEd + lq(e, L, k)];
       if (ent & 1) {   // t2 = (V dx2 - U dy2) h
         gU += -gvf * ld(cr + 3) * h;
         gV += gvf * ld(cr + 2) * h;
@@ -763,13 +770,30 @@ __global__ void __launch_bounds__(B, kRevMinBlocks) r_uv(Adj A) {
       }
     }
   }
-  if (A.acc & kAccUV) {
-    A.guv[2 * i] += gU;
-    A.guv[2 * i + 1] += gV;
+  if (acc & kAccUV) {
+    guv[2 * i] += gU;
+    guv[2 * i + 1] += gV;
   } else {
-    A.guv[2 * i] = gU;
-    A.guv[2 * i + 1] = gV;
+    guv[2 * i] = gU;
+    guv[2 * i + 1] = gV;
   }
+}
+
+__global__ void __launch_bounds__(B, kRevMinBlocks) r_uv(Adj A) {
+  const int64_t i = lane_index();
+  if (i >= int64_t(A.in.m->E) * A.in.m->L) return;
+  uv_transpose(*A.in.m, A.in.helem, A.a.gvf, A.in.ntr, A.a.sEd, A.guv, A.acc, i);
+}
+
+// the same transpose of the deferred sum (fct_adjoint_flush_uv)
+__global__ void __launch_bounds__(B, kRevMinBlocks) r_uv_sum(const DevMesh* __restrict__ mp,
+                                                             const double* __restrict__ helem,
+                                                             const double* __restrict__ gvf_sum,
+                                                             double* __restrict__ guv,
+                                                             int acc) {
+  const int64_t i = lane_index();
+  if (i >= int64_t(mp->E) * mp->L) return;
+  uv_transpose(*mp, helem, gvf_sum, 1, 0, guv, acc, i);
 }
 
 // --------------------------------- compute_w reverse: w = mask * suffix-sum(div) / area
@@ -842,7 +866,7 @@ int reserve_adj_ws(FctPlan* P, int max_tracers) {
   }
   const int64_t sN = int64_t(P->N) * P->L, sE = int64_t(P->E) * P->L, sEd = int64_t(P->Ed) * P->L;
   const int64_t nd = int64_t(max_tracers) * (kAdjNodeFields * sN + kAdjEdgeFields * sEd +
-                                             kAdjElemFields * sE);
+                                             kAdjElemFields * sE) + sEd;
   double* p = nullptr;
   FCT_CUDA(cudaMalloc(&p, size_t(nd) * sizeof(double)));
   FCT_CUDA(cudaMemset(p, 0, size_t(nd) * sizeof(double)));
@@ -862,6 +886,7 @@ int reserve_adj_ws(FctPlan* P, int max_tracers) {
   double** elem[] = {&a.gax, &a.gan, &a.gtrx, &a.gtry};
   static_assert(sizeof(elem) / sizeof(elem[0]) == kAdjElemFields, "elem field count");
   for (double** f : elem) *f = take(sE);
+  a.gvf_sum = p;   // zeroed with the rest; fct_adjoint_flush_uv clears it after each use
   P->adj_tracers = max_tracers;
   return FCT_OK;
 }
@@ -1021,8 +1046,9 @@ int fct_adjoint_ex(FctPlan* P, const FctFields* f, const double* gT_new, double 
                    fct_stream_t stream) {
   if (!P || !f || !g || !gT_new) return set_error(FCT_ERR_INVALID, "NULL argument");
   if (ntr < 1) return set_error(FCT_ERR_INVALID, "ntr must be >= 1");
-  if (accumulate & ~(kAccT | kAccTo | kAccUV | kAccW))
+  if (accumulate & ~(kAccT | kAccTo | kAccUV | kAccW | kDeferUV))
     return set_error(FCT_ERR_INVALID, "unknown accumulate bits 0x%x", accumulate);
+  const bool defer_uv = accumulate & kDeferUV;
   if (ntr > P->adj_tracers)
     return set_error(FCT_ERR_CAPACITY, "ntr=%d exceeds the reserved adjoint workspace (%d); "
                      "call fct_plan_reserve_adjoint first", ntr, P->adj_tracers);
@@ -1042,7 +1068,7 @@ int fct_adjoint_ex(FctPlan* P, const FctFields* f, const double* gT_new, double 
   }
   int st = check_fields(f);
   if (st) return st;
-  if (!g->gT || !g->gT_old || !g->guv || !g->gw_e)
+  if (!g->gT || !g->gT_old || (!g->guv && !defer_uv) || !g->gw_e)
     return set_error(FCT_ERR_INVALID, "a gradient output pointer is NULL");
   if (!(dt > 0.0)) return set_error(FCT_ERR_INVALID, "dt must be positive");
   DeviceGuard guard(P->device);
@@ -1082,9 +1108,11 @@ int fct_adjoint_ex(FctPlan* P, const FctFields* f, const double* gT_new, double 
   r_vert<<<grid(hm.n_layer, B), B, 0, P->adj_side>>>(A);
   FCT_CUDA(cudaEventRecord(P->adj_ev[1], P->adj_side));
   r_edge<<<grid(hm.n_edge, B), B, 0, s>>>(A);
-  FCT_CUDA(cudaEventRecord(P->adj_ev[2], s));
-  FCT_CUDA(cudaStreamWaitEvent(P->adj_side, P->adj_ev[2], 0));
-  r_uv<<<grid(int64_t(P->E) * P->L, B), B, 0, P->adj_side>>>(A);
+  if (!defer_uv) {
+    FCT_CUDA(cudaEventRecord(P->adj_ev[2], s));
+    FCT_CUDA(cudaStreamWaitEvent(P->adj_side, P->adj_ev[2], 0));
+    r_uv<<<grid(int64_t(P->E) * P->L, B), B, 0, P->adj_side>>>(A);
+  }
   FCT_CUDA(cudaEventRecord(P->adj_ev[3], P->adj_side));
   r_gnode<<<grid(hm.n_layer, B), B, 0, s>>>(A);
   r_tr<<<grid(hm.n_elem, B), B, 0, s>>>(A);
@@ -1099,6 +1127,26 @@ int fct_adjoint_ex(FctPlan* P, const FctFields* f, const double* gT_new, double 
 int fct_adjoint(FctPlan* P, const FctFields* f, const double* gT_new, double dt, int ntr,
                 const FctGrads* g, fct_stream_t stream) {
   return fct_adjoint_ex(P, f, gT_new, dt, ntr, g, nullptr, 0, 0, stream);
+}
+
+int fct_adjoint_flush_uv(FctPlan* P, const double* helem, double* guv, int accumulate,
+                         fct_stream_t stream) {
+  if (!P || !helem || !guv) return set_error(FCT_ERR_INVALID, "NULL argument");
+  if (accumulate != 0 && accumulate != 1)
+    return set_error(FCT_ERR_INVALID, "accumulate must be 0 or 1");
+  if (P->adj_tracers < 1)
+    return set_error(FCT_ERR_CAPACITY, "call fct_plan_reserve_adjoint first");
+  DeviceGuard guard(P->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  PlanUse use(P, s);
+  if (use.status()) return use.status();
+  const int64_t n = int64_t(P->E) * P->L;
+  r_uv_sum<<<dim3(unsigned(std::max<int64_t>(1, (n + B - 1) / B))), B, 0, s>>>(
+      P->d_mesh, helem, P->aws.gvf_sum, guv, accumulate ? kAccUV : 0);
+  FCT_CUDA(cudaMemsetAsync(P->aws.gvf_sum, 0, size_t(P->aws.sEd) * sizeof(double), s));
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_error(e, "uv flush launch");
+  return use.release();
 }
 
 int fct_compute_w_adjoint(FctPlan* P, const double* gw, const double* helem, double* guv,

@@ -232,6 +232,9 @@ struct AdjWorkspace {
   // element [E, L] per tracer: the element bounds' shares (divided by the vertex tie
   // counts) and the element gradients
   double *gax, *gan, *gtrx, *gtry;
+  // [Ed, L], once (not per tracer): the volume-flux cotangents of the calls made with
+  // FCT_ADJ_DEFER_UV, summed over their tracers and over the calls
+  double* gvf_sum;
   int64_t sN, sE, sEd;
 };
 constexpr int kAdjNodeFields = 16, kAdjEdgeFields = 7, kAdjElemFields = 4;

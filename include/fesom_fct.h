@@ -244,6 +244,14 @@ int fct_tape_mark_recorded(FctTape* tape, int slot, double dt);
 #define FCT_ACC_T_OLD 2
 #define FCT_ACC_UV 4
 #define FCT_ACC_W 8
+/* Bit of fct_adjoint_ex: do not write guv (it may be NULL); add this step's volume-flux
+ * cotangents, summed over its tracers, into the plan's running sum instead. The uv
+ * cotangent is linear in them with coefficients that depend only on the mesh and helem, so
+ * for a chain of steps that share uv and helem one fct_adjoint_flush_uv after the last
+ * step gives the sum over the chain of what each call would have added to guv (to
+ * rounding: the sum is taken before the transpose). No reference counterpart (XLA sums
+ * the per-step cotangents of the shared uv itself). */
+#define FCT_ADJ_DEFER_UV 16
 /* fct_adjoint with options: ``tape`` (NULL: recompute the step; else the step recorded
  * in ``slot`` with the same fields and dt) and ``accumulate`` (FCT_ACC_* bits). The
  * cotangents are bit-identical to fct_adjoint's (plus the accumulated contents). */
@@ -275,6 +283,13 @@ typedef struct FctXlaOpaque {
 #define FCT_XLA_ADJ_STATUS 14
 void fct_xla_forward(void* stream, void** buffers, const char* opaque, size_t opaque_len);
 void fct_xla_adjoint(void* stream, void** buffers, const char* opaque, size_t opaque_len);
+
+/* guv (+)= the transpose of edge_vflux (fesom_jax/tracer_adv.py:69-93) applied to the
+ * running sum of the FCT_ADJ_DEFER_UV calls made since the last flush, with ``helem``
+ * [elem2D,nl] (the one those steps used); then clears the sum. ``accumulate`` = 0
+ * overwrites guv, 1 adds. Ordered like the other calls on the plan. */
+int fct_adjoint_flush_uv(FctPlan* plan, const double* helem, double* guv, int accumulate,
+                         fct_stream_t stream);
 
 /* Vector-Jacobian product of fct_compute_w (fesom_jax/ale.py:309-365) w.r.t. uv:
  * guv (+)= J^T gw, [elem2D,nl,2]; ``accumulate`` = 0 overwrites, 1 adds. */

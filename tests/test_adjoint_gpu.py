@@ -177,9 +177,9 @@ def test_adjoint_accumulate_bits(torch, pi):
         _adjoint(plan, _fields(pi, *args, T, To), gTn, DT, 1, *outs, None, 0, acc, T.device)
         for bit, o, b, r in zip((ACC_T, ACC_T_OLD, ACC_UV, ACC_W), outs, base, ref):
             assert torch.equal(o, b + r if acc & bit else r), (acc, bit)
-    with pytest.raises(RuntimeError, match="accumulate"):
+    with pytest.raises(RuntimeError, match="accumulate"):   # 16 is FCT_ADJ_DEFER_UV
         _adjoint(plan, _fields(pi, *args, T, To), gTn, DT, 1, *[b.clone() for b in base],
-                 None, 0, 16, T.device)
+                 None, 0, 32, T.device)
 
 
 def test_tape_rejects_misuse(torch, pi):
@@ -341,3 +341,42 @@ def test_chain_grad_uv_taylor_core2(torch):
     # gradient leaves r/|h<g,v>| constant as h -> 0 (order 1)
     assert r[1e-3] <= 0.05 * abs(1e-3 * gv), r
     assert r[1e-3] <= r[1e-2] / 20.0, r
+
+
+def test_chain_deferred_uv_equals_per_step_transpose(torch, pi):
+    """FCT_ADJ_DEFER_UV + fct_adjoint_flush_uv (the uv cotangent transposed once from the
+    sum of the steps' volume-flux cotangents) against a transpose per step: the T
+    gradients are the same bits, the uv gradient agrees to rounding; the flush clears the
+    sum and checks its arguments."""
+    import ctypes as C
+
+    from fesom_jax_b200 import _lib
+    from fesom_jax_b200.adjoint import _bind, chain_loss_and_grad
+    from fesom_jax_b200.tracer_adv import get_plan
+    f = I.make_fields(pi, seed=5, ab2=True, kind="white", sigma=0.02)
+    c = [_d(torch, x) for x in (f.helem, f.hnode, f.hnode_new)]
+    T0, To0, uv = _d(torch, f.tracers[0]), _d(torch, f.tracers_old[0]), _d(torch, f.uv)
+    target = torch.from_numpy(np.random.default_rng(8).normal(15.0, 3.0, pi.nod2D))
+    for mode in ("tape", "recompute"):
+        a = chain_loss_and_grad(pi, T0, uv, *c, target, 4, dt=DT, T_old0=To0, checkpoint=mode,
+                                defer_uv=True)
+        b = chain_loss_and_grad(pi, T0, uv, *c, target, 4, dt=DT, T_old0=To0, checkpoint=mode,
+                                defer_uv=False)
+        assert a[0] == b[0] and torch.equal(a[1], b[1])
+        # the per-step uv cotangents are larger than their sum and partly cancel, so the
+        # two summation orders differ by more than an ulp of the result (6e-13 measured on
+        # B200), far inside the 1e-10 of the comparison with the reference's autodiff
+        err = float((a[2] - b[2]).abs().max()) / float(b[2].abs().max())
+        assert err <= 1e-11, (mode, err)
+    # the sum was cleared by the last flush: flushing again adds nothing
+    L = _bind(_lib.lib())
+    plan = get_plan(pi, 0)
+    g = torch.zeros_like(uv)
+    s = C.c_void_p(int(torch.cuda.current_stream().cuda_stream))
+    assert L.fct_adjoint_flush_uv(plan.handle, C.c_void_p(c[0].data_ptr()),
+                                  C.c_void_p(g.data_ptr()), 1, s) == 0
+    torch.cuda.synchronize()
+    assert float(g.abs().max()) == 0.0
+    assert L.fct_adjoint_flush_uv(plan.handle, C.c_void_p(c[0].data_ptr()),
+                                  C.c_void_p(g.data_ptr()), 2, s) == -1
+    assert L.fct_adjoint_flush_uv(plan.handle, None, C.c_void_p(g.data_ptr()), 0, s) == -1
