@@ -472,12 +472,17 @@ def e2e_host(args, mesh, cfg, dev, per_thread=None) -> dict:
     h2d = sum(h[k].numel() * 8 for h in host for k in ("T", "T_old", "uv", "w_e"))
     d2h = sum(h["out"].numel() * 8 for h in host)
 
-    def one():
-        start = torch.cuda.Event()
-        start.record(main)
+    def one(first=True, last=True):
+        """One bench step: every member in, S FCT steps, out. The streams carry on from
+        one step to the next (each member's next copy in is ordered after its copy out on
+        its stream), so a run of steps is joined to the main stream only at its end."""
+        if first:
+            start = torch.cuda.Event()
+            start.record(main)
+            for st in streams:
+                st.wait_event(start)
         for i, (e, h) in enumerate(zip(ens, host)):
             st = streams[i % len(streams)]
-            st.wait_event(start)
             with torch.cuda.stream(st):
                 mb = e.members[0]
                 e.set_state(0, h["T"], h["T_old"], non_blocking=True, interleaved=True)
@@ -485,10 +490,11 @@ def e2e_host(args, mesh, cfg, dev, per_thread=None) -> dict:
                 mb.w_e.copy_(h["w_e"], non_blocking=True)
                 e.run(S, stream=st.cuda_stream)
                 h["out"].copy_(e.state_interleaved(0)[0], non_blocking=True)
-        for st in streams:
-            done = torch.cuda.Event()
-            done.record(st)
-            main.wait_event(done)
+        if last:
+            for st in streams:
+                done = torch.cuda.Event()
+                done.record(st)
+                main.wait_event(done)
 
     for _ in range(max(1, min(args.warmup, 2))):
         one()
@@ -497,8 +503,8 @@ def e2e_host(args, mesh, cfg, dev, per_thread=None) -> dict:
     reps = max(1, min(args.steps, 3))
     w0 = time.perf_counter()
     e0.record(main)
-    for _ in range(reps):
-        one()
+    for r in range(reps):
+        one(first=r == 0, last=r == reps - 1)
     e1.record(main)
     torch.cuda.synchronize()
     wall = time.perf_counter() - w0
