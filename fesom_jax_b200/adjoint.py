@@ -53,10 +53,11 @@ def _bind(L):
     L.fct_forward_taped.argtypes = [C.c_void_p, C.POINTER(_lib.FctFields), C.c_double, C.c_int,
                                     C.c_void_p, C.c_int, C.c_void_p]
     L.fct_tape_mark_recorded.argtypes = [C.c_void_p, C.c_int, C.c_double]
+    L.fct_tape_share_vflux.argtypes = [C.c_void_p]
     for n in ("fct_plan_reserve_adjoint", "fct_adjoint", "fct_adjoint_ex",
               "fct_compute_w_adjoint", "fct_adjoint_flush_uv", "fct_tape_bytes",
               "fct_tape_create", "fct_tape_destroy",
-              "fct_forward_taped", "fct_tape_mark_recorded"):
+              "fct_forward_taped", "fct_tape_mark_recorded", "fct_tape_share_vflux"):
         getattr(L, n).restype = C.c_int
     L._adj_bound = True
     return L
@@ -129,6 +130,12 @@ class Tape:
                 self.plan.handle, C.byref(f), float(dt), ntr, self._h, int(slot),
                 _stream(torch, T.device)))
         return out
+
+    def share_vflux(self) -> None:
+        """Every step recorded on this tape uses the same uv and helem: slot 0's forward
+        computes the edge volume fluxes and the other slots reuse them
+        (``fct_tape_share_vflux``; record slot 0 first)."""
+        _lib.check(_bind(_lib.lib()).fct_tape_share_vflux(self._h))
 
     def close(self) -> None:
         if getattr(self, "_h", None) is not None and self._h.value:
@@ -301,6 +308,8 @@ def chain_loss_and_grad(mesh: Mesh, T0, uv, helem, hnode, hnode_new, target, ste
         checkpoint = "tape" if _tape_fits(torch, mesh, steps, dev) else "recompute"
     if tape is None and checkpoint == "tape":
         tape, own_tape = Tape(mesh, steps, 1, dev.index), True
+    if tape is not None:
+        tape.share_vflux()   # uv and helem are the same at every step of the chain
     if tape is None:
         _lib.check(_bind(_lib.lib()).fct_plan_reserve_adjoint(plan.handle, 1))
     try:

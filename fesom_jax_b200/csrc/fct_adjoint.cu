@@ -43,6 +43,7 @@ struct FctTape {
   std::vector<Workspace> ws;
   std::vector<char> recorded;
   std::vector<double> dt;
+  bool share_vflux = false;   // every slot reads slot 0's volume fluxes (fct_tape_share_vflux)
 };
 
 namespace {
@@ -995,6 +996,13 @@ int fct_tape_create(FctPlan* P, int ntr, int steps, void* mem, int64_t bytes, Fc
   return FCT_OK;
 }
 
+int fct_tape_share_vflux(FctTape* T) {
+  if (!T) return set_error(FCT_ERR_INVALID, "tape is NULL");
+  T->share_vflux = true;
+  for (size_t s = 1; s < T->ws.size(); ++s) T->ws[s].vflux = T->ws[0].vflux;
+  return FCT_OK;
+}
+
 int fct_tape_destroy(FctTape* T) {
   if (!T) return FCT_OK;
   DeviceGuard g(T->plan->device);
@@ -1025,14 +1033,17 @@ int fct_forward_taped(FctPlan* P, const FctFields* f, double dt, int ntr, FctTap
   if (st) return st;
   if (!f->T_new) return set_error(FCT_ERR_INVALID, "T_new is NULL");
   if (!(dt > 0.0)) return set_error(FCT_ERR_INVALID, "dt must be positive");
+  if (tape->share_vflux && slot > 0 && !tape->recorded[0])
+    return set_error(FCT_ERR_INVALID, "a tape sharing its volume fluxes records slot 0 first");
   DeviceGuard g(P->device);
   Inst in = make_inst(P, f, dt, ntr, tape->ws[size_t(slot)]);
   in.nonfinite = P->d_health;
+  LaunchDims dims = unfused_dims(P, ntr);
+  dims.skip_vflux = tape->share_vflux && slot > 0;   // slot 0's fluxes are this step's
   {
     PlanUse use(P, static_cast<cudaStream_t>(stream));
     st = use.status();
-    if (!st) st = launch_forward(in, nullptr, 1, unfused_dims(P, ntr),
-                                 static_cast<cudaStream_t>(stream));
+    if (!st) st = launch_forward(in, nullptr, 1, dims, static_cast<cudaStream_t>(stream));
     if (!st) st = use.release();
   }
   if (st) return st;

@@ -824,8 +824,10 @@ int launch_forward_events(const Inst& single, const Inst* tab, int n, const Laun
         const int st = launch_compute_w_tab(tab, n, d.max_nodes, s);
         if (st) return st;
       }
-      if (tab) k_vflux_n<<<grid(d.max_edge), B, 0, s>>>(tab);
-      else k_vflux_1<<<grid(d.max_edge), B, 0, s>>>(single);
+      if (!d.skip_vflux) {
+        if (tab) k_vflux_n<<<grid(d.max_edge), B, 0, s>>>(tab);
+        else k_vflux_1<<<grid(d.max_edge), B, 0, s>>>(single);
+      }
     }
     mark();
     if (d.fused) {

@@ -42,6 +42,7 @@ struct LaunchDims {
   bool copy_dry;    // launch the dry-level copy
   bool any_vdiff = false;  // launch the implicit vertical diffusion after each chunk
   bool any_derive_w = false;  // derive w_e from uv (compute_w) before the step
+  bool skip_vflux = false;    // the workspace already holds this step's volume fluxes
   bool fused = true;  // fused stages (lean workspace); false: every stage kernel writes its
                       // intermediates (what the reverse pass reads)
   // fused (segment) stages: per stage (LO, edge, limiter, final) the most tracers and the

@@ -239,6 +239,13 @@ int fct_forward_taped(FctPlan* plan, const FctFields* fields, double dt, int ntr
  * recorded by fct_forward_taped with ``dt`` (through another tape over the same memory,
  * e.g. in a separate forward and backward call of a stateless custom-call handler). */
 int fct_tape_mark_recorded(FctTape* tape, int slot, double dt);
+/* Declares that every step recorded on this tape uses the same uv and helem (a multi-step
+ * loss with fixed velocities): slot 0's forward computes the edge volume fluxes
+ * (fesom_jax/tracer_adv.py:69-93) and the other slots read them instead of recomputing
+ * and storing their own. Slot 0 must be recorded first (FCT_ERR_INVALID otherwise);
+ * recording slot 0 again with other velocities changes every slot's fluxes. No reference
+ * counterpart (XLA may hoist the loop-invariant flux out of a scan by itself). */
+int fct_tape_share_vflux(FctTape* tape);
 /* Accumulate bits of fct_adjoint_ex: add into the output instead of overwriting it. */
 #define FCT_ACC_T 1
 #define FCT_ACC_T_OLD 2

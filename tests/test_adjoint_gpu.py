@@ -380,3 +380,32 @@ def test_chain_deferred_uv_equals_per_step_transpose(torch, pi):
     assert L.fct_adjoint_flush_uv(plan.handle, C.c_void_p(c[0].data_ptr()),
                                   C.c_void_p(g.data_ptr()), 2, s) == -1
     assert L.fct_adjoint_flush_uv(plan.handle, None, C.c_void_p(g.data_ptr()), 0, s) == -1
+
+
+def test_tape_shared_volume_fluxes(torch, pi):
+    """fct_tape_share_vflux: with uv and helem fixed, slots after the first reuse slot 0's
+    volume fluxes; the recorded steps and their adjoints are the same bits as without
+    sharing, and a sharing tape refuses to record another slot before slot 0."""
+    from fesom_jax_b200.adjoint import Tape, advect_one_fct_vjp
+    f = I.make_fields(pi, seed=9, ab2=True, kind="white", sigma=0.02)
+    args = [_d(torch, x) for x in (f.uv, f.w_e, f.helem, f.hnode, f.hnode_new)]
+    T, To = _d(torch, f.tracers[0]), _d(torch, f.tracers_old[0])
+    gTn = _d(torch, np.random.default_rng(13).normal(size=T.shape))
+    res = []
+    for share in (False, True):
+        with Tape(pi, steps=3) as tape:
+            if share:
+                tape.share_vflux()
+                with pytest.raises(RuntimeError, match="slot 0 first"):
+                    tape.forward(1, *args, T, To, DT)
+            states = [To, T]
+            for s in range(3):
+                states.append(tape.forward(s, *args, states[-1], states[-2], DT))
+            grads = [advect_one_fct_vjp(pi, *args, states[s + 1], states[s], gTn, dt=DT,
+                                        tape=tape, slot=s) for s in range(3)]
+        res.append((states, grads))
+    for a, b in zip(res[0][0], res[1][0]):
+        assert torch.equal(a, b)
+    for ga, gb in zip(res[0][1], res[1][1]):
+        for x, y in zip(ga, gb):
+            assert torch.equal(x, y)
