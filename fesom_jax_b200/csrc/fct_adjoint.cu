@@ -523,11 +523,14 @@ __global__ void __launch_bounds__(B, kRevMinBlocks) r_gnode(Adj A) {
   const int n = lane_ent(uint32_t(rec.x)), k = lane_lev(uint32_t(rec.x)), L = m.L;
   const uint32_t qn = lq(n, L, k);
   const int e0 = rec.y, e1 = rec.y + int((pk >> 16) & 255u);
+  // no edge of the node takes the node-average gradient at k (kGradBit): its cotangent is 0
+  const int nzmin = int(pk & 255u);
+  const bool grad = (__ldg(m.nflags + __ldg(m.nrec + n).w + (k - nzmin)) >> kGradBit) & 1ull;
   for (int t = 0; t < in.ntr; ++t) {
     const int64_t oa = t * A.a.sN, oe = t * A.a.sEd;
     double gx = 0.0, gy = 0.0;
 #pragma unroll 2
-    for (int j = e0; j < e1; ++j) {   // loads unconditional (in bounds), off edges selected away
+    for (int j = grad ? e0 : e1; j < e1; ++j) {   // loads unconditional (in bounds), off edges selected away
       const int4 sl = __ldg(m.ne4 + j);
       const int e = sl.x >> 1;
       const bool on = in_range(k, unsigned(sl.z)) && !in_range(k, unsigned(ld(m.etr + e)));
@@ -636,8 +639,6 @@ __global__ void __launch_bounds__(B, kRevMinBlocks) r_tr(Adj A) {
   const uint32_t qv[3] = {lq(ld(m.enodes + 3 * el), L, k),
                          lq(ld(m.enodes + 3 * el + 1), L, k),
                          lq(ld(m.enodes + 3 * el + 2), L, k)};
-  // the forward's (safe) node-average denominators of the three vertices
-  const double dd[3] = {in.ws.nden[qv[0]], in.ws.nden[qv[1]], in.ws.nden[qv[2]]};
   for (int t = 0; t < in.ntr; ++t) {
     const int64_t oa = t * A.a.sN, oe = t * A.a.sEd;
     double gx = 0.0, gy = 0.0;
@@ -653,8 +654,14 @@ __global__ void __launch_bounds__(B, kRevMinBlocks) r_tr(Adj A) {
     }
 #pragma unroll
     for (int v = 0; v < 3; ++v) {   // gnode(n) = sum_e a_e tr_e / den(n)
-      gx += A.a.ggnx[oa + qv[v]] * aw / dd[v];
-      gy += A.a.ggny[oa + qv[v]] * aw / dd[v];
+      // the cotangent is nonzero only at levels where an edge of the vertex takes the
+      // node-average gradient, the only levels whose denominator the forward stored
+      const double cx = A.a.ggnx[oa + qv[v]], cy = A.a.ggny[oa + qv[v]];
+      if (cx != 0.0 || cy != 0.0) {
+        const double dd = in.ws.nden[qv[v]];   // the forward's (safe) denominator
+        gx += cx * aw / dd;
+        gy += cy * aw / dd;
+      }
     }
     A.a.gtrx[t * A.a.sE + lq(el, L, k)] = gx;
     A.a.gtry[t * A.a.sE + lq(el, L, k)] = gy;

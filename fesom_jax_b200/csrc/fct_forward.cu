@@ -135,37 +135,41 @@ __device__ __forceinline__ void body_node_lo(const Inst& in, int64_t i, int t0, 
       lo[t] = valid ? divr(Tc[t] * hn + divr((div[t] + (fvk[t] - fvk1[t])) * dt, rav), rhn)
                     : 0.0;
     stn<NTR, IL>(in.ws.lo, qn, w0, in.ws.sN, in.wtg, lo);
-    // _node_avg_grad: area-weighted mean over the node's active elements
-    double nx[NTR], ny[NTR], den = 0.0;
+    // _node_avg_grad: area-weighted mean over the node's active elements, at the levels
+    // where an edge of the node takes it (kGradBit; its readers, the edge stage's and the
+    // reverse pass's node-gradient lanes, read no other level)
+    const int fw = __ldg(m.nrec + n).w;
+    if ((__ldg(m.nflags + fw + (k - nzmin)) >> kGradBit) & 1ull) {
+      double nx[NTR], ny[NTR], den = 0.0;
 #pragma unroll
-    for (int t = 0; t < NTR; ++t) nx[t] = ny[t] = 0.0;
-    const int c0 = rec.z, c1 = rec.z + int(pk >> 24);
-    for (int j = c0; j < c1; ++j) {
-      const int el = ld(m.nel_idx + j);
-      if (k >= ld(m.eul + el) && k < ld(m.enl + el)) {
-        const double a = ld(m.earea + el);
-        const uint32_t qe = lq(el, L, k);
-        double gx[NTR], gy[NTR];
-        ldn<NTR, IL>(in.ws.gx, qe, w0, in.ws.sE, in.wtg, gx);
-        ldn<NTR, IL>(in.ws.gy, qe, w0, in.ws.sE, in.wtg, gy);
+      for (int t = 0; t < NTR; ++t) nx[t] = ny[t] = 0.0;
+      const int c0 = rec.z, c1 = rec.z + int(pk >> 24);
+      for (int j = c0; j < c1; ++j) {
+        const int el = ld(m.nel_idx + j);
+        if (k >= ld(m.eul + el) && k < ld(m.enl + el)) {
+          const double a = ld(m.earea + el);
+          const uint32_t qe = lq(el, L, k);
+          double gx[NTR], gy[NTR];
+          ldn<NTR, IL>(in.ws.gx, qe, w0, in.ws.sE, in.wtg, gx);
+          ldn<NTR, IL>(in.ws.gy, qe, w0, in.ws.sE, in.wtg, gy);
 #pragma unroll
-        for (int t = 0; t < NTR; ++t) {
-          nx[t] += gx[t] * a;
-          ny[t] += gy[t] * a;
+          for (int t = 0; t < NTR; ++t) {
+            nx[t] += gx[t] * a;
+            ny[t] += gy[t] * a;
+          }
+          den += a;
         }
-        den += a;
       }
-    }
-  
-    const Rcp rdd = rcp(den > 0.0 ? den : 1.0);
-    if (w0 == 0) in.ws.nden[qn] = rdd.y;   // kept for the reverse pass (tracer independent)
+      const Rcp rdd = rcp(den > 0.0 ? den : 1.0);
+      if (w0 == 0) in.ws.nden[qn] = rdd.y;   // kept for the reverse pass (tracer independent)
 #pragma unroll
-    for (int t = 0; t < NTR; ++t) {
-      nx[t] = divr(nx[t], rdd);
-      ny[t] = divr(ny[t], rdd);
+      for (int t = 0; t < NTR; ++t) {
+        nx[t] = divr(nx[t], rdd);
+        ny[t] = divr(ny[t], rdd);
+      }
+      stn<NTR, IL>(in.ws.gnx, qn, w0, in.ws.sN, in.wtg, nx);
+      stn<NTR, IL>(in.ws.gny, qn, w0, in.ws.sN, in.wtg, ny);
     }
-    stn<NTR, IL>(in.ws.gnx, qn, w0, in.ws.sN, in.wtg, nx);
-    stn<NTR, IL>(in.ws.gny, qn, w0, in.ws.sN, in.wtg, ny);
   }
 
   // adv_flux_ver_ho (QR4C on ttfAB) minus the LO vertical flux (tracer_adv.py:241-295)

@@ -58,6 +58,8 @@ constexpr int kMaxSlots = 24;      // edges per node
 constexpr int kSlotWet = 24;       // bits 24..47: a cell of the slot's edge is wet
 constexpr int kOwnBit = 48;        // some cell of the node is wet at the level
 constexpr int kOffBit = 49;        // some cell of the node is dry at the level
+constexpr int kGradBit = 50;       // an edge of the node takes the node-average gradients
+                                   // at the level (MFCT outside its up/down-cell range)
 constexpr int kSegLevels[kSegVariants] = {1, 2, 4, 8};
 __host__ __device__ constexpr int seg_variant(int lpt) {
   return lpt == 1 ? 0 : lpt == 2 ? 1 : lpt == 4 ? 2 : 3;

@@ -405,7 +405,9 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   // the remaining edge lanes
   // and, per node layer, the flags of the node's edge slots at that level: bit j (slot j
   // has the level: its flux is counted), bit kSlotWet + j (a cell of slot j is wet there),
-  // kOwnBit (some cell of the node is wet) and kOffBit (some cell of the node is dry)
+  // kOwnBit (some cell of the node is wet), kOffBit (some cell of the node is dry) and
+  // kGradBit (an edge lane of the node at that level takes the node-average gradients:
+  // the only levels where the one-kernel-per-stage forward computes them)
   std::vector<int4> nrec(static_cast<size_t>(N));
   std::vector<unsigned long long> nflags;
   for (int n = 0; n < N; ++n) {
@@ -420,11 +422,13 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
                         int(nflags.size()));
     for (int k = std::max(nzmin[n], 0); k < std::min(nzmax[n], L); ++k) {
       unsigned long long f = 0;
-      bool own = false, off = false;
+      bool own = false, off = false, grad = false;
       for (int j = ne_off[n]; j < ne_off[n + 1]; ++j) {
         const int4 sl = ne4[j];
         const unsigned rg = unsigned(sl.z), tr = unsigned(sl.w);
         const bool on = k >= int(rg & 255u) && k < int((rg >> 8) & 255u);
+        const unsigned et = unsigned(etr[sl.x >> 1]);
+        grad = grad || (on && !(k >= int(et & 255u) && k < int((et >> 8) & 255u)));
         const bool has2 = ((tr >> 16) & 255u) != kNoCell;
         const bool c1 = k >= int(tr & 255u) && k < int((tr >> 8) & 255u);
         const bool c2 = has2 && k >= int((tr >> 16) & 255u) && k < int((tr >> 24) & 255u);
@@ -436,6 +440,7 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
       }
       f |= (unsigned long long)(own) << kOwnBit;
       f |= (unsigned long long)(off) << kOffBit;
+      f |= (unsigned long long)(grad) << kGradBit;
       nflags.push_back(f);
     }
   }
