@@ -313,6 +313,10 @@ def chain_loss_and_grad(mesh: Mesh, T0, uv, helem, hnode, hnode_new, target, ste
     if tape is None:
         _lib.check(_bind(_lib.lib()).fct_plan_reserve_adjoint(plan.handle, 1))
     try:
+        # loss weights and target on the device first: no host copy between the forward
+        # and the reverse pass, which would wait for the forward to finish
+        av0 = torch.from_numpy(mesh.areasvol[:, 0].copy()).to(dev)
+        tgt = target.to(dev)
         w = compute_w(mesh, uv, helem)
         states = [T_old0 if T_old0 is not None else T0, T0]   # [T_{-1}, T_0, T_1, ...]
         for s in range(steps):
@@ -323,10 +327,8 @@ def chain_loss_and_grad(mesh: Mesh, T0, uv, helem, hnode, hnode_new, target, ste
                 states.append(plan.forward(uv, w, helem, hnode, hnode_new, states[-1],
                                            states[-2], dt, stagewise=True))
         TK = states[-1]
-        av0 = torch.from_numpy(mesh.areasvol[:, 0].copy()).to(dev)
-        tgt = target.to(dev)
         diff = TK[:, 0] - tgt
-        loss = float((av0 * diff * diff).sum().item())
+        loss_t = (av0 * diff * diff).sum()   # read back after the reverse pass is queued
         lam = torch.zeros_like(TK)
         lam[:, 0] = 2.0 * av0 * diff
         guv = torch.zeros_like(uv)
@@ -347,6 +349,7 @@ def chain_loss_and_grad(mesh: Mesh, T0, uv, helem, hnode, hnode_new, target, ste
                     plan.handle, C.c_void_p(helem.data_ptr()), C.c_void_p(guv.data_ptr()), 1,
                     _stream(torch, dev)))
         compute_w_vjp(mesh, gw, helem, guv)
+        loss = float(loss_t.item())
     finally:
         if own_tape:
             tape.close()

@@ -476,7 +476,7 @@ __global__ void __launch_bounds__(B, kRevEdgeMinBlocks) r_edge(Adj A) {
     // HO = -0.5 ((vf + |vf|) Tm1 + (vf - |vf|) Tm2); fl = -0.5 (T1 (vf + |vf|) + T2 (vf - |vf|))
     double gvf = -0.5 * ((1.0 + s) * Tm1 + (1.0 - s) * Tm2) * gHO;
     gvf += -0.5 * (T1 * (1.0 + s) + T2 * (1.0 - s)) * gfl;
-    A.a.gvf[oe + qe] = gvf;
+    if (!(A.acc & kDeferUV)) A.a.gvf[oe + qe] = gvf;   // r_uv's input (not run when deferred)
     gvf_t += gvf;
     // per-end terms for the node and element gathers: T1/T2 through the upwind flux;
     // ttfAB at the ends through Tm1 = A1 + X1 / 6 and Tm2 = A2 - X2 / 6 with
