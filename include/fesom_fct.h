@@ -256,8 +256,9 @@ int fct_tape_share_vflux(FctTape* tape);
  * cotangent is linear in them with coefficients that depend only on the mesh and helem, so
  * for a chain of steps that share uv and helem one fct_adjoint_flush_uv after the last
  * step gives the sum over the chain of what each call would have added to guv (to
- * rounding: the sum is taken before the transpose). No reference counterpart (XLA sums
- * the per-step cotangents of the shared uv itself). */
+ * rounding: the sum is taken before the transpose). The sum lives in the plan's adjoint
+ * workspace: a fct_plan_reserve_adjoint that grows it clears the sum. No reference
+ * counterpart (XLA sums the per-step cotangents of the shared uv itself). */
 #define FCT_ADJ_DEFER_UV 16
 /* fct_adjoint with options: ``tape`` (NULL: recompute the step; else the step recorded
  * in ``slot`` with the same fields and dt) and ``accumulate`` (FCT_ACC_* bits). The
