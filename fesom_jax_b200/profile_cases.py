@@ -5,6 +5,7 @@ time or profile one kernel family on its own.
     python -m fesom_jax_b200.profile_cases compute_w   # k_compute_w   (ale.compute_w)
     python -m fesom_jax_b200.profile_cases vdiff       # k_vdiff       (tracer_diff, T and S)
     python -m fesom_jax_b200.profile_cases ice         # k_ice_*       (ice_adv.fct_solve)
+    python -m fesom_jax_b200.profile_cases wsplit      # k_vert_impl   (advect_one_fct, w_i)
 
 Every call is checked for finite output; the process prints one line with the mean
 CUDA-event time per call and exits 0.
@@ -16,7 +17,7 @@ import json
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["compute_w", "vdiff", "ice"])
+    ap.add_argument("case", choices=["compute_w", "vdiff", "ice", "wsplit"])
     ap.add_argument("--reps", type=int, default=3)
     args = ap.parse_args(argv)
 
@@ -49,6 +50,16 @@ def main(argv=None):
 
         def call():
             return list(impl_vert_diff(mesh, T, S, Kv, thick.hnode_new, dt=cfg["dt"]))
+    elif args.case == "wsplit":
+        # the split vertical velocity of tracer_adv.py:487-529: half of w_e explicit, half
+        # implicit (w_i), T and S in one call
+        from .tracer_adv import advect_one_fct
+        w_half = (0.5 * inp["w_e"]).contiguous()
+        T, To = inp["T"], inp["T_old"]
+
+        def call():
+            return [advect_one_fct(mesh, inp["uv"], w_half, thick.helem, thick.hnode,
+                                   thick.hnode_new, T, To, dt=cfg["dt"], w_i=w_half)[0]]
     else:
         a = torch.rand(N, generator=g, device=dev, dtype=torch.float64)
         m = 2.0 * torch.rand(N, generator=g, device=dev, dtype=torch.float64)
