@@ -418,21 +418,28 @@ def run_ours(args, D: Dist) -> dict | None:
     ens.close()   # the end-to-end run below builds its own ensemble
     del ens
     torch.cuda.empty_cache()
-    if D.rank == 0 and member_inputs[0] is not None:
-        inp = member_inputs[0]
-        if not args.no_cpu:
-            host = {k: (v.cpu().numpy() if hasattr(v, "cpu") else v) for k, v in inp.items()}
-        member_inputs.clear()
-        del inp
-        torch.cuda.empty_cache()
-        if not args.no_e2e:
-            out["e2e"] = e2e_host(args, mesh, cfg, dev, per_thread=tuned)
-        if not args.no_cpu:
-            out["cpu_baseline"] = cpu_oracle_rate(mesh, host, cfg["ntr"], cfg["dt"])
+    host = None
+    if D.rank == 0 and member_inputs[0] is not None and not args.no_cpu:
+        host = {k: (v.cpu().numpy() if hasattr(v, "cpu") else v)
+                for k, v in member_inputs[0].items()}
+    member_inputs.clear()
+    torch.cuda.empty_cache()
+    if not args.no_e2e:
+        # every rank streams its own members; the whole-job rate is all ranks' updates over
+        # the slowest rank's time, as for the headline value
+        e = e2e_host(args, mesh, cfg, dev, per_thread=tuned, rank=D.rank)
+        value_e, t_e = D.weak_value(e["updates"], e["t"], dev)
+        if D.rank == 0:
+            e.update(value=value_e, t_max_s=t_e, ranks=D.world,
+                     h2d_bytes_per_step=e["h2d_bytes_per_step"] * D.world,
+                     d2h_bytes_per_step=e["d2h_bytes_per_step"] * D.world)
+            out["e2e"] = e
+    if host is not None:
+        out["cpu_baseline"] = cpu_oracle_rate(mesh, host, cfg["ntr"], cfg["dt"])
     return out
 
 
-def e2e_host(args, mesh, cfg, dev, per_thread=None) -> dict:
+def e2e_host(args, mesh, cfg, dev, per_thread=None, rank: int = 0) -> dict:
     """The same metric through the public ensemble API with HOST buffers: every bench step
     copies each member's inputs (T, T_old, uv, w_e) from pinned host memory, runs the
     FCT steps and copies the final T back; copies are inside the timed region. Members are
@@ -447,7 +454,8 @@ def e2e_host(args, mesh, cfg, dev, per_thread=None) -> dict:
     streams = [torch.cuda.Stream(dev) for _ in range(3)]
     ens, host = [], []
     for i in range(nm):
-        inp = W.member_inputs_gpu(mesh, seed=500000 + i, ntr=cfg["ntr"], device=dev,
+        inp = W.member_inputs_gpu(mesh, seed=500000 + member_seed(rank, i), ntr=cfg["ntr"],
+                                  device=dev,
                                   thickness=thick, sigma=cfg["sigma"], n_vortices=cfg["n_vortices"],
                                   kind=cfg["velocity"])
         e = Ensemble(device=dev.index, workspace_budget=int(args.workspace_gb * (1 << 30)))
@@ -513,7 +521,7 @@ def e2e_host(args, mesh, cfg, dev, per_thread=None) -> dict:
     for e in ens:
         e.close()
     return dict(value=upd / t, unit=UNIT, h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h,
-                members=nm, steps=reps, wall_s=wall, streams=len(streams),
+                members=nm, steps=reps, wall_s=wall, streams=len(streams), updates=upd, t=t,
                 how="Ensemble API, pinned host buffers in/out every step, members pipelined "
                     "over 3 streams")
 
