@@ -507,6 +507,7 @@ def e2e_host(args, mesh, cfg, dev, per_thread=None, rank: int = 0) -> dict:
     for _ in range(max(1, min(args.warmup, 2))):
         one()
     torch.cuda.synchronize()
+    first_out = host[0]["out"].clone()   # every step starts from the same inputs
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     reps = max(1, min(args.steps, 3))
     w0 = time.perf_counter()
@@ -518,10 +519,15 @@ def e2e_host(args, mesh, cfg, dev, per_thread=None, rank: int = 0) -> dict:
     wall = time.perf_counter() - w0
     t = max(e0.elapsed_time(e1) / 1e3, 1e-9)
     upd = sum(e.info()["updates_per_step"] for e in ens) * S * reps
+    # the first member's host result of the timed steps is the warm-up's bit for bit, and
+    # every member's is finite
+    same = bool(torch.equal(first_out, host[0]["out"]))
+    finite = all(bool(torch.isfinite(h["out"]).all()) for h in host)
     for e in ens:
         e.close()
     return dict(value=upd / t, unit=UNIT, h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h,
                 members=nm, steps=reps, wall_s=wall, streams=len(streams), updates=upd, t=t,
+                outputs_repeat_bitwise=same, outputs_finite=finite,
                 how="Ensemble API, pinned host buffers in/out every step, members pipelined "
                     "over 3 streams")
 
@@ -907,10 +913,14 @@ def main():
     for k in ("plain", "e2e", "cpu_baseline", "side"):
         if k in r:
             line[k] = r[k]
-    failed = not r["finite"] or (r["gates"] is not None and not r["gates"]["passed"])
+    e2e_ok = "e2e" not in r or (r["e2e"]["outputs_finite"] and r["e2e"]["outputs_repeat_bitwise"])
+    failed = (not r["finite"] or (r["gates"] is not None and not r["gates"]["passed"])
+              or not e2e_ok)
     if failed:   # a state that went non-finite or failed a gate gives no throughput
         line["value"] = None
-        line["error"] = ("non-finite state" if not r["finite"] else "correctness gate failed")
+        line["error"] = ("non-finite state" if not r["finite"] else
+                         "end-to-end outputs not finite or not repeatable" if not e2e_ok else
+                         "correctness gate failed")
     print(json.dumps(line), flush=True)
     if failed:
         sys.exit(1)
