@@ -136,3 +136,29 @@ def test_plan_create_rejects_nodes_of_more_than_255_cells():
     st = _lib.lib().fct_plan_create(ctypes.byref(desc), 0, 1, ctypes.byref(plan))
     assert st == -1 and not plan.value
     assert b"more than 255" in _lib.lib().fct_last_error()
+
+
+def test_plan_create_rejects_nodes_of_more_than_24_edges():
+    """The segment kernels keep one flag bit per edge slot of a node layer: a fan of 30
+    triangles (a node with 30 edges) is refused on the host, before any CUDA call."""
+    from fesom_jax_b200 import _lib
+    from fesom_jax_b200.mesh import Mesh
+    from fesom_jax_b200.meshgen import _edges_from_triangles, derive, stretched_zbar
+    k = 30
+    ang = np.linspace(0.0, 2.0 * np.pi, k, endpoint=False)
+    nodes = np.concatenate([[[10.0, 0.0]], np.stack([10.0 + np.cos(ang), np.sin(ang)], 1)])
+    tri = np.array([[0, 1 + i, 1 + (i + 1) % k] for i in range(k)], np.int64)
+    zbar = stretched_zbar(6)
+    edges, edge_tri = _edges_from_triangles(tri, np.radians(nodes[:, 0]), np.radians(nodes[:, 1]))
+    raw = dict(nodes_deg=nodes, elem_nodes=tri.astype(np.int32), nl=6, zbar=zbar,
+               depth=np.full(k + 1, -zbar[-1]), nlevels_nod2D=np.full(k + 1, 6, np.int32),
+               nlevels=np.full(k, 6, np.int32), edges=edges, edge_tri=edge_tri, nod2D=k + 1,
+               elem2D=k, coast=np.zeros(k + 1, np.int32))
+    m = Mesh(**derive(raw), name="fan30")
+    m.validate()
+    keep = []
+    desc = _lib.mesh_desc(m, keep)
+    plan = ctypes.c_void_p()
+    st = _lib.lib().fct_plan_create(ctypes.byref(desc), 0, 1, ctypes.byref(plan))
+    assert st == -1 and not plan.value
+    assert b"at most 24" in _lib.lib().fct_last_error()
