@@ -224,7 +224,8 @@ class Ensemble:
         self.stage_map[int(stage)] = (int(tracers_per_thread), int(levels_per_thread))
 
     # (tracers per thread, levels per thread) tried by autotune
-    MAPPINGS = ((1, 1), (1, 2), (1, 4), (1, 8), (2, 1), (2, 2), (2, 4), (4, 1), (4, 2))
+    MAPPINGS = ((1, 1), (1, 2), (1, 4), (1, 8), (2, 1), (2, 2), (2, 4), (2, 8), (4, 1), (4, 2),
+                (4, 4))
     # the fused stages as profile_step names them, in mapping order
     STAGES = ("node_lo", "edge_adf", "node_factors", "node_final")
 
