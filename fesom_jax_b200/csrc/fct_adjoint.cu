@@ -132,13 +132,13 @@ __global__ void __launch_bounds__(B, kRevMinBlocks) r_seed(Adj A) {
 __global__ void __launch_bounds__(B, kRevMinBlocks) r_dry(Adj A) {
   const Inst& in = A.in;
   const DevMesh& m = *in.m;
-  const int64_t i = lane_index();
+  const int64_t li = lane_index();
   const int L = m.L;
-  if (i >= int64_t(m.N) * L) return;
-  int n, k;
-  split_dense(i, L, n, k);
+  if (li >= m.n_dry) return;
+  const uint32_t lane = ld(m.dry_lanes + li);
+  const int n = lane_ent(lane), k = lane_lev(lane);
+  const int64_t i = lq(n, L, k);
   const int nzmin = ld(m.nzmin + n), nzmax = ld(m.nzmax + n);
-  if (k >= nzmin && k < nzmax) return;
   const bool above_cavity = k + 1 == nzmin && nzmin < nzmax;
   const double gA = 0.0;
   for (int t = 0; t < in.ntr; ++t) {
@@ -929,6 +929,7 @@ LaunchDims unfused_dims(const FctPlan* P, int ntr) {
   LaunchDims d{};
   d.max_iface = P->hm.n_iface; d.max_layer = P->hm.n_layer; d.max_edge = P->hm.n_edge;
   d.max_elem = P->hm.n_elem; d.max_dense = int64_t(P->N) * P->L; d.max_nodes = P->N;
+  d.max_dry = P->hm.n_dry;
   d.ntr = ntr; d.chunk = 0; d.per_thread = 8; d.any_wi = false; d.copy_dry = true;
   d.fused = false;   // the reverse kernels read every stage's intermediates
   return d;
@@ -1116,7 +1117,7 @@ int fct_adjoint_ex(FctPlan* P, const FctFields* f, const double* gT_new, double 
   // pairs share the SMs.
   FCT_CUDA(cudaEventRecord(P->adj_ev[0], s));
   FCT_CUDA(cudaStreamWaitEvent(P->adj_side, P->adj_ev[0], 0));
-  r_dry<<<grid(int64_t(P->N) * P->L, B), B, 0, P->adj_side>>>(A);
+  r_dry<<<grid(hm.n_dry, B), B, 0, P->adj_side>>>(A);
   r_seed<<<grid(hm.n_layer, B), B, 0, s>>>(A);
   r_ratio_window<<<dim3(unsigned(std::max<int64_t>(1, (hm.n_layer + B - 3) / (B - 2)))), B, 0, s>>>(A);
   r_cluster<<<grid(hm.n_elem, B), B, 0, s>>>(A);

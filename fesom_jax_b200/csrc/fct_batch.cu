@@ -287,7 +287,7 @@ int fct_batch_prepare(FctBatch* B, fct_stream_t stream) {
   // phase 0 copies buf[1] -> buf[2]; phase 1 then copies buf[2] -> buf[0]
   for (int p = 0; p < 2 && !st; ++p)
     for (auto& g : B->groups)
-      if ((st = launch_copy_dry(g.d_tab[p], g.count, g.dims.max_dense, s))) break;
+      if ((st = launch_copy_dry(g.d_tab[p], g.count, g.dims.max_dry, s))) break;
   if (prev >= 0) cudaSetDevice(prev);
   return st;
 }

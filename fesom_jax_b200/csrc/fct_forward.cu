@@ -15,7 +15,7 @@
 //   zalesak_limit a4, b1, b2 (:407-451)                      -> k_node_factors (layer lanes)
 //   zalesak_limit b3 (:453-465), flux2dtracer_fct (:469-484),
 //   ale_reconstruct (:142-151)                               -> k_node_final (layer lanes)
-//   invalid lanes keep T (ale_reconstruct)                   -> k_copy_dry   (dense)
+//   invalid lanes keep T (ale_reconstruct)                   -> k_copy_dry   (dry lanes)
 //
 // Each thread owns one lane and NTR tracers (a compile-time chunk of the instance's
 // tracers, which share its velocities): mesh indices, geometry and velocity terms are
@@ -685,13 +685,11 @@ __device__ __forceinline__ void body_vdiff(const Inst& in, int64_t n, int t0, in
 template <bool IL>
 __device__ __forceinline__ void body_copy_dry(const Inst& in, int64_t i) {
   const DevMesh& m = *in.m;
-  const int64_t NL = int64_t(m.N) * m.L;
-  if (i >= NL) return;
-  int n, k;
-  split_dense(i, m.L, n, k);
-  if (k >= m.nzmin[n] && k < m.nzmax[n]) return;
+  if (i >= m.n_dry) return;
+  const uint32_t lane = __ldg(m.dry_lanes + i);
+  const uint32_t q = lq(lane_ent(lane), m.L, lane_lev(lane));
   for (int t = 0; t < in.ntr; ++t) {
-    const int64_t a = tix<IL>(uint32_t(i), t, in.tstride, in.tg);
+    const int64_t a = tix<IL>(q, t, in.tstride, in.tg);
     in.T_new[a] = in.T[a];
   }
 }
@@ -869,8 +867,8 @@ int launch_forward_events(const Inst& single, const Inst* tab, int n, const Laun
       if ((st = launch_seg_final(single, tab, n, d, c0, c1, s))) return st;
       if (d.any_vdiff) {   // epilogue: implicit vertical diffusion of this chunk, in place
         if (d.copy_dry) {  // the dry levels of T_new must hold T before it runs
-          if (tab) k_copy_dry_n<<<grid(d.max_dense), B, 0, s>>>(tab);
-          else k_copy_dry_1<<<grid(d.max_dense), B, 0, s>>>(single);
+          if (tab) k_copy_dry_n<<<grid(d.max_dry), B, 0, s>>>(tab);
+          else k_copy_dry_1<<<grid(d.max_dry), B, 0, s>>>(single);
         }
         FCT_STAGE(k_vdiff, d.max_nodes);
       }
@@ -896,8 +894,8 @@ int launch_forward_events(const Inst& single, const Inst* tab, int n, const Laun
     mark();
   }
   if (d.copy_dry && !stop_before_final && (chunk_sel < 0 || chunk_sel == nchunks - 1)) {
-    if (tab) k_copy_dry_n<<<grid(d.max_dense), B, 0, s>>>(tab);
-    else k_copy_dry_1<<<grid(d.max_dense), B, 0, s>>>(single);
+    if (tab) k_copy_dry_n<<<grid(d.max_dry), B, 0, s>>>(tab);
+    else k_copy_dry_1<<<grid(d.max_dry), B, 0, s>>>(single);
   }
   if (after) cudaEventRecord(after[kNumStages - 1], s);
   cudaError_t e = cudaGetLastError();
@@ -928,8 +926,8 @@ int launch_vdiff(const Inst& single, const LaunchDims& d, cudaStream_t s) {
   return e == cudaSuccess ? FCT_OK : cuda_error(e, "vertical diffusion launch");
 }
 
-int launch_copy_dry(const Inst* tab, int n, int64_t max_dense, cudaStream_t s) {
-  const dim3 g(unsigned(std::max<int64_t>(1, (max_dense + 255) / 256)), unsigned(n), 1);
+int launch_copy_dry(const Inst* tab, int n, int64_t max_dry, cudaStream_t s) {
+  const dim3 g(unsigned(std::max<int64_t>(1, (max_dry + 255) / 256)), unsigned(n), 1);
   k_copy_dry_n<<<g, 256, 0, s>>>(tab);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? FCT_OK : cuda_error(e, "copy_dry launch");

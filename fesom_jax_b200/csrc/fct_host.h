@@ -34,6 +34,7 @@ enum { kStageLo = 0, kStageEdge = 1, kStageLimit = 2, kStageFinal = 3 };
 // whose lane counts are bounded by the ``max_*`` arguments.
 struct LaunchDims {
   int64_t max_iface, max_layer, max_edge, max_elem, max_dense, max_nodes;
+  int64_t max_dry = 0;   // dry node levels (kept from T)
   int ntr;           // tracers per instance (every instance of a launch has the same)
   int chunk = 0;     // tracers whose intermediates share the workspace (0 = all ntr);
                      // stages run chunk by chunk
@@ -75,6 +76,7 @@ inline void dims_cover(LaunchDims& d, const FctPlan* P) {
   d.max_edge = std::max(d.max_edge, m.n_edge);
   d.max_elem = std::max(d.max_elem, m.n_elem);
   d.max_dense = std::max(d.max_dense, int64_t(P->N) * P->L);
+  d.max_dry = std::max(d.max_dry, P->hm.n_dry);
   d.max_nodes = std::max(d.max_nodes, int64_t(P->N));
   for (int v = 0; v < kSegVariants; ++v) {
     d.max_nseg[v] = std::max(d.max_nseg[v], m.n_nseg[v]);
@@ -110,7 +112,7 @@ int launch_forward_stages(const Inst& single, const LaunchDims& d, cudaStream_t 
 // fct_plan_reserve (declared in the public header) is used by the adjoint reservation.
 
 // Copy T's dry levels into T_new for ``n`` instances of ``tab`` (ignores Inst::copy_dry).
-int launch_copy_dry(const Inst* tab, int n, int64_t max_dense, cudaStream_t s);
+int launch_copy_dry(const Inst* tab, int n, int64_t max_dry, cudaStream_t s);
 // compute_w of every table instance with w_derived set (fct_producers.cu).
 int launch_compute_w_tab(const Inst* tab, int n, int64_t max_nodes, cudaStream_t s);
 // Implicit vertical diffusion alone (fct_vert_diff): single instance, tracer-major.

@@ -112,6 +112,7 @@ struct DevMesh {
   // lanes
   const uint32_t* iface_lanes;  int64_t n_iface;   // nodes, k in [nzmin, nzmax]
   const uint32_t* layer_lanes;  int64_t n_layer;   // nodes, k in [nzmin, nzmax)
+  const uint32_t* dry_lanes;    int64_t n_dry;     // nodes, k outside [nzmin, nzmax)
   const uint32_t* edge_lanes;   int64_t n_edge;    // edges, k in the union of cell layers
   const uint32_t* elem_lanes;   int64_t n_elem;    // elements, k in [eul, enl)
   // lane records of the fused kernels, one 16-byte load per thread:

@@ -345,12 +345,14 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   for (int k = 0; k < L - 1; ++k) Zp[k] = d->Z[k];
   Zp[L - 1] = d->Z[L - 2];
   // lanes
-  std::vector<uint32_t> iface, layer, edgel, eleml;
+  std::vector<uint32_t> iface, layer, edgel, eleml, dry;
   for (int n = 0; n < N; ++n) {
     for (int k = std::max(nzmin[n], 0); k <= std::min(nzmax[n], L - 1); ++k) {
       iface.push_back((uint32_t(n) << kLevelBits) | uint32_t(k));
       if (k < nzmax[n]) layer.push_back((uint32_t(n) << kLevelBits) | uint32_t(k));
     }
+    for (int k = 0; k < L; ++k)   // the levels that keep T (ale_reconstruct)
+      if (!(k >= nzmin[n] && k < nzmax[n])) dry.push_back((uint32_t(n) << kLevelBits) | uint32_t(k));
   }
   int64_t wet_elem = 0;
   for (int e = 0; e < E; ++e)
@@ -520,6 +522,7 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   size_t o_nelr = b.add(nelr.data(), nelr.size());
   size_t o_Zp = b.add(Zp.data(), L), o_zbar = b.add(d->zbar, L);
   size_t o_if = b.add(iface.data(), iface.size()), o_ly = b.add(layer.data(), layer.size());
+  size_t o_dry = b.add(dry.data(), std::max<size_t>(dry.size(), 1));
   size_t o_ed = b.add(edgel.data(), edgel.size()), o_el = b.add(eleml.data(), eleml.size());
   size_t o_if4 = b.add(iface4.data(), iface4.size()), o_ly4 = b.add(layer4.data(), layer4.size());
   size_t o_ed4 = b.add(edge4.data(), edge4.size());
@@ -575,6 +578,7 @@ static int plan_build(const FctMeshDesc* d, int device, FctPlan* P) {
   m.zbar = (const double*)(base + o_zbar);
   m.iface_lanes = (const uint32_t*)(base + o_if);  m.n_iface = int64_t(iface.size());
   m.layer_lanes = (const uint32_t*)(base + o_ly);  m.n_layer = int64_t(layer.size());
+  m.dry_lanes = (const uint32_t*)(base + o_dry);  m.n_dry = int64_t(dry.size());
   m.edge_lanes = (const uint32_t*)(base + o_ed);   m.n_edge = int64_t(edgel.size());
   m.elem_lanes = (const uint32_t*)(base + o_el);   m.n_elem = int64_t(eleml.size());
   m.iface4 = (const int4*)(base + o_if4);
