@@ -107,9 +107,10 @@ def test_xla_opaque_and_buffer_layout_agree_with_the_header():
 
 
 def test_adjoint_accumulate_bits_agree_with_the_header():
-    from fesom_jax_b200.adjoint import ACC_T, ACC_T_OLD, ACC_UV, ACC_W
-    assert (ACC_T, ACC_T_OLD, ACC_UV, ACC_W) == tuple(
-        _header_define(n) for n in ("FCT_ACC_T", "FCT_ACC_T_OLD", "FCT_ACC_UV", "FCT_ACC_W"))
+    from fesom_jax_b200.adjoint import ACC_T, ACC_T_OLD, ACC_UV, ACC_W, DEFER_UV
+    assert (ACC_T, ACC_T_OLD, ACC_UV, ACC_W, DEFER_UV) == tuple(
+        _header_define(n) for n in ("FCT_ACC_T", "FCT_ACC_T_OLD", "FCT_ACC_UV", "FCT_ACC_W",
+                                    "FCT_ADJ_DEFER_UV"))
 
 
 def test_plan_create_rejects_nodes_of_more_than_255_cells():
